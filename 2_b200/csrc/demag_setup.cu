@@ -1,0 +1,225 @@
+// demag_setup.cu -- the demag tensor in FP64 on the GPU and its transform.
+//
+// Kernel_Arne (src/mumax/modules/kernel_magnetostatic.go:30-181) integrates the field
+// of the face charges of a source cell over the volume of each destination cell with
+// a distance-adaptive number of points.  The reference runs it on the CPU in FP64 and
+// stores float32 (:170-173); here one GPU thread computes one (source, x, y, z) entry
+// in FP64 and the result stays FP64 through the transform (maxwell_convolution.go:
+// 313-410: FFT, keep the real part, scale by 1/prod(L)).  Only one octant of the
+// (even or odd) transformed tensor is kept, as FP32.
+#include <cmath>
+#include <cstdio>
+#include <vector>
+
+#include "mm_internal.h"
+
+namespace mm {
+
+__device__ __forceinline__ int wrap_i(int number, int max) {
+    number %= max;
+    return number < 0 ? number + max : number;
+}
+__device__ __forceinline__ double delta_d(int d) {
+    if (d < 0) d = -d;
+    if (d > 0) d -= 1;
+    return (double)d;
+}
+
+struct ArneArgs {
+    int size[3];
+    double cs[3];
+    int x1, y1, z1;
+    int nx_, ny_, nz_;     // loop extents
+    double accuracy;
+    double Lmin;
+    double* K;             // [6][L0][L1][L2]: xx yy zz yz xz xy
+    int accumulate;        // periodic images map several points to one index
+};
+
+// component index of (s, d) with s <= d in the order xx yy zz yz xz xy; -1 if s > d
+__device__ __forceinline__ int sym_q(int s, int d) {
+    if (s > d) return -1;
+    if (s == d) return s;
+    if (s == 1 && d == 2) return 3;
+    if (s == 0 && d == 2) return 4;
+    return 5;
+}
+
+__global__ void kernel_arne_kernel(ArneArgs A) {
+    const long long total = 3LL * A.nx_ * A.ny_ * A.nz_;
+    for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < total;
+         g += (long long)gridDim.x * blockDim.x) {
+        const int s = (int)(g / ((long long)A.nx_ * A.ny_ * A.nz_));
+        long long r = g % ((long long)A.nx_ * A.ny_ * A.nz_);
+        const int x = A.x1 + (int)(r / ((long long)A.ny_ * A.nz_));
+        r %= ((long long)A.ny_ * A.nz_);
+        const int y = A.y1 + (int)(r / A.nz_);
+        const int z = A.z1 + (int)(r % A.nz_);
+        const double* cs = A.cs;
+        const int u = s, v = (s + 1) % 3, w = (s + 2) % 3;
+        double R[3] = {(double)x * cs[0], (double)y * cs[1], (double)z * cs[2]};
+        double dx = delta_d(x) * cs[0], dy = delta_d(y) * cs[1], dz = delta_d(z) * cs[2];
+        double d = sqrt(dx * dx + dy * dy + dz * dz);
+        if (d == 0) d = A.Lmin;
+        double maxSize = d / A.accuracy;
+        int nv = (int)(fmax(cs[v] / maxSize, 1.) + 0.5);
+        int nw = (int)(fmax(cs[w] / maxSize, 1.) + 0.5);
+        int nx = (int)(fmax(cs[0] / maxSize, 1.) + 0.5);
+        int ny = (int)(fmax(cs[1] / maxSize, 1.) + 0.5);
+        int nz = (int)(fmax(cs[2] / maxSize, 1.) + 0.5);
+        nv *= 2;
+        nw *= 2;
+        const double scale = 1 / (double)(nv * nw * nx * ny * nz);
+        const double charge = cs[v] * cs[w] * scale;
+        const double pu1 = cs[u] / 2., pu2 = -pu1;
+        const double fourpi = 4.0 * 3.14159265358979323846;
+        double B[3] = {0, 0, 0};
+        double pole[3];
+        for (int i = 0; i < nv; i++) {
+            pole[v] = -(cs[v] / 2.) + cs[v] / (double)(2 * nv) + (double)i * (cs[v] / (double)nv);
+            for (int j = 0; j < nw; j++) {
+                pole[w] = -(cs[w] / 2.) + cs[w] / (double)(2 * nw) + (double)j * (cs[w] / (double)nw);
+                for (int a = 0; a < nx; a++) {
+                    double rx = R[0] - cs[0] / 2. + cs[0] / (double)(2 * nx) + (cs[0] / (double)nx) * (double)a;
+                    for (int b = 0; b < ny; b++) {
+                        double ry = R[1] - cs[1] / 2. + cs[1] / (double)(2 * ny) + (cs[1] / (double)ny) * (double)b;
+                        for (int c = 0; c < nz; c++) {
+                            double rz = R[2] - cs[2] / 2. + cs[2] / (double)(2 * nz) + (cs[2] / (double)nz) * (double)c;
+                            pole[u] = pu1;
+                            double X0 = rx - pole[0], Y0 = ry - pole[1], Z0 = rz - pole[2];
+                            double rr = sqrt(X0 * X0 + Y0 * Y0 + Z0 * Z0);
+                            double qr = charge / (fourpi * rr * rr * rr);
+                            double bx = X0 * qr, by = Y0 * qr, bz = Z0 * qr;
+                            pole[u] = pu2;
+                            X0 = rx - pole[0]; Y0 = ry - pole[1]; Z0 = rz - pole[2];
+                            rr = sqrt(X0 * X0 + Y0 * Y0 + Z0 * Z0);
+                            qr = -charge / (fourpi * rr * rr * rr);
+                            B[0] += (bx + X0 * qr);
+                            B[1] += (by + Y0 * qr);
+                            B[2] += (bz + Z0 * qr);
+                        }
+                    }
+                }
+            }
+        }
+        const int xw = wrap_i(x, A.size[0]), yw = wrap_i(y, A.size[1]), zw = wrap_i(z, A.size[2]);
+        const long long NL = (long long)A.size[0] * A.size[1] * A.size[2];
+        const long long idx = ((long long)xw * A.size[1] + yw) * A.size[2] + zw;
+        for (int dd = 0; dd < 3; dd++) {
+            int q = sym_q(s, dd);
+            if (q < 0) continue;
+            if (A.accumulate) atomicAdd(A.K + q * NL + idx, B[dd]);
+            else A.K[q * NL + idx] = B[dd];
+        }
+    }
+}
+
+__global__ void maxabs_kernel(const double* a, long long n, unsigned long long* out) {
+    double m = 0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        m = fmax(m, fabs(a[i]));
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
+}
+
+// real part of the transformed component, one octant, scaled, as float
+__global__ void extract_octant_kernel(const double2* spec, int L0, int L1, int hp, int kd0, int kd1, int kd2,
+                                      double scale, float* out) {
+    const long long n = (long long)kd0 * kd1 * kd2;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        int kx = (int)(i % kd2);
+        long long r = i / kd2;
+        int ky = (int)(r % kd1);
+        int kz = (int)(r / kd1);
+        out[i] = (float)(spec[((long long)kz * L1 + ky) * hp + kx].x * scale);
+    }
+}
+
+#define CK(...)                                                                                 \
+    do {                                                                                        \
+        cudaError_t e_ = (__VA_ARGS__);                                                                \
+        if (e_ != cudaSuccess) {                                                                \
+            snprintf(err, errlen, "%s: %s (%s:%d)", #__VA_ARGS__, cudaGetErrorString(e_), __FILE__, __LINE__); \
+            goto fail;                                                                          \
+        }                                                                                       \
+    } while (0)
+
+// Builds khat [6][kd0][kd1][kd2] (FP32, device, caller-allocated) and nz[6].
+int build_demag_kernel(const int L[3], const double cell[3], const int pbc[3], int accuracy, float* khat,
+                       const int kd[3], int nz[6], cudaStream_t st, char* err, int errlen) {
+    const long long NL = (long long)L[0] * L[1] * L[2];
+    const int M = L[2] / 2;
+    const int hp = M + 1;
+    double* K = nullptr;
+    double2* spec = nullptr;
+    unsigned long long* dmax = nullptr;
+    unsigned long long hmax[7];
+    int rc = MM_ERR_CUDA;
+    {
+        ArneArgs A;
+        for (int i = 0; i < 3; i++) { A.size[i] = L[i]; A.cs[i] = cell[i]; }
+        int x1 = -(L[0] - 1) / 2, x2 = L[0] / 2 - 1;
+        int y1 = -(L[1] - 1) / 2, y2 = L[1] / 2 - 1;
+        int z1 = -(L[2] - 1) / 2, z2 = L[2] / 2 - 1;
+        if (L[0] == 1 && pbc[0] == 0) x2 = 0;
+        x1 *= (pbc[0] + 1); x2 *= (pbc[0] + 1);
+        y1 *= (pbc[1] + 1); y2 *= (pbc[1] + 1);
+        z1 *= (pbc[2] + 1); z2 *= (pbc[2] + 1);
+        A.x1 = x1; A.y1 = y1; A.z1 = z1;
+        A.nx_ = x2 - x1 + 1; A.ny_ = y2 - y1 + 1; A.nz_ = z2 - z1 + 1;
+        A.accuracy = (double)(accuracy > 0 ? accuracy : 6);
+        A.Lmin = fmin(cell[0], fmin(cell[1], cell[2]));
+        A.accumulate = (pbc[0] || pbc[1] || pbc[2]) ? 1 : 0;
+        CK(cudaMalloc(&K, sizeof(double) * 6 * NL));
+        CK(cudaMemsetAsync(K, 0, sizeof(double) * 6 * NL, st));
+        A.K = K;
+        long long total = 3LL * A.nx_ * A.ny_ * A.nz_;
+        int blocks = (int)std::min<long long>((total + 127) / 128, 148LL * 64);
+        kernel_arne_kernel<<<blocks, 128, 0, st>>>(A);
+        CK(cudaGetLastError());
+        CK(cudaMalloc(&dmax, sizeof(unsigned long long) * 7));
+        CK(cudaMemsetAsync(dmax, 0, sizeof(unsigned long long) * 7, st));
+        for (int q = 0; q < 6; q++) maxabs_kernel<<<296, 256, 0, st>>>(K + q * NL, NL, dmax + q);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(hmax, dmax, sizeof(unsigned long long) * 6, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        double cmax[6], gmax = 0;
+        for (int q = 0; q < 6; q++) {
+            memcpy(&cmax[q], &hmax[q], sizeof(double));
+            gmax = fmax(gmax, cmax[q]);
+        }
+        // maxwell_convolution.go:412-418: a component is zero if its max is below
+        // 1e-5 of the largest element of the whole tensor
+        for (int q = 0; q < 6; q++) nz[q] = (gmax > 0 && cmax[q] / gmax >= 1e-5) ? 1 : 0;
+        CK(cudaMalloc(&spec, sizeof(double2) * (size_t)L[0] * L[1] * hp));
+        const double scale = 1.0 / (double)NL;
+        const long long oct = (long long)kd[0] * kd[1] * kd[2];
+        for (int q = 0; q < 6; q++) {
+            if (!nz[q]) {
+                CK(cudaMemsetAsync(khat + q * oct, 0, sizeof(float) * oct, st));
+                continue;
+            }
+            PP none = {nullptr, nullptr, 0};
+            CK(launch_xfwd<double2, double>(M, K + q * NL, none, nullptr, spec, L[0] * L[1], L[0], L[1], L[1], L[2],
+                                            L[2], hp, nullptr, 0, st));
+            if (L[1] > 1)
+                CK(launch_colfft<double2>(L[1], -1, spec, hp, L[0], (long long)L[1] * hp, hp, L[1], L[1], nullptr, 0,
+                                          st));
+            if (L[0] > 1)
+                CK(launch_colfft<double2>(L[0], -1, spec, hp, L[1], hp, (long long)L[1] * hp, L[0], L[0], nullptr, 0,
+                                          st));
+            extract_octant_kernel<<<296, 256, 0, st>>>(spec, L[0], L[1], hp, kd[0], kd[1], kd[2], scale,
+                                                       khat + q * oct);
+            CK(cudaGetLastError());
+        }
+        CK(cudaStreamSynchronize(st));
+        rc = MM_OK;
+    }
+fail:
+    if (K) cudaFree(K);
+    if (spec) cudaFree(spec);
+    if (dmax) cudaFree(dmax);
+    return rc;
+}
+
+}  // namespace mm

@@ -1,0 +1,165 @@
+// mm_internal.h -- internal structures shared by the kernels and the host runtime.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/mm_b200.h"
+
+namespace mm {
+
+// Spectrum layout (the half-spectrum buffer that the convolution passes work in):
+//   S[((c*N0 + z)*L1 + y)*hp + kx],  c in 0..2, z < N0, y < L1, kx < h = L2/2+1
+// Only z < N0 rows exist: the z transform is done forward, multiplied and inverted
+// inside one pass, so the padded z half never reaches HBM.
+struct ConvGeom {
+    int n[3];     // grid (internal order)
+    int L[3];     // padded sizes
+    int M;        // L2/2 : complex length of the row transform
+    int h;        // L2/2 + 1 : stored half-spectrum columns
+    int hp;       // row pitch of S in complex elements
+    int kd[3];    // stored kernel octant: L0/2+1, L1/2+1, L2/2+1
+    long long N;  // cells
+};
+
+// Device-side control block of the time stepper.  One per plan; all kernels of an
+// attempt read it, the controller kernel writes it.  Every decision (accept/reject,
+// dt, done) is made on the device so that attempts can be queued without host syncs.
+struct DevCtl {
+    double t, dt;            // time of the accepted state, dt for the next attempt
+    double t_end;            // stop when t >= t_end
+    long long step_end;      // stop when step >= step_end
+    double maxerr, mindt, maxdt, headroom;
+    double err, peakerr;     // last error estimate, all-time max of accepted errors
+    double torque_thr;       // stop when maxtorque < torque_thr (<= 0: off)
+    double maxtorque;        // gamma * max|tau| of the last evaluated derivative
+    double gamma;
+    double h;                // dt * gamma used by the current attempt
+    unsigned int err_bits;   // max |sum e_j k_j| over cells/components (float bits)
+    unsigned int tq_bits;    // max |tau|^2 over cells (float bits)
+    int cur;                 // which ping-pong state holds the accepted state
+    int done;                // 1: target reached -> kernels are no-ops
+    int tries;               // rejected attempts of the current step
+    int status;              // MM_OK, MM_ERR_NOT_CONVERGED, MM_ERR_NAN
+    int fsal_valid;          // derivative buffer K1[cur] holds f(Y[cur])
+    int pad0;
+    long long step, badsteps, attempts, evals;
+    long long noise_step;    // thermal noise counter (advanced once per accepted step)
+    double dt_thermal;       // > 0: fixed dt for the thermal scale (cutoff_dt), else dt
+};
+
+// Parameters of the effective field and torque, device pointers for masks
+// (NULL = uniform 1), multipliers in SI units, internal axis order.
+struct FieldParams {
+    int demag, exchange, anis, zeeman, thermal, zhangli, slonczewski;
+    int n[3];
+    int pbc[3];
+    long long N;
+    float msat;                 // Msat multiplier (A/m)
+    float ex_pre;               // 2 Aex/(mu0 Msat)
+    float cinv2[3];             // 1/cell^2
+    float alpha;
+    float hz[3];                // B_ext/mu0 (A/m)
+    float kmul;                 // 2 Ku/(mu0 Msat)
+    float anisu[3];
+    // thermal: H = eta * sqrt(alpha_mask*T_mask*therm_num / (therm_den*dt*Ms_mask))
+    float therm_num;            // alpha * kB * 2 * T
+    double therm_den;           // mu0 * V * gamma * Msat  (dt applied on device)
+    unsigned long long seed;
+    // Zhang-Li
+    float zl_pre;               // P muB/(e Msat)
+    float xi;
+    float jmul[3];
+    float c12inv[3];            // 1/(12 cell)
+    // Slonczewski
+    float sl_beta_prime, sl_pre_fld, lambda, t_fl;
+    float p[3];
+    float inv_gamma;
+    const float *msat_mask, *aex_mask, *alpha_mask, *ku_mask;
+    const float *anisu_mask[3], *bext_mask[3], *j_mask[3];
+    const float *temp_mask, *xi_mask, *zl_pol_mask;
+    const float *p_mask[3];
+    const float *sl_pol_mask, *lambda_mask, *eps_prime_mask, *t_fl_mask;
+};
+
+// Selects which of the two ping-pong buffers is read/written, from ctl->cur:
+// sel==0: fixed pointer p0; sel==1: the accepted side (p0 if cur==0 else p1);
+// sel==2: the other side.  Resolved on the device so that attempts can be queued
+// (or captured in a CUDA graph) without knowing whether earlier attempts were accepted.
+struct PP {
+    float* p0;
+    float* p1;
+    int sel;
+    __host__ __device__ float* get(int cur) const {
+        return sel == 0 ? p0 : (sel == 1 ? (cur ? p1 : p0) : (cur ? p0 : p1));
+    }
+};
+
+// What the fused epilogue does with the derivative k it has just computed at a cell:
+//   k_out[cell] = k
+//   next[cell]  = normalise(B + h * sum_j ak[j] * K_j[cell])   (if do_combine)
+//                 B = base[cell], or the evaluated state itself when base_is_cur;
+//                 the term j == kcur uses k from registers
+//   err        <- max over cells/components of |sum_j ek[j] * K_j[cell]|   (if ne > 0)
+//   tq         <- max |k|^2                                               (if want_tq)
+#define MM_MAXK 8
+struct StageOp {
+    PP m_in;
+    PP k_out;
+    int do_combine;
+    int base_is_cur;
+    PP base;
+    PP next;
+    int nk;
+    int kcur;
+    PP kp[MM_MAXK];
+    double ak[MM_MAXK];
+    int ne;
+    int ecur;
+    PP ep[MM_MAXK];
+    double ek[MM_MAXK];
+    int want_tq;
+    int want_energy;
+    int skip_if_retry;   // k0 of RK12/Heun: a retried attempt keeps the old k0
+    int pad;
+};
+
+// Symmetric demag kernel in k-space, stored for one octant only:
+// k[q][kz][ky][kx], kz <= L0/2, ky <= L1/2, kx <= L2/2; q = xx yy zz yz xz xy.
+struct KernelView {
+    const float* k;
+    int kd0, kd1, kd2;
+    int L0, L1;
+    int nz[6];
+};
+
+// Arguments of the fused epilogue (rhs.cu).
+struct EpiArgs {
+    FieldParams P;
+    StageOp op;
+    DevCtl* ctl;               // NULL for a standalone evaluation
+    long long noise_step;      // standalone thermal sample
+    double dt_thermal;         // standalone thermal dt
+    float* dbg[6];             // optional per-term outputs: demag, ex, anis, zee, therm, eff
+    float* red;                // energy block partials [nblocks][8]
+    unsigned int* tq_out;      // standalone max |k|^2 (float bits), may be NULL
+    int skip_retry;
+};
+
+// ---- launchers (conv.cu, rhs.cu)
+template <typename V, typename S>
+cudaError_t launch_xfwd(int M, const S* in, PP pp, const float* mask, V* out, int nrows, int Z, int Y, int Yout,
+                        int in_pitch, int n_in, int hp, const DevCtl* ctl, int skip_retry, cudaStream_t st);
+template <typename V>
+cudaError_t launch_colfft(int L, int sign, V* S, int ncols, int nouter, long long outer_stride,
+                          long long line_stride, int n_in, int n_out, const DevCtl* ctl, int skip_retry,
+                          cudaStream_t st);
+cudaError_t launch_colmul(int L, float2* S, const KernelView& K, int ncols, int nouter, long long comp_stride,
+                          long long outer_stride, long long line_stride, int n_in, int kaxis, float scale,
+                          const DevCtl* ctl, int skip_retry, cudaStream_t st);
+cudaError_t launch_xinv_epi(int M, const float2* S, int hp, int L1, const EpiArgs& A, bool terms, cudaStream_t st,
+                            int* nblocks);
+cudaError_t launch_local_epi(const EpiArgs& A, bool terms, cudaStream_t st, int* nblocks);
+int xinv_blocks(int M, int n0n1);
+int local_blocks(long long N);
+
+}  // namespace mm

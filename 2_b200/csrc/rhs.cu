@@ -1,0 +1,581 @@
+// rhs.cu -- fused right-hand side epilogue.
+//
+// One pass over the cells computes, per cell,
+//   H_eff = H_demag (inverse row transform of the convolved spectrum, in shared memory)
+//         + H_ex (exchange6.cu:12-142)  + B_ext/mu0 (mod_zeeman.go, add.cu:82-95)
+//         + H_anis (uniaxialanisotropy.cu:12-86) + H_therm (temperature.cu:14-66 with
+//           in-register Philox normals instead of a cuRAND noise buffer)
+//   k     = (m x H - alpha m x (m x H))/(1+alpha^2)            (torque.cu:13-57)
+//         + (zzt + stt)/gamma                                  (update_addterm.go:37-40,
+//           zhang-li_torque.cu:123-300, slonczewski_torque.cu:14-116)
+// and then whatever the time stepper needs from k at that cell (StageOp): the store
+// of k, the next Runge-Kutta stage state (normalised, normalize.cu:14-42), the error
+// estimate and the max-torque reduction.  The reference runs these as separate
+// kernels with a host sync after each (libmumax2.go), plus a D2H copy per reduction
+// (reductor.go:69-186).
+#include <cstdio>
+
+#include "fft.cuh"
+#include "mm_internal.h"
+
+namespace mm {
+using namespace mmfft;
+
+__device__ __forceinline__ bool skip_eval(const DevCtl* ctl, int skip_retry) {
+    return ctl && (ctl->done || (skip_retry && ctl->tries > 0));
+}
+
+// ---------------------------------------------------------------- Philox4x32-10
+// Salmon, Moraes, Dror, Shaw, SC'11 (published constants of the Philox4x32 family).
+__device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint2 k) {
+#pragma unroll
+    for (int r = 0; r < 10; r++) {
+        unsigned int hi0 = __umulhi(0xD2511F53u, c.x), lo0 = 0xD2511F53u * c.x;
+        unsigned int hi1 = __umulhi(0xCD9E8D57u, c.z), lo1 = 0xCD9E8D57u * c.z;
+        c = make_uint4(hi1 ^ c.y ^ k.x, lo1, hi0 ^ c.w ^ k.y, lo0);
+        k.x += 0x9E3779B9u;
+        k.y += 0xBB67AE85u;
+    }
+    return c;
+}
+
+// Three standard normals for (cell, step): Box-Muller on 24-bit uniforms in (0,1).
+__device__ __forceinline__ void thermal_normals(unsigned long long seed, long long cell, long long step, float eta[3]) {
+    uint4 c = make_uint4((unsigned)cell, (unsigned)((unsigned long long)step & 0xffffffffu),
+                         (unsigned)((unsigned long long)step >> 32), 0x7e57u);
+    uint4 r = philox4x32_10(c, make_uint2((unsigned)(seed & 0xffffffffu), (unsigned)(seed >> 32)));
+    const float s = 5.9604644775390625e-08f;  // 2^-24
+    float u0 = ((float)(r.x >> 8) + 0.5f) * s, u1 = ((float)(r.y >> 8) + 0.5f) * s;
+    float u2 = ((float)(r.z >> 8) + 0.5f) * s, u3 = ((float)(r.w >> 8) + 0.5f) * s;
+    float r0 = sqrtf(-2.0f * logf(u0)), r1 = sqrtf(-2.0f * logf(u2));
+    float s1, c1, s3, c3;
+    sincospif(2.0f * u1, &s1, &c1);
+    sincospif(2.0f * u3, &s3, &c3);
+    eta[0] = r0 * c1;
+    eta[1] = r0 * s1;
+    eta[2] = r1 * c3;
+}
+
+__device__ __forceinline__ float mval(const float* m, long long i) { return m ? __ldg(m + i) : 1.0f; }
+__device__ __forceinline__ float fdiv_zero(float a, float b) { return (b == 0.0f) ? 0.0f : a / b; }
+__device__ __forceinline__ float avg_geom_zero(float a, float b) {
+    float ab = a + b;
+    return (ab == 0.0f) ? 0.0f : 2.0f * a * b / ab;
+}
+// crossf of common_func.h:222-225: -(a x b)
+__device__ __forceinline__ float3 crossf(float3 a, float3 b) {
+    return make_float3(-a.y * b.z + a.z * b.y, -a.z * b.x + a.x * b.z, -a.x * b.y + a.y * b.x);
+}
+
+// neighbour index for the 6-point stencil: clamp, or wrap when periodic
+__device__ __forceinline__ int nb6(int i, int d, int n, int wrap) {
+    int j = i + d;
+    if (d < 0) { if (j < 0 && wrap) j += n; j = max(j, 0); }
+    else { if (j == n && wrap) j -= n; j = min(j, n - 1); }
+    return j;
+}
+// neighbour index for the 5-point Zhang-Li stencil: out of range -> the cell itself,
+// unless periodic (zhang-li_torque.cu:187-225)
+__device__ __forceinline__ int nb5(int i, int d, int n, int wrap) {
+    int j = i + d;
+    if (!wrap && (j < 0 || j >= n)) return i;
+    if (j < 0) j += n;
+    if (j >= n) j -= n;
+    return j;
+}
+
+struct CellTerms {
+    float hd[3], hex[3], han[3], hz[3], hth[3];
+};
+
+// Effective field and torque at one cell.  Returns k (tau/gamma + STT/gamma).
+template <bool WANT_TERMS>
+__device__ __forceinline__ float3 cell_rhs(const FieldParams& P, const float* __restrict__ m, long long i, int z,
+                                           int y, int x, float3 hd, long long noise_step, float dt_th, float3& m0,
+                                           CellTerms* terms) {
+    const long long N = P.N;
+    m0 = make_float3(__ldg(m + i), __ldg(m + N + i), __ldg(m + 2 * N + i));
+    float3 H = hd;
+    if (WANT_TERMS) { terms->hd[0] = hd.x; terms->hd[1] = hd.y; terms->hd[2] = hd.z; }
+    if (P.exchange) {
+        const int n0 = P.n[0], n1 = P.n[1], n2 = P.n[2];
+        const bool masked = P.msat_mask || P.aex_mask;
+        const float lex0 = masked ? fdiv_zero(mval(P.aex_mask, i), mval(P.msat_mask, i)) : 1.0f;
+        float3 hex = make_float3(0.f, 0.f, 0.f);
+        const int c[3] = {z, y, x};
+        const long long str[3] = {(long long)n1 * n2, n2, 1};
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            if (P.n[d] == 1) continue;  // both neighbours clamp onto the cell itself: no contribution
+            int lo = nb6(c[d], -1, P.n[d], P.pbc[d]);
+            int hi = nb6(c[d], +1, P.n[d], P.pbc[d]);
+            long long il = i + (long long)(lo - c[d]) * str[d];
+            long long ih = i + (long long)(hi - c[d]) * str[d];
+            float l1 = 1.f, l2 = 1.f;
+            if (masked) {
+                l1 = avg_geom_zero(lex0, fdiv_zero(mval(P.aex_mask, il), mval(P.msat_mask, il)));
+                l2 = avg_geom_zero(lex0, fdiv_zero(mval(P.aex_mask, ih), mval(P.msat_mask, ih)));
+            }
+            const float f = P.ex_pre * P.cinv2[d];
+            float3 a = make_float3(__ldg(m + il), __ldg(m + N + il), __ldg(m + 2 * N + il));
+            float3 b = make_float3(__ldg(m + ih), __ldg(m + N + ih), __ldg(m + 2 * N + ih));
+            hex.x += f * (l1 * (a.x - m0.x) + l2 * (b.x - m0.x));
+            hex.y += f * (l1 * (a.y - m0.y) + l2 * (b.y - m0.y));
+            hex.z += f * (l1 * (a.z - m0.z) + l2 * (b.z - m0.z));
+        }
+        H.x += hex.x; H.y += hex.y; H.z += hex.z;
+        if (WANT_TERMS) { terms->hex[0] = hex.x; terms->hex[1] = hex.y; terms->hex[2] = hex.z; }
+    }
+    if (P.zeeman) {
+        float3 hz = make_float3(P.hz[0] * mval(P.bext_mask[0], i), P.hz[1] * mval(P.bext_mask[1], i),
+                                P.hz[2] * mval(P.bext_mask[2], i));
+        H.x += hz.x; H.y += hz.y; H.z += hz.z;
+        if (WANT_TERMS) { terms->hz[0] = hz.x; terms->hz[1] = hz.y; terms->hz[2] = hz.z; }
+    }
+    if (P.anis) {
+        float msm = P.msat_mask ? __ldg(P.msat_mask + i) : 1.0f;
+        if (msm == 0.0f) msm = 1.0f;
+        float k2 = (P.kmul / msm) * mval(P.ku_mask, i);
+        float ux = P.anisu[0] * mval(P.anisu_mask[0], i);
+        float uy = P.anisu[1] * mval(P.anisu_mask[1], i);
+        float uz = P.anisu[2] * mval(P.anisu_mask[2], i);
+        float mu = m0.x * ux + m0.y * uy + m0.z * uz;
+        float3 ha = make_float3(k2 * mu * ux, k2 * mu * uy, k2 * mu * uz);
+        H.x += ha.x; H.y += ha.y; H.z += ha.z;
+        if (WANT_TERMS) { terms->han[0] = ha.x; terms->han[1] = ha.y; terms->han[2] = ha.z; }
+    }
+    if (P.thermal) {
+        float ms = mval(P.msat_mask, i);
+        float3 ht = make_float3(0.f, 0.f, 0.f);
+        if (ms != 0.0f) {
+            float eta[3];
+            thermal_normals(P.seed, i, noise_step, eta);
+            float a = mval(P.alpha_mask, i), tm = mval(P.temp_mask, i);
+            float den = (float)(P.therm_den * (double)dt_th);
+            float sc = sqrtf((a * tm * P.therm_num) / (den * ms));
+            ht = make_float3(eta[0] * sc, eta[1] * sc, eta[2] * sc);
+        }
+        H.x += ht.x; H.y += ht.y; H.z += ht.z;
+        if (WANT_TERMS) { terms->hth[0] = ht.x; terms->hth[1] = ht.y; terms->hth[2] = ht.z; }
+    }
+    // LLG torque
+    const float al = P.alpha * mval(P.alpha_mask, i);
+    float cx = m0.y * H.z - H.y * m0.z, cy = -m0.x * H.z + H.x * m0.z, cz = m0.x * H.y - H.x * m0.y;
+    float dx = -m0.y * cz + cy * m0.z, dy = m0.x * cz - cx * m0.z, dz = -m0.x * cy + cx * m0.y;
+    float g = 1.0f / (1.0f + al * al);
+    float3 k = make_float3(g * (cx + dx * al), g * (cy + dy * al), g * (cz + dz * al));
+    if (P.zhangli) {
+        float msat = P.msat_mask ? __ldg(P.msat_mask + i) : 1.0f;
+        float3 j0 = make_float3(P.j_mask[0] ? __ldg(P.j_mask[0] + i) * P.jmul[0] : P.jmul[0],
+                                P.j_mask[1] ? __ldg(P.j_mask[1] + i) * P.jmul[1] : P.jmul[1],
+                                P.j_mask[2] ? __ldg(P.j_mask[2] + i) * P.jmul[2] : P.jmul[2]);
+        float njn = sqrtf(j0.x * j0.x + j0.y * j0.y + j0.z * j0.z);
+        if (msat != 0.0f && njn != 0.0f) {
+            msat = 1.0f / msat;
+            float PP = P.zl_pol_mask ? __ldg(P.zl_pol_mask + i) : 1.0f;
+            float pred = njn * PP * P.zl_pre;
+            float ee = P.xi_mask ? __ldg(P.xi_mask + i) * P.xi : P.xi;
+            pred = pred / ((1.0f + ee * ee) * (1.0f + al * al));
+            float pret = pred * (ee - al);
+            pred = pred * (1.0f + ee * al);
+            const float inv = 1.0f / njn;
+            const float nj[3] = {j0.x * inv, j0.y * inv, j0.z * inv};
+            const int c[3] = {z, y, x};
+            const long long str[3] = {(long long)P.n[1] * P.n[2], P.n[2], 1};
+            float3 dmdj = make_float3(0.f, 0.f, 0.f);
+#pragma unroll
+            for (int d = 0; d < 3; d++) {
+                if (nj[d] == 0.0f) continue;
+                long long ib2 = i + (long long)(nb5(c[d], -2, P.n[d], P.pbc[d]) - c[d]) * str[d];
+                long long ib1 = i + (long long)(nb5(c[d], -1, P.n[d], P.pbc[d]) - c[d]) * str[d];
+                long long if1 = i + (long long)(nb5(c[d], +1, P.n[d], P.pbc[d]) - c[d]) * str[d];
+                long long if2 = i + (long long)(nb5(c[d], +2, P.n[d], P.pbc[d]) - c[d]) * str[d];
+                const float s = P.c12inv[d] * nj[d];
+#pragma unroll
+                for (int q = 0; q < 3; q++) {
+                    const float* a = m + q * N;
+                    float dv = __ldg(a + ib2) - 8.0f * __ldg(a + ib1) + 8.0f * __ldg(a + if1) - __ldg(a + if2);
+                    if (q == 0) dmdj.x += s * dv;
+                    else if (q == 1) dmdj.y += s * dv;
+                    else dmdj.z += s * dv;
+                }
+            }
+            float3 dmdjxm = crossf(dmdj, m0);
+            float3 mxdmxm = crossf(m0, dmdjxm);
+            k.x += P.inv_gamma * msat * (pred * mxdmxm.x + pret * dmdjxm.x);
+            k.y += P.inv_gamma * msat * (pred * mxdmxm.y + pret * dmdjxm.y);
+            k.z += P.inv_gamma * msat * (pred * mxdmxm.z + pret * dmdjxm.z);
+        }
+    }
+    if (P.slonczewski) {
+        float Ms = P.msat_mask ? __ldg(P.msat_mask + i) : 1.0f;
+        float3 J = make_float3(P.j_mask[0] ? __ldg(P.j_mask[0] + i) * P.jmul[0] : P.jmul[0],
+                               P.j_mask[1] ? __ldg(P.j_mask[1] + i) * P.jmul[1] : P.jmul[1],
+                               P.j_mask[2] ? __ldg(P.j_mask[2] + i) * P.jmul[2] : P.jmul[2]);
+        float nJn = sqrtf(J.x * J.x + J.y * J.y + J.z * J.z);
+        float tfl = P.t_fl_mask ? __ldg(P.t_fl_mask + i) * P.t_fl : P.t_fl;
+        if (nJn != 0.0f && Ms != 0.0f && tfl != 0.0f) {
+            tfl = 1.0f / tfl;
+            Ms = 1.0f / Ms;
+            float prex = P.sl_beta_prime * Ms, prey = P.sl_pre_fld * Ms;
+            float3 p = make_float3(P.p_mask[0] ? P.p[0] * __ldg(P.p_mask[0] + i) : P.p[0],
+                                   P.p_mask[1] ? P.p[1] * __ldg(P.p_mask[1] + i) : P.p[1],
+                                   P.p_mask[2] ? P.p[2] * __ldg(P.p_mask[2] + i) : P.p[2]);
+            float pl = sqrtf(p.x * p.x + p.y * p.y + p.z * p.z);
+            float pinv = (pl != 0.0f) ? 1.0f / pl : 0.0f;
+            p.x *= pinv; p.y *= pinv; p.z *= pinv;
+            float3 pxm = crossf(p, m0);
+            float3 mxpxm = crossf(m0, pxm);
+            float pdotm = p.x * m0.x + p.y * m0.y + p.z * m0.z;
+            float jinv = 1.0f / nJn;
+            float Jdir = J.x * jinv + J.y * jinv + J.z * jinv;
+            float Jsign = Jdir / fabsf(Jdir);
+            float nj = nJn * Jsign;
+            prex *= nj; prey *= nj;
+            prex *= tfl; prey *= tfl;
+            float lam = P.lambda_mask ? P.lambda * __ldg(P.lambda_mask + i) : P.lambda;
+            float l2 = lam * lam;
+            float eps = l2 / ((l2 + 1.0f) + (l2 - 1.0f) * pdotm);
+            prex *= eps;
+            float af = 1.0f / (1.0f + al * al);
+            prex *= P.sl_pol_mask ? __ldg(P.sl_pol_mask + i) : 1.0f;
+            prey *= P.eps_prime_mask ? __ldg(P.eps_prime_mask + i) : 1.0f;
+            float f1 = (prex - al * prey) * af;
+            float f2 = (prey - al * prex) * af;
+            k.x += P.inv_gamma * (f1 * mxpxm.x + f2 * pxm.x);
+            k.y += P.inv_gamma * (f1 * mxpxm.y + f2 * pxm.y);
+            k.z += P.inv_gamma * (f1 * mxpxm.z + f2 * pxm.z);
+        }
+    }
+    return k;
+}
+
+// Kahan-style compensated accumulation of FP32 values (Neumaier's variant).
+struct KSum {
+    float s, c;
+    __device__ __forceinline__ void add(float v) {
+        float t = s + v;
+        if (fabsf(s) >= fabsf(v)) c += (s - t) + v;
+        else c += (v - t) + s;
+        s = t;
+    }
+};
+__device__ __forceinline__ KSum ksum_merge(KSum a, KSum b) {
+    KSum r = a;
+    r.add(b.s);
+    r.c += b.c;
+    return r;
+}
+
+// Everything after k is known at one cell (StageOp).  Resolved pointers in `rp`.
+struct ResolvedOp {
+    float* k_out;
+    const float* base;
+    float* next;
+    const float* kp[MM_MAXK];
+    float ak[MM_MAXK];
+    const float* ep[MM_MAXK];
+    float ek[MM_MAXK];
+};
+
+__device__ __forceinline__ void resolve_op(const StageOp& op, int cur, float h, ResolvedOp& r) {
+    r.k_out = op.k_out.get(cur);
+    r.base = op.base.get(cur);
+    r.next = op.next.get(cur);
+#pragma unroll
+    for (int j = 0; j < MM_MAXK; j++) {
+        r.kp[j] = (j < op.nk) ? op.kp[j].get(cur) : nullptr;
+        r.ak[j] = (j < op.nk) ? (float)(op.ak[j] * (double)h) : 0.f;
+        r.ep[j] = (j < op.ne) ? op.ep[j].get(cur) : nullptr;
+        r.ek[j] = (j < op.ne) ? (float)op.ek[j] : 0.f;
+    }
+}
+
+struct ThreadRed {
+    float tq;
+    float err;
+    int bad;
+    KSum e[4];
+};
+
+__device__ __forceinline__ void cell_post(const FieldParams& P, const StageOp& op, const ResolvedOp& r, long long i,
+                                          float3 m0, float3 k, ThreadRed& tr) {
+    const long long N = P.N;
+    if (!(isfinite(k.x) && isfinite(k.y) && isfinite(k.z))) tr.bad = 1;
+    if (r.k_out) {
+        r.k_out[i] = k.x;
+        r.k_out[N + i] = k.y;
+        r.k_out[2 * N + i] = k.z;
+    }
+    if (op.want_tq) tr.tq = fmaxf(tr.tq, k.x * k.x + k.y * k.y + k.z * k.z);
+    if (op.do_combine) {
+        float3 v = op.base_is_cur ? m0 : make_float3(r.base[i], r.base[N + i], r.base[2 * N + i]);
+#pragma unroll
+        for (int j = 0; j < MM_MAXK; j++) {
+            if (j >= op.nk) break;
+            float3 kj = (j == op.kcur) ? k : make_float3(r.kp[j][i], r.kp[j][N + i], r.kp[j][2 * N + i]);
+            v.x += r.ak[j] * kj.x;
+            v.y += r.ak[j] * kj.y;
+            v.z += r.ak[j] * kj.z;
+        }
+        // normalize.cu:14-42 with the Msat mask as norm map
+        float norm = P.msat_mask ? __ldg(P.msat_mask + i) : 1.0f;
+        float mn = sqrtf(v.x * v.x + v.y * v.y + v.z * v.z);
+        float sc = (norm == 0.0f) ? 0.0f : 1.0f;
+        sc = (mn != 0.0f) ? sc / mn : 0.0f;
+        r.next[i] = v.x * sc;
+        r.next[N + i] = v.y * sc;
+        r.next[2 * N + i] = v.z * sc;
+    }
+    if (op.ne > 0) {
+        float3 e = make_float3(0.f, 0.f, 0.f);
+#pragma unroll
+        for (int j = 0; j < MM_MAXK; j++) {
+            if (j >= op.ne) break;
+            float3 kj = (j == op.ecur) ? k : make_float3(r.ep[j][i], r.ep[j][N + i], r.ep[j][2 * N + i]);
+            e.x += r.ek[j] * kj.x;
+            e.y += r.ek[j] * kj.y;
+            e.z += r.ek[j] * kj.z;
+        }
+        tr.err = fmaxf(tr.err, fmaxf(fabsf(e.x), fmaxf(fabsf(e.y), fabsf(e.z))));
+    }
+}
+
+__device__ __forceinline__ void energy_acc(const FieldParams& P, long long i, float3 m0, const CellTerms& t,
+                                           ThreadRed& tr) {
+    // m . B_ext (T): B_ext = mu0 * hz
+    const float mu0 = 1.2566370614359172e-06f;
+    tr.e[0].add(mu0 * (m0.x * t.hz[0] + m0.y * t.hz[1] + m0.z * t.hz[2]));
+    tr.e[1].add(m0.x * t.hex[0] + m0.y * t.hex[1] + m0.z * t.hex[2]);
+    tr.e[2].add(m0.x * t.hd[0] + m0.y * t.hd[1] + m0.z * t.hd[2]);
+    tr.e[3].add(m0.x * t.han[0] + m0.y * t.han[1] + m0.z * t.han[2]);
+}
+
+// Block-level reduction of ThreadRed; thread 0 publishes.
+__device__ void block_reduce_publish(ThreadRed tr, const StageOp& op, DevCtl* ctl, unsigned int* tq_out, float* red) {
+    __shared__ float s_tq[32], s_err[32];
+    __shared__ int s_bad[32];
+    __shared__ float s_e[32][8];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        tr.tq = fmaxf(tr.tq, __shfl_xor_sync(0xffffffffu, tr.tq, o));
+        tr.err = fmaxf(tr.err, __shfl_xor_sync(0xffffffffu, tr.err, o));
+        tr.bad |= __shfl_xor_sync(0xffffffffu, tr.bad, o);
+    }
+    if (op.want_energy) {
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                KSum b;
+                b.s = __shfl_xor_sync(0xffffffffu, tr.e[q].s, o);
+                b.c = __shfl_xor_sync(0xffffffffu, tr.e[q].c, o);
+                tr.e[q] = ksum_merge(tr.e[q], b);
+            }
+        }
+    }
+    if (lane == 0) {
+        s_tq[wid] = tr.tq;
+        s_err[wid] = tr.err;
+        s_bad[wid] = tr.bad;
+        for (int q = 0; q < 4; q++) { s_e[wid][2 * q] = tr.e[q].s; s_e[wid][2 * q + 1] = tr.e[q].c; }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float tq = 0.f, err = 0.f;
+        int bad = 0;
+        KSum e[4] = {{0.f, 0.f}, {0.f, 0.f}, {0.f, 0.f}, {0.f, 0.f}};
+        for (int w = 0; w < nw; w++) {
+            tq = fmaxf(tq, s_tq[w]);
+            err = fmaxf(err, s_err[w]);
+            bad |= s_bad[w];
+            for (int q = 0; q < 4; q++) {
+                KSum b = {s_e[w][2 * q], s_e[w][2 * q + 1]};
+                e[q] = ksum_merge(e[q], b);
+            }
+        }
+        if (ctl) {
+            if (op.want_tq) atomicMax(&ctl->tq_bits, __float_as_uint(tq));
+            if (op.ne > 0) atomicMax(&ctl->err_bits, __float_as_uint(err));
+            if (bad) atomicExch(&ctl->status, (int)MM_ERR_NAN);
+        } else if (tq_out && op.want_tq) {
+            atomicMax(tq_out, __float_as_uint(tq));
+        }
+        if (op.want_energy && red) {
+            for (int q = 0; q < 4; q++) {
+                red[blockIdx.x * 8 + 2 * q] = e[q].s;
+                red[blockIdx.x * 8 + 2 * q + 1] = e[q].c;
+            }
+        }
+    }
+}
+
+__device__ __forceinline__ void write_terms(float* const* dbg, long long N, long long i, const CellTerms& t) {
+    const float* src[5] = {t.hd, t.hex, t.han, t.hz, t.hth};
+    for (int q = 0; q < 5; q++)
+        if (dbg[q])
+            for (int c = 0; c < 3; c++) dbg[q][c * N + i] = src[q][c];
+    if (dbg[5])
+        for (int c = 0; c < 3; c++)
+            dbg[5][c * N + i] = t.hd[c] + t.hex[c] + t.han[c] + t.hz[c] + t.hth[c];
+}
+
+template <bool TERMS>
+__device__ __forceinline__ void process_cell(const EpiArgs& A, const float* m, const ResolvedOp& r, long long i,
+                                             int z, int y, int x, float3 hd, long long ns, float dtth,
+                                             ThreadRed& tr) {
+    float3 m0;
+    if (TERMS) {
+        CellTerms t = {};
+        float3 k = cell_rhs<true>(A.P, m, i, z, y, x, hd, ns, dtth, m0, &t);
+        if (A.op.want_energy) energy_acc(A.P, i, m0, t, tr);
+        write_terms(A.dbg, A.P.N, i, t);
+        cell_post(A.P, A.op, r, i, m0, k, tr);
+    } else {
+        float3 k = cell_rhs<false>(A.P, m, i, z, y, x, hd, ns, dtth, m0, nullptr);
+        cell_post(A.P, A.op, r, i, m0, k, tr);
+    }
+}
+
+// ---------------------------------------------------------------- C2R row pass + epilogue
+template <int M, bool TERMS>
+__global__ void __launch_bounds__(512) xinv_epi_kernel(const float2* __restrict__ S, int hp, int L1, EpiArgs A) {
+    const DevCtl* ctl = A.ctl;
+    if (skip_eval(ctl, A.skip_retry)) return;
+    constexpr int TPL = tpl(M);
+    constexpr int LL = line_len(M);
+    extern __shared__ unsigned char smem_raw[];
+    float2* sm = reinterpret_cast<float2*>(smem_raw);
+    const int n0 = A.P.n[0], n1 = A.P.n[1], n2 = A.P.n[2];
+    const int nrows = n0 * n1;
+    const int rpb = blockDim.x / (3 * TPL);
+    const int lr = threadIdx.x / (3 * TPL);
+    const int c = (threadIdx.x / TPL) % 3;
+    const int t = threadIdx.x % TPL;
+    const int row = blockIdx.x * rpb + lr;
+    const bool active = (lr < rpb) && (row < nrows);
+    float2* xl = sm + (lr * 3 + c) * LL;
+    if (active) {
+        const int z = row / n1, y = row % n1;
+        const float2* src = S + ((long long)(c * n0 + z) * L1 + y) * hp;
+        // Z[k] = (X[k] + conj X[M-k]) + i W^-k (X[k] - conj X[M-k]),  W = exp(-2 pi i / 2M)
+        for (int k = t; k < M; k += TPL) {
+            float2 a = src[k], b = src[M - k];
+            float2 s = make_float2(a.x + b.x, a.y - b.y);
+            float2 d = make_float2(a.x - b.x, a.y + b.y);
+            float2 w = Tw<+1, float2>::get(k, 2 * M);
+            float2 wd = cmul(w, d);
+            xl[padx(k)] = make_float2(s.x - wd.y, s.y + wd.x);
+        }
+    }
+    __syncthreads();
+    fft_line<M, +1, float2>(lr < rpb ? xl : sm, t, active);
+    // epilogue over the cells of this block's rows
+    const int cur = ctl ? ctl->cur : 0;
+    const float h = ctl ? (float)ctl->h : 0.f;
+    const long long ns = ctl ? ctl->noise_step : A.noise_step;
+    const float dtth = ctl ? (float)(ctl->dt_thermal > 0 ? ctl->dt_thermal : ctl->dt) : (float)A.dt_thermal;
+    ResolvedOp r;
+    resolve_op(A.op, cur, h, r);
+    const float* m = A.op.m_in.get(cur);
+    ThreadRed tr = {0.f, 0.f, 0, {{0.f, 0.f}, {0.f, 0.f}, {0.f, 0.f}, {0.f, 0.f}}};
+    const int row0 = blockIdx.x * rpb;
+    const int nrow_here = min(rpb, nrows - row0);
+    for (int e = threadIdx.x; e < nrow_here * n2; e += blockDim.x) {
+        const int lrow = e / n2, x = e % n2;
+        const int grow = row0 + lrow;
+        const int z = grow / n1, y = grow % n1;
+        const long long i = (long long)grow * n2 + x;
+        const int pi = padx(x >> 1);
+        float2 v0 = sm[(lrow * 3 + 0) * LL + pi];
+        float2 v1 = sm[(lrow * 3 + 1) * LL + pi];
+        float2 v2 = sm[(lrow * 3 + 2) * LL + pi];
+        float3 hd = (x & 1) ? make_float3(v0.y, v1.y, v2.y) : make_float3(v0.x, v1.x, v2.x);
+        process_cell<TERMS>(A, m, r, i, z, y, x, hd, ns, dtth, tr);
+    }
+    block_reduce_publish(tr, A.op, A.ctl, A.tq_out, A.red);
+}
+
+// ---------------------------------------------------------------- epilogue without demag
+template <bool TERMS>
+__global__ void __launch_bounds__(256) local_epi_kernel(EpiArgs A) {
+    const DevCtl* ctl = A.ctl;
+    if (skip_eval(ctl, A.skip_retry)) return;
+    const int n1 = A.P.n[1], n2 = A.P.n[2];
+    const int cur = ctl ? ctl->cur : 0;
+    const float h = ctl ? (float)ctl->h : 0.f;
+    const long long ns = ctl ? ctl->noise_step : A.noise_step;
+    const float dtth = ctl ? (float)(ctl->dt_thermal > 0 ? ctl->dt_thermal : ctl->dt) : (float)A.dt_thermal;
+    ResolvedOp r;
+    resolve_op(A.op, cur, h, r);
+    const float* m = A.op.m_in.get(cur);
+    ThreadRed tr = {0.f, 0.f, 0, {{0.f, 0.f}, {0.f, 0.f}, {0.f, 0.f}, {0.f, 0.f}}};
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < A.P.N;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int x = (int)(i % n2);
+        const long long zy = i / n2;
+        const int y = (int)(zy % n1), z = (int)(zy / n1);
+        process_cell<TERMS>(A, m, r, i, z, y, x, make_float3(0.f, 0.f, 0.f), ns, dtth, tr);
+    }
+    block_reduce_publish(tr, A.op, A.ctl, A.tq_out, A.red);
+}
+
+// ---------------------------------------------------------------- launchers
+template <int M, bool TERMS>
+static cudaError_t launch_xinv_t(const float2* S, int hp, int L1, const EpiArgs& A, cudaStream_t st, int* nblocks) {
+    constexpr int TPL = tpl(M);
+    int rpb = (3 * TPL >= 384) ? 1 : 384 / (3 * TPL);
+    size_t smem = (size_t)rpb * 3 * line_len(M) * sizeof(float2);
+    while (smem > 100 * 1024 && rpb > 1) { rpb /= 2; smem = (size_t)rpb * 3 * line_len(M) * sizeof(float2); }
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(xinv_epi_kernel<M, TERMS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    const int nrows = A.P.n[0] * A.P.n[1];
+    int blocks = (nrows + rpb - 1) / rpb;
+    int threads = rpb * 3 * TPL;
+    if (threads < 32) threads = 32;
+    *nblocks = blocks;
+    xinv_epi_kernel<M, TERMS><<<blocks, threads, smem, st>>>(S, hp, L1, A);
+    return cudaGetLastError();
+}
+
+int xinv_blocks(int M, int n0n1) {
+    int TPL = mmfft::tpl(M);
+    int rpb = (3 * TPL >= 384) ? 1 : 384 / (3 * TPL);
+    size_t smem = (size_t)rpb * 3 * mmfft::line_len(M) * sizeof(float2);
+    while (smem > 100 * 1024 && rpb > 1) { rpb /= 2; smem = (size_t)rpb * 3 * mmfft::line_len(M) * sizeof(float2); }
+    return (n0n1 + rpb - 1) / rpb;
+}
+
+cudaError_t launch_xinv_epi(int M, const float2* S, int hp, int L1, const EpiArgs& A, bool terms, cudaStream_t st,
+                            int* nblocks) {
+    switch (M) {
+#define X(m)                                                                      \
+    case m:                                                                       \
+        return terms ? launch_xinv_t<m, true>(S, hp, L1, A, st, nblocks)          \
+                     : launch_xinv_t<m, false>(S, hp, L1, A, st, nblocks);
+        X(1) X(2) X(4) X(8) X(16) X(32) X(64) X(128) X(256) X(512) X(1024) X(2048)
+#undef X
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+int local_blocks(long long N) {
+    long long b = (N + 255) / 256;
+    if (b > 148 * 16) b = 148 * 16;
+    if (b < 1) b = 1;
+    return (int)b;
+}
+
+cudaError_t launch_local_epi(const EpiArgs& A, bool terms, cudaStream_t st, int* nblocks) {
+    int b = local_blocks(A.P.N);
+    *nblocks = b;
+    if (terms) local_epi_kernel<true><<<b, 256, 0, st>>>(A);
+    else local_epi_kernel<false><<<b, 256, 0, st>>>(A);
+    return cudaGetLastError();
+}
+
+}  // namespace mm

@@ -1,0 +1,150 @@
+"""ctypes binding of libmm_b200.so (the sm_100a CUDA library, C-ABI in include/mm_b200.h).
+
+The library is loaded from the package directory (built in-tree by 2_b200/build.py).
+There is no fallback: if the library is missing or cannot be loaded, every entry
+point raises.
+"""
+import ctypes as C
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.normpath(os.path.join(_HERE, "..", "libmm_b200.so"))
+_lib = None
+
+FP = C.POINTER(C.c_float)
+DP = C.POINTER(C.c_double)
+
+MM_OK = 0
+MM_ERR_ARG = -1
+MM_ERR_CUDA = -2
+MM_ERR_NOT_CONVERGED = -3
+MM_ERR_NAN = -4
+MM_ERR_STATE = -5
+MM_ERR_TIMEOUT = -6
+
+SOLVERS = {"euler": 0, "heun": 1, "rk12": 2, "rk23": 3, "rk45": 4}
+
+
+class MMProblem(C.Structure):
+    """mm_problem of include/mm_b200.h (device mask pointers)."""
+    _fields_ = [
+        ("n", C.c_int * 3), ("cell", C.c_double * 3), ("pbc", C.c_int * 3),
+        ("demag", C.c_int), ("exchange", C.c_int), ("anis", C.c_int), ("zeeman", C.c_int),
+        ("thermal", C.c_int), ("zhangli", C.c_int), ("slonczewski", C.c_int),
+        ("demag_accuracy", C.c_int),
+        ("msat", C.c_double), ("aex", C.c_double), ("alpha", C.c_double), ("gamma", C.c_double),
+        ("bext", C.c_double * 3), ("ku", C.c_double), ("anisu", C.c_double * 3),
+        ("temp", C.c_double), ("seed", C.c_ulonglong),
+        ("j", C.c_double * 3), ("zl_pol", C.c_double), ("xi", C.c_double),
+        ("p", C.c_double * 3), ("sl_pol", C.c_double), ("lambda_", C.c_double),
+        ("eps_prime", C.c_double), ("t_fl", C.c_double),
+        ("msat_mask", C.c_void_p), ("aex_mask", C.c_void_p), ("alpha_mask", C.c_void_p),
+        ("ku_mask", C.c_void_p),
+        ("anisu_mask", C.c_void_p * 3), ("bext_mask", C.c_void_p * 3), ("j_mask", C.c_void_p * 3),
+        ("temp_mask", C.c_void_p), ("xi_mask", C.c_void_p), ("zl_pol_mask", C.c_void_p),
+        ("p_mask", C.c_void_p * 3),
+        ("sl_pol_mask", C.c_void_p), ("lambda_mask", C.c_void_p), ("eps_prime_mask", C.c_void_p),
+        ("t_fl_mask", C.c_void_p),
+    ]
+
+
+class MMStats(C.Structure):
+    _fields_ = [
+        ("t", C.c_double), ("dt", C.c_double), ("err", C.c_double), ("peakerr", C.c_double),
+        ("maxtorque", C.c_double), ("step", C.c_longlong), ("badsteps", C.c_longlong),
+        ("attempts", C.c_longlong), ("evals", C.c_longlong), ("status", C.c_int), ("done", C.c_int),
+    ]
+
+
+class MMError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"mm_b200 error {code}: {msg}")
+        self.code = code
+
+
+_PROTOS = {
+    "mm_last_error": (C.c_char_p, []),
+    "mm_version": (C.c_char_p, []),
+    "mm_plan_create": (C.c_int, [C.POINTER(MMProblem), C.POINTER(C.c_void_p)]),
+    "mm_plan_destroy": (C.c_int, [C.c_void_p]),
+    "mm_plan_set_problem": (C.c_int, [C.c_void_p, C.POINTER(MMProblem)]),
+    "mm_plan_kernel_nonzero": (C.c_int, [C.c_void_p, C.c_int * 6]),
+    "mm_plan_device_bytes": (C.c_longlong, [C.c_void_p]),
+    "mm_fields": (C.c_int, [C.c_void_p, C.c_void_p, C.c_longlong, C.c_double] + [C.c_void_p] * 6 + [C.c_void_p]),
+    "mm_torque": (C.c_int, [C.c_void_p, C.c_void_p, C.c_longlong, C.c_double, C.c_void_p, C.c_void_p]),
+    "mm_solver_init": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double]),
+    "mm_set_state": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
+    "mm_get_state": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
+    "mm_set_time": (C.c_int, [C.c_void_p, C.c_double, C.c_double]),
+    "mm_set_thermal_dt": (C.c_int, [C.c_void_p, C.c_double]),
+    "mm_step": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "mm_run": (C.c_int, [C.c_void_p, C.c_double, C.c_void_p]),
+    "mm_steps": (C.c_int, [C.c_void_p, C.c_longlong, C.c_void_p]),
+    "mm_run_until_maxtorque": (C.c_int, [C.c_void_p, C.c_double, C.c_longlong, C.c_void_p]),
+    "mm_queue_attempts": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    "mm_get_stats": (C.c_int, [C.c_void_p, C.POINTER(MMStats), C.c_void_p]),
+    "mm_maxtorque": (C.c_int, [C.c_void_p, DP, C.c_void_p]),
+    "mm_average": (C.c_int, [C.c_void_p, C.c_double * 3, C.c_void_p]),
+    "mm_energy": (C.c_int, [C.c_void_p, C.c_double * 5, C.c_void_p]),
+}
+
+
+def lib():
+    """Load libmm_b200.so (raises if it is missing: there is no CPU fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `python 2_b200/build.py`")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in _PROTOS.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(rc):
+    if rc != MM_OK:
+        msg = lib().mm_last_error().decode(errors="replace")
+        raise MMError(rc, msg)
+    return rc
+
+
+MASK_SCALARS = ["msat", "aex", "alpha", "ku", "temp", "xi", "zl_pol", "sl_pol", "lambda",
+                "eps_prime", "t_fl"]
+MASK_VECTORS = ["anisu", "bext", "j", "p"]
+
+
+def make_problem(d, masks=None):
+    """Fill an MMProblem from a dict (same keys as the oracle's problem dict);
+    `masks` maps mask names to device pointers (ints) or, for vectors, 3-lists."""
+    s = MMProblem()
+    s.n[:] = [int(x) for x in d["n"]]
+    s.cell[:] = [float(x) for x in d["cell"]]
+    s.pbc[:] = [int(x) for x in d.get("pbc", (0, 0, 0))]
+    for k in ["demag", "exchange", "anis", "zeeman", "thermal", "zhangli", "slonczewski"]:
+        setattr(s, k, int(d.get(k, 0)))
+    s.demag_accuracy = int(d.get("demag_accuracy", 6))
+    for k, dv in [("msat", 8e5), ("aex", 1.3e-11), ("alpha", 0.02), ("gamma", 2.211e5), ("ku", 0.0),
+                  ("temp", 0.0), ("zl_pol", 1.0), ("xi", 0.05), ("sl_pol", 1.0), ("eps_prime", 0.0),
+                  ("t_fl", 0.0)]:
+        setattr(s, k, float(d.get(k, dv)))
+    s.lambda_ = float(d.get("lambda", 1.0))
+    s.seed = int(d.get("seed", 0))
+    s.bext[:] = [float(x) for x in d.get("bext", (0, 0, 0))]
+    s.anisu[:] = [float(x) for x in d.get("anisu", (0, 0, 1))]
+    s.j[:] = [float(x) for x in d.get("j", (0, 0, 0))]
+    s.p[:] = [float(x) for x in d.get("p", (0, 0, 1))]
+    masks = masks or {}
+    for k in MASK_SCALARS:
+        if masks.get(k) is not None:
+            setattr(s, k + "_mask", int(masks[k]))
+    for k in MASK_VECTORS:
+        v = masks.get(k)
+        if v is not None:
+            arr = getattr(s, k + "_mask")
+            for c in range(3):
+                if v[c] is not None:
+                    arr[c] = int(v[c])
+    return s

@@ -1,0 +1,163 @@
+"""Python handle of one fused plan (geometry + parameters + demag kernel + stepper).
+
+Device memory for masks and state lives in torch CUDA tensors (plumbing only); all
+computation runs in libmm_b200.so.  Arrays are in the reference's internal axis
+order (Z,Y,X), SoA [comp][n0][n1][n2].
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import _native as nat
+
+
+def _torch():
+    import torch
+    if not torch.cuda.is_available():
+        raise RuntimeError("mm_b200 needs a CUDA device (sm_100a); none is available")
+    return torch
+
+
+def _ptr(t):
+    return C.c_void_p(t.data_ptr()) if t is not None else None
+
+
+class Plan:
+    def __init__(self, problem, masks=None, device=0):
+        torch = _torch()
+        self.torch = torch
+        self.device = torch.device("cuda", device) if isinstance(device, int) else torch.device(device)
+        torch.cuda.set_device(self.device)
+        self.problem = dict(problem)
+        n = self.problem["n"]
+        self.N = int(n[0]) * int(n[1]) * int(n[2])
+        self._masks = {}
+        self._mask_ptrs = {}
+        self._upload_masks(masks or {})
+        self._struct = nat.make_problem(self.problem, self._mask_ptrs)
+        h = C.c_void_p()
+        nat.check(nat.lib().mm_plan_create(C.byref(self._struct), C.byref(h)))
+        self.h = h
+        self._solver = None
+
+    def _upload_masks(self, masks):
+        torch = self.torch
+        self._masks = {}
+        self._mask_ptrs = {}
+        for k, v in masks.items():
+            if v is None:
+                continue
+            if k in nat.MASK_VECTORS:
+                ts = [None if c is None else torch.as_tensor(np.ascontiguousarray(c, dtype=np.float32).ravel(),
+                                                              device=self.device) for c in v]
+                self._masks[k] = ts
+                self._mask_ptrs[k] = [None if t is None else t.data_ptr() for t in ts]
+            else:
+                t = torch.as_tensor(np.ascontiguousarray(v, dtype=np.float32).ravel(), device=self.device)
+                self._masks[k] = t
+                self._mask_ptrs[k] = t.data_ptr()
+
+    def set_problem(self, problem, masks=None):
+        self.problem = dict(problem)
+        if masks is not None:
+            self._upload_masks(masks)
+        self._struct = nat.make_problem(self.problem, self._mask_ptrs)
+        nat.check(nat.lib().mm_plan_set_problem(self.h, C.byref(self._struct)))
+
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            nat.lib().mm_plan_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _dev(self, a):
+        torch = self.torch
+        if isinstance(a, torch.Tensor):
+            return a.to(self.device, torch.float32).contiguous()
+        return torch.as_tensor(np.ascontiguousarray(a, dtype=np.float32).ravel(), device=self.device)
+
+    def kernel_nonzero(self):
+        out = (C.c_int * 6)()
+        nat.check(nat.lib().mm_plan_kernel_nonzero(self.h, out))
+        return list(out[:])
+
+    def device_bytes(self):
+        return nat.lib().mm_plan_device_bytes(self.h)
+
+    def fields(self, m, noise_step=0, dt_thermal=0.0):
+        torch = self.torch
+        md = self._dev(m)
+        out = {k: torch.zeros(3 * self.N, device=self.device) for k in ["demag", "ex", "anis", "zee", "therm", "eff"]}
+        nat.check(nat.lib().mm_fields(self.h, _ptr(md), noise_step, dt_thermal, _ptr(out["demag"]), _ptr(out["ex"]),
+                                      _ptr(out["anis"]), _ptr(out["zee"]), _ptr(out["therm"]), _ptr(out["eff"]), None))
+        torch.cuda.synchronize(self.device)
+        return out
+
+    def torque(self, m, noise_step=0, dt_thermal=0.0):
+        """Returns (torque array tau/gamma incl. STT/gamma, normalised m) as device tensors."""
+        torch = self.torch
+        md = self._dev(m).clone()
+        t = torch.zeros(3 * self.N, device=self.device)
+        nat.check(nat.lib().mm_torque(self.h, _ptr(md), noise_step, dt_thermal, _ptr(t), None))
+        torch.cuda.synchronize(self.device)
+        return t, md
+
+    # ---- stepping
+    def solver(self, name="rk12", dt=1e-15, mindt=1e-38, maxdt=1e38, maxerr=1.0 / 2000):
+        nat.check(nat.lib().mm_solver_init(self.h, nat.SOLVERS[name], dt, mindt, maxdt, maxerr))
+        self._solver = name
+
+    def set_state(self, m):
+        md = self._dev(m)
+        nat.check(nat.lib().mm_set_state(self.h, _ptr(md), 0, None))
+
+    def get_state(self):
+        out = np.zeros(3 * self.N, dtype=np.float32)
+        nat.check(nat.lib().mm_get_state(self.h, out.ctypes.data_as(C.c_void_p), 1, None))
+        return out
+
+    def set_time(self, t, dt=0.0):
+        nat.check(nat.lib().mm_set_time(self.h, t, dt))
+
+    def set_thermal_dt(self, dt):
+        nat.check(nat.lib().mm_set_thermal_dt(self.h, dt))
+
+    def step(self):
+        nat.check(nat.lib().mm_step(self.h, None))
+
+    def steps(self, n):
+        nat.check(nat.lib().mm_steps(self.h, int(n), None))
+
+    def run(self, duration):
+        nat.check(nat.lib().mm_run(self.h, float(duration), None))
+
+    def run_until_maxtorque(self, thr, max_steps=0):
+        nat.check(nat.lib().mm_run_until_maxtorque(self.h, float(thr), int(max_steps), None))
+
+    def queue_attempts(self, n, stream=None):
+        nat.check(nat.lib().mm_queue_attempts(self.h, int(n), stream))
+
+    def stats(self):
+        s = nat.MMStats()
+        nat.check(nat.lib().mm_get_stats(self.h, C.byref(s), None))
+        return {k: getattr(s, k) for k, _ in nat.MMStats._fields_}
+
+    def maxtorque(self):
+        v = C.c_double()
+        nat.check(nat.lib().mm_maxtorque(self.h, C.byref(v), None))
+        return v.value
+
+    def average(self):
+        out = (C.c_double * 3)()
+        nat.check(nat.lib().mm_average(self.h, out, None))
+        return np.array(out[:])
+
+    def energy(self):
+        out = (C.c_double * 5)()
+        nat.check(nat.lib().mm_energy(self.h, out, None))
+        return dict(zip(["E_zeeman", "E_ex", "E_demag", "E_anis", "E"], out[:]))

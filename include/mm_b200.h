@@ -1,0 +1,144 @@
+/* mm_b200.h -- C-ABI of the B200-native micromagnetic hot path (fused tier).
+ *
+ * Plain C: pointers, sizes and status codes; no torch types.  All arrays are SoA
+ * float32, one contiguous block per component, C order [z][y][x] in the reference's
+ * INTERNAL axis order (Z,Y,X) = (0,1,2) (src/mumax/gpu/array.go:120-130,
+ * src/mumax/engine/api.go:13,44).  Device pointers unless stated otherwise.
+ *
+ * Which reference interface each entry point replaces:
+ *   mm_plan_create        MaxwellPlan.init/EnableDemag/loadDipoleKernel/LoadKernel
+ *                         (src/mumax/modules/maxwell_convolution.go:72-100,112-120,176-192,313-410)
+ *                         + Kernel_Arne (src/mumax/modules/kernel_magnetostatic.go:30-181)
+ *   mm_fields             the H_eff SumUpdater and its parents: MaxwellPlan.UpdateB
+ *                         (maxwell_convolution.go:222-309), exch6Updater (mod_exchange6.go:40-51),
+ *                         UniaxialAnisUpdater (mod_uniaxialanisotropy.go:44-57), zeeman
+ *                         (mod_zeeman.go:23-31, update_sum.go:29-75), TempBrownUpdater
+ *                         (mod_temperature.go:71-134)
+ *   mm_torque             torqueUpdater (mod_llg.go:59-70) + AddTermUpdater of zzt/stt
+ *                         (update_addterm.go:26-40, mod_zhang-li.go:50-70, mod_slonczewski.go:56-99)
+ *   mm_solver_init/mm_step/mm_run/mm_steps/mm_run_until_maxtorque
+ *                         Solver.Step (src/mumax/engine/solver.go:14-17): solver/rk12
+ *                         (solve_rk12.go:91-214), euler (solve_euler.go:22-50), heun
+ *                         (solve_heun.go:27-79); Engine.Run/Steps (engine.go:489-524);
+ *                         API.Run_Until_Smaller (api.go:122-131).  rk23/rk45 are new.
+ *   mm_maxtorque          MaxNormUpdater (update_reduce.go:103-108, reductor.go:173-186)
+ *   mm_average            AverageUpdater (update_reduce.go:47-69)
+ *   mm_energy             EnergyUpdater/SDotUpdater (mod_energy.go:24-95, update_sdot.go:36-62)
+ */
+#ifndef MM_B200_H
+#define MM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(_WIN32)
+#define MM_API __declspec(dllexport)
+#else
+#define MM_API __attribute__((visibility("default")))
+#endif
+
+/* status codes (0 = ok, negative = error class) */
+enum {
+    MM_OK = 0,
+    MM_ERR_ARG = -1,           /* invalid argument / unsupported size */
+    MM_ERR_CUDA = -2,          /* CUDA runtime error */
+    MM_ERR_NOT_CONVERGED = -3, /* more than 10 rejected attempts in one step (solve_rk12.go:205) */
+    MM_ERR_NAN = -4,           /* NaN in the state (quant.go:427-432) */
+    MM_ERR_STATE = -5,         /* call out of order (no solver, no state, ...) */
+    MM_ERR_TIMEOUT = -6        /* a bounded device wait gave up */
+};
+
+/* solvers */
+enum { MM_EULER = 0, MM_HEUN = 1, MM_RK12 = 2, MM_RK23 = 3, MM_RK45 = 4 };
+
+/* Problem description.  Multipliers in SI units; masks are DEVICE float arrays of
+ * n0*n1*n2 values multiplying the multiplier (NULL = uniform 1), exactly the
+ * MASK-quantity convention of the reference (common_func.h:298-301). */
+typedef struct mm_problem {
+    int n[3];          /* cells, internal order (Z,Y,X) */
+    double cell[3];    /* cell size (m), internal order */
+    int pbc[3];        /* periodic flags, internal order */
+    int demag, exchange, anis, zeeman, thermal, zhangli, slonczewski; /* terms on/off */
+    int demag_accuracy;                  /* Kernel_Arne accuracy (6 for module demag) */
+    double msat, aex, alpha, gamma;      /* A/m, J/m, -, m/As */
+    double bext[3];                      /* T */
+    double ku, anisu[3];                 /* J/m^3, unit vector */
+    double temp;                         /* K */
+    unsigned long long seed;             /* thermal Philox key */
+    double j[3];                         /* A/m^2 */
+    double zl_pol, xi;                   /* Zhang-Li polarisation, non-adiabaticity */
+    double p[3], sl_pol, lambda, eps_prime, t_fl; /* Slonczewski */
+    const float *msat_mask, *aex_mask, *alpha_mask, *ku_mask;
+    const float *anisu_mask[3], *bext_mask[3], *j_mask[3];
+    const float *temp_mask, *xi_mask, *zl_pol_mask;
+    const float *p_mask[3];
+    const float *sl_pol_mask, *lambda_mask, *eps_prime_mask, *t_fl_mask;
+} mm_problem;
+
+typedef struct mm_stats {
+    double t, dt, err, peakerr, maxtorque;
+    long long step, badsteps, attempts, evals;
+    int status, done;
+} mm_stats;
+
+typedef struct mm_plan_s* mm_plan;
+typedef struct CUstream_st* mm_stream; /* cudaStream_t; NULL = legacy default stream */
+
+/* Last error message of the calling thread ("" if none). */
+MM_API const char* mm_last_error(void);
+MM_API const char* mm_version(void);
+
+/* Builds the plan: geometry, demag tensor (FP64 on the GPU), its transform, and all
+ * workspaces; nothing is allocated after this call.  Runs on the current device. */
+MM_API int mm_plan_create(const mm_problem* prob, mm_plan* out);
+MM_API int mm_plan_destroy(mm_plan plan);
+/* Replaces multipliers/masks/terms of an existing plan (same grid, cell, pbc). */
+MM_API int mm_plan_set_problem(mm_plan plan, const mm_problem* prob);
+/* Non-zero demag tensor components (xx yy zz yz xz xy, internal order). */
+MM_API int mm_plan_kernel_nonzero(mm_plan plan, int out6[6]);
+/* Bytes of device memory held by the plan. */
+MM_API long long mm_plan_device_bytes(mm_plan plan);
+
+/* Per-term fields at m (which is used as given, not normalised).  Any output may be
+ * NULL.  noise_step selects the thermal noise sample, dt_thermal its dt. */
+MM_API int mm_fields(mm_plan plan, const float* m, long long noise_step, double dt_thermal,
+                     float* h_demag, float* h_ex, float* h_anis, float* h_zee, float* h_therm,
+                     float* h_eff, mm_stream stream);
+/* Torque array tau/gamma (+ spin-transfer terms / gamma) at normalise(m); m is
+ * normalised in place first, as pulling "m" does in the reference. */
+MM_API int mm_torque(mm_plan plan, float* m, long long noise_step, double dt_thermal,
+                     float* torque, mm_stream stream);
+
+/* ---- time stepping: the plan owns the state; all control runs on the device ---- */
+MM_API int mm_solver_init(mm_plan plan, int solver, double dt, double mindt, double maxdt,
+                          double maxerr);
+MM_API int mm_set_state(mm_plan plan, const float* m, int from_host, mm_stream stream);
+MM_API int mm_get_state(mm_plan plan, float* m, int to_host, mm_stream stream);
+MM_API int mm_set_time(mm_plan plan, double t, double dt);
+MM_API int mm_set_thermal_dt(mm_plan plan, double dt_thermal);
+/* One accepted step (retries included). */
+MM_API int mm_step(mm_plan plan, mm_stream stream);
+/* Steps until t >= t_start + duration (Engine.Run). */
+MM_API int mm_run(mm_plan plan, double duration, mm_stream stream);
+/* Exactly n accepted steps (Engine.Steps). */
+MM_API int mm_steps(mm_plan plan, long long n, mm_stream stream);
+/* Steps until maxtorque = gamma*max|tau| < thr (run_until_smaller("maxtorque", thr)). */
+MM_API int mm_run_until_maxtorque(mm_plan plan, double thr, long long max_steps, mm_stream stream);
+/* Queue `attempts` step attempts with no host synchronisation (CUDA-graph replay). */
+MM_API int mm_queue_attempts(mm_plan plan, int attempts, mm_stream stream);
+MM_API int mm_get_stats(mm_plan plan, mm_stats* out, mm_stream stream);
+
+/* ---- reductions of the current state ---- */
+MM_API int mm_maxtorque(mm_plan plan, double* out, mm_stream stream);
+MM_API int mm_average(mm_plan plan, double out[3], mm_stream stream);
+/* E_zeeman, E_ex, E_demag, E_anis, E (J) -- compensated FP32 sums. */
+MM_API int mm_energy(mm_plan plan, double out[5], mm_stream stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MM_B200_H */

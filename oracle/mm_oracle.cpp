@@ -1,0 +1,938 @@
+// mm_oracle.cpp -- FP64 CPU oracle for the micromagnetic hot path.
+//
+// TEST INFRASTRUCTURE ONLY.  This file is the checker: only tests/, the smoke()
+// entry point and bench.py's cpu_baseline / reference legs may load it.  The
+// product (2_b200/) never links, loads or calls it.
+//
+// It restates, in double precision and in plain loops, the discretisation used by
+// MuMax2 (reference paths are relative to the mumax/2 project root):
+//   demag tensor         src/mumax/modules/kernel_magnetostatic.go:30-193 (Kernel_Arne, delta)
+//                        src/mumax/modules/kernel.go:19-40 (Wrap, padSize)
+//   demag convolution    src/mumax/modules/maxwell_convolution.go:222-309 (UpdateB/update),
+//                        :313-410 (LoadKernel: symmetric use of the upper triangle, IsZero drop),
+//                        src/mumax/engine/zeropad.go:12-22 (PadSize)
+//   exchange6            src/libmumax2/exchange6.cu:12-142, common_func.h:298-317
+//                        src/mumax/modules/mod_exchange6.go:40-51 (pre = 2 Aex/(mu0 Ms))
+//   uniaxial anisotropy  src/libmumax2/uniaxialanisotropy.cu:12-86, mod_uniaxialanisotropy.go:44-57
+//   zeeman               src/mumax/modules/mod_zeeman.go:23-31 (H += B_ext/mu0)
+//   thermal (Brown)      src/libmumax2/temperature.cu:14-66, mod_temperature.go:71-134
+//   LLG torque           src/libmumax2/torque.cu:13-57, mod_llg.go:59-70 (multiplier gamma)
+//   Zhang-Li             src/libmumax2/zhang-li_torque.cu:123-300, mod_zhang-li.go:50-70
+//   Slonczewski          src/libmumax2/slonczewski_torque.cu:14-116, mod_slonczewski.go:56-99
+//   STT sum              src/mumax/engine/update_addterm.go:26-40 (added with weight 1/gamma)
+//   normalize            src/libmumax2/normalize.cu:14-42
+//   RK12 (adaptive Heun) src/mumax/engine/solve_rk12.go:91-214
+//   Heun / Euler         src/mumax/engine/solve_heun.go:27-79, solve_euler.go:22-50
+//   reductions           src/mumax/engine/update_reduce.go:47-108, gpu/reductor.go:69-186
+//   energy               src/mumax/modules/mod_energy.go:24-95, engine/update_sdot.go:36-62
+//   constants            src/mumax/common/constants.go:16-25
+// RK23 (Bogacki-Shampine 1989) and RK45 (Dormand-Prince 1980) have no counterpart in
+// the reference; they follow the published tableaux with the RK12 step controller.
+//
+// Axis convention: everything here is in the reference's INTERNAL order
+// (Z,Y,X) = (0,1,2); arrays are SoA [comp][n0][n1][n2], C order.
+
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+typedef std::complex<double> cplx;
+
+static const double PI = 3.14159265358979323846264338327950288;
+static const double MU0 = 4.0 * PI * 1e-7;
+static const double KB = 1.380650424E-23;
+static const double MUB = 9.2740091523E-24;
+static const double QE = 1.60217646E-19;
+static const double HBAR = 1.054571726E-34;
+
+extern "C" {
+
+// Problem description shared with the Python test harness (field order matters).
+typedef struct {
+    int n[3];
+    double cell[3];
+    int pbc[3];
+    int demag, exchange, anis, zeeman, thermal, zhangli, slonczewski;
+    int demag_accuracy;
+    double msat, aex, alpha, gamma;
+    double bext[3];
+    double ku, anisu[3];
+    double temp;
+    unsigned long long seed;
+    double j[3];
+    double zl_pol, xi;
+    double p[3], sl_pol, lambda, eps_prime, t_fl;
+    // masks: host float arrays of n0*n1*n2 values, NULL = uniform 1
+    const float *msat_mask, *aex_mask, *alpha_mask, *ku_mask;
+    const float *anisu_mask[3], *bext_mask[3], *j_mask[3];
+    const float *temp_mask, *xi_mask, *zl_pol_mask;
+    const float *p_mask[3];
+    const float *sl_pol_mask, *lambda_mask, *eps_prime_mask, *t_fl_mask;
+} or_desc;
+
+typedef struct {
+    double t, dt, mindt, maxdt, maxerr;
+    double err, peakerr;
+    long long step, badsteps, evals;
+    long long noise_step;   // counter used for the thermal field of this step
+    double dt_thermal;      // dt used to scale the thermal field (0 = use dt)
+} or_state;
+
+}  // extern "C"
+
+// ---------------------------------------------------------------- helpers
+static inline double mk(const float* m, long i) { return m ? (double)m[i] : 1.0; }
+
+static bool is_pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
+
+// In-place 1-D complex FFT (sign -1 forward, +1 inverse, unnormalised).
+// Radix-2 iterative for powers of two, direct DFT otherwise.
+static void fft1d(cplx* a, int n, int sign, std::vector<cplx>& tmp) {
+    if (n <= 1) return;
+    if (is_pow2(n)) {
+        for (int i = 1, j = 0; i < n; i++) {
+            int bit = n >> 1;
+            for (; j & bit; bit >>= 1) j ^= bit;
+            j ^= bit;
+            if (i < j) std::swap(a[i], a[j]);
+        }
+        for (int len = 2; len <= n; len <<= 1) {
+            double ang = sign * 2.0 * PI / len;
+            for (int i = 0; i < n; i += len) {
+                for (int k = 0; k < len / 2; k++) {
+                    cplx w(std::cos(ang * k), std::sin(ang * k));
+                    cplx u = a[i + k], v = a[i + k + len / 2] * w;
+                    a[i + k] = u + v;
+                    a[i + k + len / 2] = u - v;
+                }
+            }
+        }
+    } else {
+        tmp.assign(n, cplx(0, 0));
+        for (int k = 0; k < n; k++) {
+            cplx s(0, 0);
+            for (int x = 0; x < n; x++) {
+                double ang = sign * 2.0 * PI * (double)((long long)k * x % n) / n;
+                s += a[x] * cplx(std::cos(ang), std::sin(ang));
+            }
+            tmp[k] = s;
+        }
+        for (int k = 0; k < n; k++) a[k] = tmp[k];
+    }
+}
+
+// In-place 3-D complex FFT over an L0 x L1 x L2 array.
+static void fft3d(cplx* a, const int L[3], int sign) {
+    const long L0 = L[0], L1 = L[1], L2 = L[2];
+    // axis 2 (contiguous)
+#pragma omp parallel
+    {
+        std::vector<cplx> tmp, line(std::max(L0, std::max(L1, L2)));
+#pragma omp for
+        for (long r = 0; r < L0 * L1; r++) fft1d(a + r * L2, (int)L2, sign, tmp);
+#pragma omp for
+        for (long r = 0; r < L0 * L2; r++) {
+            long i = r / L2, k = r % L2;
+            for (long j = 0; j < L1; j++) line[j] = a[(i * L1 + j) * L2 + k];
+            fft1d(line.data(), (int)L1, sign, tmp);
+            for (long j = 0; j < L1; j++) a[(i * L1 + j) * L2 + k] = line[j];
+        }
+#pragma omp for
+        for (long r = 0; r < L1 * L2; r++) {
+            for (long i = 0; i < L0; i++) line[i] = a[i * L1 * L2 + r];
+            fft1d(line.data(), (int)L0, sign, tmp);
+            for (long i = 0; i < L0; i++) a[i * L1 * L2 + r] = line[i];
+        }
+    }
+}
+
+// ---------------------------------------------------------------- demag tensor
+// kernel.go:19-30
+static int wrap_idx(int number, int max) {
+    while (number < 0) number += max;
+    while (number >= max) number -= max;
+    return number;
+}
+// kernel_magnetostatic.go:184-193
+static double delta_d(int d) {
+    if (d < 0) d = -d;
+    if (d > 0) d -= 1;
+    return (double)d;
+}
+
+extern "C" void or_padded_size(const int n[3], const int pbc[3], int L[3]) {
+    for (int i = 0; i < 3; i++) L[i] = (n[i] > 1 && pbc[i] == 0) ? 2 * n[i] : n[i];
+}
+
+// Kernel_Arne restated (kernel_magnetostatic.go:30-181).  K is [s][d][L0][L1][L2]
+// (9 components, source s, destination d), accumulated in double.  If round_f32 is
+// set, each contribution is rounded to float before accumulation, as the
+// reference stores into a float32 host array (:170-173).
+extern "C" void or_kernel_arne(const int size[3], const double cs[3], const int periodic[3],
+                               int accuracy_, int round_f32, double* K) {
+    const long NL = (long)size[0] * size[1] * size[2];
+    std::fill(K, K + 9 * NL, 0.0);
+    const double accuracy = (double)accuracy_;
+    int x1 = -(size[0] - 1) / 2, x2 = size[0] / 2 - 1;
+    int y1 = -(size[1] - 1) / 2, y2 = size[1] / 2 - 1;
+    int z1 = -(size[2] - 1) / 2, z2 = size[2] / 2 - 1;
+    if (size[0] == 1 && periodic[0] == 0) x2 = 0;
+    x1 *= (periodic[0] + 1); x2 *= (periodic[0] + 1);
+    y1 *= (periodic[1] + 1); y2 *= (periodic[1] + 1);
+    z1 *= (periodic[2] + 1); z2 *= (periodic[2] + 1);
+    double L = cs[0];
+    if (cs[1] < L) L = cs[1];
+    if (cs[2] < L) L = cs[2];
+
+    for (int s = 0; s < 3; s++) {
+        const int u = s, v = (s + 1) % 3, w = (s + 2) % 3;
+        // Parallel over x only when the x loop has no periodic images that wrap onto
+        // the same output index (then accumulation would race).
+        const bool par_ok = (periodic[0] == 0);
+#pragma omp parallel for schedule(dynamic) if (par_ok)
+        for (int x = x1; x <= x2; x++) {
+            const int xw = wrap_idx(x, size[0]);
+            double R[3], R2[3], pole[3];
+            R[0] = (double)x * cs[0];
+            for (int y = y1; y <= y2; y++) {
+                const int yw = wrap_idx(y, size[1]);
+                R[1] = (double)y * cs[1];
+                for (int z = z1; z <= z2; z++) {
+                    const int zw = wrap_idx(z, size[2]);
+                    R[2] = (double)z * cs[2];
+                    double dx = delta_d(x) * cs[0], dy = delta_d(y) * cs[1], dz = delta_d(z) * cs[2];
+                    double d = std::sqrt(dx * dx + dy * dy + dz * dz);
+                    if (d == 0) d = L;
+                    double maxSize = d / accuracy;
+                    int nv = (int)(std::max(cs[v] / maxSize, 1.) + 0.5);
+                    int nw = (int)(std::max(cs[w] / maxSize, 1.) + 0.5);
+                    int nx = (int)(std::max(cs[0] / maxSize, 1.) + 0.5);
+                    int ny = (int)(std::max(cs[1] / maxSize, 1.) + 0.5);
+                    int nz = (int)(std::max(cs[2] / maxSize, 1.) + 0.5);
+                    nv *= 2;
+                    nw *= 2;
+                    double scale = 1 / (double)(nv * nw * nx * ny * nz);
+                    double surface = cs[v] * cs[w];
+                    double charge = surface * scale;
+                    double pu1 = cs[u] / 2.;
+                    double pu2 = -pu1;
+                    double B[3] = {0, 0, 0};
+                    for (int i = 0; i < nv; i++) {
+                        double pv = -(cs[v] / 2.) + cs[v] / (double)(2 * nv) + (double)i * (cs[v] / (double)nv);
+                        pole[v] = pv;
+                        for (int j = 0; j < nw; j++) {
+                            double pw = -(cs[w] / 2.) + cs[w] / (double)(2 * nw) + (double)j * (cs[w] / (double)nw);
+                            pole[w] = pw;
+                            for (int a = 0; a < nx; a++) {
+                                double rx = R[0] - cs[0] / 2. + cs[0] / (double)(2 * nx) + (cs[0] / (double)nx) * (double)a;
+                                for (int b = 0; b < ny; b++) {
+                                    double ry = R[1] - cs[1] / 2. + cs[1] / (double)(2 * ny) + (cs[1] / (double)ny) * (double)b;
+                                    for (int c = 0; c < nz; c++) {
+                                        double rz = R[2] - cs[2] / 2. + cs[2] / (double)(2 * nz) + (cs[2] / (double)nz) * (double)c;
+                                        pole[u] = pu1;
+                                        R2[0] = rx - pole[0]; R2[1] = ry - pole[1]; R2[2] = rz - pole[2];
+                                        double r = std::sqrt(R2[0] * R2[0] + R2[1] * R2[1] + R2[2] * R2[2]);
+                                        double qr = charge / (4. * PI * r * r * r);
+                                        double bx = R2[0] * qr, by = R2[1] * qr, bz = R2[2] * qr;
+                                        pole[u] = pu2;
+                                        R2[0] = rx - pole[0]; R2[1] = ry - pole[1]; R2[2] = rz - pole[2];
+                                        r = std::sqrt(R2[0] * R2[0] + R2[1] * R2[1] + R2[2] * R2[2]);
+                                        qr = -charge / (4. * PI * r * r * r);
+                                        B[0] += (bx + R2[0] * qr);
+                                        B[1] += (by + R2[1] * qr);
+                                        B[2] += (bz + R2[2] * qr);
+                                    }
+                                }
+                            }
+                        }
+                    }
+                    long idx = ((long)xw * size[1] + yw) * size[2] + zw;
+                    for (int dd = 0; dd < 3; dd++) {
+                        double val = round_f32 ? (double)(float)B[dd] : B[dd];
+                        K[(long)(s * 3 + dd) * NL + idx] += val;
+                    }
+                }
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------- Philox4x32-10
+// Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as easy as 1, 2, 3", SC'11.
+static inline void philox4x32_10(uint32_t ctr[4], uint32_t key0, uint32_t key1) {
+    const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u, W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
+    for (int r = 0; r < 10; r++) {
+        uint64_t p0 = (uint64_t)M0 * ctr[0];
+        uint64_t p1 = (uint64_t)M1 * ctr[2];
+        uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
+        uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+        uint32_t n0 = hi1 ^ ctr[1] ^ key0;
+        uint32_t n1 = lo1;
+        uint32_t n2 = hi0 ^ ctr[3] ^ key1;
+        uint32_t n3 = lo0;
+        ctr[0] = n0; ctr[1] = n1; ctr[2] = n2; ctr[3] = n3;
+        key0 += W0;
+        key1 += W1;
+    }
+}
+
+// Three standard normals for (cell, step): counter = (cell, step_lo, step_hi, 0x7e57),
+// key = seed; Box-Muller on the two pairs of 24-bit uniforms ((u>>8) + 0.5) * 2^-24 in (0,1).
+extern "C" void or_thermal_normals(unsigned long long seed, long long cell, long long step, double out[3]) {
+    uint32_t c[4] = {(uint32_t)cell, (uint32_t)((unsigned long long)step & 0xffffffffu),
+                     (uint32_t)((unsigned long long)step >> 32), 0x7e57u};
+    philox4x32_10(c, (uint32_t)(seed & 0xffffffffu), (uint32_t)(seed >> 32));
+    const double s = 5.9604644775390625e-08;  // 2^-24 (24-bit uniforms, exact in float too)
+    double u0 = ((double)(c[0] >> 8) + 0.5) * s, u1 = ((double)(c[1] >> 8) + 0.5) * s;
+    double u2 = ((double)(c[2] >> 8) + 0.5) * s, u3 = ((double)(c[3] >> 8) + 0.5) * s;
+    double r0 = std::sqrt(-2.0 * std::log(u0));
+    double r1 = std::sqrt(-2.0 * std::log(u2));
+    out[0] = r0 * std::cos(2.0 * PI * u1);
+    out[1] = r0 * std::sin(2.0 * PI * u1);
+    out[2] = r1 * std::cos(2.0 * PI * u3);
+}
+
+// ---------------------------------------------------------------- problem
+struct OrProblem {
+    or_desc d;
+    long N;
+    int L[3];
+    long NL;
+    bool comp_nonzero[6];             // xx yy zz yz xz xy
+    std::vector<cplx> khat[6];        // FFT of K (full complex, unnormalised)
+    std::vector<cplx> work[3];
+    // owned mask copies (the desc points at caller memory only during or_create)
+    std::vector<std::vector<float>> owned;
+};
+
+static const float* own_mask(OrProblem* P, const float* src) {
+    if (!src) return nullptr;
+    P->owned.emplace_back(src, src + P->N);
+    return P->owned.back().data();
+}
+
+// (s,d) pairs of the six unique symmetric components, in the order xx yy zz yz xz xy,
+// taken from the upper triangle as LoadKernel does (maxwell_convolution.go:340-376,
+// common/index.go IdxToIJ).
+static const int SYM_S[6] = {0, 1, 2, 1, 0, 0};
+static const int SYM_D[6] = {0, 1, 2, 2, 2, 1};
+static int sym_index(int s, int d) {
+    if (s > d) std::swap(s, d);
+    if (s == d) return s;
+    if (s == 1 && d == 2) return 3;
+    if (s == 0 && d == 2) return 4;
+    return 5;
+}
+
+extern "C" void* or_create(const or_desc* desc) {
+    OrProblem* P = new OrProblem();
+    P->d = *desc;
+    or_desc& d = P->d;
+    P->N = (long)d.n[0] * d.n[1] * d.n[2];
+    d.msat_mask = own_mask(P, desc->msat_mask);
+    d.aex_mask = own_mask(P, desc->aex_mask);
+    d.alpha_mask = own_mask(P, desc->alpha_mask);
+    d.ku_mask = own_mask(P, desc->ku_mask);
+    d.temp_mask = own_mask(P, desc->temp_mask);
+    d.xi_mask = own_mask(P, desc->xi_mask);
+    d.zl_pol_mask = own_mask(P, desc->zl_pol_mask);
+    d.sl_pol_mask = own_mask(P, desc->sl_pol_mask);
+    d.lambda_mask = own_mask(P, desc->lambda_mask);
+    d.eps_prime_mask = own_mask(P, desc->eps_prime_mask);
+    d.t_fl_mask = own_mask(P, desc->t_fl_mask);
+    for (int c = 0; c < 3; c++) {
+        d.anisu_mask[c] = own_mask(P, desc->anisu_mask[c]);
+        d.bext_mask[c] = own_mask(P, desc->bext_mask[c]);
+        d.j_mask[c] = own_mask(P, desc->j_mask[c]);
+        d.p_mask[c] = own_mask(P, desc->p_mask[c]);
+    }
+    or_padded_size(d.n, d.pbc, P->L);
+    P->NL = (long)P->L[0] * P->L[1] * P->L[2];
+    if (d.demag) {
+        std::vector<double> K(9 * P->NL);
+        or_kernel_arne(P->L, d.cell, d.pbc, d.demag_accuracy > 0 ? d.demag_accuracy : 6, 0, K.data());
+        double kmax = 0;
+        for (double v : K) kmax = std::max(kmax, std::fabs(v));
+        for (int q = 0; q < 6; q++) {
+            const double* src = &K[(long)(SYM_S[q] * 3 + SYM_D[q]) * P->NL];
+            double cmax = 0;
+            for (long i = 0; i < P->NL; i++) cmax = std::max(cmax, std::fabs(src[i]));
+            // maxwell_convolution.go:412-418 IsZero (zero_tolerance 1e-5 of the global max)
+            P->comp_nonzero[q] = kmax > 0 && (cmax / kmax) >= 1e-5;
+            if (!P->comp_nonzero[q]) continue;
+            P->khat[q].resize(P->NL);
+            for (long i = 0; i < P->NL; i++) P->khat[q][i] = cplx(src[i], 0);
+            fft3d(P->khat[q].data(), P->L, -1);
+        }
+        for (int c = 0; c < 3; c++) P->work[c].resize(P->NL);
+    }
+    return P;
+}
+
+extern "C" void or_destroy(void* p) { delete (OrProblem*)p; }
+
+extern "C" void or_kernel_nonzero(void* p, int* out6) {
+    OrProblem* P = (OrProblem*)p;
+    for (int q = 0; q < 6; q++) out6[q] = P->comp_nonzero[q];
+}
+
+// normalize.cu:14-42 (norm map = Msat mask)
+extern "C" void or_normalize(void* p, double* m) {
+    OrProblem* P = (OrProblem*)p;
+    const long N = P->N;
+    for (long i = 0; i < N; i++) {
+        double norm = P->d.msat_mask ? (double)P->d.msat_mask[i] : 1.0;
+        double x = m[i], y = m[N + i], z = m[2 * N + i];
+        double Mn = std::sqrt(x * x + y * y + z * z);
+        double scale = (norm == 0.0) ? 0.0 : 1.0;
+        scale = (Mn != 0.0) ? scale / Mn : 0.0;
+        m[i] = x * scale; m[N + i] = y * scale; m[2 * N + i] = z * scale;
+    }
+}
+
+// Demag field H = B/mu0 = Ms_mul * IFFT(Khat . FFT(pad(m * Msat_mask))) / prod(L)
+// (maxwell_convolution.go:222-309).
+static void demag_field(OrProblem* P, const double* m, double* H) {
+    const or_desc& d = P->d;
+    const int* n = d.n;
+    const int* L = P->L;
+    const long N = P->N, NL = P->NL;
+    for (int c = 0; c < 3; c++) {
+        cplx* w = P->work[c].data();
+        std::fill(w, w + NL, cplx(0, 0));
+        for (int i = 0; i < n[0]; i++)
+            for (int j = 0; j < n[1]; j++)
+                for (int k = 0; k < n[2]; k++) {
+                    long src = ((long)i * n[1] + j) * n[2] + k;
+                    long dst = ((long)i * L[1] + j) * L[2] + k;
+                    w[dst] = cplx(m[c * N + src] * mk(d.msat_mask, src), 0);
+                }
+        fft3d(w, L, -1);
+    }
+    std::vector<cplx> out(3 * NL);
+#pragma omp parallel for
+    for (long i = 0; i < NL; i++) {
+        cplx M[3] = {P->work[0][i], P->work[1][i], P->work[2][i]};
+        for (int dd = 0; dd < 3; dd++) {
+            cplx acc(0, 0);
+            for (int s = 0; s < 3; s++) {
+                int q = sym_index(s, dd);
+                if (P->comp_nonzero[q]) acc += P->khat[q][i] * M[s];
+            }
+            out[dd * NL + i] = acc;
+        }
+    }
+    for (int c = 0; c < 3; c++) {
+        fft3d(&out[c * NL], L, +1);
+        for (int i = 0; i < n[0]; i++)
+            for (int j = 0; j < n[1]; j++)
+                for (int k = 0; k < n[2]; k++) {
+                    long dst = ((long)i * n[1] + j) * n[2] + k;
+                    long src = ((long)i * L[1] + j) * L[2] + k;
+                    H[c * N + dst] = d.msat * out[c * NL + src].real() / (double)NL;
+                }
+    }
+}
+
+static inline double avg_geom_zero(double a, double b) {
+    double ab = a + b;
+    return (ab == 0.0) ? 0.0 : 2.0 * a * b / ab;
+}
+static inline double fdiv_zero(double a, double b) { return (b == 0.0) ? 0.0 : a / b; }
+
+// exchange6.cu:12-142 with pre = 2 Aex/(mu0 Ms) (mod_exchange6.go:47)
+static void exchange_field(OrProblem* P, const double* m, double* H) {
+    const or_desc& d = P->d;
+    const int N0 = d.n[0], N1 = d.n[1], N2 = d.n[2];
+    const long N = P->N;
+    const double pre = 2.0 * d.aex / (MU0 * d.msat);
+    const double c2[3] = {1.0 / (d.cell[0] * d.cell[0]), 1.0 / (d.cell[1] * d.cell[1]), 1.0 / (d.cell[2] * d.cell[2])};
+    const float* ms = d.msat_mask;
+    const float* ae = d.aex_mask;
+#pragma omp parallel for
+    for (int i = 0; i < N0; i++)
+        for (int j = 0; j < N1; j++)
+            for (int k = 0; k < N2; k++) {
+                long I = ((long)i * N1 + j) * N2 + k;
+                double lex0 = fdiv_zero(mk(ae, I), mk(ms, I));
+                double h[3] = {0, 0, 0};
+                for (int dir = 0; dir < 3; dir++) {
+                    int c[3] = {i, j, k};
+                    int nn = d.n[dir];
+                    long addr[2];
+                    for (int side = 0; side < 2; side++) {
+                        int idx = c[dir] + (side == 0 ? -1 : 1);
+                        if (side == 0) {
+                            if (idx < 0 && d.pbc[dir]) idx += nn;
+                            idx = std::max(idx, 0);
+                        } else {
+                            if (idx == nn && d.pbc[dir]) idx -= nn;
+                            idx = std::min(idx, nn - 1);
+                        }
+                        int cc[3] = {i, j, k};
+                        cc[dir] = idx;
+                        addr[side] = ((long)cc[0] * N1 + cc[1]) * N2 + cc[2];
+                    }
+                    double l1 = avg_geom_zero(lex0, fdiv_zero(mk(ae, addr[0]), mk(ms, addr[0])));
+                    double l2 = avg_geom_zero(lex0, fdiv_zero(mk(ae, addr[1]), mk(ms, addr[1])));
+                    for (int q = 0; q < 3; q++) {
+                        double m0 = m[q * N + I];
+                        h[q] += pre * c2[dir] * (l1 * (m[q * N + addr[0]] - m0) + l2 * (m[q * N + addr[1]] - m0));
+                    }
+                }
+                for (int q = 0; q < 3; q++) H[q * N + I] = h[q];
+            }
+}
+
+// uniaxialanisotropy.cu:12-86, multiplier 2 Ku/(mu0 Ms) (mod_uniaxialanisotropy.go:54)
+static void anis_field(OrProblem* P, const double* m, double* H) {
+    const or_desc& d = P->d;
+    const long N = P->N;
+    const double kmul = 2.0 * d.ku / (MU0 * d.msat);
+    for (long i = 0; i < N; i++) {
+        double msm = d.msat_mask ? (double)d.msat_mask[i] : 1.0;
+        if (msm == 0.0) msm = 1.0;
+        double k2 = (kmul / msm) * mk(d.ku_mask, i);
+        double u[3];
+        for (int c = 0; c < 3; c++) u[c] = d.anisu[c] * mk(d.anisu_mask[c], i);
+        double mu = m[i] * u[0] + m[N + i] * u[1] + m[2 * N + i] * u[2];
+        for (int c = 0; c < 3; c++) H[c * N + i] = k2 * mu * u[c];
+    }
+}
+
+// temperature.cu:14-66 scaling of standard normals; mod_temperature.go:115-127
+static void thermal_field(OrProblem* P, long long noise_step, double dt, double* H) {
+    const or_desc& d = P->d;
+    const long N = P->N;
+    const double V = d.cell[0] * d.cell[1] * d.cell[2];
+    const double aKT = d.alpha * KB * 2.0 * d.temp;
+    const double den = MU0 * V * d.gamma * dt * d.msat;
+    for (long i = 0; i < N; i++) {
+        double eta[3];
+        or_thermal_normals(d.seed, i, noise_step, eta);
+        double a = mk(d.alpha_mask, i), ms = mk(d.msat_mask, i), tm = mk(d.temp_mask, i);
+        for (int c = 0; c < 3; c++)
+            H[c * N + i] = (ms != 0.0) ? eta[c] * std::sqrt((a * tm * aKT) / (den * ms)) : 0.0;
+    }
+}
+
+// Per-term fields; any output may be NULL.
+extern "C" void or_fields(void* p, const double* m, long long noise_step, double dt_thermal,
+                          double* h_demag, double* h_ex, double* h_anis, double* h_zee,
+                          double* h_therm, double* h_eff) {
+    OrProblem* P = (OrProblem*)p;
+    const or_desc& d = P->d;
+    const long N = P->N;
+    std::vector<double> tmp(3 * N);
+    if (h_eff) std::fill(h_eff, h_eff + 3 * N, 0.0);
+    auto add = [&](double* dst) {
+        if (h_eff) for (long i = 0; i < 3 * N; i++) h_eff[i] += tmp[i];
+        if (dst) std::copy(tmp.begin(), tmp.end(), dst);
+    };
+    if (d.demag) { demag_field(P, m, tmp.data()); add(h_demag); }
+    if (d.exchange) { exchange_field(P, m, tmp.data()); add(h_ex); }
+    if (d.zeeman) {
+        for (int c = 0; c < 3; c++)
+            for (long i = 0; i < N; i++) tmp[c * N + i] = d.bext[c] * mk(d.bext_mask[c], i) / MU0;
+        add(h_zee);
+    }
+    if (d.anis) { anis_field(P, m, tmp.data()); add(h_anis); }
+    if (d.thermal && d.temp != 0.0) { thermal_field(P, noise_step, dt_thermal, tmp.data()); add(h_therm); }
+}
+
+// torque.cu:13-57 -> tau = (m x H - alpha m x (m x H)) / (1 + alpha^2), in the array
+// representation tau/gamma (multiplier gamma, mod_llg.go:59-70).
+static void llg_torque(const OrProblem* P, const double* m, const double* H, double* T) {
+    const or_desc& d = P->d;
+    const long N = P->N;
+    for (long i = 0; i < N; i++) {
+        double a = d.alpha * mk(d.alpha_mask, i);
+        double Mx = m[i], My = m[N + i], Mz = m[2 * N + i];
+        double Hx = H[i], Hy = H[N + i], Hz = H[2 * N + i];
+        double cx = My * Hz - Hy * Mz, cy = -Mx * Hz + Hx * Mz, cz = Mx * Hy - Hx * My;
+        double ddx = -My * cz + cy * Mz, ddy = Mx * cz - cx * Mz, ddz = -Mx * cy + cx * My;
+        double g = 1.0 / (1.0 + a * a);
+        T[i] = g * (cx + ddx * a);
+        T[N + i] = g * (cy + ddy * a);
+        T[2 * N + i] = g * (cz + ddz * a);
+    }
+}
+
+// "LHR" cross product of common_func.h:222-225 (crossf): -(a x b)
+static inline void crossf(const double a[3], const double b[3], double r[3]) {
+    r[0] = -a[1] * b[2] + a[2] * b[1];
+    r[1] = -a[2] * b[0] + a[0] * b[2];
+    r[2] = -a[0] * b[1] + a[1] * b[0];
+}
+
+// Zhang-Li torque zzt (units 1/s), zhang-li_torque.cu:123-300; pred from mod_zhang-li.go:66
+static void zhangli(const OrProblem* P, const double* m, double* out) {
+    const or_desc& d = P->d;
+    const int sx = d.n[0], sy = d.n[1], sz = d.n[2];
+    const long N = P->N, syz = (long)sy * sz;
+    const double pre = d.zl_pol * MUB / (QE * d.msat);
+    const double ms[3] = {1.0 / (12.0 * d.cell[0]), 1.0 / (12.0 * d.cell[1]), 1.0 / (12.0 * d.cell[2])};
+    // pbc.x = periodic[0], pbc.y = periodic[2]; dimension 1 wraps through the neighbour-GPU
+    // pointers, which on one GPU are the array itself when periodic[1] is set (:354-382)
+    const int pbc0 = d.pbc[0], pbc1 = d.pbc[1], pbc2 = d.pbc[2];
+    for (int i = 0; i < sx; i++)
+        for (int j = 0; j < sy; j++)
+            for (int k = 0; k < sz; k++) {
+                long x0 = i * syz + (long)j * sz + k;
+                double msat = d.msat_mask ? (double)d.msat_mask[x0] : 1.0;
+                double j0[3];
+                for (int c = 0; c < 3; c++) j0[c] = d.j_mask[c] ? d.j_mask[c][x0] * d.j[c] : d.j[c];
+                double njn = std::sqrt(j0[0] * j0[0] + j0[1] * j0[1] + j0[2] * j0[2]);
+                if (msat == 0.0 || njn == 0.0) {
+                    for (int c = 0; c < 3; c++) out[c * N + x0] = 0.0;
+                    continue;
+                }
+                msat = 1.0 / msat;
+                double PP = d.zl_pol_mask ? (double)d.zl_pol_mask[x0] : 1.0;
+                double pred = njn * PP * pre;
+                double ee = d.xi_mask ? d.xi_mask[x0] * d.xi : d.xi;
+                double al = d.alpha_mask ? d.alpha_mask[x0] * d.alpha : d.alpha;
+                pred = pred / ((1.0 + ee * ee) * (1.0 + al * al));
+                double pret = pred * (ee - al);
+                pred = pred * (1.0 + ee * al);
+                int xb2 = i - 2, xb1 = i - 1, xf1 = i + 1, xf2 = i + 2;
+                int yb2 = j - 2, yb1 = j - 1, yf1 = j + 1, yf2 = j + 2;
+                int zb2 = k - 2, zb1 = k - 1, zf1 = k + 1, zf2 = k + 2;
+                if (!pbc0) {
+                    if (xb2 < 0) xb2 = i; if (xb1 < 0) xb1 = i;
+                    if (xf1 >= sx) xf1 = i; if (xf2 >= sx) xf2 = i;
+                }
+                if (!pbc1) {
+                    if (yb2 < 0) yb2 = j; if (yb1 < 0) yb1 = j;
+                    if (yf1 >= sy) yf1 = j; if (yf2 >= sy) yf2 = j;
+                }
+                if (!pbc2) {
+                    if (zb2 < 0) zb2 = k; if (zb1 < 0) zb1 = k;
+                    if (zf1 >= sz) zf1 = k; if (zf2 >= sz) zf2 = k;
+                }
+                auto wr = [](int a, int n) { return a < 0 ? a + n : (a >= n ? a - n : a); };
+                xb2 = wr(xb2, sx); xb1 = wr(xb1, sx); xf1 = wr(xf1, sx); xf2 = wr(xf2, sx);
+                yb2 = wr(yb2, sy); yb1 = wr(yb1, sy); yf1 = wr(yf1, sy); yf2 = wr(yf2, sy);
+                zb2 = wr(zb2, sz); zb1 = wr(zb1, sz); zf1 = wr(zf1, sz); zf2 = wr(zf2, sz);
+                long comm = (long)j * sz + k;
+                long xn[4] = {xb2 * syz + comm, xb1 * syz + comm, xf1 * syz + comm, xf2 * syz + comm};
+                comm = i * syz + k;
+                long yn[4] = {(long)yb2 * sz + comm, (long)yb1 * sz + comm, (long)yf1 * sz + comm, (long)yf2 * sz + comm};
+                comm = i * syz + (long)j * sz;
+                long zn[4] = {zb2 + comm, zb1 + comm, zf1 + comm, zf2 + comm};
+                double dm[3][3];  // dm[c][dir]: derivative of m_c along internal axis dir
+                for (int c = 0; c < 3; c++) {
+                    const double* a = m + c * N;
+                    dm[c][0] = ms[0] * (a[xn[0]] - 8.0 * a[xn[1]] + 8.0 * a[xn[2]] - a[xn[3]]);
+                    dm[c][1] = ms[1] * (a[yn[0]] - 8.0 * a[yn[1]] + 8.0 * a[yn[2]] - a[yn[3]]);
+                    dm[c][2] = ms[2] * (a[zn[0]] - 8.0 * a[zn[1]] + 8.0 * a[zn[2]] - a[zn[3]]);
+                }
+                double nj[3] = {j0[0] / njn, j0[1] / njn, j0[2] / njn};
+                double dmdj[3];
+                for (int c = 0; c < 3; c++) dmdj[c] = dm[c][0] * nj[0] + dm[c][1] * nj[1] + dm[c][2] * nj[2];
+                double mm[3] = {m[x0], m[N + x0], m[2 * N + x0]};
+                double dmdjxm[3], mxdmxm[3];
+                crossf(dmdj, mm, dmdjxm);
+                crossf(mm, dmdjxm, mxdmxm);
+                for (int c = 0; c < 3; c++) out[c * N + x0] = msat * (pred * mxdmxm[c] + pret * dmdjxm[c]);
+            }
+}
+
+// Slonczewski torque stt (units 1/s), slonczewski_torque.cu:14-116; prefactors from
+// mod_slonczewski.go:77-79.  The world size (meshSize) argument is unused there.
+static void slonczewski(const OrProblem* P, const double* m, double* out) {
+    const or_desc& d = P->d;
+    const long N = P->N;
+    const double beta = HBAR * d.gamma / (MU0 * QE * d.msat);
+    const double beta_prime = d.sl_pol * beta;
+    const double pre_fld = beta * d.eps_prime;
+    for (long I = 0; I < N; I++) {
+        double Ms = d.msat_mask ? (double)d.msat_mask[I] : 1.0;
+        double J[3];
+        for (int c = 0; c < 3; c++) J[c] = d.j_mask[c] ? d.j_mask[c][I] * d.j[c] : d.j[c];
+        double nJn = std::sqrt(J[0] * J[0] + J[1] * J[1] + J[2] * J[2]);
+        double tfl = d.t_fl_mask ? d.t_fl_mask[I] * d.t_fl : d.t_fl;
+        if (nJn == 0.0 || Ms == 0.0 || tfl == 0.0) {
+            for (int c = 0; c < 3; c++) out[c * N + I] = 0.0;
+            continue;
+        }
+        tfl = 1.0 / tfl;
+        Ms = 1.0 / Ms;
+        double prex = beta_prime * Ms, prey = pre_fld * Ms;
+        double mm[3] = {m[I], m[N + I], m[2 * N + I]};
+        double p[3];
+        for (int c = 0; c < 3; c++) p[c] = d.p_mask[c] ? d.p[c] * d.p_mask[c][I] : d.p[c];
+        double pl = std::sqrt(p[0] * p[0] + p[1] * p[1] + p[2] * p[2]);
+        double pinv = (pl != 0.0) ? 1.0 / pl : 0.0;
+        for (int c = 0; c < 3; c++) p[c] *= pinv;
+        double pxm[3], mxpxm[3];
+        crossf(p, mm, pxm);
+        crossf(mm, pxm, mxpxm);
+        double pdotm = p[0] * mm[0] + p[1] * mm[1] + p[2] * mm[2];
+        double jinv = 1.0 / nJn;
+        double Jdir = (J[0] + J[1] + J[2]) * jinv;
+        double Jsign = Jdir / std::fabs(Jdir);  // NaN when Jx+Jy+Jz == 0, as in the reference
+        double nj = nJn * Jsign;
+        prex *= nj; prey *= nj;
+        prex *= tfl; prey *= tfl;
+        double lam = d.lambda_mask ? d.lambda * d.lambda_mask[I] : d.lambda;
+        double l2 = lam * lam;
+        double eps = l2 / ((l2 + 1.0) + (l2 - 1.0) * pdotm);
+        prex *= eps;
+        double al = d.alpha_mask ? d.alpha_mask[I] * d.alpha : d.alpha;
+        double af = 1.0 / (1.0 + al * al);
+        prex *= d.sl_pol_mask ? (double)d.sl_pol_mask[I] : 1.0;
+        prey *= d.eps_prime_mask ? (double)d.eps_prime_mask[I] : 1.0;
+        double f1 = (prex - al * prey) * af;
+        double f2 = (prey - al * prex) * af;
+        for (int c = 0; c < 3; c++) out[c * N + I] = f1 * mxpxm[c] + f2 * pxm[c];
+    }
+}
+
+// Torque array (tau/gamma, including spin-transfer terms divided by gamma) at m.
+// m is normalised in place first, as pulling "m" does in the reference.
+extern "C" void or_torque(void* p, double* m, long long noise_step, double dt_thermal,
+                          double* torque, double* h_eff_out) {
+    OrProblem* P = (OrProblem*)p;
+    const or_desc& d = P->d;
+    const long N = P->N;
+    or_normalize(p, m);
+    std::vector<double> H(3 * N);
+    or_fields(p, m, noise_step, dt_thermal, nullptr, nullptr, nullptr, nullptr, nullptr, H.data());
+    llg_torque(P, m, H.data(), torque);
+    if (h_eff_out) std::copy(H.begin(), H.end(), h_eff_out);
+    std::vector<double> s(3 * N);
+    if (d.zhangli) {
+        zhangli(P, m, s.data());
+        for (long i = 0; i < 3 * N; i++) torque[i] += s[i] / d.gamma;
+    }
+    if (d.slonczewski) {
+        slonczewski(P, m, s.data());
+        for (long i = 0; i < 3 * N; i++) torque[i] += s[i] / d.gamma;
+    }
+}
+
+extern "C" void or_stt(void* p, const double* m, double* zl, double* sl) {
+    OrProblem* P = (OrProblem*)p;
+    if (zl) zhangli(P, m, zl);
+    if (sl) slonczewski(P, m, sl);
+}
+
+// ---------------------------------------------------------------- reductions
+extern "C" double or_maxtorque(void* p, const double* torque) {
+    OrProblem* P = (OrProblem*)p;
+    const long N = P->N;
+    double mx = 0;
+    for (long i = 0; i < N; i++) {
+        double v = torque[i] * torque[i] + torque[N + i] * torque[N + i] + torque[2 * N + i] * torque[2 * N + i];
+        mx = std::max(mx, v);
+    }
+    return std::sqrt(mx) * P->d.gamma;
+}
+
+extern "C" void or_average(void* p, const double* a, double out[3]) {
+    OrProblem* P = (OrProblem*)p;
+    const long N = P->N;
+    for (int c = 0; c < 3; c++) {
+        double s = 0;
+        for (long i = 0; i < N; i++) s += a[c * N + i];
+        out[c] = s / (double)N;
+    }
+}
+
+// Energies E_zeeman, E_ex, E_demag, E_anis and the total (mod_energy.go:24-95).
+extern "C" void or_energy(void* p, const double* m_in, double out[5]) {
+    OrProblem* P = (OrProblem*)p;
+    const or_desc& d = P->d;
+    const long N = P->N;
+    const double V = d.cell[0] * d.cell[1] * d.cell[2];
+    std::vector<double> m(m_in, m_in + 3 * N);
+    or_normalize(p, m.data());
+    std::vector<double> H(3 * N);
+    auto dotsum = [&](const double* a, const double* b) {
+        double s = 0;
+        for (long i = 0; i < 3 * N; i++) s += a[i] * b[i];
+        return s;
+    };
+    for (int q = 0; q < 5; q++) out[q] = 0;
+    if (d.zeeman) {
+        for (int c = 0; c < 3; c++)
+            for (long i = 0; i < N; i++) H[c * N + i] = d.bext[c] * mk(d.bext_mask[c], i);
+        out[0] = -V * dotsum(m.data(), H.data()) * d.msat;
+    }
+    if (d.exchange) {
+        exchange_field(P, m.data(), H.data());
+        out[1] = -0.5 * V * MU0 * dotsum(m.data(), H.data()) * d.msat;
+    }
+    if (d.demag) {
+        demag_field(P, m.data(), H.data());
+        out[2] = -0.5 * V * MU0 * dotsum(m.data(), H.data()) * d.msat;  // B = mu0 H
+    }
+    if (d.anis) {
+        anis_field(P, m.data(), H.data());
+        out[3] = -0.5 * V * MU0 * dotsum(m.data(), H.data()) * d.msat;
+    }
+    out[4] = out[0] + out[1] + out[2] + out[3];
+}
+
+// ---------------------------------------------------------------- solvers
+enum { OR_EULER = 0, OR_HEUN = 1, OR_RK12 = 2, OR_RK23 = 3, OR_RK45 = 4 };
+
+static double ctrl_factor(double maxErr, double err, bool bad, int q) {
+    double factor = bad ? std::pow(maxErr / err, 1.0 / (q + 2)) : std::pow(maxErr / err, 1.0 / (q + 1));
+    factor *= 0.8;
+    if (factor > 1.5) factor = 1.5;
+    if (factor < 0.1) factor = 0.1;
+    return factor;
+}
+
+// Butcher tableaux (lower-triangular a, 5th/3rd-order b, error weights e = b - b*)
+static const double BS_A[4][4] = {{0, 0, 0, 0}, {0.5, 0, 0, 0}, {0, 0.75, 0, 0}, {2. / 9, 1. / 3, 4. / 9, 0}};
+static const double BS_E[4] = {2. / 9 - 7. / 24, 1. / 3 - 1. / 4, 4. / 9 - 1. / 3, -1. / 8};
+static const double DP_A[7][7] = {
+    {0, 0, 0, 0, 0, 0, 0},
+    {1. / 5, 0, 0, 0, 0, 0, 0},
+    {3. / 40, 9. / 40, 0, 0, 0, 0, 0},
+    {44. / 45, -56. / 15, 32. / 9, 0, 0, 0, 0},
+    {19372. / 6561, -25360. / 2187, 64448. / 6561, -212. / 729, 0, 0, 0},
+    {9017. / 3168, -355. / 33, 46732. / 5247, 49. / 176, -5103. / 18656, 0, 0},
+    {35. / 384, 0, 500. / 1113, 125. / 192, -2187. / 6784, 11. / 84, 0}};
+static const double DP_E[7] = {35. / 384 - 5179. / 57600, 0, 500. / 1113 - 7571. / 16695,
+                               125. / 192 - 393. / 640, -2187. / 6784 + 92097. / 339200,
+                               11. / 84 - 187. / 2100, -1. / 40};
+
+// One solver step in the reference's semantics.  m (3N) is the state; k_fsal (3N,
+// may be NULL for non-FSAL solvers) carries f(m) between RK23/RK45 steps and must be
+// flagged valid via *fsal_valid.  Returns 0, or -1 when the step failed to converge.
+extern "C" int or_step(void* p, int solver, double* m, or_state* st, double* k_fsal, int* fsal_valid) {
+    OrProblem* P = (OrProblem*)p;
+    const long N3 = 3 * P->N;
+    const double gam = P->d.gamma;
+    const long long ns = st->noise_step;
+    auto f = [&](double* y, double* k, double dtth) {
+        or_torque(p, y, ns, dtth, k, nullptr);
+        st->evals++;
+    };
+    if (solver == OR_EULER || solver == OR_HEUN) {
+        double dt = st->dt;
+        double dtth = st->dt_thermal > 0 ? st->dt_thermal : dt;
+        std::vector<double> k0(N3), k1(N3);
+        f(m, k0.data(), dtth);
+        for (long i = 0; i < N3; i++) m[i] += dt * gam * k0[i];
+        st->t += dt;
+        if (solver == OR_HEUN) {
+            f(m, k1.data(), dtth);
+            double h = dt * gam;
+            for (long i = 0; i < N3; i++) m[i] += 0.5 * h * k1[i] - 0.5 * h * k0[i];
+        }
+        or_normalize(p, m);
+        st->step++;
+        st->noise_step++;
+        return 0;
+    }
+    if (solver == OR_RK12) {
+        std::vector<double> y0(N3), k0(N3), k1(N3);
+        f(m, k0.data(), st->dt);
+        std::copy(m, m + N3, y0.begin());
+        const double t0 = st->t;
+        const int maxTry = 10;
+        int tr = 0;
+        for (;;) {
+            double dt = st->dt;
+            if (tr > 0) std::copy(y0.begin(), y0.end(), m);
+            for (long i = 0; i < N3; i++) m[i] += dt * gam * k0[i];
+            st->t = t0 + dt;
+            f(m, k1.data(), dt);
+            double h = dt * gam;
+            double md = 0;
+            for (long i = 0; i < N3; i++) {
+                m[i] += 0.5 * h * k1[i] - 0.5 * h * k0[i];
+                md = std::max(md, std::fabs(k1[i] - k0[i]));
+            }
+            double err = md * h;
+            st->err = err;
+            bool bad = err > st->maxerr;
+            if (bad) st->badsteps++;
+            if ((!bad || tr == maxTry - 1) && err > st->peakerr) st->peakerr = err;
+            double newDt = dt * ctrl_factor(st->maxerr, err, bad, 1);
+            newDt = std::max(newDt, st->mindt);
+            newDt = std::min(newDt, st->maxdt);
+            st->dt = newDt;
+            if (!bad || newDt == st->mindt) break;
+            if (tr > maxTry) return -1;
+            tr++;
+        }
+        or_normalize(p, m);
+        st->step++;
+        return 0;
+    }
+    // RK23 / RK45 with FSAL
+    const bool dp = (solver == OR_RK45);
+    const int S = dp ? 7 : 4;
+    const int q = dp ? 4 : 2;
+    std::vector<std::vector<double>> k(S, std::vector<double>(N3));
+    std::vector<double> y0(m, m + N3), y(N3);
+    if (k_fsal && fsal_valid && *fsal_valid) std::copy(k_fsal, k_fsal + N3, k[0].begin());
+    else { f(y0.data(), k[0].data(), st->dt); std::copy(y0.begin(), y0.end(), m); }
+    // y0 has been normalised by f (in place on the copy) -- keep m consistent
+    or_normalize(p, y0.data());
+    const double t0 = st->t;
+    const int maxTry = 10;
+    int tr = 0;
+    for (;;) {
+        double dt = st->dt;
+        double h = dt * gam;
+        for (int s = 1; s < S; s++) {
+            const double* a = dp ? DP_A[s] : BS_A[s];
+            for (long i = 0; i < N3; i++) {
+                double acc = y0[i];
+                for (int jj = 0; jj < s; jj++) acc += h * a[jj] * k[jj][i];
+                y[i] = acc;
+            }
+            if (s == S - 1) std::copy(y.begin(), y.end(), m);
+            f(y.data(), k[s].data(), dt);
+            if (s == S - 1) or_normalize(p, m);
+        }
+        double md = 0;
+        const double* e = dp ? DP_E : BS_E;
+        for (long i = 0; i < N3; i++) {
+            double acc = 0;
+            for (int s = 0; s < S; s++) acc += e[s] * k[s][i];
+            md = std::max(md, std::fabs(acc));
+        }
+        double err = md * h;
+        st->err = err;
+        st->t = t0 + dt;
+        bool bad = err > st->maxerr;
+        if (bad) st->badsteps++;
+        if ((!bad || tr == maxTry - 1) && err > st->peakerr) st->peakerr = err;
+        double newDt = dt * ctrl_factor(st->maxerr, err, bad, q);
+        newDt = std::max(newDt, st->mindt);
+        newDt = std::min(newDt, st->maxdt);
+        st->dt = newDt;
+        if (!bad || newDt == st->mindt) break;
+        if (tr > maxTry) return -1;
+        tr++;
+    }
+    if (k_fsal) std::copy(k[S - 1].begin(), k[S - 1].end(), k_fsal);
+    if (fsal_valid) *fsal_valid = 1;
+    st->step++;
+    return 0;
+}
+
+extern "C" int or_num_threads(void) {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}

@@ -1,0 +1,162 @@
+"""GPU parity of the effective-field terms and the torque against the FP64 oracle.
+
+Tolerance: FP32 arithmetic on the GPU against FP64 on the CPU; every field term must
+agree to 1e-5 relative (max |difference| / max |oracle|), the bound stated for H_eff.
+"""
+import numpy as np
+import pytest
+
+from helpers import rand_m, rel_err, to_np
+
+pytestmark = pytest.mark.gpu
+
+TOL_FIELD = 1e-5
+TOL_TORQUE = 1e-5
+
+
+def _pair(problem, masks_host=None):
+    import oracle as O
+    from mumax2 import Plan
+    prob = O.full_desc(**problem)
+    if masks_host:
+        prob["masks"] = masks_host
+    o = O.Oracle(prob)
+    g = Plan(prob, masks=masks_host or {})
+    return o, g
+
+
+@pytest.mark.parametrize("n,cell", [
+    ((1, 16, 32), (3e-9, 4e-9, 5e-9)),       # 2-D film, 4 kernel components
+    ((1, 32, 128), (3e-9, 3.90625e-9, 3.90625e-9)),  # SP4 geometry
+    ((4, 8, 16), (2e-9, 4e-9, 4e-9)),        # 3-D, 6 components
+    ((2, 4, 4), (4e-9, 4e-9, 3e-9)),         # tiny 3-D
+    ((8, 16, 8), (3e-9, 3e-9, 3e-9)),
+])
+def test_demag_field(n, cell):
+    o, g = _pair(dict(n=n, cell=cell, demag=1, exchange=0, msat=8e5))
+    assert g.kernel_nonzero() == o.nonzero_components()
+    m = rand_m(n, seed=1)
+    ho = o.fields(m)["demag"]
+    hg = to_np(g.fields(m)["demag"])
+    err = rel_err(hg, ho)
+    print("demag", n, err)
+    assert err < TOL_FIELD
+
+
+def test_demag_uniform_film_known_answer():
+    # uniform out-of-plane magnetisation of a wide thin film: H_z ~ -Ms in the centre
+    n = (1, 64, 64)
+    o, g = _pair(dict(n=n, cell=(2e-9, 5e-9, 5e-9), demag=1, exchange=0, msat=1e6))
+    N = 64 * 64
+    m = np.zeros(3 * N)
+    m[:N] = 1.0
+    hg = to_np(g.fields(m)["demag"]).reshape(3, 64, 64)
+    assert -1.0 < hg[0, 32, 32] / 1e6 < -0.95
+    assert abs(hg[1, 32, 32]) < 1e-3 * 1e6
+
+
+@pytest.mark.parametrize("n,pbc", [((3, 5, 7), (0, 0, 0)), ((1, 6, 9), (0, 1, 1)), ((4, 4, 4), (1, 0, 1)),
+                                   ((1, 1, 16), (0, 0, 0))])
+def test_exchange_with_masks(n, pbc):
+    rng = np.random.default_rng(3)
+    N = n[0] * n[1] * n[2]
+    msat_mask = rng.uniform(0.5, 1.5, N).astype(np.float32)
+    msat_mask[rng.random(N) < 0.1] = 0.0
+    aex_mask = rng.uniform(0.5, 2.0, N).astype(np.float32)
+    masks = dict(msat=msat_mask, aex=aex_mask)
+    o, g = _pair(dict(n=n, cell=(2e-9, 3e-9, 4e-9), pbc=pbc, demag=0, exchange=1, msat=7e5, aex=1.1e-11), masks)
+    m = o.normalize(rand_m(n, seed=2))
+    ho = o.fields(m)["ex"]
+    hg = to_np(g.fields(m)["ex"])
+    err = rel_err(hg, ho)
+    print("exchange", n, pbc, err)
+    assert err < TOL_FIELD
+
+
+def test_anisotropy_zeeman_masks():
+    n = (2, 6, 10)
+    rng = np.random.default_rng(4)
+    N = 120
+    masks = dict(msat=rng.uniform(0, 1, N).astype(np.float32), ku=rng.uniform(0, 2, N).astype(np.float32),
+                 anisu=[rng.uniform(-1, 1, N), None, rng.uniform(-1, 1, N)],
+                 bext=[None, rng.uniform(-1, 1, N), rng.uniform(0, 1, N)])
+    masks["msat"][:7] = 0
+    o, g = _pair(dict(n=n, cell=(3e-9, 3e-9, 3e-9), demag=0, exchange=0, anis=1, zeeman=1, ku=5e5,
+                      anisu=(0.3, 0.5, 0.8), bext=(0.01, -0.02, 0.03), msat=1.1e6), masks)
+    m = rand_m(n, seed=5)
+    fo, fg = o.fields(m), g.fields(m)
+    for k in ["anis", "zee"]:
+        err = rel_err(to_np(fg[k]), fo[k])
+        print(k, err)
+        assert err < TOL_FIELD
+
+
+def test_thermal_field_matches_oracle_noise():
+    n = (1, 8, 12)
+    o, g = _pair(dict(n=n, cell=(3e-9, 4e-9, 4e-9), demag=0, exchange=0, thermal=1, temp=300.0, alpha=0.05,
+                      seed=1234))
+    m = rand_m(n, seed=6)
+    for step in [0, 1, 77, 2**33 + 5]:
+        ho = o.fields(m, noise_step=step, dt_thermal=5e-14)["therm"]
+        hg = to_np(g.fields(m, noise_step=step, dt_thermal=5e-14)["therm"])
+        err = rel_err(hg, ho)
+        print("thermal", step, err)
+        assert err < 1e-5
+
+
+def test_thermal_statistics():
+    # the noise is standard normal per component and uncorrelated between steps
+    n = (1, 64, 64)
+    o, g = _pair(dict(n=n, cell=(3e-9, 4e-9, 4e-9), demag=0, exchange=0, thermal=1, temp=300.0, alpha=0.1,
+                      seed=99))
+    m = rand_m(n, seed=7)
+    a = to_np(g.fields(m, noise_step=0, dt_thermal=1e-13)["therm"])
+    b = to_np(g.fields(m, noise_step=1, dt_thermal=1e-13)["therm"])
+    V = 3e-9 * 4e-9 * 4e-9
+    sigma = np.sqrt(2 * 0.1 * 1.380650424e-23 * 300.0 / (4e-7 * np.pi * V * 2.211e5 * 1e-13 * 8e5))
+    z = a / sigma
+    assert abs(z.mean()) < 0.03 and abs(z.std() - 1) < 0.02
+    assert abs(np.corrcoef(a, b)[0, 1]) < 0.03
+
+
+@pytest.mark.parametrize("terms", [
+    dict(demag=1, exchange=1, zeeman=1, bext=(0.0, 4.3e-3, -24.6e-3)),
+    dict(demag=1, exchange=1, anis=1, ku=5e5, anisu=(1, 0, 0), alpha=0.1),
+    dict(demag=0, exchange=1, zhangli=1, j=(0, 0, 1e12), zl_pol=0.5, xi=0.05),
+    dict(demag=0, exchange=1, zhangli=1, j=(2e11, -1e12, 5e11), zl_pol=0.7, xi=0.1, pbc=(0, 1, 0)),
+    dict(demag=1, exchange=1, slonczewski=1, j=(1e11, 0, 0), p=(1, 0, 0), sl_pol=0.5669, **{"lambda": 2.0},
+         eps_prime=0.1, t_fl=3e-9),
+])
+def test_torque_parity(terms):
+    n = (2, 8, 16)
+    prob = dict(n=n, cell=(3e-9, 4e-9, 4e-9), msat=8.6e5, aex=1.3e-11, alpha=0.02)
+    prob.update(terms)
+    o, g = _pair(prob)
+    m = rand_m(n, seed=8)
+    to, _, _ = o.torque(m)
+    tg, _ = g.torque(m)
+    err = rel_err(to_np(tg), to)
+    print("torque", terms, err)
+    assert err < TOL_TORQUE
+
+
+def test_stt_with_masks():
+    n = (1, 12, 20)
+    N = 240
+    rng = np.random.default_rng(9)
+    masks = dict(msat=(rng.random(N) > 0.2).astype(np.float32), j=[None, None, rng.uniform(0.5, 1.5, N)],
+                 xi=rng.uniform(0.5, 1.5, N), zl_pol=rng.uniform(0.5, 1, N), alpha=rng.uniform(0.5, 2, N),
+                 p=[rng.uniform(-1, 1, N), rng.uniform(-1, 1, N), rng.uniform(0.1, 1, N)],
+                 t_fl=rng.uniform(0.5, 1.5, N), lambda_=None)
+    masks.pop("lambda_")
+    for kind in [dict(zhangli=1), dict(slonczewski=1, eps_prime=0.2, t_fl=2e-9, **{"lambda": 1.5})]:
+        prob = dict(n=n, cell=(2e-9, 2e-9, 2e-9), demag=0, exchange=1, msat=8.6e5, j=(0.0, 0.0, 1e12), zl_pol=0.5,
+                    xi=0.05, p=(0, 0, 1))
+        prob.update(kind)
+        o, g = _pair(prob, masks)
+        m = o.normalize(rand_m(n, seed=10))
+        to, _, _ = o.torque(m)
+        tg, _ = g.torque(m)
+        err = rel_err(to_np(tg), to)
+        print("stt masks", kind, err)
+        assert err < TOL_TORQUE
