@@ -245,6 +245,8 @@ struct mm_plan_s {
     unsigned int* tq = nullptr;
     bool state_set = false;
     bool run_until = false;
+    long long launches = 0;          // kernels enqueued by this plan (graph replays counted per node)
+    int graph_nodes = 0;
     cudaGraphExec_t graph = nullptr;
     int graph_solver = -1;
     bool graph_run_until = false;
@@ -508,8 +510,10 @@ static int launch_eval(mm_plan p, const StageOp& op, DevCtl* ctl, int skip_retry
             CUCHK(launch_colfft<float2>(L1, +1, p->S, g.h, 3 * n0, plane, g.hp, L1, n1, ctl, skip_retry, st));
         }
         CUCHK(launch_xinv_epi(g.M, p->S, g.hp, L1, A, terms, st, &nb));
+        p->launches += (L0 == 1) ? 3 : 5;
     } else {
         CUCHK(launch_local_epi(A, terms, st, &nb));
+        p->launches += 1;
     }
     if (nblocks_out) *nblocks_out = nb;
     return MM_OK;
@@ -591,6 +595,7 @@ static int launch_combine(mm_plan p, PP base, PP next, int nk, const PP* kp, con
     A.ctl = p->ctl;
     combine_kernel<<<local_blocks(p->g.N), 256, 0, st>>>(A);
     CUCHK(cudaGetLastError());
+    p->launches++;
     return MM_OK;
 }
 
@@ -627,6 +632,7 @@ static int enqueue_attempt(mm_plan p, cudaStream_t st) {
         if (p->run_until) {
             torque_check_kernel<<<1, 1, 0, st>>>(ctl);
             CUCHK(cudaGetLastError());
+            p->launches++;
         }
         if (s == MM_RK12) {
             // Euler predictor from the saved k0 (solve_rk12.go:133), also on retries
@@ -659,6 +665,7 @@ static int enqueue_attempt(mm_plan p, cudaStream_t st) {
         }
         controller_kernel<<<1, 1, 0, st>>>(ctl, s == MM_RK12 ? 1 : 0, 1, 0, s == MM_EULER ? 1 : 2, s == MM_RK12);
         CUCHK(cudaGetLastError());
+        p->launches++;
         return MM_OK;
     }
     // RK23 / RK45 (FSAL): K1[cur] = f(Y[cur]) is valid
@@ -714,6 +721,7 @@ static int enqueue_attempt(mm_plan p, cudaStream_t st) {
     }
     controller_kernel<<<1, 1, 0, st>>>(ctl, 1, dp ? 4 : 2, 1, S - 1, 0);
     CUCHK(cudaGetLastError());
+    p->launches++;
     return MM_OK;
 }
 
@@ -822,7 +830,10 @@ static int capture_attempt(mm_plan p) {
     cudaGraph_t gr;
     cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) { cudaStreamDestroy(cs); return set_err(MM_ERR_CUDA, "begin capture: %s", cudaGetErrorString(e)); }
+    const long long before = p->launches;
     int rc = enqueue_attempt(p, cs);
+    p->graph_nodes = (int)(p->launches - before);
+    p->launches = before;
     e = cudaStreamEndCapture(cs, &gr);
     cudaStreamDestroy(cs);
     if (rc) return rc;
@@ -842,6 +853,7 @@ extern "C" MM_API int mm_queue_attempts(mm_plan p, int attempts, mm_stream strea
     int rc = capture_attempt(p);
     if (rc) return rc;
     for (int a = 0; a < attempts; a++) CUCHK(cudaGraphLaunch(p->graph, st));
+    p->launches += (long long)attempts * p->graph_nodes;
     return MM_OK;
 }
 
@@ -1028,5 +1040,84 @@ extern "C" MM_API int mm_energy(mm_plan p, double out[5], mm_stream stream) {
     out[2] = q.demag ? -0.5 * V * MU0 * r[2] * q.msat : 0.0;
     out[3] = q.anis ? -0.5 * V * MU0 * r[3] * q.msat : 0.0;
     out[4] = out[0] + out[1] + out[2] + out[3];
+    return MM_OK;
+}
+
+extern "C" MM_API long long mm_plan_launch_count(mm_plan p) { return p ? p->launches : 0; }
+
+// Times each pass of one right-hand-side evaluation (at the accepted state, result
+// discarded) with CUDA events recorded on the launching stream between the passes;
+// ms_out[i] = average duration of pass i over `reps` evaluations.  Pass order:
+// 3-D: xfwd, y fwd, z mul, y inv, x inv + epilogue; 2-D: xfwd, y mul, x inv + epilogue;
+// no demag: epilogue only.
+extern "C" MM_API int mm_profile_eval(mm_plan p, int reps, double* ms_out, int* npass, mm_stream stream) {
+    if (!p || !ms_out || !npass || reps < 1) return set_err(MM_ERR_ARG, "bad argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    int rc = read_ctl(p, st);
+    if (rc) return rc;
+    const ConvGeom& g = p->g;
+    StageOp op = op_blank();
+    op.m_in = fixed(p->Y[p->ctl_host->cur]);
+    op.k_out = fixed(p->Mtmp);
+    EpiArgs A;
+    memset(&A, 0, sizeof A);
+    A.P = p->P;
+    A.op = op;
+    const int np = p->demag ? (g.L[0] == 1 ? 3 : 5) : 1;
+    *npass = np;
+    std::vector<cudaEvent_t> ev(np + 1);
+    for (auto& e : ev) CUCHK(cudaEventCreate(&e));
+    std::vector<double> acc(np, 0.0);
+    for (int r = 0; r < reps; r++) {
+        int k = 0;
+        CUCHK(cudaEventRecord(ev[k++], st));
+        int nb = 0;
+        if (p->demag) {
+            const int n0 = g.n[0], n1 = g.n[1], n2 = g.n[2];
+            const int L0 = g.L[0], L1 = g.L[1];
+            const long long plane = (long long)L1 * g.hp;
+            const float scale = (float)p->prob.msat;
+            CUCHK(launch_xfwd<float2, float>(g.M, nullptr, op.m_in, p->P.msat_mask, p->S, 3 * n0 * n1, n0, n1, L1,
+                                             n2, n2, g.hp, nullptr, 0, st));
+            CUCHK(cudaEventRecord(ev[k++], st));
+            if (L0 == 1) {
+                CUCHK(launch_colmul(L1, p->S, p->kv, g.h, 1, plane, 0, g.hp, n1, 1, scale, nullptr, 0, st));
+                CUCHK(cudaEventRecord(ev[k++], st));
+            } else {
+                CUCHK(launch_colfft<float2>(L1, -1, p->S, g.h, 3 * n0, plane, g.hp, n1, L1, nullptr, 0, st));
+                CUCHK(cudaEventRecord(ev[k++], st));
+                CUCHK(launch_colmul(L0, p->S, p->kv, g.h, L1, (long long)n0 * plane, g.hp, plane, n0, 0, scale,
+                                    nullptr, 0, st));
+                CUCHK(cudaEventRecord(ev[k++], st));
+                CUCHK(launch_colfft<float2>(L1, +1, p->S, g.h, 3 * n0, plane, g.hp, L1, n1, nullptr, 0, st));
+                CUCHK(cudaEventRecord(ev[k++], st));
+            }
+            CUCHK(launch_xinv_epi(g.M, p->S, g.hp, L1, A, false, st, &nb));
+        } else {
+            CUCHK(launch_local_epi(A, false, st, &nb));
+        }
+        CUCHK(cudaEventRecord(ev[k++], st));
+        CUCHK(cudaEventSynchronize(ev[np]));
+        for (int i = 0; i < np; i++) {
+            float ms = 0.f;
+            CUCHK(cudaEventElapsedTime(&ms, ev[i], ev[i + 1]));
+            acc[i] += ms;
+        }
+    }
+    for (int i = 0; i < np; i++) ms_out[i] = acc[i] / reps;
+    for (auto& e : ev) cudaEventDestroy(e);
+    return MM_OK;
+}
+
+// Geometry of the plan's transform: L[3], M, h, hp, kd[3], nonzero kernel components.
+extern "C" MM_API int mm_plan_geometry(mm_plan p, int* out12) {
+    if (!p || !out12) return set_err(MM_ERR_ARG, "bad argument");
+    const ConvGeom& g = p->g;
+    int v[12] = {g.L[0], g.L[1], g.L[2], g.M, g.h, g.hp, g.kd[0], g.kd[1], g.kd[2], 0, 0, 0};
+    int nzc = 0;
+    for (int q = 0; q < 6; q++) nzc += p->demag ? p->kv.nz[q] : 0;
+    v[9] = nzc;
+    v[10] = p->demag ? 1 : 0;
+    memcpy(out12, v, sizeof v);
     return MM_OK;
 }

@@ -86,6 +86,9 @@ _PROTOS = {
     "mm_maxtorque": (C.c_int, [C.c_void_p, DP, C.c_void_p]),
     "mm_average": (C.c_int, [C.c_void_p, C.c_double * 3, C.c_void_p]),
     "mm_energy": (C.c_int, [C.c_void_p, C.c_double * 5, C.c_void_p]),
+    "mm_plan_launch_count": (C.c_longlong, [C.c_void_p]),
+    "mm_profile_eval": (C.c_int, [C.c_void_p, C.c_int, DP, C.POINTER(C.c_int), C.c_void_p]),
+    "mm_plan_geometry": (C.c_int, [C.c_void_p, C.c_int * 12]),
 }
 
 

@@ -161,3 +161,19 @@ class Plan:
         out = (C.c_double * 5)()
         nat.check(nat.lib().mm_energy(self.h, out, None))
         return dict(zip(["E_zeeman", "E_ex", "E_demag", "E_anis", "E"], out[:]))
+
+    # ---- instrumentation
+    def launch_count(self):
+        return nat.lib().mm_plan_launch_count(self.h)
+
+    def profile_eval(self, reps=10):
+        out = (C.c_double * 8)()
+        npass = C.c_int()
+        nat.check(nat.lib().mm_profile_eval(self.h, int(reps), out, C.byref(npass), None))
+        return list(out[:npass.value])
+
+    def geometry(self):
+        out = (C.c_int * 12)()
+        nat.check(nat.lib().mm_plan_geometry(self.h, out))
+        v = list(out[:])
+        return dict(L=tuple(v[0:3]), M=v[3], h=v[4], hp=v[5], kd=tuple(v[6:9]), nk=v[9], demag=v[10])

@@ -1,0 +1,341 @@
+#!/usr/bin/env python
+"""Benchmark of the micromagnetic hot path (one JSON line on rank 0).
+
+Workload (default): 3-D film with perpendicular anisotropy, 256x256x16 cells of
+4x4x2 nm, Ms 1.1e6 A/m, Aex 1.5e-11 J/m, Ku1 5e5 J/m^3 along z, alpha 0.1, m seeded
+i.i.d. uniform on the sphere, no applied field, demag + exchange + anisotropy,
+adaptive RK23 (max error 1e-5).  A "step" is one accepted solver step (its rejected
+attempts included).  Metric: cell-steps/s = cells x accepted steps / device time.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+N > 1 (torchrun, one process per GPU): independent replicas, one simulation per GPU
+with its own seed (weak scaling); no collective in the step.  The reference arm times
+the FP64 CPU oracle (a restatement of the reference's discretisation; the reference
+itself has no CPU implementation of this path) on the host cores.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "2_b200"))
+
+MU0 = 4e-7 * np.pi
+
+WORKLOAD = dict(
+    name="film3d_256x256x16_perp_anis_rk23",
+    n=(16, 256, 256),                 # internal (z, y, x)
+    cell=(2e-9, 4e-9, 4e-9),
+    demag=1, exchange=1, anis=1, zeeman=0,
+    msat=1.1e6, aex=1.5e-11, ku=5e5, anisu=(1.0, 0.0, 0.0), alpha=0.1, gamma=2.211e5,
+    solver="rk23", maxerr=1e-5, dt0=1e-15,
+)
+
+
+def problem():
+    w = WORKLOAD
+    return dict(n=w["n"], cell=w["cell"], demag=w["demag"], exchange=w["exchange"], anis=w["anis"],
+                zeeman=w["zeeman"], msat=w["msat"], aex=w["aex"], ku=w["ku"], anisu=w["anisu"],
+                alpha=w["alpha"], gamma=w["gamma"])
+
+
+def initial_m(seed):
+    n = WORKLOAD["n"]
+    N = n[0] * n[1] * n[2]
+    rng = np.random.default_rng(seed)
+    v = rng.normal(size=(3, N))
+    v /= np.linalg.norm(v, axis=0, keepdims=True)
+    return v.astype(np.float32).ravel()
+
+
+# ---------------------------------------------------------------- byte model
+def pass_bytes(geo, n, masks=0):
+    """Algorithmic HBM bytes of each pass of one standalone field evaluation
+    (k written, no stage combine) in this design: only the non-zero half of the
+    padded data is stored, the kernel is one octant of nk FP32 components."""
+    N0, N1, N2 = n
+    N = N0 * N1 * N2
+    L0, L1, L2 = geo["L"]
+    h = geo["h"]
+    oct_ = geo["kd"][0] * geo["kd"][1] * geo["kd"][2]
+    kb = 4 * geo["nk"] * oct_
+    a = 24 * N0 * N1 * h
+    b = 24 * N0 * L1 * h
+    if L0 == 1:
+        return [("xfwd", 12 * N + 4 * N * masks + a), ("ymul", a + kb + a), ("xinv_epi", a + 12 * N + 12 * N)]
+    return [("xfwd", 12 * N + 4 * N * masks + a), ("yfwd", a + b), ("zmul", b + kb + b), ("yinv", b + a),
+            ("xinv_epi", a + 12 * N + 12 * N)]
+
+
+def step_bytes_rk23(geo, n):
+    """Algorithmic bytes of one RK23 attempt: start combine + 3 fused evaluations."""
+    N = n[0] * n[1] * n[2]
+    conv = sum(b for _, b in pass_bytes(geo, n)) - 24 * N   # passes without the epilogue's m read / k write
+    ev = conv + 12 * N + 12 * N                               # + read m, write k
+    combine0 = 36 * N                                         # Y, K1 -> M1
+    e1 = ev + 12 * N + 12 * N                                 # + read Y, write M2
+    e2 = ev + 12 * N * 3 + 12 * N                             # + read Y, K1, K2, write Y'
+    e3 = ev + 12 * N * 3                                      # + error: read K1, K2, K3
+    return combine0 + e1 + e2 + e3
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- CPU baseline (oracle)
+def cpu_baseline(max_seconds=25.0):
+    """FP64 oracle on the host cores: RK23 steps of the same workload (bounded)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    if not os.path.exists(os.path.join(ROOT, "oracle", "liboracle.so")):
+        subprocess.check_call(["make", "-s", "-C", os.path.join(ROOT, "oracle")])
+    w = WORKLOAD
+    o = O.Oracle(O.full_desc(**problem()))
+    r = O.OracleRun(o, initial_m(0).astype(np.float64), solver=w["solver"], dt=w["dt0"], maxerr=w["maxerr"])
+    r.step()   # FSAL start-up evaluation excluded from the sample
+    t0 = time.perf_counter()
+    steps = 0
+    while True:
+        r.step()
+        steps += 1
+        if time.perf_counter() - t0 > max_seconds or steps >= 8:
+            break
+    dt = time.perf_counter() - t0
+    N = w["n"][0] * w["n"][1] * w["n"][2]
+    return {"value": N * steps / dt, "unit": "cell-steps/s", "cores": int(O.lib().or_num_threads()),
+            "kind": "port", "sample": f"{steps} RK23 steps of the full 256x256x16 workload after one warm-up "
+                                      f"step, FP64 oracle with OpenMP ({dt:.1f} s)", "seconds": dt}
+
+
+def reference_arm(args, rank, world):
+    if rank != 0:
+        return
+    cb = cpu_baseline(max_seconds=min(120.0, 15.0 * max(1, args.steps)))
+    line = {"impl": "reference", "metric": "cell-steps/s", "value": cb["value"], "unit": "cell-steps/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD["name"], "cells": 16 * 256 * 256, "solver": "rk23",
+                       "parallelism": f"replicas{world}"},
+            "cpu_baseline": {k: cb[k] for k in ["value", "unit", "cores", "kind", "sample"]},
+            "e2e": {"value": cb["value"], "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------- main
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-reps", type=int, default=10)
+    ap.add_argument("--profile-only", action="store_true",
+                    help="only time the passes of one field evaluation (few launches; for ncu captures)")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        reference_arm(args, rank, world)
+        return
+
+    import torch
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    from mumax2 import Plan
+    w = WORKLOAD
+    n = w["n"]
+    N = n[0] * n[1] * n[2]
+    plan = Plan(problem(), device=local_rank)
+    plan.solver(w["solver"], dt=w["dt0"], maxerr=w["maxerr"])
+    plan.set_state(initial_m(1000 + rank))
+    if args.profile_only:
+        geo = plan.geometry()
+        pass_ms = plan.profile_eval(args.profile_reps)
+        print(json.dumps({"passes": [{"pass": nm, "ms": t, "algorithmic_bytes": b}
+                                     for (nm, b), t in zip(pass_bytes(geo, n), pass_ms)]}), flush=True)
+        plan.close()
+        return
+    plan.steps(args.warmup)
+    torch.cuda.synchronize()
+
+    sampler = ClockSampler(local_rank)
+    sampler.start()
+    time.sleep(0.3)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    st0 = plan.stats()
+    l0 = plan.launch_count()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    plan.steps(args.steps)
+    e1.record()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ms = e0.elapsed_time(e1)
+    clocks = sampler.stop()
+    launches = plan.launch_count() - l0
+    st1 = plan.stats()
+    attempts = st1["attempts"] - st0["attempts"]
+    evals = st1["evals"] - st0["evals"]
+    ms_max = ms
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max = float(t.item())
+    value = N * args.steps * world / (ms_max / 1e3)
+
+    # per-pass timing of one evaluation (CUDA events on the launching stream)
+    geo = plan.geometry()
+    pass_ms = plan.profile_eval(args.profile_reps)
+    pb = pass_bytes(geo, n)
+    shares = [x / sum(pass_ms) for x in pass_ms]
+    dom = int(np.argmax(pass_ms))
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(peaks_path):
+        peaks = json.load(open(peaks_path))
+        peak, peak_src = float(peaks["hbm_gbs"]), "measured"
+    else:
+        peak, peak_src = 6650.0, "fallback"
+    achieved = pb[dom][1] / (pass_ms[dom] * 1e-3) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        tr = json.load(open(tpath))
+        traffic = tr.get(pb[dom][0])
+    step_b = step_bytes_rk23(geo, n) * attempts / max(1, args.steps)
+    step_gbs = step_b * args.steps / (ms / 1e3) / 1e9
+
+    # end-to-end through the C-ABI with host buffers: per step H2D of the state from
+    # pinned memory, one mm_step, D2H of the state
+    e2e_steps = min(args.steps, 10)
+    host_in = torch.from_numpy(plan.get_state()).pin_memory()
+    host_out = torch.empty_like(host_in).pin_memory()
+    import ctypes as C
+    from mumax2 import _native as nat
+    L = nat.lib()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    f0 = torch.cuda.Event(enable_timing=True)
+    f1 = torch.cuda.Event(enable_timing=True)
+    f0.record()
+    for _ in range(e2e_steps):
+        nat.check(L.mm_set_state(plan.h, C.c_void_p(host_in.data_ptr()), 1, None))
+        nat.check(L.mm_step(plan.h, None))
+        nat.check(L.mm_get_state(plan.h, C.c_void_p(host_out.data_ptr()), 1, None))
+    f1.record()
+    torch.cuda.synchronize()
+    e2e_ms = f0.elapsed_time(f1)
+    if dist:
+        t = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = N * e2e_steps * world / (e2e_ms / 1e3)
+
+    cb = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cb = cpu_baseline()
+        except Exception as ex:  # reported, not fatal
+            cb = {"value": None, "unit": "cell-steps/s", "cores": None, "kind": "port", "sample": f"failed: {ex}"}
+
+    if rank == 0:
+        line = {
+            "metric": "cell-steps/s", "value": value, "unit": "cell-steps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": w["name"], "cells": N, "grid_xyz": [n[2], n[1], n[0]],
+                       "cell_nm": [4, 4, 2], "solver": "rk23", "maxerr": w["maxerr"],
+                       "parallelism": f"replicas{world}",
+                       "l2": "per-step working set (state, stages, half spectrum, kernel) ~250 MB > 126 MB L2"},
+            "roofline": {"bound": "hbm", "kernel": pb[dom][0], "achieved": achieved, "peak": peak,
+                         "peak_source": peak_src, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                         "algorithmic_bytes": pb[dom][1], "launch_ms": pass_ms[dom]},
+            "passes": [{"pass": nm, "ms": t, "share": s, "algorithmic_bytes": b, "gbs": b / (t * 1e-3) / 1e9}
+                       for (nm, b), t, s in zip(pb, pass_ms, shares)],
+            "step_roofline": {"bytes_per_step": step_b, "achieved_gbs": step_gbs, "frac": step_gbs / peak},
+            "attempts_per_step": attempts / args.steps, "evals_per_step": evals / args.steps,
+            "e2e": {"value": e2e_value, "unit": "cell-steps/s", "h2d_bytes_per_step": 12 * N,
+                    "d2h_bytes_per_step": 12 * N, "steps": e2e_steps},
+            "gpu_launches": int(launches),
+            "clocks": clocks,
+            "cpu_baseline": cb if cb is None else {k: cb[k] for k in ["value", "unit", "cores", "kind", "sample"]},
+        }
+        print(json.dumps(line), flush=True)
+    plan.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

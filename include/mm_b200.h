@@ -138,6 +138,15 @@ MM_API int mm_average(mm_plan plan, double out[3], mm_stream stream);
 /* E_zeeman, E_ex, E_demag, E_anis, E (J) -- compensated FP32 sums. */
 MM_API int mm_energy(mm_plan plan, double out[5], mm_stream stream);
 
+/* ---- instrumentation ---- */
+/* Kernels this plan has enqueued so far (graph replays counted per kernel node). */
+MM_API long long mm_plan_launch_count(mm_plan plan);
+/* Average duration (ms) of each pass of one field evaluation, timed with CUDA events
+ * on `stream` around each pass; *npass = 5 (3-D), 3 (2-D film) or 1 (no demag). */
+MM_API int mm_profile_eval(mm_plan plan, int reps, double* ms_out, int* npass, mm_stream stream);
+/* L0 L1 L2, M, h, hp, kd0 kd1 kd2, number of non-zero kernel components, demag flag, 0 */
+MM_API int mm_plan_geometry(mm_plan plan, int out12[12]);
+
 #ifdef __cplusplus
 }
 #endif
