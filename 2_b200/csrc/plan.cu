@@ -1068,7 +1068,7 @@ extern "C" MM_API int mm_profile_eval(mm_plan p, int reps, double* ms_out, int* 
     std::vector<cudaEvent_t> ev(np + 1);
     for (auto& e : ev) CUCHK(cudaEventCreate(&e));
     std::vector<double> acc(np, 0.0);
-    for (int r = 0; r < reps; r++) {
+    for (int r = -1; r < reps; r++) {  // r = -1: untimed warm-up evaluation
         int k = 0;
         CUCHK(cudaEventRecord(ev[k++], st));
         int nb = 0;
@@ -1098,6 +1098,7 @@ extern "C" MM_API int mm_profile_eval(mm_plan p, int reps, double* ms_out, int* 
         }
         CUCHK(cudaEventRecord(ev[k++], st));
         CUCHK(cudaEventSynchronize(ev[np]));
+        if (r < 0) continue;
         for (int i = 0; i < np; i++) {
             float ms = 0.f;
             CUCHK(cudaEventElapsedTime(&ms, ev[i], ev[i + 1]));
