@@ -14,6 +14,9 @@
 //   3     x rows  C2R + epilogue (rhs.cu)    z cols fwd * K inv (colmul)
 //   4                                        y cols inv   (colfft)
 //   5                                        x rows C2R + epilogue (rhs.cu)
+//
+// Column passes work on tiles of TC adjacent kx columns (TC a compile-time function
+// of the line length), so every global access moves TC*8 contiguous bytes.
 #include <cstdio>
 
 #include "fft.cuh"
@@ -34,56 +37,147 @@ __device__ __forceinline__ bool conv_skip(const DevCtl* ctl, int skip_retry) {
 template <int M, typename V, typename S>
 __global__ void __launch_bounds__(256) xfwd_kernel(const S* __restrict__ in_fixed, PP in_pp, const float* __restrict__ mask,
                                                    V* __restrict__ out, int nrows, int Z, int Y, int Yout,
-                                                   int in_pitch, int n_in, int hp, const DevCtl* ctl, int skip_retry) {
+                                                   int in_pitch, int n_in, int hp, const float2* __restrict__ tw,
+                                                   const DevCtl* ctl, int skip_retry) {
     if (conv_skip(ctl, skip_retry)) return;
     const S* in = in_fixed ? in_fixed : reinterpret_cast<const S*>(in_pp.get(ctl ? ctl->cur : 0));
     constexpr int TPL = tpl(M);
     constexpr int LL = line_len(M);
+    constexpr int RPB = TPL >= 256 ? 1 : 256 / TPL;
     extern __shared__ unsigned char smem_raw[];
     V* sm = reinterpret_cast<V*>(smem_raw);
-    const int rpb = blockDim.x / TPL;
     const int lr = threadIdx.x / TPL;
     const int t = threadIdx.x % TPL;
-    const int row = blockIdx.x * rpb + lr;
-    const bool active = (row < nrows) && (lr < rpb);
-    V* x = sm + lr * LL;
+    const int row = blockIdx.x * RPB + lr;
+    const bool active = (row < nrows) && (lr < RPB);
+    V* x = sm + (lr < RPB ? lr : 0) * LL;
+    typedef typename Scalar<V>::T T;
     if (active) {
         const S* src = in + (long long)row * in_pitch;
         const int zy = row % (Z * Y);
         const float* msk = mask ? mask + (long long)zy * in_pitch : nullptr;
-        for (int e = t; e < M; e += TPL) {
-            S a = 0, b = 0;
-            if (2 * e < n_in) a = src[2 * e] * (msk ? (S)msk[2 * e] : (S)1);
-            if (2 * e + 1 < n_in) b = src[2 * e + 1] * (msk ? (S)msk[2 * e + 1] : (S)1);
-            x[padx(e)] = mkv(a, b);
+        const bool pairs = ((in_pitch & 1) == 0) && ((n_in & 1) == 0);
+        if (pairs) {
+            // two reals per load: z[e] = x[2e] + i x[2e+1]
+            const int ne = n_in >> 1;
+#pragma unroll 4
+            for (int e = t; e < M; e += TPL) {
+                V v = mkv((T)0, (T)0);
+                if (e < ne) {
+                    if constexpr (sizeof(S) == 4) {
+                        float2 a = __ldg(reinterpret_cast<const float2*>(src) + e);
+                        if (msk) {
+                            float2 mm = __ldg(reinterpret_cast<const float2*>(msk) + e);
+                            a.x *= mm.x;
+                            a.y *= mm.y;
+                        }
+                        v = mkv((T)a.x, (T)a.y);
+                    } else {
+                        v = mkv((T)src[2 * e], (T)src[2 * e + 1]);
+                    }
+                }
+                x[padx(e)] = v;
+            }
+        } else {
+            for (int e = t; e < M; e += TPL) {
+                S a = 0, b = 0;
+                if (2 * e < n_in) a = src[2 * e] * (msk ? (S)msk[2 * e] : (S)1);
+                if (2 * e + 1 < n_in) b = src[2 * e + 1] * (msk ? (S)msk[2 * e + 1] : (S)1);
+                x[padx(e)] = mkv((T)a, (T)b);
+            }
         }
     }
     __syncthreads();
-    fft_line<M, -1, V>(x, t, active);
+    fft_line<M, -1, V>(x, t, active, tw);
     if (active) {
         // X[k] = E[k] + W^k O[k], E = (Z[k] + conj Z[M-k])/2, O = (Z[k] - conj Z[M-k])/(2i)
         const int c = row / (Z * Y);
         const int zy = row % (Z * Y);
         const int z = zy / Y, y = zy % Y;
         V* dst = out + ((long long)(c * Z + z) * Yout + y) * hp;
-        typedef typename Scalar<V>::T T;
         for (int k = t; k <= M / 2; k += TPL) {
-            V zk = x[padx(k % M)];
-            V zm = x[padx((M - k) % M)];
+            V zk = x[padx(k & (M - 1))];
+            V zm = x[padx((M - k) & (M - 1))];
             V e = cscale(cadd(zk, cconj(zm)), (T)0.5);
             V o = cscale(csub(zk, cconj(zm)), (T)0.5);
             o = mkv(o.y, -o.x);  // divide by i
-            V w = Tw<-1, V>::get(k, 2 * M);
-            V wo = cmul(w, o);
-            dst[k] = cadd(e, wo);
+            V w = TwSrc<-1, V>::get(tw, k, 2 * M);
+            dst[k] = cadd(e, cmul(w, o));
             if (k != M - k) {
-                // X[M-k] = conj(E[k]) - conj(W^k O[k]) ... computed directly:
-                // E[M-k] = conj(E[k]), O[M-k] = conj(O[k]), W^(M-k) = -conj(W^k)
-                V em = cconj(e);
-                V om = cconj(o);
+                // E[M-k] = conj E[k], O[M-k] = conj O[k], W^(M-k) = -conj W^k
                 V wm = mkv(-w.x, w.y);
-                dst[M - k] = cadd(em, cmul(wm, om));
+                dst[M - k] = cadd(cconj(e), cmul(wm, cconj(o)));
             }
+        }
+    }
+}
+
+// ---------------------------------------------------------------- column tiles
+// Tile width: up to 32 columns, as many as fit 56 KB of shared memory and 1024 threads.
+__host__ __device__ constexpr int col_tile(int L, int ncomp, int vsize) {
+    int tc = 32;
+    while (tc > 1 && (ncomp * tc * line_len(L) * vsize > 56 * 1024 || tc * tpl(L) > 1024)) tc /= 2;
+    return tc;
+}
+
+// Copies rows e < n of the tile's columns (base + e*line_stride + col) into shared
+// memory lines sm[(cline + col)*LL + padx(e)], zero-filling e in [n, L) if `zero`.
+template <int L, int TC, typename V>
+__device__ __forceinline__ void tile_load(V* sm, const V* __restrict__ base, long long line_stride, int n, int ncols_here,
+                                          int cline, bool zero) {
+    constexpr int LL = line_len(L);
+    const int nthr = blockDim.x;
+    bool done_vec = false;
+    if constexpr (TC >= 2 && sizeof(V) == 8) {
+        if (ncols_here == TC) {
+            constexpr int TP = TC / 2;  // two columns per 16-byte access
+            for (int i = threadIdx.x; i < n * TP; i += nthr) {
+                const int e = i / TP, cp = (i % TP) * 2;
+                float4 v = __ldg(reinterpret_cast<const float4*>(base + e * line_stride + cp));
+                sm[(cline + cp) * LL + padx(e)] = make_float2(v.x, v.y);
+                sm[(cline + cp + 1) * LL + padx(e)] = make_float2(v.z, v.w);
+            }
+            done_vec = true;
+        }
+    }
+    if (!done_vec) {
+        for (int i = threadIdx.x; i < n * TC; i += nthr) {
+            const int e = i / TC, col = i % TC;
+            V v = mkv((typename Scalar<V>::T)0, (typename Scalar<V>::T)0);
+            if (col < ncols_here) v = base[e * line_stride + col];
+            sm[(cline + col) * LL + padx(e)] = v;
+        }
+    }
+    if (zero) {
+        for (int i = threadIdx.x; i < (L - n) * TC; i += nthr) {
+            const int e = n + i / TC, col = i % TC;
+            sm[(cline + col) * LL + padx(e)] = mkv((typename Scalar<V>::T)0, (typename Scalar<V>::T)0);
+        }
+    }
+}
+
+template <int L, int TC, typename V>
+__device__ __forceinline__ void tile_store(const V* sm, V* __restrict__ base, long long line_stride, int n, int ncols_here,
+                                           int cline) {
+    constexpr int LL = line_len(L);
+    const int nthr = blockDim.x;
+    bool done_vec = false;
+    if constexpr (TC >= 2 && sizeof(V) == 8) {
+        if (ncols_here == TC) {
+            constexpr int TP = TC / 2;
+            for (int i = threadIdx.x; i < n * TP; i += nthr) {
+                const int e = i / TP, cp = (i % TP) * 2;
+                V a = sm[(cline + cp) * LL + padx(e)];
+                V b = sm[(cline + cp + 1) * LL + padx(e)];
+                *reinterpret_cast<float4*>(base + e * line_stride + cp) = make_float4(a.x, a.y, b.x, b.y);
+            }
+            done_vec = true;
+        }
+    }
+    if (!done_vec) {
+        for (int i = threadIdx.x; i < n * TC; i += nthr) {
+            const int e = i / TC, col = i % TC;
+            if (col < ncols_here) base[e * line_stride + col] = sm[(cline + col) * LL + padx(e)];
         }
     }
 }
@@ -94,9 +188,10 @@ __global__ void __launch_bounds__(256) xfwd_kernel(const S* __restrict__ in_fixe
 //   base + o*outer_stride + e*line_stride + kx.
 // Reads elements e < n_in (rest zero), writes elements e < n_out.
 template <int L, int SIGN, typename V>
-__global__ void colfft_kernel(V* __restrict__ S, int ncols, int TC, long long outer_stride, long long line_stride,
-                              int n_in, int n_out, const DevCtl* ctl, int skip_retry) {
+__global__ void colfft_kernel(V* __restrict__ S, int ncols, long long outer_stride, long long line_stride, int n_in,
+                              int n_out, const float2* __restrict__ tw, const DevCtl* ctl, int skip_retry) {
     if (conv_skip(ctl, skip_retry)) return;
+    constexpr int TC = col_tile(L, 1, sizeof(V));
     constexpr int TPL = tpl(L);
     constexpr int LL = line_len(L);
     extern __shared__ unsigned char smem_raw[];
@@ -104,22 +199,14 @@ __global__ void colfft_kernel(V* __restrict__ S, int ncols, int TC, long long ou
     const int ntiles = (ncols + TC - 1) / TC;
     const int o = blockIdx.x / ntiles;
     const int kx0 = (blockIdx.x % ntiles) * TC;
+    const int nh = min(TC, ncols - kx0);
     V* base = S + (long long)o * outer_stride + kx0;
-    const int nthr = blockDim.x;
-    for (int i = threadIdx.x; i < L * TC; i += nthr) {
-        int e = i / TC, col = i % TC;
-        V v = mkv((typename Scalar<V>::T)0, (typename Scalar<V>::T)0);
-        if (e < n_in && kx0 + col < ncols) v = base[(long long)e * line_stride + col];
-        sm[col * LL + padx(e)] = v;
-    }
+    tile_load<L, TC, V>(sm, base, line_stride, n_in, nh, 0, true);
     __syncthreads();
     const int col = threadIdx.x / TPL;
     const int t = threadIdx.x % TPL;
-    fft_line<L, SIGN, V>(sm + col * LL, t, col < TC);
-    for (int i = threadIdx.x; i < n_out * TC; i += nthr) {
-        int e = i / TC, c2 = i % TC;
-        if (kx0 + c2 < ncols) base[(long long)e * line_stride + c2] = sm[c2 * LL + padx(e)];
-    }
+    fft_line<L, SIGN, V>(sm + (col < TC ? col : 0) * LL, t, col < TC, tw);
+    tile_store<L, TC, V>(sm, base, line_stride, n_out, nh, 0);
 }
 
 // ---------------------------------------------------------------- multiply pass
@@ -128,10 +215,10 @@ __global__ void colfft_kernel(V* __restrict__ S, int ncols, int TC, long long ou
 // kaxis = 1: the line runs along y (kz = 0, 2-D films).
 __device__ __forceinline__ void kernel_at(const KernelView& K, int kz, int ky, int kx, float out[6]) {
     float sz = 1.f, sy = 1.f;
-    if (kz > K.L0 / 2) { kz = K.L0 - kz; sz = -1.f; }
-    if (ky > K.L1 / 2) { ky = K.L1 - ky; sy = -1.f; }
-    const long long cs = (long long)K.kd0 * K.kd1 * K.kd2;
-    const long long idx = ((long long)kz * K.kd1 + ky) * K.kd2 + kx;
+    if (kz > (K.L0 >> 1)) { kz = K.L0 - kz; sz = -1.f; }
+    if (ky > (K.L1 >> 1)) { ky = K.L1 - ky; sy = -1.f; }
+    const int cs = K.kd0 * K.kd1 * K.kd2;
+    const int idx = (kz * K.kd1 + ky) * K.kd2 + kx;
     // real-space K_sd is odd along axes s and d (s != d), so its transform flips sign
     // under k -> L-k along those axes; diagonal components are even.
     const float sg[6] = {1.f, 1.f, 1.f, sy, sz, sz * sy};
@@ -140,10 +227,11 @@ __device__ __forceinline__ void kernel_at(const KernelView& K, int kz, int ky, i
 }
 
 template <int L>
-__global__ void colmul_kernel(float2* __restrict__ S, KernelView K, int ncols, int TC, long long comp_stride,
+__global__ void colmul_kernel(float2* __restrict__ S, KernelView K, int ncols, long long comp_stride,
                               long long outer_stride, long long line_stride, int n_in, int kaxis, float scale,
-                              const DevCtl* ctl, int skip_retry) {
+                              const float2* __restrict__ tw, const DevCtl* ctl, int skip_retry) {
     if (conv_skip(ctl, skip_retry)) return;
+    constexpr int TC = col_tile(L, 3, 8);
     constexpr int TPL = tpl(L);
     constexpr int LL = line_len(L);
     extern __shared__ unsigned char smem_raw[];
@@ -151,61 +239,43 @@ __global__ void colmul_kernel(float2* __restrict__ S, KernelView K, int ncols, i
     const int ntiles = (ncols + TC - 1) / TC;
     const int o = blockIdx.x / ntiles;
     const int kx0 = (blockIdx.x % ntiles) * TC;
+    const int nh = min(TC, ncols - kx0);
     float2* base = S + (long long)o * outer_stride + kx0;
-    const int nthr = blockDim.x;
-    for (int i = threadIdx.x; i < 3 * L * TC; i += nthr) {
-        int c = i / (L * TC), r = i % (L * TC);
-        int e = r / TC, col = r % TC;
-        float2 v = make_float2(0.f, 0.f);
-        if (e < n_in && kx0 + col < ncols) v = base[c * comp_stride + (long long)e * line_stride + col];
-        sm[(c * TC + col) * LL + padx(e)] = v;
-    }
+#pragma unroll 1
+    for (int c = 0; c < 3; c++) tile_load<L, TC, float2>(sm, base + c * comp_stride, line_stride, n_in, nh, c * TC, true);
     __syncthreads();
     const int col = threadIdx.x / TPL;
     const int t = threadIdx.x % TPL;
     const bool act = col < TC;
 #pragma unroll 1
-    for (int c = 0; c < 3; c++) fft_line<L, -1, float2>(sm + (c * TC + (act ? col : 0)) * LL, t, act);
-    for (int i = threadIdx.x; i < L * TC; i += nthr) {
-        int e = i / TC, c2 = i % TC;
-        int kx = kx0 + c2;
-        if (kx >= ncols) continue;
+    for (int c = 0; c < 3; c++) fft_line<L, -1, float2>(sm + (c * TC + (act ? col : 0)) * LL, t, act, tw);
+    for (int i = threadIdx.x; i < L * TC; i += blockDim.x) {
+        const int e = i / TC, c2 = i % TC;
+        const int kx = kx0 + c2;
+        if (c2 >= nh) continue;
         float kk[6];
         if (kaxis == 0) kernel_at(K, e, o, kx, kk);
         else kernel_at(K, 0, e, kx, kk);
-        float2 m0 = sm[(0 * TC + c2) * LL + padx(e)];
-        float2 m1 = sm[(1 * TC + c2) * LL + padx(e)];
-        float2 m2 = sm[(2 * TC + c2) * LL + padx(e)];
+        const int p = padx(e);
+        float2 m0 = sm[(0 * TC + c2) * LL + p];
+        float2 m1 = sm[(1 * TC + c2) * LL + p];
+        float2 m2 = sm[(2 * TC + c2) * LL + p];
         // q: 0 xx, 1 yy, 2 zz, 3 yz, 4 xz, 5 xy
-        float2 h0 = make_float2(kk[0] * m0.x + kk[5] * m1.x + kk[4] * m2.x, kk[0] * m0.y + kk[5] * m1.y + kk[4] * m2.y);
-        float2 h1 = make_float2(kk[5] * m0.x + kk[1] * m1.x + kk[3] * m2.x, kk[5] * m0.y + kk[1] * m1.y + kk[3] * m2.y);
-        float2 h2 = make_float2(kk[4] * m0.x + kk[3] * m1.x + kk[2] * m2.x, kk[4] * m0.y + kk[3] * m1.y + kk[2] * m2.y);
-        sm[(0 * TC + c2) * LL + padx(e)] = make_float2(h0.x * scale, h0.y * scale);
-        sm[(1 * TC + c2) * LL + padx(e)] = make_float2(h1.x * scale, h1.y * scale);
-        sm[(2 * TC + c2) * LL + padx(e)] = make_float2(h2.x * scale, h2.y * scale);
+        sm[(0 * TC + c2) * LL + p] = make_float2(scale * (kk[0] * m0.x + kk[5] * m1.x + kk[4] * m2.x),
+                                                 scale * (kk[0] * m0.y + kk[5] * m1.y + kk[4] * m2.y));
+        sm[(1 * TC + c2) * LL + p] = make_float2(scale * (kk[5] * m0.x + kk[1] * m1.x + kk[3] * m2.x),
+                                                 scale * (kk[5] * m0.y + kk[1] * m1.y + kk[3] * m2.y));
+        sm[(2 * TC + c2) * LL + p] = make_float2(scale * (kk[4] * m0.x + kk[3] * m1.x + kk[2] * m2.x),
+                                                 scale * (kk[4] * m0.y + kk[3] * m1.y + kk[2] * m2.y));
     }
     __syncthreads();
 #pragma unroll 1
-    for (int c = 0; c < 3; c++) fft_line<L, +1, float2>(sm + (c * TC + (act ? col : 0)) * LL, t, act);
-    for (int i = threadIdx.x; i < 3 * n_in * TC; i += nthr) {
-        int c = i / (n_in * TC), r = i % (n_in * TC);
-        int e = r / TC, c2 = r % TC;
-        if (kx0 + c2 < ncols) base[c * comp_stride + (long long)e * line_stride + c2] = sm[(c * TC + c2) * LL + padx(e)];
-    }
+    for (int c = 0; c < 3; c++) fft_line<L, +1, float2>(sm + (c * TC + (act ? col : 0)) * LL, t, act, tw);
+#pragma unroll 1
+    for (int c = 0; c < 3; c++) tile_store<L, TC, float2>(sm, base + c * comp_stride, line_stride, n_in, nh, c * TC);
 }
 
 // ---------------------------------------------------------------- launch helpers
-static int g_max_smem = 0;
-static int max_smem() {
-    if (!g_max_smem) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&g_max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-        if (g_max_smem <= 0) g_max_smem = 48 * 1024;
-    }
-    return g_max_smem;
-}
-
 template <typename KT> static cudaError_t set_smem(KT kern, size_t bytes) {
     if (bytes > 48 * 1024) return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
     return cudaSuccess;
@@ -215,69 +285,62 @@ template <typename KT> static cudaError_t set_smem(KT kern, size_t bytes) {
 
 template <int M, typename V, typename S>
 static cudaError_t launch_xfwd_t(const S* in, PP pp, const float* mask, V* out, int nrows, int Z, int Y, int Yout,
-                                 int in_pitch, int n_in, int hp, const DevCtl* ctl, int skip_retry, cudaStream_t st) {
+                                 int in_pitch, int n_in, int hp, const float2* tw, const DevCtl* ctl, int skip_retry,
+                                 cudaStream_t st) {
     constexpr int TPL = tpl(M);
-    int rpb = TPL >= 256 ? 1 : 256 / TPL;
-    size_t smem = (size_t)rpb * line_len(M) * sizeof(V);
-    while (smem > (size_t)max_smem() && rpb > 1) { rpb /= 2; smem = (size_t)rpb * line_len(M) * sizeof(V); }
+    constexpr int RPB = TPL >= 256 ? 1 : 256 / TPL;
+    const size_t smem = (size_t)RPB * line_len(M) * sizeof(V);
     cudaError_t e = set_smem(xfwd_kernel<M, V, S>, smem);
     if (e != cudaSuccess) return e;
-    int blocks = (nrows + rpb - 1) / rpb;
-    xfwd_kernel<M, V, S><<<blocks, rpb * TPL, smem, st>>>(in, pp, mask, out, nrows, Z, Y, Yout, in_pitch, n_in, hp, ctl,
-                                                          skip_retry);
+    int blocks = (nrows + RPB - 1) / RPB;
+    int threads = RPB * TPL < 32 ? 32 : RPB * TPL;
+    xfwd_kernel<M, V, S><<<blocks, threads, smem, st>>>(in, pp, mask, out, nrows, Z, Y, Yout, in_pitch, n_in, hp,
+                                                        tw, ctl, skip_retry);
     return cudaGetLastError();
 }
 
 template <typename V, typename S>
 cudaError_t launch_xfwd(int M, const S* in, PP pp, const float* mask, V* out, int nrows, int Z, int Y, int Yout,
-                        int in_pitch, int n_in, int hp, const DevCtl* ctl, int skip_retry, cudaStream_t st) {
+                        int in_pitch, int n_in, int hp, const float2* tw, const DevCtl* ctl, int skip_retry,
+                        cudaStream_t st) {
     switch (M) {
-#define X(m) case m: return launch_xfwd_t<m, V, S>(in, pp, mask, out, nrows, Z, Y, Yout, in_pitch, n_in, hp, ctl, skip_retry, st);
+#define X(m) case m: return launch_xfwd_t<m, V, S>(in, pp, mask, out, nrows, Z, Y, Yout, in_pitch, n_in, hp, tw, ctl, skip_retry, st);
         MM_FOR_POW2(X)
 #undef X
         default: return cudaErrorInvalidValue;
     }
 }
 
-// Picks the column tile width: as many columns as fit the shared-memory budget,
-// up to 32 (256 B contiguous per row segment), at most 1024 threads.
-static int pick_tc(int L, int ncomp, size_t vsize, int ncols) {
-    int TC = 32;
-    const size_t budget = 100 * 1024;
-    while (TC > 1 && ((size_t)ncomp * TC * mmfft::line_len(L) * vsize > budget || TC * mmfft::tpl(L) > 1024)) TC /= 2;
-    while (TC > 1 && TC / 2 >= ncols) TC /= 2;
-    return TC;
-}
-
 template <int L, int SIGN, typename V>
 static cudaError_t launch_colfft_t(V* S, int ncols, int nouter, long long outer_stride, long long line_stride,
-                                   int n_in, int n_out, const DevCtl* ctl, int skip_retry, cudaStream_t st) {
-    int TC = pick_tc(L, 1, sizeof(V), ncols);
-    size_t smem = (size_t)TC * line_len(L) * sizeof(V);
+                                   int n_in, int n_out, const float2* tw, const DevCtl* ctl, int skip_retry,
+                                   cudaStream_t st) {
+    constexpr int TC = col_tile(L, 1, sizeof(V));
+    const size_t smem = (size_t)TC * line_len(L) * sizeof(V);
     cudaError_t e = set_smem(colfft_kernel<L, SIGN, V>, smem);
     if (e != cudaSuccess) return e;
     int ntiles = (ncols + TC - 1) / TC;
     int threads = TC * tpl(L);
     if (threads < 32) threads = 32;
-    colfft_kernel<L, SIGN, V><<<nouter * ntiles, threads, smem, st>>>(S, ncols, TC, outer_stride, line_stride, n_in,
-                                                                      n_out, ctl, skip_retry);
+    colfft_kernel<L, SIGN, V><<<nouter * ntiles, threads, smem, st>>>(S, ncols, outer_stride, line_stride, n_in,
+                                                                      n_out, tw, ctl, skip_retry);
     return cudaGetLastError();
 }
 
 template <typename V>
 cudaError_t launch_colfft(int L, int sign, V* S, int ncols, int nouter, long long outer_stride,
-                          long long line_stride, int n_in, int n_out, const DevCtl* ctl, int skip_retry,
-                          cudaStream_t st) {
+                          long long line_stride, int n_in, int n_out, const float2* tw, const DevCtl* ctl,
+                          int skip_retry, cudaStream_t st) {
     if (sign < 0) {
         switch (L) {
-#define X(l) case l: return launch_colfft_t<l, -1, V>(S, ncols, nouter, outer_stride, line_stride, n_in, n_out, ctl, skip_retry, st);
+#define X(l) case l: return launch_colfft_t<l, -1, V>(S, ncols, nouter, outer_stride, line_stride, n_in, n_out, tw, ctl, skip_retry, st);
             MM_FOR_POW2(X)
 #undef X
             default: return cudaErrorInvalidValue;
         }
     } else {
         switch (L) {
-#define X(l) case l: return launch_colfft_t<l, 1, V>(S, ncols, nouter, outer_stride, line_stride, n_in, n_out, ctl, skip_retry, st);
+#define X(l) case l: return launch_colfft_t<l, 1, V>(S, ncols, nouter, outer_stride, line_stride, n_in, n_out, tw, ctl, skip_retry, st);
             MM_FOR_POW2(X)
 #undef X
             default: return cudaErrorInvalidValue;
@@ -288,24 +351,24 @@ cudaError_t launch_colfft(int L, int sign, V* S, int ncols, int nouter, long lon
 template <int L>
 static cudaError_t launch_colmul_t(float2* S, const KernelView& K, int ncols, int nouter, long long comp_stride,
                                    long long outer_stride, long long line_stride, int n_in, int kaxis, float scale,
-                                   const DevCtl* ctl, int skip_retry, cudaStream_t st) {
-    int TC = pick_tc(L, 3, sizeof(float2), ncols);
-    size_t smem = (size_t)3 * TC * line_len(L) * sizeof(float2);
+                                   const float2* tw, const DevCtl* ctl, int skip_retry, cudaStream_t st) {
+    constexpr int TC = col_tile(L, 3, 8);
+    const size_t smem = (size_t)3 * TC * line_len(L) * sizeof(float2);
     cudaError_t e = set_smem(colmul_kernel<L>, smem);
     if (e != cudaSuccess) return e;
     int ntiles = (ncols + TC - 1) / TC;
     int threads = TC * tpl(L);
     if (threads < 32) threads = 32;
-    colmul_kernel<L><<<nouter * ntiles, threads, smem, st>>>(S, K, ncols, TC, comp_stride, outer_stride, line_stride,
-                                                            n_in, kaxis, scale, ctl, skip_retry);
+    colmul_kernel<L><<<nouter * ntiles, threads, smem, st>>>(S, K, ncols, comp_stride, outer_stride, line_stride, n_in,
+                                                            kaxis, scale, tw, ctl, skip_retry);
     return cudaGetLastError();
 }
 
 cudaError_t launch_colmul(int L, float2* S, const KernelView& K, int ncols, int nouter, long long comp_stride,
                           long long outer_stride, long long line_stride, int n_in, int kaxis, float scale,
-                          const DevCtl* ctl, int skip_retry, cudaStream_t st) {
+                          const float2* tw, const DevCtl* ctl, int skip_retry, cudaStream_t st) {
     switch (L) {
-#define X(l) case l: return launch_colmul_t<l>(S, K, ncols, nouter, comp_stride, outer_stride, line_stride, n_in, kaxis, scale, ctl, skip_retry, st);
+#define X(l) case l: return launch_colmul_t<l>(S, K, ncols, nouter, comp_stride, outer_stride, line_stride, n_in, kaxis, scale, tw, ctl, skip_retry, st);
         MM_FOR_POW2(X)
 #undef X
         default: return cudaErrorInvalidValue;
@@ -313,12 +376,12 @@ cudaError_t launch_colmul(int L, float2* S, const KernelView& K, int ncols, int 
 }
 
 template cudaError_t launch_xfwd<float2, float>(int, const float*, PP, const float*, float2*, int, int, int, int, int,
-                                                int, int, const DevCtl*, int, cudaStream_t);
+                                                int, int, const float2*, const DevCtl*, int, cudaStream_t);
 template cudaError_t launch_xfwd<double2, double>(int, const double*, PP, const float*, double2*, int, int, int, int,
-                                                  int, int, int, const DevCtl*, int, cudaStream_t);
-template cudaError_t launch_colfft<float2>(int, int, float2*, int, int, long long, long long, int, int, const DevCtl*,
-                                           int, cudaStream_t);
+                                                  int, int, int, const float2*, const DevCtl*, int, cudaStream_t);
+template cudaError_t launch_colfft<float2>(int, int, float2*, int, int, long long, long long, int, int,
+                                           const float2*, const DevCtl*, int, cudaStream_t);
 template cudaError_t launch_colfft<double2>(int, int, double2*, int, int, long long, long long, int, int,
-                                            const DevCtl*, int, cudaStream_t);
+                                            const float2*, const DevCtl*, int, cudaStream_t);
 
 }  // namespace mm

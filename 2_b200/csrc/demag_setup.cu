@@ -201,13 +201,13 @@ int build_demag_kernel(const int L[3], const double cell[3], const int pbc[3], i
             }
             PP none = {nullptr, nullptr, 0};
             CK(launch_xfwd<double2, double>(M, K + q * NL, none, nullptr, spec, L[0] * L[1], L[0], L[1], L[1], L[2],
-                                            L[2], hp, nullptr, 0, st));
+                                            L[2], hp, nullptr, nullptr, 0, st));
             if (L[1] > 1)
-                CK(launch_colfft<double2>(L[1], -1, spec, hp, L[0], (long long)L[1] * hp, hp, L[1], L[1], nullptr, 0,
-                                          st));
+                CK(launch_colfft<double2>(L[1], -1, spec, hp, L[0], (long long)L[1] * hp, hp, L[1], L[1], nullptr,
+                                          nullptr, 0, st));
             if (L[0] > 1)
-                CK(launch_colfft<double2>(L[0], -1, spec, hp, L[1], hp, (long long)L[1] * hp, L[0], L[0], nullptr, 0,
-                                          st));
+                CK(launch_colfft<double2>(L[0], -1, spec, hp, L[1], hp, (long long)L[1] * hp, L[0], L[0], nullptr,
+                                          nullptr, 0, st));
             extract_octant_kernel<<<296, 256, 0, st>>>(spec, L[0], L[1], hp, kd[0], kd[1], kd[2], scale,
                                                        khat + q * oct);
             CK(cudaGetLastError());

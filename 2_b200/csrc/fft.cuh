@@ -14,6 +14,8 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <cmath>
+
 namespace mmfft {
 
 __host__ __device__ constexpr int padx(int i) { return i + (i >> 3); }
@@ -106,10 +108,26 @@ template <int SIGN, typename V> struct Dft<8, SIGN, V> {
     }
 };
 
+// ---- twiddles.  FP32: read from a table of exp(-2 pi i k / TWN), k < TWN, rounded
+// once from FP64 on the host (one load instead of a sincos per factor).  FP64 (plan
+// set-up only): computed.
+constexpr int TWN = 4096;
+template <int SIGN, typename V> struct TwSrc;
+template <int SIGN> struct TwSrc<SIGN, float2> {
+    // exp(SIGN 2 pi i num / den), den a power of two <= TWN
+    static __device__ __forceinline__ float2 get(const float2* tw, int num, int den) {
+        float2 w = __ldg(tw + ((num * (TWN / den)) & (TWN - 1)));
+        return SIGN > 0 ? make_float2(w.x, -w.y) : w;
+    }
+};
+template <int SIGN> struct TwSrc<SIGN, double2> {
+    static __device__ __forceinline__ double2 get(const float2*, int num, int den) { return twiddle_d<SIGN>(num, den); }
+};
+
 // ---- one Stockham stage on a padded shared-memory line, then the remaining stages.
 // All threads of the block must call this (it synchronises); `active` masks the work.
 template <int L, int Ns, int SIGN, typename V>
-__device__ __forceinline__ void stockham(V* x, int t, bool active) {
+__device__ __forceinline__ void stockham(V* x, int t, bool active, const float2* tw) {
     constexpr int R = (L / Ns >= 8) ? 8 : (L / Ns);
     constexpr int TPL = tpl(L);
     constexpr int NB = (L / R) / TPL;
@@ -127,25 +145,33 @@ __device__ __forceinline__ void stockham(V* x, int t, bool active) {
 #pragma unroll
         for (int b = 0; b < NB; b++) {
             const int j = t + b * TPL;
-            const int k = j % Ns;
+            const int k = j & (Ns - 1);
             if (Ns > 1) {
 #pragma unroll
-                for (int r = 1; r < R; r++) v[b][r] = cmul(v[b][r], Tw<SIGN, V>::get(r * k, Ns * R));
+                for (int r = 1; r < R; r++) v[b][r] = cmul(v[b][r], TwSrc<SIGN, V>::get(tw, r * k, Ns * R));
             }
             Dft<R, SIGN, V>::run(v[b]);
-            const int base = (j / Ns) * Ns * R + k;
+            const int base = (j - k) * R + k;
 #pragma unroll
             for (int r = 0; r < R; r++) x[padx(base + r * Ns)] = v[b][r];
         }
     }
     __syncthreads();
-    if constexpr (Ns * R < L) stockham<L, Ns * R, SIGN, V>(x, t, active);
+    if constexpr (Ns * R < L) stockham<L, Ns * R, SIGN, V>(x, t, active, tw);
 }
 
 // Full in-place FFT of one padded line (unnormalised).  SIGN = -1 forward, +1 inverse.
 template <int L, int SIGN, typename V>
-__device__ __forceinline__ void fft_line(V* x, int t, bool active) {
-    if constexpr (L > 1) stockham<L, 1, SIGN, V>(x, t, active);
+__device__ __forceinline__ void fft_line(V* x, int t, bool active, const float2* tw) {
+    if constexpr (L > 1) stockham<L, 1, SIGN, V>(x, t, active, tw);
+}
+
+// Host: the FP32 twiddle table exp(-2 pi i k / TWN), rounded from FP64.
+inline void make_twiddle_table(float2* host) {
+    for (int k = 0; k < TWN; k++) {
+        double a = -2.0 * 3.14159265358979323846264338327950288 * (double)k / TWN;
+        host[k] = make_float2((float)cos(a), (float)sin(a));
+    }
 }
 
 }  // namespace mmfft

@@ -148,16 +148,17 @@ struct EpiArgs {
 // ---- launchers (conv.cu, rhs.cu)
 template <typename V, typename S>
 cudaError_t launch_xfwd(int M, const S* in, PP pp, const float* mask, V* out, int nrows, int Z, int Y, int Yout,
-                        int in_pitch, int n_in, int hp, const DevCtl* ctl, int skip_retry, cudaStream_t st);
+                        int in_pitch, int n_in, int hp, const float2* tw, const DevCtl* ctl, int skip_retry,
+                        cudaStream_t st);
 template <typename V>
 cudaError_t launch_colfft(int L, int sign, V* S, int ncols, int nouter, long long outer_stride,
-                          long long line_stride, int n_in, int n_out, const DevCtl* ctl, int skip_retry,
-                          cudaStream_t st);
+                          long long line_stride, int n_in, int n_out, const float2* tw, const DevCtl* ctl,
+                          int skip_retry, cudaStream_t st);
 cudaError_t launch_colmul(int L, float2* S, const KernelView& K, int ncols, int nouter, long long comp_stride,
                           long long outer_stride, long long line_stride, int n_in, int kaxis, float scale,
-                          const DevCtl* ctl, int skip_retry, cudaStream_t st);
-cudaError_t launch_xinv_epi(int M, const float2* S, int hp, int L1, const EpiArgs& A, bool terms, cudaStream_t st,
-                            int* nblocks);
+                          const float2* tw, const DevCtl* ctl, int skip_retry, cudaStream_t st);
+cudaError_t launch_xinv_epi(int M, const float2* S, int hp, int L1, const float2* tw, const EpiArgs& A, bool terms,
+                            cudaStream_t st, int* nblocks);
 cudaError_t launch_local_epi(const EpiArgs& A, bool terms, cudaStream_t st, int* nblocks);
 int xinv_blocks(int M, int n0n1);
 int local_blocks(long long N);

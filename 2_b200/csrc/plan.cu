@@ -16,6 +16,7 @@
 #include <string>
 #include <vector>
 
+#include "fft.cuh"
 #include "mm_internal.h"
 
 namespace mm {
@@ -227,6 +228,7 @@ struct mm_plan_s {
     FieldParams P;
     bool demag = false;
     float* khat = nullptr;
+    float2* tw = nullptr;            // FP32 twiddle table exp(-2 pi i k / 4096)
     KernelView kv;
     float2* S = nullptr;
     // solver state
@@ -371,6 +373,15 @@ extern "C" MM_API int mm_plan_create(const mm_problem* prob, mm_plan* out) {
         g.kd[2] = g.L[2] / 2 + 1;
         const long long oct = (long long)g.kd[0] * g.kd[1] * g.kd[2];
         if ((rc = dalloc(p, (void**)&p->khat, sizeof(float) * 6 * oct))) { delete p; return rc; }
+        if ((rc = dalloc(p, (void**)&p->tw, sizeof(float2) * mmfft::TWN))) { mm_plan_destroy(p); return rc; }
+        {
+            std::vector<float2> h(mmfft::TWN);
+            mmfft::make_twiddle_table(h.data());
+            if (cudaMemcpy(p->tw, h.data(), sizeof(float2) * mmfft::TWN, cudaMemcpyHostToDevice) != cudaSuccess) {
+                mm_plan_destroy(p);
+                return set_err(MM_ERR_CUDA, "twiddle table upload failed");
+            }
+        }
         if ((rc = dalloc(p, (void**)&p->S, sizeof(float2) * 3 * (size_t)g.n[0] * g.L[1] * g.hp))) {
             mm_plan_destroy(p);
             return rc;
@@ -434,7 +445,7 @@ extern "C" MM_API int mm_plan_create(const mm_problem* prob, mm_plan* out) {
 extern "C" MM_API int mm_plan_destroy(mm_plan p) {
     if (!p) return MM_OK;
     free_graph(p);
-    void* bufs[] = {p->khat, p->S, p->Y[0], p->Y[1], p->K1[0], p->K1[1], p->Ma, p->Mb, p->Mtmp, p->ctl,
+    void* bufs[] = {p->khat, p->tw, p->S, p->Y[0], p->Y[1], p->K1[0], p->K1[1], p->Ma, p->Mb, p->Mtmp, p->ctl,
                     p->red, p->dres, p->tq};
     for (void* b : bufs)
         if (b) cudaFree(b);
@@ -499,17 +510,17 @@ static int launch_eval(mm_plan p, const StageOp& op, DevCtl* ctl, int skip_retry
         const int L0 = g.L[0], L1 = g.L[1];
         const long long plane = (long long)L1 * g.hp;
         CUCHK(launch_xfwd<float2, float>(g.M, nullptr, op.m_in, p->P.msat_mask, p->S, 3 * n0 * n1, n0, n1, L1, n2,
-                                         n2, g.hp, ctl, skip_retry, st));
+                                         n2, g.hp, p->tw, ctl, skip_retry, st));
         const float scale = (float)p->prob.msat;
         if (L0 == 1) {
-            CUCHK(launch_colmul(L1, p->S, p->kv, g.h, 1, plane, 0, g.hp, n1, 1, scale, ctl, skip_retry, st));
+            CUCHK(launch_colmul(L1, p->S, p->kv, g.h, 1, plane, 0, g.hp, n1, 1, scale, p->tw, ctl, skip_retry, st));
         } else {
-            CUCHK(launch_colfft<float2>(L1, -1, p->S, g.h, 3 * n0, plane, g.hp, n1, L1, ctl, skip_retry, st));
-            CUCHK(launch_colmul(L0, p->S, p->kv, g.h, L1, (long long)n0 * plane, g.hp, plane, n0, 0, scale, ctl,
-                                skip_retry, st));
-            CUCHK(launch_colfft<float2>(L1, +1, p->S, g.h, 3 * n0, plane, g.hp, L1, n1, ctl, skip_retry, st));
+            CUCHK(launch_colfft<float2>(L1, -1, p->S, g.h, 3 * n0, plane, g.hp, n1, L1, p->tw, ctl, skip_retry, st));
+            CUCHK(launch_colmul(L0, p->S, p->kv, g.h, L1, (long long)n0 * plane, g.hp, plane, n0, 0, scale, p->tw,
+                                ctl, skip_retry, st));
+            CUCHK(launch_colfft<float2>(L1, +1, p->S, g.h, 3 * n0, plane, g.hp, L1, n1, p->tw, ctl, skip_retry, st));
         }
-        CUCHK(launch_xinv_epi(g.M, p->S, g.hp, L1, A, terms, st, &nb));
+        CUCHK(launch_xinv_epi(g.M, p->S, g.hp, L1, p->tw, A, terms, st, &nb));
         p->launches += (L0 == 1) ? 3 : 5;
     } else {
         CUCHK(launch_local_epi(A, terms, st, &nb));
@@ -1078,21 +1089,21 @@ extern "C" MM_API int mm_profile_eval(mm_plan p, int reps, double* ms_out, int* 
             const long long plane = (long long)L1 * g.hp;
             const float scale = (float)p->prob.msat;
             CUCHK(launch_xfwd<float2, float>(g.M, nullptr, op.m_in, p->P.msat_mask, p->S, 3 * n0 * n1, n0, n1, L1,
-                                             n2, n2, g.hp, nullptr, 0, st));
+                                             n2, n2, g.hp, p->tw, nullptr, 0, st));
             CUCHK(cudaEventRecord(ev[k++], st));
             if (L0 == 1) {
-                CUCHK(launch_colmul(L1, p->S, p->kv, g.h, 1, plane, 0, g.hp, n1, 1, scale, nullptr, 0, st));
+                CUCHK(launch_colmul(L1, p->S, p->kv, g.h, 1, plane, 0, g.hp, n1, 1, scale, p->tw, nullptr, 0, st));
                 CUCHK(cudaEventRecord(ev[k++], st));
             } else {
-                CUCHK(launch_colfft<float2>(L1, -1, p->S, g.h, 3 * n0, plane, g.hp, n1, L1, nullptr, 0, st));
+                CUCHK(launch_colfft<float2>(L1, -1, p->S, g.h, 3 * n0, plane, g.hp, n1, L1, p->tw, nullptr, 0, st));
                 CUCHK(cudaEventRecord(ev[k++], st));
                 CUCHK(launch_colmul(L0, p->S, p->kv, g.h, L1, (long long)n0 * plane, g.hp, plane, n0, 0, scale,
-                                    nullptr, 0, st));
+                                    p->tw, nullptr, 0, st));
                 CUCHK(cudaEventRecord(ev[k++], st));
-                CUCHK(launch_colfft<float2>(L1, +1, p->S, g.h, 3 * n0, plane, g.hp, L1, n1, nullptr, 0, st));
+                CUCHK(launch_colfft<float2>(L1, +1, p->S, g.h, 3 * n0, plane, g.hp, L1, n1, p->tw, nullptr, 0, st));
                 CUCHK(cudaEventRecord(ev[k++], st));
             }
-            CUCHK(launch_xinv_epi(g.M, p->S, g.hp, L1, A, false, st, &nb));
+            CUCHK(launch_xinv_epi(g.M, p->S, g.hp, L1, p->tw, A, false, st, &nb));
         } else {
             CUCHK(launch_local_epi(A, false, st, &nb));
         }

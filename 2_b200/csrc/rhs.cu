@@ -440,7 +440,8 @@ __device__ __forceinline__ void process_cell(const EpiArgs& A, const float* m, c
 
 // ---------------------------------------------------------------- C2R row pass + epilogue
 template <int M, bool TERMS>
-__global__ void __launch_bounds__(512) xinv_epi_kernel(const float2* __restrict__ S, int hp, int L1, EpiArgs A) {
+__global__ void __launch_bounds__(512) xinv_epi_kernel(const float2* __restrict__ S, int hp, int L1,
+                                                       const float2* __restrict__ tw, EpiArgs A) {
     const DevCtl* ctl = A.ctl;
     if (skip_eval(ctl, A.skip_retry)) return;
     constexpr int TPL = tpl(M);
@@ -464,13 +465,13 @@ __global__ void __launch_bounds__(512) xinv_epi_kernel(const float2* __restrict_
             float2 a = src[k], b = src[M - k];
             float2 s = make_float2(a.x + b.x, a.y - b.y);
             float2 d = make_float2(a.x - b.x, a.y + b.y);
-            float2 w = Tw<+1, float2>::get(k, 2 * M);
+            float2 w = TwSrc<+1, float2>::get(tw, k, 2 * M);
             float2 wd = cmul(w, d);
             xl[padx(k)] = make_float2(s.x - wd.y, s.y + wd.x);
         }
     }
     __syncthreads();
-    fft_line<M, +1, float2>(lr < rpb ? xl : sm, t, active);
+    fft_line<M, +1, float2>(lr < rpb ? xl : sm, t, active, tw);
     // epilogue over the cells of this block's rows
     const int cur = ctl ? ctl->cur : 0;
     const float h = ctl ? (float)ctl->h : 0.f;
@@ -523,7 +524,8 @@ __global__ void __launch_bounds__(256) local_epi_kernel(EpiArgs A) {
 
 // ---------------------------------------------------------------- launchers
 template <int M, bool TERMS>
-static cudaError_t launch_xinv_t(const float2* S, int hp, int L1, const EpiArgs& A, cudaStream_t st, int* nblocks) {
+static cudaError_t launch_xinv_t(const float2* S, int hp, int L1, const float2* tw, const EpiArgs& A, cudaStream_t st,
+                                 int* nblocks) {
     constexpr int TPL = tpl(M);
     int rpb = (3 * TPL >= 384) ? 1 : 384 / (3 * TPL);
     size_t smem = (size_t)rpb * 3 * line_len(M) * sizeof(float2);
@@ -538,7 +540,7 @@ static cudaError_t launch_xinv_t(const float2* S, int hp, int L1, const EpiArgs&
     int threads = rpb * 3 * TPL;
     if (threads < 32) threads = 32;
     *nblocks = blocks;
-    xinv_epi_kernel<M, TERMS><<<blocks, threads, smem, st>>>(S, hp, L1, A);
+    xinv_epi_kernel<M, TERMS><<<blocks, threads, smem, st>>>(S, hp, L1, tw, A);
     return cudaGetLastError();
 }
 
@@ -550,13 +552,13 @@ int xinv_blocks(int M, int n0n1) {
     return (n0n1 + rpb - 1) / rpb;
 }
 
-cudaError_t launch_xinv_epi(int M, const float2* S, int hp, int L1, const EpiArgs& A, bool terms, cudaStream_t st,
-                            int* nblocks) {
+cudaError_t launch_xinv_epi(int M, const float2* S, int hp, int L1, const float2* tw, const EpiArgs& A, bool terms,
+                            cudaStream_t st, int* nblocks) {
     switch (M) {
 #define X(m)                                                                      \
     case m:                                                                       \
-        return terms ? launch_xinv_t<m, true>(S, hp, L1, A, st, nblocks)          \
-                     : launch_xinv_t<m, false>(S, hp, L1, A, st, nblocks);
+        return terms ? launch_xinv_t<m, true>(S, hp, L1, tw, A, st, nblocks)      \
+                     : launch_xinv_t<m, false>(S, hp, L1, tw, A, st, nblocks);
         X(1) X(2) X(4) X(8) X(16) X(32) X(64) X(128) X(256) X(512) X(1024) X(2048)
 #undef X
         default: return cudaErrorInvalidValue;

@@ -45,9 +45,25 @@ def libs():
     return _LIBS
 
 
+_KEEP = []
+
+
 def dev(a):
+    """Device copy of `a`, kept alive until the end of the test (the kernels run
+    asynchronously: a temporary freed before the launch would hand its memory to the
+    next allocation)."""
     import torch
-    return torch.as_tensor(np.ascontiguousarray(a, dtype=np.float32), device="cuda")
+    t = torch.as_tensor(np.ascontiguousarray(a, dtype=np.float32), device="cuda")
+    _KEEP.append(t)
+    return t
+
+
+@pytest.fixture(autouse=True)
+def _release_buffers():
+    yield
+    import torch
+    torch.cuda.synchronize()
+    _KEEP.clear()
 
 
 def pp(t):
@@ -204,7 +220,7 @@ def test_cmadd_kernelmul_copypad_compat():
         L.copyUnPad3DAsync(pp(back), I(S[0]), I(S[1]), I(S[2]), pp(padded), I(D[0]), I(D[1]), I(D[2]), I(2), STREAM)
         return [d] + md + [padded, back]
     out = run_all(fn)
-    assert np.abs(out["b200"][-1] - arr).max() == 0.0
+    assert np.abs(out["b200"][-1] - arr.astype(np.float32)).max() == 0.0
     check_vs_ref(out)
 
 
