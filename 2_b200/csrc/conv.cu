@@ -275,6 +275,171 @@ __global__ void colmul_kernel(float2* __restrict__ S, KernelView K, int ncols, l
     for (int c = 0; c < 3; c++) tile_store<L, TC, float2>(sm, base + c * comp_stride, line_stride, n_in, nh, c * TC);
 }
 
+// ---------------------------------------------------------------- register z-multiply
+// The 3-D z pass without shared memory.  With the z direction zero-padded to
+// L0 = 2P (P = N0 non-zero planes), the forward transform splits into its even and odd
+// outputs, X[2k'] = DFT_P(x)[k'] and X[2k'+1] = DFT_P(x[z] W_{2P}^z)[k'], and the inverse
+// likewise; so a lane pair takes one (ky, kx) column, each lane one parity, and every
+// transform is a length-P DFT held in registers.  The two halves of the inverse are
+// summed with one shuffle.  Replaces the z column FFT + multiply + inverse of colmul.
+
+// exp(SIGN 2 pi i m / 32); m is a compile-time constant after unrolling
+template <int SIGN>
+__device__ __forceinline__ float2 w32(int m) {
+    constexpr float C[9] = {1.000000000e+00f, 9.807852804e-01f, 9.238795325e-01f, 8.314696123e-01f,
+                            7.071067812e-01f, 5.555702330e-01f, 3.826834324e-01f, 1.950903220e-01f, 0.0f};
+    m &= 31;
+    const int q = m >> 3, r = m & 7;
+    const float cr = C[r], sr = C[8 - r];
+    float2 v = (q == 0) ? make_float2(cr, sr) : (q == 1) ? make_float2(-sr, cr) : (q == 2) ? make_float2(-cr, -sr)
+                                                                                         : make_float2(sr, -cr);
+    return SIGN > 0 ? v : make_float2(v.x, -v.y);
+}
+
+// in-register DFT of length P in {1,2,4,8,16,32}: a[k] = sum_n a[n] exp(SIGN 2 pi i n k / P)
+template <int P, int SIGN> struct RDft {
+    static __device__ __forceinline__ void run(float2* a) { Dft<P, SIGN, float2>::run(a); }
+};
+template <int SIGN> struct RDft<16, SIGN> {
+    static __device__ __forceinline__ void run(float2* a) {
+        float2 t[4][4];
+#pragma unroll
+        for (int r = 0; r < 4; r++) {
+#pragma unroll
+            for (int n = 0; n < 4; n++) t[r][n] = a[4 * n + r];
+            Dft<4, SIGN, float2>::run(t[r]);
+        }
+#pragma unroll
+        for (int k1 = 0; k1 < 4; k1++) {
+            float2 u[4];
+#pragma unroll
+            for (int r = 0; r < 4; r++) u[r] = (r * k1 == 0) ? t[r][k1] : cmul(t[r][k1], w32<SIGN>(2 * r * k1));
+            Dft<4, SIGN, float2>::run(u);
+#pragma unroll
+            for (int k2 = 0; k2 < 4; k2++) a[k1 + 4 * k2] = u[k2];
+        }
+    }
+};
+template <int SIGN> struct RDft<32, SIGN> {
+    static __device__ __forceinline__ void run(float2* a) {
+        float2 e[16], o[16];
+#pragma unroll
+        for (int n = 0; n < 16; n++) { e[n] = a[2 * n]; o[n] = a[2 * n + 1]; }
+        RDft<16, SIGN>::run(e);
+        RDft<16, SIGN>::run(o);
+#pragma unroll
+        for (int k = 0; k < 16; k++) {
+            float2 wo = (k == 0) ? o[k] : cmul(o[k], w32<SIGN>(k));
+            a[k] = cadd(e[k], wo);
+            a[k + 16] = csub(e[k], wo);
+        }
+    }
+};
+
+// exp(SIGN 2 pi i z / (2P)) from the FP32 table
+template <int SIGN>
+__device__ __forceinline__ float2 wtab(const float2* __restrict__ tw, int num, int den) {
+    return TwSrc<SIGN, float2>::get(tw, num, den);
+}
+
+template <int P>
+__global__ void __launch_bounds__(128) zmul_reg_kernel(float2* __restrict__ S, KernelView K, int L1, int h, int hp,
+                                                       long long comp_stride, long long zstride, float scale,
+                                                       const float2* __restrict__ tw, const DevCtl* ctl,
+                                                       int skip_retry) {
+    if (conv_skip(ctl, skip_retry)) return;
+    const long long gt = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const int s = (int)(gt & 1);
+    const long long colg = gt >> 1;
+    const bool active = colg < (long long)L1 * h;
+    const int ky = active ? (int)(colg / h) : 0;
+    const int kx = active ? (int)(colg % h) : 0;
+    float2* base = S + (long long)ky * hp + kx;
+    float2 x[3][P];
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+#pragma unroll
+        for (int z = 0; z < P; z++)
+            x[c][z] = active ? base[c * comp_stride + z * zstride] : make_float2(0.f, 0.f);
+    // odd outputs: pre-multiply by W_{2P}^z (forward)
+    if (s) {
+#pragma unroll
+        for (int z = 1; z < P; z++) {
+            const float2 w = wtab<-1>(tw, z, 2 * P);
+#pragma unroll
+            for (int c = 0; c < 3; c++) x[c][z] = cmul(x[c][z], w);
+        }
+    }
+#pragma unroll
+    for (int c = 0; c < 3; c++) RDft<P, -1>::run(x[c]);
+    // multiply: x[c][k'] holds X_c[kz], kz = 2k' + s
+    const int kyy = (ky > (K.L1 >> 1)) ? K.L1 - ky : ky;
+    const float sy = (ky > (K.L1 >> 1)) ? -1.f : 1.f;
+    const int cs = K.kd0 * K.kd1 * K.kd2;
+#pragma unroll
+    for (int k = 0; k < P; k++) {
+        int kz = 2 * k + s;
+        float sz = 1.f;
+        if (kz > P) { kz = 2 * P - kz; sz = -1.f; }
+        const int idx = (kz * K.kd1 + kyy) * K.kd2 + kx;
+        const float kxx = __ldg(K.k + idx);
+        const float kyy_ = __ldg(K.k + cs + idx);
+        const float kzz = __ldg(K.k + 2 * cs + idx);
+        const float kyz = K.nz[3] ? sy * __ldg(K.k + 3 * cs + idx) : 0.f;
+        const float kxz = K.nz[4] ? sz * __ldg(K.k + 4 * cs + idx) : 0.f;
+        const float kxy = K.nz[5] ? sz * sy * __ldg(K.k + 5 * cs + idx) : 0.f;
+        const float2 m0 = x[0][k], m1 = x[1][k], m2 = x[2][k];
+        x[0][k] = make_float2(scale * (kxx * m0.x + kxy * m1.x + kxz * m2.x), scale * (kxx * m0.y + kxy * m1.y + kxz * m2.y));
+        x[1][k] = make_float2(scale * (kxy * m0.x + kyy_ * m1.x + kyz * m2.x), scale * (kxy * m0.y + kyy_ * m1.y + kyz * m2.y));
+        x[2][k] = make_float2(scale * (kxz * m0.x + kyz * m1.x + kzz * m2.x), scale * (kxz * m0.y + kyz * m1.y + kzz * m2.y));
+    }
+#pragma unroll
+    for (int c = 0; c < 3; c++) RDft<P, +1>::run(x[c]);
+    if (s) {
+#pragma unroll
+        for (int z = 1; z < P; z++) {
+            const float2 w = wtab<+1>(tw, z, 2 * P);
+#pragma unroll
+            for (int c = 0; c < 3; c++) x[c][z] = cmul(x[c][z], w);
+        }
+    }
+    // sum of the even and odd halves of the inverse; each lane stores half of the planes
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+#pragma unroll
+        for (int z = 0; z < P; z++) {
+            float2 v = x[c][z];
+            v.x += __shfl_xor_sync(0xffffffffu, v.x, 1);
+            v.y += __shfl_xor_sync(0xffffffffu, v.y, 1);
+            const bool mine = (P == 1) ? (s == 0) : ((z < P / 2) == (s == 0));
+            if (active && mine) base[c * comp_stride + z * zstride] = v;
+        }
+}
+
+template <int P>
+static cudaError_t launch_zmul_reg_t(float2* S, const KernelView& K, int L1, int h, int hp, long long comp_stride,
+                                     long long zstride, float scale, const float2* tw, const DevCtl* ctl,
+                                     int skip_retry, cudaStream_t st) {
+    const long long threads = 2LL * L1 * h;
+    const int blocks = (int)((threads + 127) / 128);
+    zmul_reg_kernel<P><<<blocks, 128, 0, st>>>(S, K, L1, h, hp, comp_stride, zstride, scale, tw, ctl, skip_retry);
+    return cudaGetLastError();
+}
+
+// P = N0 = L0/2 (zero-padded z); returns cudaErrorNotSupported for other shapes
+cudaError_t launch_zmul_reg(int P, float2* S, const KernelView& K, int L1, int h, int hp, long long comp_stride,
+                            long long zstride, float scale, const float2* tw, const DevCtl* ctl, int skip_retry,
+                            cudaStream_t st) {
+    switch (P) {
+        case 1: return launch_zmul_reg_t<1>(S, K, L1, h, hp, comp_stride, zstride, scale, tw, ctl, skip_retry, st);
+        case 2: return launch_zmul_reg_t<2>(S, K, L1, h, hp, comp_stride, zstride, scale, tw, ctl, skip_retry, st);
+        case 4: return launch_zmul_reg_t<4>(S, K, L1, h, hp, comp_stride, zstride, scale, tw, ctl, skip_retry, st);
+        case 8: return launch_zmul_reg_t<8>(S, K, L1, h, hp, comp_stride, zstride, scale, tw, ctl, skip_retry, st);
+        case 16: return launch_zmul_reg_t<16>(S, K, L1, h, hp, comp_stride, zstride, scale, tw, ctl, skip_retry, st);
+        default: return cudaErrorNotSupported;
+    }
+}
+
 // ---------------------------------------------------------------- launch helpers
 template <typename KT> static cudaError_t set_smem(KT kern, size_t bytes) {
     if (bytes > 48 * 1024) return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);

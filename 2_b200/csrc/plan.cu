@@ -483,6 +483,12 @@ extern "C" MM_API int mm_plan_kernel_nonzero(mm_plan p, int out6[6]) {
 
 extern "C" MM_API long long mm_plan_device_bytes(mm_plan p) { return p ? p->bytes : 0; }
 
+// the register z-multiply applies when z is zero-padded (L0 = 2 N0) with N0 <= 16
+static bool zreg_ok(const ConvGeom& g) {
+    const int n0 = g.n[0];
+    return g.L[0] == 2 * n0 && (n0 == 1 || n0 == 2 || n0 == 4 || n0 == 8 || n0 == 16);
+}
+
 // ---------------------------------------------------------------- one evaluation
 // Launches the convolution passes (if demag) and the epilogue for one StageOp.
 static int launch_eval(mm_plan p, const StageOp& op, DevCtl* ctl, int skip_retry, float* const* dbg,
@@ -516,8 +522,12 @@ static int launch_eval(mm_plan p, const StageOp& op, DevCtl* ctl, int skip_retry
             CUCHK(launch_colmul(L1, p->S, p->kv, g.h, 1, plane, 0, g.hp, n1, 1, scale, p->tw, ctl, skip_retry, st));
         } else {
             CUCHK(launch_colfft<float2>(L1, -1, p->S, g.h, 3 * n0, plane, g.hp, n1, L1, p->tw, ctl, skip_retry, st));
-            CUCHK(launch_colmul(L0, p->S, p->kv, g.h, L1, (long long)n0 * plane, g.hp, plane, n0, 0, scale, p->tw,
-                                ctl, skip_retry, st));
+            if (zreg_ok(g))
+                CUCHK(launch_zmul_reg(n0, p->S, p->kv, L1, g.h, g.hp, (long long)n0 * plane, plane, scale, p->tw, ctl,
+                                      skip_retry, st));
+            else
+                CUCHK(launch_colmul(L0, p->S, p->kv, g.h, L1, (long long)n0 * plane, g.hp, plane, n0, 0, scale, p->tw,
+                                    ctl, skip_retry, st));
             CUCHK(launch_colfft<float2>(L1, +1, p->S, g.h, 3 * n0, plane, g.hp, L1, n1, p->tw, ctl, skip_retry, st));
         }
         CUCHK(launch_xinv_epi(g.M, p->S, g.hp, L1, p->tw, A, terms, st, &nb));
@@ -1097,8 +1107,12 @@ extern "C" MM_API int mm_profile_eval(mm_plan p, int reps, double* ms_out, int* 
             } else {
                 CUCHK(launch_colfft<float2>(L1, -1, p->S, g.h, 3 * n0, plane, g.hp, n1, L1, p->tw, nullptr, 0, st));
                 CUCHK(cudaEventRecord(ev[k++], st));
-                CUCHK(launch_colmul(L0, p->S, p->kv, g.h, L1, (long long)n0 * plane, g.hp, plane, n0, 0, scale,
-                                    p->tw, nullptr, 0, st));
+                if (zreg_ok(g))
+                    CUCHK(launch_zmul_reg(n0, p->S, p->kv, L1, g.h, g.hp, (long long)n0 * plane, plane, scale, p->tw,
+                                          nullptr, 0, st));
+                else
+                    CUCHK(launch_colmul(L0, p->S, p->kv, g.h, L1, (long long)n0 * plane, g.hp, plane, n0, 0, scale,
+                                        p->tw, nullptr, 0, st));
                 CUCHK(cudaEventRecord(ev[k++], st));
                 CUCHK(launch_colfft<float2>(L1, +1, p->S, g.h, 3 * n0, plane, g.hp, L1, n1, p->tw, nullptr, 0, st));
                 CUCHK(cudaEventRecord(ev[k++], st));
