@@ -164,6 +164,7 @@ cudaError_t launch_xinv_epi(int M, const float2* S, int hp, int L1, const float2
                             cudaStream_t st, int* nblocks);
 cudaError_t launch_local_epi(const EpiArgs& A, bool terms, cudaStream_t st, int* nblocks);
 int xinv_blocks(int M, int n0n1);
+int report_error(int code, const char* msg);  // sets mm_last_error()
 int local_blocks(long long N);
 
 }  // namespace mm

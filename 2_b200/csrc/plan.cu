@@ -36,6 +36,11 @@ static int set_err(int code, const char* fmt, ...) {
     g_err = buf;
     return code;
 }
+namespace mm {
+// lets other translation units report through mm_last_error()
+int report_error(int code, const char* msg) { return set_err(code, "%s", msg); }
+}  // namespace mm
+
 #define CUCHK(...)                                                                                            \
     do {                                                                                                      \
         cudaError_t e_ = (__VA_ARGS__);                                                                               \

@@ -89,6 +89,7 @@ _PROTOS = {
     "mm_plan_launch_count": (C.c_longlong, [C.c_void_p]),
     "mm_profile_eval": (C.c_int, [C.c_void_p, C.c_int, DP, C.POINTER(C.c_int), C.c_void_p]),
     "mm_plan_geometry": (C.c_int, [C.c_void_p, C.c_int * 12]),
+    "mm_average_noalloc": (C.c_int, [C.c_void_p, C.c_longlong, C.c_void_p, C.c_void_p]),
 }
 
 

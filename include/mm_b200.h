@@ -138,6 +138,16 @@ MM_API int mm_average(mm_plan plan, double out[3], mm_stream stream);
 /* E_zeeman, E_ex, E_demag, E_anis, E (J) -- compensated FP32 sums. */
 MM_API int mm_energy(mm_plan plan, double out[5], mm_stream stream);
 
+/* <m> without any device allocation, for callers that cannot allocate device memory
+ * (code inside a CUDA stream capture, engines whose device memory belongs to another
+ * allocator, host code that must not block on the allocator).  No counterpart in the
+ * reference.  m: device SoA float32 3 x ncell; out: device, 3 doubles (sum m_c / ncell).
+ * ncell is limited to 16,777,216 (MM_ERR_ARG beyond): the block partials live in a fixed
+ * 192 KB file-scope device array held by every GPU that loads the library.  The first
+ * call on a device looks up that array's address and should precede any stream capture;
+ * calls share the array, so calls that overlap on the GPU race. */
+MM_API int mm_average_noalloc(const float* m, long long ncell, double* out, mm_stream stream);
+
 /* ---- instrumentation ---- */
 /* Kernels this plan has enqueued so far (graph replays counted per kernel node). */
 MM_API long long mm_plan_launch_count(mm_plan plan);
