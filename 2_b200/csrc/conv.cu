@@ -20,6 +20,7 @@
 #include <cstdio>
 
 #include "fft.cuh"
+#include "fft4.cuh"
 #include "mm_internal.h"
 
 namespace mm {
@@ -283,59 +284,6 @@ __global__ void colmul_kernel(float2* __restrict__ S, KernelView K, int ncols, l
 // transform is a length-P DFT held in registers.  The two halves of the inverse are
 // summed with one shuffle.  Replaces the z column FFT + multiply + inverse of colmul.
 
-// exp(SIGN 2 pi i m / 32); m is a compile-time constant after unrolling
-template <int SIGN>
-__device__ __forceinline__ float2 w32(int m) {
-    constexpr float C[9] = {1.000000000e+00f, 9.807852804e-01f, 9.238795325e-01f, 8.314696123e-01f,
-                            7.071067812e-01f, 5.555702330e-01f, 3.826834324e-01f, 1.950903220e-01f, 0.0f};
-    m &= 31;
-    const int q = m >> 3, r = m & 7;
-    const float cr = C[r], sr = C[8 - r];
-    float2 v = (q == 0) ? make_float2(cr, sr) : (q == 1) ? make_float2(-sr, cr) : (q == 2) ? make_float2(-cr, -sr)
-                                                                                         : make_float2(sr, -cr);
-    return SIGN > 0 ? v : make_float2(v.x, -v.y);
-}
-
-// in-register DFT of length P in {1,2,4,8,16,32}: a[k] = sum_n a[n] exp(SIGN 2 pi i n k / P)
-template <int P, int SIGN> struct RDft {
-    static __device__ __forceinline__ void run(float2* a) { Dft<P, SIGN, float2>::run(a); }
-};
-template <int SIGN> struct RDft<16, SIGN> {
-    static __device__ __forceinline__ void run(float2* a) {
-        float2 t[4][4];
-#pragma unroll
-        for (int r = 0; r < 4; r++) {
-#pragma unroll
-            for (int n = 0; n < 4; n++) t[r][n] = a[4 * n + r];
-            Dft<4, SIGN, float2>::run(t[r]);
-        }
-#pragma unroll
-        for (int k1 = 0; k1 < 4; k1++) {
-            float2 u[4];
-#pragma unroll
-            for (int r = 0; r < 4; r++) u[r] = (r * k1 == 0) ? t[r][k1] : cmul(t[r][k1], w32<SIGN>(2 * r * k1));
-            Dft<4, SIGN, float2>::run(u);
-#pragma unroll
-            for (int k2 = 0; k2 < 4; k2++) a[k1 + 4 * k2] = u[k2];
-        }
-    }
-};
-template <int SIGN> struct RDft<32, SIGN> {
-    static __device__ __forceinline__ void run(float2* a) {
-        float2 e[16], o[16];
-#pragma unroll
-        for (int n = 0; n < 16; n++) { e[n] = a[2 * n]; o[n] = a[2 * n + 1]; }
-        RDft<16, SIGN>::run(e);
-        RDft<16, SIGN>::run(o);
-#pragma unroll
-        for (int k = 0; k < 16; k++) {
-            float2 wo = (k == 0) ? o[k] : cmul(o[k], w32<SIGN>(k));
-            a[k] = cadd(e[k], wo);
-            a[k + 16] = csub(e[k], wo);
-        }
-    }
-};
-
 // exp(SIGN 2 pi i z / (2P)) from the FP32 table
 template <int SIGN>
 __device__ __forceinline__ float2 wtab(const float2* __restrict__ tw, int num, int den) {
@@ -440,6 +388,110 @@ cudaError_t launch_zmul_reg(int P, float2* S, const KernelView& K, int L1, int h
     }
 }
 
+// ---------------------------------------------------------------- four-step kernels (L <= 1024)
+// Column tile of the four-step column pass: 256 threads per block, at most 48 KB.
+__host__ __device__ constexpr int col4_tile(int L) {
+    int tc = 256 / fs_p2(L);
+    if (tc > 32) tc = 32;
+    while (tc > 1 && tc * (L / fs_p2(L)) * (fs_p2(L) + 1) * 8 > 48 * 1024) tc /= 2;
+    return tc;
+}
+
+template <int L, int SIGN>
+__global__ void __launch_bounds__(256) colfft4_kernel(float2* __restrict__ S, int ncols, long long outer_stride,
+                                                      long long line_stride, int n_in, int n_out,
+                                                      const float2* __restrict__ tw, const DevCtl* ctl,
+                                                      int skip_retry) {
+    if (conv_skip(ctl, skip_retry)) return;
+    using F = FS<L>;
+    constexpr int TC = col4_tile(L);
+    extern __shared__ unsigned char smem_raw[];
+    float2* sm = reinterpret_cast<float2*>(smem_raw);
+    const int col = threadIdx.x % TC, t = threadIdx.x / TC;
+    const int ntiles = (ncols + TC - 1) / TC;
+    const int o = blockIdx.x / ntiles;
+    const int kx0 = (blockIdx.x % ntiles) * TC;
+    const bool active = (t < F::P2) && (kx0 + col < ncols);
+    float2* base = S + (long long)o * outer_stride + kx0 + col;
+    float2 v[F::P1];
+#pragma unroll
+    for (int j = 0; j < F::P1; j++) {
+        const int n = F::in_index(t, j);
+        v[j] = (active && n < n_in) ? base[n * line_stride] : make_float2(0.f, 0.f);
+    }
+    F::template run<SIGN>(v, sm + col * F::LBUF, t, active, tw);
+#pragma unroll
+    for (int r = 0; r < F::P1; r++) {
+        const int n = F::out_index(t, r);
+        if (active && n < n_out) base[n * line_stride] = v[r];
+    }
+}
+
+// R2C rows (zero-padded to 2M reals) with the four-step transform of the packed
+// sequence z[n] = x[2n] + i x[2n+1], then the real-to-complex post-processing.
+template <int M>
+__global__ void __launch_bounds__(256) xfwd4_kernel(const float* __restrict__ in_fixed, PP in_pp,
+                                                    const float* __restrict__ mask, float2* __restrict__ out,
+                                                    int nrows, int Z, int Y, int Yout, int in_pitch, int n_in, int hp,
+                                                    const float2* __restrict__ tw, const DevCtl* ctl, int skip_retry) {
+    if (conv_skip(ctl, skip_retry)) return;
+    using F = FS<M>;
+    constexpr int RPB = (256 / F::P2) > 0 ? 256 / F::P2 : 1;
+    const float* in = in_fixed ? in_fixed : in_pp.get(ctl ? ctl->cur : 0);
+    extern __shared__ unsigned char smem_raw[];
+    float2* sm = reinterpret_cast<float2*>(smem_raw);
+    const int t = threadIdx.x % F::P2, lr = threadIdx.x / F::P2;
+    const int row = blockIdx.x * RPB + lr;
+    const bool active = (lr < RPB) && (row < nrows);
+    float2* buf = sm + (lr < RPB ? lr : 0) * F::LBUF;
+    float2 v[F::P1];
+    const float* src = in + (long long)(active ? row : 0) * in_pitch;
+    const int zy = (active ? row : 0) % (Z * Y);
+    const float* msk = mask ? mask + (long long)zy * in_pitch : nullptr;
+    const bool pairs = ((in_pitch & 1) == 0);
+#pragma unroll
+    for (int j = 0; j < F::P1; j++) {
+        const int n = F::in_index(t, j);
+        float a = 0.f, b = 0.f;
+        if (active) {
+            if (pairs && 2 * n + 1 < n_in) {
+                float2 ab = __ldg(reinterpret_cast<const float2*>(src) + n);
+                if (msk) {
+                    const float2 mm = __ldg(reinterpret_cast<const float2*>(msk) + n);
+                    ab.x *= mm.x;
+                    ab.y *= mm.y;
+                }
+                a = ab.x;
+                b = ab.y;
+            } else {
+                if (2 * n < n_in) a = src[2 * n] * (msk ? msk[2 * n] : 1.f);
+                if (2 * n + 1 < n_in) b = src[2 * n + 1] * (msk ? msk[2 * n + 1] : 1.f);
+            }
+        }
+        v[j] = make_float2(a, b);
+    }
+    F::template run<-1>(v, buf, t, active, tw);
+    if (active) {
+#pragma unroll
+        for (int r = 0; r < F::P1; r++) buf[F::out_index(t, r)] = v[r];
+    }
+    __syncthreads();
+    if (active) {
+        const int c = row / (Z * Y);
+        const int z = zy / Y, y = zy % Y;
+        float2* dst = out + ((long long)(c * Z + z) * Yout + y) * hp;
+        for (int k = t; k <= M / 2; k += F::P2) {
+            const float2 zk = buf[k & (M - 1)];
+            const float2 zm = buf[(M - k) & (M - 1)];
+            const float2 e = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
+            const float2 od = make_float2(0.5f * (zk.y + zm.y), -0.5f * (zk.x - zm.x));  // (Z[k] - conj Z[M-k]) / 2i
+            const float2 w = TwSrc<-1, float2>::get(tw, k, 2 * M);
+            dst[k] = cadd(e, cmul(w, od));
+            if (k != M - k) dst[M - k] = cadd(cconj(e), cmul(make_float2(-w.x, w.y), cconj(od)));
+        }
+    }
+}
+
 // ---------------------------------------------------------------- launch helpers
 template <typename KT> static cudaError_t set_smem(KT kern, size_t bytes) {
     if (bytes > 48 * 1024) return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
@@ -464,10 +516,33 @@ static cudaError_t launch_xfwd_t(const S* in, PP pp, const float* mask, V* out, 
     return cudaGetLastError();
 }
 
+template <int M>
+static cudaError_t launch_xfwd4_t(const float* in, PP pp, const float* mask, float2* out, int nrows, int Z, int Y,
+                                  int Yout, int in_pitch, int n_in, int hp, const float2* tw, const DevCtl* ctl,
+                                  int skip_retry, cudaStream_t st) {
+    using F = FS<M>;
+    constexpr int RPB = (256 / F::P2) > 0 ? 256 / F::P2 : 1;
+    const size_t smem = (size_t)RPB * F::LBUF * sizeof(float2);
+    cudaError_t e = set_smem(xfwd4_kernel<M>, smem);
+    if (e != cudaSuccess) return e;
+    const int blocks = (nrows + RPB - 1) / RPB;
+    xfwd4_kernel<M><<<blocks, RPB * F::P2, smem, st>>>(in, pp, mask, out, nrows, Z, Y, Yout, in_pitch, n_in, hp, tw,
+                                                        ctl, skip_retry);
+    return cudaGetLastError();
+}
+
 template <typename V, typename S>
 cudaError_t launch_xfwd(int M, const S* in, PP pp, const float* mask, V* out, int nrows, int Z, int Y, int Yout,
                         int in_pitch, int n_in, int hp, const float2* tw, const DevCtl* ctl, int skip_retry,
                         cudaStream_t st) {
+    if constexpr (sizeof(V) == 8) {
+        switch (M) {
+#define X(m) case m: return launch_xfwd4_t<m>(in, pp, mask, out, nrows, Z, Y, Yout, in_pitch, n_in, hp, tw, ctl, skip_retry, st);
+            X(4) X(8) X(16) X(32) X(64) X(128) X(256) X(512) X(1024)
+#undef X
+            default: break;
+        }
+    }
     switch (M) {
 #define X(m) case m: return launch_xfwd_t<m, V, S>(in, pp, mask, out, nrows, Z, Y, Yout, in_pitch, n_in, hp, tw, ctl, skip_retry, st);
         MM_FOR_POW2(X)
@@ -492,10 +567,44 @@ static cudaError_t launch_colfft_t(V* S, int ncols, int nouter, long long outer_
     return cudaGetLastError();
 }
 
+template <int L, int SIGN>
+static cudaError_t launch_colfft4_t(float2* S, int ncols, int nouter, long long outer_stride, long long line_stride,
+                                    int n_in, int n_out, const float2* tw, const DevCtl* ctl, int skip_retry,
+                                    cudaStream_t st) {
+    using F = FS<L>;
+    constexpr int TC = col4_tile(L);
+    const size_t smem = (size_t)TC * F::LBUF * sizeof(float2);
+    cudaError_t e = set_smem(colfft4_kernel<L, SIGN>, smem);
+    if (e != cudaSuccess) return e;
+    const int ntiles = (ncols + TC - 1) / TC;
+    int threads = TC * F::P2;
+    if (threads < 32) threads = 32;
+    colfft4_kernel<L, SIGN><<<nouter * ntiles, threads, smem, st>>>(S, ncols, outer_stride, line_stride, n_in, n_out,
+                                                                    tw, ctl, skip_retry);
+    return cudaGetLastError();
+}
+
 template <typename V>
 cudaError_t launch_colfft(int L, int sign, V* S, int ncols, int nouter, long long outer_stride,
                           long long line_stride, int n_in, int n_out, const float2* tw, const DevCtl* ctl,
                           int skip_retry, cudaStream_t st) {
+    if constexpr (sizeof(V) == 8) {
+        if (sign < 0) {
+            switch (L) {
+#define X(l) case l: return launch_colfft4_t<l, -1>(S, ncols, nouter, outer_stride, line_stride, n_in, n_out, tw, ctl, skip_retry, st);
+                X(4) X(8) X(16) X(32) X(64) X(128) X(256) X(512) X(1024)
+#undef X
+                default: break;
+            }
+        } else {
+            switch (L) {
+#define X(l) case l: return launch_colfft4_t<l, 1>(S, ncols, nouter, outer_stride, line_stride, n_in, n_out, tw, ctl, skip_retry, st);
+                X(4) X(8) X(16) X(32) X(64) X(128) X(256) X(512) X(1024)
+#undef X
+                default: break;
+            }
+        }
+    }
     if (sign < 0) {
         switch (L) {
 #define X(l) case l: return launch_colfft_t<l, -1, V>(S, ncols, nouter, outer_stride, line_stride, n_in, n_out, tw, ctl, skip_retry, st);

@@ -16,6 +16,7 @@
 #include <cstdio>
 
 #include "fft.cuh"
+#include "fft4.cuh"
 #include "mm_internal.h"
 
 namespace mm {
@@ -439,6 +440,36 @@ __device__ __forceinline__ void process_cell(const EpiArgs& A, const float* m, c
 }
 
 // ---------------------------------------------------------------- C2R row pass + epilogue
+// Cells of the block's rows; H_demag of (row, c) at cell x is element x>>1 (real part for
+// even x, imaginary part for odd x) of shared-memory line (lrow*3 + c), stride LS.
+template <bool TERMS, bool PADDED>
+__device__ __forceinline__ void epilogue_rows(const EpiArgs& A, const float2* sm, int LS, int row0, int nrow_here) {
+    const DevCtl* ctl = A.ctl;
+    const int n1 = A.P.n[1], n2 = A.P.n[2];
+    const int cur = ctl ? ctl->cur : 0;
+    const float h = ctl ? (float)ctl->h : 0.f;
+    const long long ns = ctl ? ctl->noise_step : A.noise_step;
+    const float dtth = ctl ? (float)(ctl->dt_thermal > 0 ? ctl->dt_thermal : ctl->dt) : (float)A.dt_thermal;
+    ResolvedOp r;
+    resolve_op(A.op, cur, h, r);
+    const float* m = A.op.m_in.get(cur);
+    ThreadRed tr = {0.f, 0.f, 0, {{0.f, 0.f}, {0.f, 0.f}, {0.f, 0.f}, {0.f, 0.f}}};
+    for (int e = threadIdx.x; e < nrow_here * n2; e += blockDim.x) {
+        const int lrow = e / n2, x = e % n2;
+        const int grow = row0 + lrow;
+        const int z = grow / n1, y = grow % n1;
+        const long long i = (long long)grow * n2 + x;
+        const int pi = PADDED ? padx(x >> 1) : (x >> 1);
+        const float2 v0 = sm[(lrow * 3 + 0) * LS + pi];
+        const float2 v1 = sm[(lrow * 3 + 1) * LS + pi];
+        const float2 v2 = sm[(lrow * 3 + 2) * LS + pi];
+        const float3 hd = (x & 1) ? make_float3(v0.y, v1.y, v2.y) : make_float3(v0.x, v1.x, v2.x);
+        process_cell<TERMS>(A, m, r, i, z, y, x, hd, ns, dtth, tr);
+    }
+    block_reduce_publish(tr, A.op, A.ctl, A.tq_out, A.red);
+}
+
+// Stockham variant (any power-of-two M up to 2048)
 template <int M, bool TERMS>
 __global__ void __launch_bounds__(512) xinv_epi_kernel(const float2* __restrict__ S, int hp, int L1,
                                                        const float2* __restrict__ tw, EpiArgs A) {
@@ -448,7 +479,7 @@ __global__ void __launch_bounds__(512) xinv_epi_kernel(const float2* __restrict_
     constexpr int LL = line_len(M);
     extern __shared__ unsigned char smem_raw[];
     float2* sm = reinterpret_cast<float2*>(smem_raw);
-    const int n0 = A.P.n[0], n1 = A.P.n[1], n2 = A.P.n[2];
+    const int n0 = A.P.n[0], n1 = A.P.n[1];
     const int nrows = n0 * n1;
     const int rpb = blockDim.x / (3 * TPL);
     const int lr = threadIdx.x / (3 * TPL);
@@ -456,7 +487,7 @@ __global__ void __launch_bounds__(512) xinv_epi_kernel(const float2* __restrict_
     const int t = threadIdx.x % TPL;
     const int row = blockIdx.x * rpb + lr;
     const bool active = (lr < rpb) && (row < nrows);
-    float2* xl = sm + (lr * 3 + c) * LL;
+    float2* xl = sm + (lr < rpb ? lr * 3 + c : 0) * LL;
     if (active) {
         const int z = row / n1, y = row % n1;
         const float2* src = S + ((long long)(c * n0 + z) * L1 + y) * hp;
@@ -471,31 +502,63 @@ __global__ void __launch_bounds__(512) xinv_epi_kernel(const float2* __restrict_
         }
     }
     __syncthreads();
-    fft_line<M, +1, float2>(lr < rpb ? xl : sm, t, active, tw);
-    // epilogue over the cells of this block's rows
-    const int cur = ctl ? ctl->cur : 0;
-    const float h = ctl ? (float)ctl->h : 0.f;
-    const long long ns = ctl ? ctl->noise_step : A.noise_step;
-    const float dtth = ctl ? (float)(ctl->dt_thermal > 0 ? ctl->dt_thermal : ctl->dt) : (float)A.dt_thermal;
-    ResolvedOp r;
-    resolve_op(A.op, cur, h, r);
-    const float* m = A.op.m_in.get(cur);
-    ThreadRed tr = {0.f, 0.f, 0, {{0.f, 0.f}, {0.f, 0.f}, {0.f, 0.f}, {0.f, 0.f}}};
+    fft_line<M, +1, float2>(xl, t, active, tw);
     const int row0 = blockIdx.x * rpb;
-    const int nrow_here = min(rpb, nrows - row0);
-    for (int e = threadIdx.x; e < nrow_here * n2; e += blockDim.x) {
-        const int lrow = e / n2, x = e % n2;
-        const int grow = row0 + lrow;
-        const int z = grow / n1, y = grow % n1;
-        const long long i = (long long)grow * n2 + x;
-        const int pi = padx(x >> 1);
-        float2 v0 = sm[(lrow * 3 + 0) * LL + pi];
-        float2 v1 = sm[(lrow * 3 + 1) * LL + pi];
-        float2 v2 = sm[(lrow * 3 + 2) * LL + pi];
-        float3 hd = (x & 1) ? make_float3(v0.y, v1.y, v2.y) : make_float3(v0.x, v1.x, v2.x);
-        process_cell<TERMS>(A, m, r, i, z, y, x, hd, ns, dtth, tr);
+    epilogue_rows<TERMS, true>(A, sm, LL, row0, min(rpb, nrows - row0));
+}
+
+// Four-step variant (4 <= M <= 1024): the pre-processed spectrum goes straight from
+// global memory into registers, one shared-memory transpose, the result is written to
+// shared memory in natural order for the epilogue.
+template <int M>
+__host__ __device__ constexpr int xinv4_rpb() {
+    return (384 / (3 * FS<M>::P2)) > 0 ? 384 / (3 * FS<M>::P2) : 1;
+}
+
+template <int M, bool TERMS>
+__global__ void __launch_bounds__(384) xinv4_epi_kernel(const float2* __restrict__ S, int hp, int L1,
+                                                        const float2* __restrict__ tw, EpiArgs A) {
+    const DevCtl* ctl = A.ctl;
+    if (skip_eval(ctl, A.skip_retry)) return;
+    using F = FS<M>;
+    constexpr int RPB = xinv4_rpb<M>();
+    extern __shared__ unsigned char smem_raw[];
+    float2* sm = reinterpret_cast<float2*>(smem_raw);
+    const int n0 = A.P.n[0], n1 = A.P.n[1];
+    const int nrows = n0 * n1;
+    const int t = threadIdx.x % F::P2;
+    const int c = (threadIdx.x / F::P2) % 3;
+    const int lr = threadIdx.x / (3 * F::P2);
+    const int row = blockIdx.x * RPB + lr;
+    const bool active = (lr < RPB) && (row < nrows);
+    float2* buf = sm + (lr < RPB ? lr * 3 + c : 0) * F::LBUF;
+    float2 v[F::P1];
+    {
+        const int rr = active ? row : 0;
+        const int z = rr / n1, y = rr % n1;
+        const float2* src = S + ((long long)(c * n0 + z) * L1 + y) * hp;
+#pragma unroll
+        for (int j = 0; j < F::P1; j++) {
+            const int k = F::in_index(t, j);
+            float2 val = make_float2(0.f, 0.f);
+            if (active) {
+                const float2 a = src[k], b = src[M - k];
+                const float2 s = make_float2(a.x + b.x, a.y - b.y);
+                const float2 d = make_float2(a.x - b.x, a.y + b.y);
+                const float2 wd = cmul(TwSrc<+1, float2>::get(tw, k, 2 * M), d);
+                val = make_float2(s.x - wd.y, s.y + wd.x);
+            }
+            v[j] = val;
+        }
     }
-    block_reduce_publish(tr, A.op, A.ctl, A.tq_out, A.red);
+    F::template run<+1>(v, buf, t, active, tw);
+    if (active) {
+#pragma unroll
+        for (int r = 0; r < F::P1; r++) buf[F::out_index(t, r)] = v[r];
+    }
+    __syncthreads();
+    const int row0 = blockIdx.x * RPB;
+    epilogue_rows<TERMS, false>(A, sm, F::LBUF, row0, min(RPB, nrows - row0));
 }
 
 // ---------------------------------------------------------------- epilogue without demag
@@ -544,7 +607,37 @@ static cudaError_t launch_xinv_t(const float2* S, int hp, int L1, const float2* 
     return cudaGetLastError();
 }
 
+template <int M, bool TERMS>
+static cudaError_t launch_xinv4_t(const float2* S, int hp, int L1, const float2* tw, const EpiArgs& A,
+                                  cudaStream_t st, int* nblocks) {
+    constexpr int RPB = xinv4_rpb<M>();
+    const size_t smem = (size_t)RPB * 3 * FS<M>::LBUF * sizeof(float2);
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(xinv4_epi_kernel<M, TERMS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    const int nrows = A.P.n[0] * A.P.n[1];
+    const int blocks = (nrows + RPB - 1) / RPB;
+    int threads = RPB * 3 * FS<M>::P2;
+    if (threads < 32) threads = 32;
+    *nblocks = blocks;
+    xinv4_epi_kernel<M, TERMS><<<blocks, threads, smem, st>>>(S, hp, L1, tw, A);
+    return cudaGetLastError();
+}
+
+static bool use_xinv4(int M) { return M >= 4 && M <= 1024; }
+
 int xinv_blocks(int M, int n0n1) {
+    if (use_xinv4(M)) {
+        int rpb = 1;
+        switch (M) {
+#define X(m) case m: rpb = xinv4_rpb<m>(); break;
+            X(4) X(8) X(16) X(32) X(64) X(128) X(256) X(512) X(1024)
+#undef X
+        }
+        return (n0n1 + rpb - 1) / rpb;
+    }
     int TPL = mmfft::tpl(M);
     int rpb = (3 * TPL >= 384) ? 1 : 384 / (3 * TPL);
     size_t smem = (size_t)rpb * 3 * mmfft::line_len(M) * sizeof(float2);
@@ -554,6 +647,16 @@ int xinv_blocks(int M, int n0n1) {
 
 cudaError_t launch_xinv_epi(int M, const float2* S, int hp, int L1, const float2* tw, const EpiArgs& A, bool terms,
                             cudaStream_t st, int* nblocks) {
+    if (use_xinv4(M)) {
+        switch (M) {
+#define X(m)                                                                      \
+    case m:                                                                       \
+        return terms ? launch_xinv4_t<m, true>(S, hp, L1, tw, A, st, nblocks)     \
+                     : launch_xinv4_t<m, false>(S, hp, L1, tw, A, st, nblocks);
+            X(4) X(8) X(16) X(32) X(64) X(128) X(256) X(512) X(1024)
+#undef X
+        }
+    }
     switch (M) {
 #define X(m)                                                                      \
     case m:                                                                       \
