@@ -364,6 +364,104 @@ __global__ void __launch_bounds__(128) zmul_reg_kernel(float2* __restrict__ S, K
         }
 }
 
+// Four lanes per column (P >= 4): lane s computes the outputs kz = 4k' + s, k' < P/2,
+//   X[4k'+s] = DFT_{P/2}( y )[k'],  y[z'] = sum_{j<2} x[z' + jP/2] W_{2P}^((z' + jP/2) s),
+// and contributes W_{2P}^(-z s) IDFT_{P/2}(H_s)[z mod P/2] to every output plane z; the
+// four contributions are summed by a two-round shuffle reduce-scatter after which lane s
+// owns the planes z with z mod 4 == s.
+template <int P>
+__global__ void __launch_bounds__(128) zmul_reg4_kernel(float2* __restrict__ S, KernelView K, int L1, int h, int hp,
+                                                         long long comp_stride, long long zstride, float scale,
+                                                         const float2* __restrict__ tw, const DevCtl* ctl,
+                                                         int skip_retry) {
+    if (conv_skip(ctl, skip_retry)) return;
+    constexpr int H = P / 2;
+    const long long gt = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const int s = (int)(gt & 3);
+    const long long colg = gt >> 2;
+    const bool active = colg < (long long)L1 * h;
+    const int ky = active ? (int)(colg / h) : 0;
+    const int kx = active ? (int)(colg % h) : 0;
+    float2* base = S + (long long)ky * hp + kx;
+    float2 g[3][H];
+    // forward: fold the P input planes onto P/2 with the lane's twiddles
+#pragma unroll
+    for (int zp = 0; zp < H; zp++) {
+        const float2 w0 = wtab<-1>(tw, zp * s, 2 * P);
+        const float2 w1 = wtab<-1>(tw, (zp + H) * s, 2 * P);
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            const float2 a = active ? base[c * comp_stride + zp * zstride] : make_float2(0.f, 0.f);
+            const float2 b = active ? base[c * comp_stride + (zp + H) * zstride] : make_float2(0.f, 0.f);
+            g[c][zp] = cadd(cmul(a, w0), cmul(b, w1));
+        }
+    }
+#pragma unroll
+    for (int c = 0; c < 3; c++) RDft<H, -1>::run(g[c]);
+    const int kyy = (ky > (K.L1 >> 1)) ? K.L1 - ky : ky;
+    const float sy = (ky > (K.L1 >> 1)) ? -1.f : 1.f;
+    const int cs = K.kd0 * K.kd1 * K.kd2;
+#pragma unroll
+    for (int k = 0; k < H; k++) {
+        int kz = 4 * k + s;
+        float sz = 1.f;
+        if (kz > P) { kz = 2 * P - kz; sz = -1.f; }
+        const int idx = (kz * K.kd1 + kyy) * K.kd2 + kx;
+        const float kxx = __ldg(K.k + idx);
+        const float kyy_ = __ldg(K.k + cs + idx);
+        const float kzz = __ldg(K.k + 2 * cs + idx);
+        const float kyz = K.nz[3] ? sy * __ldg(K.k + 3 * cs + idx) : 0.f;
+        const float kxz = K.nz[4] ? sz * __ldg(K.k + 4 * cs + idx) : 0.f;
+        const float kxy = K.nz[5] ? sz * sy * __ldg(K.k + 5 * cs + idx) : 0.f;
+        const float2 m0 = g[0][k], m1 = g[1][k], m2 = g[2][k];
+        g[0][k] = make_float2(scale * (kxx * m0.x + kxy * m1.x + kxz * m2.x), scale * (kxx * m0.y + kxy * m1.y + kxz * m2.y));
+        g[1][k] = make_float2(scale * (kxy * m0.x + kyy_ * m1.x + kyz * m2.x), scale * (kxy * m0.y + kyy_ * m1.y + kyz * m2.y));
+        g[2][k] = make_float2(scale * (kxz * m0.x + kyz * m1.x + kzz * m2.x), scale * (kxz * m0.y + kyz * m1.y + kzz * m2.y));
+    }
+#pragma unroll
+    for (int c = 0; c < 3; c++) RDft<H, +1>::run(g[c]);
+    // reduce-scatter.  Round A (lane ^ 2): keep the planes with bit 1 of z equal to bit 1
+    // of s; round B (lane ^ 1): keep bit 0 of z equal to bit 0 of s.
+    const int b1 = (s >> 1) & 1, b0 = s & 1;
+    float2 a[3][H];  // a[c][i]: partial sum for plane z = zA(i)
+#pragma unroll
+    for (int i = 0; i < H; i++) {
+        // the i-th plane kept after round A and the one sent: same position with bit 1 toggled
+        // (register indices chosen by select, so that g stays in registers)
+        const int z0 = ((i >> 1) << 2) | (i & 1);  // bit 1 clear
+        const int z1 = z0 | 2;                     // bit 1 set
+        const int zk = b1 ? z1 : z0;
+        const int zs = b1 ? z0 : z1;
+        const float2 wk = wtab<+1>(tw, zk * s, 2 * P);
+        const float2 ws = wtab<+1>(tw, zs * s, 2 * P);
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            const float2 g0 = g[c][z0 & (H - 1)], g1 = g[c][z1 & (H - 1)];
+            const float2 keep = cmul(wk, b1 ? g1 : g0);
+            const float2 send = cmul(ws, b1 ? g0 : g1);
+            float2 recv;
+            recv.x = __shfl_xor_sync(0xffffffffu, send.x, 2);
+            recv.y = __shfl_xor_sync(0xffffffffu, send.y, 2);
+            a[c][i] = cadd(keep, recv);
+        }
+    }
+    // round B: among the kept planes (index i, bit 0 of i = bit 0 of z), keep bit0(z) == b0
+#pragma unroll
+    for (int i2 = 0; i2 < H / 2; i2++) {
+        const int z = (i2 << 2) | (b1 << 1) | b0;
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            const float2 a0 = a[c][2 * i2], a1 = a[c][2 * i2 + 1];
+            const float2 send = b0 ? a0 : a1;
+            float2 recv;
+            recv.x = __shfl_xor_sync(0xffffffffu, send.x, 1);
+            recv.y = __shfl_xor_sync(0xffffffffu, send.y, 1);
+            const float2 v = cadd(b0 ? a1 : a0, recv);
+            if (active) base[c * comp_stride + z * zstride] = v;
+        }
+    }
+}
+
 template <int P>
 static cudaError_t launch_zmul_reg_t(float2* S, const KernelView& K, int L1, int h, int hp, long long comp_stride,
                                      long long zstride, float scale, const float2* tw, const DevCtl* ctl,
@@ -374,6 +472,16 @@ static cudaError_t launch_zmul_reg_t(float2* S, const KernelView& K, int L1, int
     return cudaGetLastError();
 }
 
+template <int P>
+static cudaError_t launch_zmul_reg4_t(float2* S, const KernelView& K, int L1, int h, int hp, long long comp_stride,
+                                      long long zstride, float scale, const float2* tw, const DevCtl* ctl,
+                                      int skip_retry, cudaStream_t st) {
+    const long long threads = 4LL * L1 * h;
+    const int blocks = (int)((threads + 127) / 128);
+    zmul_reg4_kernel<P><<<blocks, 128, 0, st>>>(S, K, L1, h, hp, comp_stride, zstride, scale, tw, ctl, skip_retry);
+    return cudaGetLastError();
+}
+
 // P = N0 = L0/2 (zero-padded z); returns cudaErrorNotSupported for other shapes
 cudaError_t launch_zmul_reg(int P, float2* S, const KernelView& K, int L1, int h, int hp, long long comp_stride,
                             long long zstride, float scale, const float2* tw, const DevCtl* ctl, int skip_retry,
@@ -381,9 +489,9 @@ cudaError_t launch_zmul_reg(int P, float2* S, const KernelView& K, int L1, int h
     switch (P) {
         case 1: return launch_zmul_reg_t<1>(S, K, L1, h, hp, comp_stride, zstride, scale, tw, ctl, skip_retry, st);
         case 2: return launch_zmul_reg_t<2>(S, K, L1, h, hp, comp_stride, zstride, scale, tw, ctl, skip_retry, st);
-        case 4: return launch_zmul_reg_t<4>(S, K, L1, h, hp, comp_stride, zstride, scale, tw, ctl, skip_retry, st);
-        case 8: return launch_zmul_reg_t<8>(S, K, L1, h, hp, comp_stride, zstride, scale, tw, ctl, skip_retry, st);
-        case 16: return launch_zmul_reg_t<16>(S, K, L1, h, hp, comp_stride, zstride, scale, tw, ctl, skip_retry, st);
+        case 4: return launch_zmul_reg4_t<4>(S, K, L1, h, hp, comp_stride, zstride, scale, tw, ctl, skip_retry, st);
+        case 8: return launch_zmul_reg4_t<8>(S, K, L1, h, hp, comp_stride, zstride, scale, tw, ctl, skip_retry, st);
+        case 16: return launch_zmul_reg4_t<16>(S, K, L1, h, hp, comp_stride, zstride, scale, tw, ctl, skip_retry, st);
         default: return cudaErrorNotSupported;
     }
 }
@@ -395,6 +503,18 @@ __host__ __device__ constexpr int col4_tile(int L) {
     if (tc > 32) tc = 32;
     while (tc > 1 && tc * (L / fs_p2(L)) * (fs_p2(L) + 1) * 8 > 48 * 1024) tc /= 2;
     return tc;
+}
+
+// Per-column stride of the exchange buffers: a half-warp holds HW = min(TC, 16) columns
+// and 16/HW consecutive t, so a stride congruent to 16/HW (mod 16) puts every
+// (column, t) pair of a half-warp on its own pair of banks.
+template <int L>
+__host__ __device__ constexpr int col4_stride() {
+    const int hw = col4_tile(L) < 16 ? col4_tile(L) : 16;
+    const int want = (16 / hw) & 15;
+    int s = FS<L>::LBUF;
+    while ((s & 15) != want) s++;
+    return s;
 }
 
 template <int L, int SIGN>
@@ -419,7 +539,7 @@ __global__ void __launch_bounds__(256) colfft4_kernel(float2* __restrict__ S, in
         const int n = F::in_index(t, j);
         v[j] = (active && n < n_in) ? base[n * line_stride] : make_float2(0.f, 0.f);
     }
-    F::template run<SIGN>(v, sm + col * F::LBUF, t, active, tw);
+    F::template run<SIGN>(v, sm + col * col4_stride<L>(), t, active, tw, TC);
 #pragma unroll
     for (int r = 0; r < F::P1; r++) {
         const int n = F::out_index(t, r);
@@ -470,7 +590,7 @@ __global__ void __launch_bounds__(256) xfwd4_kernel(const float* __restrict__ in
         }
         v[j] = make_float2(a, b);
     }
-    F::template run<-1>(v, buf, t, active, tw);
+    F::template run<-1>(v, buf, t, active, tw, 1);
     if (active) {
 #pragma unroll
         for (int r = 0; r < F::P1; r++) buf[F::out_index(t, r)] = v[r];
@@ -573,7 +693,7 @@ static cudaError_t launch_colfft4_t(float2* S, int ncols, int nouter, long long 
                                     cudaStream_t st) {
     using F = FS<L>;
     constexpr int TC = col4_tile(L);
-    const size_t smem = (size_t)TC * F::LBUF * sizeof(float2);
+    const size_t smem = (size_t)TC * col4_stride<L>() * sizeof(float2);
     cudaError_t e = set_smem(colfft4_kernel<L, SIGN>, smem);
     if (e != cudaSuccess) return e;
     const int ntiles = (ncols + TC - 1) / TC;

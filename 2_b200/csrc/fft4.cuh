@@ -95,7 +95,7 @@ struct FS {
     // the block must call it (it synchronises twice); `active` masks the buffer traffic.
     template <int SIGN>
     static __device__ __forceinline__ void run(float2 (&v)[P1], float2* buf, int t, bool active,
-                                               const float2* __restrict__ tw) {
+                                               const float2* __restrict__ tw, int pair_mask = 1) {
         if (active) {
             RDft<P1, SIGN>::run(v);
 #pragma unroll
@@ -115,6 +115,51 @@ struct FS {
 #pragma unroll
                 for (int k2 = 0; k2 < P2; k2++) v[q * P2 + k2] = u[k2];
             }
+        }
+        __syncthreads();
+    }
+};
+
+// L = 512 = 16 x 32: 32 threads per line, 16 elements each (half the registers of a
+// 32 x 16 split).  The length-32 second stage of column k1 is shared by the thread pair
+// (2 k1, 2 k1 + 1): each does a length-16 DFT of the even or odd t, and the halves are
+// combined with one shuffle, X[k1 + 16 k2] = D0[k2 mod 16] +- W_32^(k2 mod 16) D1[k2 mod 16].
+// `pair_mask` is the lane distance between threads t and t^1.
+template <>
+struct FS<512> {
+    static constexpr int P2 = 32;
+    static constexpr int P1 = 16;
+    static constexpr int PITCH = 34;  // = 2 (mod 16): the pair-strided reads hit distinct banks
+    static constexpr int LBUF = P1 * PITCH;
+
+    static __device__ __forceinline__ int in_index(int t, int j) { return t + 32 * j; }
+    static __device__ __forceinline__ int out_index(int t, int r) { return (t >> 1) + 16 * (r + 16 * (t & 1)); }
+
+    template <int SIGN>
+    static __device__ __forceinline__ void run(float2 (&v)[16], float2* buf, int t, bool active,
+                                               const float2* __restrict__ tw, int pair_mask) {
+        if (active) {
+            RDft<16, SIGN>::run(v);
+#pragma unroll
+            for (int k1 = 1; k1 < 16; k1++) v[k1] = cmul(v[k1], TwSrc<SIGN, float2>::get(tw, t * k1, 512));
+#pragma unroll
+            for (int k1 = 0; k1 < 16; k1++) buf[k1 * PITCH + t] = v[k1];
+        }
+        __syncthreads();
+        const int h = t & 1;
+        if (active) {
+            const int k1 = t >> 1;
+#pragma unroll
+            for (int u = 0; u < 16; u++) v[u] = buf[k1 * PITCH + 2 * u + h];
+            RDft<16, SIGN>::run(v);
+        }
+#pragma unroll
+        for (int k = 0; k < 16; k++) {
+            float2 o;
+            o.x = __shfl_xor_sync(0xffffffffu, v[k].x, pair_mask);
+            o.y = __shfl_xor_sync(0xffffffffu, v[k].y, pair_mask);
+            const float2 w = w32<SIGN>(k);
+            v[k] = h == 0 ? cadd(v[k], cmul(w, o)) : csub(o, cmul(w, v[k]));
         }
         __syncthreads();
     }

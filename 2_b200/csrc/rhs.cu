@@ -551,7 +551,7 @@ __global__ void __launch_bounds__(384) xinv4_epi_kernel(const float2* __restrict
             v[j] = val;
         }
     }
-    F::template run<+1>(v, buf, t, active, tw);
+    F::template run<+1>(v, buf, t, active, tw, 1);
     if (active) {
 #pragma unroll
         for (int r = 0; r < F::P1; r++) buf[F::out_index(t, r)] = v[r];
