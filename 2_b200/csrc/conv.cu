@@ -533,13 +533,16 @@ __global__ void __launch_bounds__(256) colfft4_kernel(float2* __restrict__ S, in
     const int kx0 = (blockIdx.x % ntiles) * TC;
     const bool active = (t < F::P2) && (kx0 + col < ncols);
     float2* base = S + (long long)o * outer_stride + kx0 + col;
+    float2* twt = sm + TC * col4_stride<L>();
+    F::fill_twiddles(twt, tw);
     float2 v[F::P1];
 #pragma unroll
     for (int j = 0; j < F::P1; j++) {
         const int n = F::in_index(t, j);
         v[j] = (active && n < n_in) ? base[n * line_stride] : make_float2(0.f, 0.f);
     }
-    F::template run<SIGN>(v, sm + col * col4_stride<L>(), t, active, tw, TC);
+    __syncthreads();
+    F::template run<SIGN>(v, sm + col * col4_stride<L>(), t, active, twt, TC);
 #pragma unroll
     for (int r = 0; r < F::P1; r++) {
         const int n = F::out_index(t, r);
@@ -564,6 +567,8 @@ __global__ void __launch_bounds__(256) xfwd4_kernel(const float* __restrict__ in
     const int row = blockIdx.x * RPB + lr;
     const bool active = (lr < RPB) && (row < nrows);
     float2* buf = sm + (lr < RPB ? lr : 0) * F::LBUF;
+    float2* twt = sm + RPB * F::LBUF;
+    F::fill_twiddles(twt, tw);
     float2 v[F::P1];
     const float* src = in + (long long)(active ? row : 0) * in_pitch;
     const int zy = (active ? row : 0) % (Z * Y);
@@ -590,7 +595,8 @@ __global__ void __launch_bounds__(256) xfwd4_kernel(const float* __restrict__ in
         }
         v[j] = make_float2(a, b);
     }
-    F::template run<-1>(v, buf, t, active, tw, 1);
+    __syncthreads();
+    F::template run<-1>(v, buf, t, active, twt, 1);
     if (active) {
 #pragma unroll
         for (int r = 0; r < F::P1; r++) buf[F::out_index(t, r)] = v[r];
@@ -642,7 +648,7 @@ static cudaError_t launch_xfwd4_t(const float* in, PP pp, const float* mask, flo
                                   int skip_retry, cudaStream_t st) {
     using F = FS<M>;
     constexpr int RPB = (256 / F::P2) > 0 ? 256 / F::P2 : 1;
-    const size_t smem = (size_t)RPB * F::LBUF * sizeof(float2);
+    const size_t smem = (size_t)(RPB * F::LBUF + F::TWT) * sizeof(float2);
     cudaError_t e = set_smem(xfwd4_kernel<M>, smem);
     if (e != cudaSuccess) return e;
     const int blocks = (nrows + RPB - 1) / RPB;
@@ -693,7 +699,7 @@ static cudaError_t launch_colfft4_t(float2* S, int ncols, int nouter, long long 
                                     cudaStream_t st) {
     using F = FS<L>;
     constexpr int TC = col4_tile(L);
-    const size_t smem = (size_t)TC * col4_stride<L>() * sizeof(float2);
+    const size_t smem = (size_t)(TC * col4_stride<L>() + F::TWT) * sizeof(float2);
     cudaError_t e = set_smem(colfft4_kernel<L, SIGN>, smem);
     if (e != cudaSuccess) return e;
     const int ntiles = (ncols + TC - 1) / TC;

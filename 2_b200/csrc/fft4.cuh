@@ -93,13 +93,26 @@ struct FS {
 
     // Transforms the line held by the P2 threads (t = 0..P2-1) of this line.  All threads of
     // the block must call it (it synchronises twice); `active` masks the buffer traffic.
+    // Shared-memory table of the step-1 twiddles, twt[k1 * P2 + t] = W_L^(t k1) (forward
+    // sign), filled cooperatively by the block; L entries.
+    static constexpr int TWT = P1 * P2;
+    static __device__ __forceinline__ void fill_twiddles(float2* twt, const float2* __restrict__ tw) {
+        for (int e = threadIdx.x; e < TWT; e += blockDim.x) {
+            const int k1 = e / P2, t = e % P2;
+            twt[e] = TwSrc<-1, float2>::get(tw, (t * k1) & (L - 1), L);
+        }
+    }
+
     template <int SIGN>
     static __device__ __forceinline__ void run(float2 (&v)[P1], float2* buf, int t, bool active,
-                                               const float2* __restrict__ tw, int pair_mask = 1) {
+                                               const float2* twt, int pair_mask = 1) {
         if (active) {
             RDft<P1, SIGN>::run(v);
 #pragma unroll
-            for (int k1 = 1; k1 < P1; k1++) v[k1] = cmul(v[k1], TwSrc<SIGN, float2>::get(tw, t * k1, L));
+            for (int k1 = 1; k1 < P1; k1++) {
+                const float2 w = twt[k1 * P2 + t];
+                v[k1] = cmul(v[k1], SIGN > 0 ? make_float2(w.x, -w.y) : w);
+            }
 #pragma unroll
             for (int k1 = 0; k1 < P1; k1++) buf[k1 * PITCH + t] = v[k1];
         }
@@ -135,13 +148,24 @@ struct FS<512> {
     static __device__ __forceinline__ int in_index(int t, int j) { return t + 32 * j; }
     static __device__ __forceinline__ int out_index(int t, int r) { return (t >> 1) + 16 * (r + 16 * (t & 1)); }
 
+    static constexpr int TWT = P1 * P2;
+    static __device__ __forceinline__ void fill_twiddles(float2* twt, const float2* __restrict__ tw) {
+        for (int e = threadIdx.x; e < TWT; e += blockDim.x) {
+            const int k1 = e / P2, t = e % P2;
+            twt[e] = TwSrc<-1, float2>::get(tw, t * k1, 512);
+        }
+    }
+
     template <int SIGN>
     static __device__ __forceinline__ void run(float2 (&v)[16], float2* buf, int t, bool active,
-                                               const float2* __restrict__ tw, int pair_mask) {
+                                               const float2* twt, int pair_mask) {
         if (active) {
             RDft<16, SIGN>::run(v);
 #pragma unroll
-            for (int k1 = 1; k1 < 16; k1++) v[k1] = cmul(v[k1], TwSrc<SIGN, float2>::get(tw, t * k1, 512));
+            for (int k1 = 1; k1 < 16; k1++) {
+                const float2 w = twt[k1 * P2 + t];
+                v[k1] = cmul(v[k1], SIGN > 0 ? make_float2(w.x, -w.y) : w);
+            }
 #pragma unroll
             for (int k1 = 0; k1 < 16; k1++) buf[k1 * PITCH + t] = v[k1];
         }

@@ -532,6 +532,8 @@ __global__ void __launch_bounds__(384) xinv4_epi_kernel(const float2* __restrict
     const int row = blockIdx.x * RPB + lr;
     const bool active = (lr < RPB) && (row < nrows);
     float2* buf = sm + (lr < RPB ? lr * 3 + c : 0) * F::LBUF;
+    float2* twt = sm + RPB * 3 * F::LBUF;
+    F::fill_twiddles(twt, tw);
     float2 v[F::P1];
     {
         const int rr = active ? row : 0;
@@ -551,7 +553,8 @@ __global__ void __launch_bounds__(384) xinv4_epi_kernel(const float2* __restrict
             v[j] = val;
         }
     }
-    F::template run<+1>(v, buf, t, active, tw, 1);
+    __syncthreads();
+    F::template run<+1>(v, buf, t, active, twt, 1);
     if (active) {
 #pragma unroll
         for (int r = 0; r < F::P1; r++) buf[F::out_index(t, r)] = v[r];
@@ -611,7 +614,7 @@ template <int M, bool TERMS>
 static cudaError_t launch_xinv4_t(const float2* S, int hp, int L1, const float2* tw, const EpiArgs& A,
                                   cudaStream_t st, int* nblocks) {
     constexpr int RPB = xinv4_rpb<M>();
-    const size_t smem = (size_t)RPB * 3 * FS<M>::LBUF * sizeof(float2);
+    const size_t smem = (size_t)(RPB * 3 * FS<M>::LBUF + FS<M>::TWT) * sizeof(float2);
     if (smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(xinv4_epi_kernel<M, TERMS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)smem);
