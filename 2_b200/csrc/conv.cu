@@ -383,12 +383,16 @@ __global__ void __launch_bounds__(128) zmul_reg4_kernel(float2* __restrict__ S, 
     const int ky = active ? (int)(colg / h) : 0;
     const int kx = active ? (int)(colg % h) : 0;
     float2* base = S + (long long)ky * hp + kx;
+    // W_{2P}^m, m < 2P, in shared memory (the lane-dependent twiddles below)
+    __shared__ float2 wz[2 * P];
+    for (int m = threadIdx.x; m < 2 * P; m += blockDim.x) wz[m] = wtab<-1>(tw, m, 2 * P);
+    __syncthreads();
     float2 g[3][H];
     // forward: fold the P input planes onto P/2 with the lane's twiddles
 #pragma unroll
     for (int zp = 0; zp < H; zp++) {
-        const float2 w0 = wtab<-1>(tw, zp * s, 2 * P);
-        const float2 w1 = wtab<-1>(tw, (zp + H) * s, 2 * P);
+        const float2 w0 = wz[(zp * s) & (2 * P - 1)];
+        const float2 w1 = wz[((zp + H) * s) & (2 * P - 1)];
 #pragma unroll
         for (int c = 0; c < 3; c++) {
             const float2 a = active ? base[c * comp_stride + zp * zstride] : make_float2(0.f, 0.f);
@@ -432,8 +436,8 @@ __global__ void __launch_bounds__(128) zmul_reg4_kernel(float2* __restrict__ S, 
         const int z1 = z0 | 2;                     // bit 1 set
         const int zk = b1 ? z1 : z0;
         const int zs = b1 ? z0 : z1;
-        const float2 wk = wtab<+1>(tw, zk * s, 2 * P);
-        const float2 ws = wtab<+1>(tw, zs * s, 2 * P);
+        const float2 wkf = wz[(zk * s) & (2 * P - 1)], wsf = wz[(zs * s) & (2 * P - 1)];
+        const float2 wk = make_float2(wkf.x, -wkf.y), ws = make_float2(wsf.x, -wsf.y);
 #pragma unroll
         for (int c = 0; c < 3; c++) {
             const float2 g0 = g[c][z0 & (H - 1)], g1 = g[c][z1 & (H - 1)];
