@@ -454,10 +454,13 @@ __device__ __forceinline__ void epilogue_rows(const EpiArgs& A, const float2* sm
     resolve_op(A.op, cur, h, r);
     const float* m = A.op.m_in.get(cur);
     ThreadRed tr = {0.f, 0.f, 0, {{0.f, 0.f}, {0.f, 0.f}, {0.f, 0.f}, {0.f, 0.f}}};
-    for (int e = threadIdx.x; e < nrow_here * n2; e += blockDim.x) {
-        const int lrow = e / n2, x = e % n2;
-        const int grow = row0 + lrow;
-        const int z = grow / n1, y = grow % n1;
+    // (lrow, x) of element e = threadIdx.x + k*blockDim.x, advanced without divisions
+    const int total = nrow_here * n2;
+    int lrow = threadIdx.x / n2, x = threadIdx.x - lrow * n2;
+    const int dr = blockDim.x / n2, dx = blockDim.x - dr * n2;
+    int grow = row0 + lrow;
+    int z = grow / n1, y = grow - z * n1;
+    for (int e = threadIdx.x; e < total; e += blockDim.x) {
         const long long i = (long long)grow * n2 + x;
         const int pi = PADDED ? padx(x >> 1) : (x >> 1);
         const float2 v0 = sm[(lrow * 3 + 0) * LS + pi];
@@ -465,6 +468,14 @@ __device__ __forceinline__ void epilogue_rows(const EpiArgs& A, const float2* sm
         const float2 v2 = sm[(lrow * 3 + 2) * LS + pi];
         const float3 hd = (x & 1) ? make_float3(v0.y, v1.y, v2.y) : make_float3(v0.x, v1.x, v2.x);
         process_cell<TERMS>(A, m, r, i, z, y, x, hd, ns, dtth, tr);
+        // advance by blockDim.x cells
+        x += dx;
+        int adv = dr;
+        if (x >= n2) { x -= n2; adv++; }
+        lrow += adv;
+        grow += adv;
+        y += adv;
+        while (y >= n1) { y -= n1; z++; }
     }
     block_reduce_publish(tr, A.op, A.ctl, A.tq_out, A.red);
 }
