@@ -177,6 +177,24 @@ def reference_arm(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------- replicas
+def aggregate(ms_local, cells, steps, world, dist=None, device=None):
+    """Whole-job throughput of `world` independent replicas: the slowest rank's device
+    time (max over ranks) bounds the job; every rank advanced `cells` by `steps`."""
+    ms = ms_local
+    if dist is not None and world > 1:
+        import torch
+        t = torch.tensor([ms_local], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    return ms, cells * steps * world / (ms / 1e3)
+
+
+def replica_seed(rank):
+    """Each replica integrates its own random initial state."""
+    return 1000 + rank
+
+
 # ---------------------------------------------------------------- main
 def main():
     ap = argparse.ArgumentParser()
@@ -212,7 +230,7 @@ def main():
     N = n[0] * n[1] * n[2]
     plan = Plan(problem(), device=local_rank)
     plan.solver(w["solver"], dt=w["dt0"], maxerr=w["maxerr"])
-    plan.set_state(initial_m(1000 + rank))
+    plan.set_state(initial_m(replica_seed(rank)))
     if args.profile_only:
         geo = plan.geometry()
         pass_ms = plan.profile_eval(args.profile_reps)
@@ -245,12 +263,7 @@ def main():
     st1 = plan.stats()
     attempts = st1["attempts"] - st0["attempts"]
     evals = st1["evals"] - st0["evals"]
-    ms_max = ms
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_max = float(t.item())
-    value = N * args.steps * world / (ms_max / 1e3)
+    ms_max, value = aggregate(ms, N, args.steps, world, dist, "cuda")
 
     # per-pass timing of one evaluation (CUDA events on the launching stream)
     geo = plan.geometry()
@@ -293,12 +306,7 @@ def main():
         nat.check(L.mm_get_state(plan.h, C.c_void_p(host_out.data_ptr()), 1, None))
     f1.record()
     torch.cuda.synchronize()
-    e2e_ms = f0.elapsed_time(f1)
-    if dist:
-        t = torch.tensor([e2e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e_value = N * e2e_steps * world / (e2e_ms / 1e3)
+    e2e_ms, e2e_value = aggregate(f0.elapsed_time(f1), N, e2e_steps, world, dist, "cuda")
 
     cb = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
