@@ -87,6 +87,19 @@ def step_bytes_rk23(geo, n):
     return combine0 + e1 + e2 + e3
 
 
+def read_traffic():
+    """Per-pass DRAM bytes of one launch (ncu dram__bytes_read.sum + dram__bytes_write.sum),
+    from the committed capture summary of this workload, if there is one."""
+    path = os.path.join(ROOT, "profiles", "traffic_film3d_256x256x16.txt")
+    out = {}
+    if os.path.exists(path):
+        for ln in open(path):
+            f = ln.split("#")[0].split()
+            if len(f) == 2:
+                out[f[0]] = int(f[1])
+    return out
+
+
 # ---------------------------------------------------------------- clocks
 class ClockSampler:
     def __init__(self, gpu_index):
@@ -278,11 +291,7 @@ def main():
     else:
         peak, peak_src = 6650.0, "fallback"
     achieved = pb[dom][1] / (pass_ms[dom] * 1e-3) / 1e9
-    traffic = None
-    tpath = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tpath):
-        tr = json.load(open(tpath))
-        traffic = tr.get(pb[dom][0])
+    traffic = read_traffic().get(pb[dom][0])
     step_b = step_bytes_rk23(geo, n) * attempts / max(1, args.steps)
     step_gbs = step_b * args.steps / (ms / 1e3) / 1e9
 
