@@ -31,7 +31,7 @@ __device__ __forceinline__ bool conv_skip(const DevCtl* ctl, int skip_retry) {
 }
 
 // ---------------------------------------------------------------- R2C row pass
-// rows: r = (c*Z + z)*Y + y over C components; input row r starts at in + r*in_pitch
+// rows (per simulation): r = (c*Z + z)*Y + y over C components; input row r starts at in + r*in_pitch
 // (reals, n_in of them; the rest of the length-2M row is zero);
 // output row (c, z, y) goes to out + ((c*Z + z)*Yout + y)*hp (h = M+1 complex).
 // mask (optional): input multiplied by mask[(z*Y + y)*in_pitch + x] (same for all c).
@@ -39,9 +39,14 @@ template <int M, typename V, typename S>
 __global__ void __launch_bounds__(256) xfwd_kernel(const S* __restrict__ in_fixed, PP in_pp, const float* __restrict__ mask,
                                                    V* __restrict__ out, int nrows, int Z, int Y, int Yout,
                                                    int in_pitch, int n_in, int hp, const float2* __restrict__ tw,
-                                                   const DevCtl* ctl, int skip_retry) {
+                                                   const DevCtl* ctl, int skip_retry, long long in_bstride,
+                                                   long long out_bstride, long long mask_bstride) {
+    const int sim = blockIdx.y;
+    if (ctl) ctl += sim;
     if (conv_skip(ctl, skip_retry)) return;
-    const S* in = in_fixed ? in_fixed : reinterpret_cast<const S*>(in_pp.get(ctl ? ctl->cur : 0));
+    const S* in = (in_fixed ? in_fixed : reinterpret_cast<const S*>(in_pp.get(ctl ? ctl->cur : 0))) + sim * in_bstride;
+    out += sim * out_bstride;
+    if (mask) mask += sim * mask_bstride;
     constexpr int TPL = tpl(M);
     constexpr int LL = line_len(M);
     constexpr int RPB = TPL >= 256 ? 1 : 256 / TPL;
@@ -190,8 +195,11 @@ __device__ __forceinline__ void tile_store(const V* sm, V* __restrict__ base, lo
 // Reads elements e < n_in (rest zero), writes elements e < n_out.
 template <int L, int SIGN, typename V>
 __global__ void colfft_kernel(V* __restrict__ S, int ncols, long long outer_stride, long long line_stride, int n_in,
-                              int n_out, const float2* __restrict__ tw, const DevCtl* ctl, int skip_retry) {
+                              int n_out, const float2* __restrict__ tw, const DevCtl* ctl, int skip_retry,
+                              long long sim_stride) {
+    if (ctl) ctl += blockIdx.y;
     if (conv_skip(ctl, skip_retry)) return;
+    S += blockIdx.y * sim_stride;
     constexpr int TC = col_tile(L, 1, sizeof(V));
     constexpr int TPL = tpl(L);
     constexpr int LL = line_len(L);
@@ -230,8 +238,12 @@ __device__ __forceinline__ void kernel_at(const KernelView& K, int kz, int ky, i
 template <int L>
 __global__ void colmul_kernel(float2* __restrict__ S, KernelView K, int ncols, long long comp_stride,
                               long long outer_stride, long long line_stride, int n_in, int kaxis, float scale,
-                              const float2* __restrict__ tw, const DevCtl* ctl, int skip_retry) {
+                              const float2* __restrict__ tw, const DevCtl* ctl, int skip_retry, long long sim_stride,
+                              const float* __restrict__ sim_scale) {
+    if (ctl) ctl += blockIdx.y;
     if (conv_skip(ctl, skip_retry)) return;
+    S += blockIdx.y * sim_stride;
+    if (sim_scale) scale = sim_scale[blockIdx.y];
     constexpr int TC = col_tile(L, 3, 8);
     constexpr int TPL = tpl(L);
     constexpr int LL = line_len(L);
@@ -294,8 +306,12 @@ template <int P>
 __global__ void __launch_bounds__(128) zmul_reg_kernel(float2* __restrict__ S, KernelView K, int L1, int h, int hp,
                                                        long long comp_stride, long long zstride, float scale,
                                                        const float2* __restrict__ tw, const DevCtl* ctl,
-                                                       int skip_retry) {
+                                                       int skip_retry, long long sim_stride,
+                                                       const float* __restrict__ sim_scale) {
+    if (ctl) ctl += blockIdx.y;
     if (conv_skip(ctl, skip_retry)) return;
+    S += blockIdx.y * sim_stride;
+    if (sim_scale) scale = sim_scale[blockIdx.y];
     const long long gt = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     const int s = (int)(gt & 1);
     const long long colg = gt >> 1;
@@ -373,8 +389,12 @@ template <int P>
 __global__ void __launch_bounds__(128) zmul_reg4_kernel(float2* __restrict__ S, KernelView K, int L1, int h, int hp,
                                                          long long comp_stride, long long zstride, float scale,
                                                          const float2* __restrict__ tw, const DevCtl* ctl,
-                                                         int skip_retry) {
+                                                         int skip_retry, long long sim_stride,
+                                                         const float* __restrict__ sim_scale) {
+    if (ctl) ctl += blockIdx.y;
     if (conv_skip(ctl, skip_retry)) return;
+    S += blockIdx.y * sim_stride;
+    if (sim_scale) scale = sim_scale[blockIdx.y];
     constexpr int H = P / 2;
     const long long gt = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     const int s = (int)(gt & 3);
@@ -469,33 +489,36 @@ __global__ void __launch_bounds__(128) zmul_reg4_kernel(float2* __restrict__ S, 
 template <int P>
 static cudaError_t launch_zmul_reg_t(float2* S, const KernelView& K, int L1, int h, int hp, long long comp_stride,
                                      long long zstride, float scale, const float2* tw, const DevCtl* ctl,
-                                     int skip_retry, cudaStream_t st) {
+                                     int skip_retry, cudaStream_t st, int nsim, long long sim_stride,
+                                     const float* sim_scale) {
     const long long threads = 2LL * L1 * h;
-    const int blocks = (int)((threads + 127) / 128);
-    zmul_reg_kernel<P><<<blocks, 128, 0, st>>>(S, K, L1, h, hp, comp_stride, zstride, scale, tw, ctl, skip_retry);
+    const dim3 grid((unsigned)((threads + 127) / 128), (unsigned)nsim);
+    zmul_reg_kernel<P><<<grid, 128, 0, st>>>(S, K, L1, h, hp, comp_stride, zstride, scale, tw, ctl, skip_retry,
+                                             sim_stride, sim_scale);
     return cudaGetLastError();
 }
 
 template <int P>
 static cudaError_t launch_zmul_reg4_t(float2* S, const KernelView& K, int L1, int h, int hp, long long comp_stride,
                                       long long zstride, float scale, const float2* tw, const DevCtl* ctl,
-                                      int skip_retry, cudaStream_t st) {
+                                      int skip_retry, cudaStream_t st, int nsim, long long sim_stride,
+                                      const float* sim_scale) {
     const long long threads = 4LL * L1 * h;
-    const int blocks = (int)((threads + 127) / 128);
-    zmul_reg4_kernel<P><<<blocks, 128, 0, st>>>(S, K, L1, h, hp, comp_stride, zstride, scale, tw, ctl, skip_retry);
+    const dim3 grid((unsigned)((threads + 127) / 128), (unsigned)nsim);
+    zmul_reg4_kernel<P><<<grid, 128, 0, st>>>(S, K, L1, h, hp, comp_stride, zstride, scale, tw, ctl, skip_retry,
+                                              sim_stride, sim_scale);
     return cudaGetLastError();
 }
 
 // P = N0 = L0/2 (zero-padded z); returns cudaErrorNotSupported for other shapes
 cudaError_t launch_zmul_reg(int P, float2* S, const KernelView& K, int L1, int h, int hp, long long comp_stride,
                             long long zstride, float scale, const float2* tw, const DevCtl* ctl, int skip_retry,
-                            cudaStream_t st) {
+                            cudaStream_t st, int nsim, long long sim_stride, const float* sim_scale) {
     switch (P) {
-        case 1: return launch_zmul_reg_t<1>(S, K, L1, h, hp, comp_stride, zstride, scale, tw, ctl, skip_retry, st);
-        case 2: return launch_zmul_reg_t<2>(S, K, L1, h, hp, comp_stride, zstride, scale, tw, ctl, skip_retry, st);
-        case 4: return launch_zmul_reg4_t<4>(S, K, L1, h, hp, comp_stride, zstride, scale, tw, ctl, skip_retry, st);
-        case 8: return launch_zmul_reg4_t<8>(S, K, L1, h, hp, comp_stride, zstride, scale, tw, ctl, skip_retry, st);
-        case 16: return launch_zmul_reg4_t<16>(S, K, L1, h, hp, comp_stride, zstride, scale, tw, ctl, skip_retry, st);
+#define X(p, f) case p: return f<p>(S, K, L1, h, hp, comp_stride, zstride, scale, tw, ctl, skip_retry, st, nsim, sim_stride, sim_scale);
+        X(1, launch_zmul_reg_t) X(2, launch_zmul_reg_t) X(4, launch_zmul_reg4_t) X(8, launch_zmul_reg4_t)
+        X(16, launch_zmul_reg4_t)
+#undef X
         default: return cudaErrorNotSupported;
     }
 }
@@ -525,8 +548,10 @@ template <int L, int SIGN>
 __global__ void __launch_bounds__(256) colfft4_kernel(float2* __restrict__ S, int ncols, long long outer_stride,
                                                       long long line_stride, int n_in, int n_out,
                                                       const float2* __restrict__ tw, const DevCtl* ctl,
-                                                      int skip_retry) {
+                                                      int skip_retry, long long sim_stride) {
+    if (ctl) ctl += blockIdx.y;
     if (conv_skip(ctl, skip_retry)) return;
+    S += blockIdx.y * sim_stride;
     using F = FS<L>;
     constexpr int TC = col4_tile(L);
     extern __shared__ unsigned char smem_raw[];
@@ -560,11 +585,17 @@ template <int M>
 __global__ void __launch_bounds__(256) xfwd4_kernel(const float* __restrict__ in_fixed, PP in_pp,
                                                     const float* __restrict__ mask, float2* __restrict__ out,
                                                     int nrows, int Z, int Y, int Yout, int in_pitch, int n_in, int hp,
-                                                    const float2* __restrict__ tw, const DevCtl* ctl, int skip_retry) {
+                                                    const float2* __restrict__ tw, const DevCtl* ctl, int skip_retry,
+                                                    long long in_bstride, long long out_bstride,
+                                                    long long mask_bstride) {
+    const int sim = blockIdx.y;
+    if (ctl) ctl += sim;
     if (conv_skip(ctl, skip_retry)) return;
     using F = FS<M>;
     constexpr int RPB = (256 / F::P2) > 0 ? 256 / F::P2 : 1;
-    const float* in = in_fixed ? in_fixed : in_pp.get(ctl ? ctl->cur : 0);
+    const float* in = (in_fixed ? in_fixed : in_pp.get(ctl ? ctl->cur : 0)) + sim * in_bstride;
+    out += sim * out_bstride;
+    if (mask) mask += sim * mask_bstride;
     extern __shared__ unsigned char smem_raw[];
     float2* sm = reinterpret_cast<float2*>(smem_raw);
     const int t = threadIdx.x % F::P2, lr = threadIdx.x / F::P2;
@@ -630,51 +661,54 @@ template <typename KT> static cudaError_t set_smem(KT kern, size_t bytes) {
 
 #define MM_FOR_POW2(X) X(1) X(2) X(4) X(8) X(16) X(32) X(64) X(128) X(256) X(512) X(1024) X(2048) X(4096)
 
+#define XFWD_SIM_ARGS int nsim, long long in_bstride, long long out_bstride, long long mask_bstride
+#define XFWD_SIM_PASS nsim, in_bstride, out_bstride, mask_bstride
+
 template <int M, typename V, typename S>
 static cudaError_t launch_xfwd_t(const S* in, PP pp, const float* mask, V* out, int nrows, int Z, int Y, int Yout,
                                  int in_pitch, int n_in, int hp, const float2* tw, const DevCtl* ctl, int skip_retry,
-                                 cudaStream_t st) {
+                                 cudaStream_t st, XFWD_SIM_ARGS) {
     constexpr int TPL = tpl(M);
     constexpr int RPB = TPL >= 256 ? 1 : 256 / TPL;
     const size_t smem = (size_t)RPB * line_len(M) * sizeof(V);
     cudaError_t e = set_smem(xfwd_kernel<M, V, S>, smem);
     if (e != cudaSuccess) return e;
-    int blocks = (nrows + RPB - 1) / RPB;
+    const dim3 grid((unsigned)((nrows + RPB - 1) / RPB), (unsigned)nsim);
     int threads = RPB * TPL < 32 ? 32 : RPB * TPL;
-    xfwd_kernel<M, V, S><<<blocks, threads, smem, st>>>(in, pp, mask, out, nrows, Z, Y, Yout, in_pitch, n_in, hp,
-                                                        tw, ctl, skip_retry);
+    xfwd_kernel<M, V, S><<<grid, threads, smem, st>>>(in, pp, mask, out, nrows, Z, Y, Yout, in_pitch, n_in, hp,
+                                                      tw, ctl, skip_retry, in_bstride, out_bstride, mask_bstride);
     return cudaGetLastError();
 }
 
 template <int M>
 static cudaError_t launch_xfwd4_t(const float* in, PP pp, const float* mask, float2* out, int nrows, int Z, int Y,
                                   int Yout, int in_pitch, int n_in, int hp, const float2* tw, const DevCtl* ctl,
-                                  int skip_retry, cudaStream_t st) {
+                                  int skip_retry, cudaStream_t st, XFWD_SIM_ARGS) {
     using F = FS<M>;
     constexpr int RPB = (256 / F::P2) > 0 ? 256 / F::P2 : 1;
     const size_t smem = (size_t)(RPB * F::LBUF + F::TWT) * sizeof(float2);
     cudaError_t e = set_smem(xfwd4_kernel<M>, smem);
     if (e != cudaSuccess) return e;
-    const int blocks = (nrows + RPB - 1) / RPB;
-    xfwd4_kernel<M><<<blocks, RPB * F::P2, smem, st>>>(in, pp, mask, out, nrows, Z, Y, Yout, in_pitch, n_in, hp, tw,
-                                                        ctl, skip_retry);
+    const dim3 grid((unsigned)((nrows + RPB - 1) / RPB), (unsigned)nsim);
+    xfwd4_kernel<M><<<grid, RPB * F::P2, smem, st>>>(in, pp, mask, out, nrows, Z, Y, Yout, in_pitch, n_in, hp, tw,
+                                                      ctl, skip_retry, in_bstride, out_bstride, mask_bstride);
     return cudaGetLastError();
 }
 
 template <typename V, typename S>
 cudaError_t launch_xfwd(int M, const S* in, PP pp, const float* mask, V* out, int nrows, int Z, int Y, int Yout,
                         int in_pitch, int n_in, int hp, const float2* tw, const DevCtl* ctl, int skip_retry,
-                        cudaStream_t st) {
+                        cudaStream_t st, XFWD_SIM_ARGS) {
     if constexpr (sizeof(V) == 8) {
         switch (M) {
-#define X(m) case m: return launch_xfwd4_t<m>(in, pp, mask, out, nrows, Z, Y, Yout, in_pitch, n_in, hp, tw, ctl, skip_retry, st);
+#define X(m) case m: return launch_xfwd4_t<m>(in, pp, mask, out, nrows, Z, Y, Yout, in_pitch, n_in, hp, tw, ctl, skip_retry, st, XFWD_SIM_PASS);
             X(4) X(8) X(16) X(32) X(64) X(128) X(256) X(512) X(1024)
 #undef X
             default: break;
         }
     }
     switch (M) {
-#define X(m) case m: return launch_xfwd_t<m, V, S>(in, pp, mask, out, nrows, Z, Y, Yout, in_pitch, n_in, hp, tw, ctl, skip_retry, st);
+#define X(m) case m: return launch_xfwd_t<m, V, S>(in, pp, mask, out, nrows, Z, Y, Yout, in_pitch, n_in, hp, tw, ctl, skip_retry, st, XFWD_SIM_PASS);
         MM_FOR_POW2(X)
 #undef X
         default: return cudaErrorInvalidValue;
@@ -684,7 +718,7 @@ cudaError_t launch_xfwd(int M, const S* in, PP pp, const float* mask, V* out, in
 template <int L, int SIGN, typename V>
 static cudaError_t launch_colfft_t(V* S, int ncols, int nouter, long long outer_stride, long long line_stride,
                                    int n_in, int n_out, const float2* tw, const DevCtl* ctl, int skip_retry,
-                                   cudaStream_t st) {
+                                   cudaStream_t st, int nsim, long long sim_stride) {
     constexpr int TC = col_tile(L, 1, sizeof(V));
     const size_t smem = (size_t)TC * line_len(L) * sizeof(V);
     cudaError_t e = set_smem(colfft_kernel<L, SIGN, V>, smem);
@@ -692,15 +726,15 @@ static cudaError_t launch_colfft_t(V* S, int ncols, int nouter, long long outer_
     int ntiles = (ncols + TC - 1) / TC;
     int threads = TC * tpl(L);
     if (threads < 32) threads = 32;
-    colfft_kernel<L, SIGN, V><<<nouter * ntiles, threads, smem, st>>>(S, ncols, outer_stride, line_stride, n_in,
-                                                                      n_out, tw, ctl, skip_retry);
+    colfft_kernel<L, SIGN, V><<<dim3((unsigned)(nouter * ntiles), (unsigned)nsim), threads, smem, st>>>(
+        S, ncols, outer_stride, line_stride, n_in, n_out, tw, ctl, skip_retry, sim_stride);
     return cudaGetLastError();
 }
 
 template <int L, int SIGN>
 static cudaError_t launch_colfft4_t(float2* S, int ncols, int nouter, long long outer_stride, long long line_stride,
                                     int n_in, int n_out, const float2* tw, const DevCtl* ctl, int skip_retry,
-                                    cudaStream_t st) {
+                                    cudaStream_t st, int nsim, long long sim_stride) {
     using F = FS<L>;
     constexpr int TC = col4_tile(L);
     const size_t smem = (size_t)(TC * col4_stride<L>() + F::TWT) * sizeof(float2);
@@ -709,26 +743,26 @@ static cudaError_t launch_colfft4_t(float2* S, int ncols, int nouter, long long 
     const int ntiles = (ncols + TC - 1) / TC;
     int threads = TC * F::P2;
     if (threads < 32) threads = 32;
-    colfft4_kernel<L, SIGN><<<nouter * ntiles, threads, smem, st>>>(S, ncols, outer_stride, line_stride, n_in, n_out,
-                                                                    tw, ctl, skip_retry);
+    colfft4_kernel<L, SIGN><<<dim3((unsigned)(nouter * ntiles), (unsigned)nsim), threads, smem, st>>>(
+        S, ncols, outer_stride, line_stride, n_in, n_out, tw, ctl, skip_retry, sim_stride);
     return cudaGetLastError();
 }
 
 template <typename V>
 cudaError_t launch_colfft(int L, int sign, V* S, int ncols, int nouter, long long outer_stride,
                           long long line_stride, int n_in, int n_out, const float2* tw, const DevCtl* ctl,
-                          int skip_retry, cudaStream_t st) {
+                          int skip_retry, cudaStream_t st, int nsim, long long sim_stride) {
     if constexpr (sizeof(V) == 8) {
         if (sign < 0) {
             switch (L) {
-#define X(l) case l: return launch_colfft4_t<l, -1>(S, ncols, nouter, outer_stride, line_stride, n_in, n_out, tw, ctl, skip_retry, st);
+#define X(l) case l: return launch_colfft4_t<l, -1>(S, ncols, nouter, outer_stride, line_stride, n_in, n_out, tw, ctl, skip_retry, st, nsim, sim_stride);
                 X(4) X(8) X(16) X(32) X(64) X(128) X(256) X(512) X(1024)
 #undef X
                 default: break;
             }
         } else {
             switch (L) {
-#define X(l) case l: return launch_colfft4_t<l, 1>(S, ncols, nouter, outer_stride, line_stride, n_in, n_out, tw, ctl, skip_retry, st);
+#define X(l) case l: return launch_colfft4_t<l, 1>(S, ncols, nouter, outer_stride, line_stride, n_in, n_out, tw, ctl, skip_retry, st, nsim, sim_stride);
                 X(4) X(8) X(16) X(32) X(64) X(128) X(256) X(512) X(1024)
 #undef X
                 default: break;
@@ -737,14 +771,14 @@ cudaError_t launch_colfft(int L, int sign, V* S, int ncols, int nouter, long lon
     }
     if (sign < 0) {
         switch (L) {
-#define X(l) case l: return launch_colfft_t<l, -1, V>(S, ncols, nouter, outer_stride, line_stride, n_in, n_out, tw, ctl, skip_retry, st);
+#define X(l) case l: return launch_colfft_t<l, -1, V>(S, ncols, nouter, outer_stride, line_stride, n_in, n_out, tw, ctl, skip_retry, st, nsim, sim_stride);
             MM_FOR_POW2(X)
 #undef X
             default: return cudaErrorInvalidValue;
         }
     } else {
         switch (L) {
-#define X(l) case l: return launch_colfft_t<l, 1, V>(S, ncols, nouter, outer_stride, line_stride, n_in, n_out, tw, ctl, skip_retry, st);
+#define X(l) case l: return launch_colfft_t<l, 1, V>(S, ncols, nouter, outer_stride, line_stride, n_in, n_out, tw, ctl, skip_retry, st, nsim, sim_stride);
             MM_FOR_POW2(X)
 #undef X
             default: return cudaErrorInvalidValue;
@@ -755,7 +789,8 @@ cudaError_t launch_colfft(int L, int sign, V* S, int ncols, int nouter, long lon
 template <int L>
 static cudaError_t launch_colmul_t(float2* S, const KernelView& K, int ncols, int nouter, long long comp_stride,
                                    long long outer_stride, long long line_stride, int n_in, int kaxis, float scale,
-                                   const float2* tw, const DevCtl* ctl, int skip_retry, cudaStream_t st) {
+                                   const float2* tw, const DevCtl* ctl, int skip_retry, cudaStream_t st, int nsim,
+                                   long long sim_stride, const float* sim_scale) {
     constexpr int TC = col_tile(L, 3, 8);
     const size_t smem = (size_t)3 * TC * line_len(L) * sizeof(float2);
     cudaError_t e = set_smem(colmul_kernel<L>, smem);
@@ -763,16 +798,18 @@ static cudaError_t launch_colmul_t(float2* S, const KernelView& K, int ncols, in
     int ntiles = (ncols + TC - 1) / TC;
     int threads = TC * tpl(L);
     if (threads < 32) threads = 32;
-    colmul_kernel<L><<<nouter * ntiles, threads, smem, st>>>(S, K, ncols, comp_stride, outer_stride, line_stride, n_in,
-                                                            kaxis, scale, tw, ctl, skip_retry);
+    colmul_kernel<L><<<dim3((unsigned)(nouter * ntiles), (unsigned)nsim), threads, smem, st>>>(
+        S, K, ncols, comp_stride, outer_stride, line_stride, n_in, kaxis, scale, tw, ctl, skip_retry, sim_stride,
+        sim_scale);
     return cudaGetLastError();
 }
 
 cudaError_t launch_colmul(int L, float2* S, const KernelView& K, int ncols, int nouter, long long comp_stride,
                           long long outer_stride, long long line_stride, int n_in, int kaxis, float scale,
-                          const float2* tw, const DevCtl* ctl, int skip_retry, cudaStream_t st) {
+                          const float2* tw, const DevCtl* ctl, int skip_retry, cudaStream_t st, int nsim,
+                          long long sim_stride, const float* sim_scale) {
     switch (L) {
-#define X(l) case l: return launch_colmul_t<l>(S, K, ncols, nouter, comp_stride, outer_stride, line_stride, n_in, kaxis, scale, tw, ctl, skip_retry, st);
+#define X(l) case l: return launch_colmul_t<l>(S, K, ncols, nouter, comp_stride, outer_stride, line_stride, n_in, kaxis, scale, tw, ctl, skip_retry, st, nsim, sim_stride, sim_scale);
         MM_FOR_POW2(X)
 #undef X
         default: return cudaErrorInvalidValue;
@@ -780,12 +817,14 @@ cudaError_t launch_colmul(int L, float2* S, const KernelView& K, int ncols, int 
 }
 
 template cudaError_t launch_xfwd<float2, float>(int, const float*, PP, const float*, float2*, int, int, int, int, int,
-                                                int, int, const float2*, const DevCtl*, int, cudaStream_t);
+                                                int, int, const float2*, const DevCtl*, int, cudaStream_t, int,
+                                                long long, long long, long long);
 template cudaError_t launch_xfwd<double2, double>(int, const double*, PP, const float*, double2*, int, int, int, int,
-                                                  int, int, int, const float2*, const DevCtl*, int, cudaStream_t);
+                                                  int, int, int, const float2*, const DevCtl*, int, cudaStream_t, int,
+                                                  long long, long long, long long);
 template cudaError_t launch_colfft<float2>(int, int, float2*, int, int, long long, long long, int, int,
-                                           const float2*, const DevCtl*, int, cudaStream_t);
+                                           const float2*, const DevCtl*, int, cudaStream_t, int, long long);
 template cudaError_t launch_colfft<double2>(int, int, double2*, int, int, long long, long long, int, int,
-                                            const float2*, const DevCtl*, int, cudaStream_t);
+                                            const float2*, const DevCtl*, int, cudaStream_t, int, long long);
 
 }  // namespace mm

@@ -21,8 +21,8 @@ struct ConvGeom {
     long long N;  // cells
 };
 
-// Device-side control block of the time stepper.  One per plan; all kernels of an
-// attempt read it, the controller kernel writes it.  Every decision (accept/reject,
+// Device-side control block of the time stepper.  One per simulation; all kernels of an
+// attempt read their simulation's block, the controller kernel writes it.  Every decision (accept/reject,
 // dt, done) is made on the device so that attempts can be queued without host syncs.
 struct DevCtl {
     double t, dt;            // time of the accepted state, dt for the next attempt
@@ -47,31 +47,52 @@ struct DevCtl {
     double dt_thermal;       // > 0: fixed dt for the thermal scale (cutoff_dt), else dt
 };
 
+// Written by the controller after every attempt: what the host polls between batches.
+struct CtlSummary {
+    int active;              // simulations not done
+    int status;              // first non-OK status among the simulations, else MM_OK
+    int bad_sim;             // the simulation that set it
+    int pad;
+    long long step;          // step counter of bad_sim
+    long long max_left;      // max over active simulations of step_end - step
+};
+
+// Scalars that may differ between the simulations of a batched plan (multipliers in
+// SI units, pre-folded as the reference's updaters fold them on the host).
+struct SimScalars {
+    float msat;                 // Msat multiplier (A/m)
+    float ex_pre;               // 2 Aex/(mu0 Msat)
+    float alpha;
+    float hz[3];                // B_ext/mu0 (A/m)
+    float kmul;                 // 2 Ku/(mu0 Msat)
+    float anisu[3];
+    float therm_num;            // alpha * kB * 2 * T
+    float zl_pre;               // P muB/(e Msat)
+    float sl_beta_prime, sl_pre_fld;
+    double therm_den;           // mu0 * V * gamma * Msat  (dt applied on device)
+    unsigned long long seed;    // thermal Philox key
+};
+
 // Parameters of the effective field and torque, device pointers for masks
 // (NULL = uniform 1), multipliers in SI units, internal axis order.
+//
+// Batched plans hold nsim simulations of one geometry.  Every per-cell array is laid
+// out [sim][component][z][y][x] (sim stride 3N floats); kernels take the simulation
+// from blockIdx.y.  Masks are shared (mask_bstride 0) or per simulation (N).
 struct FieldParams {
     int demag, exchange, anis, zeeman, thermal, zhangli, slonczewski;
     int n[3];
     int pbc[3];
     long long N;
-    float msat;                 // Msat multiplier (A/m)
-    float ex_pre;               // 2 Aex/(mu0 Msat)
+    SimScalars s;               // single-simulation scalars (sims == NULL)
+    const SimScalars* sims;     // per-simulation scalars (device), or NULL
+    long long bstride;          // 3N: floats between simulations in per-cell arrays
+    long long mask_bstride;     // 0 (shared masks) or N
     float cinv2[3];             // 1/cell^2
-    float alpha;
-    float hz[3];                // B_ext/mu0 (A/m)
-    float kmul;                 // 2 Ku/(mu0 Msat)
-    float anisu[3];
-    // thermal: H = eta * sqrt(alpha_mask*T_mask*therm_num / (therm_den*dt*Ms_mask))
-    float therm_num;            // alpha * kB * 2 * T
-    double therm_den;           // mu0 * V * gamma * Msat  (dt applied on device)
-    unsigned long long seed;
-    // Zhang-Li
-    float zl_pre;               // P muB/(e Msat)
     float xi;
     float jmul[3];
     float c12inv[3];            // 1/(12 cell)
-    // Slonczewski
-    float sl_beta_prime, sl_pre_fld, lambda, t_fl;
+    float lambda, t_fl;
     float p[3];
     float inv_gamma;
     const float *msat_mask, *aex_mask, *alpha_mask, *ku_mask;
@@ -140,31 +161,38 @@ struct EpiArgs {
     long long noise_step;      // standalone thermal sample
     double dt_thermal;         // standalone thermal dt
     float* dbg[6];             // optional per-term outputs: demag, ex, anis, zee, therm, eff
-    float* red;                // energy block partials [nblocks][8]
-    unsigned int* tq_out;      // standalone max |k|^2 (float bits), may be NULL
+    float* red;                // energy block partials [sim][block][8]
+    unsigned int* tq_out;      // standalone max |k|^2 per simulation (float bits), may be NULL
     int skip_retry;
+    long long spec_bstride;    // complex elements between simulations in the spectrum
 };
 
 // ---- launchers (conv.cu, rhs.cu)
+// Every launcher runs nsim simulations (gridDim.y = nsim); *_bstride are the element
+// strides between simulations, ctl (if not NULL) points to nsim control blocks, and
+// sim_scale (if not NULL) gives the demag scale per simulation.
 template <typename V, typename S>
 cudaError_t launch_xfwd(int M, const S* in, PP pp, const float* mask, V* out, int nrows, int Z, int Y, int Yout,
                         int in_pitch, int n_in, int hp, const float2* tw, const DevCtl* ctl, int skip_retry,
-                        cudaStream_t st);
+                        cudaStream_t st, int nsim = 1, long long in_bstride = 0, long long out_bstride = 0,
+                        long long mask_bstride = 0);
 template <typename V>
 cudaError_t launch_colfft(int L, int sign, V* S, int ncols, int nouter, long long outer_stride,
                           long long line_stride, int n_in, int n_out, const float2* tw, const DevCtl* ctl,
-                          int skip_retry, cudaStream_t st);
+                          int skip_retry, cudaStream_t st, int nsim = 1, long long sim_stride = 0);
 cudaError_t launch_colmul(int L, float2* S, const KernelView& K, int ncols, int nouter, long long comp_stride,
                           long long outer_stride, long long line_stride, int n_in, int kaxis, float scale,
-                          const float2* tw, const DevCtl* ctl, int skip_retry, cudaStream_t st);
+                          const float2* tw, const DevCtl* ctl, int skip_retry, cudaStream_t st, int nsim = 1,
+                          long long sim_stride = 0, const float* sim_scale = nullptr);
 cudaError_t launch_zmul_reg(int P, float2* S, const KernelView& K, int L1, int h, int hp, long long comp_stride,
                             long long zstride, float scale, const float2* tw, const DevCtl* ctl, int skip_retry,
-                            cudaStream_t st);
+                            cudaStream_t st, int nsim = 1, long long sim_stride = 0,
+                            const float* sim_scale = nullptr);
 cudaError_t launch_xinv_epi(int M, const float2* S, int hp, int L1, const float2* tw, const EpiArgs& A, bool terms,
-                            cudaStream_t st, int* nblocks);
-cudaError_t launch_local_epi(const EpiArgs& A, bool terms, cudaStream_t st, int* nblocks);
+                            cudaStream_t st, int* nblocks, int nsim = 1);
+cudaError_t launch_local_epi(const EpiArgs& A, bool terms, cudaStream_t st, int* nblocks, int nsim = 1);
 int xinv_blocks(int M, int n0n1);
 int report_error(int code, const char* msg);  // sets mm_last_error()
-int local_blocks(long long N);
+int local_blocks(long long N, int nsim = 1);
 
 }  // namespace mm

@@ -9,6 +9,7 @@
 // attempt is a fixed sequence of launches whose pointers are resolved on the device
 // from the control block (accepted-state ping-pong, retry and done flags), so attempts
 // can be queued back to back, or replayed from a CUDA graph, without a host round trip.
+#include <algorithm>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -55,7 +56,12 @@ static const double QE = 1.60217646E-19;
 static const double HBAR = 1.054571726E-34;
 
 // ---------------------------------------------------------------- device helpers
-__global__ void normalize_kernel(float* m, const float* msat_mask, long long N) {
+// All per-cell kernels take the simulation from blockIdx.y; bstride = 3N floats between
+// simulations, mask_bstride = 0 (shared masks) or N.
+__global__ void normalize_kernel(float* m, const float* msat_mask, long long N, long long bstride,
+                                 long long mask_bstride) {
+    m += blockIdx.y * bstride;
+    if (msat_mask) msat_mask += blockIdx.y * mask_bstride;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x) {
         float norm = msat_mask ? msat_mask[i] : 1.0f;
         float x = m[i], y = m[N + i], z = m[2 * N + i];
@@ -68,7 +74,7 @@ __global__ void normalize_kernel(float* m, const float* msat_mask, long long N) 
     }
 }
 
-// next = normalise(base + h * sum_j a_j K_j); h from the control block.
+// next = normalise(base + h * sum_j a_j K_j); h from the simulation's control block.
 struct CombineArgs {
     PP base, next;
     int nk;
@@ -76,20 +82,23 @@ struct CombineArgs {
     double ak[MM_MAXK];
     const float* msat_mask;
     long long N;
+    long long bstride, mask_bstride;
     DevCtl* ctl;
 };
 
 __global__ void combine_kernel(CombineArgs A) {
-    const DevCtl* ctl = A.ctl;
+    const DevCtl* ctl = A.ctl + blockIdx.y;
     if (ctl->done) return;
     const int cur = ctl->cur;
-    const float* base = A.base.get(cur);
-    float* next = A.next.get(cur);
+    const long long off = blockIdx.y * A.bstride;
+    const float* base = A.base.get(cur) + off;
+    float* next = A.next.get(cur) + off;
+    const float* msk = A.msat_mask ? A.msat_mask + blockIdx.y * A.mask_bstride : nullptr;
     const float* kp[MM_MAXK];
     float ak[MM_MAXK];
 #pragma unroll
     for (int j = 0; j < MM_MAXK; j++) {
-        kp[j] = j < A.nk ? A.kp[j].get(cur) : nullptr;
+        kp[j] = j < A.nk ? A.kp[j].get(cur) + off : nullptr;
         ak[j] = j < A.nk ? (float)(A.ak[j] * ctl->h) : 0.f;
     }
     const long long N = A.N;
@@ -102,7 +111,7 @@ __global__ void combine_kernel(CombineArgs A) {
             y += ak[j] * kp[j][N + i];
             z += ak[j] * kp[j][2 * N + i];
         }
-        float norm = A.msat_mask ? A.msat_mask[i] : 1.0f;
+        float norm = msk ? msk[i] : 1.0f;
         float mn = sqrtf(x * x + y * y + z * z);
         float sc = (norm == 0.0f) ? 0.0f : 1.0f;
         sc = (mn != 0.0f) ? sc / mn : 0.0f;
@@ -112,9 +121,9 @@ __global__ void combine_kernel(CombineArgs A) {
     }
 }
 
-// Step controller of solve_rk12.go:156-210, generalised to error order q (RK12: q=1).
-// Runs on one thread after the last evaluation of an attempt.
-__global__ void controller_kernel(DevCtl* c, int adaptive, int q, int fsal, int nevals, int first_skippable) {
+// Step controller of solve_rk12.go:156-210, generalised to error order q (RK12: q=1),
+// for one simulation.
+__device__ void control_one(DevCtl* c, int adaptive, int q, int fsal, int nevals, int first_skippable) {
     if (c->done) return;
     c->attempts++;
     c->evals += nevals - ((first_skippable && c->tries > 0) ? 1 : 0);
@@ -165,37 +174,95 @@ __global__ void controller_kernel(DevCtl* c, int adaptive, int q, int fsal, int 
     c->h = c->dt * c->gamma;
 }
 
-// run_until_smaller for non-FSAL solvers: the torque k0 of the current state is known
-// after the first evaluation of an attempt (api.go:122-131 checks before each step).
-__global__ void torque_check_kernel(DevCtl* c) {
-    if (c->done) return;
-    if (c->tries == 0) {
-        c->maxtorque = sqrt((double)__uint_as_float(c->tq_bits)) * c->gamma;
-        if (c->torque_thr > 0 && c->maxtorque < c->torque_thr) c->done = 1;
+// Summary of nsim control blocks for the host: active count, first error, and the most
+// accepted steps any active simulation still needs.  One block; `mode` selects what is
+// done to each block first (0: nothing, 1: control_one, 2: torque check).
+__device__ void summarise(const DevCtl* c, int nsim, CtlSummary* sum, int active, int bad, long long left) {
+    __shared__ int s_active[32], s_bad[32];
+    __shared__ long long s_left[32];
+    for (int o = 16; o > 0; o >>= 1) {
+        active += __shfl_xor_sync(0xffffffffu, active, o);
+        bad = min(bad, __shfl_xor_sync(0xffffffffu, bad, o));
+        left = max(left, __shfl_xor_sync(0xffffffffu, left, o));
     }
-    c->tq_bits = 0u;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    if (lane == 0) { s_active[w] = active; s_bad[w] = bad; s_left[w] = left; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int a = 0, b = 0x7fffffff;
+        long long l = 0;
+        for (int i = 0; i < nw; i++) { a += s_active[i]; b = min(b, s_bad[i]); l = max(l, s_left[i]); }
+        sum->active = a;
+        sum->bad_sim = (b == 0x7fffffff) ? -1 : b;
+        sum->status = (b == 0x7fffffff) ? MM_OK : c[b].status;
+        sum->step = (b == 0x7fffffff) ? 0 : c[b].step;
+        sum->max_left = l;
+    }
 }
 
-// deterministic compensated finish of the block partials of the energy terms
-__global__ void energy_finish_kernel(const float* red, int nblocks, double* out) {
-    if (threadIdx.x >= 4) return;
-    const int q = threadIdx.x;
-    double s = 0.0;  // partial pairs are folded in fixed block order
-    float fs = 0.f, fc = 0.f;
+__global__ void controller_kernel(DevCtl* ctl, int nsim, CtlSummary* sum, int mode, int adaptive, int q, int fsal,
+                                  int nevals, int first_skippable) {
+    int active = 0, bad = 0x7fffffff;
+    long long left = 0;
+    for (int b = threadIdx.x; b < nsim; b += blockDim.x) {
+        DevCtl* c = ctl + b;
+        if (mode == 1) control_one(c, adaptive, q, fsal, nevals, first_skippable);
+        if (mode == 2 && !c->done) {
+            // run_until_smaller for non-FSAL solvers: the torque k0 of the current state is
+            // known after the first evaluation of an attempt (api.go:122-131 checks before
+            // each step)
+            if (c->tries == 0) {
+                c->maxtorque = sqrt((double)__uint_as_float(c->tq_bits)) * c->gamma;
+                if (c->torque_thr > 0 && c->maxtorque < c->torque_thr) c->done = 1;
+            }
+            c->tq_bits = 0u;
+        }
+        if (!c->done) {
+            active++;
+            left = max(left, c->step_end - c->step);
+        }
+        if (c->status != MM_OK) bad = min(bad, b);
+    }
+    summarise(ctl, nsim, sum, active, bad, left);
+}
+
+// For each simulation whose accepted state sits in the second ping-pong buffer, copy
+// state and FSAL derivative to the first (cur is reset afterwards by reset_cur_kernel).
+__global__ void canonical_copy_kernel(float* Y0, const float* Y1, float* K0, const float* K1, const DevCtl* ctl,
+                                      long long n3) {
+    if (ctl[blockIdx.y].cur == 0) return;
+    const long long off = blockIdx.y * n3;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n3; i += (long long)gridDim.x * blockDim.x) {
+        Y0[off + i] = Y1[off + i];
+        K0[off + i] = K1[off + i];
+    }
+}
+__global__ void reset_cur_kernel(DevCtl* ctl, int nsim) {
+    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nsim; b += gridDim.x * blockDim.x) ctl[b].cur = 0;
+}
+
+// deterministic compensated finish of block partials: out[sim*4 + q] from
+// red[(sim*nblocks + b)*8 + 2q (+1)]
+__global__ void energy_finish_kernel(const float* red, int nblocks, double* out, int nsim) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= nsim * 4) return;
+    const int sim = g >> 2, q = g & 3;
+    const float* rs = red + (long long)sim * nblocks * 8;
+    float fs = 0.f, fc = 0.f;  // partial pairs are folded in fixed block order
     for (int b = 0; b < nblocks; b++) {
-        float v = red[b * 8 + 2 * q];
+        float v = rs[b * 8 + 2 * q];
         float t = fs + v;
         if (fabsf(fs) >= fabsf(v)) fc += (fs - t) + v;
         else fc += (v - t) + fs;
         fs = t;
-        fc += red[b * 8 + 2 * q + 1];
+        fc += rs[b * 8 + 2 * q + 1];
     }
-    s = (double)fs + (double)fc;
-    out[q] = s;
+    out[g] = (double)fs + (double)fc;
 }
 
-// compensated per-component sums of the state (for <m>)
-__global__ void sum3_kernel(const float* m, long long N, float* red) {
+// compensated per-component sums of the state (for <m>), one row of blocks per simulation
+__global__ void sum3_kernel(const float* m, long long N, long long bstride, float* red) {
+    m += blockIdx.y * bstride;
     float s[3] = {0.f, 0.f, 0.f}, c[3] = {0.f, 0.f, 0.f};
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x) {
         for (int q = 0; q < 3; q++) {
@@ -220,8 +287,9 @@ __global__ void sum3_kernel(const float* m, long long N, float* red) {
             fs = tt;
             fc += sh[2 * q + 1][t];
         }
-        red[blockIdx.x * 8 + 2 * q] = fs;
-        red[blockIdx.x * 8 + 2 * q + 1] = fc;
+        const long long slot = (long long)blockIdx.y * gridDim.x + blockIdx.x;
+        red[slot * 8 + 2 * q] = fs;
+        red[slot * 8 + 2 * q + 1] = fc;
     }
 }
 
@@ -229,6 +297,9 @@ __global__ void sum3_kernel(const float* m, long long N, float* red) {
 struct mm_plan_s {
     int device = 0;
     mm_problem prob;
+    int nsim = 1;
+    int masks_per_sim = 0;
+    std::vector<mm_sim> sims;        // per-simulation scalars (host copy)
     ConvGeom g;
     FieldParams P;
     bool demag = false;
@@ -236,7 +307,9 @@ struct mm_plan_s {
     float2* tw = nullptr;            // FP32 twiddle table exp(-2 pi i k / 4096)
     KernelView kv;
     float2* S = nullptr;
-    // solver state
+    SimScalars* d_sims = nullptr;    // nsim > 1: per-simulation scalars
+    float* d_sim_msat = nullptr;     // nsim > 1: demag scale of each simulation
+    // solver state (every per-cell buffer holds nsim blocks of 3N floats)
     int solver = -1;
     float* Y[2] = {nullptr, nullptr};
     float* K1[2] = {nullptr, nullptr};
@@ -244,12 +317,14 @@ struct mm_plan_s {
     float* Ma = nullptr;
     float* Mb = nullptr;
     float* Mtmp = nullptr;
-    DevCtl* ctl = nullptr;
-    DevCtl* ctl_host = nullptr;
-    float* red = nullptr;
+    DevCtl* ctl = nullptr;           // nsim control blocks
+    DevCtl* ctl_host = nullptr;      // pinned mirror
+    CtlSummary* dsum = nullptr;
+    CtlSummary* hsum = nullptr;      // pinned
+    float* red = nullptr;            // [nsim][red_blocks][8]
     int red_blocks = 0;
-    double* dres = nullptr;
-    unsigned int* tq = nullptr;
+    double* dres = nullptr;          // [nsim][8]
+    unsigned int* tq = nullptr;      // [nsim]
     bool state_set = false;
     bool run_until = false;
     long long launches = 0;          // kernels enqueued by this plan (graph replays counted per node)
@@ -257,7 +332,10 @@ struct mm_plan_s {
     cudaGraphExec_t graph = nullptr;
     int graph_solver = -1;
     bool graph_run_until = false;
+    long long version = 0;           // bumped whenever captured launches would change
     long long bytes = 0;
+    long long n3() const { return 3 * g.N; }
+    long long spec_bstride() const { return 3LL * g.n[0] * g.L[1] * g.hp; }
 };
 
 static int dalloc(mm_plan p, void** ptr, size_t bytes) {
@@ -269,6 +347,40 @@ static int dalloc(mm_plan p, void** ptr, size_t bytes) {
 
 static bool pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
 
+// Folds one simulation's multipliers the way the reference's updaters do on the host
+// (mod_exchange6.go:47, mod_uniaxialanisotropy.go:49-53, mod_temperature.go:100-112,
+// mod_zhang-li.go:60-64, mod_slonczewski.go:77-79).
+static SimScalars fold_scalars(const mm_problem& q, const mm_sim& m) {
+    SimScalars s;
+    memset(&s, 0, sizeof s);
+    s.msat = (float)m.msat;
+    s.ex_pre = (float)(2.0 * m.aex / (MU0 * m.msat));
+    s.alpha = (float)m.alpha;
+    for (int i = 0; i < 3; i++) s.hz[i] = (float)(m.bext[i] / MU0);
+    s.kmul = (float)(2.0 * m.ku / (MU0 * m.msat));
+    for (int i = 0; i < 3; i++) s.anisu[i] = (float)m.anisu[i];
+    s.therm_num = (float)(m.alpha * KB * 2.0 * m.temp);
+    s.therm_den = MU0 * (q.cell[0] * q.cell[1] * q.cell[2]) * q.gamma * m.msat;
+    s.seed = m.seed;
+    s.zl_pre = (float)(q.zl_pol * MUB / (QE * m.msat));
+    const double beta = HBAR * q.gamma / (MU0 * QE * m.msat);
+    s.sl_beta_prime = (float)(q.sl_pol * beta);
+    s.sl_pre_fld = (float)(beta * q.eps_prime);
+    return s;
+}
+
+static mm_sim sim_of(const mm_problem& q) {
+    mm_sim m;
+    m.msat = q.msat;
+    m.aex = q.aex;
+    m.alpha = q.alpha;
+    for (int i = 0; i < 3; i++) { m.bext[i] = q.bext[i]; m.anisu[i] = q.anisu[i]; }
+    m.ku = q.ku;
+    m.temp = q.temp;
+    m.seed = q.seed;
+    return m;
+}
+
 static void fill_params(mm_plan p) {
     const mm_problem& q = p->prob;
     FieldParams& P = p->P;
@@ -277,31 +389,24 @@ static void fill_params(mm_plan p) {
     P.exchange = q.exchange;
     P.anis = q.anis;
     P.zeeman = q.zeeman;
-    P.thermal = q.thermal && q.temp != 0.0;
+    bool hot = false;
+    for (const mm_sim& m : p->sims) hot = hot || m.temp != 0.0;
+    P.thermal = q.thermal && hot;
     P.zhangli = q.zhangli;
     P.slonczewski = q.slonczewski;
     for (int i = 0; i < 3; i++) { P.n[i] = q.n[i]; P.pbc[i] = q.pbc[i]; }
     P.N = (long long)q.n[0] * q.n[1] * q.n[2];
-    P.msat = (float)q.msat;
-    P.ex_pre = (float)(2.0 * q.aex / (MU0 * q.msat));
+    P.s = fold_scalars(q, p->sims[0]);
+    P.sims = p->nsim > 1 ? p->d_sims : nullptr;
+    P.bstride = 3 * P.N;
+    P.mask_bstride = p->masks_per_sim ? P.N : 0;
     for (int i = 0; i < 3; i++) P.cinv2[i] = (float)(1.0 / ((double)q.cell[i] * (double)q.cell[i]));
-    P.alpha = (float)q.alpha;
-    for (int i = 0; i < 3; i++) P.hz[i] = (float)(q.bext[i] / MU0);
-    P.kmul = (float)(2.0 * q.ku / (MU0 * q.msat));
-    for (int i = 0; i < 3; i++) P.anisu[i] = (float)q.anisu[i];
-    P.therm_num = (float)(q.alpha * KB * 2.0 * q.temp);
-    P.therm_den = MU0 * (q.cell[0] * q.cell[1] * q.cell[2]) * q.gamma * q.msat;
-    P.seed = q.seed;
-    P.zl_pre = (float)(q.zl_pol * MUB / (QE * q.msat));
     P.xi = (float)q.xi;
     for (int i = 0; i < 3; i++) {
         P.jmul[i] = (float)q.j[i];
         P.c12inv[i] = 1.0f / (12.0f * (float)q.cell[i]);
         P.p[i] = (float)q.p[i];
     }
-    const double beta = HBAR * q.gamma / (MU0 * QE * q.msat);
-    P.sl_beta_prime = (float)(q.sl_pol * beta);
-    P.sl_pre_fld = (float)(beta * q.eps_prime);
     P.lambda = (float)q.lambda;
     P.t_fl = (float)q.t_fl;
     P.inv_gamma = (float)(1.0 / q.gamma);
@@ -324,6 +429,28 @@ static void fill_params(mm_plan p) {
     P.t_fl_mask = q.t_fl_mask;
 }
 
+// Uploads the per-simulation scalars (nsim > 1) and refreshes the parameter block.
+static int upload_sims(mm_plan p) {
+    fill_params(p);
+    if (p->nsim == 1) return MM_OK;
+    std::vector<SimScalars> h(p->nsim);
+    std::vector<float> ms(p->nsim);
+    for (int b = 0; b < p->nsim; b++) {
+        h[b] = fold_scalars(p->prob, p->sims[b]);
+        ms[b] = (float)p->sims[b].msat;
+    }
+    if (cudaMemcpy(p->d_sims, h.data(), sizeof(SimScalars) * p->nsim, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(p->d_sim_msat, ms.data(), sizeof(float) * p->nsim, cudaMemcpyHostToDevice) != cudaSuccess)
+        return set_err(MM_ERR_CUDA, "upload of the per-simulation scalars failed");
+    return MM_OK;
+}
+
+static int check_sims(const mm_sim* sims, int nsim) {
+    for (int b = 0; b < nsim; b++)
+        if (!(sims[b].msat != 0.0)) return set_err(MM_ERR_ARG, "Msat of simulation %d must be non-zero", b);
+    return MM_OK;
+}
+
 static int read_ctl(mm_plan p, cudaStream_t st);
 static int write_ctl(mm_plan p, cudaStream_t st);
 
@@ -332,43 +459,74 @@ static void free_graph(mm_plan p) {
         cudaGraphExecDestroy(p->graph);
         p->graph = nullptr;
     }
+    p->version++;
 }
 
 extern "C" MM_API const char* mm_last_error(void) { return g_err.c_str(); }
-extern "C" MM_API const char* mm_version(void) { return "mm_b200 0.1 (sm_100a)"; }
+extern "C" MM_API const char* mm_version(void) { return "mm_b200 0.2 (sm_100a)"; }
 
-extern "C" MM_API int mm_plan_create(const mm_problem* prob, mm_plan* out) {
+extern "C" MM_API int mm_plan_create_batch(const mm_problem* prob, int nsim, const mm_sim* sims, int masks_per_sim,
+                                           mm_plan* out) {
     if (!prob || !out) return set_err(MM_ERR_ARG, "null argument");
     *out = nullptr;
+    if (nsim < 1 || nsim > 65535) return set_err(MM_ERR_ARG, "nsim must be in 1..65535 (got %d)", nsim);
     for (int i = 0; i < 3; i++) {
         if (prob->n[i] < 1) return set_err(MM_ERR_ARG, "grid size must be >= 1");
         if (!(prob->cell[i] > 0)) return set_err(MM_ERR_ARG, "cell size must be > 0");
     }
-    if (!(prob->msat != 0.0)) return set_err(MM_ERR_ARG, "Msat multiplier must be non-zero");
     if (!(prob->gamma != 0.0)) return set_err(MM_ERR_ARG, "gamma should be non-zero");
+    if (sims) {
+        int rc = check_sims(sims, nsim);
+        if (rc) return rc;
+    } else if (!(prob->msat != 0.0)) {
+        return set_err(MM_ERR_ARG, "Msat multiplier must be non-zero");
+    }
     mm_plan p = new mm_plan_s();
     cudaGetDevice(&p->device);
     p->prob = *prob;
+    p->nsim = nsim;
+    p->masks_per_sim = masks_per_sim ? 1 : 0;
+    p->sims.resize(nsim);
+    for (int b = 0; b < nsim; b++) p->sims[b] = sims ? sims[b] : sim_of(*prob);
+    if (sims) {
+        // the problem's own scalars follow simulation 0 (what single-simulation paths read)
+        const mm_sim& m0 = sims[0];
+        p->prob.msat = m0.msat;
+        p->prob.aex = m0.aex;
+        p->prob.alpha = m0.alpha;
+        p->prob.ku = m0.ku;
+        p->prob.temp = m0.temp;
+        p->prob.seed = m0.seed;
+        for (int i = 0; i < 3; i++) { p->prob.bext[i] = m0.bext[i]; p->prob.anisu[i] = m0.anisu[i]; }
+    }
     ConvGeom& g = p->g;
     for (int i = 0; i < 3; i++) {
         g.n[i] = prob->n[i];
         g.L[i] = (prob->n[i] > 1 && prob->pbc[i] == 0) ? 2 * prob->n[i] : prob->n[i];
     }
     g.N = (long long)g.n[0] * g.n[1] * g.n[2];
-    fill_params(p);
     p->demag = prob->demag != 0;
     int rc = MM_OK;
+    if (nsim > 1) {
+        if ((rc = dalloc(p, (void**)&p->d_sims, sizeof(SimScalars) * nsim))) { delete p; return rc; }
+        if ((rc = dalloc(p, (void**)&p->d_sim_msat, sizeof(float) * nsim))) { mm_plan_destroy(p); return rc; }
+    }
+    if ((rc = upload_sims(p))) { mm_plan_destroy(p); return rc; }
     if (p->demag) {
         // Kernel_Arne's sanity checks (kernel_magnetostatic.go:36-45)
         if (!(g.L[1] > 1 && g.L[2] > 1 && g.L[1] % 2 == 0 && g.L[2] % 2 == 0 && (g.L[0] == 1 || g.L[0] % 2 == 0))) {
-            delete p;
+            mm_plan_destroy(p);
             return set_err(MM_ERR_ARG, "demag needs even padded sizes > 1 in y and x (got %d %d %d)", g.L[0], g.L[1],
                            g.L[2]);
         }
         if (!pow2(g.L[0]) || !pow2(g.L[1]) || !pow2(g.L[2]) || g.L[2] > 4096 || g.L[1] > 4096 || g.L[0] > 4096) {
-            delete p;
+            mm_plan_destroy(p);
             return set_err(MM_ERR_ARG, "demag transform sizes must be powers of two <= 4096 (got %d %d %d)", g.L[0],
                            g.L[1], g.L[2]);
+        }
+        if (nsim > 1 && (g.L[2] < 8 || g.L[2] > 2048)) {
+            mm_plan_destroy(p);
+            return set_err(MM_ERR_ARG, "batched plans with demag need 8 <= padded L2 <= 2048 (got %d)", g.L[2]);
         }
         g.M = g.L[2] / 2;
         g.h = g.M + 1;
@@ -377,7 +535,7 @@ extern "C" MM_API int mm_plan_create(const mm_problem* prob, mm_plan* out) {
         g.kd[1] = g.L[1] / 2 + 1;
         g.kd[2] = g.L[2] / 2 + 1;
         const long long oct = (long long)g.kd[0] * g.kd[1] * g.kd[2];
-        if ((rc = dalloc(p, (void**)&p->khat, sizeof(float) * 6 * oct))) { delete p; return rc; }
+        if ((rc = dalloc(p, (void**)&p->khat, sizeof(float) * 6 * oct))) { mm_plan_destroy(p); return rc; }
         if ((rc = dalloc(p, (void**)&p->tw, sizeof(float2) * mmfft::TWN))) { mm_plan_destroy(p); return rc; }
         {
             std::vector<float2> h(mmfft::TWN);
@@ -387,7 +545,7 @@ extern "C" MM_API int mm_plan_create(const mm_problem* prob, mm_plan* out) {
                 return set_err(MM_ERR_CUDA, "twiddle table upload failed");
             }
         }
-        if ((rc = dalloc(p, (void**)&p->S, sizeof(float2) * 3 * (size_t)g.n[0] * g.L[1] * g.hp))) {
+        if ((rc = dalloc(p, (void**)&p->S, sizeof(float2) * (size_t)p->spec_bstride() * nsim))) {
             mm_plan_destroy(p);
             return rc;
         }
@@ -410,23 +568,28 @@ extern "C" MM_API int mm_plan_create(const mm_problem* prob, mm_plan* out) {
         p->kv.L1 = g.L[1];
         for (int q = 0; q < 6; q++) p->kv.nz[q] = nz[q];
     }
-    const size_t vb = sizeof(float) * 3 * (size_t)g.N;
+    const size_t vb = sizeof(float) * (size_t)p->n3() * nsim;
     void** bufs[] = {(void**)&p->Y[0], (void**)&p->Y[1], (void**)&p->K1[0], (void**)&p->K1[1], (void**)&p->Ma,
                      (void**)&p->Mb, (void**)&p->Mtmp};
     for (auto b : bufs)
         if ((rc = dalloc(p, b, vb))) { mm_plan_destroy(p); return rc; }
     for (int i = 0; i < 6; i++)
         if ((rc = dalloc(p, (void**)&p->Kst[i], vb))) { mm_plan_destroy(p); return rc; }
-    if ((rc = dalloc(p, (void**)&p->ctl, sizeof(DevCtl)))) { mm_plan_destroy(p); return rc; }
-    if (cudaMallocHost(&p->ctl_host, sizeof(DevCtl)) != cudaSuccess) {
+    if ((rc = dalloc(p, (void**)&p->ctl, sizeof(DevCtl) * nsim))) { mm_plan_destroy(p); return rc; }
+    if ((rc = dalloc(p, (void**)&p->dsum, sizeof(CtlSummary)))) { mm_plan_destroy(p); return rc; }
+    if (cudaMallocHost(&p->ctl_host, sizeof(DevCtl) * nsim) != cudaSuccess ||
+        cudaMallocHost(&p->hsum, sizeof(CtlSummary)) != cudaSuccess) {
         mm_plan_destroy(p);
         return set_err(MM_ERR_CUDA, "cudaMallocHost failed");
     }
-    p->red_blocks = std::max(p->demag ? xinv_blocks(g.M, g.n[0] * g.n[1]) : 0, local_blocks(g.N));
-    p->red_blocks = std::max(p->red_blocks, 148 * 4);
-    if ((rc = dalloc(p, (void**)&p->red, sizeof(float) * 8 * p->red_blocks))) { mm_plan_destroy(p); return rc; }
-    if ((rc = dalloc(p, (void**)&p->dres, sizeof(double) * 8))) { mm_plan_destroy(p); return rc; }
-    if ((rc = dalloc(p, (void**)&p->tq, sizeof(unsigned int) * 4))) { mm_plan_destroy(p); return rc; }
+    p->red_blocks = std::max(p->demag ? xinv_blocks(g.M, g.n[0] * g.n[1]) : 0, local_blocks(g.N, nsim));
+    if (nsim == 1) p->red_blocks = std::max(p->red_blocks, 148 * 4);
+    if ((rc = dalloc(p, (void**)&p->red, sizeof(float) * 8 * (size_t)p->red_blocks * nsim))) {
+        mm_plan_destroy(p);
+        return rc;
+    }
+    if ((rc = dalloc(p, (void**)&p->dres, sizeof(double) * 8 * nsim))) { mm_plan_destroy(p); return rc; }
+    if ((rc = dalloc(p, (void**)&p->tq, sizeof(unsigned int) * std::max(4, nsim)))) { mm_plan_destroy(p); return rc; }
     DevCtl c;
     memset(&c, 0, sizeof c);
     c.t_end = 1e300;
@@ -439,7 +602,8 @@ extern "C" MM_API int mm_plan_create(const mm_problem* prob, mm_plan* out) {
     c.gamma = prob->gamma;
     c.h = c.dt * c.gamma;
     c.done = 1;
-    if (cudaMemcpy(p->ctl, &c, sizeof c, cudaMemcpyHostToDevice) != cudaSuccess) {
+    for (int b = 0; b < nsim; b++) p->ctl_host[b] = c;
+    if (cudaMemcpy(p->ctl, p->ctl_host, sizeof(DevCtl) * nsim, cudaMemcpyHostToDevice) != cudaSuccess) {
         mm_plan_destroy(p);
         return set_err(MM_ERR_CUDA, "ctl init failed");
     }
@@ -447,18 +611,45 @@ extern "C" MM_API int mm_plan_create(const mm_problem* prob, mm_plan* out) {
     return MM_OK;
 }
 
+extern "C" MM_API int mm_plan_create(const mm_problem* prob, mm_plan* out) {
+    return mm_plan_create_batch(prob, 1, nullptr, 0, out);
+}
+
+extern "C" MM_API int mm_plan_nsim(mm_plan p) { return p ? p->nsim : 0; }
+
 extern "C" MM_API int mm_plan_destroy(mm_plan p) {
     if (!p) return MM_OK;
-    free_graph(p);
-    void* bufs[] = {p->khat, p->tw, p->S, p->Y[0], p->Y[1], p->K1[0], p->K1[1], p->Ma, p->Mb, p->Mtmp, p->ctl,
-                    p->red, p->dres, p->tq};
+    if (p->graph) cudaGraphExecDestroy(p->graph);
+    void* bufs[] = {p->khat, p->tw, p->S, p->d_sims, p->d_sim_msat, p->Y[0], p->Y[1], p->K1[0], p->K1[1], p->Ma,
+                    p->Mb, p->Mtmp, p->ctl, p->dsum, p->red, p->dres, p->tq};
     for (void* b : bufs)
         if (b) cudaFree(b);
     for (int i = 0; i < 6; i++)
         if (p->Kst[i]) cudaFree(p->Kst[i]);
     if (p->ctl_host) cudaFreeHost(p->ctl_host);
+    if (p->hsum) cudaFreeHost(p->hsum);
     delete p;
     return MM_OK;
+}
+
+extern "C" MM_API int mm_batch_set_sims(mm_plan p, const mm_sim* sims) {
+    if (!p || !sims) return set_err(MM_ERR_ARG, "null argument");
+    int rc = check_sims(sims, p->nsim);
+    if (rc) return rc;
+    for (int b = 0; b < p->nsim; b++) p->sims[b] = sims[b];
+    const mm_sim& m0 = sims[0];
+    p->prob.msat = m0.msat;
+    p->prob.aex = m0.aex;
+    p->prob.alpha = m0.alpha;
+    p->prob.ku = m0.ku;
+    p->prob.temp = m0.temp;
+    p->prob.seed = m0.seed;
+    for (int i = 0; i < 3; i++) { p->prob.bext[i] = m0.bext[i]; p->prob.anisu[i] = m0.anisu[i]; }
+    free_graph(p);
+    if ((rc = upload_sims(p))) return rc;
+    if ((rc = read_ctl(p, 0))) return rc;
+    for (int b = 0; b < p->nsim; b++) p->ctl_host[b].fsal_valid = 0;
+    return write_ctl(p, 0);
 }
 
 extern "C" MM_API int mm_plan_set_problem(mm_plan p, const mm_problem* prob) {
@@ -467,16 +658,20 @@ extern "C" MM_API int mm_plan_set_problem(mm_plan p, const mm_problem* prob) {
         if (prob->n[i] != p->prob.n[i] || prob->cell[i] != p->prob.cell[i] || prob->pbc[i] != p->prob.pbc[i])
             return set_err(MM_ERR_ARG, "geometry of a plan cannot change");
     if ((prob->demag != 0) != p->demag) return set_err(MM_ERR_ARG, "demag on/off cannot change after plan creation");
-    if (!(prob->msat != 0.0) || !(prob->gamma != 0.0)) return set_err(MM_ERR_ARG, "Msat and gamma must be non-zero");
+    if (!(prob->gamma != 0.0)) return set_err(MM_ERR_ARG, "gamma must be non-zero");
+    if (p->nsim == 1 && !(prob->msat != 0.0)) return set_err(MM_ERR_ARG, "Msat must be non-zero");
     p->prob = *prob;
-    fill_params(p);
+    if (p->nsim == 1) p->sims[0] = sim_of(*prob);   // batched plans keep their mm_sim scalars
     free_graph(p);
-    // gamma is part of h = dt*gamma on the device
-    int rc = read_ctl(p, 0);
+    int rc = upload_sims(p);
     if (rc) return rc;
-    p->ctl_host->gamma = prob->gamma;
-    p->ctl_host->h = p->ctl_host->dt * prob->gamma;
-    p->ctl_host->fsal_valid = 0;
+    // gamma is part of h = dt*gamma on the device
+    if ((rc = read_ctl(p, 0))) return rc;
+    for (int b = 0; b < p->nsim; b++) {
+        p->ctl_host[b].gamma = prob->gamma;
+        p->ctl_host[b].h = p->ctl_host[b].dt * prob->gamma;
+        p->ctl_host[b].fsal_valid = 0;
+    }
     return write_ctl(p, 0);
 }
 
@@ -495,6 +690,50 @@ static bool zreg_ok(const ConvGeom& g) {
 }
 
 // ---------------------------------------------------------------- one evaluation
+// Launches of the five (3-D) or three (2-D) convolution passes for all simulations;
+// `ev` (optional) receives an event record after each pass.
+static int launch_conv(mm_plan p, PP m_in, const DevCtl* ctl, int skip_retry, cudaStream_t st,
+                       const std::vector<cudaEvent_t>* ev = nullptr) {
+    const ConvGeom& g = p->g;
+    const int n0 = g.n[0], n1 = g.n[1], n2 = g.n[2];
+    const int L0 = g.L[0], L1 = g.L[1];
+    const int ns = p->nsim;
+    const long long plane = (long long)L1 * g.hp;
+    const long long sb = p->spec_bstride();
+    const float scale = (float)p->prob.msat;
+    const float* sim_scale = ns > 1 ? p->d_sim_msat : nullptr;
+    int k = 1;
+    auto mark = [&]() -> int {
+        if (ev) CUCHK(cudaEventRecord((*ev)[k++], st));
+        return MM_OK;
+    };
+    int rc;
+    CUCHK(launch_xfwd<float2, float>(g.M, nullptr, m_in, p->P.msat_mask, p->S, 3 * n0 * n1, n0, n1, L1, n2, n2, g.hp,
+                                     p->tw, ctl, skip_retry, st, ns, p->n3(), sb, p->P.mask_bstride));
+    if ((rc = mark())) return rc;
+    if (L0 == 1) {
+        CUCHK(launch_colmul(L1, p->S, p->kv, g.h, 1, plane, 0, g.hp, n1, 1, scale, p->tw, ctl, skip_retry, st, ns, sb,
+                            sim_scale));
+        if ((rc = mark())) return rc;
+    } else {
+        CUCHK(launch_colfft<float2>(L1, -1, p->S, g.h, 3 * n0, plane, g.hp, n1, L1, p->tw, ctl, skip_retry, st, ns,
+                                    sb));
+        if ((rc = mark())) return rc;
+        if (zreg_ok(g))
+            CUCHK(launch_zmul_reg(n0, p->S, p->kv, L1, g.h, g.hp, (long long)n0 * plane, plane, scale, p->tw, ctl,
+                                  skip_retry, st, ns, sb, sim_scale));
+        else
+            CUCHK(launch_colmul(L0, p->S, p->kv, g.h, L1, (long long)n0 * plane, g.hp, plane, n0, 0, scale, p->tw,
+                                ctl, skip_retry, st, ns, sb, sim_scale));
+        if ((rc = mark())) return rc;
+        CUCHK(launch_colfft<float2>(L1, +1, p->S, g.h, 3 * n0, plane, g.hp, L1, n1, p->tw, ctl, skip_retry, st, ns,
+                                    sb));
+        if ((rc = mark())) return rc;
+    }
+    p->launches += (L0 == 1) ? 2 : 4;
+    return MM_OK;
+}
+
 // Launches the convolution passes (if demag) and the epilogue for one StageOp.
 static int launch_eval(mm_plan p, const StageOp& op, DevCtl* ctl, int skip_retry, float* const* dbg,
                        long long noise_step, double dt_thermal, float* red, unsigned int* tq_out, cudaStream_t st,
@@ -515,32 +754,15 @@ static int launch_eval(mm_plan p, const StageOp& op, DevCtl* ctl, int skip_retry
     A.red = red;
     A.tq_out = tq_out;
     A.skip_retry = skip_retry;
-    int nb = 0;
+    A.spec_bstride = p->spec_bstride();
+    int nb = 0, rc;
     if (p->demag) {
-        const int n0 = g.n[0], n1 = g.n[1], n2 = g.n[2];
-        const int L0 = g.L[0], L1 = g.L[1];
-        const long long plane = (long long)L1 * g.hp;
-        CUCHK(launch_xfwd<float2, float>(g.M, nullptr, op.m_in, p->P.msat_mask, p->S, 3 * n0 * n1, n0, n1, L1, n2,
-                                         n2, g.hp, p->tw, ctl, skip_retry, st));
-        const float scale = (float)p->prob.msat;
-        if (L0 == 1) {
-            CUCHK(launch_colmul(L1, p->S, p->kv, g.h, 1, plane, 0, g.hp, n1, 1, scale, p->tw, ctl, skip_retry, st));
-        } else {
-            CUCHK(launch_colfft<float2>(L1, -1, p->S, g.h, 3 * n0, plane, g.hp, n1, L1, p->tw, ctl, skip_retry, st));
-            if (zreg_ok(g))
-                CUCHK(launch_zmul_reg(n0, p->S, p->kv, L1, g.h, g.hp, (long long)n0 * plane, plane, scale, p->tw, ctl,
-                                      skip_retry, st));
-            else
-                CUCHK(launch_colmul(L0, p->S, p->kv, g.h, L1, (long long)n0 * plane, g.hp, plane, n0, 0, scale, p->tw,
-                                    ctl, skip_retry, st));
-            CUCHK(launch_colfft<float2>(L1, +1, p->S, g.h, 3 * n0, plane, g.hp, L1, n1, p->tw, ctl, skip_retry, st));
-        }
-        CUCHK(launch_xinv_epi(g.M, p->S, g.hp, L1, p->tw, A, terms, st, &nb));
-        p->launches += (L0 == 1) ? 3 : 5;
+        if ((rc = launch_conv(p, op.m_in, ctl, skip_retry, st))) return rc;
+        CUCHK(launch_xinv_epi(g.M, p->S, g.hp, g.L[1], p->tw, A, terms, st, &nb, p->nsim));
     } else {
-        CUCHK(launch_local_epi(A, terms, st, &nb));
-        p->launches += 1;
+        CUCHK(launch_local_epi(A, terms, st, &nb, p->nsim));
     }
+    p->launches += 1;
     if (nblocks_out) *nblocks_out = nb;
     return MM_OK;
 }
@@ -570,8 +792,8 @@ extern "C" MM_API int mm_fields(mm_plan p, const float* m, long long noise_step,
 }
 
 static int normalize_launch(mm_plan p, float* m, cudaStream_t st) {
-    int b = local_blocks(p->g.N);
-    normalize_kernel<<<b, 256, 0, st>>>(m, p->P.msat_mask, p->g.N);
+    const dim3 grid((unsigned)local_blocks(p->g.N, p->nsim), (unsigned)p->nsim);
+    normalize_kernel<<<grid, 256, 0, st>>>(m, p->P.msat_mask, p->g.N, p->n3(), p->P.mask_bstride);
     CUCHK(cudaGetLastError());
     return MM_OK;
 }
@@ -618,11 +840,23 @@ static int launch_combine(mm_plan p, PP base, PP next, int nk, const PP* kp, con
     }
     A.msat_mask = p->P.msat_mask;
     A.N = p->g.N;
+    A.bstride = p->n3();
+    A.mask_bstride = p->P.mask_bstride;
     A.ctl = p->ctl;
-    combine_kernel<<<local_blocks(p->g.N), 256, 0, st>>>(A);
+    combine_kernel<<<dim3((unsigned)local_blocks(p->g.N, p->nsim), (unsigned)p->nsim), 256, 0, st>>>(A);
     CUCHK(cudaGetLastError());
     p->launches++;
     return MM_OK;
+}
+
+// One block over the plan's control blocks (see controller_kernel); also refreshes the
+// summary the host polls.
+static cudaError_t launch_controller(mm_plan p, cudaStream_t st, int mode, int adaptive, int q, int fsal, int nevals,
+                                     int first_skippable) {
+    const int threads = p->nsim >= 256 ? 256 : ((p->nsim + 31) / 32) * 32;
+    controller_kernel<<<1, threads, 0, st>>>(p->ctl, p->nsim, p->dsum, mode, adaptive, q, fsal, nevals,
+                                             first_skippable);
+    return cudaGetLastError();
 }
 
 // Enqueues one step attempt of the configured solver (no host synchronisation).
@@ -656,8 +890,7 @@ static int enqueue_attempt(mm_plan p, cudaStream_t st) {
         const int skip = (s == MM_RK12) ? 1 : 0;
         if ((rc = launch_eval(p, o0, ctl, skip, nullptr, 0, 0, nullptr, nullptr, st, nullptr))) return rc;
         if (p->run_until) {
-            torque_check_kernel<<<1, 1, 0, st>>>(ctl);
-            CUCHK(cudaGetLastError());
+            CUCHK(launch_controller(p, st, 2, 0, 0, 0, 0, 0));
             p->launches++;
         }
         if (s == MM_RK12) {
@@ -689,8 +922,7 @@ static int enqueue_attempt(mm_plan p, cudaStream_t st) {
             }
             if ((rc = launch_eval(p, o1, ctl, 0, nullptr, 0, 0, nullptr, nullptr, st, nullptr))) return rc;
         }
-        controller_kernel<<<1, 1, 0, st>>>(ctl, s == MM_RK12 ? 1 : 0, 1, 0, s == MM_EULER ? 1 : 2, s == MM_RK12);
-        CUCHK(cudaGetLastError());
+        CUCHK(launch_controller(p, st, 1, s == MM_RK12 ? 1 : 0, 1, 0, s == MM_EULER ? 1 : 2, s == MM_RK12));
         p->launches++;
         return MM_OK;
     }
@@ -745,19 +977,18 @@ static int enqueue_attempt(mm_plan p, cudaStream_t st) {
         }
         if ((rc = launch_eval(p, o, ctl, 0, nullptr, 0, 0, nullptr, nullptr, st, nullptr))) return rc;
     }
-    controller_kernel<<<1, 1, 0, st>>>(ctl, 1, dp ? 4 : 2, 1, S - 1, 0);
-    CUCHK(cudaGetLastError());
+    CUCHK(launch_controller(p, st, 1, 1, dp ? 4 : 2, 1, S - 1, 0));
     p->launches++;
     return MM_OK;
 }
 
 static int read_ctl(mm_plan p, cudaStream_t st) {
-    CUCHK(cudaMemcpyAsync(p->ctl_host, p->ctl, sizeof(DevCtl), cudaMemcpyDeviceToHost, st));
+    CUCHK(cudaMemcpyAsync(p->ctl_host, p->ctl, sizeof(DevCtl) * p->nsim, cudaMemcpyDeviceToHost, st));
     CUCHK(cudaStreamSynchronize(st));
     return MM_OK;
 }
 static int write_ctl(mm_plan p, cudaStream_t st) {
-    CUCHK(cudaMemcpyAsync(p->ctl, p->ctl_host, sizeof(DevCtl), cudaMemcpyHostToDevice, st));
+    CUCHK(cudaMemcpyAsync(p->ctl, p->ctl_host, sizeof(DevCtl) * p->nsim, cudaMemcpyHostToDevice, st));
     CUCHK(cudaStreamSynchronize(st));
     return MM_OK;
 }
@@ -770,29 +1001,49 @@ extern "C" MM_API int mm_solver_init(mm_plan p, int solver, double dt, double mi
     free_graph(p);
     int rc = read_ctl(p, 0);
     if (rc) return rc;
-    DevCtl& c = *p->ctl_host;
-    c.dt = dt;
-    c.mindt = mindt;
-    c.maxdt = maxdt;
-    c.maxerr = maxerr;
-    c.headroom = 0.8;
-    c.gamma = p->prob.gamma;
-    c.h = dt * c.gamma;
-    c.fsal_valid = 0;
-    c.tries = 0;
-    c.status = MM_OK;
+    for (int b = 0; b < p->nsim; b++) {
+        DevCtl& c = p->ctl_host[b];
+        c.dt = dt;
+        c.mindt = mindt;
+        c.maxdt = maxdt;
+        c.maxerr = maxerr;
+        c.headroom = 0.8;
+        c.gamma = p->prob.gamma;
+        c.h = dt * c.gamma;
+        c.fsal_valid = 0;
+        c.tries = 0;
+        c.status = MM_OK;
+    }
     return write_ctl(p, 0);
 }
+
+// Batched plans keep every accepted state in the first ping-pong buffer between runs, so
+// that state transfers and reductions see one layout.
+static int canonicalise(mm_plan p, cudaStream_t st) {
+    if (p->nsim == 1) return MM_OK;
+    const dim3 grid((unsigned)local_blocks(p->g.N, p->nsim), (unsigned)p->nsim);
+    canonical_copy_kernel<<<grid, 256, 0, st>>>(p->Y[0], p->Y[1], p->K1[0], p->K1[1], p->ctl, p->n3());
+    CUCHK(cudaGetLastError());
+    reset_cur_kernel<<<(p->nsim + 255) / 256, 256, 0, st>>>(p->ctl, p->nsim);
+    CUCHK(cudaGetLastError());
+    return MM_OK;
+}
+
+// device pointer of the accepted state (read_ctl must have run)
+static float* state_ptr(mm_plan p) { return p->Y[p->ctl_host[0].cur]; }
 
 extern "C" MM_API int mm_set_state(mm_plan p, const float* m, int from_host, mm_stream stream) {
     if (!p || !m) return set_err(MM_ERR_ARG, "null argument");
     cudaStream_t st = (cudaStream_t)stream;
     int rc = read_ctl(p, st);
     if (rc) return rc;
-    float* dst = p->Y[p->ctl_host->cur];
-    CUCHK(cudaMemcpyAsync(dst, m, sizeof(float) * 3 * p->g.N, from_host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, st));
+    if (p->nsim > 1)
+        for (int b = 0; b < p->nsim; b++) p->ctl_host[b].cur = 0;
+    float* dst = state_ptr(p);
+    CUCHK(cudaMemcpyAsync(dst, m, sizeof(float) * p->n3() * p->nsim,
+                          from_host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, st));
     if ((rc = normalize_launch(p, dst, st))) return rc;
-    p->ctl_host->fsal_valid = 0;
+    for (int b = 0; b < p->nsim; b++) p->ctl_host[b].fsal_valid = 0;
     p->state_set = true;
     return write_ctl(p, st);
 }
@@ -802,7 +1053,7 @@ extern "C" MM_API int mm_get_state(mm_plan p, float* m, int to_host, mm_stream s
     cudaStream_t st = (cudaStream_t)stream;
     int rc = read_ctl(p, st);
     if (rc) return rc;
-    CUCHK(cudaMemcpyAsync(m, p->Y[p->ctl_host->cur], sizeof(float) * 3 * p->g.N,
+    CUCHK(cudaMemcpyAsync(m, state_ptr(p), sizeof(float) * p->n3() * p->nsim,
                           to_host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, st));
     CUCHK(cudaStreamSynchronize(st));
     return MM_OK;
@@ -812,10 +1063,12 @@ extern "C" MM_API int mm_set_time(mm_plan p, double t, double dt) {
     if (!p) return set_err(MM_ERR_ARG, "null plan");
     int rc = read_ctl(p, 0);
     if (rc) return rc;
-    p->ctl_host->t = t;
-    if (dt > 0) {
-        p->ctl_host->dt = dt;
-        p->ctl_host->h = dt * p->ctl_host->gamma;
+    for (int b = 0; b < p->nsim; b++) {
+        p->ctl_host[b].t = t;
+        if (dt > 0) {
+            p->ctl_host[b].dt = dt;
+            p->ctl_host[b].h = dt * p->ctl_host[b].gamma;
+        }
     }
     return write_ctl(p, 0);
 }
@@ -824,15 +1077,17 @@ extern "C" MM_API int mm_set_thermal_dt(mm_plan p, double dt_thermal) {
     if (!p) return set_err(MM_ERR_ARG, "null plan");
     int rc = read_ctl(p, 0);
     if (rc) return rc;
-    p->ctl_host->dt_thermal = dt_thermal;
+    for (int b = 0; b < p->nsim; b++) p->ctl_host[b].dt_thermal = dt_thermal;
     return write_ctl(p, 0);
 }
 
 // FSAL solvers need f(Y[cur]) before the first attempt.
 static int ensure_fsal(mm_plan p, cudaStream_t st) {
     if (p->solver != MM_RK23 && p->solver != MM_RK45) return MM_OK;
-    if (p->ctl_host->fsal_valid) return MM_OK;
-    // a standalone evaluation with the control block (done = 0 at this point)
+    bool all = true;
+    for (int b = 0; b < p->nsim; b++) all = all && p->ctl_host[b].fsal_valid;
+    if (all) return MM_OK;
+    // a standalone evaluation with the control blocks (done = 0 at this point)
     StageOp o = op_blank();
     o.m_in = cur_of(p->Y);
     o.k_out = cur_of(p->K1);
@@ -840,11 +1095,14 @@ static int ensure_fsal(mm_plan p, cudaStream_t st) {
     int rc = launch_eval(p, o, p->ctl, 0, nullptr, 0, 0, nullptr, nullptr, st, nullptr);
     if (rc) return rc;
     if ((rc = read_ctl(p, st))) return rc;
-    float tqv;
-    memcpy(&tqv, &p->ctl_host->tq_bits, sizeof tqv);
-    p->ctl_host->maxtorque = sqrt((double)tqv) * p->ctl_host->gamma;
-    p->ctl_host->tq_bits = 0;
-    p->ctl_host->fsal_valid = 1;
+    for (int b = 0; b < p->nsim; b++) {
+        DevCtl& c = p->ctl_host[b];
+        float tqv;
+        memcpy(&tqv, &c.tq_bits, sizeof tqv);
+        c.maxtorque = sqrt((double)tqv) * c.gamma;
+        c.tq_bits = 0;
+        c.fsal_valid = 1;
+    }
     return write_ctl(p, st);
 }
 
@@ -883,89 +1141,126 @@ extern "C" MM_API int mm_queue_attempts(mm_plan p, int attempts, mm_stream strea
     return MM_OK;
 }
 
-// Runs attempts until the device sets `done`.  The host only polls the control block
-// between batches of queued attempts.
+static int read_summary(mm_plan p, cudaStream_t st) {
+    CUCHK(cudaMemcpyAsync(p->hsum, p->dsum, sizeof(CtlSummary), cudaMemcpyDeviceToHost, st));
+    CUCHK(cudaStreamSynchronize(st));
+    return MM_OK;
+}
+
+static int summary_status(mm_plan p) {
+    const CtlSummary& s = *p->hsum;
+    if (s.status == MM_OK) return MM_OK;
+    const char* who = p->nsim > 1 ? " of simulation " : "";
+    char num[32] = "";
+    if (p->nsim > 1) snprintf(num, sizeof num, "%d", s.bad_sim);
+    if (s.status == MM_ERR_NAN) return set_err(MM_ERR_NAN, "NaN in the torque at step %lld%s%s", s.step, who, num);
+    return set_err(s.status, "solver cannot converge after 10 bad steps (step %lld%s%s)", s.step, who, num);
+}
+
+// Attempts to queue next: no more than the largest number of accepted steps an active
+// simulation still needs (so fixed-count runs launch no no-op attempts), doubling from 4
+// up to 64 while the end is not known in steps.
+static int next_batch(long long max_left, int grow) {
+    long long b = grow;
+    if (max_left > 0 && max_left < b) b = max_left;
+    return (int)std::max(1LL, b);
+}
+
+// Runs attempts until the device sets `done` for every simulation.  The host only polls
+// the summary between batches of queued attempts.
 static int drive(mm_plan p, cudaStream_t st, long long max_attempts) {
-    int batch = 4;
+    int grow = 4;
     long long launched = 0;
+    long long max_left = 0;
+    for (int b = 0; b < p->nsim; b++)
+        if (!p->ctl_host[b].done) max_left = std::max(max_left, p->ctl_host[b].step_end - p->ctl_host[b].step);
     for (;;) {
+        const int batch = next_batch(max_left, grow);
         int rc = mm_queue_attempts(p, batch, (mm_stream)st);
         if (rc) return rc;
         launched += batch;
-        if ((rc = read_ctl(p, st))) return rc;
-        const DevCtl& c = *p->ctl_host;
-        if (c.status == MM_ERR_NAN) return set_err(MM_ERR_NAN, "NaN in the torque at step %lld", c.step);
-        if (c.status != MM_OK) return set_err(c.status, "solver cannot converge after 10 bad steps (step %lld)", c.step);
-        if (c.done) return MM_OK;
+        if ((rc = read_summary(p, st))) return rc;
+        if ((rc = summary_status(p))) return rc;
+        if (p->hsum->active == 0) return MM_OK;
         if (max_attempts > 0 && launched >= max_attempts) return set_err(MM_ERR_TIMEOUT, "attempt limit reached");
-        if (batch < 64) batch *= 2;
+        max_left = p->hsum->max_left;
+        if (grow < 64) grow *= 2;
     }
 }
 
-static int start_run(mm_plan p, cudaStream_t st, double t_end, long long step_end, double thr) {
+// Sets every simulation's stop condition: t_end = t + duration (duration > 0), or
+// step_end = step + nsteps (nsteps > 0), or maxtorque < thr.
+static int start_run(mm_plan p, cudaStream_t st, double duration, long long nsteps, double thr,
+                     long long max_steps) {
     if (p->solver < 0) return set_err(MM_ERR_STATE, "no solver: call mm_solver_init");
     if (!p->state_set) return set_err(MM_ERR_STATE, "no state: call mm_set_state");
     int rc = read_ctl(p, st);
     if (rc) return rc;
-    DevCtl& c = *p->ctl_host;
-    c.done = 0;
-    c.status = MM_OK;
-    c.tries = 0;
-    c.t_end = t_end;
-    c.step_end = step_end;
-    c.torque_thr = thr;
-    c.err_bits = 0;
-    c.tq_bits = 0;
-    c.gamma = p->prob.gamma;
-    c.h = c.dt * c.gamma;
+    for (int b = 0; b < p->nsim; b++) {
+        DevCtl& c = p->ctl_host[b];
+        c.done = 0;
+        c.status = MM_OK;
+        c.tries = 0;
+        c.t_end = duration > 0 ? c.t + duration : 1e300;
+        c.step_end = nsteps > 0 ? c.step + nsteps : (max_steps > 0 ? c.step + max_steps : (1LL << 62));
+        c.torque_thr = thr;
+        c.err_bits = 0;
+        c.tq_bits = 0;
+        c.gamma = p->prob.gamma;
+        c.h = c.dt * c.gamma;
+        if (duration > 0 && !(c.t < c.t_end)) c.done = 1;
+    }
     p->run_until = thr > 0;
     if ((rc = write_ctl(p, st))) return rc;
     if ((rc = ensure_fsal(p, st))) return rc;
     if (thr > 0 && (p->solver == MM_RK23 || p->solver == MM_RK45)) {
         if ((rc = read_ctl(p, st))) return rc;
-        if (p->ctl_host->maxtorque < thr) {
-            p->ctl_host->done = 1;
-            return write_ctl(p, st);
-        }
+        for (int b = 0; b < p->nsim; b++)
+            if (p->ctl_host[b].maxtorque < thr) p->ctl_host[b].done = 1;
+        return write_ctl(p, st);
     }
     return MM_OK;
 }
 
 static int finish_run(mm_plan p, cudaStream_t st) {
-    int rc = read_ctl(p, st);
+    int rc = canonicalise(p, st);
     if (rc) return rc;
-    p->ctl_host->done = 1;
-    p->ctl_host->t_end = 1e300;
-    p->ctl_host->step_end = (1LL << 62);
-    p->ctl_host->torque_thr = 0;
+    if ((rc = read_ctl(p, st))) return rc;
+    for (int b = 0; b < p->nsim; b++) {
+        DevCtl& c = p->ctl_host[b];
+        c.done = 1;
+        c.t_end = 1e300;
+        c.step_end = (1LL << 62);
+        c.torque_thr = 0;
+    }
     p->run_until = false;
     return write_ctl(p, st);
 }
 
-extern "C" MM_API int mm_run(mm_plan p, double duration, mm_stream stream) {
-    if (!p) return set_err(MM_ERR_ARG, "null plan");
-    cudaStream_t st = (cudaStream_t)stream;
-    int rc = read_ctl(p, st);
+static bool any_active(mm_plan p) {
+    for (int b = 0; b < p->nsim; b++)
+        if (!p->ctl_host[b].done) return true;
+    return false;
+}
+
+static int run_plan(mm_plan p, cudaStream_t st, double duration, long long nsteps, double thr, long long max_steps) {
+    int rc = start_run(p, st, duration, nsteps, thr, max_steps);
     if (rc) return rc;
-    const double t0 = p->ctl_host->t;
-    if (!(t0 < t0 + duration)) return MM_OK;
-    if ((rc = start_run(p, st, t0 + duration, (1LL << 62), 0))) return rc;
-    rc = drive(p, st, 0);
+    if (any_active(p)) rc = drive(p, st, 0);
     int rc2 = finish_run(p, st);
     return rc ? rc : rc2;
+}
+
+extern "C" MM_API int mm_run(mm_plan p, double duration, mm_stream stream) {
+    if (!p) return set_err(MM_ERR_ARG, "null plan");
+    if (!(duration > 0)) return MM_OK;
+    return run_plan(p, (cudaStream_t)stream, duration, 0, 0, 0);
 }
 
 extern "C" MM_API int mm_steps(mm_plan p, long long n, mm_stream stream) {
     if (!p) return set_err(MM_ERR_ARG, "null plan");
     if (n <= 0) return MM_OK;
-    cudaStream_t st = (cudaStream_t)stream;
-    int rc = read_ctl(p, st);
-    if (rc) return rc;
-    const long long s0 = p->ctl_host->step;
-    if ((rc = start_run(p, st, 1e300, s0 + n, 0))) return rc;
-    rc = drive(p, st, 0);
-    int rc2 = finish_run(p, st);
-    return rc ? rc : rc2;
+    return run_plan(p, (cudaStream_t)stream, 0, n, 0, 0);
 }
 
 extern "C" MM_API int mm_step(mm_plan p, mm_stream stream) { return mm_steps(p, 1, stream); }
@@ -973,21 +1268,10 @@ extern "C" MM_API int mm_step(mm_plan p, mm_stream stream) { return mm_steps(p, 
 extern "C" MM_API int mm_run_until_maxtorque(mm_plan p, double thr, long long max_steps, mm_stream stream) {
     if (!p) return set_err(MM_ERR_ARG, "null plan");
     if (!(thr > 0)) return set_err(MM_ERR_ARG, "threshold must be > 0");
-    cudaStream_t st = (cudaStream_t)stream;
-    int rc = read_ctl(p, st);
-    if (rc) return rc;
-    const long long s0 = p->ctl_host->step;
-    if ((rc = start_run(p, st, 1e300, max_steps > 0 ? s0 + max_steps : (1LL << 62), thr))) return rc;
-    rc = drive(p, st, 0);
-    int rc2 = finish_run(p, st);
-    return rc ? rc : rc2;
+    return run_plan(p, (cudaStream_t)stream, 0, 0, thr, max_steps);
 }
 
-extern "C" MM_API int mm_get_stats(mm_plan p, mm_stats* out, mm_stream stream) {
-    if (!p || !out) return set_err(MM_ERR_ARG, "null argument");
-    int rc = read_ctl(p, (cudaStream_t)stream);
-    if (rc) return rc;
-    const DevCtl& c = *p->ctl_host;
+static void stats_of(const DevCtl& c, mm_stats* out) {
     out->t = c.t;
     out->dt = c.dt;
     out->err = c.err;
@@ -999,74 +1283,119 @@ extern "C" MM_API int mm_get_stats(mm_plan p, mm_stats* out, mm_stream stream) {
     out->evals = c.evals;
     out->status = c.status;
     out->done = c.done;
+}
+
+static int single(mm_plan p) {
+    if (p->nsim != 1)
+        return set_err(MM_ERR_ARG, "plan holds %d simulations: use the mm_batch_* variant", p->nsim);
     return MM_OK;
 }
 
+extern "C" MM_API int mm_batch_stats(mm_plan p, mm_stats* out, mm_stream stream) {
+    if (!p || !out) return set_err(MM_ERR_ARG, "null argument");
+    int rc = read_ctl(p, (cudaStream_t)stream);
+    if (rc) return rc;
+    for (int b = 0; b < p->nsim; b++) stats_of(p->ctl_host[b], out + b);
+    return MM_OK;
+}
+
+extern "C" MM_API int mm_get_stats(mm_plan p, mm_stats* out, mm_stream stream) {
+    if (!p || !out) return set_err(MM_ERR_ARG, "null argument");
+    int rc = single(p);
+    return rc ? rc : mm_batch_stats(p, out, stream);
+}
+
 // ---------------------------------------------------------------- reductions of the state
-extern "C" MM_API int mm_maxtorque(mm_plan p, double* out, mm_stream stream) {
+extern "C" MM_API int mm_batch_maxtorque(mm_plan p, double* out, mm_stream stream) {
     if (!p || !out) return set_err(MM_ERR_ARG, "null argument");
     cudaStream_t st = (cudaStream_t)stream;
     int rc = read_ctl(p, st);
     if (rc) return rc;
-    CUCHK(cudaMemsetAsync(p->tq, 0, sizeof(unsigned int), st));
+    const DevCtl& c0 = p->ctl_host[0];
+    CUCHK(cudaMemsetAsync(p->tq, 0, sizeof(unsigned int) * p->nsim, st));
     StageOp o = op_blank();
-    o.m_in = fixed(p->Y[p->ctl_host->cur]);
+    o.m_in = fixed(state_ptr(p));
     o.k_out = fixed(p->Mtmp);
     o.want_tq = 1;
-    if ((rc = launch_eval(p, o, nullptr, 0, nullptr, p->ctl_host->noise_step,
-                          p->ctl_host->dt_thermal > 0 ? p->ctl_host->dt_thermal : p->ctl_host->dt, nullptr, p->tq,
-                          st, nullptr)))
+    if ((rc = launch_eval(p, o, nullptr, 0, nullptr, c0.noise_step, c0.dt_thermal > 0 ? c0.dt_thermal : c0.dt,
+                          nullptr, p->tq, st, nullptr)))
         return rc;
-    unsigned int bits = 0;
-    CUCHK(cudaMemcpyAsync(&bits, p->tq, sizeof bits, cudaMemcpyDeviceToHost, st));
+    std::vector<unsigned int> bits(p->nsim);
+    CUCHK(cudaMemcpyAsync(bits.data(), p->tq, sizeof(unsigned int) * p->nsim, cudaMemcpyDeviceToHost, st));
     CUCHK(cudaStreamSynchronize(st));
-    float v;
-    memcpy(&v, &bits, sizeof v);
-    *out = sqrt((double)v) * p->prob.gamma;
+    for (int b = 0; b < p->nsim; b++) {
+        float v;
+        memcpy(&v, &bits[b], sizeof v);
+        out[b] = sqrt((double)v) * p->prob.gamma;
+    }
+    return MM_OK;
+}
+
+extern "C" MM_API int mm_maxtorque(mm_plan p, double* out, mm_stream stream) {
+    if (!p || !out) return set_err(MM_ERR_ARG, "null argument");
+    int rc = single(p);
+    return rc ? rc : mm_batch_maxtorque(p, out, stream);
+}
+
+extern "C" MM_API int mm_batch_average(mm_plan p, double* out, mm_stream stream) {
+    if (!p || !out) return set_err(MM_ERR_ARG, "null argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    int rc = read_ctl(p, st);
+    if (rc) return rc;
+    const int nb = std::min(p->red_blocks, std::max(1, (148 * 2 + p->nsim - 1) / p->nsim));
+    sum3_kernel<<<dim3((unsigned)nb, (unsigned)p->nsim), 256, 0, st>>>(state_ptr(p), p->g.N, p->n3(), p->red);
+    CUCHK(cudaGetLastError());
+    energy_finish_kernel<<<(p->nsim * 4 + 127) / 128, 128, 0, st>>>(p->red, nb, p->dres, p->nsim);
+    CUCHK(cudaGetLastError());
+    std::vector<double> r(4 * (size_t)p->nsim);
+    CUCHK(cudaMemcpyAsync(r.data(), p->dres, sizeof(double) * r.size(), cudaMemcpyDeviceToHost, st));
+    CUCHK(cudaStreamSynchronize(st));
+    for (int b = 0; b < p->nsim; b++)
+        for (int c = 0; c < 3; c++) out[3 * b + c] = r[4 * b + c] / (double)p->g.N;
     return MM_OK;
 }
 
 extern "C" MM_API int mm_average(mm_plan p, double out[3], mm_stream stream) {
     if (!p || !out) return set_err(MM_ERR_ARG, "null argument");
-    cudaStream_t st = (cudaStream_t)stream;
-    int rc = read_ctl(p, st);
-    if (rc) return rc;
-    const int nb = std::min(p->red_blocks, 148 * 2);
-    sum3_kernel<<<nb, 256, 0, st>>>(p->Y[p->ctl_host->cur], p->g.N, p->red);
-    CUCHK(cudaGetLastError());
-    energy_finish_kernel<<<1, 32, 0, st>>>(p->red, nb, p->dres);
-    CUCHK(cudaGetLastError());
-    double r[4];
-    CUCHK(cudaMemcpyAsync(r, p->dres, sizeof r, cudaMemcpyDeviceToHost, st));
-    CUCHK(cudaStreamSynchronize(st));
-    for (int c = 0; c < 3; c++) out[c] = r[c] / (double)p->g.N;
-    return MM_OK;
+    int rc = single(p);
+    return rc ? rc : mm_batch_average(p, out, stream);
 }
 
-extern "C" MM_API int mm_energy(mm_plan p, double out[5], mm_stream stream) {
+extern "C" MM_API int mm_batch_energy(mm_plan p, double* out, mm_stream stream) {
     if (!p || !out) return set_err(MM_ERR_ARG, "null argument");
     cudaStream_t st = (cudaStream_t)stream;
     int rc = read_ctl(p, st);
     if (rc) return rc;
     StageOp o = op_blank();
-    o.m_in = fixed(p->Y[p->ctl_host->cur]);
+    o.m_in = fixed(state_ptr(p));
     o.want_energy = 1;
     // thermal noise does not enter the energy terms
     int nb = 0;
     if ((rc = launch_eval(p, o, nullptr, 0, nullptr, 0, 1.0, p->red, nullptr, st, &nb))) return rc;
-    energy_finish_kernel<<<1, 32, 0, st>>>(p->red, nb, p->dres);
+    energy_finish_kernel<<<(p->nsim * 4 + 127) / 128, 128, 0, st>>>(p->red, nb, p->dres, p->nsim);
     CUCHK(cudaGetLastError());
-    double r[4];
-    CUCHK(cudaMemcpyAsync(r, p->dres, sizeof r, cudaMemcpyDeviceToHost, st));
+    std::vector<double> r(4 * (size_t)p->nsim);
+    CUCHK(cudaMemcpyAsync(r.data(), p->dres, sizeof(double) * r.size(), cudaMemcpyDeviceToHost, st));
     CUCHK(cudaStreamSynchronize(st));
     const mm_problem& q = p->prob;
     const double V = q.cell[0] * q.cell[1] * q.cell[2];
-    out[0] = q.zeeman ? -V * r[0] * q.msat : 0.0;
-    out[1] = q.exchange ? -0.5 * V * MU0 * r[1] * q.msat : 0.0;
-    out[2] = q.demag ? -0.5 * V * MU0 * r[2] * q.msat : 0.0;
-    out[3] = q.anis ? -0.5 * V * MU0 * r[3] * q.msat : 0.0;
-    out[4] = out[0] + out[1] + out[2] + out[3];
+    for (int b = 0; b < p->nsim; b++) {
+        const double ms = p->sims[b].msat;
+        double* e = out + 5 * b;
+        const double* rb = r.data() + 4 * b;
+        e[0] = q.zeeman ? -V * rb[0] * ms : 0.0;
+        e[1] = q.exchange ? -0.5 * V * MU0 * rb[1] * ms : 0.0;
+        e[2] = q.demag ? -0.5 * V * MU0 * rb[2] * ms : 0.0;
+        e[3] = q.anis ? -0.5 * V * MU0 * rb[3] * ms : 0.0;
+        e[4] = e[0] + e[1] + e[2] + e[3];
+    }
     return MM_OK;
+}
+
+extern "C" MM_API int mm_energy(mm_plan p, double out[5], mm_stream stream) {
+    if (!p || !out) return set_err(MM_ERR_ARG, "null argument");
+    int rc = single(p);
+    return rc ? rc : mm_batch_energy(p, out, stream);
 }
 
 extern "C" MM_API long long mm_plan_launch_count(mm_plan p) { return p ? p->launches : 0; }
@@ -1075,7 +1404,7 @@ extern "C" MM_API long long mm_plan_launch_count(mm_plan p) { return p ? p->laun
 // discarded) with CUDA events recorded on the launching stream between the passes;
 // ms_out[i] = average duration of pass i over `reps` evaluations.  Pass order:
 // 3-D: xfwd, y fwd, z mul, y inv, x inv + epilogue; 2-D: xfwd, y mul, x inv + epilogue;
-// no demag: epilogue only.
+// no demag: epilogue only.  Batched plans time all simulations together.
 extern "C" MM_API int mm_profile_eval(mm_plan p, int reps, double* ms_out, int* npass, mm_stream stream) {
     if (!p || !ms_out || !npass || reps < 1) return set_err(MM_ERR_ARG, "bad argument");
     cudaStream_t st = (cudaStream_t)stream;
@@ -1083,50 +1412,29 @@ extern "C" MM_API int mm_profile_eval(mm_plan p, int reps, double* ms_out, int* 
     if (rc) return rc;
     const ConvGeom& g = p->g;
     StageOp op = op_blank();
-    op.m_in = fixed(p->Y[p->ctl_host->cur]);
+    op.m_in = fixed(state_ptr(p));
     op.k_out = fixed(p->Mtmp);
     EpiArgs A;
     memset(&A, 0, sizeof A);
     A.P = p->P;
     A.op = op;
+    A.spec_bstride = p->spec_bstride();
     const int np = p->demag ? (g.L[0] == 1 ? 3 : 5) : 1;
     *npass = np;
     std::vector<cudaEvent_t> ev(np + 1);
     for (auto& e : ev) CUCHK(cudaEventCreate(&e));
     std::vector<double> acc(np, 0.0);
+    const long long launches0 = p->launches;
     for (int r = -1; r < reps; r++) {  // r = -1: untimed warm-up evaluation
-        int k = 0;
-        CUCHK(cudaEventRecord(ev[k++], st));
+        CUCHK(cudaEventRecord(ev[0], st));
         int nb = 0;
         if (p->demag) {
-            const int n0 = g.n[0], n1 = g.n[1], n2 = g.n[2];
-            const int L0 = g.L[0], L1 = g.L[1];
-            const long long plane = (long long)L1 * g.hp;
-            const float scale = (float)p->prob.msat;
-            CUCHK(launch_xfwd<float2, float>(g.M, nullptr, op.m_in, p->P.msat_mask, p->S, 3 * n0 * n1, n0, n1, L1,
-                                             n2, n2, g.hp, p->tw, nullptr, 0, st));
-            CUCHK(cudaEventRecord(ev[k++], st));
-            if (L0 == 1) {
-                CUCHK(launch_colmul(L1, p->S, p->kv, g.h, 1, plane, 0, g.hp, n1, 1, scale, p->tw, nullptr, 0, st));
-                CUCHK(cudaEventRecord(ev[k++], st));
-            } else {
-                CUCHK(launch_colfft<float2>(L1, -1, p->S, g.h, 3 * n0, plane, g.hp, n1, L1, p->tw, nullptr, 0, st));
-                CUCHK(cudaEventRecord(ev[k++], st));
-                if (zreg_ok(g))
-                    CUCHK(launch_zmul_reg(n0, p->S, p->kv, L1, g.h, g.hp, (long long)n0 * plane, plane, scale, p->tw,
-                                          nullptr, 0, st));
-                else
-                    CUCHK(launch_colmul(L0, p->S, p->kv, g.h, L1, (long long)n0 * plane, g.hp, plane, n0, 0, scale,
-                                        p->tw, nullptr, 0, st));
-                CUCHK(cudaEventRecord(ev[k++], st));
-                CUCHK(launch_colfft<float2>(L1, +1, p->S, g.h, 3 * n0, plane, g.hp, L1, n1, p->tw, nullptr, 0, st));
-                CUCHK(cudaEventRecord(ev[k++], st));
-            }
-            CUCHK(launch_xinv_epi(g.M, p->S, g.hp, L1, p->tw, A, false, st, &nb));
+            if ((rc = launch_conv(p, op.m_in, nullptr, 0, st, &ev))) return rc;
+            CUCHK(launch_xinv_epi(g.M, p->S, g.hp, g.L[1], p->tw, A, false, st, &nb, p->nsim));
         } else {
-            CUCHK(launch_local_epi(A, false, st, &nb));
+            CUCHK(launch_local_epi(A, false, st, &nb, p->nsim));
         }
-        CUCHK(cudaEventRecord(ev[k++], st));
+        CUCHK(cudaEventRecord(ev[np], st));
         CUCHK(cudaEventSynchronize(ev[np]));
         if (r < 0) continue;
         for (int i = 0; i < np; i++) {
@@ -1135,6 +1443,7 @@ extern "C" MM_API int mm_profile_eval(mm_plan p, int reps, double* ms_out, int* 
             acc[i] += ms;
         }
     }
+    p->launches = launches0 + (long long)(reps + 1) * np;
     for (int i = 0; i < np; i++) ms_out[i] = acc[i] / reps;
     for (auto& e : ev) cudaEventDestroy(e);
     return MM_OK;
@@ -1149,6 +1458,147 @@ extern "C" MM_API int mm_plan_geometry(mm_plan p, int* out12) {
     for (int q = 0; q < 6; q++) nzc += p->demag ? p->kv.nz[q] : 0;
     v[9] = nzc;
     v[10] = p->demag ? 1 : 0;
+    v[11] = p->nsim;
     memcpy(out12, v, sizeof v);
     return MM_OK;
 }
+
+// ---------------------------------------------------------------- ensembles
+// Plans of different geometry stepped together: one CUDA graph whose branches (one per
+// plan, forked from and joined to the capture stream) each replay K attempts of that
+// plan.  Branches share no buffers, so the GPU overlaps the small plans' launches.
+struct mm_ensemble_s {
+    std::vector<mm_plan> plans;
+    int K = 16;
+    std::vector<cudaStream_t> streams;
+    cudaEvent_t fork = nullptr;
+    std::vector<cudaEvent_t> joins;
+    cudaGraphExec_t graph = nullptr;
+    std::vector<long long> versions;  // plan versions the graph was captured from
+    long long nodes = 0;
+    long long launches = 0;
+};
+
+extern "C" MM_API int mm_ensemble_destroy(mm_ensemble e) {
+    if (!e) return MM_OK;
+    if (e->graph) cudaGraphExecDestroy(e->graph);
+    for (auto s : e->streams) cudaStreamDestroy(s);
+    for (auto j : e->joins) cudaEventDestroy(j);
+    if (e->fork) cudaEventDestroy(e->fork);
+    delete e;
+    return MM_OK;
+}
+
+extern "C" MM_API int mm_ensemble_create(const mm_plan* plans, int nplans, int attempts_per_launch,
+                                         mm_ensemble* out) {
+    if (!plans || !out || nplans < 1) return set_err(MM_ERR_ARG, "need at least one plan");
+    if (attempts_per_launch < 1 || attempts_per_launch > 1024) return set_err(MM_ERR_ARG, "attempts_per_launch in 1..1024");
+    *out = nullptr;
+    for (int i = 0; i < nplans; i++) {
+        if (!plans[i]) return set_err(MM_ERR_ARG, "plan %d is null", i);
+        for (int j = 0; j < i; j++)
+            if (plans[j] == plans[i]) return set_err(MM_ERR_ARG, "plan %d appears twice", i);
+    }
+    mm_ensemble e = new mm_ensemble_s();
+    e->plans.assign(plans, plans + nplans);
+    e->K = attempts_per_launch;
+    e->streams.resize(nplans, nullptr);
+    e->joins.resize(nplans, nullptr);
+    cudaError_t err = cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming);
+    for (int i = 0; i < nplans && err == cudaSuccess; i++) {
+        err = cudaStreamCreateWithFlags(&e->streams[i], cudaStreamNonBlocking);
+        if (err == cudaSuccess) err = cudaEventCreateWithFlags(&e->joins[i], cudaEventDisableTiming);
+    }
+    if (err != cudaSuccess) {
+        mm_ensemble_destroy(e);
+        return set_err(MM_ERR_CUDA, "ensemble streams/events: %s", cudaGetErrorString(err));
+    }
+    *out = e;
+    return MM_OK;
+}
+
+static int ensemble_capture(mm_ensemble e) {
+    bool fresh = e->graph != nullptr && e->versions.size() == e->plans.size();
+    for (size_t i = 0; fresh && i < e->plans.size(); i++) fresh = e->versions[i] == e->plans[i]->version;
+    if (fresh) return MM_OK;
+    if (e->graph) { cudaGraphExecDestroy(e->graph); e->graph = nullptr; }
+    cudaStream_t cs;
+    CUCHK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    cudaError_t err = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+    if (err != cudaSuccess) { cudaStreamDestroy(cs); return set_err(MM_ERR_CUDA, "begin capture: %s", cudaGetErrorString(err)); }
+    int rc = MM_OK;
+    long long nodes = 0;
+    err = cudaEventRecord(e->fork, cs);
+    for (size_t i = 0; i < e->plans.size() && rc == MM_OK && err == cudaSuccess; i++) {
+        mm_plan p = e->plans[i];
+        err = cudaStreamWaitEvent(e->streams[i], e->fork, 0);
+        const long long before = p->launches;
+        for (int k = 0; k < e->K && rc == MM_OK && err == cudaSuccess; k++) rc = enqueue_attempt(p, e->streams[i]);
+        nodes += p->launches - before;
+        p->launches = before;
+        if (err == cudaSuccess) err = cudaEventRecord(e->joins[i], e->streams[i]);
+        if (err == cudaSuccess) err = cudaStreamWaitEvent(cs, e->joins[i], 0);
+    }
+    cudaGraph_t gr = nullptr;
+    cudaError_t e2 = cudaStreamEndCapture(cs, &gr);
+    cudaStreamDestroy(cs);
+    if (rc) { if (gr) cudaGraphDestroy(gr); return rc; }
+    if (err != cudaSuccess || e2 != cudaSuccess) {
+        if (gr) cudaGraphDestroy(gr);
+        return set_err(MM_ERR_CUDA, "ensemble capture: %s", cudaGetErrorString(err != cudaSuccess ? err : e2));
+    }
+    err = cudaGraphInstantiate(&e->graph, gr, 0);
+    cudaGraphDestroy(gr);
+    if (err != cudaSuccess) { e->graph = nullptr; return set_err(MM_ERR_CUDA, "instantiate: %s", cudaGetErrorString(err)); }
+    e->nodes = nodes;
+    e->versions.resize(e->plans.size());
+    for (size_t i = 0; i < e->plans.size(); i++) e->versions[i] = e->plans[i]->version;
+    return MM_OK;
+}
+
+static int ensemble_drive(mm_ensemble e, cudaStream_t st, double duration, long long nsteps) {
+    int rc = MM_OK;
+    size_t started = 0;
+    for (; started < e->plans.size() && rc == MM_OK; started++) {
+        mm_plan p = e->plans[started];
+        rc = start_run(p, st, duration, nsteps, 0, 0);
+        if (rc == MM_OK && p->run_until) rc = set_err(MM_ERR_STATE, "internal: run_until set");
+    }
+    if (rc == MM_OK) rc = ensemble_capture(e);
+    while (rc == MM_OK) {
+        bool active = false;
+        for (mm_plan p : e->plans) active = active || any_active(p);
+        if (!active) break;
+        CUCHK(cudaGraphLaunch(e->graph, st));
+        e->launches += e->nodes;
+        for (size_t i = 0; i < e->plans.size() && rc == MM_OK; i++) {
+            mm_plan p = e->plans[i];
+            CUCHK(cudaMemcpyAsync(p->hsum, p->dsum, sizeof(CtlSummary), cudaMemcpyDeviceToHost, st));
+        }
+        CUCHK(cudaStreamSynchronize(st));
+        for (size_t i = 0; i < e->plans.size() && rc == MM_OK; i++) {
+            mm_plan p = e->plans[i];
+            rc = summary_status(p);
+            for (int b = 0; b < p->nsim; b++) p->ctl_host[b].done = p->hsum->active == 0 ? 1 : 0;
+        }
+    }
+    for (size_t i = 0; i < started; i++) {
+        int rc2 = finish_run(e->plans[i], st);
+        if (rc == MM_OK) rc = rc2;
+    }
+    return rc;
+}
+
+extern "C" MM_API int mm_ensemble_steps(mm_ensemble e, long long n, mm_stream stream) {
+    if (!e) return set_err(MM_ERR_ARG, "null ensemble");
+    if (n <= 0) return MM_OK;
+    return ensemble_drive(e, (cudaStream_t)stream, 0, n);
+}
+
+extern "C" MM_API int mm_ensemble_run(mm_ensemble e, double duration, mm_stream stream) {
+    if (!e) return set_err(MM_ERR_ARG, "null ensemble");
+    if (!(duration > 0)) return MM_OK;
+    return ensemble_drive(e, (cudaStream_t)stream, duration, 0);
+}
+
+extern "C" MM_API long long mm_ensemble_launch_count(mm_ensemble e) { return e ? e->launches : 0; }

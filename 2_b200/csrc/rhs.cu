@@ -90,18 +90,21 @@ struct CellTerms {
 };
 
 // Effective field and torque at one cell.  Returns k (tau/gamma + STT/gamma).
+// m points at this simulation's state, i is the cell within the simulation, mo the
+// offset of the simulation's masks (0 when masks are shared), S its scalars.
 template <bool WANT_TERMS>
-__device__ __forceinline__ float3 cell_rhs(const FieldParams& P, const float* __restrict__ m, long long i, int z,
-                                           int y, int x, float3 hd, long long noise_step, float dt_th, float3& m0,
-                                           CellTerms* terms) {
+__device__ __forceinline__ float3 cell_rhs(const FieldParams& P, const SimScalars& S, const float* __restrict__ m,
+                                           long long i, long long mo, int z, int y, int x, float3 hd,
+                                           long long noise_step, float dt_th, float3& m0, CellTerms* terms) {
     const long long N = P.N;
+    const long long im = i + mo;
     m0 = make_float3(__ldg(m + i), __ldg(m + N + i), __ldg(m + 2 * N + i));
     float3 H = hd;
     if (WANT_TERMS) { terms->hd[0] = hd.x; terms->hd[1] = hd.y; terms->hd[2] = hd.z; }
     if (P.exchange) {
-        const int n0 = P.n[0], n1 = P.n[1], n2 = P.n[2];
+        const int n1 = P.n[1], n2 = P.n[2];
         const bool masked = P.msat_mask || P.aex_mask;
-        const float lex0 = masked ? fdiv_zero(mval(P.aex_mask, i), mval(P.msat_mask, i)) : 1.0f;
+        const float lex0 = masked ? fdiv_zero(mval(P.aex_mask, im), mval(P.msat_mask, im)) : 1.0f;
         float3 hex = make_float3(0.f, 0.f, 0.f);
         const int c[3] = {z, y, x};
         const long long str[3] = {(long long)n1 * n2, n2, 1};
@@ -114,10 +117,10 @@ __device__ __forceinline__ float3 cell_rhs(const FieldParams& P, const float* __
             long long ih = i + (long long)(hi - c[d]) * str[d];
             float l1 = 1.f, l2 = 1.f;
             if (masked) {
-                l1 = avg_geom_zero(lex0, fdiv_zero(mval(P.aex_mask, il), mval(P.msat_mask, il)));
-                l2 = avg_geom_zero(lex0, fdiv_zero(mval(P.aex_mask, ih), mval(P.msat_mask, ih)));
+                l1 = avg_geom_zero(lex0, fdiv_zero(mval(P.aex_mask, il + mo), mval(P.msat_mask, il + mo)));
+                l2 = avg_geom_zero(lex0, fdiv_zero(mval(P.aex_mask, ih + mo), mval(P.msat_mask, ih + mo)));
             }
-            const float f = P.ex_pre * P.cinv2[d];
+            const float f = S.ex_pre * P.cinv2[d];
             float3 a = make_float3(__ldg(m + il), __ldg(m + N + il), __ldg(m + 2 * N + il));
             float3 b = make_float3(__ldg(m + ih), __ldg(m + N + ih), __ldg(m + 2 * N + ih));
             hex.x += f * (l1 * (a.x - m0.x) + l2 * (b.x - m0.x));
@@ -128,54 +131,54 @@ __device__ __forceinline__ float3 cell_rhs(const FieldParams& P, const float* __
         if (WANT_TERMS) { terms->hex[0] = hex.x; terms->hex[1] = hex.y; terms->hex[2] = hex.z; }
     }
     if (P.zeeman) {
-        float3 hz = make_float3(P.hz[0] * mval(P.bext_mask[0], i), P.hz[1] * mval(P.bext_mask[1], i),
-                                P.hz[2] * mval(P.bext_mask[2], i));
+        float3 hz = make_float3(S.hz[0] * mval(P.bext_mask[0], im), S.hz[1] * mval(P.bext_mask[1], im),
+                                S.hz[2] * mval(P.bext_mask[2], im));
         H.x += hz.x; H.y += hz.y; H.z += hz.z;
         if (WANT_TERMS) { terms->hz[0] = hz.x; terms->hz[1] = hz.y; terms->hz[2] = hz.z; }
     }
     if (P.anis) {
-        float msm = P.msat_mask ? __ldg(P.msat_mask + i) : 1.0f;
+        float msm = P.msat_mask ? __ldg(P.msat_mask + im) : 1.0f;
         if (msm == 0.0f) msm = 1.0f;
-        float k2 = (P.kmul / msm) * mval(P.ku_mask, i);
-        float ux = P.anisu[0] * mval(P.anisu_mask[0], i);
-        float uy = P.anisu[1] * mval(P.anisu_mask[1], i);
-        float uz = P.anisu[2] * mval(P.anisu_mask[2], i);
+        float k2 = (S.kmul / msm) * mval(P.ku_mask, im);
+        float ux = S.anisu[0] * mval(P.anisu_mask[0], im);
+        float uy = S.anisu[1] * mval(P.anisu_mask[1], im);
+        float uz = S.anisu[2] * mval(P.anisu_mask[2], im);
         float mu = m0.x * ux + m0.y * uy + m0.z * uz;
         float3 ha = make_float3(k2 * mu * ux, k2 * mu * uy, k2 * mu * uz);
         H.x += ha.x; H.y += ha.y; H.z += ha.z;
         if (WANT_TERMS) { terms->han[0] = ha.x; terms->han[1] = ha.y; terms->han[2] = ha.z; }
     }
     if (P.thermal) {
-        float ms = mval(P.msat_mask, i);
+        float ms = mval(P.msat_mask, im);
         float3 ht = make_float3(0.f, 0.f, 0.f);
         if (ms != 0.0f) {
             float eta[3];
-            thermal_normals(P.seed, i, noise_step, eta);
-            float a = mval(P.alpha_mask, i), tm = mval(P.temp_mask, i);
-            float den = (float)(P.therm_den * (double)dt_th);
-            float sc = sqrtf((a * tm * P.therm_num) / (den * ms));
+            thermal_normals(S.seed, i, noise_step, eta);
+            float a = mval(P.alpha_mask, im), tm = mval(P.temp_mask, im);
+            float den = (float)(S.therm_den * (double)dt_th);
+            float sc = sqrtf((a * tm * S.therm_num) / (den * ms));
             ht = make_float3(eta[0] * sc, eta[1] * sc, eta[2] * sc);
         }
         H.x += ht.x; H.y += ht.y; H.z += ht.z;
         if (WANT_TERMS) { terms->hth[0] = ht.x; terms->hth[1] = ht.y; terms->hth[2] = ht.z; }
     }
     // LLG torque
-    const float al = P.alpha * mval(P.alpha_mask, i);
+    const float al = S.alpha * mval(P.alpha_mask, im);
     float cx = m0.y * H.z - H.y * m0.z, cy = -m0.x * H.z + H.x * m0.z, cz = m0.x * H.y - H.x * m0.y;
     float dx = -m0.y * cz + cy * m0.z, dy = m0.x * cz - cx * m0.z, dz = -m0.x * cy + cx * m0.y;
     float g = 1.0f / (1.0f + al * al);
     float3 k = make_float3(g * (cx + dx * al), g * (cy + dy * al), g * (cz + dz * al));
     if (P.zhangli) {
-        float msat = P.msat_mask ? __ldg(P.msat_mask + i) : 1.0f;
-        float3 j0 = make_float3(P.j_mask[0] ? __ldg(P.j_mask[0] + i) * P.jmul[0] : P.jmul[0],
-                                P.j_mask[1] ? __ldg(P.j_mask[1] + i) * P.jmul[1] : P.jmul[1],
-                                P.j_mask[2] ? __ldg(P.j_mask[2] + i) * P.jmul[2] : P.jmul[2]);
+        float msat = P.msat_mask ? __ldg(P.msat_mask + im) : 1.0f;
+        float3 j0 = make_float3(P.j_mask[0] ? __ldg(P.j_mask[0] + im) * P.jmul[0] : P.jmul[0],
+                                P.j_mask[1] ? __ldg(P.j_mask[1] + im) * P.jmul[1] : P.jmul[1],
+                                P.j_mask[2] ? __ldg(P.j_mask[2] + im) * P.jmul[2] : P.jmul[2]);
         float njn = sqrtf(j0.x * j0.x + j0.y * j0.y + j0.z * j0.z);
         if (msat != 0.0f && njn != 0.0f) {
             msat = 1.0f / msat;
-            float PP = P.zl_pol_mask ? __ldg(P.zl_pol_mask + i) : 1.0f;
-            float pred = njn * PP * P.zl_pre;
-            float ee = P.xi_mask ? __ldg(P.xi_mask + i) * P.xi : P.xi;
+            float PP = P.zl_pol_mask ? __ldg(P.zl_pol_mask + im) : 1.0f;
+            float pred = njn * PP * S.zl_pre;
+            float ee = P.xi_mask ? __ldg(P.xi_mask + im) * P.xi : P.xi;
             pred = pred / ((1.0f + ee * ee) * (1.0f + al * al));
             float pret = pred * (ee - al);
             pred = pred * (1.0f + ee * al);
@@ -209,19 +212,19 @@ __device__ __forceinline__ float3 cell_rhs(const FieldParams& P, const float* __
         }
     }
     if (P.slonczewski) {
-        float Ms = P.msat_mask ? __ldg(P.msat_mask + i) : 1.0f;
-        float3 J = make_float3(P.j_mask[0] ? __ldg(P.j_mask[0] + i) * P.jmul[0] : P.jmul[0],
-                               P.j_mask[1] ? __ldg(P.j_mask[1] + i) * P.jmul[1] : P.jmul[1],
-                               P.j_mask[2] ? __ldg(P.j_mask[2] + i) * P.jmul[2] : P.jmul[2]);
+        float Ms = P.msat_mask ? __ldg(P.msat_mask + im) : 1.0f;
+        float3 J = make_float3(P.j_mask[0] ? __ldg(P.j_mask[0] + im) * P.jmul[0] : P.jmul[0],
+                               P.j_mask[1] ? __ldg(P.j_mask[1] + im) * P.jmul[1] : P.jmul[1],
+                               P.j_mask[2] ? __ldg(P.j_mask[2] + im) * P.jmul[2] : P.jmul[2]);
         float nJn = sqrtf(J.x * J.x + J.y * J.y + J.z * J.z);
-        float tfl = P.t_fl_mask ? __ldg(P.t_fl_mask + i) * P.t_fl : P.t_fl;
+        float tfl = P.t_fl_mask ? __ldg(P.t_fl_mask + im) * P.t_fl : P.t_fl;
         if (nJn != 0.0f && Ms != 0.0f && tfl != 0.0f) {
             tfl = 1.0f / tfl;
             Ms = 1.0f / Ms;
-            float prex = P.sl_beta_prime * Ms, prey = P.sl_pre_fld * Ms;
-            float3 p = make_float3(P.p_mask[0] ? P.p[0] * __ldg(P.p_mask[0] + i) : P.p[0],
-                                   P.p_mask[1] ? P.p[1] * __ldg(P.p_mask[1] + i) : P.p[1],
-                                   P.p_mask[2] ? P.p[2] * __ldg(P.p_mask[2] + i) : P.p[2]);
+            float prex = S.sl_beta_prime * Ms, prey = S.sl_pre_fld * Ms;
+            float3 p = make_float3(P.p_mask[0] ? P.p[0] * __ldg(P.p_mask[0] + im) : P.p[0],
+                                   P.p_mask[1] ? P.p[1] * __ldg(P.p_mask[1] + im) : P.p[1],
+                                   P.p_mask[2] ? P.p[2] * __ldg(P.p_mask[2] + im) : P.p[2]);
             float pl = sqrtf(p.x * p.x + p.y * p.y + p.z * p.z);
             float pinv = (pl != 0.0f) ? 1.0f / pl : 0.0f;
             p.x *= pinv; p.y *= pinv; p.z *= pinv;
@@ -234,13 +237,13 @@ __device__ __forceinline__ float3 cell_rhs(const FieldParams& P, const float* __
             float nj = nJn * Jsign;
             prex *= nj; prey *= nj;
             prex *= tfl; prey *= tfl;
-            float lam = P.lambda_mask ? P.lambda * __ldg(P.lambda_mask + i) : P.lambda;
+            float lam = P.lambda_mask ? P.lambda * __ldg(P.lambda_mask + im) : P.lambda;
             float l2 = lam * lam;
             float eps = l2 / ((l2 + 1.0f) + (l2 - 1.0f) * pdotm);
             prex *= eps;
             float af = 1.0f / (1.0f + al * al);
-            prex *= P.sl_pol_mask ? __ldg(P.sl_pol_mask + i) : 1.0f;
-            prey *= P.eps_prime_mask ? __ldg(P.eps_prime_mask + i) : 1.0f;
+            prex *= P.sl_pol_mask ? __ldg(P.sl_pol_mask + im) : 1.0f;
+            prey *= P.eps_prime_mask ? __ldg(P.eps_prime_mask + im) : 1.0f;
             float f1 = (prex - al * prey) * af;
             float f2 = (prey - al * prex) * af;
             k.x += P.inv_gamma * (f1 * mxpxm.x + f2 * pxm.x);
@@ -279,15 +282,17 @@ struct ResolvedOp {
     float ek[MM_MAXK];
 };
 
-__device__ __forceinline__ void resolve_op(const StageOp& op, int cur, float h, ResolvedOp& r) {
-    r.k_out = op.k_out.get(cur);
-    r.base = op.base.get(cur);
-    r.next = op.next.get(cur);
+// off: this simulation's offset into the per-cell arrays
+__device__ __forceinline__ float* at_off(float* q, long long off) { return q ? q + off : nullptr; }
+__device__ __forceinline__ void resolve_op(const StageOp& op, int cur, float h, ResolvedOp& r, long long off) {
+    r.k_out = at_off(op.k_out.get(cur), off);
+    r.base = at_off(op.base.get(cur), off);
+    r.next = at_off(op.next.get(cur), off);
 #pragma unroll
     for (int j = 0; j < MM_MAXK; j++) {
-        r.kp[j] = (j < op.nk) ? op.kp[j].get(cur) : nullptr;
+        r.kp[j] = (j < op.nk) ? at_off(op.kp[j].get(cur), off) : nullptr;
         r.ak[j] = (j < op.nk) ? (float)(op.ak[j] * (double)h) : 0.f;
-        r.ep[j] = (j < op.ne) ? op.ep[j].get(cur) : nullptr;
+        r.ep[j] = (j < op.ne) ? at_off(op.ep[j].get(cur), off) : nullptr;
         r.ek[j] = (j < op.ne) ? (float)op.ek[j] : 0.f;
     }
 }
@@ -300,7 +305,7 @@ struct ThreadRed {
 };
 
 __device__ __forceinline__ void cell_post(const FieldParams& P, const StageOp& op, const ResolvedOp& r, long long i,
-                                          float3 m0, float3 k, ThreadRed& tr) {
+                                          long long mo, float3 m0, float3 k, ThreadRed& tr) {
     const long long N = P.N;
     if (!(isfinite(k.x) && isfinite(k.y) && isfinite(k.z))) tr.bad = 1;
     if (r.k_out) {
@@ -320,7 +325,7 @@ __device__ __forceinline__ void cell_post(const FieldParams& P, const StageOp& o
             v.z += r.ak[j] * kj.z;
         }
         // normalize.cu:14-42 with the Msat mask as norm map
-        float norm = P.msat_mask ? __ldg(P.msat_mask + i) : 1.0f;
+        float norm = P.msat_mask ? __ldg(P.msat_mask + i + mo) : 1.0f;
         float mn = sqrtf(v.x * v.x + v.y * v.y + v.z * v.z);
         float sc = (norm == 0.0f) ? 0.0f : 1.0f;
         sc = (mn != 0.0f) ? sc / mn : 0.0f;
@@ -396,17 +401,19 @@ __device__ void block_reduce_publish(ThreadRed tr, const StageOp& op, DevCtl* ct
                 e[q] = ksum_merge(e[q], b);
             }
         }
+        // ctl is this simulation's control block; tq_out and red are indexed by simulation
         if (ctl) {
             if (op.want_tq) atomicMax(&ctl->tq_bits, __float_as_uint(tq));
             if (op.ne > 0) atomicMax(&ctl->err_bits, __float_as_uint(err));
             if (bad) atomicExch(&ctl->status, (int)MM_ERR_NAN);
         } else if (tq_out && op.want_tq) {
-            atomicMax(tq_out, __float_as_uint(tq));
+            atomicMax(tq_out + blockIdx.y, __float_as_uint(tq));
         }
         if (op.want_energy && red) {
+            const long long slot = (long long)blockIdx.y * gridDim.x + blockIdx.x;
             for (int q = 0; q < 4; q++) {
-                red[blockIdx.x * 8 + 2 * q] = e[q].s;
-                red[blockIdx.x * 8 + 2 * q + 1] = e[q].c;
+                red[slot * 8 + 2 * q] = e[q].s;
+                red[slot * 8 + 2 * q + 1] = e[q].c;
             }
         }
     }
@@ -422,37 +429,67 @@ __device__ __forceinline__ void write_terms(float* const* dbg, long long N, long
             dbg[5][c * N + i] = t.hd[c] + t.hex[c] + t.han[c] + t.hz[c] + t.hth[c];
 }
 
+// i: cell within the simulation; m, r and the dbg outputs already point at the simulation
 template <bool TERMS>
-__device__ __forceinline__ void process_cell(const EpiArgs& A, const float* m, const ResolvedOp& r, long long i,
+__device__ __forceinline__ void process_cell(const EpiArgs& A, const SimScalars& S, const float* m,
+                                             const ResolvedOp& r, float* const* dbg, long long i, long long mo,
                                              int z, int y, int x, float3 hd, long long ns, float dtth,
                                              ThreadRed& tr) {
     float3 m0;
     if (TERMS) {
         CellTerms t = {};
-        float3 k = cell_rhs<true>(A.P, m, i, z, y, x, hd, ns, dtth, m0, &t);
+        float3 k = cell_rhs<true>(A.P, S, m, i, mo, z, y, x, hd, ns, dtth, m0, &t);
         if (A.op.want_energy) energy_acc(A.P, i, m0, t, tr);
-        write_terms(A.dbg, A.P.N, i, t);
-        cell_post(A.P, A.op, r, i, m0, k, tr);
+        write_terms(dbg, A.P.N, i, t);
+        cell_post(A.P, A.op, r, i, mo, m0, k, tr);
     } else {
-        float3 k = cell_rhs<false>(A.P, m, i, z, y, x, hd, ns, dtth, m0, nullptr);
-        cell_post(A.P, A.op, r, i, m0, k, tr);
+        float3 k = cell_rhs<false>(A.P, S, m, i, mo, z, y, x, hd, ns, dtth, m0, nullptr);
+        cell_post(A.P, A.op, r, i, mo, m0, k, tr);
     }
+}
+
+// Per-block context of one simulation for the epilogue kernels.  BATCH = false is the
+// single-simulation plan: simulation 0, scalars straight from the kernel parameters, no
+// offsets.  BATCH = true takes the simulation from blockIdx.y and its scalars from
+// S (staged in shared memory by the kernel).
+template <bool TERMS, bool BATCH>
+__device__ __forceinline__ void epilogue_cells_begin(const EpiArgs& A, const DevCtl*& ctl, ResolvedOp& r,
+                                                     const float*& m, float** dbg, long long& mo, long long& ns,
+                                                     float& dtth) {
+    const int sim = BATCH ? (int)blockIdx.y : 0;
+    const long long off = BATCH ? (long long)sim * A.P.bstride : 0;
+    mo = BATCH ? (long long)sim * A.P.mask_bstride : 0;
+    ctl = A.ctl ? A.ctl + sim : nullptr;
+    const int cur = ctl ? ctl->cur : 0;
+    const float h = ctl ? (float)ctl->h : 0.f;
+    ns = ctl ? ctl->noise_step : A.noise_step;
+    dtth = ctl ? (float)(ctl->dt_thermal > 0 ? ctl->dt_thermal : ctl->dt) : (float)A.dt_thermal;
+    resolve_op(A.op, cur, h, r, off);
+    m = A.op.m_in.get(cur) + off;
+    if (TERMS)
+        for (int q = 0; q < 6; q++) dbg[q] = at_off(A.dbg[q], off);
+}
+
+template <bool BATCH>
+__device__ __forceinline__ const SimScalars& pick_scalars(const SimScalars& staged, const SimScalars& single) {
+    if constexpr (BATCH) return staged;
+    else return single;
 }
 
 // ---------------------------------------------------------------- C2R row pass + epilogue
 // Cells of the block's rows; H_demag of (row, c) at cell x is element x>>1 (real part for
 // even x, imaginary part for odd x) of shared-memory line (lrow*3 + c), stride LS.
-template <bool TERMS, bool PADDED>
-__device__ __forceinline__ void epilogue_rows(const EpiArgs& A, const float2* sm, int LS, int row0, int nrow_here) {
-    const DevCtl* ctl = A.ctl;
+template <bool TERMS, bool PADDED, bool BATCH>
+__device__ __forceinline__ void epilogue_rows(const EpiArgs& A, const SimScalars& S, const float2* sm, int LS,
+                                              int row0, int nrow_here) {
     const int n1 = A.P.n[1], n2 = A.P.n[2];
-    const int cur = ctl ? ctl->cur : 0;
-    const float h = ctl ? (float)ctl->h : 0.f;
-    const long long ns = ctl ? ctl->noise_step : A.noise_step;
-    const float dtth = ctl ? (float)(ctl->dt_thermal > 0 ? ctl->dt_thermal : ctl->dt) : (float)A.dt_thermal;
+    const DevCtl* ctl;
     ResolvedOp r;
-    resolve_op(A.op, cur, h, r);
-    const float* m = A.op.m_in.get(cur);
+    const float* m;
+    float* dbg[6];
+    long long mo, ns;
+    float dtth;
+    epilogue_cells_begin<TERMS, BATCH>(A, ctl, r, m, dbg, mo, ns, dtth);
     ThreadRed tr = {0.f, 0.f, 0, {{0.f, 0.f}, {0.f, 0.f}, {0.f, 0.f}, {0.f, 0.f}}};
     // (lrow, x) of element e = threadIdx.x + k*blockDim.x, advanced without divisions
     const int total = nrow_here * n2;
@@ -467,7 +504,7 @@ __device__ __forceinline__ void epilogue_rows(const EpiArgs& A, const float2* sm
         const float2 v1 = sm[(lrow * 3 + 1) * LS + pi];
         const float2 v2 = sm[(lrow * 3 + 2) * LS + pi];
         const float3 hd = (x & 1) ? make_float3(v0.y, v1.y, v2.y) : make_float3(v0.x, v1.x, v2.x);
-        process_cell<TERMS>(A, m, r, i, z, y, x, hd, ns, dtth, tr);
+        process_cell<TERMS>(A, S, m, r, dbg, i, mo, z, y, x, hd, ns, dtth, tr);
         // advance by blockDim.x cells
         x += dx;
         int adv = dr;
@@ -477,15 +514,16 @@ __device__ __forceinline__ void epilogue_rows(const EpiArgs& A, const float2* sm
         y += adv;
         while (y >= n1) { y -= n1; z++; }
     }
-    block_reduce_publish(tr, A.op, A.ctl, A.tq_out, A.red);
+    block_reduce_publish(tr, A.op, const_cast<DevCtl*>(ctl), A.tq_out, A.red);
 }
 
-// Stockham variant (any power-of-two M up to 2048)
+// Stockham variant (any power-of-two M up to 2048; single-simulation plans)
 template <int M, bool TERMS>
 __global__ void __launch_bounds__(512) xinv_epi_kernel(const float2* __restrict__ S, int hp, int L1,
                                                        const float2* __restrict__ tw, EpiArgs A) {
-    const DevCtl* ctl = A.ctl;
+    const DevCtl* ctl = A.ctl ? A.ctl + blockIdx.y : nullptr;
     if (skip_eval(ctl, A.skip_retry)) return;
+    S += blockIdx.y * A.spec_bstride;
     constexpr int TPL = tpl(M);
     constexpr int LL = line_len(M);
     extern __shared__ unsigned char smem_raw[];
@@ -515,7 +553,7 @@ __global__ void __launch_bounds__(512) xinv_epi_kernel(const float2* __restrict_
     __syncthreads();
     fft_line<M, +1, float2>(xl, t, active, tw);
     const int row0 = blockIdx.x * rpb;
-    epilogue_rows<TERMS, true>(A, sm, LL, row0, min(rpb, nrows - row0));
+    epilogue_rows<TERMS, true, false>(A, A.P.s, sm, LL, row0, min(rpb, nrows - row0));
 }
 
 // Four-step variant (4 <= M <= 1024): the pre-processed spectrum goes straight from
@@ -526,11 +564,14 @@ __host__ __device__ constexpr int xinv4_rpb() {
     return (384 / (3 * FS<M>::P2)) > 0 ? 384 / (3 * FS<M>::P2) : 1;
 }
 
-template <int M, bool TERMS>
+template <int M, bool TERMS, bool BATCH>
 __global__ void __launch_bounds__(384) xinv4_epi_kernel(const float2* __restrict__ S, int hp, int L1,
                                                         const float2* __restrict__ tw, EpiArgs A) {
-    const DevCtl* ctl = A.ctl;
+    const DevCtl* ctl = A.ctl ? A.ctl + blockIdx.y : nullptr;
     if (skip_eval(ctl, A.skip_retry)) return;
+    S += blockIdx.y * A.spec_bstride;
+    __shared__ SimScalars s_sim;  // this simulation's scalars (BATCH); covered by the barriers below
+    if (BATCH && threadIdx.x == 0) s_sim = A.P.sims[blockIdx.y];
     using F = FS<M>;
     constexpr int RPB = xinv4_rpb<M>();
     extern __shared__ unsigned char smem_raw[];
@@ -572,37 +613,43 @@ __global__ void __launch_bounds__(384) xinv4_epi_kernel(const float2* __restrict
     }
     __syncthreads();
     const int row0 = blockIdx.x * RPB;
-    epilogue_rows<TERMS, false>(A, sm, F::LBUF, row0, min(RPB, nrows - row0));
+    epilogue_rows<TERMS, false, BATCH>(A, pick_scalars<BATCH>(s_sim, A.P.s), sm, F::LBUF, row0,
+                                       min(RPB, nrows - row0));
 }
 
 // ---------------------------------------------------------------- epilogue without demag
-template <bool TERMS>
+template <bool TERMS, bool BATCH>
 __global__ void __launch_bounds__(256) local_epi_kernel(EpiArgs A) {
-    const DevCtl* ctl = A.ctl;
-    if (skip_eval(ctl, A.skip_retry)) return;
+    if (skip_eval(A.ctl ? A.ctl + blockIdx.y : nullptr, A.skip_retry)) return;
     const int n1 = A.P.n[1], n2 = A.P.n[2];
-    const int cur = ctl ? ctl->cur : 0;
-    const float h = ctl ? (float)ctl->h : 0.f;
-    const long long ns = ctl ? ctl->noise_step : A.noise_step;
-    const float dtth = ctl ? (float)(ctl->dt_thermal > 0 ? ctl->dt_thermal : ctl->dt) : (float)A.dt_thermal;
+    __shared__ SimScalars s_sim;
+    if (BATCH) {
+        if (threadIdx.x == 0) s_sim = A.P.sims[blockIdx.y];
+        __syncthreads();
+    }
+    const SimScalars& S = pick_scalars<BATCH>(s_sim, A.P.s);
+    const DevCtl* ctl;
     ResolvedOp r;
-    resolve_op(A.op, cur, h, r);
-    const float* m = A.op.m_in.get(cur);
+    const float* m;
+    float* dbg[6];
+    long long mo, ns;
+    float dtth;
+    epilogue_cells_begin<TERMS, BATCH>(A, ctl, r, m, dbg, mo, ns, dtth);
     ThreadRed tr = {0.f, 0.f, 0, {{0.f, 0.f}, {0.f, 0.f}, {0.f, 0.f}, {0.f, 0.f}}};
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < A.P.N;
          i += (long long)gridDim.x * blockDim.x) {
         const int x = (int)(i % n2);
         const long long zy = i / n2;
         const int y = (int)(zy % n1), z = (int)(zy / n1);
-        process_cell<TERMS>(A, m, r, i, z, y, x, make_float3(0.f, 0.f, 0.f), ns, dtth, tr);
+        process_cell<TERMS>(A, S, m, r, dbg, i, mo, z, y, x, make_float3(0.f, 0.f, 0.f), ns, dtth, tr);
     }
-    block_reduce_publish(tr, A.op, A.ctl, A.tq_out, A.red);
+    block_reduce_publish(tr, A.op, const_cast<DevCtl*>(ctl), A.tq_out, A.red);
 }
 
 // ---------------------------------------------------------------- launchers
 template <int M, bool TERMS>
 static cudaError_t launch_xinv_t(const float2* S, int hp, int L1, const float2* tw, const EpiArgs& A, cudaStream_t st,
-                                 int* nblocks) {
+                                 int* nblocks, int nsim) {
     constexpr int TPL = tpl(M);
     int rpb = (3 * TPL >= 384) ? 1 : 384 / (3 * TPL);
     size_t smem = (size_t)rpb * 3 * line_len(M) * sizeof(float2);
@@ -617,18 +664,18 @@ static cudaError_t launch_xinv_t(const float2* S, int hp, int L1, const float2* 
     int threads = rpb * 3 * TPL;
     if (threads < 32) threads = 32;
     *nblocks = blocks;
-    xinv_epi_kernel<M, TERMS><<<blocks, threads, smem, st>>>(S, hp, L1, tw, A);
+    xinv_epi_kernel<M, TERMS><<<dim3((unsigned)blocks, (unsigned)nsim), threads, smem, st>>>(S, hp, L1, tw, A);
     return cudaGetLastError();
 }
 
-template <int M, bool TERMS>
+template <int M, bool TERMS, bool BATCH>
 static cudaError_t launch_xinv4_t(const float2* S, int hp, int L1, const float2* tw, const EpiArgs& A,
-                                  cudaStream_t st, int* nblocks) {
+                                  cudaStream_t st, int* nblocks, int nsim) {
     constexpr int RPB = xinv4_rpb<M>();
     const size_t smem = (size_t)(RPB * 3 * FS<M>::LBUF + FS<M>::TWT) * sizeof(float2);
     if (smem > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(xinv4_epi_kernel<M, TERMS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)smem);
+        cudaError_t e = cudaFuncSetAttribute(xinv4_epi_kernel<M, TERMS, BATCH>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
     }
     const int nrows = A.P.n[0] * A.P.n[1];
@@ -636,7 +683,8 @@ static cudaError_t launch_xinv4_t(const float2* S, int hp, int L1, const float2*
     int threads = RPB * 3 * FS<M>::P2;
     if (threads < 32) threads = 32;
     *nblocks = blocks;
-    xinv4_epi_kernel<M, TERMS><<<blocks, threads, smem, st>>>(S, hp, L1, tw, A);
+    xinv4_epi_kernel<M, TERMS, BATCH><<<dim3((unsigned)blocks, (unsigned)nsim), threads, smem, st>>>(S, hp, L1, tw,
+                                                                                                     A);
     return cudaGetLastError();
 }
 
@@ -660,40 +708,52 @@ int xinv_blocks(int M, int n0n1) {
 }
 
 cudaError_t launch_xinv_epi(int M, const float2* S, int hp, int L1, const float2* tw, const EpiArgs& A, bool terms,
-                            cudaStream_t st, int* nblocks) {
+                            cudaStream_t st, int* nblocks, int nsim) {
     if (use_xinv4(M)) {
         switch (M) {
 #define X(m)                                                                      \
     case m:                                                                       \
-        return terms ? launch_xinv4_t<m, true>(S, hp, L1, tw, A, st, nblocks)     \
-                     : launch_xinv4_t<m, false>(S, hp, L1, tw, A, st, nblocks);
+        if (nsim > 1)                                                                   \
+            return terms ? launch_xinv4_t<m, true, true>(S, hp, L1, tw, A, st, nblocks, nsim)  \
+                         : launch_xinv4_t<m, false, true>(S, hp, L1, tw, A, st, nblocks, nsim); \
+        return terms ? launch_xinv4_t<m, true, false>(S, hp, L1, tw, A, st, nblocks, 1)     \
+                     : launch_xinv4_t<m, false, false>(S, hp, L1, tw, A, st, nblocks, 1);
             X(4) X(8) X(16) X(32) X(64) X(128) X(256) X(512) X(1024)
 #undef X
         }
     }
+    if (nsim > 1) return cudaErrorNotSupported;  // batched plans use the four-step pass
     switch (M) {
 #define X(m)                                                                      \
     case m:                                                                       \
-        return terms ? launch_xinv_t<m, true>(S, hp, L1, tw, A, st, nblocks)      \
-                     : launch_xinv_t<m, false>(S, hp, L1, tw, A, st, nblocks);
+        return terms ? launch_xinv_t<m, true>(S, hp, L1, tw, A, st, nblocks, nsim)      \
+                     : launch_xinv_t<m, false>(S, hp, L1, tw, A, st, nblocks, nsim);
         X(1) X(2) X(4) X(8) X(16) X(32) X(64) X(128) X(256) X(512) X(1024) X(2048)
 #undef X
         default: return cudaErrorInvalidValue;
     }
 }
 
-int local_blocks(long long N) {
+// blocks per simulation of the grid-stride cell kernels (about 16 per SM in total)
+int local_blocks(long long N, int nsim) {
     long long b = (N + 255) / 256;
-    if (b > 148 * 16) b = 148 * 16;
+    long long cap = (148 * 16 + nsim - 1) / nsim;
+    if (b > cap) b = cap;
     if (b < 1) b = 1;
     return (int)b;
 }
 
-cudaError_t launch_local_epi(const EpiArgs& A, bool terms, cudaStream_t st, int* nblocks) {
-    int b = local_blocks(A.P.N);
+cudaError_t launch_local_epi(const EpiArgs& A, bool terms, cudaStream_t st, int* nblocks, int nsim) {
+    int b = local_blocks(A.P.N, nsim);
     *nblocks = b;
-    if (terms) local_epi_kernel<true><<<b, 256, 0, st>>>(A);
-    else local_epi_kernel<false><<<b, 256, 0, st>>>(A);
+    const dim3 grid((unsigned)b, (unsigned)nsim);
+    if (nsim > 1) {
+        if (terms) local_epi_kernel<true, true><<<grid, 256, 0, st>>>(A);
+        else local_epi_kernel<false, true><<<grid, 256, 0, st>>>(A);
+    } else {
+        if (terms) local_epi_kernel<true, false><<<grid, 256, 0, st>>>(A);
+        else local_epi_kernel<false, false><<<grid, 256, 0, st>>>(A);
+    }
     return cudaGetLastError();
 }
 

@@ -4,4 +4,4 @@
 API (load/setv/run/...) mirroring src/python/mumax2.py lives in `engine`.
 """
 from . import _native  # noqa: F401
-from .plan import Plan  # noqa: F401
+from .plan import Ensemble, Plan  # noqa: F401

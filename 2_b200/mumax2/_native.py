@@ -56,6 +56,35 @@ class MMStats(C.Structure):
     ]
 
 
+class MMSim(C.Structure):
+    """mm_sim of include/mm_b200.h: the scalars of one simulation of a batched plan."""
+    _fields_ = [
+        ("msat", C.c_double), ("aex", C.c_double), ("alpha", C.c_double), ("bext", C.c_double * 3),
+        ("ku", C.c_double), ("anisu", C.c_double * 3), ("temp", C.c_double), ("seed", C.c_ulonglong),
+    ]
+
+
+SIM_KEYS = ["msat", "aex", "alpha", "bext", "ku", "anisu", "temp", "seed"]
+
+
+def make_sims(problem, sims):
+    """Array of MMSim: each entry of `sims` (dicts) overrides the problem's scalars."""
+    arr = (MMSim * len(sims))()
+    for b, d in enumerate(sims):
+        q = dict(problem)
+        q.update(d)
+        s = arr[b]
+        s.msat = float(q.get("msat", 8e5))
+        s.aex = float(q.get("aex", 1.3e-11))
+        s.alpha = float(q.get("alpha", 0.02))
+        s.bext[:] = [float(x) for x in q.get("bext", (0, 0, 0))]
+        s.ku = float(q.get("ku", 0.0))
+        s.anisu[:] = [float(x) for x in q.get("anisu", (0, 0, 1))]
+        s.temp = float(q.get("temp", 0.0))
+        s.seed = int(q.get("seed", 0))
+    return arr
+
+
 class MMError(RuntimeError):
     def __init__(self, code, msg):
         super().__init__(f"mm_b200 error {code}: {msg}")
@@ -90,6 +119,18 @@ _PROTOS = {
     "mm_profile_eval": (C.c_int, [C.c_void_p, C.c_int, DP, C.POINTER(C.c_int), C.c_void_p]),
     "mm_plan_geometry": (C.c_int, [C.c_void_p, C.c_int * 12]),
     "mm_average_noalloc": (C.c_int, [C.c_void_p, C.c_longlong, C.c_void_p, C.c_void_p]),
+    "mm_plan_create_batch": (C.c_int, [C.POINTER(MMProblem), C.c_int, C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]),
+    "mm_plan_nsim": (C.c_int, [C.c_void_p]),
+    "mm_batch_set_sims": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "mm_batch_stats": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "mm_batch_maxtorque": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "mm_batch_average": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "mm_batch_energy": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "mm_ensemble_create": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
+    "mm_ensemble_destroy": (C.c_int, [C.c_void_p]),
+    "mm_ensemble_steps": (C.c_int, [C.c_void_p, C.c_longlong, C.c_void_p]),
+    "mm_ensemble_run": (C.c_int, [C.c_void_p, C.c_double, C.c_void_p]),
+    "mm_ensemble_launch_count": (C.c_longlong, [C.c_void_p]),
 }
 
 

@@ -2,7 +2,8 @@
 
 Device memory for masks and state lives in torch CUDA tensors (plumbing only); all
 computation runs in libmm_b200.so.  Arrays are in the reference's internal axis
-order (Z,Y,X), SoA [comp][n0][n1][n2].
+order (Z,Y,X), SoA [comp][n0][n1][n2]; a batched plan (`sims` given) holds nsim such
+blocks one after the other, [sim][comp][n0][n1][n2].
 """
 import ctypes as C
 
@@ -23,7 +24,11 @@ def _ptr(t):
 
 
 class Plan:
-    def __init__(self, problem, masks=None, device=0):
+    """One simulation, or nsim = len(sims) simulations of one geometry when `sims` (a list
+    of dicts overriding msat, aex, alpha, bext, ku, anisu, temp, seed) is given.  Masks are
+    shared by all simulations unless masks_per_sim, in which case each holds nsim x N."""
+
+    def __init__(self, problem, masks=None, device=0, sims=None, masks_per_sim=False):
         torch = _torch()
         self.torch = torch
         self.device = torch.device("cuda", device) if isinstance(device, int) else torch.device(device)
@@ -31,12 +36,18 @@ class Plan:
         self.problem = dict(problem)
         n = self.problem["n"]
         self.N = int(n[0]) * int(n[1]) * int(n[2])
+        self.nsim = len(sims) if sims else 1
         self._masks = {}
         self._mask_ptrs = {}
         self._upload_masks(masks or {})
         self._struct = nat.make_problem(self.problem, self._mask_ptrs)
         h = C.c_void_p()
-        nat.check(nat.lib().mm_plan_create(C.byref(self._struct), C.byref(h)))
+        if sims:
+            self._sims = nat.make_sims(self.problem, sims)
+            nat.check(nat.lib().mm_plan_create_batch(C.byref(self._struct), self.nsim, C.cast(self._sims, C.c_void_p),
+                                                     1 if masks_per_sim else 0, C.byref(h)))
+        else:
+            nat.check(nat.lib().mm_plan_create(C.byref(self._struct), C.byref(h)))
         self.h = h
         self._solver = None
 
@@ -92,7 +103,8 @@ class Plan:
     def fields(self, m, noise_step=0, dt_thermal=0.0):
         torch = self.torch
         md = self._dev(m)
-        out = {k: torch.zeros(3 * self.N, device=self.device) for k in ["demag", "ex", "anis", "zee", "therm", "eff"]}
+        out = {k: torch.zeros(3 * self.N * self.nsim, device=self.device)
+               for k in ["demag", "ex", "anis", "zee", "therm", "eff"]}
         nat.check(nat.lib().mm_fields(self.h, _ptr(md), noise_step, dt_thermal, _ptr(out["demag"]), _ptr(out["ex"]),
                                       _ptr(out["anis"]), _ptr(out["zee"]), _ptr(out["therm"]), _ptr(out["eff"]), None))
         torch.cuda.synchronize(self.device)
@@ -102,7 +114,7 @@ class Plan:
         """Returns (torque array tau/gamma incl. STT/gamma, normalised m) as device tensors."""
         torch = self.torch
         md = self._dev(m).clone()
-        t = torch.zeros(3 * self.N, device=self.device)
+        t = torch.zeros(3 * self.N * self.nsim, device=self.device)
         nat.check(nat.lib().mm_torque(self.h, _ptr(md), noise_step, dt_thermal, _ptr(t), None))
         torch.cuda.synchronize(self.device)
         return t, md
@@ -117,7 +129,7 @@ class Plan:
         nat.check(nat.lib().mm_set_state(self.h, _ptr(md), 0, None))
 
     def get_state(self):
-        out = np.zeros(3 * self.N, dtype=np.float32)
+        out = np.zeros(3 * self.N * self.nsim, dtype=np.float32)
         nat.check(nat.lib().mm_get_state(self.h, out.ctypes.data_as(C.c_void_p), 1, None))
         return out
 
@@ -162,6 +174,32 @@ class Plan:
         nat.check(nat.lib().mm_energy(self.h, out, None))
         return dict(zip(["E_zeeman", "E_ex", "E_demag", "E_anis", "E"], out[:]))
 
+    # ---- batched plans: one entry per simulation
+    def set_sims(self, sims):
+        self._sims = nat.make_sims(self.problem, sims)
+        nat.check(nat.lib().mm_batch_set_sims(self.h, C.cast(self._sims, C.c_void_p)))
+
+    def batch_stats(self):
+        arr = (nat.MMStats * self.nsim)()
+        nat.check(nat.lib().mm_batch_stats(self.h, C.cast(arr, C.c_void_p), None))
+        return [{k: getattr(s, k) for k, _ in nat.MMStats._fields_} for s in arr]
+
+    def batch_maxtorque(self):
+        out = np.zeros(self.nsim)
+        nat.check(nat.lib().mm_batch_maxtorque(self.h, out.ctypes.data_as(C.c_void_p), None))
+        return out
+
+    def batch_average(self):
+        out = np.zeros((self.nsim, 3))
+        nat.check(nat.lib().mm_batch_average(self.h, out.ctypes.data_as(C.c_void_p), None))
+        return out
+
+    def batch_energy(self):
+        """nsim x 5: E_zeeman, E_ex, E_demag, E_anis, E."""
+        out = np.zeros((self.nsim, 5))
+        nat.check(nat.lib().mm_batch_energy(self.h, out.ctypes.data_as(C.c_void_p), None))
+        return out
+
     # ---- instrumentation
     def launch_count(self):
         return nat.lib().mm_plan_launch_count(self.h)
@@ -176,4 +214,36 @@ class Plan:
         out = (C.c_int * 12)()
         nat.check(nat.lib().mm_plan_geometry(self.h, out))
         v = list(out[:])
-        return dict(L=tuple(v[0:3]), M=v[3], h=v[4], hp=v[5], kd=tuple(v[6:9]), nk=v[9], demag=v[10])
+        return dict(L=tuple(v[0:3]), M=v[3], h=v[4], hp=v[5], kd=tuple(v[6:9]), nk=v[9], demag=v[10], nsim=v[11])
+
+
+class Ensemble:
+    """Several plans (typically one batched plan per grid size) stepped together from one
+    CUDA graph; `attempts` step attempts of every plan per graph launch."""
+
+    def __init__(self, plans, attempts=16):
+        self.plans = list(plans)
+        arr = (C.c_void_p * len(self.plans))(*[p.h.value for p in self.plans])
+        h = C.c_void_p()
+        nat.check(nat.lib().mm_ensemble_create(arr, len(self.plans), int(attempts), C.byref(h)))
+        self.h = h
+
+    def steps(self, n):
+        nat.check(nat.lib().mm_ensemble_steps(self.h, int(n), None))
+
+    def run(self, duration):
+        nat.check(nat.lib().mm_ensemble_run(self.h, float(duration), None))
+
+    def launch_count(self):
+        return nat.lib().mm_ensemble_launch_count(self.h)
+
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            nat.lib().mm_ensemble_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -24,6 +24,10 @@
  *   mm_maxtorque          MaxNormUpdater (update_reduce.go:103-108, reductor.go:173-186)
  *   mm_average            AverageUpdater (update_reduce.go:47-69)
  *   mm_energy             EnergyUpdater/SDotUpdater (mod_energy.go:24-95, update_sdot.go:36-62)
+ *   mm_plan_create_batch, mm_batch_*, mm_ensemble_*
+ *                         many independent simulations per launch; the reference runs one
+ *                         simulation per engine (engine.go:22-40), so a batch replaces nsim
+ *                         engines, each with its own Solver.Step, stepped side by side.
  */
 #ifndef MM_B200_H
 #define MM_B200_H
@@ -79,6 +83,16 @@ typedef struct mm_problem {
     const float *sl_pol_mask, *lambda_mask, *eps_prime_mask, *t_fl_mask;
 } mm_problem;
 
+/* Scalars of one simulation of a batched plan (the multipliers of Msat, Aex, alpha, B_ext,
+ * Ku1, anisU, Temp and the thermal seed); everything else comes from the mm_problem. */
+typedef struct mm_sim {
+    double msat, aex, alpha;             /* A/m, J/m, - */
+    double bext[3];                      /* T */
+    double ku, anisu[3];                 /* J/m^3, unit vector */
+    double temp;                         /* K */
+    unsigned long long seed;             /* thermal Philox key */
+} mm_sim;
+
 typedef struct mm_stats {
     double t, dt, err, peakerr, maxtorque;
     long long step, badsteps, attempts, evals;
@@ -86,6 +100,7 @@ typedef struct mm_stats {
 } mm_stats;
 
 typedef struct mm_plan_s* mm_plan;
+typedef struct mm_ensemble_s* mm_ensemble;
 typedef struct CUstream_st* mm_stream; /* cudaStream_t; NULL = legacy default stream */
 
 /* Last error message of the calling thread ("" if none). */
@@ -96,6 +111,18 @@ MM_API const char* mm_version(void);
  * workspaces; nothing is allocated after this call.  Runs on the current device. */
 MM_API int mm_plan_create(const mm_problem* prob, mm_plan* out);
 MM_API int mm_plan_destroy(mm_plan plan);
+/* A plan of nsim independent simulations of one geometry (grid, cell, pbc, terms, demag
+ * tensor).  Per-cell arrays (state, fields, torque) hold nsim blocks of 3 x N floats,
+ * simulation-major.  sims[nsim] gives each simulation's scalars; NULL takes them all from
+ * prob.  Masks in prob hold N values shared by all simulations (masks_per_sim = 0) or
+ * nsim x N values (masks_per_sim = 1).  Each simulation has its own time step, accept /
+ * reject decisions and stop condition; all run in the same kernel launches.  With demag,
+ * nsim > 1 needs 8 <= padded L2 <= 2048.  mm_plan_create(prob) = (prob, 1, NULL, 0). */
+MM_API int mm_plan_create_batch(const mm_problem* prob, int nsim, const mm_sim* sims, int masks_per_sim,
+                                mm_plan* out);
+MM_API int mm_plan_nsim(mm_plan plan);
+/* Replaces the per-simulation scalars of a batched plan. */
+MM_API int mm_batch_set_sims(mm_plan plan, const mm_sim* sims);
 /* Replaces multipliers/masks/terms of an existing plan (same grid, cell, pbc). */
 MM_API int mm_plan_set_problem(mm_plan plan, const mm_problem* prob);
 /* Non-zero demag tensor components (xx yy zz yz xz xy, internal order). */
@@ -147,6 +174,23 @@ MM_API int mm_energy(mm_plan plan, double out[5], mm_stream stream);
  * call on a device looks up that array's address and should precede any stream capture;
  * calls share the array, so calls that overlap on the GPU race. */
 MM_API int mm_average_noalloc(const float* m, long long ncell, double* out, mm_stream stream);
+
+/* ---- per-simulation results of a (batched) plan; out arrays have nsim entries ---- */
+MM_API int mm_batch_stats(mm_plan plan, mm_stats* out, mm_stream stream);
+MM_API int mm_batch_maxtorque(mm_plan plan, double* out, mm_stream stream);
+MM_API int mm_batch_average(mm_plan plan, double* out3, mm_stream stream);   /* nsim x 3 */
+MM_API int mm_batch_energy(mm_plan plan, double* out5, mm_stream stream);    /* nsim x 5 */
+
+/* ---- ensembles: several plans (e.g. one batched plan per grid size) stepped together,
+ * each on its own branch of one CUDA graph that replays `attempts_per_launch` attempts of
+ * every plan.  The plans stay owned by the caller and must outlive the ensemble. ---- */
+MM_API int mm_ensemble_create(const mm_plan* plans, int nplans, int attempts_per_launch, mm_ensemble* out);
+MM_API int mm_ensemble_destroy(mm_ensemble ens);
+/* Every simulation of every plan takes n accepted steps. */
+MM_API int mm_ensemble_steps(mm_ensemble ens, long long n, mm_stream stream);
+/* Every simulation advances by `duration` seconds. */
+MM_API int mm_ensemble_run(mm_ensemble ens, double duration, mm_stream stream);
+MM_API long long mm_ensemble_launch_count(mm_ensemble ens);
 
 /* ---- instrumentation ---- */
 /* Kernels this plan has enqueued so far (graph replays counted per kernel node). */
