@@ -302,16 +302,18 @@ __device__ __forceinline__ float2 wtab(const float2* __restrict__ tw, int num, i
     return TwSrc<SIGN, float2>::get(tw, num, den);
 }
 
-template <int P>
+template <int P, bool BATCH>
 __global__ void __launch_bounds__(128) zmul_reg_kernel(float2* __restrict__ S, KernelView K, int L1, int h, int hp,
                                                        long long comp_stride, long long zstride, float scale,
                                                        const float2* __restrict__ tw, const DevCtl* ctl,
                                                        int skip_retry, long long sim_stride,
                                                        const float* __restrict__ sim_scale) {
-    if (ctl) ctl += blockIdx.y;
+    if (BATCH) {
+        if (ctl) ctl += blockIdx.y;
+        S += blockIdx.y * sim_stride;
+        if (sim_scale) scale = sim_scale[blockIdx.y];
+    }
     if (conv_skip(ctl, skip_retry)) return;
-    S += blockIdx.y * sim_stride;
-    if (sim_scale) scale = sim_scale[blockIdx.y];
     const long long gt = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     const int s = (int)(gt & 1);
     const long long colg = gt >> 1;
@@ -385,16 +387,18 @@ __global__ void __launch_bounds__(128) zmul_reg_kernel(float2* __restrict__ S, K
 // and contributes W_{2P}^(-z s) IDFT_{P/2}(H_s)[z mod P/2] to every output plane z; the
 // four contributions are summed by a two-round shuffle reduce-scatter after which lane s
 // owns the planes z with z mod 4 == s.
-template <int P>
+template <int P, bool BATCH>
 __global__ void __launch_bounds__(128) zmul_reg4_kernel(float2* __restrict__ S, KernelView K, int L1, int h, int hp,
                                                          long long comp_stride, long long zstride, float scale,
                                                          const float2* __restrict__ tw, const DevCtl* ctl,
                                                          int skip_retry, long long sim_stride,
                                                          const float* __restrict__ sim_scale) {
-    if (ctl) ctl += blockIdx.y;
+    if (BATCH) {  // the single-simulation variant keeps the shorter prologue
+        if (ctl) ctl += blockIdx.y;
+        S += blockIdx.y * sim_stride;
+        if (sim_scale) scale = sim_scale[blockIdx.y];
+    }
     if (conv_skip(ctl, skip_retry)) return;
-    S += blockIdx.y * sim_stride;
-    if (sim_scale) scale = sim_scale[blockIdx.y];
     constexpr int H = P / 2;
     const long long gt = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     const int s = (int)(gt & 3);
@@ -493,8 +497,12 @@ static cudaError_t launch_zmul_reg_t(float2* S, const KernelView& K, int L1, int
                                      const float* sim_scale) {
     const long long threads = 2LL * L1 * h;
     const dim3 grid((unsigned)((threads + 127) / 128), (unsigned)nsim);
-    zmul_reg_kernel<P><<<grid, 128, 0, st>>>(S, K, L1, h, hp, comp_stride, zstride, scale, tw, ctl, skip_retry,
-                                             sim_stride, sim_scale);
+    if (nsim > 1)
+        zmul_reg_kernel<P, true><<<grid, 128, 0, st>>>(S, K, L1, h, hp, comp_stride, zstride, scale, tw, ctl,
+                                                       skip_retry, sim_stride, sim_scale);
+    else
+        zmul_reg_kernel<P, false><<<grid, 128, 0, st>>>(S, K, L1, h, hp, comp_stride, zstride, scale, tw, ctl,
+                                                        skip_retry, sim_stride, sim_scale);
     return cudaGetLastError();
 }
 
@@ -505,8 +513,12 @@ static cudaError_t launch_zmul_reg4_t(float2* S, const KernelView& K, int L1, in
                                       const float* sim_scale) {
     const long long threads = 4LL * L1 * h;
     const dim3 grid((unsigned)((threads + 127) / 128), (unsigned)nsim);
-    zmul_reg4_kernel<P><<<grid, 128, 0, st>>>(S, K, L1, h, hp, comp_stride, zstride, scale, tw, ctl, skip_retry,
-                                              sim_stride, sim_scale);
+    if (nsim > 1)
+        zmul_reg4_kernel<P, true><<<grid, 128, 0, st>>>(S, K, L1, h, hp, comp_stride, zstride, scale, tw, ctl,
+                                                        skip_retry, sim_stride, sim_scale);
+    else
+        zmul_reg4_kernel<P, false><<<grid, 128, 0, st>>>(S, K, L1, h, hp, comp_stride, zstride, scale, tw, ctl,
+                                                         skip_retry, sim_stride, sim_scale);
     return cudaGetLastError();
 }
 

@@ -100,6 +100,14 @@ def read_traffic():
     return out
 
 
+def step_bytes_heun(geo, n):
+    """Algorithmic bytes of one Heun step: two fused evaluations; the first also writes the
+    predictor, the second reads the saved k0 and writes the corrected state."""
+    N = n[0] * n[1] * n[2]
+    conv = sum(b for _, b in pass_bytes(geo, n)) - 36 * N   # passes without reading m / writing k
+    return 2 * conv + 2 * (12 * N + 12 * N + 12 * N + 12 * N)
+
+
 # ---------------------------------------------------------------- clocks
 class ClockSampler:
     def __init__(self, gpu_index):
@@ -208,6 +216,126 @@ def replica_seed(rank):
     return 1000 + rank
 
 
+# ---------------------------------------------------------------- ensemble workload
+def ensemble_bench(args, rank, world, local_rank, dist):
+    """2048 independent thermal simulations of five grid sizes, one batched plan per size,
+    all stepped from one CUDA graph (stochastic Heun, fixed 50 fs).  A step advances every
+    simulation by one Heun step; value = total cells x steps / device time.  Beside it:
+    the same simulations run one at a time (a sample of one per grid size) and their <m>
+    against the batched run."""
+    import ctypes as C
+    import torch
+    from mumax2 import Ensemble, Plan
+    from mumax2 import _native as nat
+    from mumax2 import workloads as W
+    classes = W.ensemble(nsim=args.nsim, seed=rank)
+    plans, states = [], []
+    for c in classes:
+        p = Plan(c["problem"], sims=c["sims"], device=local_rank)
+        p.solver("heun", dt=W.ENSEMBLE_DT)
+        m0 = W.uniform_state(c["n"], c["m0"], len(c["sims"]))
+        p.set_state(m0)
+        plans.append(p)
+        states.append(m0)
+    ens = Ensemble(plans, attempts=args.ens_attempts)
+    cells = W.cells_of(classes)
+    ens.steps(args.warmup)
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local_rank)
+    sampler.start()
+    time.sleep(0.3)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    l0 = ens.launch_count()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    ens.steps(args.steps)
+    e1.record()
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    ms = e0.elapsed_time(e1)
+    launches = ens.launch_count() - l0
+    ms_max, value = aggregate(ms, cells, args.steps, world, dist, "cuda")
+    step_b = 0
+    for c, p in zip(classes, plans):
+        step_b += step_bytes_heun(p.geometry(), c["n"]) * len(c["sims"])
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    peak, peak_src = (float(json.load(open(peaks_path))["hbm_gbs"]), "measured") if os.path.exists(peaks_path) \
+        else (6650.0, "fallback")
+    achieved = step_b * args.steps / (ms / 1e3) / 1e9
+
+    # end to end: states from pinned host memory, the steps, states back to the host
+    L = nat.lib()
+    hin = [torch.from_numpy(s).pin_memory() for s in states]
+    hout = [torch.empty_like(h).pin_memory() for h in hin]
+    torch.cuda.synchronize()
+    f0 = torch.cuda.Event(enable_timing=True)
+    f1 = torch.cuda.Event(enable_timing=True)
+    f0.record()
+    for p, h in zip(plans, hin):
+        nat.check(L.mm_set_state(p.h, C.c_void_p(h.data_ptr()), 1, None))
+    ens.steps(args.steps)
+    for p, h in zip(plans, hout):
+        nat.check(L.mm_get_state(p.h, C.c_void_p(h.data_ptr()), 1, None))
+    f1.record()
+    torch.cuda.synchronize()
+    e2e_ms, e2e_value = aggregate(f0.elapsed_time(f1), cells, args.steps, world, dist, "cuda")
+    io_bytes = sum(h.numel() * 4 for h in hin)
+
+    # unbatched comparison: the first simulation of each grid size alone, same inputs
+    # and steps (warm-up + timed + end-to-end run), then its <m> against the batch
+    avg_b = [p.batch_average() for p in plans]
+    uni_cells_steps, uni_ms, dm = 0, 0.0, 0.0
+    for c, p, m0, ab in zip(classes, plans, states, avg_b):
+        q = dict(c["problem"])
+        q.update(c["sims"][0])
+        s = Plan(q, device=local_rank)
+        s.solver("heun", dt=W.ENSEMBLE_DT)
+        N = int(np.prod(c["n"]))
+        s.set_state(m0[:3 * N])
+        s.steps(args.warmup + args.steps)
+        s.set_state(m0[:3 * N])
+        torch.cuda.synchronize()
+        u0 = torch.cuda.Event(enable_timing=True)
+        u1 = torch.cuda.Event(enable_timing=True)
+        u0.record()
+        s.steps(args.steps)
+        u1.record()
+        torch.cuda.synchronize()
+        uni_ms += u0.elapsed_time(u1)
+        uni_cells_steps += N * args.steps
+        dm = max(dm, float(np.abs(s.average() - ab[0]).max()))
+        s.close()
+    unbatched = uni_cells_steps / (uni_ms / 1e3)
+    if rank == 0:
+        line = {"metric": "cell-steps/s", "value": value, "unit": "cell-steps/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic",
+                "config": {"workload": f"thermal_ensemble_{args.nsim}", "simulations": args.nsim, "cells": cells,
+                           "grids_xyz": [list(g) for g in W.ENSEMBLE_GRIDS_USER],
+                           "sims_per_grid": [len(c["sims"]) for c in classes], "cell_nm": [4, 4, 3],
+                           "solver": "heun", "dt_fs": 50, "temperature_K": W.ENSEMBLE_TEMP,
+                           "attempts_per_graph_launch": args.ens_attempts, "parallelism": f"replicas{world}",
+                           "l2": f"working set ~{sum(p.device_bytes() for p in plans) / 1e9:.1f} GB > 126 MB L2"},
+                "roofline": {"bound": "hbm", "kernel": "whole Heun step (all passes of all simulations)",
+                             "achieved": achieved, "peak": peak, "peak_source": peak_src, "unit": "GB/s",
+                             "frac": achieved / peak, "traffic": None, "algorithmic_bytes_per_step": step_b},
+                "e2e": {"value": e2e_value, "unit": "cell-steps/s", "h2d_bytes_per_step": io_bytes / args.steps,
+                        "d2h_bytes_per_step": io_bytes / args.steps, "steps": args.steps},
+                "unbatched": {"value": unbatched, "unit": "cell-steps/s",
+                              "sample": f"first simulation of each of the {len(classes)} grid sizes, one plan each, "
+                                        f"{args.steps} steps", "batched_over_unbatched": value / unbatched,
+                              "max_abs_avg_m_diff": dm},
+                "gpu_launches": launches, "clocks": clocks}
+        print(json.dumps(line), flush=True)
+    ens.close()
+    for p in plans:
+        p.close()
+
+
 # ---------------------------------------------------------------- main
 def main():
     ap = argparse.ArgumentParser()
@@ -219,6 +347,10 @@ def main():
     ap.add_argument("--profile-reps", type=int, default=10)
     ap.add_argument("--profile-only", action="store_true",
                     help="only time the passes of one field evaluation (few launches; for ncu captures)")
+    ap.add_argument("--workload", default="film3d", choices=["film3d", "ensemble"],
+                    help="film3d: the 256x256x16 RK23 film (default); ensemble: 2048 thermal simulations")
+    ap.add_argument("--nsim", type=int, default=2048, help="ensemble: number of simulations")
+    ap.add_argument("--ens-attempts", type=int, default=50, help="ensemble: attempts per graph launch")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -236,6 +368,12 @@ def main():
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    if args.workload == "ensemble":
+        ensemble_bench(args, rank, world, local_rank, dist)
+        if dist:
+            dist.destroy_process_group()
+        return
 
     from mumax2 import Plan
     w = WORKLOAD

@@ -137,7 +137,7 @@ def test_batch_relax_until_maxtorque_and_reductions():
     g = Plan(base, sims=sims)
     g.solver("rk23", dt=1e-14, maxerr=1e-4)
     N = n[0] * n[1] * n[2]
-    m = _batch_m(n, 3, 400)
+    m = np.concatenate([rand_m(n, 400 + b, kind="near_x") for b in range(3)])
     g.set_state(m)
     thr = 1e-4 * 2.211e5 * np.array([s["msat"] for s in sims])
     # one threshold for all: the smallest, so that every simulation must reach it
