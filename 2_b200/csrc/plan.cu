@@ -1189,9 +1189,9 @@ static int drive(mm_plan p, cudaStream_t st, long long max_attempts) {
 }
 
 // Sets every simulation's stop condition: t_end = t + duration (duration > 0), or
-// step_end = step + nsteps (nsteps > 0), or maxtorque < thr.
+// step_end = step + nsteps (nsteps > 0), or maxtorque < thr (thr_sim[b] if given).
 static int start_run(mm_plan p, cudaStream_t st, double duration, long long nsteps, double thr,
-                     long long max_steps) {
+                     long long max_steps, const double* thr_sim = nullptr) {
     if (p->solver < 0) return set_err(MM_ERR_STATE, "no solver: call mm_solver_init");
     if (!p->state_set) return set_err(MM_ERR_STATE, "no state: call mm_set_state");
     int rc = read_ctl(p, st);
@@ -1203,7 +1203,7 @@ static int start_run(mm_plan p, cudaStream_t st, double duration, long long nste
         c.tries = 0;
         c.t_end = duration > 0 ? c.t + duration : 1e300;
         c.step_end = nsteps > 0 ? c.step + nsteps : (max_steps > 0 ? c.step + max_steps : (1LL << 62));
-        c.torque_thr = thr;
+        c.torque_thr = thr_sim ? thr_sim[b] : thr;
         c.err_bits = 0;
         c.tq_bits = 0;
         c.gamma = p->prob.gamma;
@@ -1216,7 +1216,7 @@ static int start_run(mm_plan p, cudaStream_t st, double duration, long long nste
     if (thr > 0 && (p->solver == MM_RK23 || p->solver == MM_RK45)) {
         if ((rc = read_ctl(p, st))) return rc;
         for (int b = 0; b < p->nsim; b++)
-            if (p->ctl_host[b].maxtorque < thr) p->ctl_host[b].done = 1;
+            if (p->ctl_host[b].maxtorque < p->ctl_host[b].torque_thr) p->ctl_host[b].done = 1;
         return write_ctl(p, st);
     }
     return MM_OK;
@@ -1243,8 +1243,9 @@ static bool any_active(mm_plan p) {
     return false;
 }
 
-static int run_plan(mm_plan p, cudaStream_t st, double duration, long long nsteps, double thr, long long max_steps) {
-    int rc = start_run(p, st, duration, nsteps, thr, max_steps);
+static int run_plan(mm_plan p, cudaStream_t st, double duration, long long nsteps, double thr, long long max_steps,
+                    const double* thr_sim = nullptr) {
+    int rc = start_run(p, st, duration, nsteps, thr, max_steps, thr_sim);
     if (rc) return rc;
     if (any_active(p)) rc = drive(p, st, 0);
     int rc2 = finish_run(p, st);
@@ -1269,6 +1270,14 @@ extern "C" MM_API int mm_run_until_maxtorque(mm_plan p, double thr, long long ma
     if (!p) return set_err(MM_ERR_ARG, "null plan");
     if (!(thr > 0)) return set_err(MM_ERR_ARG, "threshold must be > 0");
     return run_plan(p, (cudaStream_t)stream, 0, 0, thr, max_steps);
+}
+
+extern "C" MM_API int mm_batch_run_until_maxtorque(mm_plan p, const double* thr, long long max_steps,
+                                                   mm_stream stream) {
+    if (!p || !thr) return set_err(MM_ERR_ARG, "null argument");
+    for (int b = 0; b < p->nsim; b++)
+        if (!(thr[b] > 0)) return set_err(MM_ERR_ARG, "threshold of simulation %d must be > 0", b);
+    return run_plan(p, (cudaStream_t)stream, 0, 0, 1.0, max_steps, thr);
 }
 
 static void stats_of(const DevCtl& c, mm_stats* out) {

@@ -179,6 +179,13 @@ class Plan:
         self._sims = nat.make_sims(self.problem, sims)
         nat.check(nat.lib().mm_batch_set_sims(self.h, C.cast(self._sims, C.c_void_p)))
 
+    def batch_run_until_maxtorque(self, thr, max_steps=0):
+        """Each simulation b steps until its maxtorque < thr[b]."""
+        self._thr = np.ascontiguousarray(thr, dtype=np.float64)
+        assert self._thr.shape == (self.nsim,)
+        nat.check(nat.lib().mm_batch_run_until_maxtorque(self.h, self._thr.ctypes.data_as(C.c_void_p),
+                                                         int(max_steps), None))
+
     def batch_stats(self):
         arr = (nat.MMStats * self.nsim)()
         nat.check(nat.lib().mm_batch_stats(self.h, C.cast(arr, C.c_void_p), None))

@@ -69,3 +69,61 @@ def uniform_state(n, direction, count=1):
 
 def cells_of(classes):
     return sum(int(np.prod(c["n"])) * len(c["sims"]) for c in classes)
+
+
+# ---------------------------------------------------------------- relaxation set
+RELAX_GRID_USER = (64, 64, 1)
+RELAX_CELL_USER = (4e-9, 4e-9, 3e-9)
+
+
+def geometry_mask(rng, nx, ny):
+    """1-3 ellipses or rectangles (union) filling 40-100 % of the nx x ny film; returns a
+    float32 [ny][nx] 0/1 mask.  Shapes are redrawn until the fill is in range."""
+    yy, xx = np.mgrid[0:ny, 0:nx]
+    xx = (xx + 0.5) / nx
+    yy = (yy + 0.5) / ny
+    for _ in range(1000):
+        m = np.zeros((ny, nx), dtype=bool)
+        for _ in range(int(rng.integers(1, 4))):
+            cx, cy = rng.uniform(0.2, 0.8, size=2)
+            ax, ay = rng.uniform(0.25, 0.75, size=2)
+            if rng.uniform() < 0.5:
+                m |= ((xx - cx) / ax) ** 2 + ((yy - cy) / ay) ** 2 <= 1.0
+            else:
+                m |= (np.abs(xx - cx) <= ax / 2) & (np.abs(yy - cy) <= ay / 2)
+        fill = m.mean()
+        if 0.4 <= fill <= 1.0:
+            return m.astype(np.float32)
+    raise RuntimeError("no mask with 40-100 % fill")
+
+
+def relax_set(nsim, seed=0):
+    """Seeded relaxation problems on 64x64x1 films of 4x4x3 nm cells: a geometry mask,
+    Ms ~ U[4e5, 1.2e6], Aex ~ U[5e-12, 2e-11], Ku1 ~ U[0, 5e5] along an in-plane axis,
+    |B| ~ U[0, 100] mT at an in-plane angle.  Returns (problem, sims, masks [nsim][N]) with
+    the relax damping alpha = 1."""
+    rng = np.random.default_rng(seed)
+    nx, ny, nz = RELAX_GRID_USER
+    n = (nz, ny, nx)
+    problem = dict(n=n, cell=_internal(RELAX_CELL_USER), pbc=(0, 0, 0), demag=1, exchange=1, zeeman=1, anis=1,
+                   thermal=0, demag_accuracy=6, msat=8e5, aex=1.3e-11, alpha=1.0, gamma=2.211e5)
+    sims, masks = [], []
+    for i in range(nsim):
+        masks.append(geometry_mask(rng, nx, ny).ravel())
+        ms = rng.uniform(4e5, 1.2e6)
+        aex = rng.uniform(5e-12, 2e-11)
+        ku = rng.uniform(0.0, 5e5)
+        phi_u = rng.uniform(0, 2 * np.pi)
+        bmag = rng.uniform(0.0, 0.1)
+        phi_b = rng.uniform(0, 2 * np.pi)
+        u = (np.cos(phi_u), np.sin(phi_u), 0.0)            # user (x, y, z)
+        b = (bmag * np.cos(phi_b), bmag * np.sin(phi_b), 0.0)
+        sims.append(dict(msat=float(ms), aex=float(aex), alpha=1.0, ku=float(ku),
+                         anisu=tuple(float(x) for x in _internal(u)),
+                         bext=tuple(float(x) for x in _internal(b)), temp=0.0, seed=int(seed) * 1_000_003 + i))
+    return problem, sims, masks
+
+
+def cold_state(n, count):
+    """The uninformed start of a plain relax: uniform along user +x (internal component 2)."""
+    return uniform_state(n, (0.0, 0.0, 1.0), count)

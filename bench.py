@@ -336,6 +336,70 @@ def ensemble_bench(args, rank, world, local_rank, dist):
         p.close()
 
 
+# ---------------------------------------------------------------- relaxation workload
+def relax_bench(args, rank, world, local_rank, dist):
+    """Batched plain relaxations: 64x64x1 films with seeded geometry masks and parameters,
+    `--relax-batch` per plan, from the cold start (uniform along +x), RK23 with
+    alpha = 1 until each simulation's maxtorque / (gamma Ms) < 1e-4.  value =
+    relaxations / device time.  Every batch reuses one plan (new masks and scalars)."""
+    import torch
+    from mumax2 import Plan
+    from mumax2 import workloads as W
+    B = args.relax_batch
+    nb = max(1, args.nsim // B)
+    problem, sims, masks = W.relax_set(nb * B, seed=rank)
+    n = problem["n"]
+    gamma = problem["gamma"]
+    plan = None
+    total_ms, steps, conv, worst = 0.0, [], 0, 0.0
+    sampler = ClockSampler(local_rank)
+    sampler.start()
+    for k in range(nb + 1):  # batch 0 is an untimed warm-up (the same problems as batch 1)
+        j = max(0, k - 1)
+        bs = sims[j * B:(j + 1) * B]
+        bm = {"msat": np.concatenate(masks[j * B:(j + 1) * B])}
+        if plan is None:
+            plan = Plan(problem, masks=bm, sims=bs, masks_per_sim=True, device=local_rank)
+            plan.solver("rk23", dt=1e-14, maxerr=args.relax_maxerr)
+        else:
+            plan.set_problem(problem, masks=bm)
+            plan.set_sims(bs)
+            plan.solver("rk23", dt=1e-14, maxerr=args.relax_maxerr)
+        thr = np.array([1e-4 * gamma * s["msat"] for s in bs])
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        plan.set_state(W.cold_state(n, B))
+        plan.batch_run_until_maxtorque(thr, max_steps=args.relax_max_steps)
+        e1.record()
+        torch.cuda.synchronize()
+        if k == 0:
+            continue
+        total_ms += e0.elapsed_time(e1)
+        st = plan.batch_stats()
+        steps += [s["step"] for s in st]
+        conv += sum(1 for s, t in zip(st, thr) if s["maxtorque"] < t)
+        worst = max(worst, max(s["maxtorque"] / (gamma * q["msat"]) for s, q in zip(st, bs)))
+    clocks = sampler.stop()
+    nrel = nb * B
+    ms_max, value = aggregate(total_ms, 1, nrel, world, dist, "cuda")
+    if rank == 0:
+        line = {"metric": "relaxations/s", "value": value, "unit": "relaxations/s", "n_gpus": world,
+                "steps": nrel, "warmup": 1, "ms_per_step": ms_max / nrel, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": "relax_64x64x1_cold", "relaxations": nrel, "batch": B,
+                           "grid_xyz": list(W.RELAX_GRID_USER), "cell_nm": [4, 4, 3], "solver": "rk23",
+                           "maxerr": args.relax_maxerr, "alpha": 1.0, "start": "cold (uniform +x)",
+                           "criterion": "maxtorque / (gamma Ms) < 1e-4 per simulation",
+                           "parallelism": f"replicas{world}"},
+                "relax": {"converged": conv, "of": nrel, "steps_mean": float(np.mean(steps)),
+                          "steps_max": int(np.max(steps)), "worst_torque_over_gamma_ms": worst},
+                "clocks": clocks}
+        print(json.dumps(line), flush=True)
+    plan.close()
+
+
 # ---------------------------------------------------------------- main
 def main():
     ap = argparse.ArgumentParser()
@@ -347,8 +411,12 @@ def main():
     ap.add_argument("--profile-reps", type=int, default=10)
     ap.add_argument("--profile-only", action="store_true",
                     help="only time the passes of one field evaluation (few launches; for ncu captures)")
-    ap.add_argument("--workload", default="film3d", choices=["film3d", "ensemble"],
-                    help="film3d: the 256x256x16 RK23 film (default); ensemble: 2048 thermal simulations")
+    ap.add_argument("--workload", default="film3d", choices=["film3d", "ensemble", "relax"],
+                    help="film3d: the 256x256x16 RK23 film (default); ensemble: 2048 thermal simulations; "
+                         "relax: batched cold relaxations of 64x64x1 films")
+    ap.add_argument("--relax-batch", type=int, default=256)
+    ap.add_argument("--relax-maxerr", type=float, default=1e-6)
+    ap.add_argument("--relax-max-steps", type=int, default=100000)
     ap.add_argument("--nsim", type=int, default=2048, help="ensemble: number of simulations")
     ap.add_argument("--ens-attempts", type=int, default=50, help="ensemble: attempts per graph launch")
     args = ap.parse_args()
@@ -369,8 +437,8 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
-    if args.workload == "ensemble":
-        ensemble_bench(args, rank, world, local_rank, dist)
+    if args.workload in ("ensemble", "relax"):
+        (ensemble_bench if args.workload == "ensemble" else relax_bench)(args, rank, world, local_rank, dist)
         if dist:
             dist.destroy_process_group()
         return

@@ -175,6 +175,10 @@ MM_API int mm_energy(mm_plan plan, double out[5], mm_stream stream);
  * calls share the array, so calls that overlap on the GPU race. */
 MM_API int mm_average_noalloc(const float* m, long long ncell, double* out, mm_stream stream);
 
+/* run_until_maxtorque with one threshold per simulation (thr[nsim]); each simulation
+ * stops, and stays frozen, once its own maxtorque falls below its threshold. */
+MM_API int mm_batch_run_until_maxtorque(mm_plan plan, const double* thr, long long max_steps, mm_stream stream);
+
 /* ---- per-simulation results of a (batched) plan; out arrays have nsim entries ---- */
 MM_API int mm_batch_stats(mm_plan plan, mm_stats* out, mm_stream stream);
 MM_API int mm_batch_maxtorque(mm_plan plan, double* out, mm_stream stream);

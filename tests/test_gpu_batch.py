@@ -135,7 +135,9 @@ def test_batch_relax_until_maxtorque_and_reductions():
     base = _base(n)
     sims = [dict(s, alpha=1.0) for s in SIMS]
     g = Plan(base, sims=sims)
-    g.solver("rk23", dt=1e-14, maxerr=1e-4)
+    # an explicit solver relaxes only down to a torque floor set by its error tolerance:
+    # 1e-6 takes these films below the threshold in a few hundred to a few thousand steps
+    g.solver("rk23", dt=1e-14, maxerr=1e-6)
     N = n[0] * n[1] * n[2]
     m = np.concatenate([rand_m(n, 400 + b, kind="near_x") for b in range(3)])
     g.set_state(m)
@@ -148,9 +150,9 @@ def test_batch_relax_until_maxtorque_and_reductions():
     av = g.batch_average()
     en = g.batch_energy()
     for b, sim in enumerate(sims):
-        assert st[b]["maxtorque"] < thr.min()
+        assert st[b]["maxtorque"] < thr.min(), (b, st[b])
         s = _single(base, sim)
-        s.solver("rk23", dt=1e-14, maxerr=1e-4)
+        s.solver("rk23", dt=1e-14, maxerr=1e-6)
         s.set_state(m[3 * N * b:3 * N * (b + 1)])
         s.run_until_maxtorque(float(thr.min()), max_steps=20000)
         assert st[b]["step"] == s.stats()["step"], b
@@ -203,3 +205,28 @@ def test_ensemble_of_grid_classes_matches_plans_alone():
         alone.set_state(m)
         alone.steps(30)
         assert np.abs(got - alone.get_state()).max() < TOL_SAME
+
+
+def test_batch_per_simulation_thresholds():
+    """mm_batch_run_until_maxtorque: each simulation stops at its own threshold."""
+    from mumax2 import Plan
+    n = (1, 16, 16)
+    base = _base(n)
+    sims = [dict(s, alpha=1.0) for s in SIMS]
+    g = Plan(base, sims=sims)
+    g.solver("rk23", dt=1e-14, maxerr=1e-6)
+    N = n[0] * n[1] * n[2]
+    m = np.concatenate([rand_m(n, 700 + b, kind="near_x") for b in range(3)])
+    g.set_state(m)
+    thr = np.array([1e-4 * 2.211e5 * s["msat"] for s in sims])
+    g.batch_run_until_maxtorque(thr, max_steps=50000)
+    st = g.batch_stats()
+    mb = g.get_state()
+    for b, sim in enumerate(sims):
+        assert st[b]["maxtorque"] < thr[b], (b, st[b])
+        s = _single(base, sim)
+        s.solver("rk23", dt=1e-14, maxerr=1e-6)
+        s.set_state(m[3 * N * b:3 * N * (b + 1)])
+        s.run_until_maxtorque(float(thr[b]), max_steps=50000)
+        assert st[b]["step"] == s.stats()["step"], b
+        assert np.abs(mb[3 * N * b:3 * N * (b + 1)] - s.get_state()).max() < TOL_SAME
