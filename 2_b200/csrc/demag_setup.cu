@@ -15,7 +15,7 @@
 
 namespace mm {
 
-__device__ __forceinline__ int wrap_i(int number, int max) {
+__host__ __device__ __forceinline__ int wrap_i(int number, int max) {
     number %= max;
     return number < 0 ? number + max : number;
 }
@@ -220,6 +220,77 @@ fail:
     if (spec) cudaFree(spec);
     if (dmax) cudaFree(dmax);
     return rc;
+}
+
+
+// Exch6NgbrKernel (kernel_exchange.go:102-123), module demagexch: the 6-neighbour
+// Laplacian as a convolution kernel on the padded grid, written in the reference's
+// order (centre, then the +-1 neighbours along x, y, z with wrapped indices,
+// kernel.go:19-27; along a dimension of size 1 the neighbour writes overwrite the
+// centre) and rounded to float as the reference stores it.  Its FP64 transform (real
+// part / prod L, one octant) goes to kex[kd0][kd1][kd2]; it is the same for xx, yy, zz.
+int build_exchange_kernel(const int L[3], const double cell[3], float* kex, const int kd[3], cudaStream_t st,
+                          char* err, int errlen) {
+    const long long NL = (long long)L[0] * L[1] * L[2];
+    const int M = L[2] / 2;
+    const int hp = M + 1;
+    double* K = nullptr;
+    double2* spec = nullptr;
+    int rc = MM_ERR_CUDA;
+    {
+        // host list of (index, value), later writes replacing earlier ones
+        std::vector<std::pair<long long, double>> w;
+        auto put = [&](int x, int y, int z, double v) {
+            const long long idx = ((long long)wrap_i(x, L[0]) * L[1] + wrap_i(y, L[1])) * L[2] + wrap_i(z, L[2]);
+            for (auto& e : w)
+                if (e.first == idx) { e.second = v; return; }
+            w.push_back({idx, v});
+        };
+        const double hx = cell[0] * cell[0], hy = cell[1] * cell[1], hz = cell[2] * cell[2];
+        put(0, 0, 0, (float)(-2 / hx - 2 / hy - 2 / hz));
+        put(+1, 0, 0, (float)(1 / hx));
+        put(-1, 0, 0, (float)(1 / hx));
+        put(0, +1, 0, (float)(1 / hy));
+        put(0, -1, 0, (float)(1 / hy));
+        put(0, 0, +1, (float)(1 / hz));
+        put(0, 0, -1, (float)(1 / hz));
+        CK(cudaMalloc(&K, sizeof(double) * NL));
+        CK(cudaMemsetAsync(K, 0, sizeof(double) * NL, st));
+        for (auto& e : w) CK(cudaMemcpyAsync(K + e.first, &e.second, sizeof(double), cudaMemcpyHostToDevice, st));
+        CK(cudaMalloc(&spec, sizeof(double2) * (size_t)L[0] * L[1] * hp));
+        PP none = {nullptr, nullptr, 0};
+        CK(launch_xfwd<double2, double>(M, K, none, nullptr, spec, L[0] * L[1], L[0], L[1], L[1], L[2], L[2], hp,
+                                        nullptr, nullptr, 0, st));
+        if (L[1] > 1)
+            CK(launch_colfft<double2>(L[1], -1, spec, hp, L[0], (long long)L[1] * hp, hp, L[1], L[1], nullptr, nullptr,
+                                      0, st));
+        if (L[0] > 1)
+            CK(launch_colfft<double2>(L[0], -1, spec, hp, L[1], hp, (long long)L[1] * hp, L[0], L[0], nullptr, nullptr,
+                                      0, st));
+        extract_octant_kernel<<<296, 256, 0, st>>>(spec, L[0], L[1], hp, kd[0], kd[1], kd[2], 1.0 / (double)NL, kex);
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(st));  // the host list must outlive the copies
+        rc = MM_OK;
+    }
+fail:
+    if (K) cudaFree(K);
+    if (spec) cudaFree(spec);
+    return rc;
+}
+
+// khat = kd + c * kex on the diagonal components (mod_demagexchange.go:145-157 with the
+// Ms factor applied by the convolution passes: c = 2 Aex / (mu0 Ms^2)), kd elsewhere.
+__global__ void combine_dex_kernel(const float* kd, const float* kex, long long oct, double c, float* khat) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < 6 * oct;
+         i += (long long)gridDim.x * blockDim.x) {
+        const long long q = i / oct;
+        khat[i] = q < 3 ? (float)((double)kd[i] + c * (double)kex[i - q * oct]) : kd[i];
+    }
+}
+
+int combine_dex(const float* kd, const float* kex, long long oct, double c, float* khat, cudaStream_t st) {
+    combine_dex_kernel<<<296, 256, 0, st>>>(kd, kex, oct, c, khat);
+    return cudaGetLastError() == cudaSuccess ? MM_OK : MM_ERR_CUDA;
 }
 
 }  // namespace mm

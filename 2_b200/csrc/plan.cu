@@ -23,6 +23,9 @@
 namespace mm {
 int build_demag_kernel(const int L[3], const double cell[3], const int pbc[3], int accuracy, float* khat,
                        const int kd[3], int nz[6], cudaStream_t st, char* err, int errlen);
+int build_exchange_kernel(const int L[3], const double cell[3], float* kex, const int kd[3], cudaStream_t st,
+                          char* err, int errlen);
+int combine_dex(const float* kd, const float* kex, long long oct, double c, float* khat, cudaStream_t st);
 }
 
 using namespace mm;
@@ -304,6 +307,8 @@ struct mm_plan_s {
     FieldParams P;
     bool demag = false;
     float* khat = nullptr;
+    float* khat_d = nullptr;         // demagexch: pure demag octant (khat holds the sum)
+    float* khat_ex = nullptr;        // demagexch: Laplacian octant
     float2* tw = nullptr;            // FP32 twiddle table exp(-2 pi i k / 4096)
     KernelView kv;
     float2* S = nullptr;
@@ -386,7 +391,7 @@ static void fill_params(mm_plan p) {
     FieldParams& P = p->P;
     memset(&P, 0, sizeof P);
     P.demag = q.demag;
-    P.exchange = q.exchange;
+    P.exchange = q.exchange && !q.demag_exchange;
     P.anis = q.anis;
     P.zeeman = q.zeeman;
     bool hot = false;
@@ -499,6 +504,10 @@ extern "C" MM_API int mm_plan_create_batch(const mm_problem* prob, int nsim, con
         p->prob.seed = m0.seed;
         for (int i = 0; i < 3; i++) { p->prob.bext[i] = m0.bext[i]; p->prob.anisu[i] = m0.anisu[i]; }
     }
+    if (prob->demag_exchange && (!prob->demag || prob->aex_mask || nsim != 1)) {
+        delete p;
+        return set_err(MM_ERR_ARG, "demag_exchange needs demag = 1, a uniform Aex (no mask) and one simulation");
+    }
     ConvGeom& g = p->g;
     for (int i = 0; i < 3; i++) {
         g.n[i] = prob->n[i];
@@ -553,8 +562,22 @@ extern "C" MM_API int mm_plan_create_batch(const mm_problem* prob, int nsim, con
         cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
         char err[512] = {0};
         int nz[6];
-        rc = build_demag_kernel(g.L, prob->cell, prob->pbc, prob->demag_accuracy, p->khat, g.kd, nz, st, err,
-                                sizeof err);
+        if (prob->demag_exchange) {
+            if (!(rc = dalloc(p, (void**)&p->khat_d, sizeof(float) * 6 * oct)) &&
+                !(rc = dalloc(p, (void**)&p->khat_ex, sizeof(float) * oct))) {
+                rc = build_demag_kernel(g.L, prob->cell, prob->pbc, prob->demag_accuracy, p->khat_d, g.kd, nz, st,
+                                        err, sizeof err);
+                if (rc == MM_OK) rc = build_exchange_kernel(g.L, prob->cell, p->khat_ex, g.kd, st, err, sizeof err);
+                if (rc == MM_OK)
+                    rc = combine_dex(p->khat_d, p->khat_ex, oct, 2.0 * prob->aex / (MU0 * prob->msat * prob->msat),
+                                     p->khat, st);
+                for (int q = 0; q < 3; q++) nz[q] = 1;
+            }
+        } else {
+            rc = build_demag_kernel(g.L, prob->cell, prob->pbc, prob->demag_accuracy, p->khat, g.kd, nz, st, err,
+                                    sizeof err);
+        }
+        if (rc == MM_OK && cudaStreamSynchronize(st) != cudaSuccess) rc = MM_ERR_CUDA;
         cudaStreamDestroy(st);
         if (rc != MM_OK) {
             mm_plan_destroy(p);
@@ -620,7 +643,7 @@ extern "C" MM_API int mm_plan_nsim(mm_plan p) { return p ? p->nsim : 0; }
 extern "C" MM_API int mm_plan_destroy(mm_plan p) {
     if (!p) return MM_OK;
     if (p->graph) cudaGraphExecDestroy(p->graph);
-    void* bufs[] = {p->khat, p->tw, p->S, p->d_sims, p->d_sim_msat, p->Y[0], p->Y[1], p->K1[0], p->K1[1], p->Ma,
+    void* bufs[] = {p->khat, p->khat_d, p->khat_ex, p->tw, p->S, p->d_sims, p->d_sim_msat, p->Y[0], p->Y[1], p->K1[0], p->K1[1], p->Ma,
                     p->Mb, p->Mtmp, p->ctl, p->dsum, p->red, p->dres, p->tq};
     for (void* b : bufs)
         if (b) cudaFree(b);
@@ -658,6 +681,9 @@ extern "C" MM_API int mm_plan_set_problem(mm_plan p, const mm_problem* prob) {
         if (prob->n[i] != p->prob.n[i] || prob->cell[i] != p->prob.cell[i] || prob->pbc[i] != p->prob.pbc[i])
             return set_err(MM_ERR_ARG, "geometry of a plan cannot change");
     if ((prob->demag != 0) != p->demag) return set_err(MM_ERR_ARG, "demag on/off cannot change after plan creation");
+    if ((prob->demag_exchange != 0) != (p->khat_d != nullptr))
+        return set_err(MM_ERR_ARG, "demag_exchange on/off cannot change after plan creation");
+    if (prob->demag_exchange && prob->aex_mask) return set_err(MM_ERR_ARG, "demag_exchange needs a uniform Aex");
     if (!(prob->gamma != 0.0)) return set_err(MM_ERR_ARG, "gamma must be non-zero");
     if (p->nsim == 1 && !(prob->msat != 0.0)) return set_err(MM_ERR_ARG, "Msat must be non-zero");
     p->prob = *prob;
@@ -665,6 +691,12 @@ extern "C" MM_API int mm_plan_set_problem(mm_plan p, const mm_problem* prob) {
     free_graph(p);
     int rc = upload_sims(p);
     if (rc) return rc;
+    if (p->khat_d) {  // the demag+exchange kernel depends on Aex and Ms
+        const long long oct = (long long)p->g.kd[0] * p->g.kd[1] * p->g.kd[2];
+        if ((rc = combine_dex(p->khat_d, p->khat_ex, oct, 2.0 * prob->aex / (MU0 * prob->msat * prob->msat), p->khat,
+                              0)))
+            return set_err(rc, "demag+exchange kernel update failed");
+    }
     // gamma is part of h = dt*gamma on the device
     if ((rc = read_ctl(p, 0))) return rc;
     for (int b = 0; b < p->nsim; b++) {
@@ -708,7 +740,9 @@ static int launch_conv(mm_plan p, PP m_in, const DevCtl* ctl, int skip_retry, cu
         return MM_OK;
     };
     int rc;
-    CUCHK(launch_xfwd<float2, float>(g.M, nullptr, m_in, p->P.msat_mask, p->S, 3 * n0 * n1, n0, n1, L1, n2, n2, g.hp,
+    // demagexch convolves m itself (mod_demagexchange.go:207-209), demag convolves Ms_mask m
+    const float* in_mask = p->khat_d ? nullptr : p->P.msat_mask;
+    CUCHK(launch_xfwd<float2, float>(g.M, nullptr, m_in, in_mask, p->S, 3 * n0 * n1, n0, n1, L1, n2, n2, g.hp,
                                      p->tw, ctl, skip_retry, st, ns, p->n3(), sb, p->P.mask_bstride));
     if ((rc = mark())) return rc;
     if (L0 == 1) {

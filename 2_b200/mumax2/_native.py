@@ -45,6 +45,7 @@ class MMProblem(C.Structure):
         ("p_mask", C.c_void_p * 3),
         ("sl_pol_mask", C.c_void_p), ("lambda_mask", C.c_void_p), ("eps_prime_mask", C.c_void_p),
         ("t_fl_mask", C.c_void_p),
+        ("demag_exchange", C.c_int),
     ]
 
 
@@ -172,6 +173,7 @@ def make_problem(d, masks=None):
     for k in ["demag", "exchange", "anis", "zeeman", "thermal", "zhangli", "slonczewski"]:
         setattr(s, k, int(d.get(k, 0)))
     s.demag_accuracy = int(d.get("demag_accuracy", 6))
+    s.demag_exchange = int(d.get("demag_exchange", 0))
     for k, dv in [("msat", 8e5), ("aex", 1.3e-11), ("alpha", 0.02), ("gamma", 2.211e5), ("ku", 0.0),
                   ("temp", 0.0), ("zl_pol", 1.0), ("xi", 0.05), ("sl_pol", 1.0), ("eps_prime", 0.0),
                   ("t_fl", 0.0)]:

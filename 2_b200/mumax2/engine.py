@@ -107,6 +107,7 @@ class Engine:
             return
         loaders = {
             "micromagnetism": self._load_micromag, "demag": self._load_demag, "exchange6": self._load_exchange,
+            "demagexch": self._load_demagexch,
             "llg": self._load_llg, "zeeman": self._load_zeeman, "anisotropy/uniaxial": self._load_anis,
             "temperature/brown": self._load_temp, "zhang-li": self._load_zl, "slonczewski": self._load_slon,
             "maxtorque": self._load_maxtorque, "micromag/energy": self._load_energy,
@@ -135,6 +136,12 @@ class Engine:
     def _load_demag(self):
         self._load_magnetization()
         self._add("B", 3, FIELD, "T", "demag field")
+
+    def _load_demagexch(self):  # mod_demagexchange.go:26-78
+        self._load_magnetization()
+        self._add("Aex", 1, VALUE, "J/m", "exchange coefficient")
+        self._add("demag_acc", 1, VALUE, "", "demag field accuracy", [8.0])
+        self._add("H_dex", 3, FIELD, "A/m", "demag+exchange field")
 
     def _load_exchange(self):
         self._load_magnetization()
@@ -213,7 +220,9 @@ class Engine:
             raise RuntimeError("set the grid size and cell size first")
         has = self.has
         prob = dict(n=self.size, cell=self.cell, pbc=tuple(self.periodic),
-                    demag=int("demag" in self.modules or "micromagnetism" in self.modules),
+                    demag=int("demag" in self.modules or "micromagnetism" in self.modules
+                              or "demagexch" in self.modules),
+                    demag_exchange=int("demagexch" in self.modules),
                     exchange=int(has("Aex")), anis=int(has("Ku")), zeeman=int(has("B_ext")),
                     thermal=int(has("Temp")), zhangli=int("zhang-li" in self.modules),
                     slonczewski=int("slonczewski" in self.modules),
@@ -227,6 +236,8 @@ class Engine:
                     p=tuple(self.quant("p").mult) if has("p") else (0, 0, 1), sl_pol=self._mult("pol", 1.0),
                     eps_prime=self._mult("epsilon_prime"), t_fl=self._mult("t_fl"))
         prob["lambda"] = self._mult("lambda", 1.0)
+        if "demagexch" in self.modules:
+            prob["demag_accuracy"] = int(self._mult("demag_acc", 8.0))
         masks = {}
         names = {"msat": "Msat", "aex": "Aex", "alpha": "alpha", "ku": "Ku", "temp": "Temp", "xi": "xi",
                  "zl_pol": "polarisation", "sl_pol": "pol", "lambda": "lambda", "eps_prime": "epsilon_prime",
@@ -243,7 +254,8 @@ class Engine:
     def _ensure_plan(self):
         from .plan import Plan
         prob, masks = self._problem()
-        key = (prob["n"], prob["cell"], prob["pbc"], prob["demag"])
+        key = (prob["n"], prob["cell"], prob["pbc"], prob["demag"], prob.get("demag_exchange", 0),
+               prob.get("demag_accuracy", 6))
         if self.plan is None or self._plan_key != key:
             m = self._state_host()
             if self.plan is not None:
@@ -376,7 +388,7 @@ class Engine:
         m = torch.as_tensor(plan.get_state(), device=plan.device)
         st = plan.stats()
         f = plan.fields(m, noise_step=0, dt_thermal=st["dt"])
-        table = {"h_eff": "eff", "h_ex": "ex", "h_anis": "anis", "h_therm": "therm"}
+        table = {"h_eff": "eff", "h_ex": "ex", "h_anis": "anis", "h_therm": "therm", "h_dex": "demag"}
         if lname in table:
             return f[table[lname]].cpu().numpy()
         if lname == "b":

@@ -8,7 +8,9 @@
  * Which reference interface each entry point replaces:
  *   mm_plan_create        MaxwellPlan.init/EnableDemag/loadDipoleKernel/LoadKernel
  *                         (src/mumax/modules/maxwell_convolution.go:72-100,112-120,176-192,313-410)
- *                         + Kernel_Arne (src/mumax/modules/kernel_magnetostatic.go:30-181)
+ *                         + Kernel_Arne (src/mumax/modules/kernel_magnetostatic.go:30-181);
+ *                         with demag_exchange, module demagexch's kernel chain
+ *                         (mod_demagexchange.go:26-205, kernel_exchange.go:102-123)
  *   mm_fields             the H_eff SumUpdater and its parents: MaxwellPlan.UpdateB
  *                         (maxwell_convolution.go:222-309), exch6Updater (mod_exchange6.go:40-51),
  *                         UniaxialAnisUpdater (mod_uniaxialanisotropy.go:44-57), zeeman
@@ -81,6 +83,11 @@ typedef struct mm_problem {
     const float *temp_mask, *xi_mask, *zl_pol_mask;
     const float *p_mask[3];
     const float *sl_pol_mask, *lambda_mask, *eps_prime_mask, *t_fl_mask;
+    /* 1: module demagexch (mod_demagexchange.go:26-205): the exchange field is folded into
+     * the demag kernel (Ms K_demag + 2Aex/(mu0 Ms) Laplacian, kernel_exchange.go:102-123)
+     * and computed by the same convolution of m; the 6-neighbour stencil term is off.
+     * Needs demag = 1, a uniform Aex (no aex_mask) and nsim = 1. */
+    int demag_exchange;
 } mm_problem;
 
 /* Scalars of one simulation of a batched plan (the multipliers of Msat, Aex, alpha, B_ext,

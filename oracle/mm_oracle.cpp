@@ -77,6 +77,7 @@ typedef struct {
     const float *temp_mask, *xi_mask, *zl_pol_mask;
     const float *p_mask[3];
     const float *sl_pol_mask, *lambda_mask, *eps_prime_mask, *t_fl_mask;
+    int demag_exchange;   // module demagexch: exchange inside the demag convolution
 } or_desc;
 
 typedef struct {
@@ -301,6 +302,29 @@ extern "C" void or_thermal_normals(unsigned long long seed, long long cell, long
     out[2] = r1 * std::cos(2.0 * PI * u3);
 }
 
+// ---------------------------------------------------------------- exchange kernel
+// Exch6NgbrKernel (kernel_exchange.go:102-123): the 6-neighbour Laplacian as a convolution
+// kernel on the padded grid, written in the reference's order -- centre first, then the
+// +-1 neighbours along x, y, z, each index wrapped (kernel.go:19-27) -- so that along a
+// dimension of size 1 the neighbour values overwrite the centre.
+static void or_exchange_kernel(const int L[3], const double cell[3], std::vector<double>& k) {
+    const long NL = (long)L[0] * L[1] * L[2];
+    k.assign(NL, 0.0);
+    auto wrap = [](int v, int n) { while (v < 0) v += n; while (v >= n) v -= n; return v; };
+    auto at = [&](int x, int y, int z) -> double& {
+        return k[((long)wrap(x, L[0]) * L[1] + wrap(y, L[1])) * L[2] + wrap(z, L[2])];
+    };
+    const double hx = cell[0] * cell[0], hy = cell[1] * cell[1], hz = cell[2] * cell[2];
+    // the reference stores float32 values (host.Array)
+    at(0, 0, 0) = (float)(-2 / hx - 2 / hy - 2 / hz);
+    at(+1, 0, 0) = (float)(1 / hx);
+    at(-1, 0, 0) = (float)(1 / hx);
+    at(0, +1, 0) = (float)(1 / hy);
+    at(0, -1, 0) = (float)(1 / hy);
+    at(0, 0, +1) = (float)(1 / hz);
+    at(0, 0, -1) = (float)(1 / hz);
+}
+
 // ---------------------------------------------------------------- problem
 struct OrProblem {
     or_desc d;
@@ -357,6 +381,7 @@ extern "C" void* or_create(const or_desc* desc) {
     }
     or_padded_size(d.n, d.pbc, P->L);
     P->NL = (long)P->L[0] * P->L[1] * P->L[2];
+    if (d.demag_exchange) d.exchange = 0;  // the stencil term is inside the kernel
     if (d.demag) {
         std::vector<double> K(9 * P->NL);
         or_kernel_arne(P->L, d.cell, d.pbc, d.demag_accuracy > 0 ? d.demag_accuracy : 6, 0, K.data());
@@ -368,9 +393,18 @@ extern "C" void* or_create(const or_desc* desc) {
             for (long i = 0; i < P->NL; i++) cmax = std::max(cmax, std::fabs(src[i]));
             // maxwell_convolution.go:412-418 IsZero (zero_tolerance 1e-5 of the global max)
             P->comp_nonzero[q] = kmax > 0 && (cmax / kmax) >= 1e-5;
+            if (q < 3 && d.demag_exchange) P->comp_nonzero[q] = true;
             if (!P->comp_nonzero[q]) continue;
             P->khat[q].resize(P->NL);
             for (long i = 0; i < P->NL; i++) P->khat[q][i] = cplx(src[i], 0);
+            if (q < 3 && d.demag_exchange) {
+                // mod_demagexchange.go:145-157: dex = Ms K_demag + 2Aex/(mu0 Ms) K_exch; the
+                // field is Ms * conv(K, m) here, so K gets K_exch * 2Aex/(mu0 Ms^2)
+                const double c = 2.0 * d.aex / (MU0 * d.msat * d.msat);
+                std::vector<double> kex;
+                or_exchange_kernel(P->L, d.cell, kex);
+                for (long i = 0; i < P->NL; i++) P->khat[q][i] += cplx(c * kex[i], 0);
+            }
             fft3d(P->khat[q].data(), P->L, -1);
         }
         for (int c = 0; c < 3; c++) P->work[c].resize(P->NL);
@@ -400,7 +434,8 @@ extern "C" void or_normalize(void* p, double* m) {
 }
 
 // Demag field H = B/mu0 = Ms_mul * IFFT(Khat . FFT(pad(m * Msat_mask))) / prod(L)
-// (maxwell_convolution.go:222-309).
+// (maxwell_convolution.go:222-309).  With demagexch the convolved input is m itself
+// (mod_demagexchange.go:207-209, ConvPlan.Convolve of m).
 static void demag_field(OrProblem* P, const double* m, double* H) {
     const or_desc& d = P->d;
     const int* n = d.n;
@@ -414,7 +449,7 @@ static void demag_field(OrProblem* P, const double* m, double* H) {
                 for (int k = 0; k < n[2]; k++) {
                     long src = ((long)i * n[1] + j) * n[2] + k;
                     long dst = ((long)i * L[1] + j) * L[2] + k;
-                    w[dst] = cplx(m[c * N + src] * mk(d.msat_mask, src), 0);
+                    w[dst] = cplx(m[c * N + src] * (d.demag_exchange ? 1.0 : mk(d.msat_mask, src)), 0);
                 }
         fft3d(w, L, -1);
     }

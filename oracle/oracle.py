@@ -36,6 +36,7 @@ class OrDesc(C.Structure):
         ("temp_mask", FP), ("xi_mask", FP), ("zl_pol_mask", FP),
         ("p_mask", FP * 3),
         ("sl_pol_mask", FP), ("lambda_mask", FP), ("eps_prime_mask", FP), ("t_fl_mask", FP),
+        ("demag_exchange", C.c_int),
     ]
 
 
@@ -94,7 +95,7 @@ DEFAULTS = dict(
     demag_accuracy=6, msat=8e5, aex=1.3e-11, alpha=0.02, gamma=2.211e5,
     bext=(0.0, 0.0, 0.0), ku=0.0, anisu=(0.0, 0.0, 1.0), temp=0.0, seed=0,
     j=(0.0, 0.0, 0.0), zl_pol=1.0, xi=0.05, p=(0.0, 0.0, 1.0), sl_pol=1.0, **{"lambda": 1.0},
-    eps_prime=0.0, t_fl=0.0,
+    eps_prime=0.0, t_fl=0.0, demag_exchange=0,
 )
 
 
@@ -114,6 +115,7 @@ def make_desc(d):
     for k in ["demag", "exchange", "anis", "zeeman", "thermal", "zhangli", "slonczewski",
               "demag_accuracy"]:
         setattr(s, k, int(d[k]))
+    s.demag_exchange = int(d.get("demag_exchange", 0))
     for k in ["msat", "aex", "alpha", "gamma", "ku", "temp", "zl_pol", "xi", "sl_pol",
               "eps_prime", "t_fl"]:
         setattr(s, k, float(d[k]))

@@ -66,3 +66,35 @@ def test_relax_idiom_run_until_smaller():
     mm.run_until_smaller("maxtorque", thr)     # api.go:122-131, relax idiom of stdproblem5.py:55
     assert mm.gets("maxtorque") < thr
     mm.reset()
+
+
+def test_demagexch_module_script():
+    """load("demagexch") + llg + solver: the combined convolution drives the dynamics."""
+    import oracle as O
+    from mumax2 import engine as mm
+    mm.reset()
+    mm.setgridsize(16, 8, 2)
+    mm.setcellsize(4e-9, 4e-9, 3e-9)
+    mm.load("demagexch")
+    mm.load("llg")
+    mm.load("solver/rk23")
+    mm.setv("Msat", 8e5)
+    mm.setv("Aex", 1.3e-11)
+    mm.setv("alpha", 0.1)
+    mm.setv("m_maxerror", 1e-5)
+    mm.setarray("m", [[[[1]]], [[[0.2]]], [[[0.1]]]])
+    mm.run(2e-12)
+    m_user = mm.getv("<m>")
+    n = (2, 8, 16)
+    o = O.Oracle(O.full_desc(n=n, cell=(3e-9, 4e-9, 4e-9), demag=1, exchange=1, msat=8e5, aex=1.3e-11,
+                             alpha=0.1, demag_exchange=1, demag_accuracy=8))
+    N = 2 * 8 * 16
+    m = np.zeros(3 * N)
+    m[:N], m[N:2 * N], m[2 * N:] = 0.1, 0.2, 1.0
+    r = O.OracleRun(o, m, solver="rk23", dt=1e-15, maxerr=1e-5)
+    r.run(2e-12)
+    mo = o.average(o.normalize(r.m))[::-1]
+    assert np.abs(np.array(m_user) - mo).max() < 1e-4
+    h = mm.getarray("H_dex")
+    assert h.shape == (3, 16, 8, 2) and np.abs(h).max() > 0
+    mm.reset()
