@@ -69,6 +69,7 @@ struct SimScalars {
     float therm_num;            // alpha * kB * 2 * T
     float zl_pre;               // P muB/(e Msat)
     float sl_beta_prime, sl_pre_fld;
+    float jmul[3];              // current density multiplier (A/m^2)
     double therm_den;           // mu0 * V * gamma * Msat  (dt applied on device)
     unsigned long long seed;    // thermal Philox key
 };
@@ -90,7 +91,6 @@ struct FieldParams {
     long long mask_bstride;     // 0 (shared masks) or N
     float cinv2[3];             // 1/cell^2
     float xi;
-    float jmul[3];
     float c12inv[3];            // 1/(12 cell)
     float lambda, t_fl;
     float p[3];
@@ -100,6 +100,12 @@ struct FieldParams {
     const float *temp_mask, *xi_mask, *zl_pol_mask;
     const float *p_mask[3];
     const float *sl_pol_mask, *lambda_mask, *eps_prime_mask, *t_fl_mask;
+    // SetPointwise time tables (device, rows t v0 v1 v2): 0 = B_ext (T), 1 = j (A/m^2)
+    struct TimeTable {
+        const double* rows;
+        int n;
+        int pad;
+    } tab[2];
 };
 
 // Selects which of the two ping-pong buffers is read/written, from ctl->cur:
@@ -142,6 +148,7 @@ struct StageOp {
     int want_energy;
     int skip_if_retry;   // k0 of RK12/Heun: a retried attempt keeps the old k0
     int pad;
+    double c_time;       // the evaluation is at t + c_time * dt (time tables)
 };
 
 // Symmetric demag kernel in k-space, stored for one octant only:
@@ -165,6 +172,7 @@ struct EpiArgs {
     unsigned int* tq_out;      // standalone max |k|^2 per simulation (float bits), may be NULL
     int skip_retry;
     long long spec_bstride;    // complex elements between simulations in the spectrum
+    double t_eval;             // time of a standalone evaluation (time tables)
 };
 
 // ---- launchers (conv.cu, rhs.cu)

@@ -338,6 +338,11 @@ struct mm_plan_s {
     int graph_solver = -1;
     bool graph_run_until = false;
     long long version = 0;           // bumped whenever captured launches would change
+    double* tab[2] = {nullptr, nullptr};  // SetPointwise tables (device rows t v0 v1 v2)
+    int tab_n[2] = {0, 0};
+    int tab_cap[2] = {0, 0};
+    std::vector<double> tab_host[2];
+    double t_eval = 0.0;             // time of standalone evaluations
     long long bytes = 0;
     long long n3() const { return 3 * g.N; }
     long long spec_bstride() const { return 3LL * g.n[0] * g.L[1] * g.hp; }
@@ -371,6 +376,7 @@ static SimScalars fold_scalars(const mm_problem& q, const mm_sim& m) {
     const double beta = HBAR * q.gamma / (MU0 * QE * m.msat);
     s.sl_beta_prime = (float)(q.sl_pol * beta);
     s.sl_pre_fld = (float)(beta * q.eps_prime);
+    for (int i = 0; i < 3; i++) s.jmul[i] = (float)q.j[i];
     return s;
 }
 
@@ -408,7 +414,6 @@ static void fill_params(mm_plan p) {
     for (int i = 0; i < 3; i++) P.cinv2[i] = (float)(1.0 / ((double)q.cell[i] * (double)q.cell[i]));
     P.xi = (float)q.xi;
     for (int i = 0; i < 3; i++) {
-        P.jmul[i] = (float)q.j[i];
         P.c12inv[i] = 1.0f / (12.0f * (float)q.cell[i]);
         P.p[i] = (float)q.p[i];
     }
@@ -432,6 +437,10 @@ static void fill_params(mm_plan p) {
     P.lambda_mask = q.lambda_mask;
     P.eps_prime_mask = q.eps_prime_mask;
     P.t_fl_mask = q.t_fl_mask;
+    for (int w = 0; w < 2; w++) {
+        P.tab[w].rows = p->tab[w];
+        P.tab[w].n = p->tab_n[w];
+    }
 }
 
 // Uploads the per-simulation scalars (nsim > 1) and refreshes the parameter block.
@@ -643,7 +652,7 @@ extern "C" MM_API int mm_plan_nsim(mm_plan p) { return p ? p->nsim : 0; }
 extern "C" MM_API int mm_plan_destroy(mm_plan p) {
     if (!p) return MM_OK;
     if (p->graph) cudaGraphExecDestroy(p->graph);
-    void* bufs[] = {p->khat, p->khat_d, p->khat_ex, p->tw, p->S, p->d_sims, p->d_sim_msat, p->Y[0], p->Y[1], p->K1[0], p->K1[1], p->Ma,
+    void* bufs[] = {p->tab[0], p->tab[1], p->khat, p->khat_d, p->khat_ex, p->tw, p->S, p->d_sims, p->d_sim_msat, p->Y[0], p->Y[1], p->K1[0], p->K1[1], p->Ma,
                     p->Mb, p->Mtmp, p->ctl, p->dsum, p->red, p->dres, p->tq};
     for (void* b : bufs)
         if (b) cudaFree(b);
@@ -789,6 +798,7 @@ static int launch_eval(mm_plan p, const StageOp& op, DevCtl* ctl, int skip_retry
     A.tq_out = tq_out;
     A.skip_retry = skip_retry;
     A.spec_bstride = p->spec_bstride();
+    A.t_eval = p->t_eval;
     int nb = 0, rc;
     if (p->demag) {
         if ((rc = launch_conv(p, op.m_in, ctl, skip_retry, st))) return rc;
@@ -814,11 +824,56 @@ static StageOp op_blank() {
     return o;
 }
 
+// host copy of the device table lookup (update_pointwise.go:30-88); false past the end
+static bool host_table_ok(const std::vector<double>& rows, double t) {
+    const size_t n = rows.size() / 4;
+    return n == 0 || rows[4 * (n - 1)] >= t;
+}
+
+// Standalone evaluations happen at simulation 0's time when time tables are set.
+static int standalone_time(mm_plan p, cudaStream_t st) {
+    if (!p->tab_n[0] && !p->tab_n[1]) return MM_OK;
+    int rc = read_ctl(p, st);
+    if (rc) return rc;
+    p->t_eval = p->ctl_host[0].t;
+    for (int w = 0; w < 2; w++)
+        if (!host_table_ok(p->tab_host[w], p->t_eval))
+            return set_err(MM_ERR_RANGE, "time %g s is past the end of the %s table", p->t_eval,
+                           w == 0 ? "B_ext" : "j");
+    return MM_OK;
+}
+
+extern "C" MM_API int mm_set_table(mm_plan p, int quantity, int npoints, const double* rows) {
+    if (!p) return set_err(MM_ERR_ARG, "null plan");
+    if (quantity != MM_TABLE_BEXT && quantity != MM_TABLE_J) return set_err(MM_ERR_ARG, "unknown table %d", quantity);
+    if (npoints < 0 || npoints == 1) return set_err(MM_ERR_ARG, "a time table needs at least two points");
+    if (npoints > 0 && !rows) return set_err(MM_ERR_ARG, "null rows");
+    for (int i = 1; i < npoints; i++)
+        if (!(rows[4 * i] >= rows[4 * (i - 1)])) return set_err(MM_ERR_ARG, "table times must be non-decreasing");
+    const int w = quantity;
+    if (npoints > p->tab_cap[w]) {
+        if (p->tab[w]) cudaFree(p->tab[w]);
+        p->tab[w] = nullptr;
+        p->tab_cap[w] = 0;
+        int rc = dalloc(p, (void**)&p->tab[w], sizeof(double) * 4 * (size_t)npoints);
+        if (rc) return rc;
+        p->tab_cap[w] = npoints;
+    }
+    if (npoints > 0) CUCHK(cudaMemcpy(p->tab[w], rows, sizeof(double) * 4 * (size_t)npoints, cudaMemcpyHostToDevice));
+    p->tab_host[w].assign(rows, rows + 4 * (size_t)npoints);
+    p->tab_n[w] = npoints;
+    fill_params(p);
+    free_graph(p);
+    return MM_OK;
+}
+
 extern "C" MM_API int mm_fields(mm_plan p, const float* m, long long noise_step, double dt_thermal, float* h_demag,
                                 float* h_ex, float* h_anis, float* h_zee, float* h_therm, float* h_eff,
                                 mm_stream stream) {
     if (!p || !m) return set_err(MM_ERR_ARG, "null argument");
     cudaStream_t st = (cudaStream_t)stream;
+    int rc = standalone_time(p, st);
+    if (rc) return rc;
     StageOp op = op_blank();
     op.m_in = fixed(const_cast<float*>(m));
     float* dbg[6] = {h_demag, h_ex, h_anis, h_zee, h_therm, h_eff};
@@ -836,8 +891,9 @@ extern "C" MM_API int mm_torque(mm_plan p, float* m, long long noise_step, doubl
                                 mm_stream stream) {
     if (!p || !m || !torque) return set_err(MM_ERR_ARG, "null argument");
     cudaStream_t st = (cudaStream_t)stream;
-    int rc = normalize_launch(p, m, st);
+    int rc = standalone_time(p, st);
     if (rc) return rc;
+    if ((rc = normalize_launch(p, m, st))) return rc;
     StageOp op = op_blank();
     op.m_in = fixed(m);
     op.k_out = fixed(torque);
@@ -922,6 +978,7 @@ static int enqueue_attempt(mm_plan p, cudaStream_t st) {
             o0.ak[0] = 1.0;
         }
         const int skip = (s == MM_RK12) ? 1 : 0;
+        o0.c_time = 0.0;
         if ((rc = launch_eval(p, o0, ctl, skip, nullptr, 0, 0, nullptr, nullptr, st, nullptr))) return rc;
         if (p->run_until) {
             CUCHK(launch_controller(p, st, 2, 0, 0, 0, 0, 0));
@@ -937,6 +994,7 @@ static int enqueue_attempt(mm_plan p, cudaStream_t st) {
             // corrector: y = y_pred + h/2 k1 - h/2 k0 (solve_rk12.go:154, solve_heun.go:63)
             StageOp o1 = op_blank();
             o1.m_in = fixed(p->Ma);
+            o1.c_time = 1.0;  // the corrector is evaluated at t + dt (solve_rk12.go:138, solve_heun.go:56)
             o1.do_combine = 1;
             o1.base_is_cur = 1;
             o1.next = oth_of(p->Y);
@@ -985,6 +1043,7 @@ static int enqueue_attempt(mm_plan p, cudaStream_t st) {
         StageOp o = op_blank();
         o.m_in = mbuf(i);
         o.k_out = kbuf(i);
+        for (int j = 0; j < i; j++) o.c_time += A(i, j);  // stage time t + c_i dt
         if (i + 1 < S) {
             o.do_combine = 1;
             o.base = cur_of(p->Y);
@@ -1188,6 +1247,8 @@ static int summary_status(mm_plan p) {
     char num[32] = "";
     if (p->nsim > 1) snprintf(num, sizeof num, "%d", s.bad_sim);
     if (s.status == MM_ERR_NAN) return set_err(MM_ERR_NAN, "NaN in the torque at step %lld%s%s", s.step, who, num);
+    if (s.status == MM_ERR_RANGE)
+        return set_err(MM_ERR_RANGE, "time past the end of a time table (step %lld%s%s)", s.step, who, num);
     return set_err(s.status, "solver cannot converge after 10 bad steps (step %lld%s%s)", s.step, who, num);
 }
 
@@ -1355,6 +1416,7 @@ extern "C" MM_API int mm_batch_maxtorque(mm_plan p, double* out, mm_stream strea
     int rc = read_ctl(p, st);
     if (rc) return rc;
     const DevCtl& c0 = p->ctl_host[0];
+    if ((rc = standalone_time(p, st))) return rc;
     CUCHK(cudaMemsetAsync(p->tq, 0, sizeof(unsigned int) * p->nsim, st));
     StageOp o = op_blank();
     o.m_in = fixed(state_ptr(p));
@@ -1409,6 +1471,7 @@ extern "C" MM_API int mm_batch_energy(mm_plan p, double* out, mm_stream stream) 
     cudaStream_t st = (cudaStream_t)stream;
     int rc = read_ctl(p, st);
     if (rc) return rc;
+    if ((rc = standalone_time(p, st))) return rc;
     StageOp o = op_blank();
     o.m_in = fixed(state_ptr(p));
     o.want_energy = 1;

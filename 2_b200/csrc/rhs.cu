@@ -170,9 +170,9 @@ __device__ __forceinline__ float3 cell_rhs(const FieldParams& P, const SimScalar
     float3 k = make_float3(g * (cx + dx * al), g * (cy + dy * al), g * (cz + dz * al));
     if (P.zhangli) {
         float msat = P.msat_mask ? __ldg(P.msat_mask + im) : 1.0f;
-        float3 j0 = make_float3(P.j_mask[0] ? __ldg(P.j_mask[0] + im) * P.jmul[0] : P.jmul[0],
-                                P.j_mask[1] ? __ldg(P.j_mask[1] + im) * P.jmul[1] : P.jmul[1],
-                                P.j_mask[2] ? __ldg(P.j_mask[2] + im) * P.jmul[2] : P.jmul[2]);
+        float3 j0 = make_float3(P.j_mask[0] ? __ldg(P.j_mask[0] + im) * S.jmul[0] : S.jmul[0],
+                                P.j_mask[1] ? __ldg(P.j_mask[1] + im) * S.jmul[1] : S.jmul[1],
+                                P.j_mask[2] ? __ldg(P.j_mask[2] + im) * S.jmul[2] : S.jmul[2]);
         float njn = sqrtf(j0.x * j0.x + j0.y * j0.y + j0.z * j0.z);
         if (msat != 0.0f && njn != 0.0f) {
             msat = 1.0f / msat;
@@ -213,9 +213,9 @@ __device__ __forceinline__ float3 cell_rhs(const FieldParams& P, const SimScalar
     }
     if (P.slonczewski) {
         float Ms = P.msat_mask ? __ldg(P.msat_mask + im) : 1.0f;
-        float3 J = make_float3(P.j_mask[0] ? __ldg(P.j_mask[0] + im) * P.jmul[0] : P.jmul[0],
-                               P.j_mask[1] ? __ldg(P.j_mask[1] + im) * P.jmul[1] : P.jmul[1],
-                               P.j_mask[2] ? __ldg(P.j_mask[2] + im) * P.jmul[2] : P.jmul[2]);
+        float3 J = make_float3(P.j_mask[0] ? __ldg(P.j_mask[0] + im) * S.jmul[0] : S.jmul[0],
+                               P.j_mask[1] ? __ldg(P.j_mask[1] + im) * S.jmul[1] : S.jmul[1],
+                               P.j_mask[2] ? __ldg(P.j_mask[2] + im) * S.jmul[2] : S.jmul[2]);
         float nJn = sqrtf(J.x * J.x + J.y * J.y + J.z * J.z);
         float tfl = P.t_fl_mask ? __ldg(P.t_fl_mask + im) * P.t_fl : P.t_fl;
         if (nJn != 0.0f && Ms != 0.0f && tfl != 0.0f) {
@@ -470,6 +470,44 @@ __device__ __forceinline__ void epilogue_cells_begin(const EpiArgs& A, const Dev
         for (int q = 0; q < 6; q++) dbg[q] = at_off(A.dbg[q], off);
 }
 
+// PointwiseUpdater.Update (update_pointwise.go:30-88): first row with time >= t, linear
+// interpolation from the row before; 0 at or before the first row; false past the last.
+__device__ bool table_value(const FieldParams::TimeTable& T, double t, double out[3]) {
+    int i = 0;
+    while (i < T.n && T.rows[4 * i] < t) i++;
+    if (i >= T.n) return false;
+    if (i == 0) {
+        out[0] = out[1] = out[2] = 0.0;
+        return true;
+    }
+    const double* a = T.rows + 4 * (i - 1);
+    const double* b = T.rows + 4 * i;
+    const double f = (t - a[0]) / (b[0] - a[0]);
+    for (int c = 0; c < 3; c++) out[c] = a[1 + c] + f * (b[1 + c] - a[1 + c]);
+    return true;
+}
+
+// The block's simulation scalars for the staged (shared-memory) variants: the
+// simulation's entry, with B_ext and j from their time tables at this evaluation's time.
+// Called by one thread.
+__device__ void stage_scalars(const EpiArgs& A, const DevCtl* ctl, SimScalars& s) {
+    s = A.P.sims ? A.P.sims[blockIdx.y] : A.P.s;
+    if (A.P.tab[0].n || A.P.tab[1].n) {
+        const double t = ctl ? ctl->t + A.op.c_time * ctl->dt : A.t_eval;
+        double v[3];
+        bool ok = true;
+        if (A.P.tab[0].n) {
+            ok = table_value(A.P.tab[0], t, v) && ok;
+            for (int c = 0; c < 3; c++) s.hz[c] = (float)(v[c] / 1.2566370614359172e-06);
+        }
+        if (A.P.tab[1].n) {
+            ok = table_value(A.P.tab[1], t, v) && ok;
+            for (int c = 0; c < 3; c++) s.jmul[c] = (float)v[c];
+        }
+        if (!ok && ctl) atomicExch(&const_cast<DevCtl*>(ctl)->status, (int)MM_ERR_RANGE);
+    }
+}
+
 template <bool BATCH>
 __device__ __forceinline__ const SimScalars& pick_scalars(const SimScalars& staged, const SimScalars& single) {
     if constexpr (BATCH) return staged;
@@ -571,7 +609,7 @@ __global__ void __launch_bounds__(384) xinv4_epi_kernel(const float2* __restrict
     if (skip_eval(ctl, A.skip_retry)) return;
     S += blockIdx.y * A.spec_bstride;
     __shared__ SimScalars s_sim;  // this simulation's scalars (BATCH); covered by the barriers below
-    if (BATCH && threadIdx.x == 0) s_sim = A.P.sims[blockIdx.y];
+    if (BATCH && threadIdx.x == 0) stage_scalars(A, ctl, s_sim);
     using F = FS<M>;
     constexpr int RPB = xinv4_rpb<M>();
     extern __shared__ unsigned char smem_raw[];
@@ -624,7 +662,7 @@ __global__ void __launch_bounds__(256) local_epi_kernel(EpiArgs A) {
     const int n1 = A.P.n[1], n2 = A.P.n[2];
     __shared__ SimScalars s_sim;
     if (BATCH) {
-        if (threadIdx.x == 0) s_sim = A.P.sims[blockIdx.y];
+        if (threadIdx.x == 0) stage_scalars(A, A.ctl ? A.ctl + blockIdx.y : nullptr, s_sim);
         __syncthreads();
     }
     const SimScalars& S = pick_scalars<BATCH>(s_sim, A.P.s);
@@ -707,13 +745,17 @@ int xinv_blocks(int M, int n0n1) {
     return (n0n1 + rpb - 1) / rpb;
 }
 
+// Staged variants (scalars in shared memory) serve batched plans and time tables.
+static bool staged_scalars(const EpiArgs& A, int nsim) { return nsim > 1 || A.P.tab[0].n || A.P.tab[1].n; }
+
 cudaError_t launch_xinv_epi(int M, const float2* S, int hp, int L1, const float2* tw, const EpiArgs& A, bool terms,
                             cudaStream_t st, int* nblocks, int nsim) {
+    const bool staged = staged_scalars(A, nsim);
     if (use_xinv4(M)) {
         switch (M) {
 #define X(m)                                                                      \
     case m:                                                                       \
-        if (nsim > 1)                                                                   \
+        if (staged)                                                                     \
             return terms ? launch_xinv4_t<m, true, true>(S, hp, L1, tw, A, st, nblocks, nsim)  \
                          : launch_xinv4_t<m, false, true>(S, hp, L1, tw, A, st, nblocks, nsim); \
         return terms ? launch_xinv4_t<m, true, false>(S, hp, L1, tw, A, st, nblocks, 1)     \
@@ -722,7 +764,7 @@ cudaError_t launch_xinv_epi(int M, const float2* S, int hp, int L1, const float2
 #undef X
         }
     }
-    if (nsim > 1) return cudaErrorNotSupported;  // batched plans use the four-step pass
+    if (staged) return cudaErrorNotSupported;  // batched plans and time tables use the four-step pass
     switch (M) {
 #define X(m)                                                                      \
     case m:                                                                       \
@@ -747,7 +789,7 @@ cudaError_t launch_local_epi(const EpiArgs& A, bool terms, cudaStream_t st, int*
     int b = local_blocks(A.P.N, nsim);
     *nblocks = b;
     const dim3 grid((unsigned)b, (unsigned)nsim);
-    if (nsim > 1) {
+    if (staged_scalars(A, nsim)) {
         if (terms) local_epi_kernel<true, true><<<grid, 256, 0, st>>>(A);
         else local_epi_kernel<false, true><<<grid, 256, 0, st>>>(A);
     } else {

@@ -21,6 +21,8 @@ MM_ERR_NOT_CONVERGED = -3
 MM_ERR_NAN = -4
 MM_ERR_STATE = -5
 MM_ERR_TIMEOUT = -6
+MM_ERR_RANGE = -7
+TABLES = {"bext": 0, "j": 1}
 
 SOLVERS = {"euler": 0, "heun": 1, "rk12": 2, "rk23": 3, "rk45": 4}
 
@@ -120,6 +122,7 @@ _PROTOS = {
     "mm_profile_eval": (C.c_int, [C.c_void_p, C.c_int, DP, C.POINTER(C.c_int), C.c_void_p]),
     "mm_plan_geometry": (C.c_int, [C.c_void_p, C.c_int * 12]),
     "mm_average_noalloc": (C.c_int, [C.c_void_p, C.c_longlong, C.c_void_p, C.c_void_p]),
+    "mm_set_table": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
     "mm_plan_create_batch": (C.c_int, [C.POINTER(MMProblem), C.c_int, C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]),
     "mm_plan_nsim": (C.c_int, [C.c_void_p]),
     "mm_batch_set_sims": (C.c_int, [C.c_void_p, C.c_void_p]),

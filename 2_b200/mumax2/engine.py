@@ -63,6 +63,8 @@ class Engine:
         self._dirty_params = True
         self._solver_dirty = True
         self._m = None       # host copy when the plan is not built yet
+        self._pointwise = {}  # SetPointwise tables: quantity -> [(t, internal value)]
+        self._tables_dirty = False
         for name, unit in [("t", "s"), ("dt", "s"), ("step", "")]:
             self._add(name, 1, VALUE, unit)
         self.q["dt"].mult = [1e-15]
@@ -262,6 +264,7 @@ class Engine:
                 self.plan.close()
             self.plan = Plan(prob, masks=masks, device=self.device)
             self._plan_key = key
+            self._tables_dirty = True
             self._dirty_params = False
             self._solver_dirty = True
             if m is not None:
@@ -270,6 +273,11 @@ class Engine:
         elif self._dirty_params:
             self.plan.set_problem(prob, masks)
             self._dirty_params = False
+        if self._tables_dirty:
+            for lname, table in (("b_ext", "bext"), ("j", "j")):
+                pts = self._pointwise.get(lname, [])
+                self.plan.set_table(table, [t for t, _ in pts], [v for _, v in pts])
+            self._tables_dirty = False
         if self._solver_dirty and self.solver_name is not None:
             self.plan.solver(self.solver_name, dt=self.quant("dt").mult[0], mindt=self._mult("mindt", 1e-38),
                              maxdt=self._mult("maxdt", 1e38), maxerr=self._mult("m_maxerror", 1.0 / 2000))
@@ -311,6 +319,24 @@ class Engine:
             self._solver_dirty = True
         else:
             self._dirty_params = True
+
+    def setpointwise(self, name, time, value):
+        """SetPointwise (api.go:172-190): `name` follows a piecewise linear function of
+        time through the given (time, value) points, evaluated on the device at every
+        solver stage.  Appending a time earlier than the last one starts a new list
+        (update_pointwise.go:91-97).  The device path covers B_ext and j."""
+        q = self.quant(name)
+        lname = name.lower()
+        if lname not in ("b_ext", "j"):
+            raise NotImplementedError(f"time tables are evaluated on the device for B_ext and j, not {name}")
+        value = [float(v) for v in np.atleast_1d(value)]
+        if len(value) != q.ncomp:
+            raise ValueError(f"{name} has {q.ncomp} components")
+        pts = self._pointwise.setdefault(lname, [])
+        if pts and pts[-1][0] > time:
+            pts.clear()
+        pts.append((float(time), _swap_vec(value)))
+        self._tables_dirty = True
 
     def getv(self, name):
         q = self.quant(name)
@@ -471,6 +497,10 @@ def setv(name, value):
     if name == "<m>":
         raise ValueError("<m> is derived")
     engine().setv(name, value)
+
+
+def setpointwise(name, time, value):
+    engine().setpointwise(name, time, value)
 
 
 def getv(name):

@@ -174,6 +174,21 @@ class Plan:
         nat.check(nat.lib().mm_energy(self.h, out, None))
         return dict(zip(["E_zeeman", "E_ex", "E_demag", "E_anis", "E"], out[:]))
 
+    # ---- time-dependent inputs
+    def set_table(self, quantity, times, values):
+        """SetPointwise table of "bext" (T) or "j" (A/m^2): values[i] (internal component
+        order) at times[i]; piecewise linear in between, evaluated on the device at every
+        stage time.  An empty table removes it."""
+        times = np.asarray(times, dtype=np.float64)
+        rows = np.zeros((len(times), 4))
+        if len(times):
+            rows[:, 0] = times
+            rows[:, 1:] = np.asarray(values, dtype=np.float64).reshape(-1, 3)
+        self._tab = getattr(self, "_tab", {})
+        self._tab[quantity] = np.ascontiguousarray(rows.ravel())
+        nat.check(nat.lib().mm_set_table(self.h, nat.TABLES[quantity], len(times),
+                                         self._tab[quantity].ctypes.data_as(C.c_void_p)))
+
     # ---- batched plans: one entry per simulation
     def set_sims(self, sims):
         self._sims = nat.make_sims(self.problem, sims)

@@ -55,7 +55,8 @@ enum {
     MM_ERR_NOT_CONVERGED = -3, /* more than 10 rejected attempts in one step (solve_rk12.go:205) */
     MM_ERR_NAN = -4,           /* NaN in the state (quant.go:427-432) */
     MM_ERR_STATE = -5,         /* call out of order (no solver, no state, ...) */
-    MM_ERR_TIMEOUT = -6        /* a bounded device wait gave up */
+    MM_ERR_TIMEOUT = -6,       /* a bounded device wait gave up */
+    MM_ERR_RANGE = -7          /* time outside a SetPointwise table (update_pointwise.go:66) */
 };
 
 /* solvers */
@@ -185,6 +186,17 @@ MM_API int mm_average_noalloc(const float* m, long long ncell, double* out, mm_s
 /* run_until_maxtorque with one threshold per simulation (thr[nsim]); each simulation
  * stops, and stays frozen, once its own maxtorque falls below its threshold. */
 MM_API int mm_batch_run_until_maxtorque(mm_plan plan, const double* thr, long long max_steps, mm_stream stream);
+
+/* ---- time-dependent inputs: SetPointwise (api.go:172-190, update_pointwise.go:30-88) ----
+ * A table of npoints rows (t, v0, v1, v2), internal component order, times
+ * non-decreasing, makes B_ext (MM_TABLE_BEXT, T) or j (MM_TABLE_J, A/m^2) a piecewise
+ * linear function of time that the kernels evaluate on the device at every stage time
+ * (t + c dt), replacing the multiplier.  As in the reference the value is 0 at or before
+ * the first time and a time past the last row is an error (MM_ERR_RANGE).  npoints = 0
+ * removes the table; otherwise npoints >= 2.  Standalone evaluations (mm_fields,
+ * mm_torque, reductions) use simulation 0's time. */
+enum { MM_TABLE_BEXT = 0, MM_TABLE_J = 1 };
+MM_API int mm_set_table(mm_plan plan, int quantity, int npoints, const double* rows);
 
 /* ---- per-simulation results of a (batched) plan; out arrays have nsim entries ---- */
 MM_API int mm_batch_stats(mm_plan plan, mm_stats* out, mm_stream stream);

@@ -336,7 +336,50 @@ struct OrProblem {
     std::vector<cplx> work[3];
     // owned mask copies (the desc points at caller memory only during or_create)
     std::vector<std::vector<float>> owned;
+    // time tables of SetPointwise (api.go:172-190): 0 = B_ext (T), 1 = j (A/m^2), rows
+    // (t, v0, v1, v2) in internal component order; the time of the current evaluation
+    std::vector<double> tab[2];
+    double t_eval = 0.0;
+    double base_bext[3], base_j[3];
 };
+
+// PointwiseUpdater.Update (update_pointwise.go:30-88): the first row with time >= t,
+// linear interpolation from the row before it; zero at or before the first row's time,
+// an error past the last row.  Returns false when t is past the table.
+static bool table_value(const std::vector<double>& tab, double t, double out[3]) {
+    const long n = (long)tab.size() / 4;
+    long i = 0;
+    while (i < n && tab[4 * i] < t) i++;
+    if (i >= n) return false;
+    if (i == 0) { out[0] = out[1] = out[2] = 0.0; return true; }
+    const double t1 = tab[4 * (i - 1)], t2 = tab[4 * i];
+    const double f = (t - t1) / (t2 - t1);
+    for (int c = 0; c < 3; c++) out[c] = tab[4 * (i - 1) + 1 + c] + f * (tab[4 * i + 1 + c] - tab[4 * (i - 1) + 1 + c]);
+    return true;
+}
+
+// Sets B_ext and j from the tables at t_eval (the multipliers otherwise).
+static bool apply_tables(OrProblem* P) {
+    bool ok = true;
+    if (!P->tab[0].empty()) ok = table_value(P->tab[0], P->t_eval, P->d.bext) && ok;
+    if (!P->tab[1].empty()) ok = table_value(P->tab[1], P->t_eval, P->d.j) && ok;
+    return ok;
+}
+
+// one table: n rows of (t, v0, v1, v2); n = 0 removes it
+extern "C" int or_set_table(void* p, int which, long n, const double* rows) {
+    OrProblem* P = (OrProblem*)p;
+    if (which < 0 || which > 1) return -1;
+    P->tab[which].assign(rows, rows + 4 * n);
+    if (n == 0) {
+        double* dst = which == 0 ? P->d.bext : P->d.j;
+        const double* src = which == 0 ? P->base_bext : P->base_j;
+        for (int c = 0; c < 3; c++) dst[c] = src[c];
+    }
+    return 0;
+}
+
+extern "C" void or_set_time(void* p, double t) { ((OrProblem*)p)->t_eval = t; }
 
 static const float* own_mask(OrProblem* P, const float* src) {
     if (!src) return nullptr;
@@ -361,6 +404,7 @@ extern "C" void* or_create(const or_desc* desc) {
     OrProblem* P = new OrProblem();
     P->d = *desc;
     or_desc& d = P->d;
+    for (int c = 0; c < 3; c++) { P->base_bext[c] = d.bext[c]; P->base_j[c] = d.j[c]; }
     P->N = (long)d.n[0] * d.n[1] * d.n[2];
     d.msat_mask = own_mask(P, desc->msat_mask);
     d.aex_mask = own_mask(P, desc->aex_mask);
@@ -564,6 +608,7 @@ static void thermal_field(OrProblem* P, long long noise_step, double dt, double*
 extern "C" void or_fields(void* p, const double* m, long long noise_step, double dt_thermal,
                           double* h_demag, double* h_ex, double* h_anis, double* h_zee,
                           double* h_therm, double* h_eff) {
+    apply_tables((OrProblem*)p);
     OrProblem* P = (OrProblem*)p;
     const or_desc& d = P->d;
     const long N = P->N;
@@ -853,7 +898,11 @@ extern "C" int or_step(void* p, int solver, double* m, or_state* st, double* k_f
     const long N3 = 3 * P->N;
     const double gam = P->d.gamma;
     const long long ns = st->noise_step;
-    auto f = [&](double* y, double* k, double dtth) {
+    // f at time tt (the stage time: time tables are evaluated there)
+    bool in_range = true;
+    auto f = [&](double* y, double* k, double dtth, double tt) {
+        P->t_eval = tt;
+        if (!apply_tables(P)) in_range = false;
         or_torque(p, y, ns, dtth, k, nullptr);
         st->evals++;
     };
@@ -861,22 +910,22 @@ extern "C" int or_step(void* p, int solver, double* m, or_state* st, double* k_f
         double dt = st->dt;
         double dtth = st->dt_thermal > 0 ? st->dt_thermal : dt;
         std::vector<double> k0(N3), k1(N3);
-        f(m, k0.data(), dtth);
+        f(m, k0.data(), dtth, st->t);
         for (long i = 0; i < N3; i++) m[i] += dt * gam * k0[i];
         st->t += dt;
         if (solver == OR_HEUN) {
-            f(m, k1.data(), dtth);
+            f(m, k1.data(), dtth, st->t);
             double h = dt * gam;
             for (long i = 0; i < N3; i++) m[i] += 0.5 * h * k1[i] - 0.5 * h * k0[i];
         }
         or_normalize(p, m);
         st->step++;
         st->noise_step++;
-        return 0;
+        return in_range ? 0 : -2;
     }
     if (solver == OR_RK12) {
         std::vector<double> y0(N3), k0(N3), k1(N3);
-        f(m, k0.data(), st->dt);
+        f(m, k0.data(), st->dt, st->t);
         std::copy(m, m + N3, y0.begin());
         const double t0 = st->t;
         const int maxTry = 10;
@@ -886,7 +935,7 @@ extern "C" int or_step(void* p, int solver, double* m, or_state* st, double* k_f
             if (tr > 0) std::copy(y0.begin(), y0.end(), m);
             for (long i = 0; i < N3; i++) m[i] += dt * gam * k0[i];
             st->t = t0 + dt;
-            f(m, k1.data(), dt);
+            f(m, k1.data(), dt, t0 + dt);
             double h = dt * gam;
             double md = 0;
             for (long i = 0; i < N3; i++) {
@@ -908,7 +957,7 @@ extern "C" int or_step(void* p, int solver, double* m, or_state* st, double* k_f
         }
         or_normalize(p, m);
         st->step++;
-        return 0;
+        return in_range ? 0 : -2;
     }
     // RK23 / RK45 with FSAL
     const bool dp = (solver == OR_RK45);
@@ -917,7 +966,7 @@ extern "C" int or_step(void* p, int solver, double* m, or_state* st, double* k_f
     std::vector<std::vector<double>> k(S, std::vector<double>(N3));
     std::vector<double> y0(m, m + N3), y(N3);
     if (k_fsal && fsal_valid && *fsal_valid) std::copy(k_fsal, k_fsal + N3, k[0].begin());
-    else { f(y0.data(), k[0].data(), st->dt); std::copy(y0.begin(), y0.end(), m); }
+    else { f(y0.data(), k[0].data(), st->dt, st->t); std::copy(y0.begin(), y0.end(), m); }
     // y0 has been normalised by f (in place on the copy) -- keep m consistent
     or_normalize(p, y0.data());
     const double t0 = st->t;
@@ -928,13 +977,15 @@ extern "C" int or_step(void* p, int solver, double* m, or_state* st, double* k_f
         double h = dt * gam;
         for (int s = 1; s < S; s++) {
             const double* a = dp ? DP_A[s] : BS_A[s];
+            double cs = 0;
+            for (int jj = 0; jj < s; jj++) cs += a[jj];
             for (long i = 0; i < N3; i++) {
                 double acc = y0[i];
                 for (int jj = 0; jj < s; jj++) acc += h * a[jj] * k[jj][i];
                 y[i] = acc;
             }
             if (s == S - 1) std::copy(y.begin(), y.end(), m);
-            f(y.data(), k[s].data(), dt);
+            f(y.data(), k[s].data(), dt, t0 + cs * dt);
             if (s == S - 1) or_normalize(p, m);
         }
         double md = 0;
@@ -961,7 +1012,7 @@ extern "C" int or_step(void* p, int solver, double* m, or_state* st, double* k_f
     if (k_fsal) std::copy(k[S - 1].begin(), k[S - 1].end(), k_fsal);
     if (fsal_valid) *fsal_valid = 1;
     st->step++;
-    return 0;
+    return in_range ? 0 : -2;
 }
 
 extern "C" int or_num_threads(void) {

@@ -81,6 +81,9 @@ def lib():
         L.or_step.argtypes = [C.c_void_p, C.c_int, DP, C.POINTER(OrState), DP, C.POINTER(C.c_int)]
         L.or_thermal_normals.argtypes = [C.c_ulonglong, C.c_longlong, C.c_longlong, C.c_double * 3]
         L.or_num_threads.restype = C.c_int
+        L.or_set_table.restype = C.c_int
+        L.or_set_table.argtypes = [C.c_void_p, C.c_int, C.c_long, DP]
+        L.or_set_time.argtypes = [C.c_void_p, C.c_double]
         _LIB = L
     return _LIB
 
@@ -168,6 +171,17 @@ class Oracle:
         lib().or_normalize(self.h, _dp(m))
         return m
 
+    def set_table(self, which, times, values):
+        """Time table of B_ext (which=0, T) or j (which=1, A/m^2): rows (t, v0, v1, v2),
+        internal component order (SetPointwise, api.go:172-190)."""
+        rows = np.ascontiguousarray(np.column_stack([np.asarray(times, float),
+                                                     np.asarray(values, float).reshape(-1, 3)]).ravel()
+                                    if len(times) else np.zeros(0))
+        lib().or_set_table(self.h, int(which), len(times), _dp(rows))
+
+    def set_time(self, t):
+        lib().or_set_time(self.h, float(t))
+
     def fields(self, m, noise_step=0, dt_thermal=0.0):
         m = self._m(m)
         out = {k: np.zeros(3 * self.N) for k in ["demag", "ex", "anis", "zee", "therm", "eff"]}
@@ -227,6 +241,8 @@ class OracleRun:
 
     def step(self):
         rc = lib().or_step(self.o.h, self.solver, _dp(self.m), C.byref(self.st), _dp(self.kf), C.byref(self.fv))
+        if rc == -2:
+            raise RuntimeError("time outside a pointwise table")
         if rc != 0:
             raise RuntimeError("oracle solver failed to converge")
 
