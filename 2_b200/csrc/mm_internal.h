@@ -45,6 +45,15 @@ struct DevCtl {
     long long step, badsteps, attempts, evals;
     long long noise_step;    // thermal noise counter (advanced once per accepted step)
     double dt_thermal;       // > 0: fixed dt for the thermal scale (cutoff_dt), else dt
+    // autotabulate on the device (notify_tabulate.go:23-28): after an accepted step with
+    // t - count*period >= period a record is due (tab_pending), written by the record
+    // kernels of the same attempt into this simulation's rows
+    double tab_period;       // <= 0: off
+    long long tab_count;     // records due so far (the reference's count)
+    long long tab_lost;      // records that found the buffer full
+    int tab_n, tab_cap;      // rows written since the last read, capacity
+    int tab_pending;
+    int pad1;
 };
 
 // Written by the controller after every attempt: what the host polls between batches.

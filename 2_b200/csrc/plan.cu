@@ -170,6 +170,11 @@ __device__ void control_one(DevCtl* c, int adaptive, int q, int fsal, int nevals
         }
         if (c->t >= c->t_end) c->done = 1;
         if (c->step >= c->step_end) c->done = 1;
+        if (c->tab_period > 0 && c->t - (double)c->tab_count * c->tab_period >= c->tab_period) {
+            if (c->tab_n < c->tab_cap) c->tab_pending = 1;
+            else c->tab_lost++;
+            c->tab_count++;
+        }
     }
     if (!fsal && c->tq_bits) c->maxtorque = sqrt((double)__uint_as_float(c->tq_bits)) * c->gamma;
     c->tq_bits = 0u;
@@ -263,9 +268,8 @@ __global__ void energy_finish_kernel(const float* red, int nblocks, double* out,
     out[g] = (double)fs + (double)fc;
 }
 
-// compensated per-component sums of the state (for <m>), one row of blocks per simulation
-__global__ void sum3_kernel(const float* m, long long N, long long bstride, float* red) {
-    m += blockIdx.y * bstride;
+// compensated per-component sums of one simulation's state m into the block's slot of red
+__device__ void sum3_block(const float* m, long long N, float* red) {
     float s[3] = {0.f, 0.f, 0.f}, c[3] = {0.f, 0.f, 0.f};
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x) {
         for (int q = 0; q < 3; q++) {
@@ -293,6 +297,53 @@ __global__ void sum3_kernel(const float* m, long long N, long long bstride, floa
         const long long slot = (long long)blockIdx.y * gridDim.x + blockIdx.x;
         red[slot * 8 + 2 * q] = fs;
         red[slot * 8 + 2 * q + 1] = fc;
+    }
+}
+
+// <m> partial sums, one row of blocks per simulation
+__global__ void sum3_kernel(const float* m, long long N, long long bstride, float* red) {
+    sum3_block(m + blockIdx.y * bstride, N, red);
+}
+
+// autotabulate: partial sums of the just-accepted state of simulations with a record due
+__global__ void tab_sum_kernel(const float* Y0, const float* Y1, const DevCtl* ctl, long long N, long long bstride,
+                               float* red) {
+    const DevCtl* c = ctl + blockIdx.y;
+    if (!c->tab_pending) return;
+    sum3_block((c->cur ? Y1 : Y0) + blockIdx.y * bstride, N, red);
+}
+
+// autotabulate: one thread per simulation folds the partials (fixed order, compensated)
+// and appends the row (t, <m>_0, <m>_1, <m>_2, maxtorque, dt, step, 0)
+__global__ void tab_finish_kernel(const float* red, int nblocks, DevCtl* ctl, int nsim, double* rec, long long N) {
+    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nsim; b += gridDim.x * blockDim.x) {
+        DevCtl* c = ctl + b;
+        if (!c->tab_pending) continue;
+        double avg[3];
+        for (int q = 0; q < 3; q++) {
+            const float* rs = red + (long long)b * nblocks * 8;
+            float fs = 0.f, fc = 0.f;
+            for (int k = 0; k < nblocks; k++) {
+                float v = rs[k * 8 + 2 * q];
+                float t = fs + v;
+                if (fabsf(fs) >= fabsf(v)) fc += (fs - t) + v;
+                else fc += (v - t) + fs;
+                fs = t;
+                fc += rs[k * 8 + 2 * q + 1];
+            }
+            avg[q] = ((double)fs + (double)fc) / (double)N;
+        }
+        double* row = rec + ((long long)b * c->tab_cap + c->tab_n) * 8;
+        row[0] = c->t;
+        row[1] = avg[0];
+        row[2] = avg[1];
+        row[3] = avg[2];
+        row[4] = c->maxtorque;
+        row[5] = c->dt;
+        row[6] = (double)c->step;
+        row[7] = 0.0;
+        c->tab_n++;
+        c->tab_pending = 0;
     }
 }
 
@@ -343,6 +394,9 @@ struct mm_plan_s {
     int tab_cap[2] = {0, 0};
     std::vector<double> tab_host[2];
     double t_eval = 0.0;             // time of standalone evaluations
+    double* rec = nullptr;           // autotabulate rows [nsim][rec_cap][8]
+    int rec_cap = 0;
+    bool tab_on = false;
     long long bytes = 0;
     long long n3() const { return 3 * g.N; }
     long long spec_bstride() const { return 3LL * g.n[0] * g.L[1] * g.hp; }
@@ -652,7 +706,7 @@ extern "C" MM_API int mm_plan_nsim(mm_plan p) { return p ? p->nsim : 0; }
 extern "C" MM_API int mm_plan_destroy(mm_plan p) {
     if (!p) return MM_OK;
     if (p->graph) cudaGraphExecDestroy(p->graph);
-    void* bufs[] = {p->tab[0], p->tab[1], p->khat, p->khat_d, p->khat_ex, p->tw, p->S, p->d_sims, p->d_sim_msat, p->Y[0], p->Y[1], p->K1[0], p->K1[1], p->Ma,
+    void* bufs[] = {p->rec, p->tab[0], p->tab[1], p->khat, p->khat_d, p->khat_ex, p->tw, p->S, p->d_sims, p->d_sim_msat, p->Y[0], p->Y[1], p->K1[0], p->K1[1], p->Ma,
                     p->Mb, p->Mtmp, p->ctl, p->dsum, p->red, p->dres, p->tq};
     for (void* b : bufs)
         if (b) cudaFree(b);
@@ -867,6 +921,51 @@ extern "C" MM_API int mm_set_table(mm_plan p, int quantity, int npoints, const d
     return MM_OK;
 }
 
+extern "C" MM_API int mm_tabulate(mm_plan p, double period, int capacity) {
+    if (!p) return set_err(MM_ERR_ARG, "null plan");
+    if (period > 0 && capacity < 1) return set_err(MM_ERR_ARG, "capacity must be >= 1");
+    if (period > 0 && capacity > p->rec_cap) {
+        if (p->rec) cudaFree(p->rec);
+        p->rec = nullptr;
+        p->rec_cap = 0;
+        int rc = dalloc(p, (void**)&p->rec, sizeof(double) * 8 * (size_t)capacity * p->nsim);
+        if (rc) return rc;
+        p->rec_cap = capacity;
+    }
+    int rc = read_ctl(p, 0);
+    if (rc) return rc;
+    for (int b = 0; b < p->nsim; b++) {
+        DevCtl& c = p->ctl_host[b];
+        c.tab_period = period > 0 ? period : 0.0;
+        c.tab_count = 0;
+        c.tab_lost = 0;
+        c.tab_n = 0;
+        c.tab_cap = period > 0 ? capacity : 0;
+        c.tab_pending = 0;
+    }
+    p->tab_on = period > 0;
+    free_graph(p);
+    return write_ctl(p, 0);
+}
+
+extern "C" MM_API int mm_tabulate_read(mm_plan p, double* out, int* counts, long long* lost, mm_stream stream) {
+    if (!p || !out || !counts) return set_err(MM_ERR_ARG, "null argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    int rc = read_ctl(p, st);
+    if (rc) return rc;
+    if (p->rec_cap > 0)
+        CUCHK(cudaMemcpyAsync(out, p->rec, sizeof(double) * 8 * (size_t)p->rec_cap * p->nsim, cudaMemcpyDeviceToHost,
+                              st));
+    CUCHK(cudaStreamSynchronize(st));
+    for (int b = 0; b < p->nsim; b++) {
+        counts[b] = p->ctl_host[b].tab_n;
+        if (lost) lost[b] = p->ctl_host[b].tab_lost;
+        p->ctl_host[b].tab_n = 0;
+        p->ctl_host[b].tab_lost = 0;
+    }
+    return write_ctl(p, st);
+}
+
 extern "C" MM_API int mm_fields(mm_plan p, const float* m, long long noise_step, double dt_thermal, float* h_demag,
                                 float* h_ex, float* h_anis, float* h_zee, float* h_therm, float* h_eff,
                                 mm_stream stream) {
@@ -949,6 +1048,22 @@ static cudaError_t launch_controller(mm_plan p, cudaStream_t st, int mode, int a
     return cudaGetLastError();
 }
 
+// blocks per simulation of the record sums
+static int tab_blocks(mm_plan p) { return std::min(p->red_blocks, std::max(1, (148 * 2 + p->nsim - 1) / p->nsim)); }
+
+// The autotabulate record kernels (no-ops unless a record is due).
+static int launch_records(mm_plan p, cudaStream_t st) {
+    if (!p->tab_on) return MM_OK;
+    const int nb = tab_blocks(p);
+    tab_sum_kernel<<<dim3((unsigned)nb, (unsigned)p->nsim), 256, 0, st>>>(p->Y[0], p->Y[1], p->ctl, p->g.N, p->n3(),
+                                                                          p->red);
+    CUCHK(cudaGetLastError());
+    tab_finish_kernel<<<(p->nsim + 127) / 128, 128, 0, st>>>(p->red, nb, p->ctl, p->nsim, p->rec, p->g.N);
+    CUCHK(cudaGetLastError());
+    p->launches += 2;
+    return MM_OK;
+}
+
 // Enqueues one step attempt of the configured solver (no host synchronisation).
 static int enqueue_attempt(mm_plan p, cudaStream_t st) {
     DevCtl* ctl = p->ctl;
@@ -1016,7 +1131,7 @@ static int enqueue_attempt(mm_plan p, cudaStream_t st) {
         }
         CUCHK(launch_controller(p, st, 1, s == MM_RK12 ? 1 : 0, 1, 0, s == MM_EULER ? 1 : 2, s == MM_RK12));
         p->launches++;
-        return MM_OK;
+        return launch_records(p, st);
     }
     // RK23 / RK45 (FSAL): K1[cur] = f(Y[cur]) is valid
     const bool dp = (s == MM_RK45);
@@ -1072,7 +1187,7 @@ static int enqueue_attempt(mm_plan p, cudaStream_t st) {
     }
     CUCHK(launch_controller(p, st, 1, 1, dp ? 4 : 2, 1, S - 1, 0));
     p->launches++;
-    return MM_OK;
+    return launch_records(p, st);
 }
 
 static int read_ctl(mm_plan p, cudaStream_t st) {

@@ -123,6 +123,8 @@ _PROTOS = {
     "mm_plan_geometry": (C.c_int, [C.c_void_p, C.c_int * 12]),
     "mm_average_noalloc": (C.c_int, [C.c_void_p, C.c_longlong, C.c_void_p, C.c_void_p]),
     "mm_set_table": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
+    "mm_tabulate": (C.c_int, [C.c_void_p, C.c_double, C.c_int]),
+    "mm_tabulate_read": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "mm_plan_create_batch": (C.c_int, [C.POINTER(MMProblem), C.c_int, C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]),
     "mm_plan_nsim": (C.c_int, [C.c_void_p]),
     "mm_batch_set_sims": (C.c_int, [C.c_void_p, C.c_void_p]),

@@ -64,6 +64,7 @@ class Engine:
         self._solver_dirty = True
         self._m = None       # host copy when the plan is not built yet
         self._pointwise = {}  # SetPointwise tables: quantity -> [(t, internal value)]
+        self._autotab = None  # (quants, filename, period, header written)
         self._tables_dirty = False
         for name, unit in [("t", "s"), ("dt", "s"), ("step", "")]:
             self._add(name, 1, VALUE, unit)
@@ -262,9 +263,13 @@ class Engine:
             m = self._state_host()
             if self.plan is not None:
                 self.plan.close()
+            if self.plan is not None and self._autotab:
+                self._drain_tab()
             self.plan = Plan(prob, masks=masks, device=self.device)
             self._plan_key = key
             self._tables_dirty = True
+            if self._autotab:
+                self.plan.tabulate(self._autotab[2], self.TAB_CAPACITY)
             self._dirty_params = False
             self._solver_dirty = True
             if m is not None:
@@ -444,19 +449,90 @@ class Engine:
     def average_m(self):
         return _swap_vec(self._ensure_plan().average())
 
+    # ------------------------------------------------------------ autotabulate
+    TAB_CAPACITY = 65536
+    TAB_COLUMNS = {"t": ([0], "s"), "<m>": ([1, 2, 3], ""), "maxtorque": ([4], "/s"), "dt": ([5], "s"),
+                   "step": ([6], "")}
+
+    def autotabulate(self, quants, filename, period):
+        """AutoTabulate (engine.go:609-617, notify_tabulate.go:23-28): the rows are
+        recorded on the device during the run and written to `filename` after it, in the
+        reference's table format (table.go:33-70).  Device columns: t, <m>, maxtorque, dt,
+        step."""
+        for q in quants:
+            if q.lower() not in self.TAB_COLUMNS and q not in self.TAB_COLUMNS:
+                raise NotImplementedError(f"device autotabulate records t, <m>, maxtorque, dt, step; not {q}")
+        self._autotab = [list(quants), filename, float(period), False]
+        if self.plan is not None:
+            self.plan.tabulate(float(period), self.TAB_CAPACITY)
+
+    def _drain_tab(self):
+        quants, filename, _, header = self._autotab
+        rows = self.plan.tabulate_read()[0]
+        cols = [self.TAB_COLUMNS.get(q, self.TAB_COLUMNS.get(q.lower())) for q in quants]
+        with open(filename, "a") as f:
+            if not header:
+                h = "#"
+                for q, (idx, unit) in zip(quants, cols):
+                    n = len(idx)
+                    for i in range(n - 1, -1, -1):
+                        comp = "_" + chr(ord("z") - i) if n > 1 else ""
+                        h += f"{q}{comp} ({unit})\t"
+                f.write(h + "\n")
+                self._autotab[3] = True
+            for r in rows:
+                line = ""
+                for idx, _ in cols:
+                    for i in reversed(idx):   # internal ZYX -> user XYZ
+                        line += go_float(r[i]) + "\t"
+                f.write(line + "\n")
+
+    def _after_run(self):
+        self._sync_stats()
+        if self._autotab:
+            self._drain_tab()
+
     def run(self, duration):
         self._ensure_plan().run(duration)
-        self._sync_stats()
+        self._after_run()
 
     def steps(self, n):
         self._ensure_plan().steps(n)
-        self._sync_stats()
+        self._after_run()
 
     def run_until_smaller(self, name, value):
         if name.lower() != "maxtorque":
             raise NotImplementedError("run_until_smaller is supported for maxtorque (the relax idiom)")
         self._ensure_plan().run_until_maxtorque(value)
-        self._sync_stats()
+        self._after_run()
+
+
+def go_float(v):
+    """A float64 the way Go's fmt.Fprint writes it: shortest round-trip digits in
+    strconv's 'g' form, with the exponent form when the decimal exponent is < -4 or >= 6
+    (the precision strconv uses for that decision with shortest digits)."""
+    import decimal
+    v = float(v)
+    if v != v:
+        return "NaN"
+    if v in (float("inf"), float("-inf")):
+        return "+Inf" if v > 0 else "-Inf"
+    if v == 0.0:
+        return "0"
+    sign, digits, exp = decimal.Decimal(repr(v)).normalize().as_tuple()
+    ds = "".join(str(d) for d in digits)
+    nd = len(ds)
+    dp = nd + exp        # position of the decimal point
+    x = dp - 1
+    s = "-" if sign else ""
+    if x < -4 or x >= 6:
+        mant = ds[0] + ("." + ds[1:] if nd > 1 else "")
+        return f"{s}{mant}e{'+' if x >= 0 else '-'}{abs(x):02d}"
+    if dp <= 0:
+        return s + "0." + "0" * (-dp) + ds
+    if dp >= nd:
+        return s + ds + "0" * (dp - nd)
+    return s + ds[:dp] + "." + ds[dp:]
 
 
 # ---------------------------------------------------------------- script API (src/python/mumax2.py)
@@ -497,6 +573,10 @@ def setv(name, value):
     if name == "<m>":
         raise ValueError("<m> is derived")
     engine().setv(name, value)
+
+
+def autotabulate(quants, filename, period):
+    engine().autotabulate(quants, filename, period)
 
 
 def setpointwise(name, time, value):

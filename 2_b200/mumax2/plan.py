@@ -189,6 +189,25 @@ class Plan:
         nat.check(nat.lib().mm_set_table(self.h, nat.TABLES[quantity], len(times),
                                          self._tab[quantity].ctypes.data_as(C.c_void_p)))
 
+    # ---- autotabulate on the device
+    def tabulate(self, period, capacity=4096):
+        """Record (t, <m>, maxtorque, dt, step) on the device every `period` of simulated
+        time (no host synchronisation); period <= 0 turns it off."""
+        nat.check(nat.lib().mm_tabulate(self.h, float(period), int(capacity)))
+        self._tab_cap = int(capacity) if period > 0 else getattr(self, "_tab_cap", 0)
+
+    def tabulate_read(self):
+        """Rows recorded since the last read: a list (one per simulation) of arrays
+        [rows][8] = (t, <m>_0, <m>_1, <m>_2, maxtorque, dt, step, 0), internal order."""
+        cap = max(1, getattr(self, "_tab_cap", 0))
+        out = np.zeros((self.nsim, cap, 8))
+        counts = np.zeros(self.nsim, dtype=np.int32)
+        lost = np.zeros(self.nsim, dtype=np.int64)
+        nat.check(nat.lib().mm_tabulate_read(self.h, out.ctypes.data_as(C.c_void_p), counts.ctypes.data_as(C.c_void_p),
+                                             lost.ctypes.data_as(C.c_void_p), None))
+        self.tab_lost = lost
+        return [out[b, :counts[b]].copy() for b in range(self.nsim)]
+
     # ---- batched plans: one entry per simulation
     def set_sims(self, sims):
         self._sims = nat.make_sims(self.problem, sims)

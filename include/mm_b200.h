@@ -198,6 +198,17 @@ MM_API int mm_batch_run_until_maxtorque(mm_plan plan, const double* thr, long lo
 enum { MM_TABLE_BEXT = 0, MM_TABLE_J = 1 };
 MM_API int mm_set_table(mm_plan plan, int quantity, int npoints, const double* rows);
 
+/* ---- autotabulate on the device (AutoTabulate, notify_tabulate.go:23-28) ----
+ * After every accepted step with t - count*period >= period, the step's own launches
+ * append a row (t, <m>_0, <m>_1, <m>_2 (internal order), maxtorque, dt, step, 0) to the
+ * simulation's device table: no host synchronisation.  capacity rows per simulation;
+ * period <= 0 turns it off.  mm_tabulate_read copies all tables to out
+ * [nsim][capacity][8] (host), the rows written per simulation to counts[nsim] and the
+ * rows that found the table full to lost[nsim] (may be NULL), and empties the tables.
+ * maxtorque is that of the new state for RK23/RK45 and of the previous state otherwise. */
+MM_API int mm_tabulate(mm_plan plan, double period, int capacity);
+MM_API int mm_tabulate_read(mm_plan plan, double* out, int* counts, long long* lost, mm_stream stream);
+
 /* ---- per-simulation results of a (batched) plan; out arrays have nsim entries ---- */
 MM_API int mm_batch_stats(mm_plan plan, mm_stats* out, mm_stream stream);
 MM_API int mm_batch_maxtorque(mm_plan plan, double* out, mm_stream stream);

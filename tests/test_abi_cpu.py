@@ -75,3 +75,10 @@ def test_headers_compile_as_c(hdr, tmp_path):
     r = subprocess.run(["gcc", "-std=c99", "-fsyntax-only", f"-I{INC}", "-I/usr/local/cuda/include", str(src)],
                        capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
+
+
+def test_go_float_format():
+    """Table values are written as Go's fmt.Fprint writes float64 (table.go:45)."""
+    from mumax2.engine import go_float
+    assert [go_float(v) for v in [1e-11, 1.5e6, 0.25, -3.2e-5, 123456.0, 1.0, 0.0, 1e6, 2.5e-4]] == \
+        ["1e-11", "1.5e+06", "0.25", "-3.2e-05", "123456", "1", "0", "1e+06", "0.00025"]
