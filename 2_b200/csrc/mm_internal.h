@@ -53,7 +53,11 @@ struct DevCtl {
     long long tab_lost;      // records that found the buffer full
     int tab_n, tab_cap;      // rows written since the last read, capacity
     int tab_pending;
-    int pad1;
+    int save_pending;        // autosave (notify_autosave.go:25-31): a state copy is due
+    double save_period;      // <= 0: off
+    double save_start;       // time autosave was turned on
+    long long save_count, save_lost;
+    int save_n, save_cap;    // states held since the last read, capacity
 };
 
 // Written by the controller after every attempt: what the host polls between batches.

@@ -15,6 +15,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "fft.cuh"
@@ -175,6 +176,11 @@ __device__ void control_one(DevCtl* c, int adaptive, int q, int fsal, int nevals
             else c->tab_lost++;
             c->tab_count++;
         }
+        if (c->save_period > 0 && (c->t - c->save_start) - (double)c->save_count * c->save_period >= c->save_period) {
+            if (c->save_n < c->save_cap) c->save_pending = 1;
+            else c->save_lost++;
+            c->save_count++;
+        }
     }
     if (!fsal && c->tq_bits) c->maxtorque = sqrt((double)__uint_as_float(c->tq_bits)) * c->gamma;
     c->tq_bits = 0u;
@@ -313,11 +319,30 @@ __global__ void tab_sum_kernel(const float* Y0, const float* Y1, const DevCtl* c
     sum3_block((c->cur ? Y1 : Y0) + blockIdx.y * bstride, N, red);
 }
 
-// autotabulate: one thread per simulation folds the partials (fixed order, compensated)
-// and appends the row (t, <m>_0, <m>_1, <m>_2, maxtorque, dt, step, 0)
+// autosave: copy of the just-accepted state of simulations with a save due into their
+// next ring slot
+__global__ void save_copy_kernel(const float* Y0, const float* Y1, const DevCtl* ctl, long long n3, float* ring,
+                                 double* ring_t) {
+    const DevCtl* c = ctl + blockIdx.y;
+    if (!c->save_pending) return;
+    const float* src = (c->cur ? Y1 : Y0) + blockIdx.y * n3;
+    const long long slot = (long long)blockIdx.y * c->save_cap + c->save_n;
+    float* dst = ring + slot * n3;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n3; i += (long long)gridDim.x * blockDim.x)
+        dst[i] = src[i];
+    if (blockIdx.x == 0 && threadIdx.x == 0) ring_t[slot] = c->t;
+}
+
+// autotabulate / autosave bookkeeping, one thread per simulation: folds the <m>
+// partials (fixed order, compensated) and appends the row (t, <m>_0, <m>_1, <m>_2,
+// maxtorque, dt, step, 0); counts the saved state
 __global__ void tab_finish_kernel(const float* red, int nblocks, DevCtl* ctl, int nsim, double* rec, long long N) {
     for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nsim; b += gridDim.x * blockDim.x) {
         DevCtl* c = ctl + b;
+        if (c->save_pending) {
+            c->save_n++;
+            c->save_pending = 0;
+        }
         if (!c->tab_pending) continue;
         double avg[3];
         for (int q = 0; q < 3; q++) {
@@ -394,9 +419,22 @@ struct mm_plan_s {
     int tab_cap[2] = {0, 0};
     std::vector<double> tab_host[2];
     double t_eval = 0.0;             // time of standalone evaluations
+    // asynchronous snapshots (mm_save_async): device staging is Mtmp; pinned host copy,
+    // side stream, events and the writer thread are made on first use
+    float* snap_host = nullptr;
+    double* snap_t_host = nullptr;
+    double* snap_t_dev = nullptr;
+    cudaStream_t snap_stream = nullptr;
+    cudaEvent_t snap_ready = nullptr, snap_copied = nullptr;
+    std::thread snap_writer;
+    int snap_rc = MM_OK;
     double* rec = nullptr;           // autotabulate rows [nsim][rec_cap][8]
     int rec_cap = 0;
     bool tab_on = false;
+    float* ring = nullptr;           // autosave states [nsim][ring_cap][3N]
+    double* ring_t = nullptr;        // their times [nsim][ring_cap]
+    int ring_cap = 0;
+    bool save_on = false;
     long long bytes = 0;
     long long n3() const { return 3 * g.N; }
     long long spec_bstride() const { return 3LL * g.n[0] * g.L[1] * g.hp; }
@@ -703,10 +741,19 @@ extern "C" MM_API int mm_plan_create(const mm_problem* prob, mm_plan* out) {
 
 extern "C" MM_API int mm_plan_nsim(mm_plan p) { return p ? p->nsim : 0; }
 
+extern "C" MM_API int mm_save_wait(mm_plan p);
+
 extern "C" MM_API int mm_plan_destroy(mm_plan p) {
     if (!p) return MM_OK;
+    mm_save_wait(p);
+    if (p->snap_host) cudaFreeHost(p->snap_host);
+    if (p->snap_t_host) cudaFreeHost(p->snap_t_host);
+    if (p->snap_t_dev) cudaFree(p->snap_t_dev);
+    if (p->snap_stream) cudaStreamDestroy(p->snap_stream);
+    if (p->snap_ready) cudaEventDestroy(p->snap_ready);
+    if (p->snap_copied) cudaEventDestroy(p->snap_copied);
     if (p->graph) cudaGraphExecDestroy(p->graph);
-    void* bufs[] = {p->rec, p->tab[0], p->tab[1], p->khat, p->khat_d, p->khat_ex, p->tw, p->S, p->d_sims, p->d_sim_msat, p->Y[0], p->Y[1], p->K1[0], p->K1[1], p->Ma,
+    void* bufs[] = {p->ring, p->ring_t, p->rec, p->tab[0], p->tab[1], p->khat, p->khat_d, p->khat_ex, p->tw, p->S, p->d_sims, p->d_sim_msat, p->Y[0], p->Y[1], p->K1[0], p->K1[1], p->Ma,
                     p->Mb, p->Mtmp, p->ctl, p->dsum, p->red, p->dres, p->tq};
     for (void* b : bufs)
         if (b) cudaFree(b);
@@ -948,6 +995,60 @@ extern "C" MM_API int mm_tabulate(mm_plan p, double period, int capacity) {
     return write_ctl(p, 0);
 }
 
+extern "C" MM_API int mm_autosave(mm_plan p, double period, int capacity) {
+    if (!p) return set_err(MM_ERR_ARG, "null plan");
+    if (period > 0 && capacity < 1) return set_err(MM_ERR_ARG, "capacity must be >= 1");
+    if (period > 0 && capacity > p->ring_cap) {
+        if (p->ring) cudaFree(p->ring);
+        if (p->ring_t) cudaFree(p->ring_t);
+        p->ring = nullptr;
+        p->ring_t = nullptr;
+        p->ring_cap = 0;
+        int rc = dalloc(p, (void**)&p->ring, sizeof(float) * (size_t)p->n3() * capacity * p->nsim);
+        if (!rc) rc = dalloc(p, (void**)&p->ring_t, sizeof(double) * (size_t)capacity * p->nsim);
+        if (rc) return rc;
+        p->ring_cap = capacity;
+    }
+    int rc = read_ctl(p, 0);
+    if (rc) return rc;
+    for (int b = 0; b < p->nsim; b++) {
+        DevCtl& c = p->ctl_host[b];
+        c.save_period = period > 0 ? period : 0.0;
+        c.save_start = c.t;
+        c.save_count = 0;
+        c.save_lost = 0;
+        c.save_n = 0;
+        c.save_cap = period > 0 ? capacity : 0;
+        c.save_pending = 0;
+    }
+    p->save_on = period > 0;
+    free_graph(p);
+    return write_ctl(p, 0);
+}
+
+extern "C" MM_API int mm_autosave_read(mm_plan p, float* states, double* times, int* counts, long long* lost,
+                                       mm_stream stream) {
+    if (!p || !states || !times || !counts) return set_err(MM_ERR_ARG, "null argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    int rc = read_ctl(p, st);
+    if (rc) return rc;
+    for (int b = 0; b < p->nsim; b++) {
+        const int n = p->ctl_host[b].save_n;
+        const size_t off = (size_t)b * p->ring_cap;
+        if (n > 0) {
+            CUCHK(cudaMemcpyAsync(states + off * p->n3(), p->ring + off * p->n3(), sizeof(float) * p->n3() * n,
+                                  cudaMemcpyDeviceToHost, st));
+            CUCHK(cudaMemcpyAsync(times + off, p->ring_t + off, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+        }
+        counts[b] = n;
+        if (lost) lost[b] = p->ctl_host[b].save_lost;
+        p->ctl_host[b].save_n = 0;
+        p->ctl_host[b].save_lost = 0;
+    }
+    CUCHK(cudaStreamSynchronize(st));
+    return write_ctl(p, st);
+}
+
 extern "C" MM_API int mm_tabulate_read(mm_plan p, double* out, int* counts, long long* lost, mm_stream stream) {
     if (!p || !out || !counts) return set_err(MM_ERR_ARG, "null argument");
     cudaStream_t st = (cudaStream_t)stream;
@@ -1051,16 +1152,25 @@ static cudaError_t launch_controller(mm_plan p, cudaStream_t st, int mode, int a
 // blocks per simulation of the record sums
 static int tab_blocks(mm_plan p) { return std::min(p->red_blocks, std::max(1, (148 * 2 + p->nsim - 1) / p->nsim)); }
 
-// The autotabulate record kernels (no-ops unless a record is due).
+// The autotabulate / autosave record kernels (no-ops unless a record is due).
 static int launch_records(mm_plan p, cudaStream_t st) {
-    if (!p->tab_on) return MM_OK;
+    if (!p->tab_on && !p->save_on) return MM_OK;
     const int nb = tab_blocks(p);
-    tab_sum_kernel<<<dim3((unsigned)nb, (unsigned)p->nsim), 256, 0, st>>>(p->Y[0], p->Y[1], p->ctl, p->g.N, p->n3(),
-                                                                          p->red);
-    CUCHK(cudaGetLastError());
+    if (p->tab_on) {
+        tab_sum_kernel<<<dim3((unsigned)nb, (unsigned)p->nsim), 256, 0, st>>>(p->Y[0], p->Y[1], p->ctl, p->g.N,
+                                                                              p->n3(), p->red);
+        CUCHK(cudaGetLastError());
+        p->launches++;
+    }
+    if (p->save_on) {
+        save_copy_kernel<<<dim3((unsigned)local_blocks(p->n3(), p->nsim), (unsigned)p->nsim), 256, 0, st>>>(
+            p->Y[0], p->Y[1], p->ctl, p->n3(), p->ring, p->ring_t);
+        CUCHK(cudaGetLastError());
+        p->launches++;
+    }
     tab_finish_kernel<<<(p->nsim + 127) / 128, 128, 0, st>>>(p->red, nb, p->ctl, p->nsim, p->rec, p->g.N);
     CUCHK(cudaGetLastError());
-    p->launches += 2;
+    p->launches++;
     return MM_OK;
 }
 
@@ -1823,3 +1933,70 @@ extern "C" MM_API int mm_ensemble_run(mm_ensemble e, double duration, mm_stream 
 }
 
 extern "C" MM_API long long mm_ensemble_launch_count(mm_ensemble e) { return e ? e->launches : 0; }
+
+// ---------------------------------------------------------------- asynchronous snapshots
+extern "C" MM_API int mm_write_field(const char* path, int format, const float* data, int ncomp, const int n[3],
+                                     const double cell[3], double time, const char* name, const char* unit);
+
+// copies the accepted state (resolved on the device) and the time to the staging buffers
+__global__ void snapshot_kernel(PP y, const DevCtl* ctl, float* dst, long long n, double* t_out) {
+    const float* src = y.get(ctl->cur);
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        dst[i] = src[i];
+    if (blockIdx.x == 0 && threadIdx.x == 0) *t_out = ctl->t;
+}
+
+extern "C" MM_API int mm_save_wait(mm_plan p) {
+    if (!p) return set_err(MM_ERR_ARG, "null plan");
+    if (p->snap_writer.joinable()) p->snap_writer.join();
+    const int rc = p->snap_rc;
+    p->snap_rc = MM_OK;
+    return rc;
+}
+
+extern "C" MM_API int mm_save_async(mm_plan p, const char* path, int format, mm_stream stream) {
+    if (!p || !path) return set_err(MM_ERR_ARG, "null argument");
+    if (format < MM_FMT_OVF2_BIN4 || format > MM_FMT_DUMP) return set_err(MM_ERR_ARG, "unknown format %d", format);
+    if (p->nsim > 1 && format != MM_FMT_DUMP)
+        return set_err(MM_ERR_ARG, "a batched plan saves dump frames (one per simulation)");
+    cudaStream_t st = (cudaStream_t)stream;
+    const size_t n3 = (size_t)p->n3() * p->nsim;
+    if (!p->snap_host) {
+        CUCHK(cudaMallocHost(&p->snap_host, sizeof(float) * n3));
+        CUCHK(cudaMallocHost(&p->snap_t_host, sizeof(double)));
+        CUCHK(cudaMalloc(&p->snap_t_dev, sizeof(double)));
+        CUCHK(cudaStreamCreateWithFlags(&p->snap_stream, cudaStreamNonBlocking));
+        CUCHK(cudaEventCreateWithFlags(&p->snap_ready, cudaEventDisableTiming));
+        CUCHK(cudaEventCreateWithFlags(&p->snap_copied, cudaEventDisableTiming));
+    }
+    // one snapshot in flight at a time: the previous writer releases the pinned buffer
+    if (p->snap_writer.joinable()) p->snap_writer.join();
+    // batched plans keep every accepted state in Y[0] between runs, so simulation 0's
+    // control block selects the buffer for all of them
+    snapshot_kernel<<<local_blocks((long long)n3), 256, 0, st>>>(cur_of(p->Y), p->ctl, p->Mtmp, (long long)n3,
+                                                                  p->snap_t_dev);
+    CUCHK(cudaGetLastError());
+    CUCHK(cudaEventRecord(p->snap_ready, st));
+    CUCHK(cudaStreamWaitEvent(p->snap_stream, p->snap_ready, 0));
+    CUCHK(cudaMemcpyAsync(p->snap_host, p->Mtmp, sizeof(float) * n3, cudaMemcpyDeviceToHost, p->snap_stream));
+    CUCHK(cudaMemcpyAsync(p->snap_t_host, p->snap_t_dev, sizeof(double), cudaMemcpyDeviceToHost, p->snap_stream));
+    CUCHK(cudaEventRecord(p->snap_copied, p->snap_stream));
+    // later work on the caller's stream may reuse the staging buffer: it waits for the copy
+    CUCHK(cudaStreamWaitEvent(st, p->snap_copied, 0));
+    const std::string file(path);
+    const int device = p->device;
+    p->snap_writer = std::thread([p, file, format, device]() {
+        cudaSetDevice(device);
+        if (cudaEventSynchronize(p->snap_copied) != cudaSuccess) {
+            p->snap_rc = MM_ERR_CUDA;
+            return;
+        }
+        const int n[3] = {p->g.n[0], p->g.n[1], p->g.n[2]};
+        for (int b = 0; b < p->nsim && p->snap_rc == MM_OK; b++) {
+            const int rc = mm_write_field(file.c_str(), format, p->snap_host + (size_t)b * p->n3(), 3, n,
+                                          p->prob.cell, *p->snap_t_host, "m", "");
+            if (rc != MM_OK) p->snap_rc = rc;
+        }
+    });
+    return MM_OK;
+}

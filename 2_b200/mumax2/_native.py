@@ -23,6 +23,49 @@ MM_ERR_STATE = -5
 MM_ERR_TIMEOUT = -6
 MM_ERR_RANGE = -7
 TABLES = {"bext": 0, "j": 1}
+FORMATS = {"ovf": 0, "ovf_text": 1, "omf": 2, "omf_text": 3, "dump": 4}
+
+
+def format_code(fmt, options=()):
+    """The reference's (format, options) pair -> MM_FMT_* ("ovf"/"omf" with [] or
+    ["Binary 4"] -> binary, ["Text"] -> text; "dump")."""
+    fmt = fmt.lower()
+    opts = [o.lower() for o in (options or [])]
+    if fmt == "dump":
+        if opts:
+            raise ValueError("dump output format does not take options")
+        return FORMATS["dump"]
+    if fmt not in ("ovf", "omf"):
+        raise ValueError(f"unknown output format {fmt!r}")
+    if len(opts) > 1:
+        raise ValueError(f"illegal {fmt.upper()} options: {options}")
+    if not opts or opts[0] == "binary 4":
+        return FORMATS[fmt]
+    if opts[0] == "text":
+        return FORMATS[fmt + "_text"]
+    raise ValueError(f"illegal {fmt.upper()} data format {options[0]!r}: options are Text, Binary 4")
+
+
+def write_field(path, fmt_code, data, n, cell, time, name, unit):
+    """data: float32 [ncomp][n0][n1][n2] (internal order) on the host."""
+    import numpy as np
+    a = np.ascontiguousarray(data, dtype=np.float32)
+    ncomp = a.size // (int(n[0]) * int(n[1]) * int(n[2]))
+    check(lib().mm_write_field(str(path).encode(), int(fmt_code), a.ctypes.data_as(C.c_void_p), ncomp,
+                               (C.c_int * 3)(*[int(x) for x in n]), (C.c_double * 3)(*[float(x) for x in cell]),
+                               float(time), name.encode(), unit.encode()))
+
+
+def read_field(path):
+    """-> (data float32 [ncomp][n0][n1][n2] internal order, n, time)."""
+    import numpy as np
+    nc = C.c_int()
+    n = (C.c_int * 3)()
+    t = C.c_double()
+    check(lib().mm_read_field(str(path).encode(), None, 0, C.byref(nc), n, C.byref(t)))
+    a = np.zeros(nc.value * n[0] * n[1] * n[2], dtype=np.float32)
+    check(lib().mm_read_field(str(path).encode(), a.ctypes.data_as(C.c_void_p), a.size, C.byref(nc), n, C.byref(t)))
+    return a.reshape(nc.value, n[0], n[1], n[2]), tuple(n), t.value
 
 SOLVERS = {"euler": 0, "heun": 1, "rk12": 2, "rk23": 3, "rk45": 4}
 
@@ -124,6 +167,15 @@ _PROTOS = {
     "mm_average_noalloc": (C.c_int, [C.c_void_p, C.c_longlong, C.c_void_p, C.c_void_p]),
     "mm_set_table": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
     "mm_tabulate": (C.c_int, [C.c_void_p, C.c_double, C.c_int]),
+    "mm_autosave": (C.c_int, [C.c_void_p, C.c_double, C.c_int]),
+    "mm_autosave_read": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "mm_write_field": (C.c_int, [C.c_char_p, C.c_int, C.c_void_p, C.c_int, C.c_int * 3, C.c_double * 3, C.c_double,
+                                 C.c_char_p, C.c_char_p]),
+    "mm_read_field": (C.c_int, [C.c_char_p, C.c_void_p, C.c_longlong, C.POINTER(C.c_int), C.c_int * 3,
+                                C.POINTER(C.c_double)]),
+    "mm_crc64_iso": (C.c_uint64, [C.c_void_p, C.c_size_t]),
+    "mm_save_async": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int, C.c_void_p]),
+    "mm_save_wait": (C.c_int, [C.c_void_p]),
     "mm_tabulate_read": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "mm_plan_create_batch": (C.c_int, [C.POINTER(MMProblem), C.c_int, C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]),
     "mm_plan_nsim": (C.c_int, [C.c_void_p]),

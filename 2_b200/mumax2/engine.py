@@ -38,6 +38,14 @@ class Quant:
         return f"Quant({self.name}, {self.kind}, mult={self.mult})"
 
 
+def _file_to_user(a):
+    """[ncomp][n0][n1][n2] internal -> user layout [ncomp][x][y][z]."""
+    a = np.asarray(a)
+    if a.shape[0] == 3:
+        a = a[::-1]
+    return np.ascontiguousarray(np.transpose(a, (0, 3, 2, 1)))
+
+
 def _swap_vec(v):
     """User (x,y,z) <-> internal (z,y,x) for vectors (common/index.go:70-85)."""
     v = list(v)
@@ -65,6 +73,10 @@ class Engine:
         self._m = None       # host copy when the plan is not built yet
         self._pointwise = {}  # SetPointwise tables: quantity -> [(t, internal value)]
         self._autotab = None  # (quants, filename, period, header written)
+        self._autosave = None  # (quantity, format code, extension, period)
+        self.outdir = "."
+        self._last_output_t = 0.0
+        self._output_id = 0
         self._tables_dirty = False
         for name, unit in [("t", "s"), ("dt", "s"), ("step", "")]:
             self._add(name, 1, VALUE, unit)
@@ -270,6 +282,8 @@ class Engine:
             self._tables_dirty = True
             if self._autotab:
                 self.plan.tabulate(self._autotab[2], self.TAB_CAPACITY)
+            if self._autosave:
+                self.plan.autosave(self._autosave[3], self.SAVE_CAPACITY)
             self._dirty_params = False
             self._solver_dirty = True
             if m is not None:
@@ -487,10 +501,81 @@ class Engine:
                         line += go_float(r[i]) + "\t"
                 f.write(line + "\n")
 
+    # ------------------------------------------------------------ output (engine.go:555-640)
+    SAVE_CAPACITY = 32
+    EXT = {0: "ovf", 1: "ovf", 2: "omf", 3: "omf", 4: "dump"}
+
+    def _output_id(self, t):
+        if t != self._last_output_t:
+            self._last_output_t = t
+            self._output_id += 1
+        return self._output_id
+
+    def _auto_filename(self, quant, code, t):
+        import os
+        return os.path.join(self.outdir, f"{quant}{self._output_id(t):06d}.{self.EXT[code]}")
+
+    def _field_array(self, name):
+        lname = name.lower()
+        q = self.quant(name)
+        if lname == "m":
+            return self._ensure_plan().get_state(), q
+        if q.kind == MASK:
+            if q.mask is None:
+                return np.repeat(np.array(q.mult, dtype=np.float32), self.ncell), q
+            return (q.mask * np.array(q.mult)[:, None, None, None]).reshape(-1).astype(np.float32), q
+        return np.asarray(self._field(lname), dtype=np.float32), q
+
+    def saveas(self, name, fmt, options, filename):
+        from . import _native as nat
+        code = nat.format_code(fmt, options)
+        data, q = self._field_array(name)
+        self._sync_stats() if self.plan is not None else None
+        nat.write_field(filename, code, data, self.size, self.cell, self.quant("t").mult[0], q.name, q.unit)
+
+    def save(self, name, fmt, options):
+        from . import _native as nat
+        code = nat.format_code(fmt, options)
+        if self.plan is not None:
+            self._sync_stats()
+        self.saveas(name, fmt, options, self._auto_filename(name, code, self.quant("t").mult[0]))
+
+    def autosave(self, name, fmt, options, period):
+        """AutoSave (engine.go:576-582): m is copied on the device by the step that
+        crosses each save time and written to the auto-numbered files after the run."""
+        from . import _native as nat
+        if name.lower() != "m":
+            raise NotImplementedError("device autosave covers m")
+        code = nat.format_code(fmt, options)
+        self._autosave = (name, code, self.EXT[code], float(period))
+        if self.plan is not None:
+            self.plan.autosave(float(period), self.SAVE_CAPACITY)
+
+    def _drain_save(self):
+        from . import _native as nat
+        name, code, _, _ = self._autosave
+        times, states = self.plan.autosave_read()[0]
+        q = self.quant(name)
+        for t, m in zip(times, states):
+            nat.write_field(self._auto_filename(name, code, t), code, m, self.size, self.cell, t, q.name, q.unit)
+
+    def setarray_file(self, name, filename):
+        """SetArray_File (api.go:267-269): read an OMF/OVF/dump file into a field."""
+        from . import _native as nat
+        data, n, _ = nat.read_field(filename)
+        self.setarray(name, _file_to_user(data))
+
+    def setmask_file(self, name, filename):
+        from . import _native as nat
+        data, n, _ = nat.read_field(filename)
+        self.setmask(name, _file_to_user(data))
+
     def _after_run(self):
         self._sync_stats()
         if self._autotab:
             self._drain_tab()
+        if self._autosave:
+            self._drain_save()
 
     def run(self, duration):
         self._ensure_plan().run(duration)
@@ -573,6 +658,26 @@ def setv(name, value):
     if name == "<m>":
         raise ValueError("<m> is derived")
     engine().setv(name, value)
+
+
+def save(name, fmt, options=()):
+    engine().save(name, fmt, options)
+
+
+def saveas(name, fmt, options, filename):
+    engine().saveas(name, fmt, options, filename)
+
+
+def autosave(name, fmt, options, period):
+    engine().autosave(name, fmt, options, period)
+
+
+def setarray_file(name, filename):
+    engine().setarray_file(name, filename)
+
+
+def setmask_file(name, filename):
+    engine().setmask_file(name, filename)
 
 
 def autotabulate(quants, filename, period):

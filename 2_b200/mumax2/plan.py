@@ -189,6 +189,34 @@ class Plan:
         nat.check(nat.lib().mm_set_table(self.h, nat.TABLES[quantity], len(times),
                                          self._tab[quantity].ctypes.data_as(C.c_void_p)))
 
+    # ---- output
+    def save_async(self, path, fmt="ovf", options=()):
+        """Snapshot of m written to `path` by a host thread while the GPU keeps going."""
+        nat.check(nat.lib().mm_save_async(self.h, str(path).encode(), nat.format_code(fmt, options), None))
+
+    def save_wait(self):
+        nat.check(nat.lib().mm_save_wait(self.h))
+
+    def autosave(self, period, capacity=16):
+        """Copy m on the device every `period` of simulated time (notify_autosave.go)."""
+        nat.check(nat.lib().mm_autosave(self.h, float(period), int(capacity)))
+        self._save_cap = int(capacity) if period > 0 else getattr(self, "_save_cap", 0)
+
+    def autosave_read(self):
+        """States saved since the last read: a list (one per simulation) of
+        (times [k], states [k][3N])."""
+        cap = max(1, getattr(self, "_save_cap", 0))
+        n3 = 3 * self.N
+        states = np.zeros((self.nsim, cap, n3), dtype=np.float32)
+        times = np.zeros((self.nsim, cap))
+        counts = np.zeros(self.nsim, dtype=np.int32)
+        lost = np.zeros(self.nsim, dtype=np.int64)
+        nat.check(nat.lib().mm_autosave_read(self.h, states.ctypes.data_as(C.c_void_p), times.ctypes.data_as(C.c_void_p),
+                                             counts.ctypes.data_as(C.c_void_p), lost.ctypes.data_as(C.c_void_p),
+                                             None))
+        self.save_lost = lost
+        return [(times[b, :counts[b]].copy(), states[b, :counts[b]].copy()) for b in range(self.nsim)]
+
     # ---- autotabulate on the device
     def tabulate(self, period, capacity=4096):
         """Record (t, <m>, maxtorque, dt, step) on the device every `period` of simulated

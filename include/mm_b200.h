@@ -209,6 +209,17 @@ MM_API int mm_set_table(mm_plan plan, int quantity, int npoints, const double* r
 MM_API int mm_tabulate(mm_plan plan, double period, int capacity);
 MM_API int mm_tabulate_read(mm_plan plan, double* out, int* counts, long long* lost, mm_stream stream);
 
+/* ---- autosave of m on the device (AutoSave, notify_autosave.go:25-31) ----
+ * After every accepted step with (t - t_on) - count*period >= period, the step's own
+ * launches copy the new state into the next of `capacity` device slots per simulation
+ * (no host synchronisation); t_on is the time of this call.  mm_autosave_read copies the
+ * held states to states [nsim][capacity][3N] and their times to times [nsim][capacity]
+ * (host), the count per simulation to counts, the states that found the slots full to
+ * lost (may be NULL), and frees the slots.  period <= 0 turns it off. */
+MM_API int mm_autosave(mm_plan plan, double period, int capacity);
+MM_API int mm_autosave_read(mm_plan plan, float* states, double* times, int* counts, long long* lost,
+                            mm_stream stream);
+
 /* ---- per-simulation results of a (batched) plan; out arrays have nsim entries ---- */
 MM_API int mm_batch_stats(mm_plan plan, mm_stats* out, mm_stream stream);
 MM_API int mm_batch_maxtorque(mm_plan plan, double* out, mm_stream stream);
@@ -225,6 +236,25 @@ MM_API int mm_ensemble_steps(mm_ensemble ens, long long n, mm_stream stream);
 /* Every simulation advances by `duration` seconds. */
 MM_API int mm_ensemble_run(mm_ensemble ens, double duration, mm_stream stream);
 MM_API long long mm_ensemble_launch_count(mm_ensemble ens);
+
+/* ---- output and input formats (host side; ovf/, dump/ and engine/format_dump.go) ----
+ * data: host float32 [ncomp][n0][n1][n2] in internal order (ncomp 1 or 3), n and cell
+ * internal.  OVF 2.0 (ovf2_output.go:34-161) and OMF 1.0 (omf_output.go:34-206) write
+ * one file; a dump frame (dump/writer.go:34-97, format_dump.go:40-62, CRC-64 ISO) is
+ * appended to the file.  mm_read_field reads the first field of any of them (data NULL:
+ * sizes only), checking the OMF control number and the dump CRC. */
+enum { MM_FMT_OVF2_BIN4 = 0, MM_FMT_OVF2_TEXT = 1, MM_FMT_OMF_BIN4 = 2, MM_FMT_OMF_TEXT = 3, MM_FMT_DUMP = 4 };
+MM_API int mm_write_field(const char* path, int format, const float* data, int ncomp, const int n[3],
+                          const double cell[3], double time, const char* name, const char* unit);
+MM_API int mm_read_field(const char* path, float* data, long long capacity, int* ncomp, int n[3], double* time);
+/* CRC-64 with the ISO polynomial as Go's hash/crc64 computes it (the dump checksum). */
+MM_API uint64_t mm_crc64_iso(const void* data, size_t n);
+/* Snapshot of the plan's state without stopping the GPU: copies m to pinned host memory on
+ * a side stream once the work queued on `stream` is done (later work on `stream` waits only
+ * for that copy), then formats and writes the file on a host thread.  mm_save_wait blocks
+ * until every pending snapshot of the plan is on disk and returns the first error. */
+MM_API int mm_save_async(mm_plan plan, const char* path, int format, mm_stream stream);
+MM_API int mm_save_wait(mm_plan plan);
 
 /* ---- instrumentation ---- */
 /* Kernels this plan has enqueued so far (graph replays counted per kernel node). */
