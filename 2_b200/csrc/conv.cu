@@ -26,8 +26,11 @@
 namespace mm {
 using namespace mmfft;
 
+// skip_retry: 1 = the kernel belongs to a retried attempt's reusable first evaluation
+// (skipped when tries > 0); 2 = an evaluation inside an AM12 fixed-point loop (skipped
+// once the loop has ended or the attempt was abandoned)
 __device__ __forceinline__ bool conv_skip(const DevCtl* ctl, int skip_retry) {
-    return ctl && (ctl->done || (skip_retry && ctl->tries > 0));
+    return ctl && (ctl->done || (skip_retry == 1 && ctl->tries > 0) || (skip_retry == 2 && ctl->am_skip));
 }
 
 // ---------------------------------------------------------------- R2C row pass

@@ -58,6 +58,18 @@ struct DevCtl {
     double save_start;       // time autosave was turned on
     long long save_count, save_lost;
     int save_n, save_cap;    // states held since the last read, capacity
+    // solver/am12 (solve_am01.go:46-301), see am12.cu
+    double am_abs_err, am_rel_err;   // m_maxAbsError, m_maxRelError
+    double am_er;            // error of the previous fixed-point iteration
+    double am_alpha;         // convergence ratio of the last iteration
+    double am_alpha_bdf;     // last predictor ratio (kept across steps)
+    long long am_iterations; // iterations of the current step (bdf_iterations)
+    int am_iter;             // iterations of the current loop
+    int am_phase;            // loop state: 0 running, 1 converged, 2 failed
+    int am_skip;             // the remaining kernels of the loop / attempt do nothing
+    int am_restrict;         // limit the next dt by the predictor ratio
+    int am_try;              // bad steps of this step (the reference's try)
+    unsigned int am_red[6];  // max |y - yb| and max |yb| per component (float bits)
 };
 
 // Written by the controller after every attempt: what the host polls between batches.
@@ -159,7 +171,7 @@ struct StageOp {
     double ek[MM_MAXK];
     int want_tq;
     int want_energy;
-    int skip_if_retry;   // k0 of RK12/Heun: a retried attempt keeps the old k0
+    int skip_if_retry;   // 1: skip when retrying (k0 of RK12/Heun/AM12); 2: skip while am_skip
     int pad;
     double c_time;       // the evaluation is at t + c_time * dt (time tables)
 };
@@ -212,6 +224,16 @@ cudaError_t launch_zmul_reg(int P, float2* S, const KernelView& K, int L1, int h
 cudaError_t launch_xinv_epi(int M, const float2* S, int hp, int L1, const float2* tw, const EpiArgs& A, bool terms,
                             cudaStream_t st, int* nblocks, int nsim = 1);
 cudaError_t launch_local_epi(const EpiArgs& A, bool terms, cudaStream_t st, int* nblocks, int nsim = 1);
+// solver/am12 (am12.cu)
+cudaError_t am_begin(DevCtl* ctl, int nsim, cudaStream_t st);
+cudaError_t am_update(PP y0, PP y, const float* dy, const float* dy0, const float* y1, DevCtl* ctl, long long N,
+                      int nsim, int bps, int mode, cudaStream_t st);
+cudaError_t am_test(DevCtl* ctl, int nsim, int predictor, cudaStream_t st);
+cudaError_t am_between(DevCtl* ctl, int nsim, int predictor, cudaStream_t st);
+cudaError_t am_final(DevCtl* ctl, int nsim, cudaStream_t st);
+cudaError_t am_copy(PP src, PP dst, const DevCtl* ctl, long long n3, int nsim, int bps, cudaStream_t st);
+cudaError_t am_normalize(PP m, const float* msat_mask, const DevCtl* ctl, long long N, long long mask_bstride, int nsim,
+                         int bps, int skip, cudaStream_t st);
 int xinv_blocks(int M, int n0n1);
 int report_error(int code, const char* msg);  // sets mm_last_error()
 int local_blocks(long long N, int nsim = 1);

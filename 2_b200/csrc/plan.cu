@@ -88,6 +88,7 @@ struct CombineArgs {
     long long N;
     long long bstride, mask_bstride;
     DevCtl* ctl;
+    int no_norm;  // leave the result unnormalised (the AM12 Euler start)
 };
 
 __global__ void combine_kernel(CombineArgs A) {
@@ -115,10 +116,13 @@ __global__ void combine_kernel(CombineArgs A) {
             y += ak[j] * kp[j][N + i];
             z += ak[j] * kp[j][2 * N + i];
         }
-        float norm = msk ? msk[i] : 1.0f;
-        float mn = sqrtf(x * x + y * y + z * z);
-        float sc = (norm == 0.0f) ? 0.0f : 1.0f;
-        sc = (mn != 0.0f) ? sc / mn : 0.0f;
+        float sc = 1.0f;
+        if (!A.no_norm) {
+            float norm = msk ? msk[i] : 1.0f;
+            float mn = sqrtf(x * x + y * y + z * z);
+            sc = (norm == 0.0f) ? 0.0f : 1.0f;
+            sc = (mn != 0.0f) ? sc / mn : 0.0f;
+        }
         next[i] = x * sc;
         next[N + i] = y * sc;
         next[2 * N + i] = z * sc;
@@ -1116,9 +1120,11 @@ static const double DP_E[7] = {35. / 384 - 5179. / 57600, 0, 500. / 1113 - 7571.
                                125. / 192 - 393. / 640, -2187. / 6784 + 92097. / 339200,
                                11. / 84 - 187. / 2100, -1. / 40};
 
-static int launch_combine(mm_plan p, PP base, PP next, int nk, const PP* kp, const double* ak, cudaStream_t st) {
+static int launch_combine(mm_plan p, PP base, PP next, int nk, const PP* kp, const double* ak, cudaStream_t st,
+                          int no_norm = 0) {
     CombineArgs A;
     memset(&A, 0, sizeof A);
+    A.no_norm = no_norm;
     A.base = base;
     A.next = next;
     A.nk = 0;
@@ -1174,11 +1180,79 @@ static int launch_records(mm_plan p, cudaStream_t st) {
     return MM_OK;
 }
 
+// One attempt of solver/am12 (am12.cu).  Buffers: y0 = Y[cur] (accepted state), the
+// iterate y = Y[other] (accepted by flipping cur), dy0 = Kst[0], dy = Kst[1], the RHS at
+// the Euler point = Kst[2], the predictor y1 = Ma.
+static int enqueue_am12(mm_plan p, cudaStream_t st) {
+    DevCtl* ctl = p->ctl;
+    const int ns = p->nsim, bps = local_blocks(p->g.N, ns);
+    const long long N = p->g.N;
+    int rc;
+    auto normalize = [&](PP m, int skip) -> int {
+        CUCHK(am_normalize(m, p->P.msat_mask, ctl, N, p->P.mask_bstride, ns, bps, skip, st));
+        p->launches++;
+        return MM_OK;
+    };
+    auto eval = [&](PP m_in, float* k_out, int skip, double c_time, int want_tq) -> int {
+        StageOp o = op_blank();
+        o.m_in = m_in;
+        o.k_out = fixed(k_out);
+        o.want_tq = want_tq;
+        o.c_time = c_time;
+        return launch_eval(p, o, ctl, skip, nullptr, 0, 0, nullptr, nullptr, st, nullptr);
+    };
+    // dy0 = f(y0) at the start of the step (pulling m normalises it); reused by retries
+    if ((rc = normalize(cur_of(p->Y), 1))) return rc;
+    if ((rc = eval(cur_of(p->Y), p->Kst[0], 1, 0.0, 1))) return rc;
+    if (p->run_until) {
+        CUCHK(launch_controller(p, st, 2, 0, 0, 0, 0, 0));
+        p->launches++;
+    }
+    CUCHK(am_begin(ctl, ns, st));
+    p->launches++;
+    // explicit Euler start y = y0 + h dy0 (not normalised), then f at t0 + dt
+    {
+        PP kp[1] = {fixed(p->Kst[0])};
+        double ak[1] = {1.0};
+        if ((rc = launch_combine(p, cur_of(p->Y), oth_of(p->Y), 1, kp, ak, st, 1))) return rc;
+    }
+    if ((rc = normalize(oth_of(p->Y), 2))) return rc;
+    if ((rc = eval(oth_of(p->Y), p->Kst[1], 2, 1.0, 0))) return rc;
+    CUCHK(am_copy(fixed(p->Kst[1]), fixed(p->Kst[2]), ctl, p->n3(), ns, bps, st));
+    p->launches++;
+    for (int loop = 0; loop < 2; loop++) {  // 0: implicit Euler predictor, 1: trapezoidal corrector
+        if (loop == 1) {
+            CUCHK(am_copy(oth_of(p->Y), fixed(p->Ma), ctl, p->n3(), ns, bps, st));
+            CUCHK(am_copy(fixed(p->Kst[2]), fixed(p->Kst[1]), ctl, p->n3(), ns, bps, st));
+            p->launches += 2;
+        }
+        for (int it = 0; it < 6; it++) {
+            CUCHK(am_update(cur_of(p->Y), oth_of(p->Y), p->Kst[1], p->Kst[0], nullptr, ctl, N, ns, bps,
+                            loop == 0 ? 0 : 1, st));
+            CUCHK(am_test(ctl, ns, loop == 0, st));
+            p->launches += 2;
+            if (it < 5) {
+                if ((rc = normalize(oth_of(p->Y), 2))) return rc;
+                if ((rc = eval(oth_of(p->Y), p->Kst[1], 2, 1.0, 0))) return rc;
+            }
+        }
+        CUCHK(am_between(ctl, ns, loop == 0, st));
+        p->launches++;
+    }
+    CUCHK(am_update(cur_of(p->Y), oth_of(p->Y), nullptr, nullptr, p->Ma, ctl, N, ns, bps, 2, st));
+    CUCHK(am_final(ctl, ns, st));
+    p->launches += 2;
+    CUCHK(launch_controller(p, st, 0, 0, 0, 0, 0, 0));
+    p->launches++;
+    return launch_records(p, st);
+}
+
 // Enqueues one step attempt of the configured solver (no host synchronisation).
 static int enqueue_attempt(mm_plan p, cudaStream_t st) {
     DevCtl* ctl = p->ctl;
     int rc;
     const int s = p->solver;
+    if (s == MM_AM12) return enqueue_am12(p, st);
     if (s == MM_EULER || s == MM_HEUN || s == MM_RK12) {
         // eval k0 at the accepted state
         StageOp o0 = op_blank();
@@ -1313,7 +1387,7 @@ static int write_ctl(mm_plan p, cudaStream_t st) {
 
 extern "C" MM_API int mm_solver_init(mm_plan p, int solver, double dt, double mindt, double maxdt, double maxerr) {
     if (!p) return set_err(MM_ERR_ARG, "null plan");
-    if (solver < MM_EULER || solver > MM_RK45) return set_err(MM_ERR_ARG, "unknown solver %d", solver);
+    if (solver < MM_EULER || solver > MM_AM12) return set_err(MM_ERR_ARG, "unknown solver %d", solver);
     if (!(dt > 0) || !(mindt > 0) || !(maxdt > 0) || !(maxerr > 0)) return set_err(MM_ERR_ARG, "dt, mindt, maxdt, maxerr must be > 0");
     p->solver = solver;
     free_graph(p);
@@ -1331,6 +1405,21 @@ extern "C" MM_API int mm_solver_init(mm_plan p, int solver, double dt, double mi
         c.fsal_valid = 0;
         c.tries = 0;
         c.status = MM_OK;
+        if (c.am_abs_err <= 0) c.am_abs_err = 1e-4;  // solve_am01.go:355-358 defaults
+        if (c.am_rel_err <= 0) c.am_rel_err = 1e-3;
+        c.am_restrict = 0;
+    }
+    return write_ctl(p, 0);
+}
+
+extern "C" MM_API int mm_solver_am12_tolerances(mm_plan p, double abs_err, double rel_err) {
+    if (!p) return set_err(MM_ERR_ARG, "null plan");
+    if (!(abs_err > 0) || !(rel_err > 0)) return set_err(MM_ERR_ARG, "tolerances must be > 0");
+    int rc = read_ctl(p, 0);
+    if (rc) return rc;
+    for (int b = 0; b < p->nsim; b++) {
+        p->ctl_host[b].am_abs_err = abs_err;
+        p->ctl_host[b].am_rel_err = rel_err;
     }
     return write_ctl(p, 0);
 }
@@ -1545,6 +1634,11 @@ static int start_run(mm_plan p, cudaStream_t st, double duration, long long nste
 static int finish_run(mm_plan p, cudaStream_t st) {
     int rc = canonicalise(p, st);
     if (rc) return rc;
+    if (p->solver == MM_AM12) {
+        // AM12 leaves its last iterate unnormalised; reading m normalises it
+        CUCHK(am_normalize(cur_of(p->Y), p->P.msat_mask, p->ctl, p->g.N, p->P.mask_bstride, p->nsim,
+                           local_blocks(p->g.N, p->nsim), 0, st));
+    }
     if ((rc = read_ctl(p, st))) return rc;
     for (int b = 0; b < p->nsim; b++) {
         DevCtl& c = p->ctl_host[b];
@@ -1612,6 +1706,7 @@ static void stats_of(const DevCtl& c, mm_stats* out) {
     out->evals = c.evals;
     out->status = c.status;
     out->done = c.done;
+    out->iterations = c.am_iterations;
 }
 
 static int single(mm_plan p) {

@@ -23,7 +23,7 @@ namespace mm {
 using namespace mmfft;
 
 __device__ __forceinline__ bool skip_eval(const DevCtl* ctl, int skip_retry) {
-    return ctl && (ctl->done || (skip_retry && ctl->tries > 0));
+    return ctl && (ctl->done || (skip_retry == 1 && ctl->tries > 0) || (skip_retry == 2 && ctl->am_skip));
 }
 
 // ---------------------------------------------------------------- Philox4x32-10

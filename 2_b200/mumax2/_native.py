@@ -67,7 +67,7 @@ def read_field(path):
     check(lib().mm_read_field(str(path).encode(), a.ctypes.data_as(C.c_void_p), a.size, C.byref(nc), n, C.byref(t)))
     return a.reshape(nc.value, n[0], n[1], n[2]), tuple(n), t.value
 
-SOLVERS = {"euler": 0, "heun": 1, "rk12": 2, "rk23": 3, "rk45": 4}
+SOLVERS = {"euler": 0, "heun": 1, "rk12": 2, "rk23": 3, "rk45": 4, "am12": 5}
 
 
 class MMProblem(C.Structure):
@@ -99,6 +99,7 @@ class MMStats(C.Structure):
         ("t", C.c_double), ("dt", C.c_double), ("err", C.c_double), ("peakerr", C.c_double),
         ("maxtorque", C.c_double), ("step", C.c_longlong), ("badsteps", C.c_longlong),
         ("attempts", C.c_longlong), ("evals", C.c_longlong), ("status", C.c_int), ("done", C.c_int),
+        ("iterations", C.c_longlong),
     ]
 
 
@@ -147,6 +148,7 @@ _PROTOS = {
     "mm_plan_device_bytes": (C.c_longlong, [C.c_void_p]),
     "mm_fields": (C.c_int, [C.c_void_p, C.c_void_p, C.c_longlong, C.c_double] + [C.c_void_p] * 6 + [C.c_void_p]),
     "mm_torque": (C.c_int, [C.c_void_p, C.c_void_p, C.c_longlong, C.c_double, C.c_void_p, C.c_void_p]),
+    "mm_solver_am12_tolerances": (C.c_int, [C.c_void_p, C.c_double, C.c_double]),
     "mm_solver_init": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double]),
     "mm_set_state": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
     "mm_get_state": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),

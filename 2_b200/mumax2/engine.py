@@ -56,7 +56,7 @@ def _swap_vec(v):
 
 class Engine:
     SOLVERS = {"solver/euler": "euler", "solver/heun": "heun", "solver/rk12": "rk12", "solver/rk23": "rk23",
-               "solver/rk45": "rk45"}
+               "solver/rk45": "rk45", "solver/am12": "am12"}
 
     def __init__(self, device=0):
         self.device = device
@@ -223,6 +223,10 @@ class Engine:
         self._add("m_error", 1, VALUE, "", "Error/step estimate for m")
         self._add("m_peakerror", 1, VALUE, "", "All-time maximum error/step for m")
         self._add("m_maxerror", 1, VALUE, "", "Maximum error/step for m", [1.0 / 2000.0])
+        if self.solver_name == "am12":  # solve_am01.go:316-366
+            self._add("bdf_iterations", 1, VALUE, "", "Number of iterations per step")
+            self._add("m_maxAbsError", 1, VALUE, "", "Maximum absolute error per step for m", [1e-4])
+            self._add("m_maxRelError", 1, VALUE, "", "Maximum relative error per step for m", [1e-3])
 
     # ------------------------------------------------------------ problem
     def _mult(self, name, default=0.0, comp=0):
@@ -299,7 +303,8 @@ class Engine:
             self._tables_dirty = False
         if self._solver_dirty and self.solver_name is not None:
             self.plan.solver(self.solver_name, dt=self.quant("dt").mult[0], mindt=self._mult("mindt", 1e-38),
-                             maxdt=self._mult("maxdt", 1e38), maxerr=self._mult("m_maxerror", 1.0 / 2000))
+                             maxdt=self._mult("maxdt", 1e38), maxerr=self._mult("m_maxerror", 1.0 / 2000),
+                             abs_err=self._mult("m_maxAbsError", 1e-4), rel_err=self._mult("m_maxRelError", 1e-3))
             st = self.plan.stats()
             self.plan.set_time(self.quant("t").mult[0], self.quant("dt").mult[0])
             del st
@@ -323,6 +328,8 @@ class Engine:
             self.quant("badsteps").mult = [float(st["badsteps"])]
             self.quant("m_error").mult = [st["err"]]
             self.quant("m_peakerror").mult = [st["peakerr"]]
+        if self.has("bdf_iterations"):
+            self.quant("bdf_iterations").mult = [float(st["iterations"])]
 
     # ------------------------------------------------------------ API (api.go)
     def setv(self, name, value):
@@ -334,7 +341,7 @@ class Engine:
         lname = name.lower()
         if lname == "m":
             raise ValueError("m is a field: use setarray")
-        if lname in ("dt", "mindt", "maxdt", "m_maxerror", "t", "cutoff_dt"):
+        if lname in ("dt", "mindt", "maxdt", "m_maxerror", "t", "cutoff_dt", "m_maxabserror", "m_maxrelerror"):
             self._solver_dirty = True
         else:
             self._dirty_params = True
@@ -505,7 +512,8 @@ class Engine:
     SAVE_CAPACITY = 32
     EXT = {0: "ovf", 1: "ovf", 2: "omf", 3: "omf", 4: "dump"}
 
-    def _output_id(self, t):
+    def _next_output_id(self, t):
+        """OutputID (engine.go:98-105): a new number whenever the time has changed."""
         if t != self._last_output_t:
             self._last_output_t = t
             self._output_id += 1
@@ -513,7 +521,7 @@ class Engine:
 
     def _auto_filename(self, quant, code, t):
         import os
-        return os.path.join(self.outdir, f"{quant}{self._output_id(t):06d}.{self.EXT[code]}")
+        return os.path.join(self.outdir, f"{quant}{self._next_output_id(t):06d}.{self.EXT[code]}")
 
     def _field_array(self, name):
         lname = name.lower()

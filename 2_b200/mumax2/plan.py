@@ -120,8 +120,12 @@ class Plan:
         return t, md
 
     # ---- stepping
-    def solver(self, name="rk12", dt=1e-15, mindt=1e-38, maxdt=1e38, maxerr=1.0 / 2000):
+    def solver(self, name="rk12", dt=1e-15, mindt=1e-38, maxdt=1e38, maxerr=1.0 / 2000, abs_err=1e-4, rel_err=1e-3):
+        """maxerr: the explicit solvers' error per step; abs_err/rel_err: solver/am12's
+        m_maxAbsError and m_maxRelError."""
         nat.check(nat.lib().mm_solver_init(self.h, nat.SOLVERS[name], dt, mindt, maxdt, maxerr))
+        if name == "am12":
+            nat.check(nat.lib().mm_solver_am12_tolerances(self.h, abs_err, rel_err))
         self._solver = name
 
     def set_state(self, m):

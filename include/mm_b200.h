@@ -21,7 +21,8 @@
  *   mm_solver_init/mm_step/mm_run/mm_steps/mm_run_until_maxtorque
  *                         Solver.Step (src/mumax/engine/solver.go:14-17): solver/rk12
  *                         (solve_rk12.go:91-214), euler (solve_euler.go:22-50), heun
- *                         (solve_heun.go:27-79); Engine.Run/Steps (engine.go:489-524);
+ *                         (solve_heun.go:27-79), am12 (solve_am01.go:46-301);
+ *                         Engine.Run/Steps (engine.go:489-524);
  *                         API.Run_Until_Smaller (api.go:122-131).  rk23/rk45 are new.
  *   mm_maxtorque          MaxNormUpdater (update_reduce.go:103-108, reductor.go:173-186)
  *   mm_average            AverageUpdater (update_reduce.go:47-69)
@@ -60,7 +61,7 @@ enum {
 };
 
 /* solvers */
-enum { MM_EULER = 0, MM_HEUN = 1, MM_RK12 = 2, MM_RK23 = 3, MM_RK45 = 4 };
+enum { MM_EULER = 0, MM_HEUN = 1, MM_RK12 = 2, MM_RK23 = 3, MM_RK45 = 4, MM_AM12 = 5 };
 
 /* Problem description.  Multipliers in SI units; masks are DEVICE float arrays of
  * n0*n1*n2 values multiplying the multiplier (NULL = uniform 1), exactly the
@@ -105,6 +106,7 @@ typedef struct mm_stats {
     double t, dt, err, peakerr, maxtorque;
     long long step, badsteps, attempts, evals;
     int status, done;
+    long long iterations;  /* solver/am12: fixed-point iterations of the last step */
 } mm_stats;
 
 typedef struct mm_plan_s* mm_plan;
@@ -151,6 +153,8 @@ MM_API int mm_torque(mm_plan plan, float* m, long long noise_step, double dt_the
 /* ---- time stepping: the plan owns the state; all control runs on the device ---- */
 MM_API int mm_solver_init(mm_plan plan, int solver, double dt, double mindt, double maxdt,
                           double maxerr);
+/* solver/am12 error tolerances m_maxAbsError, m_maxRelError (defaults 1e-4, 1e-3). */
+MM_API int mm_solver_am12_tolerances(mm_plan plan, double abs_err, double rel_err);
 MM_API int mm_set_state(mm_plan plan, const float* m, int from_host, mm_stream stream);
 MM_API int mm_get_state(mm_plan plan, float* m, int to_host, mm_stream stream);
 MM_API int mm_set_time(mm_plan plan, double t, double dt);

@@ -1015,6 +1015,120 @@ extern "C" int or_step(void* p, int solver, double* m, or_state* st, double* k_f
     return in_range ? 0 : -2;
 }
 
+// solver/am12 (solve_am01.go:46-301): explicit Euler start, implicit Euler (BDF1)
+// predictor and trapezoidal (Adams-Moulton 2) corrector, each solved by fixed-point
+// iteration; the difference of the two controls dt.  Error norm of solve_am01.go:129-137:
+// sqrt(mean over components of (max|a-b| / (abs_err + max|b| rel_err))^2).  As in the
+// reference the iterate y is left as computed (normalised only when the RHS pulls it),
+// badsteps and iterations count this step only, and *alpha carries the last predictor
+// convergence ratio across steps.
+static double am_norm(const double* a, const double* b, long N, double abs_err, double rel_err) {
+    double t = 0;
+    for (int c = 0; c < 3; c++) {
+        double md = 0, mb = 0;
+        for (long i = 0; i < N; i++) {
+            md = std::max(md, std::fabs(a[c * N + i] - b[c * N + i]));
+            mb = std::max(mb, std::fabs(b[c * N + i]));
+        }
+        const double r = md / (abs_err + mb * rel_err);
+        t += r * r;
+    }
+    return std::sqrt(t) / std::sqrt(3.0);
+}
+
+extern "C" int or_step_am12(void* p, double* m, or_state* st, double abs_err, double rel_err, double* alpha,
+                            long long* iterations) {
+    OrProblem* P = (OrProblem*)p;
+    const long N = P->N, N3 = 3 * N;
+    const double gam = P->d.gamma;
+    const long long ns = st->noise_step;
+    bool in_range = true;
+    auto f = [&](double* y, double* k, double tt) {
+        P->t_eval = tt;
+        if (!apply_tables(P)) in_range = false;
+        or_torque(p, y, ns, st->dt_thermal > 0 ? st->dt_thermal : st->dt, k, nullptr);
+        st->evals++;
+    };
+    const double t0 = st->t;
+    st->badsteps = 0;
+    *iterations = 0;
+    std::vector<double> y0(N3), dy0(N3), dy(N3), dybuf(N3), yb(N3), y1(N3);
+    f(m, dy0.data(), t0);
+    std::copy(m, m + N3, y0.begin());
+    const int maxTry = 10, maxIter = 5;
+    const double headRoom = 0.8, maxIterErr = 0.1, alpha_ref = 0.6;
+    int tr = 0;
+    bool restrict_step = false;
+    for (;;) {
+        const double dt = st->dt, h = dt * gam;
+        bool badStep = false, badIt = false;
+        for (long i = 0; i < N3; i++) m[i] = y0[i] + h * dy0[i];
+        (*iterations)++;
+        st->t = t0 + dt;
+        f(m, dy.data(), t0 + dt);
+        dybuf = dy;
+        double er = maxIterErr, a = 0;
+        int iter = 0;
+        for (;;) {  // implicit Euler
+            for (long i = 0; i < N3; i++) yb[i] = y0[i] + h * dy[i];
+            const double te = am_norm(m, yb.data(), N, abs_err, rel_err);
+            a = te / er;
+            *alpha = a;
+            er = te;
+            std::copy(yb.begin(), yb.end(), m);
+            iter++;
+            (*iterations)++;
+            if (te <= maxIterErr) break;
+            if (a >= 1.0 || iter > maxIter) { badIt = true; break; }
+            f(m, dy.data(), t0 + dt);
+        }
+        if (badIt && tr == maxTry - 1) return -1;
+        if (badIt) {
+            st->dt = a > alpha_ref ? dt * std::sqrt(alpha_ref / a) : 0.5 * dt;
+            restrict_step = true;
+            continue;
+        }
+        std::copy(m, m + N3, y1.begin());
+        dy = dybuf;
+        er = maxIterErr;
+        iter = 0;
+        for (;;) {  // trapezoidal
+            for (long i = 0; i < N3; i++) yb[i] = y0[i] + 0.5 * h * (dy[i] + dy0[i]);
+            const double te = am_norm(m, yb.data(), N, abs_err, rel_err);
+            a = te / er;
+            er = te;
+            std::copy(yb.begin(), yb.end(), m);
+            iter++;
+            (*iterations)++;
+            if (te <= maxIterErr) break;
+            if (a >= 1.0 || iter > maxIter) { badIt = true; break; }
+            f(m, dy.data(), t0 + dt);
+        }
+        if (badIt && tr == maxTry - 1) return -1;
+        if (badIt) {
+            st->dt = a > alpha_ref ? dt * std::sqrt(alpha_ref / a) : 0.5 * dt;
+            continue;
+        }
+        const double te = am_norm(m, y1.data(), N, abs_err, rel_err);
+        if (te > 1.0) { st->badsteps++; badStep = true; }
+        st->err = te;
+        double nd = dt * std::sqrt(headRoom / te);
+        if (restrict_step) {
+            nd = std::min(nd, dt * std::sqrt(alpha_ref / *alpha));
+            restrict_step = false;
+        }
+        nd = std::max(nd, st->mindt);
+        nd = std::min(nd, st->maxdt);
+        st->dt = nd;
+        if (!badStep || nd == st->mindt) break;
+        if (tr > maxTry) return -1;
+        tr++;
+    }
+    st->step++;
+    st->noise_step++;
+    return in_range ? 0 : -2;
+}
+
 extern "C" int or_num_threads(void) {
 #ifdef _OPENMP
     return omp_get_max_threads();

@@ -49,7 +49,7 @@ class OrState(C.Structure):
     ]
 
 
-SOLVERS = {"euler": 0, "heun": 1, "rk12": 2, "rk23": 3, "rk45": 4}
+SOLVERS = {"euler": 0, "heun": 1, "rk12": 2, "rk23": 3, "rk45": 4, "am12": 5}
 
 MASK_SCALARS = ["msat", "aex", "alpha", "ku", "temp", "xi", "zl_pol", "sl_pol", "lambda",
                 "eps_prime", "t_fl"]
@@ -84,6 +84,9 @@ def lib():
         L.or_set_table.restype = C.c_int
         L.or_set_table.argtypes = [C.c_void_p, C.c_int, C.c_long, DP]
         L.or_set_time.argtypes = [C.c_void_p, C.c_double]
+        L.or_step_am12.restype = C.c_int
+        L.or_step_am12.argtypes = [C.c_void_p, DP, C.POINTER(OrState), C.c_double, C.c_double,
+                                   C.POINTER(C.c_double), C.POINTER(C.c_longlong)]
         _LIB = L
     return _LIB
 
@@ -230,7 +233,8 @@ class OracleRun:
     """Time integration with the oracle's solvers (reference semantics)."""
 
     def __init__(self, oracle, m, solver="rk12", dt=1e-15, mindt=1e-38, maxdt=1e38, maxerr=1.0 / 2000,
-                 dt_thermal=0.0):
+                 dt_thermal=0.0, abs_err=1e-4, rel_err=1e-3):
+        self.abs_err, self.rel_err = abs_err, rel_err
         self.o = oracle
         self.m = oracle._m(m)
         self.solver = SOLVERS[solver]
@@ -240,6 +244,17 @@ class OracleRun:
         self.fv = C.c_int(0)
 
     def step(self):
+        if self.solver == SOLVERS["am12"]:
+            if not hasattr(self, "am_alpha"):
+                self.am_alpha = C.c_double(0.0)
+                self.am_iterations = C.c_longlong(0)
+            rc = lib().or_step_am12(self.o.h, _dp(self.m), C.byref(self.st), self.abs_err, self.rel_err,
+                                    C.byref(self.am_alpha), C.byref(self.am_iterations))
+            if rc == -2:
+                raise RuntimeError("time outside a pointwise table")
+            if rc != 0:
+                raise RuntimeError("the Adams-Moulton iterator cannot converge")
+            return
         rc = lib().or_step(self.o.h, self.solver, _dp(self.m), C.byref(self.st), _dp(self.kf), C.byref(self.fv))
         if rc == -2:
             raise RuntimeError("time outside a pointwise table")
