@@ -423,6 +423,7 @@ struct mm_plan_s {
     int tab_cap[2] = {0, 0};
     std::vector<double> tab_host[2];
     double t_eval = 0.0;             // time of standalone evaluations
+    double dt0 = 1e-15;              // initial dt of the solver (mm_batch_restart)
     // asynchronous snapshots (mm_save_async): device staging is Mtmp; pinned host copy,
     // side stream, events and the writer thread are made on first use
     float* snap_host = nullptr;
@@ -1396,6 +1397,7 @@ extern "C" MM_API int mm_solver_init(mm_plan p, int solver, double dt, double mi
     for (int b = 0; b < p->nsim; b++) {
         DevCtl& c = p->ctl_host[b];
         c.dt = dt;
+        p->dt0 = dt;
         c.mindt = mindt;
         c.maxdt = maxdt;
         c.maxerr = maxerr;
@@ -1577,7 +1579,7 @@ static int next_batch(long long max_left, int grow) {
 
 // Runs attempts until the device sets `done` for every simulation.  The host only polls
 // the summary between batches of queued attempts.
-static int drive(mm_plan p, cudaStream_t st, long long max_attempts) {
+static int drive(mm_plan p, cudaStream_t st, long long max_attempts, int target_active = 0) {
     int grow = 4;
     long long launched = 0;
     long long max_left = 0;
@@ -1590,7 +1592,7 @@ static int drive(mm_plan p, cudaStream_t st, long long max_attempts) {
         launched += batch;
         if ((rc = read_summary(p, st))) return rc;
         if ((rc = summary_status(p))) return rc;
-        if (p->hsum->active == 0) return MM_OK;
+        if (p->hsum->active <= target_active) return MM_OK;
         if (max_attempts > 0 && launched >= max_attempts) return set_err(MM_ERR_TIMEOUT, "attempt limit reached");
         max_left = p->hsum->max_left;
         if (grow < 64) grow *= 2;
@@ -2094,4 +2096,101 @@ extern "C" MM_API int mm_save_async(mm_plan p, const char* path, int format, mm_
         }
     });
     return MM_OK;
+}
+
+// ---------------------------------------------------------------- continuous batching
+// A batched plan as a pool of slots: finished simulations are replaced by new problems
+// while the others keep their state, so the GPU never waits for a batch's slowest member.
+
+extern "C" MM_API int mm_batch_restart(mm_plan p, int count, const int* idx, const float* m, int from_host,
+                                       const mm_sim* sims, const double* thr, mm_stream stream) {
+    if (!p || count < 0 || (count > 0 && (!idx || !m || !thr))) return set_err(MM_ERR_ARG, "bad argument");
+    if (p->solver < 0) return set_err(MM_ERR_STATE, "no solver: call mm_solver_init");
+    cudaStream_t st = (cudaStream_t)stream;
+    for (int k = 0; k < count; k++) {
+        if (idx[k] < 0 || idx[k] >= p->nsim) return set_err(MM_ERR_ARG, "slot %d out of range", idx[k]);
+        if (!(thr[k] > 0)) return set_err(MM_ERR_ARG, "threshold must be > 0");
+    }
+    if (sims) {
+        int rc = check_sims(sims, count);
+        if (rc) return rc;
+    }
+    int rc = canonicalise(p, st);
+    if (rc) return rc;
+    if ((rc = read_ctl(p, st))) return rc;
+    std::vector<int> was_done(p->nsim);
+    for (int b = 0; b < p->nsim; b++) was_done[b] = p->ctl_host[b].done;
+    std::vector<char> restarted(p->nsim, 0);
+    const size_t n3 = (size_t)p->n3();
+    for (int k = 0; k < count; k++) {
+        const int b = idx[k];
+        restarted[b] = 1;
+        if (sims) p->sims[b] = sims[k];
+        CUCHK(cudaMemcpyAsync(p->Y[0] + b * n3, m + k * n3, sizeof(float) * n3,
+                              from_host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, st));
+        normalize_kernel<<<local_blocks(p->g.N), 256, 0, st>>>(
+            p->Y[0] + b * n3, p->P.msat_mask ? p->P.msat_mask + b * p->P.mask_bstride : nullptr, p->g.N, 0, 0);
+        CUCHK(cudaGetLastError());
+        DevCtl& c = p->ctl_host[b];
+        const DevCtl keep = c;
+        memset(&c, 0, sizeof c);
+        c.dt = p->dt0;
+        c.mindt = keep.mindt;
+        c.maxdt = keep.maxdt;
+        c.maxerr = keep.maxerr;
+        c.headroom = keep.headroom;
+        c.gamma = keep.gamma;
+        c.h = c.dt * c.gamma;
+        c.dt_thermal = keep.dt_thermal;
+        c.t_end = 1e300;
+        c.step_end = (1LL << 62);
+        c.torque_thr = thr[k];
+        c.am_abs_err = keep.am_abs_err;
+        c.am_rel_err = keep.am_rel_err;
+    }
+    if (sims) {
+        if ((rc = upload_sims(p))) return rc;
+        if (p->nsim == 1) free_graph(p);  // a single plan's scalars live in the captured parameters
+    }
+    // the FSAL derivative of the new states: the other slots sit out this evaluation
+    for (int b = 0; b < p->nsim; b++) p->ctl_host[b].done = restarted[b] ? 0 : 1;
+    if ((rc = write_ctl(p, st))) return rc;
+    if (p->solver == MM_RK23 || p->solver == MM_RK45) {
+        StageOp o = op_blank();
+        o.m_in = cur_of(p->Y);
+        o.k_out = cur_of(p->K1);
+        o.want_tq = 1;
+        if ((rc = launch_eval(p, o, p->ctl, 0, nullptr, 0, 0, nullptr, nullptr, st, nullptr))) return rc;
+    }
+    if ((rc = read_ctl(p, st))) return rc;
+    for (int b = 0; b < p->nsim; b++) {
+        DevCtl& c = p->ctl_host[b];
+        if (!restarted[b]) {
+            c.done = was_done[b];
+            continue;
+        }
+        if (p->solver == MM_RK23 || p->solver == MM_RK45) {
+            float tqv;
+            memcpy(&tqv, &c.tq_bits, sizeof tqv);
+            c.maxtorque = sqrt((double)tqv) * c.gamma;
+            c.fsal_valid = 1;
+            if (c.maxtorque < c.torque_thr) c.done = 1;
+        }
+        c.tq_bits = 0;
+    }
+    p->state_set = true;
+    return write_ctl(p, st);
+}
+
+extern "C" MM_API int mm_batch_drive(mm_plan p, int target_active, long long max_attempts, mm_stream stream) {
+    if (!p) return set_err(MM_ERR_ARG, "null plan");
+    if (p->solver < 0) return set_err(MM_ERR_STATE, "no solver: call mm_solver_init");
+    cudaStream_t st = (cudaStream_t)stream;
+    p->run_until = true;
+    int rc = read_ctl(p, st);
+    if (rc) return rc;
+    if (any_active(p)) rc = drive(p, st, max_attempts, target_active);
+    int rc2 = canonicalise(p, st);
+    int rc3 = read_ctl(p, st);
+    return rc ? rc : (rc2 ? rc2 : rc3);
 }

@@ -252,6 +252,27 @@ class Plan:
         nat.check(nat.lib().mm_batch_run_until_maxtorque(self.h, self._thr.ctypes.data_as(C.c_void_p),
                                                          int(max_steps), None))
 
+    def batch_restart(self, idx, m, thr, sims=None):
+        """Put new problems into slots idx (continuous batching): states m [k][3N] (host),
+        torque thresholds thr [k], optional scalar dicts sims [k].  Per-simulation masks
+        are updated by writing into this plan's mask tensors before the call."""
+        idx = np.ascontiguousarray(idx, dtype=np.int32)
+        m = np.ascontiguousarray(m, dtype=np.float32).reshape(len(idx), -1)
+        thr = np.ascontiguousarray(thr, dtype=np.float64)
+        sa = nat.make_sims(self.problem, sims) if sims is not None else None
+        nat.check(nat.lib().mm_batch_restart(self.h, len(idx), idx.ctypes.data_as(C.c_void_p),
+                                             m.ctypes.data_as(C.c_void_p), 1,
+                                             C.cast(sa, C.c_void_p) if sa is not None else None,
+                                             thr.ctypes.data_as(C.c_void_p), None))
+
+    def batch_drive(self, target_active=0, max_attempts=0):
+        """Step until at most target_active simulations are still running."""
+        nat.check(nat.lib().mm_batch_drive(self.h, int(target_active), int(max_attempts), None))
+
+    def mask_tensor(self, name):
+        """The device tensor behind a mask (for in-place slot updates)."""
+        return self._masks[name]
+
     def batch_stats(self):
         arr = (nat.MMStats * self.nsim)()
         nat.check(nat.lib().mm_batch_stats(self.h, C.cast(arr, C.c_void_p), None))

@@ -339,36 +339,43 @@ def ensemble_bench(args, rank, world, local_rank, dist):
 # ---------------------------------------------------------------- relaxation workload
 def relax_bench(args, rank, world, local_rank, dist):
     """Batched plain relaxations: 64x64x1 films with seeded geometry masks and parameters,
-    `--relax-batch` per plan, from the cold start (uniform along +x), RK23 with
-    alpha = 1 until each simulation's maxtorque / (gamma Ms) < 1e-4.  value =
-    relaxations / device time.  Every batch reuses one plan (new masks and scalars)."""
+    from the cold start (uniform along +x), RK23 with alpha = 1 until each simulation's
+    maxtorque / (gamma Ms) < 1e-4.  Two schedules over one plan of --relax-batch slots:
+    synchronous batches (a batch waits for its slowest member) and continuous batching
+    (a finished slot takes the next problem at once).  value = relaxations / device time
+    of the continuous schedule."""
     import torch
     from mumax2 import Plan
     from mumax2 import workloads as W
     B = args.relax_batch
     nb = max(1, args.nsim // B)
-    problem, sims, masks = W.relax_set(nb * B, seed=rank)
+    nrel = nb * B
+    problem, sims, masks = W.relax_set(nrel, seed=rank)
     n = problem["n"]
+    N = int(np.prod(n))
     gamma = problem["gamma"]
-    plan = None
-    total_ms, steps, conv, worst = 0.0, [], 0, 0.0
+    thr_all = np.array([1e-4 * gamma * s["msat"] for s in sims])
+    cold1 = W.cold_state(n, 1)
+    plan = Plan(problem, masks={"msat": np.concatenate(masks[:B])}, sims=sims[:B], masks_per_sim=True,
+                device=local_rank)
+    plan.solver("rk23", dt=1e-14, maxerr=args.relax_maxerr)
     sampler = ClockSampler(local_rank)
     sampler.start()
-    for k in range(nb + 1):  # batch 0 is an untimed warm-up (the same problems as batch 1)
+
+    def events():
+        return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    # synchronous batches (batch 0 repeated first as an untimed warm-up)
+    sync_ms, sync_steps, sync_conv = 0.0, [], 0
+    for k in range(nb + 1):
         j = max(0, k - 1)
         bs = sims[j * B:(j + 1) * B]
-        bm = {"msat": np.concatenate(masks[j * B:(j + 1) * B])}
-        if plan is None:
-            plan = Plan(problem, masks=bm, sims=bs, masks_per_sim=True, device=local_rank)
-            plan.solver("rk23", dt=1e-14, maxerr=args.relax_maxerr)
-        else:
-            plan.set_problem(problem, masks=bm)
-            plan.set_sims(bs)
-            plan.solver("rk23", dt=1e-14, maxerr=args.relax_maxerr)
-        thr = np.array([1e-4 * gamma * s["msat"] for s in bs])
+        plan.mask_tensor("msat").copy_(torch.from_numpy(np.concatenate(masks[j * B:(j + 1) * B])))
+        plan.set_sims(bs)
+        plan.solver("rk23", dt=1e-14, maxerr=args.relax_maxerr)
+        thr = thr_all[j * B:(j + 1) * B]
         torch.cuda.synchronize()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
+        e0, e1 = events()
         e0.record()
         plan.set_state(W.cold_state(n, B))
         plan.batch_run_until_maxtorque(thr, max_steps=args.relax_max_steps)
@@ -376,25 +383,76 @@ def relax_bench(args, rank, world, local_rank, dist):
         torch.cuda.synchronize()
         if k == 0:
             continue
-        total_ms += e0.elapsed_time(e1)
+        sync_ms += e0.elapsed_time(e1)
         st = plan.batch_stats()
-        steps += [s["step"] for s in st]
-        conv += sum(1 for s, t in zip(st, thr) if s["maxtorque"] < t)
-        worst = max(worst, max(s["maxtorque"] / (gamma * q["msat"]) for s, q in zip(st, bs)))
+        sync_steps += [s["step"] for s in st]
+        sync_conv += sum(1 for s, t in zip(st, thr) if s["maxtorque"] < t)
+
+    # continuous batching over the same problems
+    refill = max(1, B // 8)
+    mt = plan.mask_tensor("msat")
+    slot_job = [-1] * B
+    nxt = 0
+    cont_steps, cont_conv, worst = [], 0, 0.0
+    torch.cuda.synchronize()
+    e0, e1 = events()
+    e0.record()
+
+    def fill(slots):
+        nonlocal nxt
+        idx, jobs = [], []
+        for b in slots:
+            if nxt >= nrel:
+                break
+            mt[b * N:(b + 1) * N].copy_(torch.from_numpy(masks[nxt]))
+            slot_job[b] = nxt
+            idx.append(b)
+            jobs.append(nxt)
+            nxt += 1
+        if idx:
+            plan.batch_restart(idx, np.repeat(cold1[None, :], len(idx), axis=0), thr_all[jobs],
+                               sims=[sims[q] for q in jobs])
+
+    fill(range(B))
+    done_count = 0
+    while done_count < nrel:
+        target = max(0, B - refill) if nxt < nrel else 0
+        plan.batch_drive(target_active=target)
+        st = plan.batch_stats()
+        free = []
+        for b in range(B):
+            if slot_job[b] >= 0 and st[b]["done"]:
+                q = slot_job[b]
+                cont_steps.append(st[b]["step"])
+                if st[b]["maxtorque"] < thr_all[q]:
+                    cont_conv += 1
+                worst = max(worst, st[b]["maxtorque"] / (gamma * sims[q]["msat"]))
+                slot_job[b] = -1
+                done_count += 1
+                free.append(b)
+        fill(free)
+    e1.record()
+    torch.cuda.synchronize()
+    cont_ms = e0.elapsed_time(e1)
     clocks = sampler.stop()
-    nrel = nb * B
-    ms_max, value = aggregate(total_ms, 1, nrel, world, dist, "cuda")
+    ms_max, value = aggregate(cont_ms, 1, nrel, world, dist, "cuda")
+    _, sync_value = aggregate(sync_ms, 1, nrel, world, dist, "cuda")
     if rank == 0:
         line = {"metric": "relaxations/s", "value": value, "unit": "relaxations/s", "n_gpus": world,
                 "steps": nrel, "warmup": 1, "ms_per_step": ms_max / nrel, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": {"workload": "relax_64x64x1_cold", "relaxations": nrel, "batch": B,
-                           "grid_xyz": list(W.RELAX_GRID_USER), "cell_nm": [4, 4, 3], "solver": "rk23",
-                           "maxerr": args.relax_maxerr, "alpha": 1.0, "start": "cold (uniform +x)",
+                "config": {"workload": "relax_64x64x1_cold", "relaxations": nrel, "slots": B,
+                           "refill_per_drive": refill, "grid_xyz": list(W.RELAX_GRID_USER), "cell_nm": [4, 4, 3],
+                           "solver": "rk23", "maxerr": args.relax_maxerr, "alpha": 1.0,
+                           "start": "cold (uniform +x)",
                            "criterion": "maxtorque / (gamma Ms) < 1e-4 per simulation",
                            "parallelism": f"replicas{world}"},
-                "relax": {"converged": conv, "of": nrel, "steps_mean": float(np.mean(steps)),
-                          "steps_max": int(np.max(steps)), "worst_torque_over_gamma_ms": worst},
+                "relax": {"schedule": "continuous batching", "converged": cont_conv, "of": nrel,
+                          "steps_mean": float(np.mean(cont_steps)), "steps_max": int(np.max(cont_steps)),
+                          "worst_torque_over_gamma_ms": worst},
+                "synchronous_batches": {"value": sync_value, "unit": "relaxations/s", "converged": sync_conv,
+                                        "steps_mean": float(np.mean(sync_steps)),
+                                        "steps_max": int(np.max(sync_steps))},
                 "clocks": clocks}
         print(json.dumps(line), flush=True)
     plan.close()

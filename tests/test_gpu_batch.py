@@ -230,3 +230,39 @@ def test_batch_per_simulation_thresholds():
         s.run_until_maxtorque(float(thr[b]), max_steps=50000)
         assert st[b]["step"] == s.stats()["step"], b
         assert np.abs(mb[3 * N * b:3 * N * (b + 1)] - s.get_state()).max() < TOL_SAME
+
+
+def test_continuous_batching_slots_restart_independently():
+    """mm_batch_restart / mm_batch_drive: a finished slot takes a new problem while the
+    other slots keep running; every problem ends exactly as it does alone."""
+    from mumax2 import Plan
+    n = (1, 16, 16)
+    base = _base(n)
+    N = n[0] * n[1] * n[2]
+    probs = [dict(s, alpha=1.0) for s in SIMS] + [dict(SIMS[0], alpha=1.0, msat=6e5)]
+    ms = [rand_m(n, 800 + q, kind="near_x") for q in range(4)]
+    thr = [1e-4 * 2.211e5 * p["msat"] * 3 for p in probs]
+    g = Plan(base, sims=probs[:2])
+    g.solver("rk23", dt=1e-14, maxerr=1e-6)
+    g.batch_restart([0, 1], np.stack(ms[:2]), thr[:2], sims=probs[:2])
+    slot_job, nxt, results = [0, 1], 2, {}
+    while len(results) < 4:
+        g.batch_drive(target_active=1 if nxt < 4 else 0)
+        st = g.batch_stats()
+        state = g.get_state()
+        for b in range(2):
+            q = slot_job[b]
+            if q >= 0 and st[b]["done"]:
+                results[q] = (st[b]["step"], state[3 * N * b:3 * N * (b + 1)].copy())
+                slot_job[b] = -1
+                if nxt < 4:
+                    g.batch_restart([b], ms[nxt][None, :], [thr[nxt]], sims=[probs[nxt]])
+                    slot_job[b] = nxt
+                    nxt += 1
+    for q in range(4):
+        s = _single(base, probs[q])
+        s.solver("rk23", dt=1e-14, maxerr=1e-6)
+        s.set_state(ms[q])
+        s.run_until_maxtorque(thr[q], max_steps=50000)
+        assert results[q][0] == s.stats()["step"], q
+        assert np.abs(results[q][1] - s.get_state()).max() < TOL_SAME, q
