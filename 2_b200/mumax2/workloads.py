@@ -127,3 +127,49 @@ def relax_set(nsim, seed=0):
 def cold_state(n, count):
     """The uninformed start of a plain relax: uniform along user +x (internal component 2)."""
     return uniform_state(n, (0.0, 0.0, 1.0), count)
+
+
+# ---------------------------------------------------------------- single-simulation configs
+def sp4_film(seed=0):
+    """128x32x1 film of 3.90625x3.90625x3 nm (the SP4 geometry): Ms 8e5, Aex 1.3e-11,
+    alpha 0.02; m = (1, 0.1, 0) + seeded uniform noise of amplitude 0.01, renormalised;
+    an in-plane field of seeded magnitude U[10, 30] mT at a seeded angle.  Returns
+    (problem, m0) in internal order."""
+    rng = np.random.default_rng(seed)
+    n = (1, 32, 128)
+    N = 32 * 128
+    bmag = rng.uniform(0.01, 0.03)
+    phi = rng.uniform(0, 2 * np.pi)
+    b_user = (bmag * np.cos(phi), bmag * np.sin(phi), 0.0)
+    problem = dict(n=n, cell=(3e-9, 3.90625e-9, 3.90625e-9), pbc=(0, 0, 0), demag=1, exchange=1, zeeman=1,
+                   msat=8e5, aex=1.3e-11, alpha=0.02, gamma=2.211e5, bext=_internal(b_user))
+    m = np.zeros((3, N))
+    m[2] = 1.0   # user x
+    m[1] = 0.1   # user y
+    m += 0.01 * rng.uniform(-1, 1, size=(3, N))
+    m /= np.linalg.norm(m, axis=0, keepdims=True)
+    return problem, m.astype(np.float32).ravel()
+
+
+def neel_wall_strip(seed=0, current=1e12):
+    """512x128x1 strip of 2 nm cells: Ms 8.6e5, Aex 1.3e-11, alpha 0.02, a Neel wall
+    m_x = -tanh((x - x0)/20 nm), m_y = sech((x - x0)/20 nm) with x0 ~ U[300, 700] nm, and
+    Zhang-Li torque with j along x (P 0.5, xi 0.05).  Returns (problem, m0, x0)."""
+    rng = np.random.default_rng(seed)
+    nx, ny = 512, 128
+    x0 = rng.uniform(300e-9, 700e-9)
+    x = (np.arange(nx) + 0.5) * 2e-9
+    u = (x - x0) / 20e-9
+    mx, my = -np.tanh(u), 1.0 / np.cosh(u)
+    m = np.zeros((3, 1, ny, nx))
+    m[2] = mx[None, None, :]
+    m[1] = my[None, None, :]
+    problem = dict(n=(1, ny, nx), cell=(2e-9, 2e-9, 2e-9), pbc=(0, 0, 0), demag=1, exchange=1, zhangli=1,
+                   msat=8.6e5, aex=1.3e-11, alpha=0.02, gamma=2.211e5, zl_pol=0.5, xi=0.05,
+                   j=(0.0, 0.0, float(current)))
+    return problem, m.astype(np.float32).ravel(), x0
+
+
+def wall_position(avg_mx_user, length):
+    """Position of a +x | -x wall from <m_x>: <m_x> = (2 x_w - L) / L."""
+    return 0.5 * length * (1.0 + avg_mx_user)

@@ -458,6 +458,84 @@ def relax_bench(args, rank, world, local_rank, dist):
     plan.close()
 
 
+# ---------------------------------------------------------------- single-simulation configs
+def single_bench(args, rank, world, local_rank, dist):
+    """configs[0] (--workload sp4: the 128x32x1 film, RK45, <m> every 10 ps) and configs[2]
+    (--workload wall: the 512x128x1 Neel wall under Zhang-Li current, RK45, with the wall
+    position from <m_x> every 10 ps, plus the Slonczewski variant on a 128x128x1 disk).
+    Latency-bound sizes: the numbers are simulated time and steps per second."""
+    import torch
+    from mumax2 import Plan
+    from mumax2 import workloads as W
+    dur = args.duration
+    runs = []
+    if args.workload == "sp4":
+        prob, m0 = W.sp4_film(seed=rank)
+        runs.append(("sp4_film_128x32x1_rk45", prob, m0, None))
+        dur = dur or 1e-9
+    else:
+        prob, m0, x0 = W.neel_wall_strip(seed=rank)
+        runs.append(("neel_wall_512x128x1_zhangli_rk45", prob, m0, x0))
+        # Slonczewski variant: 128x128x1 disk, p = +z (user), lambda 1, current along z
+        n = (1, 128, 128)
+        yy, xx = np.mgrid[0:128, 0:128]
+        disk = (((xx + 0.5 - 64) ** 2 + (yy + 0.5 - 64) ** 2) <= 64 ** 2).astype(np.float32).ravel()
+        sprob = dict(n=n, cell=(2e-9, 2e-9, 2e-9), pbc=(0, 0, 0), demag=1, exchange=1, slonczewski=1,
+                     msat=8.6e5, aex=1.3e-11, alpha=0.02, gamma=2.211e5, p=(1.0, 0.0, 0.0), sl_pol=0.5,
+                     **{"lambda": 1.0}, eps_prime=0.0, t_fl=2e-9, j=(1e11, 0.0, 0.0))
+        sm = W.uniform_state(n, (0.1, 0.0, 1.0)).reshape(3, -1) * disk[None, :]
+        runs.append(("slonczewski_disk_128x128x1_rk45", (sprob, {"msat": disk}), sm.ravel(), None))
+        dur = dur or 5e-9
+    out = []
+    sampler = ClockSampler(local_rank)
+    sampler.start()
+    for name, prob, m0, x0 in runs:
+        masks = {}
+        if isinstance(prob, tuple):
+            prob, masks = prob
+        plan = Plan(prob, masks=masks, device=local_rank)
+        plan.solver("rk45", dt=1e-15, maxerr=1e-5)
+        plan.set_state(m0)
+        plan.tabulate(1e-11, capacity=int(dur / 1e-11) + 16)
+        plan.run(2e-11)       # warm-up: graph capture, first steps
+        plan.tabulate_read()
+        st0 = plan.stats()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        plan.run(dur)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        st = plan.stats()
+        rows = plan.tabulate_read()[0]
+        N = int(np.prod(prob["n"]))
+        steps = st["step"] - st0["step"]
+        rec = {"workload": name, "cells": N, "simulated_s": dur, "steps": steps, "ms": ms,
+               "steps_per_s": steps / (ms / 1e3), "cell_steps_per_s": N * steps / (ms / 1e3),
+               "simulated_ns_per_s": dur * 1e9 / (ms / 1e3), "attempts": st["attempts"] - st0["attempts"],
+               "avg_m_user_end": [float(v) for v in plan.average()[::-1]], "table_rows": len(rows)}
+        if x0 is not None and len(rows) > 4:
+            L = prob["n"][2] * prob["cell"][2]
+            xw = W.wall_position(rows[:, 3], L)   # internal component 2 = user x
+            h = len(rows) // 2
+            v = np.polyfit(rows[h:, 0], xw[h:], 1)[0]
+            rec.update({"wall_x0_m": x0, "wall_x_end_m": float(xw[-1]), "wall_velocity_m_per_s": float(v)})
+        out.append(rec)
+        plan.close()
+    clocks = sampler.stop()
+    if rank == 0:
+        first = out[0]
+        line = {"metric": "cell-steps/s", "value": first["cell_steps_per_s"], "unit": "cell-steps/s",
+                "n_gpus": world, "steps": first["steps"], "warmup": 1, "ms_per_step": first["ms"] / first["steps"],
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic", "config": {"workload": first["workload"], "solver": "rk45", "maxerr": 1e-5,
+                                                "parallelism": f"replicas{world}"},
+                "runs": out, "clocks": clocks}
+        print(json.dumps(line), flush=True)
+
+
 # ---------------------------------------------------------------- main
 def main():
     ap = argparse.ArgumentParser()
@@ -469,9 +547,11 @@ def main():
     ap.add_argument("--profile-reps", type=int, default=10)
     ap.add_argument("--profile-only", action="store_true",
                     help="only time the passes of one field evaluation (few launches; for ncu captures)")
-    ap.add_argument("--workload", default="film3d", choices=["film3d", "ensemble", "relax"],
+    ap.add_argument("--workload", default="film3d", choices=["film3d", "ensemble", "relax", "sp4", "wall"],
                     help="film3d: the 256x256x16 RK23 film (default); ensemble: 2048 thermal simulations; "
-                         "relax: batched cold relaxations of 64x64x1 films")
+                         "relax: batched cold relaxations of 64x64x1 films; sp4: the 128x32x1 RK45 film; "
+                         "wall: Zhang-Li domain wall and Slonczewski disk")
+    ap.add_argument("--duration", type=float, default=0.0, help="sp4/wall: simulated time (s)")
     ap.add_argument("--relax-batch", type=int, default=256)
     ap.add_argument("--relax-maxerr", type=float, default=1e-6)
     ap.add_argument("--relax-max-steps", type=int, default=100000)
@@ -495,8 +575,9 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
-    if args.workload in ("ensemble", "relax"):
-        (ensemble_bench if args.workload == "ensemble" else relax_bench)(args, rank, world, local_rank, dist)
+    if args.workload in ("ensemble", "relax", "sp4", "wall"):
+        fn = {"ensemble": ensemble_bench, "relax": relax_bench, "sp4": single_bench, "wall": single_bench}
+        fn[args.workload](args, rank, world, local_rank, dist)
         if dist:
             dist.destroy_process_group()
         return
