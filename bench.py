@@ -374,6 +374,7 @@ def relax_bench(args, rank, world, local_rank, dist):
         plan.set_sims(bs)
         plan.solver("rk23", dt=1e-14, maxerr=args.relax_maxerr)
         thr = thr_all[j * B:(j + 1) * B]
+        step0 = [s["step"] for s in plan.batch_stats()]
         torch.cuda.synchronize()
         e0, e1 = events()
         e0.record()
@@ -385,7 +386,7 @@ def relax_bench(args, rank, world, local_rank, dist):
             continue
         sync_ms += e0.elapsed_time(e1)
         st = plan.batch_stats()
-        sync_steps += [s["step"] for s in st]
+        sync_steps += [s["step"] - s0 for s, s0 in zip(st, step0)]
         sync_conv += sum(1 for s, t in zip(st, thr) if s["maxtorque"] < t)
 
     # continuous batching over the same problems
