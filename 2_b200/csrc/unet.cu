@@ -1,0 +1,532 @@
+// unet.cu -- kernels of the learned warm start: a small convolutional U-Net in BF16 with
+// FP32 accumulation (forward, data gradient, weight gradient) and its optimiser.
+//
+// Activations are NHWC bf16 tensors addressed through channel views (pixel stride
+// `cs`, channel offset `co`), so a decoder's concatenated input is one buffer that the
+// encoder writes into and the upsampler fills.  Convolutions are 3x3, "same" padding.
+//
+// conv3x3_fwd: implicit GEMM, M = pixels, N = output channels, K = 9 taps x Cin, on the
+// BF16 tensor cores (mma.sync m16n8k16, FP32 accumulators), operands staged in shared
+// memory by cp.async (zero-filled outside the image) and fed by ldmatrix.  A block
+// computes 64 pixels x 64 channels with 4 warps of 32 x 32; K advances one
+// (tap, 16-channel) slice per stage, double-buffered.  The data gradient is the same
+// kernel on the flipped, transposed weights.
+// conv3x3_wgrad: dW[co][tap][ci] = sum_p dY[p][co] X[p + tap][ci], M = co, N = (tap, ci),
+// K = pixels, split over blocks and accumulated in FP32 with atomics.
+#include <cuda_bf16.h>
+#include <cstdint>
+
+#include "mm_internal.h"
+
+namespace mm {
+
+typedef __nv_bfloat16 bf16;
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+    return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, bool valid) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_u32(dst)), "l"(src),
+                 "r"(valid ? 16 : 0));
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+__device__ __forceinline__ void ldm_x4(unsigned (&r)[4], const void* p) {
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+                 : "r"(smem_u32(p)));
+}
+__device__ __forceinline__ void ldm_x4_t(unsigned (&r)[4], const void* p) {
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+                 : "r"(smem_u32(p)));
+}
+__device__ __forceinline__ void mma_bf16(float (&d)[4], const unsigned (&a)[4], unsigned b0, unsigned b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};\n"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// ---------------------------------------------------------------- forward / data gradient
+// out[p][co] = act(bias[co] + sum_{tap, ci} W[co][tap][ci] in[p + tap][ci])
+// Cin % 16 == 0; W rows hold Cout_w >= Cout rows (extra rows ignored); accumulate: add to out.
+#define FWD_BM 64
+#define FWD_BN 64
+#define FWD_PITCH 24  // bf16 per smem row (16 + 8: ldmatrix rows on distinct banks)
+
+__global__ void __launch_bounds__(128) conv3x3_fwd_kernel(const bf16* __restrict__ in, int in_cs, int in_co, int Cin,
+                                                          const bf16* __restrict__ W, const float* __restrict__ bias,
+                                                          bf16* __restrict__ out, int out_cs, int out_co, int Cout,
+                                                          int B, int H, int Wd, int relu) {
+    __shared__ __align__(128) bf16 sA[2][FWD_BM * FWD_PITCH];
+    __shared__ __align__(128) bf16 sB[2][FWD_BN * FWD_PITCH];
+    const long long P = (long long)B * H * Wd;
+    const long long p0 = (long long)blockIdx.x * FWD_BM;
+    const int n0 = blockIdx.y * FWD_BN;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int wm = (warp & 1) * 32, wn = (warp >> 1) * 32;
+    // loader roles: row r (pixel or output channel), 16-byte half h
+    const int lr = tid >> 1, lh = tid & 1;
+    const long long pr = p0 + lr;
+    int py = 0, px = 0, pb = 0;
+    if (pr < P) {
+        px = (int)(pr % Wd);
+        const long long t = pr / Wd;
+        py = (int)(t % H);
+        pb = (int)(t / H);
+    }
+    const int nslices = Cin / 16;
+    const int nk = 9 * nslices;
+    auto load = [&](int stage, int kk) {
+        const int tap = kk / nslices, cs = (kk % nslices) * 16;
+        const int dy = tap / 3 - 1, dx = tap % 3 - 1;
+        const int yy = py + dy, xx = px + dx;
+        const bool ok = pr < P && yy >= 0 && yy < H && xx >= 0 && xx < Wd;
+        const long long q = ok ? ((long long)pb * H + yy) * Wd + xx : 0;
+        cp_async16(&sA[stage][lr * FWD_PITCH + lh * 8], in + q * in_cs + in_co + cs + lh * 8, ok);
+        const int co = n0 + lr;
+        const bool okb = co < Cout;
+        cp_async16(&sB[stage][lr * FWD_PITCH + lh * 8],
+                   W + ((long long)(okb ? co : 0) * 9 + tap) * Cin + cs + lh * 8, okb);
+    };
+    float acc[2][4][4];
+#pragma unroll
+    for (int i = 0; i < 2; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+#pragma unroll
+            for (int q = 0; q < 4; q++) acc[i][j][q] = 0.f;
+    load(0, 0);
+    cp_commit();
+    for (int kk = 0; kk < nk; kk++) {
+        const int st = kk & 1;
+        if (kk + 1 < nk) load(st ^ 1, kk + 1);
+        cp_commit();
+        cp_wait<1>();
+        __syncthreads();
+        unsigned a[2][4], b[2][4];
+#pragma unroll
+        for (int i = 0; i < 2; i++)
+            ldm_x4(a[i], &sA[st][(wm + i * 16 + (lane & 15)) * FWD_PITCH + (lane >> 4) * 8]);
+#pragma unroll
+        for (int j = 0; j < 2; j++)
+            ldm_x4(b[j], &sB[st][(wn + j * 16 + (lane & 7) + ((lane >> 4) << 3)) * FWD_PITCH + ((lane >> 3) & 1) * 8]);
+#pragma unroll
+        for (int i = 0; i < 2; i++)
+#pragma unroll
+            for (int j = 0; j < 4; j++) mma_bf16(acc[i][j], a[i], b[j >> 1][(j & 1) * 2], b[j >> 1][(j & 1) * 2 + 1]);
+        __syncthreads();
+    }
+    // epilogue
+    const int g = lane >> 2, t4 = lane & 3;
+#pragma unroll
+    for (int i = 0; i < 2; i++)
+#pragma unroll
+        for (int hr = 0; hr < 2; hr++) {
+            const long long p = p0 + wm + i * 16 + g + hr * 8;
+            if (p >= P) continue;
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const int co = n0 + wn + j * 8 + t4 * 2;
+                if (co >= Cout) continue;
+                float v0 = acc[i][j][hr * 2], v1 = acc[i][j][hr * 2 + 1];
+                if (bias) {
+                    v0 += bias[co];
+                    if (co + 1 < Cout) v1 += bias[co + 1];
+                }
+                if (relu) {
+                    v0 = fmaxf(v0, 0.f);
+                    v1 = fmaxf(v1, 0.f);
+                }
+                bf16* o = out + p * out_cs + out_co + co;
+                if (co + 1 < Cout) {
+                    *reinterpret_cast<__nv_bfloat162*>(o) = __floats2bfloat162_rn(v0, v1);
+                } else {
+                    o[0] = __float2bfloat16_rn(v0);
+                }
+            }
+        }
+}
+
+// ---------------------------------------------------------------- weight gradient
+// dW[co][tap][ci] += sum_{p in this block's pixels} dY[p][co] X[p + tap][ci]  (FP32)
+#define WG_BM 64   // output channels
+#define WG_BN 64   // (tap, ci) columns
+#define WG_BK 32   // pixels per stage
+#define WG_PA 72   // bf16 per smem row of A (64 + 8)
+#define WG_PB 72
+
+__global__ void __launch_bounds__(128) conv3x3_wgrad_kernel(const bf16* __restrict__ dy, int dy_cs, int dy_co, int Cout,
+                                                            const bf16* __restrict__ x, int x_cs, int x_co, int Cin,
+                                                            float* __restrict__ dW, int B, int H, int Wd,
+                                                            long long pix_per_block) {
+    __shared__ __align__(128) bf16 sA[2][WG_BK * WG_PA];  // [pixel][co]
+    __shared__ __align__(128) bf16 sB[2][WG_BK * WG_PB];  // [pixel][(tap, ci)]
+    const long long P = (long long)B * H * Wd;
+    const int m0 = blockIdx.x * WG_BM;
+    const int n0 = blockIdx.y * WG_BN;
+    const int Ncols = 9 * Cin;
+    const long long pstart = (long long)blockIdx.z * pix_per_block;
+    const long long pend = pstart + pix_per_block < P ? pstart + pix_per_block : P;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int wm = (warp & 1) * 32, wn = (warp >> 1) * 32;
+    auto load = [&](int stage, long long pk) {
+        // A: 32 pixels x 64 channels = 256 chunks of 8 channels; 2 per thread
+#pragma unroll
+        for (int r = 0; r < 2; r++) {
+            const int c = tid + r * 128;
+            const int row = c >> 3, ch = (c & 7) * 8;
+            const long long p = pk + row;
+            const bool ok = p < pend && m0 + ch < Cout;
+            cp_async16(&sA[stage][row * WG_PA + ch], dy + (ok ? p : 0) * dy_cs + dy_co + (ok ? m0 + ch : 0), ok);
+        }
+        // B: 32 pixels x 64 (tap, ci) columns, 8 columns (one tap, 8 channels) per chunk
+#pragma unroll
+        for (int r = 0; r < 2; r++) {
+            const int c = tid + r * 128;
+            const int row = c >> 3, col = (c & 7) * 8;
+            const long long p = pk + row;
+            const int n = n0 + col;
+            bool ok = p < pend && n < Ncols;
+            long long q = 0;
+            int ci = 0;
+            if (ok) {
+                const int tap = n / Cin;
+                ci = n - tap * Cin;
+                const int xx0 = (int)(p % Wd);
+                const long long tt = p / Wd;
+                const int yy = (int)(tt % H) + tap / 3 - 1, xx = xx0 + tap % 3 - 1;
+                const int bb = (int)(tt / H);
+                ok = yy >= 0 && yy < H && xx >= 0 && xx < Wd;
+                q = ((long long)bb * H + yy) * Wd + xx;
+            }
+            cp_async16(&sB[stage][row * WG_PB + col], x + (ok ? q : 0) * x_cs + x_co + (ok ? ci : 0), ok);
+        }
+    };
+    float acc[2][4][4];
+#pragma unroll
+    for (int i = 0; i < 2; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+#pragma unroll
+            for (int q = 0; q < 4; q++) acc[i][j][q] = 0.f;
+    const long long nk = (pend - pstart + WG_BK - 1) / WG_BK;
+    if (nk <= 0) return;
+    load(0, pstart);
+    cp_commit();
+    for (long long kk = 0; kk < nk; kk++) {
+        const int st = (int)(kk & 1);
+        if (kk + 1 < nk) load(st ^ 1, pstart + (kk + 1) * WG_BK);
+        cp_commit();
+        cp_wait<1>();
+        __syncthreads();
+#pragma unroll
+        for (int ks = 0; ks < WG_BK; ks += 16) {
+            unsigned a[2][4], b[2][4];
+#pragma unroll
+            for (int i = 0; i < 2; i++)
+                ldm_x4_t(a[i], &sA[st][(ks + (lane & 7) + ((lane >> 4) << 3)) * WG_PA + wm + i * 16 +
+                                       ((lane >> 3) & 1) * 8]);
+#pragma unroll
+            for (int j = 0; j < 2; j++)
+                ldm_x4_t(b[j], &sB[st][(ks + (lane & 7) + (((lane >> 3) & 1) << 3)) * WG_PB + wn + j * 16 +
+                                       (lane >> 4) * 8]);
+#pragma unroll
+            for (int i = 0; i < 2; i++)
+#pragma unroll
+                for (int j = 0; j < 4; j++)
+                    mma_bf16(acc[i][j], a[i], b[j >> 1][(j & 1) * 2], b[j >> 1][(j & 1) * 2 + 1]);
+        }
+        __syncthreads();
+    }
+    const int g = lane >> 2, t4 = lane & 3;
+#pragma unroll
+    for (int i = 0; i < 2; i++)
+#pragma unroll
+        for (int hr = 0; hr < 2; hr++) {
+            const int co = m0 + wm + i * 16 + g + hr * 8;
+            if (co >= Cout) continue;
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const int n = n0 + wn + j * 8 + t4 * 2;
+                if (n < Ncols) atomicAdd(dW + (long long)co * Ncols + n, acc[i][j][hr * 2]);
+                if (n + 1 < Ncols) atomicAdd(dW + (long long)co * Ncols + n + 1, acc[i][j][hr * 2 + 1]);
+            }
+        }
+}
+
+// ---------------------------------------------------------------- elementwise pieces
+// 2x2 average pool: out (H/2 x W/2) <- in (H x W), channel views
+__global__ void pool_fwd_kernel(const bf16* in, int in_cs, int in_co, bf16* out, int out_cs, int out_co, int C, int B,
+                                int Ho, int Wo) {
+    const long long n = (long long)B * Ho * Wo * C;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+        const int c = (int)(e % C);
+        const long long p = e / C;
+        const int x = (int)(p % Wo);
+        const long long t = p / Wo;
+        const int y = (int)(t % Ho), b = (int)(t / Ho);
+        const int Wi = 2 * Wo, Hi = 2 * Ho;
+        float s = 0.f;
+        for (int i = 0; i < 2; i++)
+            for (int j = 0; j < 2; j++)
+                s += __bfloat162float(in[(((long long)b * Hi + 2 * y + i) * Wi + 2 * x + j) * in_cs + in_co + c]);
+        out[p * out_cs + out_co + c] = __float2bfloat16_rn(0.25f * s);
+    }
+}
+// gradient of the pool, added into din (the skip branch already wrote its part there)
+__global__ void pool_bwd_kernel(const bf16* dout, int do_cs, int do_co, bf16* din, int di_cs, int di_co, int C, int B,
+                                int Ho, int Wo) {
+    const long long n = (long long)B * (2 * Ho) * (2 * Wo) * C;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+        const int c = (int)(e % C);
+        const long long p = e / C;
+        const int Wi = 2 * Wo, Hi = 2 * Ho;
+        const int x = (int)(p % Wi);
+        const long long t = p / Wi;
+        const int y = (int)(t % Hi), b = (int)(t / Hi);
+        const float g = 0.25f * __bfloat162float(dout[(((long long)b * Ho + y / 2) * Wo + x / 2) * do_cs + do_co + c]);
+        bf16* d = din + p * di_cs + di_co + c;
+        *d = __float2bfloat16_rn(__bfloat162float(*d) + g);
+    }
+}
+// nearest 2x upsample: out (2H x 2W) <- in (H x W)
+__global__ void up_fwd_kernel(const bf16* in, int in_cs, int in_co, bf16* out, int out_cs, int out_co, int C, int B,
+                              int Hi, int Wi) {
+    const long long n = (long long)B * (2 * Hi) * (2 * Wi) * C;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+        const int c = (int)(e % C);
+        const long long p = e / C;
+        const int Wo = 2 * Wi, Ho = 2 * Hi;
+        const int x = (int)(p % Wo);
+        const long long t = p / Wo;
+        const int y = (int)(t % Ho), b = (int)(t / Ho);
+        out[p * out_cs + out_co + c] = in[(((long long)b * Hi + y / 2) * Wi + x / 2) * in_cs + in_co + c];
+    }
+}
+// gradient of the upsample: din (H x W) = sum of the 2x2 block of dout
+__global__ void up_bwd_kernel(const bf16* dout, int do_cs, int do_co, bf16* din, int di_cs, int di_co, int C, int B,
+                              int Hi, int Wi) {
+    const long long n = (long long)B * Hi * Wi * C;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+        const int c = (int)(e % C);
+        const long long p = e / C;
+        const int x = (int)(p % Wi);
+        const long long t = p / Wi;
+        const int y = (int)(t % Hi), b = (int)(t / Hi);
+        const int Wo = 2 * Wi, Ho = 2 * Hi;
+        float s = 0.f;
+        for (int i = 0; i < 2; i++)
+            for (int j = 0; j < 2; j++)
+                s += __bfloat162float(dout[(((long long)b * Ho + 2 * y + i) * Wo + 2 * x + j) * do_cs + do_co + c]);
+        din[p * di_cs + di_co + c] = __float2bfloat16_rn(s);
+    }
+}
+// dpre = dout * (out > 0) in place on the gradient view
+__global__ void relu_bwd_kernel(const bf16* out, int o_cs, int o_co, bf16* d, int d_cs, int d_co, int C, long long P) {
+    const long long n = P * C;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+        const int c = (int)(e % C);
+        const long long p = e / C;
+        if (!(__bfloat162float(out[p * o_cs + o_co + c]) > 0.f)) d[p * d_cs + d_co + c] = __float2bfloat16_rn(0.f);
+    }
+}
+// db[c] += sum_p d[p][c]
+__global__ void bias_grad_kernel(const bf16* d, int d_cs, int d_co, int C, long long P, float* db) {
+    const int c = blockIdx.y;
+    float s = 0.f;
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < P; p += (long long)gridDim.x * blockDim.x)
+        s += __bfloat162float(d[p * d_cs + d_co + c]);
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    __shared__ float sh[32];
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float t = 0.f;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += sh[w];
+        atomicAdd(db + c, t);
+    }
+}
+// masked mean-square error of the first 3 channels against a float target [P][3]:
+// loss += sum mask |out - target|^2 / norm ; dout = 2 mask (out - target) / norm
+__global__ void mse_kernel(const bf16* out, int o_cs, const float* target, const float* mask, long long P, float norm,
+                           bf16* dout, int d_cs, float* loss) {
+    float s = 0.f;
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < P; p += (long long)gridDim.x * blockDim.x) {
+        const float w = mask[p];
+        for (int c = 0; c < 3; c++) {
+            const float diff = __bfloat162float(out[p * o_cs + c]) - target[p * 3 + c];
+            s += w * diff * diff;
+            dout[p * d_cs + c] = __float2bfloat16_rn(2.f * w * diff / norm);
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    __shared__ float sh[32];
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float t = 0.f;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += sh[w];
+        atomicAdd(loss, t / norm);
+    }
+}
+// Adam (Kingma & Ba) on FP32 master weights; refreshes the bf16 copy
+__global__ void adam_kernel(float* w, const float* g, float* m, float* v, long long n, float lr, float b1, float b2,
+                            float eps, float c1, float c2, bf16* wb) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const float gi = g[i];
+        const float mi = b1 * m[i] + (1.f - b1) * gi;
+        const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+        m[i] = mi;
+        v[i] = vi;
+        const float wi = w[i] - lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+        w[i] = wi;
+        if (wb) wb[i] = __float2bfloat16_rn(wi);
+    }
+}
+// Wt[ci][tap'][co] = W[co][8 - tap'][ci] for the data gradient (rows padded to Cin_t >= Cout,
+// columns Coutp >= Cin)
+__global__ void flip_kernel(const bf16* W, int Cout, int Cin, bf16* Wt, int Cin_t, int Cout_t) {
+    const long long n = (long long)Cout_t * 9 * Cin_t;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+        const int co = (int)(e % Cin_t);          // column: the original output channel
+        const long long r = e / Cin_t;
+        const int tap = (int)(r % 9), ci = (int)(r / 9);
+        bf16 v = __float2bfloat16_rn(0.f);
+        if (co < Cout && ci < Cin) v = W[((long long)co * 9 + (8 - tap)) * Cin + ci];
+        Wt[e] = v;
+    }
+}
+// float -> bf16 into a channel view; in [P][C] float
+__global__ void to_bf16_kernel(const float* in, long long P, int C, bf16* out, int o_cs, int o_co) {
+    const long long n = P * C;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+        const int c = (int)(e % C);
+        const long long p = e / C;
+        out[p * o_cs + o_co + c] = __float2bfloat16_rn(in[e]);
+    }
+}
+
+// ---------------------------------------------------------------- C-ABI (host launchers)
+static int grid1(long long n) {
+    long long b = (n + 255) / 256;
+    if (b > 148 * 32) b = 148 * 32;
+    return (int)(b < 1 ? 1 : b);
+}
+
+}  // namespace mm
+
+using namespace mm;
+
+#define NN_CHECK()                                                                              \
+    do {                                                                                        \
+        cudaError_t e_ = cudaGetLastError();                                                    \
+        if (e_ != cudaSuccess) return report_error(MM_ERR_CUDA, cudaGetErrorString(e_));        \
+    } while (0)
+
+extern "C" MM_API int mm_nn_conv3x3(const void* in, int in_cs, int in_co, int Cin, const void* W, const float* bias,
+                                    void* out, int out_cs, int out_co, int Cout, int B, int H, int Wd, int relu,
+                                    mm_stream st) {
+    if (Cin % 16 || in_cs % 8 || in_co % 8 || Cout < 1 || B < 1 || H < 1 || Wd < 1 || (out_co & 1) || (out_cs & 1))
+        return report_error(MM_ERR_ARG, "mm_nn_conv3x3: Cin, channel stride and offset must be multiples of 16/8/8");
+    const long long P = (long long)B * H * Wd;
+    dim3 grid((unsigned)((P + FWD_BM - 1) / FWD_BM), (unsigned)((Cout + FWD_BN - 1) / FWD_BN));
+    conv3x3_fwd_kernel<<<grid, 128, 0, (cudaStream_t)st>>>((const bf16*)in, in_cs, in_co, Cin, (const bf16*)W, bias,
+                                                           (bf16*)out, out_cs, out_co, Cout, B, H, Wd, relu);
+    NN_CHECK();
+    return MM_OK;
+}
+
+extern "C" MM_API int mm_nn_conv3x3_wgrad(const void* dy, int dy_cs, int dy_co, int Cout, const void* x, int x_cs,
+                                          int x_co, int Cin, float* dW, int B, int H, int Wd, mm_stream st) {
+    if (Cin % 8 || Cout % 8 || dy_cs % 8 || dy_co % 8 || x_cs % 8 || x_co % 8)
+        return report_error(MM_ERR_ARG, "mm_nn_conv3x3_wgrad: channel counts, strides and offsets must be multiples of 8");
+    const long long P = (long long)B * H * Wd;
+    const int mt = (Cout + WG_BM - 1) / WG_BM, nt = (9 * Cin + WG_BN - 1) / WG_BN;
+    // split the pixels so that about 4 waves of blocks cover the GPU
+    long long splits = (148LL * 4 * 4 + mt * nt - 1) / (mt * nt);
+    long long ppb = (P + splits - 1) / splits;
+    ppb = ((ppb + WG_BK - 1) / WG_BK) * WG_BK;
+    if (ppb < 4 * WG_BK) ppb = 4 * WG_BK;
+    splits = (P + ppb - 1) / ppb;
+    dim3 grid((unsigned)mt, (unsigned)nt, (unsigned)splits);
+    conv3x3_wgrad_kernel<<<grid, 128, 0, (cudaStream_t)st>>>((const bf16*)dy, dy_cs, dy_co, Cout, (const bf16*)x, x_cs,
+                                                             x_co, Cin, dW, B, H, Wd, ppb);
+    NN_CHECK();
+    return MM_OK;
+}
+
+extern "C" MM_API int mm_nn_pool(const void* in, int in_cs, int in_co, void* out, int out_cs, int out_co, int C, int B,
+                                 int Ho, int Wo, int backward, mm_stream st) {
+    const long long n = (long long)B * Ho * Wo * C * (backward ? 4 : 1);
+    if (backward)
+        pool_bwd_kernel<<<grid1(n), 256, 0, (cudaStream_t)st>>>((const bf16*)in, in_cs, in_co, (bf16*)out, out_cs,
+                                                                 out_co, C, B, Ho, Wo);
+    else
+        pool_fwd_kernel<<<grid1(n), 256, 0, (cudaStream_t)st>>>((const bf16*)in, in_cs, in_co, (bf16*)out, out_cs,
+                                                                 out_co, C, B, Ho, Wo);
+    NN_CHECK();
+    return MM_OK;
+}
+
+extern "C" MM_API int mm_nn_upsample(const void* in, int in_cs, int in_co, void* out, int out_cs, int out_co, int C,
+                                     int B, int Hi, int Wi, int backward, mm_stream st) {
+    const long long n = (long long)B * Hi * Wi * C * (backward ? 1 : 4);
+    if (backward)
+        up_bwd_kernel<<<grid1(n), 256, 0, (cudaStream_t)st>>>((const bf16*)in, in_cs, in_co, (bf16*)out, out_cs, out_co,
+                                                               C, B, Hi, Wi);
+    else
+        up_fwd_kernel<<<grid1(n), 256, 0, (cudaStream_t)st>>>((const bf16*)in, in_cs, in_co, (bf16*)out, out_cs, out_co,
+                                                               C, B, Hi, Wi);
+    NN_CHECK();
+    return MM_OK;
+}
+
+extern "C" MM_API int mm_nn_relu_bwd(const void* out, int o_cs, int o_co, void* d, int d_cs, int d_co, int C,
+                                     long long P, mm_stream st) {
+    relu_bwd_kernel<<<grid1(P * C), 256, 0, (cudaStream_t)st>>>((const bf16*)out, o_cs, o_co, (bf16*)d, d_cs, d_co, C, P);
+    NN_CHECK();
+    return MM_OK;
+}
+
+extern "C" MM_API int mm_nn_bias_grad(const void* d, int d_cs, int d_co, int C, long long P, float* db, mm_stream st) {
+    long long b = (P + 255) / 256;
+    if (b > 64) b = 64;
+    bias_grad_kernel<<<dim3((unsigned)b, (unsigned)C), 256, 0, (cudaStream_t)st>>>((const bf16*)d, d_cs, d_co, C, P, db);
+    NN_CHECK();
+    return MM_OK;
+}
+
+extern "C" MM_API int mm_nn_mse(const void* out, int o_cs, const float* target, const float* mask, long long P,
+                                float norm, void* dout, int d_cs, float* loss, mm_stream st) {
+    mse_kernel<<<grid1(P), 256, 0, (cudaStream_t)st>>>((const bf16*)out, o_cs, target, mask, P, norm, (bf16*)dout, d_cs,
+                                                       loss);
+    NN_CHECK();
+    return MM_OK;
+}
+
+extern "C" MM_API int mm_nn_adam(float* w, const float* g, float* m, float* v, long long n, float lr, float b1,
+                                 float b2, float eps, int t, void* wb, mm_stream st) {
+    const float c1 = 1.f - powf(b1, (float)t), c2 = 1.f - powf(b2, (float)t);
+    adam_kernel<<<grid1(n), 256, 0, (cudaStream_t)st>>>(w, g, m, v, n, lr, b1, b2, eps, c1, c2, (bf16*)wb);
+    NN_CHECK();
+    return MM_OK;
+}
+
+extern "C" MM_API int mm_nn_flip(const void* W, int Cout, int Cin, void* Wt, int Cin_t, int Cout_t, mm_stream st) {
+    flip_kernel<<<grid1((long long)Cout_t * 9 * Cin_t), 256, 0, (cudaStream_t)st>>>((const bf16*)W, Cout, Cin, (bf16*)Wt,
+                                                                                      Cin_t, Cout_t);
+    NN_CHECK();
+    return MM_OK;
+}
+
+extern "C" MM_API int mm_nn_to_bf16(const float* in, long long P, int C, void* out, int o_cs, int o_co, mm_stream st) {
+    to_bf16_kernel<<<grid1(P * C), 256, 0, (cudaStream_t)st>>>(in, P, C, (bf16*)out, o_cs, o_co);
+    NN_CHECK();
+    return MM_OK;
+}

@@ -271,6 +271,34 @@ MM_API uint64_t mm_crc64_iso(const void* data, size_t n);
 MM_API int mm_save_async(mm_plan plan, const char* path, int format, mm_stream stream);
 MM_API int mm_save_wait(mm_plan plan);
 
+/* ---- learned warm start: BF16 U-Net kernels (no counterpart in the reference) ----
+ * NHWC bf16 tensors addressed as channel views (pixel stride cs, channel offset co);
+ * FP32 accumulation; pointers are device pointers.  conv3x3: out = act(bias + W * in),
+ * W [Cout][9][Cin] bf16, Cin % 16 == 0 (relu 0/1, bias may be NULL).  wgrad: dW[Cout][9][Cin]
+ * += sum over pixels (FP32, atomics).  pool: 2x2 average (backward adds into the input
+ * gradient); upsample: nearest 2x (backward sums); relu_bwd zeroes d where out <= 0;
+ * mse: masked mean-square error of the first three channels against a float target
+ * [P][3] (loss accumulated, gradient written); adam: one Adam step on FP32 master
+ * weights with a bf16 copy; flip: the transposed, tap-reversed weights of the data
+ * gradient. */
+MM_API int mm_nn_conv3x3(const void* in, int in_cs, int in_co, int Cin, const void* W, const float* bias, void* out,
+                         int out_cs, int out_co, int Cout, int B, int H, int Wd, int relu, mm_stream st);
+MM_API int mm_nn_conv3x3_wgrad(const void* dy, int dy_cs, int dy_co, int Cout, const void* x, int x_cs, int x_co,
+                               int Cin, float* dW, int B, int H, int Wd, mm_stream st);
+MM_API int mm_nn_pool(const void* in, int in_cs, int in_co, void* out, int out_cs, int out_co, int C, int B, int Ho,
+                      int Wo, int backward, mm_stream st);
+MM_API int mm_nn_upsample(const void* in, int in_cs, int in_co, void* out, int out_cs, int out_co, int C, int B,
+                          int Hi, int Wi, int backward, mm_stream st);
+MM_API int mm_nn_relu_bwd(const void* out, int o_cs, int o_co, void* d, int d_cs, int d_co, int C, long long P,
+                          mm_stream st);
+MM_API int mm_nn_bias_grad(const void* d, int d_cs, int d_co, int C, long long P, float* db, mm_stream st);
+MM_API int mm_nn_mse(const void* out, int o_cs, const float* target, const float* mask, long long P, float norm,
+                     void* dout, int d_cs, float* loss, mm_stream st);
+MM_API int mm_nn_adam(float* w, const float* g, float* m, float* v, long long n, float lr, float b1, float b2,
+                      float eps, int t, void* wb, mm_stream st);
+MM_API int mm_nn_flip(const void* W, int Cout, int Cin, void* Wt, int Cin_t, int Cout_t, mm_stream st);
+MM_API int mm_nn_to_bf16(const float* in, long long P, int C, void* out, int o_cs, int o_co, mm_stream st);
+
 /* ---- instrumentation ---- */
 /* Kernels this plan has enqueued so far (graph replays counted per kernel node). */
 MM_API long long mm_plan_launch_count(mm_plan plan);

@@ -1,0 +1,123 @@
+"""BF16 tensor-core kernels of the warm-start U-Net against the numpy oracle
+(oracle/unet_ref.py, float64 with bf16 rounding where the GPU stores bf16).
+
+Tolerances: a convolution output may differ from the oracle by one bf16 rounding step
+(2^-8 relative) because the FP32 sums run in another order; weight gradients (FP32
+accumulation of bf16 products) agree to 1e-3 relative in norm; the gradients of the whole
+network, where a flipped rounding of an activation propagates, to 3e-2.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _dev(a, dtype):
+    import torch
+    return torch.tensor(np.asarray(a, dtype=np.float32), device="cuda").to(dtype).reshape(-1).contiguous()
+
+
+def _p(t):
+    return C.c_void_p(t.data_ptr())
+
+
+def _relnorm(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30))
+
+
+@pytest.mark.parametrize("cin,cout,B,H,W,relu", [(16, 32, 2, 8, 8, 1), (64, 128, 1, 16, 16, 0), (96, 32, 2, 8, 16, 1),
+                                                 (32, 16, 1, 4, 4, 0)])
+def test_conv3x3_forward_and_data_gradient(cin, cout, B, H, W, relu):
+    import torch
+    import unet_ref as R
+    from mumax2 import _native as nat
+    rng = np.random.default_rng(cin + cout)
+    x = R.bf16(rng.normal(size=(B, H, W, cin)))
+    w = R.bf16(rng.normal(size=(cout, 9, cin)) / np.sqrt(9 * cin))
+    b = rng.normal(size=cout).astype(np.float32)
+    xd, wd = _dev(x, torch.bfloat16), _dev(w, torch.bfloat16)
+    bd = torch.tensor(b, device="cuda")
+    out = torch.zeros(B * H * W * cout, dtype=torch.bfloat16, device="cuda")
+    nat.check(nat.lib().mm_nn_conv3x3(_p(xd), cin, 0, cin, _p(wd), _p(bd), _p(out), cout, 0, cout, B, H, W, relu,
+                                      None))
+    ref = R.conv3x3(x, w, b)
+    if relu:
+        ref = np.maximum(ref, 0)
+    got = out.float().cpu().numpy().reshape(ref.shape)
+    assert np.abs(got - ref).max() <= 2 ** -7 * np.abs(ref).max() + 1e-6
+    # data gradient through the flipped weights
+    dy = R.bf16(rng.normal(size=(B, H, W, cout)))
+    dyd = _dev(dy, torch.bfloat16)
+    cin_t = ((cout + 15) // 16) * 16
+    wt = torch.zeros(cin * 9 * cin_t, dtype=torch.bfloat16, device="cuda")
+    nat.check(nat.lib().mm_nn_flip(_p(wd), cout, cin, _p(wt), cin_t, cin, None))
+    dx = torch.zeros(B * H * W * cin, dtype=torch.bfloat16, device="cuda")
+    nat.check(nat.lib().mm_nn_conv3x3(_p(dyd), cout, 0, cin_t, _p(wt), None, _p(dx), cin, 0, cin, B, H, W, 0, None))
+    rdx, rdw, rdb = R.conv3x3_backward(x, w, dy)
+    gdx = dx.float().cpu().numpy().reshape(rdx.shape)
+    assert np.abs(gdx - rdx).max() <= 2 ** -7 * np.abs(rdx).max() + 1e-6
+    # weight and bias gradients
+    dw = torch.zeros(cout * 9 * cin, dtype=torch.float32, device="cuda")
+    db = torch.zeros(cout, dtype=torch.float32, device="cuda")
+    nat.check(nat.lib().mm_nn_conv3x3_wgrad(_p(dyd), cout, 0, cout, _p(xd), cin, 0, cin, _p(dw), B, H, W, None))
+    nat.check(nat.lib().mm_nn_bias_grad(_p(dyd), cout, 0, cout, B * H * W, _p(db), None))
+    assert _relnorm(dw.cpu().numpy().reshape(rdw.shape), rdw) < 1e-3
+    assert _relnorm(db.cpu().numpy(), rdb) < 1e-3
+
+
+def test_network_gradients_match_oracle():
+    import unet_ref as R
+    from mumax2 import unet as U
+    B, H, W = 2, 16, 16
+    rng = np.random.default_rng(7)
+    params = U.init_params(seed=3)
+    for name in params:   # non-zero biases exercise the bias paths
+        w, b = params[name]
+        params[name] = (w, (0.05 * rng.normal(size=b.shape)).astype(np.float32))
+    feats = np.zeros((B, H * W, U.FEAT), dtype=np.float32)
+    feats[..., :9] = rng.normal(size=(B, H * W, 9))
+    target = rng.normal(size=(B, H * W, 3)).astype(np.float32)
+    mask = (rng.uniform(size=(B, H * W)) > 0.2).astype(np.float32)
+    net = U.UNet(B, H, W, params=params)
+    net.set_input(feats)
+    net.forward()
+    net.set_target(target, mask)
+    loss = float(net.loss_and_grad().item())
+    net.backward()
+    arch = (U.BUFFERS, U.CONVS, U.POOLS, U.UPS, U.SCHEDULE)
+    rloss, rgrads, rout = R.forward_backward(arch, params, feats, target, mask, H, W)
+    assert loss == pytest.approx(rloss, rel=1e-2)
+    errs = {}
+    for name, (dw, db) in rgrads.items():
+        d = net.p[name]
+        errs[name] = _relnorm(d["gw"].cpu().numpy().reshape(dw.shape), dw)
+    print(errs)
+    assert max(errs.values()) < 3e-2
+
+
+def test_training_lowers_the_loss():
+    """A few Adam steps on a fixed batch fit a smooth target."""
+    from mumax2 import unet as U
+    B, H, W = 4, 16, 16
+    rng = np.random.default_rng(1)
+    feats = np.zeros((B, H * W, U.FEAT), dtype=np.float32)
+    feats[..., 0] = 1.0
+    feats[..., 6:8] = rng.normal(size=(B, 1, 2))
+    feats[..., 8] = 1.0
+    target = np.zeros((B, H * W, 3), dtype=np.float32)
+    target[..., 0] = np.cos(feats[..., 6])
+    target[..., 1] = np.sin(feats[..., 6])
+    mask = np.ones((B, H * W), dtype=np.float32)
+    net = U.UNet(B, H, W, seed=0)
+    net.set_input(feats)
+    net.set_target(target, mask)
+    losses = []
+    for _ in range(60):
+        net.forward()
+        losses.append(float(net.loss_and_grad().item()))
+        net.backward()
+        net.adam(lr=3e-3)
+    print(losses[0], losses[-1])
+    assert losses[-1] < 0.2 * losses[0]
