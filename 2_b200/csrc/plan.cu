@@ -2103,7 +2103,8 @@ extern "C" MM_API int mm_save_async(mm_plan p, const char* path, int format, mm_
 // while the others keep their state, so the GPU never waits for a batch's slowest member.
 
 extern "C" MM_API int mm_batch_restart(mm_plan p, int count, const int* idx, const float* m, int from_host,
-                                       const mm_sim* sims, const double* thr, mm_stream stream) {
+                                       const mm_sim* sims, const double* thr, long long max_steps,
+                                       mm_stream stream) {
     if (!p || count < 0 || (count > 0 && (!idx || !m || !thr))) return set_err(MM_ERR_ARG, "bad argument");
     if (p->solver < 0) return set_err(MM_ERR_STATE, "no solver: call mm_solver_init");
     cudaStream_t st = (cudaStream_t)stream;
@@ -2143,7 +2144,7 @@ extern "C" MM_API int mm_batch_restart(mm_plan p, int count, const int* idx, con
         c.h = c.dt * c.gamma;
         c.dt_thermal = keep.dt_thermal;
         c.t_end = 1e300;
-        c.step_end = (1LL << 62);
+        c.step_end = max_steps > 0 ? max_steps : (1LL << 62);
         c.torque_thr = thr[k];
         c.am_abs_err = keep.am_abs_err;
         c.am_rel_err = keep.am_rel_err;

@@ -201,7 +201,7 @@ _PROTOS = {
     "mm_batch_set_sims": (C.c_int, [C.c_void_p, C.c_void_p]),
     "mm_batch_stats": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "mm_batch_restart": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
-                                    C.c_void_p]),
+                                    C.c_longlong, C.c_void_p]),
     "mm_batch_drive": (C.c_int, [C.c_void_p, C.c_int, C.c_longlong, C.c_void_p]),
     "mm_batch_run_until_maxtorque": (C.c_int, [C.c_void_p, C.c_void_p, C.c_longlong, C.c_void_p]),
     "mm_batch_maxtorque": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),

@@ -252,7 +252,7 @@ class Plan:
         nat.check(nat.lib().mm_batch_run_until_maxtorque(self.h, self._thr.ctypes.data_as(C.c_void_p),
                                                          int(max_steps), None))
 
-    def batch_restart(self, idx, m, thr, sims=None):
+    def batch_restart(self, idx, m, thr, sims=None, max_steps=0):
         """Put new problems into slots idx (continuous batching): states m [k][3N] (host),
         torque thresholds thr [k], optional scalar dicts sims [k].  Per-simulation masks
         are updated by writing into this plan's mask tensors before the call."""
@@ -263,7 +263,7 @@ class Plan:
         nat.check(nat.lib().mm_batch_restart(self.h, len(idx), idx.ctypes.data_as(C.c_void_p),
                                              m.ctypes.data_as(C.c_void_p), 1,
                                              C.cast(sa, C.c_void_p) if sa is not None else None,
-                                             thr.ctypes.data_as(C.c_void_p), None))
+                                             thr.ctypes.data_as(C.c_void_p), int(max_steps), None))
 
     def batch_drive(self, target_active=0, max_attempts=0):
         """Step until at most target_active simulations are still running."""

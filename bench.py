@@ -537,6 +537,45 @@ def single_bench(args, rank, world, local_rank, dist):
         print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------- learned warm start
+def warmstart_bench(args, rank, world, local_rank, dist):
+    """relaxed states of --train problems (plain relax from the cold start,
+    continuous batching) train the BF16 U-Net on the GPU; on --nsim held-out problems the
+    warm start (network inference + relax) is timed against the cold relax.  value =
+    warm relaxations/s (fallbacks to the cold start included)."""
+    import torch
+    from mumax2 import unet as U
+    from mumax2 import warmstart as WS
+    t0 = time.perf_counter()
+    problem, sims, masks, res = WS.generate(args.train, seed=1000 + rank, device=local_rank)
+    t_gen = time.perf_counter() - t0
+    data = WS.Dataset(problem, sims, masks, res["state"], device=local_rank)
+    t0 = time.perf_counter()
+    net, losses = WS.train(data, epochs=args.epochs, batch=256, lr=2e-3, device=local_rank)
+    torch.cuda.synchronize()
+    t_train = time.perf_counter() - t0
+    steps_per_epoch = len(data) // 256
+    flops = 3 * U.conv_flops(64, 64) * 256 * steps_per_epoch * args.epochs
+    _, hs, hm = __import__("mumax2.workloads", fromlist=["relax_set"]).relax_set(args.nsim, seed=5000 + rank)
+    ev = WS.evaluate(net, problem, hs, hm, device=local_rank)
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    peak = float(json.load(open(peaks_path))["bf16_tflops_sustained"]) if os.path.exists(peaks_path) else 1400.0
+    if rank == 0:
+        line = {"metric": "relaxations/s", "value": ev["warm_per_s"], "unit": "relaxations/s", "n_gpus": world,
+                "steps": ev["relaxations"], "warmup": 0, "ms_per_step": 1e3 / ev["warm_per_s"],
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "bf16+f32",
+                "data": "synthetic",
+                "config": {"workload": "relax_64x64x1_warm_start", "held_out": args.nsim, "train": args.train,
+                           "epochs": args.epochs, "net": "U-Net 4 levels, 32/64/128/256 channels, 3x3, bf16",
+                           "parallelism": f"replicas{world}"},
+                "warm_vs_cold": ev,
+                "training": {"generate_s": t_gen, "train_s": t_train, "loss_first_epoch": losses[0],
+                             "loss_last_epoch": losses[-1],
+                             "tflops_achieved": flops / t_train / 1e12, "tflops_peak_sustained": peak,
+                             "frac": flops / t_train / 1e12 / peak}}
+        print(json.dumps(line), flush=True)
+
+
 # ---------------------------------------------------------------- main
 def main():
     ap = argparse.ArgumentParser()
@@ -548,15 +587,19 @@ def main():
     ap.add_argument("--profile-reps", type=int, default=10)
     ap.add_argument("--profile-only", action="store_true",
                     help="only time the passes of one field evaluation (few launches; for ncu captures)")
-    ap.add_argument("--workload", default="film3d", choices=["film3d", "ensemble", "relax", "sp4", "wall"],
+    ap.add_argument("--workload", default="film3d",
+                    choices=["film3d", "ensemble", "relax", "sp4", "wall", "warmstart"],
                     help="film3d: the 256x256x16 RK23 film (default); ensemble: 2048 thermal simulations; "
                          "relax: batched cold relaxations of 64x64x1 films; sp4: the 128x32x1 RK45 film; "
-                         "wall: Zhang-Li domain wall and Slonczewski disk")
+                         "wall: Zhang-Li domain wall and Slonczewski disk; warmstart: the learned warm start")
+    ap.add_argument("--train", type=int, default=20000, help="warmstart: training relaxations")
+    ap.add_argument("--epochs", type=int, default=20, help="warmstart: training epochs")
     ap.add_argument("--duration", type=float, default=0.0, help="sp4/wall: simulated time (s)")
     ap.add_argument("--relax-batch", type=int, default=256)
     ap.add_argument("--relax-maxerr", type=float, default=1e-6)
     ap.add_argument("--relax-max-steps", type=int, default=100000)
-    ap.add_argument("--nsim", type=int, default=2048, help="ensemble: number of simulations")
+    ap.add_argument("--nsim", type=int, default=0,
+                    help="ensemble: simulations (2048); relax: relaxations (2048); warmstart: held-out problems (4096)")
     ap.add_argument("--ens-attempts", type=int, default=50, help="ensemble: attempts per graph launch")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -576,8 +619,11 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
-    if args.workload in ("ensemble", "relax", "sp4", "wall"):
-        fn = {"ensemble": ensemble_bench, "relax": relax_bench, "sp4": single_bench, "wall": single_bench}
+    if args.workload in ("ensemble", "relax", "sp4", "wall", "warmstart"):
+        fn = {"ensemble": ensemble_bench, "relax": relax_bench, "sp4": single_bench, "wall": single_bench,
+              "warmstart": warmstart_bench}
+        if not args.nsim:
+            args.nsim = 4096 if args.workload == "warmstart" else 2048
         fn[args.workload](args, rank, world, local_rank, dist)
         if dist:
             dist.destroy_process_group()

@@ -228,11 +228,12 @@ MM_API int mm_autosave_read(mm_plan plan, float* states, double* times, int* cou
  * mm_batch_restart puts new problems into `count` slots idx[] of a batched plan: state
  * m[count][3N] (host if from_host, else device), scalars sims[count] (NULL: keep the
  * slot's), torque thresholds thr[count]; the slots restart at t = 0 with the solver's
- * initial dt while the other slots keep their state.  Per-simulation masks are the
+ * initial dt while the other slots keep their state; a slot stops after max_steps steps
+ * (0: no limit) whether or not it reached its threshold.  Per-simulation masks are the
  * caller's device arrays: write the new slot's values before this call.
  * mm_batch_drive steps until at most target_active simulations are still running. */
 MM_API int mm_batch_restart(mm_plan plan, int count, const int* idx, const float* m, int from_host,
-                            const mm_sim* sims, const double* thr, mm_stream stream);
+                            const mm_sim* sims, const double* thr, long long max_steps, mm_stream stream);
 MM_API int mm_batch_drive(mm_plan plan, int target_active, long long max_attempts, mm_stream stream);
 
 /* ---- per-simulation results of a (batched) plan; out arrays have nsim entries ---- */
