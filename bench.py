@@ -546,6 +546,7 @@ def warmstart_bench(args, rank, world, local_rank, dist):
     import torch
     from mumax2 import unet as U
     from mumax2 import warmstart as WS
+    from mumax2 import workloads as W
     t0 = time.perf_counter()
     problem, sims, masks, res = WS.generate(args.train, seed=1000 + rank, device=local_rank)
     t_gen = time.perf_counter() - t0
@@ -556,7 +557,7 @@ def warmstart_bench(args, rank, world, local_rank, dist):
     t_train = time.perf_counter() - t0
     steps_per_epoch = len(data) // 256
     flops = 3 * U.conv_flops(64, 64) * 256 * steps_per_epoch * args.epochs
-    _, hs, hm = __import__("mumax2.workloads", fromlist=["relax_set"]).relax_set(args.nsim, seed=5000 + rank)
+    _, hs, hm = W.relax_set(args.nsim, seed=5000 + rank)
     ev = WS.evaluate(net, problem, hs, hm, device=local_rank)
     peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     peak = float(json.load(open(peaks_path))["bf16_tflops_sustained"]) if os.path.exists(peaks_path) else 1400.0
