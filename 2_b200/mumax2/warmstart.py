@@ -111,8 +111,8 @@ def generate(nsim, seed, slots=256, device=0):
     return problem, sims, masks, res
 
 
-def train(data, epochs=20, batch=256, lr=2e-3, seed=0, device=0, log=None):
-    """Adam with a cosine learning-rate decay; returns (net, losses per epoch)."""
+def train(data, epochs=20, batch=256, lr=1e-3, seed=0, device=0, log=None):
+    """Adam with a short linear warm-up and a cosine decay; returns (net, losses per epoch)."""
     import torch
     H, Wd = data.n[1], data.n[2]
     net = U.UNet(batch, H, Wd, device=device, seed=seed)
@@ -131,7 +131,8 @@ def train(data, epochs=20, batch=256, lr=2e-3, seed=0, device=0, log=None):
             net.set_target(data.targets[idx], data.masks[idx])
             acc += net.loss_and_grad()[0]
             net.backward()
-            net.adam(lr=lr * 0.5 * (1 + np.cos(np.pi * k / total)))
+            warm = min(1.0, (k + 1) / max(1, total // 20))
+            net.adam(lr=lr * warm * 0.5 * (1 + np.cos(np.pi * k / total)))
             k += 1
         losses.append(float(acc.item()) / nb)
         if log:
@@ -140,19 +141,53 @@ def train(data, epochs=20, batch=256, lr=2e-3, seed=0, device=0, log=None):
 
 
 def predict(net, sims, masks, n):
-    """Initial states (internal SoA, normalised, masked) for the problems, net.B per launch."""
+    """Initial states (internal SoA, normalised, masked) for the problems, net.B per launch;
+    the features are built once and kept on the GPU."""
+    import torch
     B = net.B
+    feats = torch.tensor(U.features(sims, masks, n), device=net.device)
+    if len(sims) % B:
+        pad = torch.zeros((B - len(sims) % B,) + tuple(feats.shape[1:]), device=net.device)
+        feats = torch.cat([feats, pad])
     out = []
     for i in range(0, len(sims), B):
-        s, m = sims[i:i + B], masks[i:i + B]
-        f = U.features(s, m, n)
-        if len(s) < B:
-            f = np.concatenate([f, np.zeros((B - len(s),) + f.shape[1:], dtype=np.float32)])
-        net.set_input(f)
+        net.set_input(feats[i:i + B])
         net.forward()
-        o = net.output3()[:len(s)]
-        out.append(U.state_from_output(o, np.stack(m)))
+        o = net.output3()[:min(B, len(sims) - i)]
+        out.append(U.state_from_output(o, np.stack(masks[i:i + B])))
     return np.concatenate(out)
+
+
+def choose_starts(problem, sims, masks, candidates, slots=256, device=0, plan=None):
+    """Per problem, the candidate start of lowest energy (the judge of a predicted start:
+    a prediction above the cold start's energy is not used).  candidates: list of
+    [nq][3N] arrays; returns (states, index of the chosen candidate per problem)."""
+    from .plan import Plan
+    import torch
+    n = problem["n"]
+    N = int(np.prod(n))
+    nq = len(sims)
+    B = min(slots, nq)
+    own = plan is None
+    if own:
+        plan = Plan(problem, masks={"msat": np.concatenate(masks[:B])}, sims=sims[:B], masks_per_sim=True,
+                    device=device)
+    mt = plan.mask_tensor("msat")
+    energies = np.zeros((len(candidates), nq))
+    for i in range(0, nq, B):
+        k = min(B, nq - i)
+        mt[:k * N].copy_(torch.from_numpy(np.concatenate(masks[i:i + k])))
+        plan.set_sims(sims[i:i + k] + sims[i:i + 1] * (plan.nsim - k))
+        for c, cand in enumerate(candidates):
+            st = np.zeros((plan.nsim, 3 * N), dtype=np.float32)
+            st[:k] = cand[i:i + k]
+            plan.set_state(st.ravel())
+            energies[c, i:i + k] = plan.batch_energy()[:k, 4]
+    if own:
+        plan.close()
+    pick = np.argmin(energies, axis=0)
+    states = np.stack([candidates[pick[q]][q] for q in range(nq)])
+    return states, pick
 
 
 def evaluate(net, problem, sims, masks, slots=256, device=0, energy_tol=1e-4, max_steps=20000):
@@ -174,7 +209,9 @@ def evaluate(net, problem, sims, masks, slots=256, device=0, energy_tol=1e-4, ma
     torch.cuda.synchronize()
     t_cold = time.perf_counter() - t0
     t0 = time.perf_counter()
-    init = predict(net, sims, masks, n)
+    pred = predict(net, sims, masks, n)
+    init, pick = choose_starts(problem, sims, masks, [pred, np.repeat(cold[None, :], len(sims), axis=0)],
+                               slots=slots, device=device, plan=plan)
     torch.cuda.synchronize()
     t_inf = time.perf_counter() - t0
     rw = relax_pool(problem, sims, masks, list(init), thr, slots=slots, device=device, max_steps=max_steps,
@@ -199,7 +236,8 @@ def evaluate(net, problem, sims, masks, slots=256, device=0, energy_tol=1e-4, ma
         "speedup": t_cold / (t_warm + t_fb),
         "cold_steps_mean": float(rc["steps"].mean()), "warm_steps_mean": float(rw["steps"].mean()),
         "steps_saved_frac": float(1 - rw["steps"].sum() / max(1, rc["steps"].sum())),
-        "inference_s": t_inf, "warm_ok_frac": float(ok.mean()), "fallbacks": int(len(fail)),
+        "inference_s": t_inf, "predicted_start_used_frac": float((pick == 0).mean()),
+        "warm_ok_frac": float(ok.mean()), "fallbacks": int(len(fail)),
         "energy_within_tol_frac": float((erel <= energy_tol).mean()),
         "energy_rel_median": float(np.median(erel)),
         "warm_lower_energy_frac": float((rw["energy"] < rc["energy"]).mean()),
