@@ -530,3 +530,223 @@ extern "C" MM_API int mm_nn_to_bf16(const float* in, long long P, int C, void* o
     NN_CHECK();
     return MM_OK;
 }
+
+// ---------------------------------------------------------------- tcgen05 forward convolution
+// The same implicit GEMM on the 5th-generation tensor cores: D[128 pixels][N] in TMEM
+// (FP32), A = pixel rows x (tap, channel) and B = output channels x (tap, channel), both
+// K-major bf16 in shared memory in the canonical no-swizzle layout (8-row x 16-byte core
+// matrices; K-adjacent core matrices 128 bytes apart, 8-row groups 256 bytes apart).  One
+// thread issues tcgen05.mma (M 128, N, K 16) per (tap, 16-channel) slice; each stage
+// holds 4 slices and is released by a tcgen05.commit to that stage's mbarrier.  Waits are
+// bounded: a wait that runs out sets *err and the block frees its TMEM and returns.
+namespace mm {
+
+__device__ __forceinline__ uint64_t umma_desc(unsigned saddr, unsigned lbo, unsigned sbo) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFF);
+    d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
+    d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
+    d |= (uint64_t)1 << 46;  // descriptor version of sm_100
+    return d;                // base offset 0, no swizzle
+}
+
+__device__ __forceinline__ bool mbar_wait(unsigned addr, unsigned parity, long long limit) {
+    for (long long i = 0; i < limit; i++) {
+        unsigned ok;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(ok)
+            : "r"(addr), "r"(parity));
+        if (ok) return true;
+    }
+    return false;
+}
+
+template <int N>
+__global__ void __launch_bounds__(128) conv3x3_tc_kernel(const bf16* __restrict__ in, int in_cs, int in_co, int Cin,
+                                                         const bf16* __restrict__ W, const float* __restrict__ bias,
+                                                         bf16* __restrict__ out, int out_cs, int out_co, int Cout,
+                                                         int B, int H, int Wd, int relu, int* err) {
+    constexpr int M = 128, SL = 4;                 // rows, slices per stage
+    constexpr int A_SLICE = M * 16 * 2;            // bytes of one 128 x 16 bf16 slice
+    constexpr int B_SLICE = N * 16 * 2;
+    constexpr int STAGE = SL * (A_SLICE + B_SLICE);
+    constexpr int TCOLS = N < 32 ? 32 : N;         // TMEM columns (power of two >= 32)
+    extern __shared__ __align__(1024) unsigned char smem[];
+    __shared__ __align__(8) unsigned long long mbar[2];
+    __shared__ unsigned tmem_base_sh;
+    __shared__ int fail_sh;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const long long P = (long long)B * H * Wd;
+    const long long p0 = (long long)blockIdx.x * M;
+    const int n0 = blockIdx.y * N;
+    if (tid == 0) {
+        fail_sh = 0;
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&mbar[0])));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&mbar[1])));
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::);
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
+                         smem_u32(&tmem_base_sh)),
+                     "n"(TCOLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+    }
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+    const unsigned tmem = tmem_base_sh;
+    // this thread's pixel (A rows: one 16-byte chunk of each of its 2 halves per slice)
+    const long long pr = p0 + (tid & 127);
+    int py = 0, px = 0, pb = 0;
+    if (pr < P) {
+        px = (int)(pr % Wd);
+        const long long t = pr / Wd;
+        py = (int)(t % H);
+        pb = (int)(t / H);
+    }
+    const int nslices = 9 * (Cin / 16);
+    const int nstages = (nslices + SL - 1) / SL;
+    const unsigned idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((unsigned)(N >> 3) << 17) | ((unsigned)(M >> 4) << 24);
+    const long long LIMIT = 1LL << 26;
+    // core-matrix offset of (row r, k-half h) in a slice: ((r >> 3) * 2 + h) * 128 + (r & 7) * 16
+    auto core_off = [](int r, int h) { return ((r >> 3) * 2 + h) * 128 + (r & 7) * 16; };
+    for (int s = 0; s < nstages; s++) {
+        const int st = s & 1;
+        unsigned char* base = smem + st * STAGE;
+        if (s >= 2) {  // the MMAs of stage s-2 read this buffer
+            if (!mbar_wait(smem_u32(&mbar[st]), ((s - 2) >> 1) & 1, LIMIT)) {
+                if (lane == 0) atomicExch(&fail_sh, 1);
+            }
+        }
+        __syncthreads();
+        if (fail_sh) break;
+        const int nsl = min(SL, nslices - s * SL);
+        for (int j = 0; j < nsl; j++) {
+            const int sl = s * SL + j;
+            const int tap = sl / (Cin / 16), cs = (sl % (Cin / 16)) * 16;
+            const int yy = py + tap / 3 - 1, xx = px + tap % 3 - 1;
+            const bool ok = pr < P && yy >= 0 && yy < H && xx >= 0 && xx < Wd;
+            const long long q = ok ? ((long long)pb * H + yy) * Wd + xx : 0;
+            unsigned char* as = base + j * A_SLICE;
+            const int r = tid;  // 128 rows, 2 halves each
+#pragma unroll
+            for (int h = 0; h < 2; h++)
+                cp_async16(as + core_off(r, h), in + q * in_cs + in_co + cs + h * 8, ok);
+            unsigned char* bs = base + SL * A_SLICE + j * B_SLICE;
+            for (int c = tid; c < N * 2; c += 128) {
+                const int rr = c >> 1, h = c & 1;
+                const int co = n0 + rr;
+                const bool okb = co < Cout;
+                cp_async16(bs + core_off(rr, h), W + ((long long)(okb ? co : 0) * 9 + tap) * Cin + cs + h * 8, okb);
+            }
+        }
+        cp_commit();
+        cp_wait<0>();
+        asm volatile("fence.proxy.async.shared::cta;\n" ::);
+        __syncthreads();
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+            for (int j = 0; j < nsl; j++) {
+                const uint64_t ad = umma_desc(smem_u32(base + j * A_SLICE), 128, 256);
+                const uint64_t bd = umma_desc(smem_u32(base + SL * A_SLICE + j * B_SLICE), 128, 256);
+                const unsigned acc = (s > 0 || j > 0) ? 1u : 0u;
+                asm volatile(
+                    "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+                    " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
+                    "l"(ad), "l"(bd), "r"(idesc), "r"(acc));
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                smem_u32(&mbar[st])));
+        }
+    }
+    // the last commit covers every MMA of the block
+    if (!fail_sh && nstages > 0) {
+        const int last = nstages - 1;
+        if (!mbar_wait(smem_u32(&mbar[last & 1]), (last >> 1) & 1, LIMIT)) {
+            if (lane == 0) atomicExch(&fail_sh, 1);
+        }
+    }
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+    if (!fail_sh) {
+        // epilogue: warp w holds TMEM lanes 32w..32w+31 = pixel rows; 16 columns per load
+        const long long p = p0 + warp * 32 + lane;
+#pragma unroll
+        for (int c0 = 0; c0 < N; c0 += 16) {
+            unsigned v[16];
+            const unsigned ta = tmem + ((unsigned)(warp * 32) << 16) + (unsigned)c0;
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
+                "[%16];\n"
+                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+                  "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
+                  "=r"(v[15])
+                : "r"(ta));
+            asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::);
+            if (p < P) {
+#pragma unroll
+                for (int e = 0; e < 16; e += 2) {
+                    const int co = n0 + c0 + e;
+                    if (co >= Cout) break;
+                    float a = __uint_as_float(v[e]), b = __uint_as_float(v[e + 1]);
+                    if (bias) {
+                        a += bias[co];
+                        if (co + 1 < Cout) b += bias[co + 1];
+                    }
+                    if (relu) {
+                        a = fmaxf(a, 0.f);
+                        b = fmaxf(b, 0.f);
+                    }
+                    bf16* o = out + p * out_cs + out_co + co;
+                    if (co + 1 < Cout) *reinterpret_cast<__nv_bfloat162*>(o) = __floats2bfloat162_rn(a, b);
+                    else o[0] = __float2bfloat16_rn(a);
+                }
+            }
+        }
+    } else if (tid == 0) {
+        atomicExch(err, 1);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "n"(TCOLS));
+    }
+}
+
+template <int N>
+static cudaError_t launch_conv_tc(const bf16* in, int in_cs, int in_co, int Cin, const bf16* W, const float* bias,
+                                  bf16* out, int out_cs, int out_co, int Cout, int B, int H, int Wd, int relu, int* err,
+                                  cudaStream_t st) {
+    constexpr int smem = 2 * 4 * (128 * 32 + N * 32);
+    cudaError_t e = cudaFuncSetAttribute(conv3x3_tc_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    const long long P = (long long)B * H * Wd;
+    dim3 grid((unsigned)((P + 127) / 128), (unsigned)((Cout + N - 1) / N));
+    conv3x3_tc_kernel<N><<<grid, 128, smem, st>>>(in, in_cs, in_co, Cin, W, bias, out, out_cs, out_co, Cout, B, H, Wd,
+                                                  relu, err);
+    return cudaGetLastError();
+}
+
+}  // namespace mm
+
+// tcgen05 variant of mm_nn_conv3x3 (same arguments plus a device error flag that a
+// timed-out wait sets); N tile = 16..128 chosen from Cout.
+extern "C" MM_API int mm_nn_conv3x3_tc(const void* in, int in_cs, int in_co, int Cin, const void* W, const float* bias,
+                                       void* out, int out_cs, int out_co, int Cout, int B, int H, int Wd, int relu,
+                                       int* err, mm_stream st) {
+    if (Cin % 16 || in_cs % 8 || in_co % 8 || Cout < 1 || B < 1 || H < 1 || Wd < 1 || (out_co & 1) || (out_cs & 1) ||
+        !err)
+        return report_error(MM_ERR_ARG, "mm_nn_conv3x3_tc: bad argument");
+    cudaError_t e;
+    const bf16* i = (const bf16*)in;
+    const bf16* w = (const bf16*)W;
+    bf16* o = (bf16*)out;
+    cudaStream_t s = (cudaStream_t)st;
+    if (Cout <= 16) e = launch_conv_tc<16>(i, in_cs, in_co, Cin, w, bias, o, out_cs, out_co, Cout, B, H, Wd, relu, err, s);
+    else if (Cout <= 32) e = launch_conv_tc<32>(i, in_cs, in_co, Cin, w, bias, o, out_cs, out_co, Cout, B, H, Wd, relu, err, s);
+    else if (Cout <= 64) e = launch_conv_tc<64>(i, in_cs, in_co, Cin, w, bias, o, out_cs, out_co, Cout, B, H, Wd, relu, err, s);
+    else e = launch_conv_tc<128>(i, in_cs, in_co, Cin, w, bias, o, out_cs, out_co, Cout, B, H, Wd, relu, err, s);
+    if (e != cudaSuccess) return report_error(MM_ERR_CUDA, cudaGetErrorString(e));
+    return MM_OK;
+}

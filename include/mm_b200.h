@@ -284,6 +284,10 @@ MM_API int mm_save_wait(mm_plan plan);
  * gradient. */
 MM_API int mm_nn_conv3x3(const void* in, int in_cs, int in_co, int Cin, const void* W, const float* bias, void* out,
                          int out_cs, int out_co, int Cout, int B, int H, int Wd, int relu, mm_stream st);
+/* conv3x3 on the 5th-generation tensor cores (tcgen05.mma, TMEM accumulators); *err
+ * (device int) is set if a bounded wait inside the kernel ran out. */
+MM_API int mm_nn_conv3x3_tc(const void* in, int in_cs, int in_co, int Cin, const void* W, const float* bias, void* out,
+                            int out_cs, int out_co, int Cout, int B, int H, int Wd, int relu, int* err, mm_stream st);
 MM_API int mm_nn_conv3x3_wgrad(const void* dy, int dy_cs, int dy_co, int Cout, const void* x, int x_cs, int x_co,
                                int Cin, float* dW, int B, int H, int Wd, mm_stream st);
 MM_API int mm_nn_pool(const void* in, int in_cs, int in_co, void* out, int out_cs, int out_co, int C, int B, int Ho,

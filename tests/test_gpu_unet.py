@@ -121,3 +121,29 @@ def test_training_lowers_the_loss():
         net.adam(lr=3e-3)
     print(losses[0], losses[-1])
     assert losses[-1] < 0.2 * losses[0]
+
+
+@pytest.mark.parametrize("cin,cout,B,H,W,relu", [(16, 32, 2, 8, 8, 1), (64, 128, 1, 16, 16, 0), (96, 32, 2, 8, 16, 1),
+                                                 (32, 16, 1, 4, 4, 0), (384, 128, 2, 16, 16, 1), (256, 256, 4, 8, 8, 1)])
+def test_conv3x3_tcgen05_matches(cin, cout, B, H, W, relu):
+    """The tcgen05 convolution (TMEM accumulators) against the numpy oracle."""
+    import torch
+    import unet_ref as R
+    from mumax2 import _native as nat
+    rng = np.random.default_rng(cin * 7 + cout)
+    x = R.bf16(rng.normal(size=(B, H, W, cin)))
+    w = R.bf16(rng.normal(size=(cout, 9, cin)) / np.sqrt(9 * cin))
+    b = rng.normal(size=cout).astype(np.float32)
+    xd, wd = _dev(x, torch.bfloat16), _dev(w, torch.bfloat16)
+    bd = torch.tensor(b, device="cuda")
+    out = torch.zeros(B * H * W * cout, dtype=torch.bfloat16, device="cuda")
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    nat.check(nat.lib().mm_nn_conv3x3_tc(_p(xd), cin, 0, cin, _p(wd), _p(bd), _p(out), cout, 0, cout, B, H, W, relu,
+                                         _p(err), None))
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    ref = R.conv3x3(x, w, b)
+    if relu:
+        ref = np.maximum(ref, 0)
+    got = out.float().cpu().numpy().reshape(ref.shape)
+    assert np.abs(got - ref).max() <= 2 ** -7 * np.abs(ref).max() + 1e-6
