@@ -750,3 +750,60 @@ extern "C" MM_API int mm_nn_conv3x3_tc(const void* in, int in_cs, int in_co, int
     if (e != cudaSuccess) return report_error(MM_ERR_CUDA, cudaGetErrorString(e));
     return MM_OK;
 }
+
+// ---------------------------------------------------------------- input features
+// feats[q][p][0..15] (bf16) of relaxation problem q: mask, Ms/1e6, Aex/1e-11, Ku/1e5,
+// axis x, axis y (all times the mask), B_x/0.05 T, B_y/0.05 T, 1, zeros; from the masks
+// [nq][P] and a parameter table prm[q][8] = (Ms, Aex, Ku, ux, uy, Bx, By, 0).
+namespace mm {
+__global__ void features_kernel(const float* masks, const float* prm, long long nq, int P, bf16* out) {
+    const long long n = nq * P;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+        const long long q = e / P;
+        const float m = masks[e];
+        const float* pr = prm + q * 8;
+        float f[16] = {m, m * pr[0] / 1e6f, m * pr[1] / 1e-11f, m * pr[2] / 1e5f, m * pr[3], m * pr[4], pr[5] / 0.05f,
+                       pr[6] / 0.05f, 1.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        __nv_bfloat162* o = reinterpret_cast<__nv_bfloat162*>(out + e * 16);
+#pragma unroll
+        for (int c = 0; c < 8; c++) o[c] = __floats2bfloat162_rn(f[2 * c], f[2 * c + 1]);
+    }
+}
+}  // namespace mm
+
+extern "C" MM_API int mm_nn_features(const float* masks, const float* prm, long long nq, int P, void* out,
+                                     mm_stream st) {
+    features_kernel<<<grid1(nq * P), 256, 0, (cudaStream_t)st>>>(masks, prm, nq, P, (bf16*)out);
+    NN_CHECK();
+    return MM_OK;
+}
+
+// ---------------------------------------------------------------- output -> initial states
+// state[q][c][p] (internal SoA: c = 0,1,2 = m_z, m_y, m_x) = mask * normalised first three
+// output channels (user order m_x, m_y, m_z) of problem q; a zero vector stays zero.
+namespace mm {
+__global__ void output_state_kernel(const bf16* out, int out_cs, const float* masks, long long nq, int P,
+                                    float* state) {
+    const long long n = nq * P;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+        const long long q = e / P;
+        const int p = (int)(e - q * P);
+        const bf16* o = out + e * out_cs;
+        const float x = __bfloat162float(o[0]), y = __bfloat162float(o[1]), z = __bfloat162float(o[2]);
+        const float r = sqrtf(x * x + y * y + z * z);
+        const float s = (r > 0.f ? 1.f / r : 0.f) * masks[e];
+        float* d = state + q * 3LL * P + p;
+        d[0] = z * s;
+        d[P] = y * s;
+        d[2LL * P] = x * s;
+    }
+}
+}  // namespace mm
+
+extern "C" MM_API int mm_nn_output_state(const void* out, int out_cs, const float* masks, long long nq, int P,
+                                         float* state, mm_stream st) {
+    if (out_cs < 3 || nq < 0 || P < 1) return report_error(MM_ERR_ARG, "mm_nn_output_state: bad argument");
+    output_state_kernel<<<grid1(nq * P), 256, 0, (cudaStream_t)st>>>((const bf16*)out, out_cs, masks, nq, P, state);
+    NN_CHECK();
+    return MM_OK;
+}

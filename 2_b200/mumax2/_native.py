@@ -186,6 +186,9 @@ _PROTOS = {
     "mm_nn_adam": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_longlong, C.c_float, C.c_float,
                              C.c_float, C.c_float, C.c_int, C.c_void_p, C.c_void_p]),
     "mm_nn_flip": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
+    "mm_nn_output_state": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_longlong, C.c_int, C.c_void_p,
+                                     C.c_void_p]),
+    "mm_nn_features": (C.c_int, [C.c_void_p, C.c_void_p, C.c_longlong, C.c_int, C.c_void_p, C.c_void_p]),
     "mm_nn_to_bf16": (C.c_int, [C.c_void_p, C.c_longlong, C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
     "mm_tabulate": (C.c_int, [C.c_void_p, C.c_double, C.c_int]),
     "mm_autosave": (C.c_int, [C.c_void_p, C.c_double, C.c_int]),

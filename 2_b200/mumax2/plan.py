@@ -253,15 +253,20 @@ class Plan:
                                                          int(max_steps), None))
 
     def batch_restart(self, idx, m, thr, sims=None, max_steps=0):
-        """Put new problems into slots idx (continuous batching): states m [k][3N] (host),
+        """Put new problems into slots idx (continuous batching): states m [k][3N] (host
+        array, or a float32 tensor on this plan's device),
         torque thresholds thr [k], optional scalar dicts sims [k].  Per-simulation masks
         are updated by writing into this plan's mask tensors before the call."""
         idx = np.ascontiguousarray(idx, dtype=np.int32)
-        m = np.ascontiguousarray(m, dtype=np.float32).reshape(len(idx), -1)
+        if hasattr(m, "data_ptr"):   # device tensor [k][3N] float32
+            m = m.reshape(len(idx), -1).contiguous()
+            mp, from_host = C.c_void_p(m.data_ptr()), 0
+        else:
+            m = np.ascontiguousarray(m, dtype=np.float32).reshape(len(idx), -1)
+            mp, from_host = m.ctypes.data_as(C.c_void_p), 1
         thr = np.ascontiguousarray(thr, dtype=np.float64)
         sa = nat.make_sims(self.problem, sims) if sims is not None else None
-        nat.check(nat.lib().mm_batch_restart(self.h, len(idx), idx.ctypes.data_as(C.c_void_p),
-                                             m.ctypes.data_as(C.c_void_p), 1,
+        nat.check(nat.lib().mm_batch_restart(self.h, len(idx), idx.ctypes.data_as(C.c_void_p), mp, from_host,
                                              C.cast(sa, C.c_void_p) if sa is not None else None,
                                              thr.ctypes.data_as(C.c_void_p), int(max_steps), None))
 

@@ -101,6 +101,16 @@ def features(sims, masks, n):
     return out
 
 
+def param_table(sims):
+    """[nsim][8] float32: Ms, Aex, Ku1, axis x, axis y, B_x, B_y, 0 (user axes) for the
+    features kernel."""
+    t = np.zeros((len(sims), 8), dtype=np.float32)
+    for q, s in enumerate(sims):
+        u, b = s["anisu"], s["bext"]   # internal (z, y, x)
+        t[q] = (s["msat"], s["aex"], s["ku"], u[2], u[1], b[2], b[1], 0.0)
+    return t
+
+
 def target_from_state(m_int, n):
     """Relaxed internal SoA state [3][N] -> [N][3] user order (mx, my, mz)."""
     m = np.asarray(m_int, dtype=np.float32).reshape(3, -1)
@@ -119,9 +129,10 @@ def state_from_output(out3, masks):
 class UNet:
     """Buffers for one batch size; forward, backward and Adam on the GPU."""
 
-    def __init__(self, batch, H=64, W=64, device=0, seed=0, params=None):
+    def __init__(self, batch, H=64, W=64, device=0, seed=0, params=None, tcgen05=True):
         import torch
         self.torch = torch
+        self.tcgen05 = tcgen05
         self.device = torch.device("cuda", device) if isinstance(device, int) else torch.device(device)
         self.B, self.H, self.W = batch, H, W
         bf = torch.bfloat16
@@ -148,6 +159,7 @@ class UNet:
         self.target = None
         self.mask = None
         self.loss_buf = torch.zeros(1, dtype=torch.float32, device=self.device)
+        self.err = torch.zeros(1, dtype=torch.int32, device=self.device)
         self._flip_all()
 
     # ---- helpers
@@ -159,6 +171,24 @@ class UNet:
 
     def _cs(self, view):
         return BUFFERS[view[0]][1]
+
+    def _conv(self, src, s_cs, s_co, cin, w, b, dst, d_cs, d_co, cout, H, W, relu):
+        """One 3x3 convolution: tcgen05 (TMEM accumulators) or the mma.sync kernel."""
+        L = nat.lib()
+        fp = self._ptr
+        bp = fp(b) if b is not None else None
+        if self.tcgen05:
+            nat.check(L.mm_nn_conv3x3_tc(fp(src), s_cs, s_co, cin, fp(w), bp, fp(dst), d_cs, d_co, cout, self.B, H, W,
+                                         relu, fp(self.err), None))
+        else:
+            nat.check(L.mm_nn_conv3x3(fp(src), s_cs, s_co, cin, fp(w), bp, fp(dst), d_cs, d_co, cout, self.B, H, W,
+                                      relu, None))
+
+    def check(self):
+        """Raises if a tcgen05 convolution reported a timed-out wait since the last check."""
+        if int(self.err.item()):
+            self.err.zero_()
+            raise RuntimeError("tcgen05 convolution: an mbarrier wait ran out")
 
     def _flip_all(self):
         for name, _, cin, _, cout, _ in CONVS:
@@ -173,6 +203,12 @@ class UNet:
         return out
 
     # ---- forward
+    def set_features(self, masks_dev, prm_dev):
+        """Builds the input features on the GPU from masks [B][H*W] and param_table rows
+        (device float32 tensors)."""
+        nat.check(nat.lib().mm_nn_features(self._ptr(masks_dev), self._ptr(prm_dev), self.B, self.H * self.W,
+                                           self._ptr(self.buf["in"]), None))
+
     def set_input(self, feats):
         """feats: float32 [B][H*W][FEAT] (numpy or device tensor)."""
         torch = self.torch
@@ -197,10 +233,8 @@ class UNet:
                 name, (iv, io), cin, (ov, oo), cout, relu = convs[op]
                 lvl = BUFFERS[iv][0]
                 d = self.p[name]
-                nat.check(L.mm_nn_conv3x3(self._ptr(self.buf[iv]), self._cs((iv,)), io, cin, self._ptr(d["wb"]),
-                                          self._ptr(d["b"]),
-                                          self._ptr(self.buf[ov]), self._cs((ov,)), oo, cout, B, H >> lvl, W >> lvl,
-                                          1 if relu else 0, None))
+                self._conv(self.buf[iv], self._cs((iv,)), io, cin, d["wb"], d["b"], self.buf[ov], self._cs((ov,)), oo,
+                           cout, H >> lvl, W >> lvl, 1 if relu else 0)
         return self.buf["out"]
 
     # ---- loss and backward
@@ -251,9 +285,8 @@ class UNet:
                 nat.check(L.mm_nn_bias_grad(self._ptr(self.grad[ov]), self._cs((ov,)), oo, cout, P, fp(d["gb"]), None))
                 if name != "e0a":
                     # dX over the whole input view (a concatenated input gets both parts)
-                    nat.check(L.mm_nn_conv3x3(self._ptr(self.grad[ov]), self._cs((ov,)), oo, d["cin_t"],
-                                              self._ptr(d["wt"]), None, self._ptr(self.grad[iv]), self._cs((iv,)), io,
-                                              cin, B, H >> lvl, W >> lvl, 0, None))
+                    self._conv(self.grad[ov], self._cs((ov,)), oo, d["cin_t"], d["wt"], None, self.grad[iv],
+                               self._cs((iv,)), io, cin, H >> lvl, W >> lvl, 0)
 
     def adam(self, lr=1e-3, b1=0.9, b2=0.999, eps=1e-8):
         L = nat.lib()
@@ -270,6 +303,12 @@ class UNet:
         w[3:].zero_()
         dl["wb"].copy_(dl["w"].to(self.torch.bfloat16))
         self._flip_all()
+
+    def states(self, masks_dev, dst):
+        """Initial states of this batch from the output: dst (float32 device tensor
+        [B][3][H*W], internal SoA) = masks_dev [B][H*W] * normalised output."""
+        nat.check(nat.lib().mm_nn_output_state(self._ptr(self.buf["out"]), OUTC, self._ptr(masks_dev), self.B,
+                                               self.H * self.W, self._ptr(dst), None))
 
     def output3(self):
         """[B][H*W][3] float32 numpy of the first three output channels."""

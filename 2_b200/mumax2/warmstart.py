@@ -4,10 +4,10 @@
                batching (a finished slot takes the next problem at once)
   generate     relaxed states of seeded problems, kept on the GPU as training data
   train        the U-Net (unet.py) on them with this library's kernels
-  predict      initial states for new problems, batched
+  predict      initial states for new problems, batched, built and kept on the GPU
   evaluate     cold vs warm relaxations of held-out problems: rate, steps, and the
                final state judged against the cold relax (max torque and energy); a warm
-               start that fails falls back to the cold start
+               start that fails is redone from the cold start in the same pool
 """
 import time
 
@@ -18,9 +18,17 @@ from . import workloads as W
 
 
 def relax_pool(problem, sims, masks, states, thr, slots=256, maxerr=1e-6, max_steps=100000, device=0,
-               keep_states=False, plan=None):
-    """Relaxes problem q from states[q] until maxtorque < thr[q].  Returns a dict of
-    arrays: steps, maxtorque, energy (J) and, with keep_states, the relaxed states."""
+               keep_states=False, plan=None, accept=None, fallback=None, fallback_max_steps=100000):
+    """Relaxes problem q from states[q] until maxtorque < thr[q].  states: a list of host
+    arrays or a float32 device tensor [nq][3N].  Returns a dict of arrays: steps,
+    maxtorque, energy (J) and, with keep_states, the relaxed states.
+
+    accept(q, steps, maxtorque, energy) -> bool and fallback (one host state): a relax that
+    accept rejects is queued again at once, in the same pool, from the fallback state with
+    fallback_max_steps as its step limit; the
+    result arrays then hold the fallback's result, "first_*" arrays the first attempt's and
+    "fell_back" marks the problems concerned."""
+    import collections
     import torch
     from .plan import Plan
     n = problem["n"]
@@ -33,33 +41,53 @@ def relax_pool(problem, sims, masks, states, thr, slots=256, maxerr=1e-6, max_st
                     device=device)
     plan.solver("rk23", dt=1e-14, maxerr=maxerr)
     mt = plan.mask_tensor("msat")
+    on_dev = hasattr(states, "data_ptr")
     slot = [-1] * B
-    nxt = 0
+    retry = [False] * B
+    queue = collections.deque((q, False) for q in range(nq))
     res = {"steps": np.zeros(nq, dtype=np.int64), "maxtorque": np.zeros(nq), "energy": np.zeros(nq)}
+    if accept is not None:
+        res.update({"first_steps": np.zeros(nq, dtype=np.int64), "first_maxtorque": np.zeros(nq),
+                    "first_energy": np.zeros(nq), "fell_back": np.zeros(nq, dtype=bool)})
     if keep_states:
         res["state"] = np.zeros((nq, 3 * N), dtype=np.float32)
+    thr = np.asarray(thr)
 
     def fill(free):
-        nonlocal nxt
-        idx, jobs = [], []
+        idx, jobs, fb = [], [], []
         for b in free:
-            if nxt >= nq:
+            if not queue:
                 break
-            mt[b * N:(b + 1) * N].copy_(torch.from_numpy(np.asarray(masks[nxt], dtype=np.float32)))
-            slot[b] = nxt
+            q, is_fb = queue.popleft()
+            mt[b * N:(b + 1) * N].copy_(torch.from_numpy(np.asarray(masks[q], dtype=np.float32)))
+            slot[b], retry[b] = q, is_fb
             idx.append(b)
-            jobs.append(nxt)
-            nxt += 1
-        if idx:
-            plan.batch_restart(idx, np.stack([states[q] for q in jobs]), np.asarray(thr)[jobs],
-                               sims=[sims[q] for q in jobs], max_steps=max_steps)
+            jobs.append(q)
+            fb.append(is_fb)
+        if not idx:
+            return
+        for flag, limit in ((False, max_steps), (True, fallback_max_steps)):
+            sel = [k for k in range(len(idx)) if fb[k] == flag]
+            if not sel:
+                continue
+            js = [jobs[k] for k in sel]
+            if flag:
+                m0 = np.stack([fallback] * len(js))
+            elif on_dev:
+                m0 = states[torch.tensor(js, device=states.device)]
+            else:
+                m0 = np.stack([states[q] for q in js])
+            plan.batch_restart([idx[k] for k in sel], m0, thr[js], sims=[sims[q] for q in js], max_steps=limit)
 
     fill(range(B))
     done = 0
     refill = max(1, B // 8)
+    t_drive = 0.0
+    t_all = time.perf_counter()
     while done < nq:
-        plan.batch_drive(target_active=max(0, B - refill) if nxt < nq else 0,
-                         max_attempts=0)
+        t1 = time.perf_counter()
+        plan.batch_drive(target_active=max(0, B - refill) if queue else 0, max_attempts=0)
+        t_drive += time.perf_counter() - t1
         st = plan.batch_stats()
         free = [b for b in range(B) if slot[b] >= 0 and st[b]["done"]]
         if not free:
@@ -74,11 +102,28 @@ def relax_pool(problem, sims, masks, states, thr, slots=256, maxerr=1e-6, max_st
             if keep_states:
                 res["state"][q] = state[3 * N * b:3 * N * (b + 1)]
             slot[b] = -1
+            if accept is not None and not retry[b]:
+                res["first_steps"][q] = res["steps"][q]
+                res["first_maxtorque"][q] = res["maxtorque"][q]
+                res["first_energy"][q] = res["energy"][q]
+                if not accept(q, res["steps"][q], res["maxtorque"][q], res["energy"][q]):
+                    res["fell_back"][q] = True
+                    queue.appendleft((q, True))
+                    continue
             done += 1
         fill(free)
+    res["drive_s"] = t_drive
+    res["host_s"] = time.perf_counter() - t_all - t_drive
     if own:
         plan.close()
     return res
+
+
+def step_budget(train_steps, q=99.0):
+    """Step budget of a warm relax: the q-th percentile of the cold relaxations' step counts
+    over the training problems (a warm start that needs more is stuck in a slow mode and
+    falls back to the cold start)."""
+    return int(np.ceil(np.percentile(np.asarray(train_steps), q)))
 
 
 def thresholds(sims, gamma=2.211e5, rel=1e-4):
@@ -111,11 +156,11 @@ def generate(nsim, seed, slots=256, device=0):
     return problem, sims, masks, res
 
 
-def train(data, epochs=20, batch=256, lr=1e-3, seed=0, device=0, log=None):
+def train(data, epochs=20, batch=256, lr=1e-3, seed=0, device=0, log=None, tcgen05=True):
     """Adam with a short linear warm-up and a cosine decay; returns (net, losses per epoch)."""
     import torch
     H, Wd = data.n[1], data.n[2]
-    net = U.UNet(batch, H, Wd, device=device, seed=seed)
+    net = U.UNet(batch, H, Wd, device=device, seed=seed, tcgen05=tcgen05)
     rng = np.random.default_rng(seed)
     nb = len(data) // batch
     losses = []
@@ -135,66 +180,43 @@ def train(data, epochs=20, batch=256, lr=1e-3, seed=0, device=0, log=None):
             net.adam(lr=lr * warm * 0.5 * (1 + np.cos(np.pi * k / total)))
             k += 1
         losses.append(float(acc.item()) / nb)
+        net.check()
         if log:
             log(ep, losses[-1])
     return net, losses
 
 
-def predict(net, sims, masks, n):
-    """Initial states (internal SoA, normalised, masked) for the problems, net.B per launch;
-    the features are built once and kept on the GPU."""
+def predict(net, sims, masks, n, host=False):
+    """Initial states [nq][3N] (internal SoA, normalised, masked) for the problems, net.B
+    per launch, built on the GPU from the problems' masks and parameters: a float32 device
+    tensor (a host array with host=True)."""
     import torch
     B = net.B
-    feats = torch.tensor(U.features(sims, masks, n), device=net.device)
-    if len(sims) % B:
-        pad = torch.zeros((B - len(sims) % B,) + tuple(feats.shape[1:]), device=net.device)
-        feats = torch.cat([feats, pad])
-    out = []
-    for i in range(0, len(sims), B):
-        net.set_input(feats[i:i + B])
-        net.forward()
-        o = net.output3()[:min(B, len(sims) - i)]
-        out.append(U.state_from_output(o, np.stack(masks[i:i + B])))
-    return np.concatenate(out)
-
-
-def choose_starts(problem, sims, masks, candidates, slots=256, device=0, plan=None):
-    """Per problem, the candidate start of lowest energy (the judge of a predicted start:
-    a prediction above the cold start's energy is not used).  candidates: list of
-    [nq][3N] arrays; returns (states, index of the chosen candidate per problem)."""
-    from .plan import Plan
-    import torch
-    n = problem["n"]
-    N = int(np.prod(n))
     nq = len(sims)
-    B = min(slots, nq)
-    own = plan is None
-    if own:
-        plan = Plan(problem, masks={"msat": np.concatenate(masks[:B])}, sims=sims[:B], masks_per_sim=True,
-                    device=device)
-    mt = plan.mask_tensor("msat")
-    energies = np.zeros((len(candidates), nq))
+    P = n[1] * n[2]
+    nqp = ((nq + B - 1) // B) * B
+    mk = np.zeros((nqp, P), dtype=np.float32)
+    mk[:nq] = np.stack(masks)
+    prm = np.zeros((nqp, 8), dtype=np.float32)
+    prm[:nq] = U.param_table(sims)
+    mk_d = torch.tensor(mk, device=net.device)
+    prm_d = torch.tensor(prm, device=net.device)
+    out = torch.empty((nqp, 3 * P), dtype=torch.float32, device=net.device)
     for i in range(0, nq, B):
-        k = min(B, nq - i)
-        mt[:k * N].copy_(torch.from_numpy(np.concatenate(masks[i:i + k])))
-        plan.set_sims(sims[i:i + k] + sims[i:i + 1] * (plan.nsim - k))
-        for c, cand in enumerate(candidates):
-            st = np.zeros((plan.nsim, 3 * N), dtype=np.float32)
-            st[:k] = cand[i:i + k]
-            plan.set_state(st.ravel())
-            energies[c, i:i + k] = plan.batch_energy()[:k, 4]
-    if own:
-        plan.close()
-    pick = np.argmin(energies, axis=0)
-    states = np.stack([candidates[pick[q]][q] for q in range(nq)])
-    return states, pick
+        net.set_features(mk_d[i:i + B], prm_d[i:i + B])
+        net.forward()
+        net.states(mk_d[i:i + B], out[i:i + B])
+    net.check()
+    out = out[:nq]
+    return out.cpu().numpy() if host else out
 
 
 def evaluate(net, problem, sims, masks, slots=256, device=0, energy_tol=1e-4, max_steps=20000):
     """Cold and warm relaxations of the same problems (times include the network's
     inference for the warm start).  A warm relax that does not reach the threshold within
-    max_steps, or ends above the cold relax's energy by more than energy_tol (relative),
-    counts as failed and is redone from the cold start (time included)."""
+    max_steps (its step budget; step_budget() derives one from the training relaxations),
+    or ends above the cold relax's energy by more than energy_tol (relative), counts as
+    failed and is redone from the cold start in the same pool (time included)."""
     import torch
     from .plan import Plan
     n = problem["n"]
@@ -208,37 +230,38 @@ def evaluate(net, problem, sims, masks, slots=256, device=0, energy_tol=1e-4, ma
     rc = relax_pool(problem, sims, masks, [cold] * len(sims), thr, slots=slots, device=device, plan=plan)
     torch.cuda.synchronize()
     t_cold = time.perf_counter() - t0
+
+    def accept(q, steps, mt, e):
+        if not mt < thr[q]:
+            return False
+        return e <= rc["energy"][q] or abs(e - rc["energy"][q]) <= energy_tol * max(abs(rc["energy"][q]), 1e-30)
+
     t0 = time.perf_counter()
-    pred = predict(net, sims, masks, n)
-    init, pick = choose_starts(problem, sims, masks, [pred, np.repeat(cold[None, :], len(sims), axis=0)],
-                               slots=slots, device=device, plan=plan)
+    init = predict(net, sims, masks, n)
     torch.cuda.synchronize()
     t_inf = time.perf_counter() - t0
-    rw = relax_pool(problem, sims, masks, list(init), thr, slots=slots, device=device, max_steps=max_steps,
-                    plan=plan)
+    rw = relax_pool(problem, sims, masks, init, thr, slots=slots, device=device, max_steps=max_steps, plan=plan,
+                    accept=accept, fallback=cold)
     torch.cuda.synchronize()
     t_warm = time.perf_counter() - t0
-    conv = rw["maxtorque"] < thr
-    erel = np.abs(rw["energy"] - rc["energy"]) / np.maximum(np.abs(rc["energy"]), 1e-30)
-    ok = conv & ((rw["energy"] <= rc["energy"]) | (erel <= energy_tol))
-    fail = np.nonzero(~ok)[0]
-    t_fb = 0.0
-    if len(fail):
-        t1 = time.perf_counter()
-        relax_pool(problem, [sims[q] for q in fail], [masks[q] for q in fail], [cold] * len(fail), thr[fail],
-                   slots=slots, device=device, plan=plan)
-        torch.cuda.synchronize()
-        t_fb = time.perf_counter() - t1
     plan.close()
+    fb = rw["fell_back"]
+    erel = np.abs(rw["first_energy"] - rc["energy"]) / np.maximum(np.abs(rc["energy"]), 1e-30)
     return {
         "relaxations": len(sims),
-        "cold_per_s": len(sims) / t_cold, "warm_per_s": len(sims) / (t_warm + t_fb),
-        "speedup": t_cold / (t_warm + t_fb),
-        "cold_steps_mean": float(rc["steps"].mean()), "warm_steps_mean": float(rw["steps"].mean()),
-        "steps_saved_frac": float(1 - rw["steps"].sum() / max(1, rc["steps"].sum())),
-        "inference_s": t_inf, "predicted_start_used_frac": float((pick == 0).mean()),
-        "warm_ok_frac": float(ok.mean()), "fallbacks": int(len(fail)),
+        "cold_per_s": len(sims) / t_cold, "warm_per_s": len(sims) / t_warm,
+        "speedup": t_cold / t_warm,
+        "cold_steps_mean": float(rc["steps"].mean()), "warm_steps_mean": float(rw["first_steps"].mean()),
+        "steps_saved_frac": float(1 - rw["first_steps"].sum() / max(1, rc["steps"].sum())),
+        "warm_steps_incl_fallbacks_mean": float((rw["first_steps"] + np.where(fb, rw["steps"], 0)).mean()),
+        "inference_s": t_inf, "warm_relax_only_per_s": len(sims) / (t_warm - t_inf),
+        "cold_drive_s": rc["drive_s"], "cold_host_s": rc["host_s"], "warm_drive_s": rw["drive_s"],
+        "warm_host_s": rw["host_s"],
+        "cold_steps_max": int(rc["steps"].max()), "warm_steps_max": int(rw["first_steps"].max()),
+        "warm_step_budget": int(max_steps),
+        "warm_ok_frac": float(1 - fb.mean()), "fallbacks": int(fb.sum()),
+        "final_converged_frac": float((rw["maxtorque"] < thr).mean()),
         "energy_within_tol_frac": float((erel <= energy_tol).mean()),
         "energy_rel_median": float(np.median(erel)),
-        "warm_lower_energy_frac": float((rw["energy"] < rc["energy"]).mean()),
+        "warm_lower_energy_frac": float((rw["first_energy"] < rc["energy"]).mean()),
     }

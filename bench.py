@@ -542,7 +542,8 @@ def warmstart_bench(args, rank, world, local_rank, dist):
     """relaxed states of --train problems (plain relax from the cold start,
     continuous batching) train the BF16 U-Net on the GPU; on --nsim held-out problems the
     warm start (network inference + relax) is timed against the cold relax.  value =
-    warm relaxations/s (fallbacks to the cold start included)."""
+    warm relaxations/s (fallbacks to the cold start included).  A warm relax gets the 99th
+    percentile of the training relaxations' step counts as its budget."""
     import torch
     from mumax2 import unet as U
     from mumax2 import warmstart as WS
@@ -552,13 +553,14 @@ def warmstart_bench(args, rank, world, local_rank, dist):
     t_gen = time.perf_counter() - t0
     data = WS.Dataset(problem, sims, masks, res["state"], device=local_rank)
     t0 = time.perf_counter()
-    net, losses = WS.train(data, epochs=args.epochs, batch=256, lr=2e-3, device=local_rank)
+    net, losses = WS.train(data, epochs=args.epochs, batch=256, lr=2e-3, device=local_rank,
+                           tcgen05=not args.mma_sync)
     torch.cuda.synchronize()
     t_train = time.perf_counter() - t0
     steps_per_epoch = len(data) // 256
     flops = 3 * U.conv_flops(64, 64) * 256 * steps_per_epoch * args.epochs
     _, hs, hm = W.relax_set(args.nsim, seed=5000 + rank)
-    ev = WS.evaluate(net, problem, hs, hm, device=local_rank)
+    ev = WS.evaluate(net, problem, hs, hm, device=local_rank, max_steps=WS.step_budget(res["steps"]))
     peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     peak = float(json.load(open(peaks_path))["bf16_tflops_sustained"]) if os.path.exists(peaks_path) else 1400.0
     if rank == 0:
@@ -568,6 +570,7 @@ def warmstart_bench(args, rank, world, local_rank, dist):
                 "data": "synthetic",
                 "config": {"workload": "relax_64x64x1_warm_start", "held_out": args.nsim, "train": args.train,
                            "epochs": args.epochs, "net": "U-Net 4 levels, 32/64/128/256 channels, 3x3, bf16",
+                           "conv": "mma.sync" if args.mma_sync else "tcgen05",
                            "parallelism": f"replicas{world}"},
                 "warm_vs_cold": ev,
                 "training": {"generate_s": t_gen, "train_s": t_train, "loss_first_epoch": losses[0],
@@ -595,6 +598,8 @@ def main():
                          "wall: Zhang-Li domain wall and Slonczewski disk; warmstart: the learned warm start")
     ap.add_argument("--train", type=int, default=20000, help="warmstart: training relaxations")
     ap.add_argument("--epochs", type=int, default=20, help="warmstart: training epochs")
+    ap.add_argument("--mma-sync", action="store_true",
+                    help="warmstart: forward and data-gradient convolutions on the mma.sync kernel")
     ap.add_argument("--duration", type=float, default=0.0, help="sp4/wall: simulated time (s)")
     ap.add_argument("--relax-batch", type=int, default=256)
     ap.add_argument("--relax-maxerr", type=float, default=1e-6)

@@ -302,6 +302,13 @@ MM_API int mm_nn_mse(const void* out, int o_cs, const float* target, const float
 MM_API int mm_nn_adam(float* w, const float* g, float* m, float* v, long long n, float lr, float b1, float b2,
                       float eps, int t, void* wb, mm_stream st);
 MM_API int mm_nn_flip(const void* W, int Cout, int Cin, void* Wt, int Cin_t, int Cout_t, mm_stream st);
+/* warm-start input features [nq][P][16] bf16 from masks [nq][P] and prm [nq][8] =
+ * (Ms, Aex, Ku1, axis x, axis y, B_x, B_y, 0) in user axes (see unet.py). */
+MM_API int mm_nn_features(const float* masks, const float* prm, long long nq, int P, void* out, mm_stream st);
+/* initial states [nq][3][P] (internal SoA: m_z, m_y, m_x) = mask * normalised first three
+ * output channels (m_x, m_y, m_z) of the network output [nq][P][out_cs]. */
+MM_API int mm_nn_output_state(const void* out, int out_cs, const float* masks, long long nq, int P, float* state,
+                              mm_stream st);
 MM_API int mm_nn_to_bf16(const float* in, long long P, int C, void* out, int o_cs, int o_co, mm_stream st);
 
 /* ---- instrumentation ---- */

@@ -67,7 +67,8 @@ def test_conv3x3_forward_and_data_gradient(cin, cout, B, H, W, relu):
     assert _relnorm(db.cpu().numpy(), rdb) < 1e-3
 
 
-def test_network_gradients_match_oracle():
+@pytest.mark.parametrize("tcgen05", [True, False])
+def test_network_gradients_match_oracle(tcgen05):
     import unet_ref as R
     from mumax2 import unet as U
     B, H, W = 2, 16, 16
@@ -80,12 +81,13 @@ def test_network_gradients_match_oracle():
     feats[..., :9] = rng.normal(size=(B, H * W, 9))
     target = rng.normal(size=(B, H * W, 3)).astype(np.float32)
     mask = (rng.uniform(size=(B, H * W)) > 0.2).astype(np.float32)
-    net = U.UNet(B, H, W, params=params)
+    net = U.UNet(B, H, W, params=params, tcgen05=tcgen05)
     net.set_input(feats)
     net.forward()
     net.set_target(target, mask)
     loss = float(net.loss_and_grad().item())
     net.backward()
+    net.check()
     arch = (U.BUFFERS, U.CONVS, U.POOLS, U.UPS, U.SCHEDULE)
     rloss, rgrads, rout = R.forward_backward(arch, params, feats, target, mask, H, W)
     assert loss == pytest.approx(rloss, rel=1e-2)
@@ -147,3 +149,38 @@ def test_conv3x3_tcgen05_matches(cin, cout, B, H, W, relu):
         ref = np.maximum(ref, 0)
     got = out.float().cpu().numpy().reshape(ref.shape)
     assert np.abs(got - ref).max() <= 2 ** -7 * np.abs(ref).max() + 1e-6
+
+
+def test_feature_kernel_matches_host_features():
+    """mm_nn_features builds the same bf16 inputs as unet.features followed by the cast."""
+    import torch
+    import unet_ref as R
+    from mumax2 import unet as U
+    from mumax2 import workloads as W
+    problem, sims, masks = W.relax_set(6, seed=11)
+    n = problem["n"]
+    net = U.UNet(6, n[1], n[2], seed=0)
+    mk = torch.tensor(np.stack(masks).astype(np.float32), device="cuda")
+    prm = torch.tensor(U.param_table(sims), device="cuda")
+    net.set_features(mk, prm)
+    got = net.buf["in"].float().cpu().numpy().reshape(6, -1, U.FEAT)
+    ref = R.bf16(U.features(sims, masks, n))
+    assert np.abs(got - ref).max() <= 2 ** -8 * np.abs(ref).max()
+
+
+def test_output_state_kernel_matches_host_conversion():
+    """mm_nn_output_state equals unet.state_from_output on the same network output."""
+    import torch
+    from mumax2 import unet as U
+    B, H, W = 3, 8, 8
+    rng = np.random.default_rng(5)
+    net = U.UNet(B, H, W, seed=0)
+    o = rng.normal(size=(B * H * W, U.OUTC)).astype(np.float32)
+    o[5, :3] = 0.0
+    net.buf["out"].copy_(torch.tensor(o.ravel(), device="cuda").to(torch.bfloat16))
+    masks = (rng.uniform(size=(B, H * W)) > 0.3).astype(np.float32)
+    md = torch.tensor(masks, device="cuda")
+    dst = torch.zeros((B, 3 * H * W), device="cuda")
+    net.states(md, dst)
+    ref = U.state_from_output(net.output3(), masks)
+    assert np.abs(dst.cpu().numpy() - ref).max() < 1e-6

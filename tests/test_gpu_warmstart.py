@@ -1,8 +1,7 @@
 """The learned warm start end to end at a small scale: relaxed states from the plain
 relaxer train the U-Net, whose predictions then start relaxations of unseen problems.
-Each problem starts from whichever of the prediction and the cold start has the lower
-energy; the network must be chosen for some problems and the warm relaxations must not
-take more steps on average than the cold ones."""
+The warm relaxations must take fewer solver steps on average than the cold ones, and
+most must end in a state the cold relax confirms (max torque and energy)."""
 import numpy as np
 import pytest
 
@@ -18,8 +17,7 @@ def test_warm_start_saves_steps():
     net, losses = WS.train(data, epochs=40, batch=256, lr=1e-3)
     assert losses[-1] < 0.5 * losses[0]
     _, hs, hm = W.relax_set(256, seed=77)
-    ev = WS.evaluate(net, problem, hs, hm)
+    ev = WS.evaluate(net, problem, hs, hm, max_steps=WS.step_budget(res["steps"]))
     print(ev)
-    assert ev["warm_ok_frac"] > 0.5
-    assert ev["predicted_start_used_frac"] > 0.0
-    assert ev["warm_steps_mean"] <= 1.02 * ev["cold_steps_mean"]
+    assert ev["warm_ok_frac"] > 0.9
+    assert ev["warm_steps_mean"] < ev["cold_steps_mean"]
