@@ -551,24 +551,29 @@ __host__ __device__ constexpr int col4_tile(int L) {
 // and 16/HW consecutive t, so a stride congruent to 16/HW (mod 16) puts every
 // (column, t) pair of a half-warp on its own pair of banks.
 template <int L>
-__host__ __device__ constexpr int col4_stride() {
-    const int hw = col4_tile(L) < 16 ? col4_tile(L) : 16;
+__host__ __device__ constexpr int col4_stride(int tc) {
+    const int hw = tc < 16 ? tc : 16;
     const int want = (16 / hw) & 15;
     int s = FS<L>::LBUF;
     while ((s & 15) != want) s++;
     return s;
 }
 
+// Tile variants picked by the plan's autotuner: shift -1, 0, +1 halves, keeps or doubles
+// the default columns (column pass) or rows (row pass) per block.  A variant that breaks a
+// limit of the kernel (threads per block, shared memory, the lane-pair shuffle of the
+// length-512 column transform) falls back to the default.
+static int shifted(int base, int shift) { return shift > 0 ? base << shift : (shift < 0 ? base >> (-shift) : base); }
+
 template <int L, int SIGN>
-__global__ void __launch_bounds__(256) colfft4_kernel(float2* __restrict__ S, int ncols, long long outer_stride,
+__global__ void __launch_bounds__(512) colfft4_kernel(float2* __restrict__ S, int ncols, long long outer_stride,
                                                       long long line_stride, int n_in, int n_out,
                                                       const float2* __restrict__ tw, const DevCtl* ctl,
-                                                      int skip_retry, long long sim_stride) {
+                                                      int skip_retry, long long sim_stride, int TC, int cstride) {
     if (ctl) ctl += blockIdx.y;
     if (conv_skip(ctl, skip_retry)) return;
     S += blockIdx.y * sim_stride;
     using F = FS<L>;
-    constexpr int TC = col4_tile(L);
     extern __shared__ unsigned char smem_raw[];
     float2* sm = reinterpret_cast<float2*>(smem_raw);
     const int col = threadIdx.x % TC, t = threadIdx.x / TC;
@@ -577,7 +582,7 @@ __global__ void __launch_bounds__(256) colfft4_kernel(float2* __restrict__ S, in
     const int kx0 = (blockIdx.x % ntiles) * TC;
     const bool active = (t < F::P2) && (kx0 + col < ncols);
     float2* base = S + (long long)o * outer_stride + kx0 + col;
-    float2* twt = sm + TC * col4_stride<L>();
+    float2* twt = sm + TC * cstride;
     F::fill_twiddles(twt, tw);
     float2 v[F::P1];
 #pragma unroll
@@ -586,7 +591,7 @@ __global__ void __launch_bounds__(256) colfft4_kernel(float2* __restrict__ S, in
         v[j] = (active && n < n_in) ? base[n * line_stride] : make_float2(0.f, 0.f);
     }
     __syncthreads();
-    F::template run<SIGN>(v, sm + col * col4_stride<L>(), t, active, twt, TC);
+    F::template run<SIGN>(v, sm + col * cstride, t, active, twt, TC);
 #pragma unroll
     for (int r = 0; r < F::P1; r++) {
         const int n = F::out_index(t, r);
@@ -597,17 +602,16 @@ __global__ void __launch_bounds__(256) colfft4_kernel(float2* __restrict__ S, in
 // R2C rows (zero-padded to 2M reals) with the four-step transform of the packed
 // sequence z[n] = x[2n] + i x[2n+1], then the real-to-complex post-processing.
 template <int M>
-__global__ void __launch_bounds__(256) xfwd4_kernel(const float* __restrict__ in_fixed, PP in_pp,
+__global__ void __launch_bounds__(512) xfwd4_kernel(const float* __restrict__ in_fixed, PP in_pp,
                                                     const float* __restrict__ mask, float2* __restrict__ out,
                                                     int nrows, int Z, int Y, int Yout, int in_pitch, int n_in, int hp,
                                                     const float2* __restrict__ tw, const DevCtl* ctl, int skip_retry,
                                                     long long in_bstride, long long out_bstride,
-                                                    long long mask_bstride) {
+                                                    long long mask_bstride, int RPB) {
     const int sim = blockIdx.y;
     if (ctl) ctl += sim;
     if (conv_skip(ctl, skip_retry)) return;
     using F = FS<M>;
-    constexpr int RPB = (256 / F::P2) > 0 ? 256 / F::P2 : 1;
     const float* in = (in_fixed ? in_fixed : in_pp.get(ctl ? ctl->cur : 0)) + sim * in_bstride;
     out += sim * out_bstride;
     if (mask) mask += sim * mask_bstride;
@@ -698,25 +702,28 @@ static cudaError_t launch_xfwd_t(const S* in, PP pp, const float* mask, V* out, 
 template <int M>
 static cudaError_t launch_xfwd4_t(const float* in, PP pp, const float* mask, float2* out, int nrows, int Z, int Y,
                                   int Yout, int in_pitch, int n_in, int hp, const float2* tw, const DevCtl* ctl,
-                                  int skip_retry, cudaStream_t st, XFWD_SIM_ARGS) {
+                                  int skip_retry, cudaStream_t st, XFWD_SIM_ARGS, int tile) {
     using F = FS<M>;
-    constexpr int RPB = (256 / F::P2) > 0 ? 256 / F::P2 : 1;
-    const size_t smem = (size_t)(RPB * F::LBUF + F::TWT) * sizeof(float2);
+    constexpr int RPB0 = (256 / F::P2) > 0 ? 256 / F::P2 : 1;
+    auto smem_of = [](int r) { return (size_t)(r * F::LBUF + F::TWT) * sizeof(float2); };
+    int RPB = shifted(RPB0, tile);
+    if (RPB < 1 || RPB * F::P2 > 512 || RPB * F::P2 < 32 || smem_of(RPB) > 200 * 1024) RPB = RPB0;
+    const size_t smem = smem_of(RPB);
     cudaError_t e = set_smem(xfwd4_kernel<M>, smem);
     if (e != cudaSuccess) return e;
     const dim3 grid((unsigned)((nrows + RPB - 1) / RPB), (unsigned)nsim);
     xfwd4_kernel<M><<<grid, RPB * F::P2, smem, st>>>(in, pp, mask, out, nrows, Z, Y, Yout, in_pitch, n_in, hp, tw,
-                                                      ctl, skip_retry, in_bstride, out_bstride, mask_bstride);
+                                                      ctl, skip_retry, in_bstride, out_bstride, mask_bstride, RPB);
     return cudaGetLastError();
 }
 
 template <typename V, typename S>
 cudaError_t launch_xfwd(int M, const S* in, PP pp, const float* mask, V* out, int nrows, int Z, int Y, int Yout,
                         int in_pitch, int n_in, int hp, const float2* tw, const DevCtl* ctl, int skip_retry,
-                        cudaStream_t st, XFWD_SIM_ARGS) {
+                        cudaStream_t st, XFWD_SIM_ARGS, int tile) {
     if constexpr (sizeof(V) == 8) {
         switch (M) {
-#define X(m) case m: return launch_xfwd4_t<m>(in, pp, mask, out, nrows, Z, Y, Yout, in_pitch, n_in, hp, tw, ctl, skip_retry, st, XFWD_SIM_PASS);
+#define X(m) case m: return launch_xfwd4_t<m>(in, pp, mask, out, nrows, Z, Y, Yout, in_pitch, n_in, hp, tw, ctl, skip_retry, st, XFWD_SIM_PASS, tile);
             X(4) X(8) X(16) X(32) X(64) X(128) X(256) X(512) X(1024)
 #undef X
             default: break;
@@ -749,35 +756,37 @@ static cudaError_t launch_colfft_t(V* S, int ncols, int nouter, long long outer_
 template <int L, int SIGN>
 static cudaError_t launch_colfft4_t(float2* S, int ncols, int nouter, long long outer_stride, long long line_stride,
                                     int n_in, int n_out, const float2* tw, const DevCtl* ctl, int skip_retry,
-                                    cudaStream_t st, int nsim, long long sim_stride) {
+                                    cudaStream_t st, int nsim, long long sim_stride, int tile) {
     using F = FS<L>;
-    constexpr int TC = col4_tile(L);
-    const size_t smem = (size_t)(TC * col4_stride<L>() + F::TWT) * sizeof(float2);
+    int TC = shifted(col4_tile(L), tile);
+    auto smem_of = [](int tc) { return (size_t)(tc * col4_stride<L>(tc) + F::TWT) * sizeof(float2); };
+    if (TC < 1 || TC > 16 || TC * F::P2 > 512 || smem_of(TC) > 200 * 1024) TC = col4_tile(L);
+    const size_t smem = smem_of(TC);
     cudaError_t e = set_smem(colfft4_kernel<L, SIGN>, smem);
     if (e != cudaSuccess) return e;
     const int ntiles = (ncols + TC - 1) / TC;
     int threads = TC * F::P2;
     if (threads < 32) threads = 32;
     colfft4_kernel<L, SIGN><<<dim3((unsigned)(nouter * ntiles), (unsigned)nsim), threads, smem, st>>>(
-        S, ncols, outer_stride, line_stride, n_in, n_out, tw, ctl, skip_retry, sim_stride);
+        S, ncols, outer_stride, line_stride, n_in, n_out, tw, ctl, skip_retry, sim_stride, TC, col4_stride<L>(TC));
     return cudaGetLastError();
 }
 
 template <typename V>
 cudaError_t launch_colfft(int L, int sign, V* S, int ncols, int nouter, long long outer_stride,
                           long long line_stride, int n_in, int n_out, const float2* tw, const DevCtl* ctl,
-                          int skip_retry, cudaStream_t st, int nsim, long long sim_stride) {
+                          int skip_retry, cudaStream_t st, int nsim, long long sim_stride, int tile) {
     if constexpr (sizeof(V) == 8) {
         if (sign < 0) {
             switch (L) {
-#define X(l) case l: return launch_colfft4_t<l, -1>(S, ncols, nouter, outer_stride, line_stride, n_in, n_out, tw, ctl, skip_retry, st, nsim, sim_stride);
+#define X(l) case l: return launch_colfft4_t<l, -1>(S, ncols, nouter, outer_stride, line_stride, n_in, n_out, tw, ctl, skip_retry, st, nsim, sim_stride, tile);
                 X(4) X(8) X(16) X(32) X(64) X(128) X(256) X(512) X(1024)
 #undef X
                 default: break;
             }
         } else {
             switch (L) {
-#define X(l) case l: return launch_colfft4_t<l, 1>(S, ncols, nouter, outer_stride, line_stride, n_in, n_out, tw, ctl, skip_retry, st, nsim, sim_stride);
+#define X(l) case l: return launch_colfft4_t<l, 1>(S, ncols, nouter, outer_stride, line_stride, n_in, n_out, tw, ctl, skip_retry, st, nsim, sim_stride, tile);
                 X(4) X(8) X(16) X(32) X(64) X(128) X(256) X(512) X(1024)
 #undef X
                 default: break;
@@ -833,13 +842,13 @@ cudaError_t launch_colmul(int L, float2* S, const KernelView& K, int ncols, int 
 
 template cudaError_t launch_xfwd<float2, float>(int, const float*, PP, const float*, float2*, int, int, int, int, int,
                                                 int, int, const float2*, const DevCtl*, int, cudaStream_t, int,
-                                                long long, long long, long long);
+                                                long long, long long, long long, int);
 template cudaError_t launch_xfwd<double2, double>(int, const double*, PP, const float*, double2*, int, int, int, int,
                                                   int, int, int, const float2*, const DevCtl*, int, cudaStream_t, int,
-                                                  long long, long long, long long);
+                                                  long long, long long, long long, int);
 template cudaError_t launch_colfft<float2>(int, int, float2*, int, int, long long, long long, int, int,
-                                           const float2*, const DevCtl*, int, cudaStream_t, int, long long);
+                                           const float2*, const DevCtl*, int, cudaStream_t, int, long long, int);
 template cudaError_t launch_colfft<double2>(int, int, double2*, int, int, long long, long long, int, int,
-                                            const float2*, const DevCtl*, int, cudaStream_t, int, long long);
+                                            const float2*, const DevCtl*, int, cudaStream_t, int, long long, int);
 
 }  // namespace mm

@@ -203,16 +203,18 @@ struct EpiArgs {
 // ---- launchers (conv.cu, rhs.cu)
 // Every launcher runs nsim simulations (gridDim.y = nsim); *_bstride are the element
 // strides between simulations, ctl (if not NULL) points to nsim control blocks, and
-// sim_scale (if not NULL) gives the demag scale per simulation.
+// sim_scale (if not NULL) gives the demag scale per simulation.  `tile` (-1, 0, +1)
+// selects the autotuner's variant of the rows or columns per block of the four-step
+// row, column and epilogue passes (0 = default).
 template <typename V, typename S>
 cudaError_t launch_xfwd(int M, const S* in, PP pp, const float* mask, V* out, int nrows, int Z, int Y, int Yout,
                         int in_pitch, int n_in, int hp, const float2* tw, const DevCtl* ctl, int skip_retry,
                         cudaStream_t st, int nsim = 1, long long in_bstride = 0, long long out_bstride = 0,
-                        long long mask_bstride = 0);
+                        long long mask_bstride = 0, int tile = 0);
 template <typename V>
 cudaError_t launch_colfft(int L, int sign, V* S, int ncols, int nouter, long long outer_stride,
                           long long line_stride, int n_in, int n_out, const float2* tw, const DevCtl* ctl,
-                          int skip_retry, cudaStream_t st, int nsim = 1, long long sim_stride = 0);
+                          int skip_retry, cudaStream_t st, int nsim = 1, long long sim_stride = 0, int tile = 0);
 cudaError_t launch_colmul(int L, float2* S, const KernelView& K, int ncols, int nouter, long long comp_stride,
                           long long outer_stride, long long line_stride, int n_in, int kaxis, float scale,
                           const float2* tw, const DevCtl* ctl, int skip_retry, cudaStream_t st, int nsim = 1,
@@ -222,7 +224,7 @@ cudaError_t launch_zmul_reg(int P, float2* S, const KernelView& K, int L1, int h
                             cudaStream_t st, int nsim = 1, long long sim_stride = 0,
                             const float* sim_scale = nullptr);
 cudaError_t launch_xinv_epi(int M, const float2* S, int hp, int L1, const float2* tw, const EpiArgs& A, bool terms,
-                            cudaStream_t st, int* nblocks, int nsim = 1);
+                            cudaStream_t st, int* nblocks, int nsim = 1, int tile = 0);
 cudaError_t launch_local_epi(const EpiArgs& A, bool terms, cudaStream_t st, int* nblocks, int nsim = 1);
 // solver/am12 (am12.cu)
 cudaError_t am_begin(DevCtl* ctl, int nsim, cudaStream_t st);

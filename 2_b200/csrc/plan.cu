@@ -13,6 +13,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <thread>
@@ -441,6 +442,10 @@ struct mm_plan_s {
     int ring_cap = 0;
     bool save_on = false;
     long long bytes = 0;
+    // autotuned tile variants (-1, 0, +1) of the row, column and epilogue passes, and the
+    // evaluation time measured with them (0 if not tuned)
+    int tiles[3] = {0, 0, 0};
+    float tuned_us = 0.f;
     long long n3() const { return 3 * g.N; }
     long long spec_bstride() const { return 3LL * g.n[0] * g.L[1] * g.hp; }
 };
@@ -575,6 +580,8 @@ static void free_graph(mm_plan p) {
 
 extern "C" MM_API const char* mm_last_error(void) { return g_err.c_str(); }
 extern "C" MM_API const char* mm_version(void) { return "mm_b200 0.2 (sm_100a)"; }
+
+static int autotune(mm_plan p);
 
 extern "C" MM_API int mm_plan_create_batch(const mm_problem* prob, int nsim, const mm_sim* sims, int masks_per_sim,
                                            mm_plan* out) {
@@ -736,6 +743,10 @@ extern "C" MM_API int mm_plan_create_batch(const mm_problem* prob, int nsim, con
         mm_plan_destroy(p);
         return set_err(MM_ERR_CUDA, "ctl init failed");
     }
+    if ((rc = autotune(p))) {
+        mm_plan_destroy(p);
+        return rc;
+    }
     *out = p;
     return MM_OK;
 }
@@ -858,7 +869,7 @@ static int launch_conv(mm_plan p, PP m_in, const DevCtl* ctl, int skip_retry, cu
     // demagexch convolves m itself (mod_demagexchange.go:207-209), demag convolves Ms_mask m
     const float* in_mask = p->khat_d ? nullptr : p->P.msat_mask;
     CUCHK(launch_xfwd<float2, float>(g.M, nullptr, m_in, in_mask, p->S, 3 * n0 * n1, n0, n1, L1, n2, n2, g.hp,
-                                     p->tw, ctl, skip_retry, st, ns, p->n3(), sb, p->P.mask_bstride));
+                                     p->tw, ctl, skip_retry, st, ns, p->n3(), sb, p->P.mask_bstride, p->tiles[0]));
     if ((rc = mark())) return rc;
     if (L0 == 1) {
         CUCHK(launch_colmul(L1, p->S, p->kv, g.h, 1, plane, 0, g.hp, n1, 1, scale, p->tw, ctl, skip_retry, st, ns, sb,
@@ -866,7 +877,7 @@ static int launch_conv(mm_plan p, PP m_in, const DevCtl* ctl, int skip_retry, cu
         if ((rc = mark())) return rc;
     } else {
         CUCHK(launch_colfft<float2>(L1, -1, p->S, g.h, 3 * n0, plane, g.hp, n1, L1, p->tw, ctl, skip_retry, st, ns,
-                                    sb));
+                                    sb, p->tiles[1]));
         if ((rc = mark())) return rc;
         if (zreg_ok(g))
             CUCHK(launch_zmul_reg(n0, p->S, p->kv, L1, g.h, g.hp, (long long)n0 * plane, plane, scale, p->tw, ctl,
@@ -876,7 +887,7 @@ static int launch_conv(mm_plan p, PP m_in, const DevCtl* ctl, int skip_retry, cu
                                 ctl, skip_retry, st, ns, sb, sim_scale));
         if ((rc = mark())) return rc;
         CUCHK(launch_colfft<float2>(L1, +1, p->S, g.h, 3 * n0, plane, g.hp, L1, n1, p->tw, ctl, skip_retry, st, ns,
-                                    sb));
+                                    sb, p->tiles[1]));
         if ((rc = mark())) return rc;
     }
     p->launches += (L0 == 1) ? 2 : 4;
@@ -908,7 +919,7 @@ static int launch_eval(mm_plan p, const StageOp& op, DevCtl* ctl, int skip_retry
     int nb = 0, rc;
     if (p->demag) {
         if ((rc = launch_conv(p, op.m_in, ctl, skip_retry, st))) return rc;
-        CUCHK(launch_xinv_epi(g.M, p->S, g.hp, g.L[1], p->tw, A, terms, st, &nb, p->nsim));
+        CUCHK(launch_xinv_epi(g.M, p->S, g.hp, g.L[1], p->tw, A, terms, st, &nb, p->nsim, p->tiles[2]));
     } else {
         CUCHK(launch_local_epi(A, terms, st, &nb, p->nsim));
     }
@@ -928,6 +939,92 @@ static StageOp op_blank() {
     o.kcur = -1;
     o.ecur = -1;
     return o;
+}
+
+// ---------------------------------------------------------------- tile autotuner
+// Times whole field evaluations (torque of a zeroed state, the plan's own buffers and
+// masks) for the tile variants of the four-step passes: rows per block of the R2C row
+// pass (1/2, 1, 2 x default), columns per block of the column passes (1/2, 1, 2 x) and
+// rows per block of the C2R + epilogue pass (1/2, 1 x).  One pass at a time from the
+// defaults (coordinate descent); a variant replaces the current choice only when it is
+// more than 2 % faster.  Runs once at plan creation; MM_AUTOTUNE=0 in the environment
+// keeps the defaults.  Tile variants change the block decomposition only: every cell's
+// arithmetic is the same, and so are the fields, torques and step sequences.
+static int autotune(mm_plan p) {
+    if (!p->demag) return MM_OK;
+    const char* env = getenv("MM_AUTOTUNE");
+    if (env && env[0] == '0') return MM_OK;
+    cudaStream_t st = nullptr;
+    const long long launches = p->launches;
+    CUCHK(cudaMemsetAsync(p->Y[0], 0, sizeof(float) * (size_t)p->n3() * p->nsim, st));
+    StageOp o = op_blank();
+    o.m_in = fixed(p->Y[0]);
+    o.k_out = fixed(p->K1[0]);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    CUCHK(cudaEventCreate(&e0));
+    if (cudaEventCreate(&e1) != cudaSuccess) {
+        cudaEventDestroy(e0);
+        return set_err(MM_ERR_CUDA, "cudaEventCreate failed");
+    }
+    int rc = MM_OK;
+    int reps = 5;
+    auto time_eval = [&](float* us) -> int {
+        int r;
+        for (int i = 0; i < 2; i++)
+            if ((r = launch_eval(p, o, nullptr, 0, nullptr, 0, 0, nullptr, nullptr, st, nullptr))) return r;
+        CUCHK(cudaEventRecord(e0, st));
+        for (int i = 0; i < reps; i++)
+            if ((r = launch_eval(p, o, nullptr, 0, nullptr, 0, 0, nullptr, nullptr, st, nullptr))) return r;
+        CUCHK(cudaEventRecord(e1, st));
+        CUCHK(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        CUCHK(cudaEventElapsedTime(&ms, e0, e1));
+        *us = 1000.f * ms / reps;
+        return MM_OK;
+    };
+    float best = 0.f;
+    if (!(rc = time_eval(&best))) {
+        // about 2 ms of timing per variant
+        reps = std::max(5, std::min(200, (int)(2000.f / std::max(best, 1.f))));
+        rc = time_eval(&best);
+    }
+    const int lo[3] = {-1, -1, -1}, hi[3] = {1, 1, 0};
+    for (int d = 0; d < 3 && !rc; d++) {
+        if (d == 1 && p->g.L[0] == 1) continue;  // single-layer films have no column FFT pass
+        int keep = p->tiles[d];
+        for (int v = lo[d]; v <= hi[d] && !rc; v++) {
+            if (v == keep) continue;
+            p->tiles[d] = v;
+            float t = 0.f;
+            if ((rc = time_eval(&t))) break;
+            if (t < 0.98f * best) {
+                best = t;
+                keep = v;
+            }
+        }
+        p->tiles[d] = keep;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    p->tuned_us = rc ? 0.f : best;
+    p->launches = launches;
+    return rc;
+}
+
+extern "C" MM_API int mm_plan_tiles(mm_plan p, int* tiles, double* eval_us) {
+    if (!p || !tiles) return set_err(MM_ERR_ARG, "null argument");
+    for (int d = 0; d < 3; d++) tiles[d] = p->tiles[d];
+    if (eval_us) *eval_us = p->tuned_us;
+    return MM_OK;
+}
+
+extern "C" MM_API int mm_plan_set_tiles(mm_plan p, const int* tiles) {
+    if (!p || !tiles) return set_err(MM_ERR_ARG, "null argument");
+    for (int d = 0; d < 3; d++)
+        if (tiles[d] < -1 || tiles[d] > (d == 2 ? 0 : 1)) return set_err(MM_ERR_ARG, "tile %d out of range", d);
+    for (int d = 0; d < 3; d++) p->tiles[d] = tiles[d];
+    free_graph(p);
+    return MM_OK;
 }
 
 // host copy of the device table lookup (update_pointwise.go:30-88); false past the end

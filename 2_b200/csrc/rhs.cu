@@ -604,14 +604,13 @@ __host__ __device__ constexpr int xinv4_rpb() {
 
 template <int M, bool TERMS, bool BATCH>
 __global__ void __launch_bounds__(384) xinv4_epi_kernel(const float2* __restrict__ S, int hp, int L1,
-                                                        const float2* __restrict__ tw, EpiArgs A) {
+                                                        const float2* __restrict__ tw, EpiArgs A, int RPB) {
     const DevCtl* ctl = A.ctl ? A.ctl + blockIdx.y : nullptr;
     if (skip_eval(ctl, A.skip_retry)) return;
     S += blockIdx.y * A.spec_bstride;
     __shared__ SimScalars s_sim;  // this simulation's scalars (BATCH); covered by the barriers below
     if (BATCH && threadIdx.x == 0) stage_scalars(A, ctl, s_sim);
     using F = FS<M>;
-    constexpr int RPB = xinv4_rpb<M>();
     extern __shared__ unsigned char smem_raw[];
     float2* sm = reinterpret_cast<float2*>(smem_raw);
     const int n0 = A.P.n[0], n1 = A.P.n[1];
@@ -706,10 +705,18 @@ static cudaError_t launch_xinv_t(const float2* S, int hp, int L1, const float2* 
     return cudaGetLastError();
 }
 
+// Rows per block of the four-step epilogue: the default, or half of it (tile -1, the
+// autotuner's other variant; at least 32 threads).
+template <int M>
+static int xinv4_rows(int tile) {
+    const int r0 = xinv4_rpb<M>();
+    return (tile < 0 && r0 >= 2 && (r0 / 2) * 3 * FS<M>::P2 >= 32) ? r0 / 2 : r0;
+}
+
 template <int M, bool TERMS, bool BATCH>
 static cudaError_t launch_xinv4_t(const float2* S, int hp, int L1, const float2* tw, const EpiArgs& A,
-                                  cudaStream_t st, int* nblocks, int nsim) {
-    constexpr int RPB = xinv4_rpb<M>();
+                                  cudaStream_t st, int* nblocks, int nsim, int tile) {
+    const int RPB = xinv4_rows<M>(tile);
     const size_t smem = (size_t)(RPB * 3 * FS<M>::LBUF + FS<M>::TWT) * sizeof(float2);
     if (smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(xinv4_epi_kernel<M, TERMS, BATCH>,
@@ -722,7 +729,7 @@ static cudaError_t launch_xinv4_t(const float2* S, int hp, int L1, const float2*
     if (threads < 32) threads = 32;
     *nblocks = blocks;
     xinv4_epi_kernel<M, TERMS, BATCH><<<dim3((unsigned)blocks, (unsigned)nsim), threads, smem, st>>>(S, hp, L1, tw,
-                                                                                                     A);
+                                                                                                     A, RPB);
     return cudaGetLastError();
 }
 
@@ -732,7 +739,7 @@ int xinv_blocks(int M, int n0n1) {
     if (use_xinv4(M)) {
         int rpb = 1;
         switch (M) {
-#define X(m) case m: rpb = xinv4_rpb<m>(); break;
+#define X(m) case m: rpb = xinv4_rows<m>(-1); break;
             X(4) X(8) X(16) X(32) X(64) X(128) X(256) X(512) X(1024)
 #undef X
         }
@@ -749,17 +756,17 @@ int xinv_blocks(int M, int n0n1) {
 static bool staged_scalars(const EpiArgs& A, int nsim) { return nsim > 1 || A.P.tab[0].n || A.P.tab[1].n; }
 
 cudaError_t launch_xinv_epi(int M, const float2* S, int hp, int L1, const float2* tw, const EpiArgs& A, bool terms,
-                            cudaStream_t st, int* nblocks, int nsim) {
+                            cudaStream_t st, int* nblocks, int nsim, int tile) {
     const bool staged = staged_scalars(A, nsim);
     if (use_xinv4(M)) {
         switch (M) {
 #define X(m)                                                                      \
     case m:                                                                       \
         if (staged)                                                                     \
-            return terms ? launch_xinv4_t<m, true, true>(S, hp, L1, tw, A, st, nblocks, nsim)  \
-                         : launch_xinv4_t<m, false, true>(S, hp, L1, tw, A, st, nblocks, nsim); \
-        return terms ? launch_xinv4_t<m, true, false>(S, hp, L1, tw, A, st, nblocks, 1)     \
-                     : launch_xinv4_t<m, false, false>(S, hp, L1, tw, A, st, nblocks, 1);
+            return terms ? launch_xinv4_t<m, true, true>(S, hp, L1, tw, A, st, nblocks, nsim, tile)  \
+                         : launch_xinv4_t<m, false, true>(S, hp, L1, tw, A, st, nblocks, nsim, tile); \
+        return terms ? launch_xinv4_t<m, true, false>(S, hp, L1, tw, A, st, nblocks, 1, tile)     \
+                     : launch_xinv4_t<m, false, false>(S, hp, L1, tw, A, st, nblocks, 1, tile);
             X(4) X(8) X(16) X(32) X(64) X(128) X(256) X(512) X(1024)
 #undef X
         }

@@ -92,6 +92,17 @@ class Plan:
             return a.to(self.device, torch.float32).contiguous()
         return torch.as_tensor(np.ascontiguousarray(a, dtype=np.float32).ravel(), device=self.device)
 
+    def tiles(self):
+        """(tiles, eval_us): the autotuned tile shifts of the row, column and epilogue
+        passes and the timed evaluation with them."""
+        t = (C.c_int * 3)()
+        us = C.c_double(0.0)
+        nat.check(nat.lib().mm_plan_tiles(self.h, t, C.byref(us)))
+        return list(t[:]), us.value
+
+    def set_tiles(self, tiles):
+        nat.check(nat.lib().mm_plan_set_tiles(self.h, (C.c_int * 3)(*tiles)))
+
     def kernel_nonzero(self):
         out = (C.c_int * 6)()
         nat.check(nat.lib().mm_plan_kernel_nonzero(self.h, out))

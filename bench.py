@@ -640,6 +640,7 @@ def main():
     n = w["n"]
     N = n[0] * n[1] * n[2]
     plan = Plan(problem(), device=local_rank)
+    tiles, tuned_us = plan.tiles()
     plan.solver(w["solver"], dt=w["dt0"], maxerr=w["maxerr"])
     plan.set_state(initial_m(replica_seed(rank)))
     if args.profile_only:
@@ -730,7 +731,7 @@ def main():
             "data": "synthetic",
             "config": {"workload": w["name"], "cells": N, "grid_xyz": [n[2], n[1], n[0]],
                        "cell_nm": [4, 4, 2], "solver": "rk23", "maxerr": w["maxerr"],
-                       "parallelism": f"replicas{world}",
+                       "parallelism": f"replicas{world}", "tiles": tiles, "tuned_eval_us": tuned_us,
                        "l2": "per-step working set (state, stages, half spectrum, kernel) ~250 MB > 126 MB L2"},
             "roofline": {"bound": "hbm", "kernel": pb[dom][0], "achieved": achieved, "peak": peak,
                          "peak_source": peak_src, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,

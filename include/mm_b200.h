@@ -131,6 +131,15 @@ MM_API int mm_plan_destroy(mm_plan plan);
 MM_API int mm_plan_create_batch(const mm_problem* prob, int nsim, const mm_sim* sims, int masks_per_sim,
                                 mm_plan* out);
 MM_API int mm_plan_nsim(mm_plan plan);
+/* Tile shapes of the FFT passes, picked at plan creation by the autotuner (timed field
+ * evaluations; MM_AUTOTUNE=0 in the environment keeps the defaults).  tiles[0]: rows per
+ * block of the R2C row pass, tiles[1]: columns per block of the column passes, tiles[2]:
+ * rows per block of the C2R + stencil/torque epilogue, each as a shift of the default
+ * (-1 = half, 0 = default, +1 = double; tiles[2] in {-1, 0}).  eval_us (may be NULL): the
+ * timed evaluation with the chosen tiles (0 if not tuned).  Results do not depend on the
+ * tiles (energies up to the order of their block partial sums). */
+MM_API int mm_plan_tiles(mm_plan plan, int tiles[3], double* eval_us);
+MM_API int mm_plan_set_tiles(mm_plan plan, const int tiles[3]);
 /* Replaces the per-simulation scalars of a batched plan. */
 MM_API int mm_batch_set_sims(mm_plan plan, const mm_sim* sims);
 /* Replaces multipliers/masks/terms of an existing plan (same grid, cell, pbc). */
