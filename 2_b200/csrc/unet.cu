@@ -532,13 +532,14 @@ extern "C" MM_API int mm_nn_to_bf16(const float* in, long long P, int C, void* o
 }
 
 // ---------------------------------------------------------------- tcgen05 forward convolution
-// The same implicit GEMM on the 5th-generation tensor cores: D[128 pixels][N] in TMEM
-// (FP32), A = pixel rows x (tap, channel) and B = output channels x (tap, channel), both
+// The same implicit GEMM on the 5th-generation tensor cores: D[128 positions][N] in TMEM
+// (FP32), A = positions x (tap, channel) and B = output channels x (tap, channel), both
 // K-major bf16 in shared memory in the canonical no-swizzle layout (8-row x 16-byte core
-// matrices; K-adjacent core matrices 128 bytes apart, 8-row groups 256 bytes apart).  One
-// thread issues tcgen05.mma (M 128, N, K 16) per (tap, 16-channel) slice; each stage
-// holds 4 slices and is released by a tcgen05.commit to that stage's mbarrier.  Waits are
-// bounded: a wait that runs out sets *err and the block frees its TMEM and returns.
+// matrices).  One thread issues the nine tcgen05.mma (M 128, N, K 16) of a 16-channel
+// slice; stages form a ring of 2-4 buffers filled by cp.async and released by a
+// tcgen05.commit to the stage's mbarrier, so several slices load while the tensor core
+// works.  Waits are bounded: a wait that runs out sets *err and the block frees its TMEM
+// and returns.
 namespace mm {
 
 __device__ __forceinline__ uint64_t umma_desc(unsigned saddr, unsigned lbo, unsigned sbo) {
@@ -562,28 +563,51 @@ __device__ __forceinline__ bool mbar_wait(unsigned addr, unsigned parity, long l
     return false;
 }
 
-template <int N>
-__global__ void __launch_bounds__(128) conv3x3_tc_kernel(const bf16* __restrict__ in, int in_cs, int in_co, int Cin,
+// Halo-band layout.  The tile runs over padded positions: image b, row y, column x sit
+// at q = b (H+1)(W+1) + y (W+1) + x + 1, so every row starts with a zero column and every
+// image ends with a zero row.  An output at q reads its tap (dy, dx) at q + dy (W+1) + dx,
+// which is a zero pad whenever the tap leaves the image.  The 128 outputs q0 .. q0+127
+// of a tile therefore read, for every tap, 128 consecutive positions of one band
+// q0 - (W+2) .. q0 + 127 + (W+2): the A operand of tap (dy, dx) is the band's descriptor
+// shifted by ((dy+1)(W+1) + dx+1) x 16 bytes.  A stage holds one 16-channel slice of the
+// band (two 8-channel planes, K-direction stride = plane size, 8-position groups 128
+// bytes apart) and the slice's weights for all nine taps; it is read from global memory
+// once instead of once per tap.  Pad positions are computed and not stored.
+constexpr int BAND_MAX = 128 + 2 * 257 + 2;  // widths up to 256
+
+template <int N, int ST>
+__global__ void __launch_bounds__(256) conv3x3_tc_kernel(const bf16* __restrict__ in, int in_cs, int in_co, int Cin,
                                                          const bf16* __restrict__ W, const float* __restrict__ bias,
                                                          bf16* __restrict__ out, int out_cs, int out_co, int Cout,
-                                                         int B, int H, int Wd, int relu, int* err) {
-    constexpr int M = 128, SL = 4;                 // rows, slices per stage
-    constexpr int A_SLICE = M * 16 * 2;            // bytes of one 128 x 16 bf16 slice
-    constexpr int B_SLICE = N * 16 * 2;
-    constexpr int STAGE = SL * (A_SLICE + B_SLICE);
+                                                         int B, int H, int Wd, int relu, int* err, int band,
+                                                         int stage_bytes) {
+    constexpr int M = 128;
     constexpr int TCOLS = N < 32 ? 32 : N;         // TMEM columns (power of two >= 32)
     extern __shared__ __align__(1024) unsigned char smem[];
-    __shared__ __align__(8) unsigned long long mbar[2];
+    __shared__ __align__(8) unsigned long long mbar[ST];
     __shared__ unsigned tmem_base_sh;
     __shared__ int fail_sh;
+    __shared__ int s_q[BAND_MAX];                  // band position -> input pixel, or -1
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const long long P = (long long)B * H * Wd;
-    const long long p0 = (long long)blockIdx.x * M;
+    const int Wp = Wd + 1;
+    const long long img = (long long)(H + 1) * Wp;
+    const long long total = (long long)B * img;
+    const long long q0 = (long long)blockIdx.x * M;
     const int n0 = blockIdx.y * N;
+    const int plane = band * 16;                   // bytes of one 8-channel plane of the band
+    for (int i = tid; i < band; i += 256) {
+        const long long q = q0 - (Wp + 1) + i;
+        int pix = -1;
+        if (q >= 0 && q < total) {
+            const long long b = q / img, r = q - b * img;
+            const int y = (int)(r / Wp), xp = (int)(r - (long long)y * Wp);
+            if (y < H && xp > 0) pix = (int)(((long long)b * H + y) * Wd + xp - 1);
+        }
+        s_q[i] = pix;
+    }
     if (tid == 0) {
         fail_sh = 0;
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&mbar[0])));
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&mbar[1])));
+        for (int i = 0; i < ST; i++) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&mbar[i])));
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::);
     }
     if (warp == 0) {
@@ -595,86 +619,94 @@ __global__ void __launch_bounds__(128) conv3x3_tc_kernel(const bf16* __restrict_
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
     const unsigned tmem = tmem_base_sh;
-    // this thread's pixel (A rows: one 16-byte chunk of each of its 2 halves per slice)
-    const long long pr = p0 + (tid & 127);
-    int py = 0, px = 0, pb = 0;
-    if (pr < P) {
-        px = (int)(pr % Wd);
-        const long long t = pr / Wd;
-        py = (int)(t % H);
-        pb = (int)(t / H);
-    }
-    const int nslices = 9 * (Cin / 16);
-    const int nstages = (nslices + SL - 1) / SL;
+    const int nstages = Cin / 16;
     const unsigned idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((unsigned)(N >> 3) << 17) | ((unsigned)(M >> 4) << 24);
     const long long LIMIT = 1LL << 26;
-    // core-matrix offset of (row r, k-half h) in a slice: ((r >> 3) * 2 + h) * 128 + (r & 7) * 16
+    // core-matrix offset of (row r, k-half h) in a 16-channel weight block: K-adjacent core
+    // matrices 128 bytes apart, 8-row groups 256 bytes apart
     auto core_off = [](int r, int h) { return ((r >> 3) * 2 + h) * 128 + (r & 7) * 16; };
-    for (int s = 0; s < nstages; s++) {
-        const int st = s & 1;
-        unsigned char* base = smem + st * STAGE;
-        if (s >= 2) {  // the MMAs of stage s-2 read this buffer
-            if (!mbar_wait(smem_u32(&mbar[st]), ((s - 2) >> 1) & 1, LIMIT)) {
-                if (lane == 0) atomicExch(&fail_sh, 1);
-            }
+    const int bwt = 2 * plane;                     // weights follow the band in a stage
+    auto load_stage = [&](int s) {
+        unsigned char* base = smem + (s % ST) * stage_bytes;
+        const int cs = s * 16;
+        // band: consecutive lanes take consecutive positions of one plane
+        for (int c = tid; c < 2 * band; c += 256) {
+            const int h = c >= band ? 1 : 0, i = c - h * band;
+            const int pix = s_q[i];
+            const bool ok = pix >= 0;
+            cp_async16(base + h * plane + i * 16, in + (long long)(ok ? pix : 0) * in_cs + in_co + cs + h * 8, ok);
         }
-        __syncthreads();
-        if (fail_sh) break;
-        const int nsl = min(SL, nslices - s * SL);
-        for (int j = 0; j < nsl; j++) {
-            const int sl = s * SL + j;
-            const int tap = sl / (Cin / 16), cs = (sl % (Cin / 16)) * 16;
-            const int yy = py + tap / 3 - 1, xx = px + tap % 3 - 1;
-            const bool ok = pr < P && yy >= 0 && yy < H && xx >= 0 && xx < Wd;
-            const long long q = ok ? ((long long)pb * H + yy) * Wd + xx : 0;
-            unsigned char* as = base + j * A_SLICE;
-            const int r = tid;  // 128 rows, 2 halves each
-#pragma unroll
-            for (int h = 0; h < 2; h++)
-                cp_async16(as + core_off(r, h), in + q * in_cs + in_co + cs + h * 8, ok);
-            unsigned char* bs = base + SL * A_SLICE + j * B_SLICE;
-            for (int c = tid; c < N * 2; c += 128) {
-                const int rr = c >> 1, h = c & 1;
-                const int co = n0 + rr;
-                const bool okb = co < Cout;
-                cp_async16(bs + core_off(rr, h), W + ((long long)(okb ? co : 0) * 9 + tap) * Cin + cs + h * 8, okb);
-            }
+        // weights of the nine taps
+        for (int c = tid; c < 9 * 2 * N; c += 256) {
+            const int tap = c / (2 * N), rem = c - tap * 2 * N;
+            const int rr = rem >> 1, h = rem & 1;
+            const int co = n0 + rr;
+            const bool okb = co < Cout;
+            cp_async16(base + bwt + tap * N * 32 + core_off(rr, h),
+                       W + ((long long)(okb ? co : 0) * 9 + tap) * Cin + cs + h * 8, okb);
         }
+    };
+    for (int s = 0; s < ST - 1; s++) {
+        if (s < nstages) load_stage(s);
         cp_commit();
-        cp_wait<0>();
+    }
+    int issued = 0;  // stages whose MMAs were issued and committed
+    for (int s = 0; s < nstages; s++) {
+        cp_wait<ST - 2>();  // this thread's copies of stage s have landed
         asm volatile("fence.proxy.async.shared::cta;\n" ::);
         __syncthreads();
+        if (fail_sh) break;
         if (tid == 0) {
             asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
-            for (int j = 0; j < nsl; j++) {
-                const uint64_t ad = umma_desc(smem_u32(base + j * A_SLICE), 128, 256);
-                const uint64_t bd = umma_desc(smem_u32(base + SL * A_SLICE + j * B_SLICE), 128, 256);
-                const unsigned acc = (s > 0 || j > 0) ? 1u : 0u;
+            const unsigned base = smem_u32(smem + (s % ST) * stage_bytes);
+#pragma unroll 1
+            for (int tap = 0; tap < 9; tap++) {
+                const unsigned off = (unsigned)(((tap / 3) * Wp + tap % 3) * 16);
+                const uint64_t ad = umma_desc(base + off, (unsigned)plane, 128);
+                const uint64_t bd = umma_desc(base + bwt + tap * N * 32, 128, 256);
+                const unsigned acc = (s > 0 || tap > 0) ? 1u : 0u;
                 asm volatile(
                     "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
                     " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
                     "l"(ad), "l"(bd), "r"(idesc), "r"(acc));
             }
             asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
-                smem_u32(&mbar[st])));
+                smem_u32(&mbar[s % ST])));
         }
+        issued = s + 1;
+        // refill the buffer of stage s-1 with stage s+ST-1 once the MMAs of s-1 are done
+        const int nx = s + ST - 1;
+        if (nx < nstages) {
+            if (s >= 1 && !mbar_wait(smem_u32(&mbar[(s - 1) % ST]), ((s - 1) / ST) & 1, LIMIT)) {
+                if (lane == 0) atomicExch(&fail_sh, 1);
+            } else {
+                load_stage(nx);
+            }
+        }
+        cp_commit();
     }
+    cp_wait<0>();
+    __syncthreads();
     // the last commit covers every MMA of the block
-    if (!fail_sh && nstages > 0) {
-        const int last = nstages - 1;
-        if (!mbar_wait(smem_u32(&mbar[last & 1]), (last >> 1) & 1, LIMIT)) {
+    if (!fail_sh && issued > 0) {
+        const int last = issued - 1;
+        if (!mbar_wait(smem_u32(&mbar[last % ST]), (last / ST) & 1, LIMIT)) {
             if (lane == 0) atomicExch(&fail_sh, 1);
         }
     }
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
-    if (!fail_sh) {
-        // epilogue: warp w holds TMEM lanes 32w..32w+31 = pixel rows; 16 columns per load
-        const long long p = p0 + warp * 32 + lane;
+    // epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31 (tile rows) and the column
+    // half w / 4 (N = 16: warps 0-3 take all columns); 16 columns per load
+    constexpr int CW = N >= 32 ? N / 2 : N;
+    const int quad = warp & 3, chalf = warp >> 2;
+    if (!fail_sh && chalf * CW < N) {
+        // this lane's output pixel (pad positions are not stored)
+        const int pix = s_q[quad * 32 + lane + Wp + 1];
 #pragma unroll
-        for (int c0 = 0; c0 < N; c0 += 16) {
+        for (int c0 = chalf * CW; c0 < chalf * CW + CW; c0 += 16) {
             unsigned v[16];
-            const unsigned ta = tmem + ((unsigned)(warp * 32) << 16) + (unsigned)c0;
+            const unsigned ta = tmem + ((unsigned)(quad * 32) << 16) + (unsigned)c0;
             asm volatile(
                 "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
                 "[%16];\n"
@@ -683,7 +715,7 @@ __global__ void __launch_bounds__(128) conv3x3_tc_kernel(const bf16* __restrict_
                   "=r"(v[15])
                 : "r"(ta));
             asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::);
-            if (p < P) {
+            if (pix >= 0) {
 #pragma unroll
                 for (int e = 0; e < 16; e += 2) {
                     const int co = n0 + c0 + e;
@@ -697,13 +729,13 @@ __global__ void __launch_bounds__(128) conv3x3_tc_kernel(const bf16* __restrict_
                         a = fmaxf(a, 0.f);
                         b = fmaxf(b, 0.f);
                     }
-                    bf16* o = out + p * out_cs + out_co + co;
+                    bf16* o = out + (long long)pix * out_cs + out_co + co;
                     if (co + 1 < Cout) *reinterpret_cast<__nv_bfloat162*>(o) = __floats2bfloat162_rn(a, b);
                     else o[0] = __float2bfloat16_rn(a);
                 }
             }
         }
-    } else if (tid == 0) {
+    } else if (fail_sh && tid == 0) {
         atomicExch(err, 1);
     }
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
@@ -714,18 +746,36 @@ __global__ void __launch_bounds__(128) conv3x3_tc_kernel(const bf16* __restrict_
     }
 }
 
+// Stages of the ring: as many (2..4) as fit in 110 KB, so that two blocks share an SM.
+template <int N, int ST>
+static cudaError_t launch_conv_tc_st(const bf16* in, int in_cs, int in_co, int Cin, const bf16* W, const float* bias,
+                                     bf16* out, int out_cs, int out_co, int Cout, int B, int H, int Wd, int relu,
+                                     int* err, cudaStream_t st, int band, int stage_bytes) {
+    const int smem = ST * stage_bytes;
+    cudaError_t e = cudaFuncSetAttribute(conv3x3_tc_kernel<N, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    const long long positions = (long long)B * (H + 1) * (Wd + 1);
+    dim3 grid((unsigned)((positions + 127) / 128), (unsigned)((Cout + N - 1) / N));
+    conv3x3_tc_kernel<N, ST><<<grid, 256, smem, st>>>(in, in_cs, in_co, Cin, W, bias, out, out_cs, out_co, Cout, B, H,
+                                                      Wd, relu, err, band, stage_bytes);
+    return cudaGetLastError();
+}
+
 template <int N>
 static cudaError_t launch_conv_tc(const bf16* in, int in_cs, int in_co, int Cin, const bf16* W, const float* bias,
                                   bf16* out, int out_cs, int out_co, int Cout, int B, int H, int Wd, int relu, int* err,
                                   cudaStream_t st) {
-    constexpr int smem = 2 * 4 * (128 * 32 + N * 32);
-    cudaError_t e = cudaFuncSetAttribute(conv3x3_tc_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    if (e != cudaSuccess) return e;
-    const long long P = (long long)B * H * Wd;
-    dim3 grid((unsigned)((P + 127) / 128), (unsigned)((Cout + N - 1) / N));
-    conv3x3_tc_kernel<N><<<grid, 128, smem, st>>>(in, in_cs, in_co, Cin, W, bias, out, out_cs, out_co, Cout, B, H, Wd,
-                                                  relu, err);
-    return cudaGetLastError();
+    const int band = 128 + 2 * (Wd + 1) + 2;
+    const int stage_bytes = ((2 * band * 16 + 9 * N * 32) + 127) / 128 * 128;
+    const int fit = (110 * 1024) / stage_bytes;
+    if (fit >= 4)
+        return launch_conv_tc_st<N, 4>(in, in_cs, in_co, Cin, W, bias, out, out_cs, out_co, Cout, B, H, Wd, relu, err,
+                                       st, band, stage_bytes);
+    if (fit == 3)
+        return launch_conv_tc_st<N, 3>(in, in_cs, in_co, Cin, W, bias, out, out_cs, out_co, Cout, B, H, Wd, relu, err,
+                                       st, band, stage_bytes);
+    return launch_conv_tc_st<N, 2>(in, in_cs, in_co, Cin, W, bias, out, out_cs, out_co, Cout, B, H, Wd, relu, err, st,
+                                   band, stage_bytes);
 }
 
 }  // namespace mm
@@ -735,8 +785,8 @@ static cudaError_t launch_conv_tc(const bf16* in, int in_cs, int in_co, int Cin,
 extern "C" MM_API int mm_nn_conv3x3_tc(const void* in, int in_cs, int in_co, int Cin, const void* W, const float* bias,
                                        void* out, int out_cs, int out_co, int Cout, int B, int H, int Wd, int relu,
                                        int* err, mm_stream st) {
-    if (Cin % 16 || in_cs % 8 || in_co % 8 || Cout < 1 || B < 1 || H < 1 || Wd < 1 || (out_co & 1) || (out_cs & 1) ||
-        !err)
+    if (Cin % 16 || in_cs % 8 || in_co % 8 || Cout < 1 || B < 1 || H < 1 || Wd < 1 || Wd > 256 || (out_co & 1) ||
+        (out_cs & 1) || !err)
         return report_error(MM_ERR_ARG, "mm_nn_conv3x3_tc: bad argument");
     cudaError_t e;
     const bf16* i = (const bf16*)in;

@@ -126,9 +126,12 @@ def test_training_lowers_the_loss():
 
 
 @pytest.mark.parametrize("cin,cout,B,H,W,relu", [(16, 32, 2, 8, 8, 1), (64, 128, 1, 16, 16, 0), (96, 32, 2, 8, 16, 1),
-                                                 (32, 16, 1, 4, 4, 0), (384, 128, 2, 16, 16, 1), (256, 256, 4, 8, 8, 1)])
+                                                 (32, 16, 1, 4, 4, 0), (384, 128, 2, 16, 16, 1), (256, 256, 4, 8, 8, 1),
+                                                 (32, 32, 2, 64, 64, 1), (16, 16, 3, 5, 7, 1), (48, 64, 2, 1, 9, 0)])
 def test_conv3x3_tcgen05_matches(cin, cout, B, H, W, relu):
-    """The tcgen05 convolution (TMEM accumulators) against the numpy oracle."""
+    """The tcgen05 convolution (TMEM accumulators, halo band over padded positions)
+    against the numpy oracle, including widths that are not multiples of 8, single-row
+    images and tiles that span several images."""
     import torch
     import unet_ref as R
     from mumax2 import _native as nat
