@@ -2199,6 +2199,20 @@ extern "C" MM_API int mm_save_async(mm_plan p, const char* path, int format, mm_
 // A batched plan as a pool of slots: finished simulations are replaced by new problems
 // while the others keep their state, so the GPU never waits for a batch's slowest member.
 
+// Stops the simulations in slots idx (their state and statistics stay as they are; the
+// slot counts as done until mm_batch_restart puts a new problem into it).
+extern "C" MM_API int mm_batch_cancel(mm_plan p, int count, const int* idx, mm_stream stream) {
+    if (!p || count < 0 || (count > 0 && !idx)) return set_err(MM_ERR_ARG, "bad argument");
+    for (int k = 0; k < count; k++)
+        if (idx[k] < 0 || idx[k] >= p->nsim) return set_err(MM_ERR_ARG, "slot %d out of range", idx[k]);
+    cudaStream_t st = (cudaStream_t)stream;
+    int rc = canonicalise(p, st);
+    if (rc) return rc;
+    if ((rc = read_ctl(p, st))) return rc;
+    for (int k = 0; k < count; k++) p->ctl_host[idx[k]].done = 1;
+    return write_ctl(p, st);
+}
+
 extern "C" MM_API int mm_batch_restart(mm_plan p, int count, const int* idx, const float* m, int from_host,
                                        const mm_sim* sims, const double* thr, long long max_steps,
                                        mm_stream stream) {

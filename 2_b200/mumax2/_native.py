@@ -207,6 +207,7 @@ _PROTOS = {
     "mm_plan_nsim": (C.c_int, [C.c_void_p]),
     "mm_batch_set_sims": (C.c_int, [C.c_void_p, C.c_void_p]),
     "mm_batch_stats": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "mm_batch_cancel": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
     "mm_batch_restart": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
                                     C.c_longlong, C.c_void_p]),
     "mm_batch_drive": (C.c_int, [C.c_void_p, C.c_int, C.c_longlong, C.c_void_p]),

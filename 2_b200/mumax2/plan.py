@@ -281,6 +281,11 @@ class Plan:
                                              C.cast(sa, C.c_void_p) if sa is not None else None,
                                              thr.ctypes.data_as(C.c_void_p), int(max_steps), None))
 
+    def batch_cancel(self, idx):
+        """Stops the simulations in slots idx (they count as done until restarted)."""
+        idx = np.ascontiguousarray(idx, dtype=np.int32)
+        nat.check(nat.lib().mm_batch_cancel(self.h, len(idx), idx.ctypes.data_as(C.c_void_p), None))
+
     def batch_drive(self, target_active=0, max_attempts=0):
         """Step until at most target_active simulations are still running."""
         nat.check(nat.lib().mm_batch_drive(self.h, int(target_active), int(max_attempts), None))

@@ -17,17 +17,37 @@ from . import unet as U
 from . import workloads as W
 
 
+def _tail_plan(plan, problem, masks0, sims0, slots, device, maxerr):
+    """The small plan (same geometry, `slots` simulations) that finishes a pool's last
+    relaxations; made once per main plan."""
+    from .plan import Plan
+    t = getattr(plan, "_tail_plan", None)
+    if t is None or t.nsim != slots:
+        t = Plan(problem, masks={"msat": np.concatenate([masks0] * slots)}, sims=[sims0] * slots,
+                 masks_per_sim=True, device=device)
+        plan._tail_plan = t
+    t.solver("rk23", dt=1e-14, maxerr=maxerr)
+    return t
+
+
 def relax_pool(problem, sims, masks, states, thr, slots=256, maxerr=1e-6, max_steps=100000, device=0,
-               keep_states=False, plan=None, accept=None, fallback=None, fallback_max_steps=100000):
+               keep_states=False, plan=None, accept=None, fallback=None, fallback_max_steps=100000,
+               tail_slots=16):
     """Relaxes problem q from states[q] until maxtorque < thr[q].  states: a list of host
     arrays or a float32 device tensor [nq][3N].  Returns a dict of arrays: steps,
     maxtorque, energy (J) and, with keep_states, the relaxed states.
 
     accept(q, steps, maxtorque, energy) -> bool and fallback (one host state): a relax that
     accept rejects is queued again at once, in the same pool, from the fallback state with
-    fallback_max_steps as its step limit; the
-    result arrays then hold the fallback's result, "first_*" arrays the first attempt's and
-    "fell_back" marks the problems concerned."""
+    fallback_max_steps as its step limit; the result arrays then hold the fallback's
+    result, "first_*" arrays the first attempt's and "fell_back" marks the problems
+    concerned.
+
+    Drain phase: once nothing is queued and at most tail_slots relaxations are left, they
+    move (state, scalars, mask and steps so far) to a plan of tail_slots simulations,
+    whose launches carry that many simulations' blocks instead of the pool's (a step of
+    the 256-slot pool costs about the same with one slot active as with all).  The moved
+    relaxations restart their step-size control from dt = 1e-14 s."""
     import collections
     import torch
     from .plan import Plan
@@ -40,10 +60,7 @@ def relax_pool(problem, sims, masks, states, thr, slots=256, maxerr=1e-6, max_st
         plan = Plan(problem, masks={"msat": np.concatenate(masks[:B])}, sims=sims[:B], masks_per_sim=True,
                     device=device)
     plan.solver("rk23", dt=1e-14, maxerr=maxerr)
-    mt = plan.mask_tensor("msat")
     on_dev = hasattr(states, "data_ptr")
-    slot = [-1] * B
-    retry = [False] * B
     queue = collections.deque((q, False) for q in range(nq))
     res = {"steps": np.zeros(nq, dtype=np.int64), "maxtorque": np.zeros(nq), "energy": np.zeros(nq)}
     if accept is not None:
@@ -52,15 +69,23 @@ def relax_pool(problem, sims, masks, states, thr, slots=256, maxerr=1e-6, max_st
     if keep_states:
         res["state"] = np.zeros((nq, 3 * N), dtype=np.float32)
     thr = np.asarray(thr)
+    # per slot of the current plan: problem, fallback flag, steps done before this plan
+    cur = plan
+    nslot = B
+    slot, retry, offset = [-1] * nslot, [False] * nslot, [0] * nslot
+
+    def restart(idx, m0, jobs, limits):
+        cur.batch_restart(idx, m0, thr[jobs], sims=[sims[q] for q in jobs], max_steps=limits)
 
     def fill(free):
+        mt = cur.mask_tensor("msat")
         idx, jobs, fb = [], [], []
         for b in free:
             if not queue:
                 break
             q, is_fb = queue.popleft()
             mt[b * N:(b + 1) * N].copy_(torch.from_numpy(np.asarray(masks[q], dtype=np.float32)))
-            slot[b], retry[b] = q, is_fb
+            slot[b], retry[b], offset[b] = q, is_fb, 0
             idx.append(b)
             jobs.append(q)
             fb.append(is_fb)
@@ -77,7 +102,32 @@ def relax_pool(problem, sims, masks, states, thr, slots=256, maxerr=1e-6, max_st
                 m0 = states[torch.tensor(js, device=states.device)]
             else:
                 m0 = np.stack([states[q] for q in js])
-            plan.batch_restart([idx[k] for k in sel], m0, thr[js], sims=[sims[q] for q in js], max_steps=limit)
+            restart([idx[k] for k in sel], m0, js, limit)
+
+    def migrate(st):
+        """Moves the running relaxations of the pool into the tail plan."""
+        nonlocal cur, nslot, slot, retry, offset
+        run = [b for b in range(nslot) if slot[b] >= 0]
+        state = cur.get_state()
+        tail = _tail_plan(plan, problem, masks[0], sims[0], tail_slots, device, maxerr)
+        mt = tail.mask_tensor("msat")
+        new_slot, new_retry, new_off = [-1] * tail_slots, [False] * tail_slots, [0] * tail_slots
+        m0, js, limits = [], [], []
+        for i, b in enumerate(run):
+            q = slot[b]
+            mt[i * N:(i + 1) * N].copy_(torch.from_numpy(np.asarray(masks[q], dtype=np.float32)))
+            new_slot[i], new_retry[i] = q, retry[b]
+            new_off[i] = offset[b] + st[b]["step"]
+            m0.append(state[3 * N * b:3 * N * (b + 1)])
+            js.append(q)
+            limits.append(max(1, (fallback_max_steps if retry[b] else max_steps) - new_off[i]))
+        cur.batch_cancel(run)
+        cur, nslot = tail, tail_slots
+        slot, retry, offset = new_slot, new_retry, new_off
+        # one restart per distinct remaining step limit
+        for lim in sorted(set(limits)):
+            sel = [i for i in range(len(run)) if limits[i] == lim]
+            restart(sel, np.stack([m0[i] for i in sel]), [js[i] for i in sel], lim)
 
     fill(range(B))
     done = 0
@@ -86,35 +136,44 @@ def relax_pool(problem, sims, masks, states, thr, slots=256, maxerr=1e-6, max_st
     t_all = time.perf_counter()
     while done < nq:
         t1 = time.perf_counter()
-        plan.batch_drive(target_active=max(0, B - refill) if queue else 0, max_attempts=0)
+        if cur is plan:
+            drain = tail_slots if nslot > tail_slots else 0
+            cur.batch_drive(target_active=max(0, nslot - refill) if queue else drain, max_attempts=0)
+        else:
+            cur.batch_drive(target_active=max(0, nslot - 1) if queue else 0, max_attempts=0)
         t_drive += time.perf_counter() - t1
-        st = plan.batch_stats()
-        free = [b for b in range(B) if slot[b] >= 0 and st[b]["done"]]
-        if not free:
-            continue
-        en = plan.batch_energy()
-        state = plan.get_state() if keep_states else None
-        for b in free:
-            q = slot[b]
-            res["steps"][q] = st[b]["step"]
-            res["maxtorque"][q] = st[b]["maxtorque"]
-            res["energy"][q] = en[b][4]
-            if keep_states:
-                res["state"][q] = state[3 * N * b:3 * N * (b + 1)]
-            slot[b] = -1
-            if accept is not None and not retry[b]:
-                res["first_steps"][q] = res["steps"][q]
-                res["first_maxtorque"][q] = res["maxtorque"][q]
-                res["first_energy"][q] = res["energy"][q]
-                if not accept(q, res["steps"][q], res["maxtorque"][q], res["energy"][q]):
-                    res["fell_back"][q] = True
-                    queue.appendleft((q, True))
-                    continue
-            done += 1
-        fill(free)
+        st = cur.batch_stats()
+        free = [b for b in range(nslot) if slot[b] >= 0 and st[b]["done"]]
+        if free:
+            en = cur.batch_energy()
+            state = cur.get_state() if keep_states else None
+            for b in free:
+                q = slot[b]
+                res["steps"][q] = offset[b] + st[b]["step"]
+                res["maxtorque"][q] = st[b]["maxtorque"]
+                res["energy"][q] = en[b][4]
+                if keep_states:
+                    res["state"][q] = state[3 * N * b:3 * N * (b + 1)]
+                slot[b] = -1
+                if accept is not None and not retry[b]:
+                    res["first_steps"][q] = res["steps"][q]
+                    res["first_maxtorque"][q] = res["maxtorque"][q]
+                    res["first_energy"][q] = res["energy"][q]
+                    if not accept(q, res["steps"][q], res["maxtorque"][q], res["energy"][q]):
+                        res["fell_back"][q] = True
+                        queue.appendleft((q, True))
+                        continue
+                done += 1
+            fill(free)
+        running = sum(1 for b in range(nslot) if slot[b] >= 0)
+        if cur is plan and nslot > tail_slots and not queue and 0 < running <= tail_slots:
+            migrate(cur.batch_stats())
     res["drive_s"] = t_drive
     res["host_s"] = time.perf_counter() - t_all - t_drive
     if own:
+        t = getattr(plan, "_tail_plan", None)
+        if t is not None:
+            t.close()
         plan.close()
     return res
 
@@ -244,6 +303,9 @@ def evaluate(net, problem, sims, masks, slots=256, device=0, energy_tol=1e-4, ma
                     accept=accept, fallback=cold)
     torch.cuda.synchronize()
     t_warm = time.perf_counter() - t0
+    t = getattr(plan, "_tail_plan", None)
+    if t is not None:
+        t.close()
     plan.close()
     fb = rw["fell_back"]
     erel = np.abs(rw["first_energy"] - rc["energy"]) / np.maximum(np.abs(rc["energy"]), 1e-30)

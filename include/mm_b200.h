@@ -243,6 +243,9 @@ MM_API int mm_autosave_read(mm_plan plan, float* states, double* times, int* cou
  * mm_batch_drive steps until at most target_active simulations are still running. */
 MM_API int mm_batch_restart(mm_plan plan, int count, const int* idx, const float* m, int from_host,
                             const mm_sim* sims, const double* thr, long long max_steps, mm_stream stream);
+/* Stops the simulations in slots idx[count]: they count as done (state and statistics
+ * kept) until mm_batch_restart reuses the slot. */
+MM_API int mm_batch_cancel(mm_plan plan, int count, const int* idx, mm_stream stream);
 MM_API int mm_batch_drive(mm_plan plan, int target_active, long long max_attempts, mm_stream stream);
 
 /* ---- per-simulation results of a (batched) plan; out arrays have nsim entries ---- */
