@@ -1011,6 +1011,17 @@ static int autotune(mm_plan p) {
     return rc;
 }
 
+extern "C" MM_API int mm_plan_demag_kernel(mm_plan p, float* out, int kd[3]) {
+    if (!p || !kd) return set_err(MM_ERR_ARG, "null argument");
+    if (!p->demag || !p->khat) return set_err(MM_ERR_STATE, "the plan has no demag kernel");
+    for (int i = 0; i < 3; i++) kd[i] = p->g.kd[i];
+    if (!out) return MM_OK;
+    const long long oct = (long long)p->g.kd[0] * p->g.kd[1] * p->g.kd[2];
+    const float* src = p->khat_d ? p->khat_d : p->khat;
+    CUCHK(cudaMemcpy(out, src, sizeof(float) * 6 * (size_t)oct, cudaMemcpyDeviceToHost));
+    return MM_OK;
+}
+
 extern "C" MM_API int mm_plan_tiles(mm_plan p, int* tiles, double* eval_us) {
     if (!p || !tiles) return set_err(MM_ERR_ARG, "null argument");
     for (int d = 0; d < 3; d++) tiles[d] = p->tiles[d];

@@ -202,6 +202,7 @@ _PROTOS = {
     "mm_save_wait": (C.c_int, [C.c_void_p]),
     "mm_tabulate_read": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "mm_plan_create_batch": (C.c_int, [C.POINTER(MMProblem), C.c_int, C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]),
+    "mm_plan_demag_kernel": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "mm_plan_tiles": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "mm_plan_set_tiles": (C.c_int, [C.c_void_p, C.c_void_p]),
     "mm_plan_nsim": (C.c_int, [C.c_void_p]),

@@ -100,6 +100,15 @@ class Plan:
         nat.check(nat.lib().mm_plan_tiles(self.h, t, C.byref(us)))
         return list(t[:]), us.value
 
+    def demag_kernel(self):
+        """The transformed demag tensor octant [6][kd0][kd1][kd2] (xx yy zz yz xz xy,
+        internal axes), scaled by 1/(L0 L1 L2)."""
+        kd = (C.c_int * 3)()
+        nat.check(nat.lib().mm_plan_demag_kernel(self.h, None, kd))
+        out = np.zeros((6, kd[0], kd[1], kd[2]), dtype=np.float32)
+        nat.check(nat.lib().mm_plan_demag_kernel(self.h, out.ctypes.data_as(C.c_void_p), kd))
+        return out
+
     def set_tiles(self, tiles):
         nat.check(nat.lib().mm_plan_set_tiles(self.h, (C.c_int * 3)(*tiles)))
 

@@ -160,6 +160,62 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------- CPU baseline (oracle)
+def reference_gpu_baseline(device, ref_steps=10, our_steps=50):
+    """The reference's own CUDA kernels on this GPU (oracle/ref_gpu.py: libmumax2 built
+    from the reference's sources, driven by a restatement of its Go RK12 loop, cuFFT for
+    the transforms) against this repository's fused path with the same solver (RK12,
+    the reference's adaptive solver; it has no RK23), configuration and initial state.
+    CUDA-event timing of whole steps after 3 warm-up steps; the reference path's host
+    syncs are part of its step, as in the reference."""
+    import torch
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ref_gpu as R
+    from mumax2 import Plan
+    if not R.available():
+        return {"unavailable": "reference library not built (oracle/build_ref.sh)"}
+    w = WORKLOAD
+    n = w["n"]
+    N = n[0] * n[1] * n[2]
+    plan = Plan(problem(), device=device)
+    ref = R.RefPath(n, w["cell"], w["msat"], w["aex"], w["alpha"], w["gamma"], w["ku"], w["anisu"],
+                    plan.demag_kernel(), dt=w["dt0"], maxerr=w["maxerr"])
+    m0 = initial_m(0)
+    ref.set_state(m0)
+    for _ in range(3):
+        ref.step()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    s0, e0 = ref.step_count, ref.evals
+    a.record()
+    for _ in range(ref_steps):
+        ref.step()
+    b.record()
+    torch.cuda.synchronize()
+    ref_ms = a.elapsed_time(b)
+    ref_evals = (ref.evals - e0) / (ref.step_count - s0)
+    del ref
+    plan.solver("rk12", dt=w["dt0"], maxerr=w["maxerr"])
+    plan.set_state(m0)
+    plan.steps(3)
+    torch.cuda.synchronize()
+    st0 = plan.stats()
+    a.record()
+    plan.steps(our_steps)
+    b.record()
+    torch.cuda.synchronize()
+    our_ms = a.elapsed_time(b)
+    st1 = plan.stats()
+    plan.close()
+    ref_v = N * ref_steps / (ref_ms * 1e-3)
+    our_v = N * our_steps / (our_ms * 1e-3)
+    return {"value": ref_v, "unit": "cell-steps/s", "kind": "reference libmumax2 kernels + cuFFT on this GPU",
+            "solver": "rk12", "steps": ref_steps, "ms_per_step": ref_ms / ref_steps,
+            "evals_per_step": ref_evals,
+            "ours_rk12": {"value": our_v, "ms_per_step": our_ms / our_steps, "steps": our_steps,
+                          "evals_per_step": (st1["evals"] - st0["evals"]) / our_steps},
+            "ours_over_reference": our_v / ref_v}
+
+
 def cpu_baseline(max_seconds=25.0):
     """FP64 oracle on the host cores: RK23 steps of the same workload (bounded)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -588,6 +644,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-ref-gpu", action="store_true",
+                    help="skip the reference-kernels-on-this-GPU comparison (RK12) of the film workload")
     ap.add_argument("--profile-reps", type=int, default=10)
     ap.add_argument("--profile-only", action="store_true",
                     help="only time the passes of one field evaluation (few launches; for ncu captures)")
@@ -722,6 +780,12 @@ def main():
             cb = cpu_baseline()
         except Exception as ex:  # reported, not fatal
             cb = {"value": None, "unit": "cell-steps/s", "cores": None, "kind": "port", "sample": f"failed: {ex}"}
+    rg = None
+    if rank == 0 and world == 1 and not args.no_ref_gpu:
+        try:
+            rg = reference_gpu_baseline(local_rank)
+        except Exception as ex:  # reported, not fatal
+            rg = {"unavailable": f"failed: {ex}"}
 
     if rank == 0:
         line = {
@@ -745,6 +809,7 @@ def main():
             "gpu_launches": int(launches),
             "clocks": clocks,
             "cpu_baseline": cb if cb is None else {k: cb[k] for k in ["value", "unit", "cores", "kind", "sample"]},
+            "reference_gpu": rg,
         }
         print(json.dumps(line), flush=True)
     plan.close()

@@ -139,6 +139,12 @@ MM_API int mm_plan_nsim(mm_plan plan);
  * timed evaluation with the chosen tiles (0 if not tuned).  Results do not depend on the
  * tiles (energies up to the order of their block partial sums). */
 MM_API int mm_plan_tiles(mm_plan plan, int tiles[3], double* eval_us);
+/* The plan's transformed demag tensor, one octant: out[6][kd0][kd1][kd2] (host, may be
+ * NULL to query kd), components xx yy zz yz xz xy in internal axis order, scaled by
+ * 1/(L0 L1 L2) like the reference's fftKern (maxwell_convolution.go:576-612); the other
+ * octants follow by symmetry (even along every axis for the diagonal, odd along s and d
+ * for K_sd).  For demagexch plans this is the demag part alone. */
+MM_API int mm_plan_demag_kernel(mm_plan plan, float* out, int kd[3]);
 MM_API int mm_plan_set_tiles(mm_plan plan, const int tiles[3]);
 /* Replaces the per-simulation scalars of a batched plan. */
 MM_API int mm_batch_set_sims(mm_plan plan, const mm_sim* sims);

@@ -29,9 +29,8 @@ def _libs():
     ours.setUsedGPUs((C.c_int * 1)(torch.cuda.current_device()), 1)
     libs = [("b200", ours)]
     if os.path.exists(REF_LIB):
-        ref = C.CDLL(REF_LIB)
-        ref.setUsedGPUs((C.c_int * 1)(torch.cuda.current_device()), 1)
-        libs.append(("ref", ref))
+        import ref_gpu
+        libs.append(("ref", ref_gpu.ref_lib()))
     return libs
 
 
