@@ -238,12 +238,14 @@ class UNet:
         return self.buf["out"]
 
     # ---- loss and backward
-    def set_target(self, target, mask):
-        """target float32 [B][H*W][3] (user order), mask float32 [B][H*W]."""
+    def set_target(self, target, mask, mask_count=None):
+        """target float32 [B][H*W][3] (user order), mask float32 [B][H*W]; mask_count (the
+        sum of the mask, if the caller knows it) spares a device-to-host read."""
         torch = self.torch
         self.target = torch.as_tensor(target, device=self.device, dtype=torch.float32).reshape(-1).contiguous()
         self.mask = torch.as_tensor(mask, device=self.device, dtype=torch.float32).reshape(-1).contiguous()
-        self.norm = float(max(1.0, self.mask.sum().item()) * 3.0)
+        cnt = float(mask_count) if mask_count is not None else float(self.mask.sum().item())
+        self.norm = max(1.0, cnt) * 3.0
 
     def loss_and_grad(self):
         L = nat.lib()

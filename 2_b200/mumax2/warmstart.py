@@ -200,7 +200,9 @@ class Dataset:
         dev = torch.device("cuda", device)
         self.feats = torch.tensor(U.features(sims, masks, n), device=dev)
         self.targets = torch.tensor(np.stack([U.target_from_state(s, n) for s in states]), device=dev)
-        self.masks = torch.tensor(np.stack([np.asarray(m, dtype=np.float32) for m in masks]), device=dev)
+        mk = np.stack([np.asarray(m, dtype=np.float32) for m in masks])
+        self.masks = torch.tensor(mk, device=dev)
+        self.mask_counts = mk.sum(axis=1).astype(np.float64)   # host copy: no device read per batch
 
     def __len__(self):
         return self.feats.shape[0]
@@ -226,13 +228,15 @@ def train(data, epochs=20, batch=256, lr=1e-3, seed=0, device=0, log=None, tcgen
     total = epochs * nb
     k = 0
     for ep in range(epochs):
-        perm = torch.tensor(rng.permutation(len(data))[:nb * batch], device=data.feats.device)
+        perm_h = rng.permutation(len(data))[:nb * batch]
+        perm = torch.tensor(perm_h, device=data.feats.device)
         acc = torch.zeros((), device=data.feats.device)
         for i in range(nb):
             idx = perm[i * batch:(i + 1) * batch]
             net.set_input(data.feats[idx])
             net.forward()
-            net.set_target(data.targets[idx], data.masks[idx])
+            net.set_target(data.targets[idx], data.masks[idx],
+                           mask_count=data.mask_counts[perm_h[i * batch:(i + 1) * batch]].sum())
             acc += net.loss_and_grad()[0]
             net.backward()
             warm = min(1.0, (k + 1) / max(1, total // 20))

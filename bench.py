@@ -216,6 +216,37 @@ def reference_gpu_baseline(device, ref_steps=10, our_steps=50):
             "ours_over_reference": our_v / ref_v}
 
 
+def cufft_comparator(L, our_eval_ms, reps=20):
+    """cuFFT (through torch.fft) as a timing comparator only: the 3-D R2C and C2R of the
+    three magnetisation components on the zero-padded volume L, the transforms the
+    reference's FFTPlanX runs per field evaluation, against this repository's five passes
+    of one evaluation (transforms, kernel multiply and the whole field/torque epilogue).
+    CUDA events, 3 warm-up repetitions."""
+    import torch
+    x = torch.randn(3, *L, device="cuda")
+    spec = torch.fft.rfftn(x, dim=(1, 2, 3))
+    y = torch.empty_like(x)
+    for _ in range(3):
+        torch.fft.rfftn(x, dim=(1, 2, 3), out=spec)
+        torch.fft.irfftn(spec, s=L, dim=(1, 2, 3), out=y)
+    a, b, c = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    torch.cuda.synchronize()
+    fwd = inv = 0.0
+    for _ in range(reps):
+        a.record()
+        torch.fft.rfftn(x, dim=(1, 2, 3), out=spec)
+        b.record()
+        torch.fft.irfftn(spec, s=L, dim=(1, 2, 3), out=y)
+        c.record()
+        torch.cuda.synchronize()
+        fwd += a.elapsed_time(b)
+        inv += b.elapsed_time(c)
+    fwd, inv = fwd / reps, inv / reps
+    return {"cufft_r2c_ms": fwd, "cufft_c2r_ms": inv, "cufft_transforms_ms": fwd + inv,
+            "ours_eval_ms": our_eval_ms, "cufft_transforms_over_ours_eval": (fwd + inv) / our_eval_ms,
+            "padded": list(L), "components": 3}
+
+
 def cpu_baseline(max_seconds=25.0):
     """FP64 oracle on the host cores: RK23 steps of the same workload (bounded)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -780,6 +811,12 @@ def main():
             cb = cpu_baseline()
         except Exception as ex:  # reported, not fatal
             cb = {"value": None, "unit": "cell-steps/s", "cores": None, "kind": "port", "sample": f"failed: {ex}"}
+    fc = None
+    if rank == 0 and world == 1 and not args.no_ref_gpu:
+        try:
+            fc = cufft_comparator(tuple(geo["L"]), sum(pass_ms))
+        except Exception as ex:  # reported, not fatal
+            fc = {"unavailable": f"failed: {ex}"}
     rg = None
     if rank == 0 and world == 1 and not args.no_ref_gpu:
         try:
@@ -810,6 +847,7 @@ def main():
             "clocks": clocks,
             "cpu_baseline": cb if cb is None else {k: cb[k] for k in ["value", "unit", "cores", "kind", "sample"]},
             "reference_gpu": rg,
+            "fft_comparator": fc,
         }
         print(json.dumps(line), flush=True)
     plan.close()
