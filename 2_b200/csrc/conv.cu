@@ -672,6 +672,82 @@ __global__ void __launch_bounds__(512) xfwd4_kernel(const float* __restrict__ in
     }
 }
 
+// Column pass of single-layer films (lines along y, kz = 0) with the four-step
+// transform: the three components of TC columns are loaded straight into registers
+// (3 x TC x P2 threads, rows n >= n_in are the zero padding and are not read), transformed,
+// put in natural order in shared memory, multiplied by the symmetric kernel there (all
+// three components of a (ky, kx) point meet in one thread), taken back into registers
+// and inverse-transformed; only the rows n < n_in are stored.  Replaces the Stockham
+// colmul_kernel for 2-D films (seven barrier-separated stages per transform and
+// component there, two barriers per transform here).
+template <int L>
+__global__ void __launch_bounds__(384) colmul4_kernel(float2* __restrict__ S, KernelView K, int ncols,
+                                                      long long comp_stride, long long line_stride, int n_in,
+                                                      float scale, const float2* __restrict__ tw, const DevCtl* ctl,
+                                                      int skip_retry, long long sim_stride,
+                                                      const float* __restrict__ sim_scale, int TC, int cstride) {
+    if (ctl) ctl += blockIdx.y;
+    if (conv_skip(ctl, skip_retry)) return;
+    S += blockIdx.y * sim_stride;
+    if (sim_scale) scale = sim_scale[blockIdx.y];
+    using F = FS<L>;
+    extern __shared__ unsigned char smem_raw[];
+    float2* sm = reinterpret_cast<float2*>(smem_raw);
+    const int per = TC * F::P2;                    // threads per component
+    const int c = threadIdx.x / per, r = threadIdx.x - c * per;
+    const int col = r % TC, t = r / TC;
+    const int kx0 = blockIdx.x * TC;
+    const bool active = c < 3 && kx0 + col < ncols;
+    float2* line = sm + ((c < 3 ? c : 0) * TC + col) * cstride;
+    float2* twt = sm + 3 * TC * cstride;
+    F::fill_twiddles(twt, tw);
+    float2* base = S + (long long)(c < 3 ? c : 0) * comp_stride + kx0 + col;
+    float2 v[F::P1];
+#pragma unroll
+    for (int j = 0; j < F::P1; j++) {
+        const int n = F::in_index(t, j);
+        v[j] = (active && n < n_in) ? base[n * line_stride] : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+    F::template run<-1>(v, line, t, active, twt, TC);
+    if (active) {
+#pragma unroll
+        for (int q = 0; q < F::P1; q++) line[F::out_index(t, q)] = v[q];
+    }
+    __syncthreads();
+    // symmetric kernel multiply at every (ky, kx) of the tile
+    const int nh = min(TC, ncols - kx0);
+    for (int e = threadIdx.x; e < L * TC; e += blockDim.x) {
+        const int ky = e / TC, c2 = e - ky * TC;
+        if (c2 >= nh) continue;
+        float kk[6];
+        kernel_at(K, 0, ky, kx0 + c2, kk);
+        float2* l0 = sm + (0 * TC + c2) * cstride + ky;
+        float2* l1 = sm + (1 * TC + c2) * cstride + ky;
+        float2* l2 = sm + (2 * TC + c2) * cstride + ky;
+        const float2 m0 = *l0, m1 = *l1, m2 = *l2;
+        // q: 0 xx, 1 yy, 2 zz, 3 yz, 4 xz, 5 xy
+        *l0 = make_float2(scale * (kk[0] * m0.x + kk[5] * m1.x + kk[4] * m2.x),
+                          scale * (kk[0] * m0.y + kk[5] * m1.y + kk[4] * m2.y));
+        *l1 = make_float2(scale * (kk[5] * m0.x + kk[1] * m1.x + kk[3] * m2.x),
+                          scale * (kk[5] * m0.y + kk[1] * m1.y + kk[3] * m2.y));
+        *l2 = make_float2(scale * (kk[4] * m0.x + kk[3] * m1.x + kk[2] * m2.x),
+                          scale * (kk[4] * m0.y + kk[3] * m1.y + kk[2] * m2.y));
+    }
+    __syncthreads();
+    if (active) {
+#pragma unroll
+        for (int j = 0; j < F::P1; j++) v[j] = line[F::in_index(t, j)];
+    }
+    __syncthreads();
+    F::template run<+1>(v, line, t, active, twt, TC);
+#pragma unroll
+    for (int q = 0; q < F::P1; q++) {
+        const int n = F::out_index(t, q);
+        if (active && n < n_in) base[n * line_stride] = v[q];
+    }
+}
+
 // ---------------------------------------------------------------- launch helpers
 template <typename KT> static cudaError_t set_smem(KT kern, size_t bytes) {
     if (bytes > 48 * 1024) return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
@@ -828,10 +904,41 @@ static cudaError_t launch_colmul_t(float2* S, const KernelView& K, int ncols, in
     return cudaGetLastError();
 }
 
+template <int L>
+static cudaError_t launch_colmul4_t(float2* S, const KernelView& K, int ncols, long long comp_stride,
+                                    long long line_stride, int n_in, float scale, const float2* tw,
+                                    const DevCtl* ctl, int skip_retry, cudaStream_t st, int nsim,
+                                    long long sim_stride, const float* sim_scale, int tile) {
+    using F = FS<L>;
+    // columns per block: 64 / P2 (192 threads) by default, halved or doubled by the tile
+    int TC = shifted((64 / F::P2) > 0 ? 64 / F::P2 : 1, tile);
+    if (TC < 1 || TC > 32 || 3 * TC * F::P2 > 384) TC = (64 / F::P2) > 0 ? 64 / F::P2 : 1;
+    if (TC > 32) TC = 32;
+    const int cstride = col4_stride<L>(TC < 16 ? TC : 16) > F::LBUF ? col4_stride<L>(TC < 16 ? TC : 16) : F::LBUF;
+    const size_t smem = (size_t)(3 * TC * cstride + F::TWT) * sizeof(float2);
+    cudaError_t e = set_smem(colmul4_kernel<L>, smem);
+    if (e != cudaSuccess) return e;
+    int threads = 3 * TC * F::P2;
+    if (threads < 32) threads = 32;
+    const int ntiles = (ncols + TC - 1) / TC;
+    colmul4_kernel<L><<<dim3((unsigned)ntiles, (unsigned)nsim), threads, smem, st>>>(
+        S, K, ncols, comp_stride, line_stride, n_in, scale, tw, ctl, skip_retry, sim_stride, sim_scale, TC, cstride);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_colmul(int L, float2* S, const KernelView& K, int ncols, int nouter, long long comp_stride,
                           long long outer_stride, long long line_stride, int n_in, int kaxis, float scale,
                           const float2* tw, const DevCtl* ctl, int skip_retry, cudaStream_t st, int nsim,
-                          long long sim_stride, const float* sim_scale) {
+                          long long sim_stride, const float* sim_scale, int tile) {
+    if (kaxis == 1 && nouter == 1 && L >= 4 && L <= 1024) {
+        // single-layer films: the four-step column pass
+        switch (L) {
+#define X(l) case l: return launch_colmul4_t<l>(S, K, ncols, comp_stride, line_stride, n_in, scale, tw, ctl, skip_retry, st, nsim, sim_stride, sim_scale, tile);
+            X(4) X(8) X(16) X(32) X(64) X(128) X(256) X(512) X(1024)
+#undef X
+            default: break;
+        }
+    }
     switch (L) {
 #define X(l) case l: return launch_colmul_t<l>(S, K, ncols, nouter, comp_stride, outer_stride, line_stride, n_in, kaxis, scale, tw, ctl, skip_retry, st, nsim, sim_stride, sim_scale);
         MM_FOR_POW2(X)

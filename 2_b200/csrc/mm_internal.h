@@ -218,7 +218,7 @@ cudaError_t launch_colfft(int L, int sign, V* S, int ncols, int nouter, long lon
 cudaError_t launch_colmul(int L, float2* S, const KernelView& K, int ncols, int nouter, long long comp_stride,
                           long long outer_stride, long long line_stride, int n_in, int kaxis, float scale,
                           const float2* tw, const DevCtl* ctl, int skip_retry, cudaStream_t st, int nsim = 1,
-                          long long sim_stride = 0, const float* sim_scale = nullptr);
+                          long long sim_stride = 0, const float* sim_scale = nullptr, int tile = 0);
 cudaError_t launch_zmul_reg(int P, float2* S, const KernelView& K, int L1, int h, int hp, long long comp_stride,
                             long long zstride, float scale, const float2* tw, const DevCtl* ctl, int skip_retry,
                             cudaStream_t st, int nsim = 1, long long sim_stride = 0,

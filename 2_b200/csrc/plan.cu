@@ -873,7 +873,7 @@ static int launch_conv(mm_plan p, PP m_in, const DevCtl* ctl, int skip_retry, cu
     if ((rc = mark())) return rc;
     if (L0 == 1) {
         CUCHK(launch_colmul(L1, p->S, p->kv, g.h, 1, plane, 0, g.hp, n1, 1, scale, p->tw, ctl, skip_retry, st, ns, sb,
-                            sim_scale));
+                            sim_scale, p->tiles[1]));
         if ((rc = mark())) return rc;
     } else {
         CUCHK(launch_colfft<float2>(L1, -1, p->S, g.h, 3 * n0, plane, g.hp, n1, L1, p->tw, ctl, skip_retry, st, ns,
@@ -944,8 +944,9 @@ static StageOp op_blank() {
 // ---------------------------------------------------------------- tile autotuner
 // Times whole field evaluations (torque of a zeroed state, the plan's own buffers and
 // masks) for the tile variants of the four-step passes: rows per block of the R2C row
-// pass (1/2, 1, 2 x default), columns per block of the column passes (1/2, 1, 2 x) and
-// rows per block of the C2R + epilogue pass (1/2, 1 x).  One pass at a time from the
+// pass (1/2, 1, 2 x default), columns per block of the column passes (the y FFTs of 3-D
+// grids, the y FFT + kernel multiply of single-layer films; 1/2, 1, 2 x) and rows per
+// block of the C2R + epilogue pass (1/2, 1 x).  One pass at a time from the
 // defaults (coordinate descent); a variant replaces the current choice only when it is
 // more than 2 % faster.  Runs once at plan creation; MM_AUTOTUNE=0 in the environment
 // keeps the defaults.  Tile variants change the block decomposition only: every cell's
@@ -990,7 +991,6 @@ static int autotune(mm_plan p) {
     }
     const int lo[3] = {-1, -1, -1}, hi[3] = {1, 1, 0};
     for (int d = 0; d < 3 && !rc; d++) {
-        if (d == 1 && p->g.L[0] == 1) continue;  // single-layer films have no column FFT pass
         int keep = p->tiles[d];
         for (int v = lo[d]; v <= hi[d] && !rc; v++) {
             if (v == keep) continue;
