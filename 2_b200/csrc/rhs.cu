@@ -602,9 +602,19 @@ __host__ __device__ constexpr int xinv4_rpb() {
     return (384 / (3 * FS<M>::P2)) > 0 ? 384 / (3 * FS<M>::P2) : 1;
 }
 
-template <int M, bool TERMS, bool BATCH>
-__global__ void __launch_bounds__(384) xinv4_epi_kernel(const float2* __restrict__ S, int hp, int L1,
-                                                        const float2* __restrict__ tw, EpiArgs A, int RPB) {
+// Rows per block of the four-step epilogue: the default, or half of it (the autotuner's
+// other variant; at least 32 threads).  A compile-time constant, so that the row loops
+// of the epilogue unroll and its register budget stays that of a fixed tile.
+template <int M, bool HALF>
+__host__ __device__ constexpr int xinv4_rows_c() {
+    return (HALF && xinv4_rpb<M>() >= 2 && (xinv4_rpb<M>() / 2) * 3 * FS<M>::P2 >= 32) ? xinv4_rpb<M>() / 2
+                                                                                          : xinv4_rpb<M>();
+}
+
+template <int M, bool TERMS, bool BATCH, bool HALF>
+__device__ __forceinline__ void xinv4_epi_body(const float2* __restrict__ S, int hp, int L1,
+                                               const float2* __restrict__ tw, const EpiArgs& A) {
+    constexpr int RPB = xinv4_rows_c<M, HALF>();
     const DevCtl* ctl = A.ctl ? A.ctl + blockIdx.y : nullptr;
     if (skip_eval(ctl, A.skip_retry)) return;
     S += blockIdx.y * A.spec_bstride;
@@ -652,6 +662,22 @@ __global__ void __launch_bounds__(384) xinv4_epi_kernel(const float2* __restrict
     const int row0 = blockIdx.x * RPB;
     epilogue_rows<TERMS, false, BATCH>(A, pick_scalars<BATCH>(s_sim, A.P.s), sm, F::LBUF, row0,
                                        min(RPB, nrows - row0));
+}
+
+// Single plans: launch bounds alone, so ptxas sizes the registers for the 384-thread tile
+// (78-80 registers); batched plans: two blocks per SM requested explicitly (their
+// staged-scalar variant would otherwise take 136-150 registers and one block).
+template <int M, bool TERMS, bool HALF>
+__global__ void __launch_bounds__(384) xinv4_epi_kernel(const float2* __restrict__ S, int hp, int L1,
+                                                        const float2* __restrict__ tw, EpiArgs A) {
+    xinv4_epi_body<M, TERMS, false, HALF>(S, hp, L1, tw, A);
+}
+
+template <int M, bool TERMS, bool HALF>
+__global__ void __launch_bounds__(384, M <= 512 ? 2 : 1) xinv4_epi_batch_kernel(const float2* __restrict__ S, int hp,
+                                                                                int L1, const float2* __restrict__ tw,
+                                                                                EpiArgs A) {
+    xinv4_epi_body<M, TERMS, true, HALF>(S, hp, L1, tw, A);
 }
 
 // ---------------------------------------------------------------- epilogue without demag
@@ -705,32 +731,44 @@ static cudaError_t launch_xinv_t(const float2* S, int hp, int L1, const float2* 
     return cudaGetLastError();
 }
 
-// Rows per block of the four-step epilogue: the default, or half of it (tile -1, the
-// autotuner's other variant; at least 32 threads).
 template <int M>
 static int xinv4_rows(int tile) {
-    const int r0 = xinv4_rpb<M>();
-    return (tile < 0 && r0 >= 2 && (r0 / 2) * 3 * FS<M>::P2 >= 32) ? r0 / 2 : r0;
+    return tile < 0 ? xinv4_rows_c<M, true>() : xinv4_rows_c<M, false>();
 }
 
-template <int M, bool TERMS, bool BATCH>
-static cudaError_t launch_xinv4_t(const float2* S, int hp, int L1, const float2* tw, const EpiArgs& A,
-                                  cudaStream_t st, int* nblocks, int nsim, int tile) {
-    const int RPB = xinv4_rows<M>(tile);
+template <int M, bool TERMS, bool BATCH, bool HALF>
+static cudaError_t launch_xinv4_h(const float2* S, int hp, int L1, const float2* tw, const EpiArgs& A,
+                                  cudaStream_t st, int* nblocks, int nsim) {
+    constexpr int RPB = xinv4_rows_c<M, HALF>();
     const size_t smem = (size_t)(RPB * 3 * FS<M>::LBUF + FS<M>::TWT) * sizeof(float2);
+    auto kern = BATCH ? xinv4_epi_batch_kernel<M, TERMS, HALF> : xinv4_epi_kernel<M, TERMS, HALF>;
     if (smem > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(xinv4_epi_kernel<M, TERMS, BATCH>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
+    }
+    // batched plans: two blocks per SM (the launch bounds) need the shared-memory carveout
+    // as well; single plans keep the default split, whose larger L1 serves the stencil's
+    // neighbour loads
+    if (BATCH) {
+        cudaError_t ec = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                              (int)cudaSharedmemCarveoutMaxShared);
+        if (ec != cudaSuccess) return ec;
     }
     const int nrows = A.P.n[0] * A.P.n[1];
     const int blocks = (nrows + RPB - 1) / RPB;
     int threads = RPB * 3 * FS<M>::P2;
     if (threads < 32) threads = 32;
     *nblocks = blocks;
-    xinv4_epi_kernel<M, TERMS, BATCH><<<dim3((unsigned)blocks, (unsigned)nsim), threads, smem, st>>>(S, hp, L1, tw,
-                                                                                                     A, RPB);
+    kern<<<dim3((unsigned)blocks, (unsigned)nsim), threads, smem, st>>>(S, hp, L1, tw, A);
     return cudaGetLastError();
+}
+
+template <int M, bool TERMS, bool BATCH>
+static cudaError_t launch_xinv4_t(const float2* S, int hp, int L1, const float2* tw, const EpiArgs& A,
+                                  cudaStream_t st, int* nblocks, int nsim, int tile) {
+    if (tile < 0 && xinv4_rows_c<M, true>() != xinv4_rows_c<M, false>())
+        return launch_xinv4_h<M, TERMS, BATCH, true>(S, hp, L1, tw, A, st, nblocks, nsim);
+    return launch_xinv4_h<M, TERMS, BATCH, false>(S, hp, L1, tw, A, st, nblocks, nsim);
 }
 
 static bool use_xinv4(int M) { return M >= 4 && M <= 1024; }
