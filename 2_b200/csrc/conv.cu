@@ -22,6 +22,7 @@
 #include "fft.cuh"
 #include "fft4.cuh"
 #include "mm_internal.h"
+#include "kernel_view.cuh"
 
 namespace mm {
 using namespace mmfft;
@@ -225,19 +226,6 @@ __global__ void colfft_kernel(V* __restrict__ S, int ncols, long long outer_stri
 // Three components per column: forward transform, H_d = sum_s Khat_sd M_s (symmetric,
 // real), inverse transform.  kaxis = 0: the line runs along z (ky = outer index);
 // kaxis = 1: the line runs along y (kz = 0, 2-D films).
-__device__ __forceinline__ void kernel_at(const KernelView& K, int kz, int ky, int kx, float out[6]) {
-    float sz = 1.f, sy = 1.f;
-    if (kz > (K.L0 >> 1)) { kz = K.L0 - kz; sz = -1.f; }
-    if (ky > (K.L1 >> 1)) { ky = K.L1 - ky; sy = -1.f; }
-    const int cs = K.kd0 * K.kd1 * K.kd2;
-    const int idx = (kz * K.kd1 + ky) * K.kd2 + kx;
-    // real-space K_sd is odd along axes s and d (s != d), so its transform flips sign
-    // under k -> L-k along those axes; diagonal components are even.
-    const float sg[6] = {1.f, 1.f, 1.f, sy, sz, sz * sy};
-#pragma unroll
-    for (int q = 0; q < 6; q++) out[q] = K.nz[q] ? sg[q] * __ldg(K.k + q * cs + idx) : 0.f;
-}
-
 template <int L>
 __global__ void colmul_kernel(float2* __restrict__ S, KernelView K, int ncols, long long comp_stride,
                               long long outer_stride, long long line_stride, int n_in, int kaxis, float scale,

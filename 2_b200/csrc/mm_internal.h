@@ -226,6 +226,12 @@ cudaError_t launch_zmul_reg(int P, float2* S, const KernelView& K, int L1, int h
 cudaError_t launch_xinv_epi(int M, const float2* S, int hp, int L1, const float2* tw, const EpiArgs& A, bool terms,
                             cudaStream_t st, int* nblocks, int nsim = 1, int tile = 0);
 cudaError_t launch_local_epi(const EpiArgs& A, bool terms, cudaStream_t st, int* nblocks, int nsim = 1);
+// fused single-layer evaluation (rhs.cu): convolution and epilogue in one launch, one
+// block per simulation; fused2d_ok tells whether a geometry is served
+bool fused2d_ok(const int n[3]);
+cudaError_t launch_fused2d(const float* in_mask, long long mask_bstride, const KernelView& K, float scale,
+                           const float* sim_scale, const float2* tw, const EpiArgs& A, cudaStream_t st, int* nblocks,
+                           int nsim);
 // solver/am12 (am12.cu)
 cudaError_t am_begin(DevCtl* ctl, int nsim, cudaStream_t st);
 cudaError_t am_update(PP y0, PP y, const float* dy, const float* dy0, const float* y1, DevCtl* ctl, long long N,

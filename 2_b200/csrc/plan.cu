@@ -444,7 +444,7 @@ struct mm_plan_s {
     long long bytes = 0;
     // autotuned tile variants (-1, 0, +1) of the row, column and epilogue passes, and the
     // evaluation time measured with them (0 if not tuned)
-    int tiles[3] = {0, 0, 0};
+    int tiles[4] = {0, 0, 0, 0};     // [3]: fused single-layer evaluation (fused2d_kernel)
     float tuned_us = 0.f;
     long long n3() const { return 3 * g.N; }
     long long spec_bstride() const { return 3LL * g.n[0] * g.L[1] * g.hp; }
@@ -917,6 +917,14 @@ static int launch_eval(mm_plan p, const StageOp& op, DevCtl* ctl, int skip_retry
     A.spec_bstride = p->spec_bstride();
     A.t_eval = p->t_eval;
     int nb = 0, rc;
+    if (p->demag && p->tiles[3] && !terms && fused2d_ok(g.n)) {
+        const float* in_mask = p->khat_d ? nullptr : p->P.msat_mask;
+        CUCHK(launch_fused2d(in_mask, p->P.mask_bstride, p->kv, (float)p->prob.msat,
+                             p->nsim > 1 ? p->d_sim_msat : nullptr, p->tw, A, st, &nb, p->nsim));
+        p->launches += 1;
+        if (nblocks_out) *nblocks_out = nb;
+        return MM_OK;
+    }
     if (p->demag) {
         if ((rc = launch_conv(p, op.m_in, ctl, skip_retry, st))) return rc;
         CUCHK(launch_xinv_epi(g.M, p->S, g.hp, g.L[1], p->tw, A, terms, st, &nb, p->nsim, p->tiles[2]));
@@ -948,8 +956,9 @@ static StageOp op_blank() {
 // grids, the y FFT + kernel multiply of single-layer films; 1/2, 1, 2 x) and rows per
 // block of the C2R + epilogue pass (1/2, 1 x).  One pass at a time from the
 // defaults (coordinate descent); a variant replaces the current choice only when it is
-// more than 2 % faster.  Runs once at plan creation; MM_AUTOTUNE=0 in the environment
-// keeps the defaults.  Tile variants change the block decomposition only: every cell's
+// more than 2 % faster.  Single-layer films whose half spectrum fits in shared memory also
+// try the fused evaluation (fused2d_kernel: convolution and epilogue in one launch).
+// Runs once at plan creation; MM_AUTOTUNE=0 in the environment keeps the defaults.  Tile variants change the block decomposition only: every cell's
 // arithmetic is the same, and so are the fields, torques and step sequences.
 static int autotune(mm_plan p) {
     if (!p->demag) return MM_OK;
@@ -1004,6 +1013,15 @@ static int autotune(mm_plan p) {
         }
         p->tiles[d] = keep;
     }
+    // single-layer films whose spectrum fits in shared memory: the fused evaluation
+    if (!rc && fused2d_ok(p->g.n)) {
+        p->tiles[3] = 1;
+        float t = 0.f;
+        if (!(rc = time_eval(&t))) {
+            if (t < 0.98f * best) best = t;
+            else p->tiles[3] = 0;
+        }
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     p->tuned_us = rc ? 0.f : best;
@@ -1024,7 +1042,7 @@ extern "C" MM_API int mm_plan_demag_kernel(mm_plan p, float* out, int kd[3]) {
 
 extern "C" MM_API int mm_plan_tiles(mm_plan p, int* tiles, double* eval_us) {
     if (!p || !tiles) return set_err(MM_ERR_ARG, "null argument");
-    for (int d = 0; d < 3; d++) tiles[d] = p->tiles[d];
+    for (int d = 0; d < 4; d++) tiles[d] = p->tiles[d];
     if (eval_us) *eval_us = p->tuned_us;
     return MM_OK;
 }
@@ -1033,7 +1051,10 @@ extern "C" MM_API int mm_plan_set_tiles(mm_plan p, const int* tiles) {
     if (!p || !tiles) return set_err(MM_ERR_ARG, "null argument");
     for (int d = 0; d < 3; d++)
         if (tiles[d] < -1 || tiles[d] > (d == 2 ? 0 : 1)) return set_err(MM_ERR_ARG, "tile %d out of range", d);
-    for (int d = 0; d < 3; d++) p->tiles[d] = tiles[d];
+    if (tiles[3] != 0 && tiles[3] != 1) return set_err(MM_ERR_ARG, "tile 3 must be 0 or 1");
+    if (tiles[3] && !fused2d_ok(p->g.n))
+        return set_err(MM_ERR_ARG, "the fused evaluation does not serve this geometry");
+    for (int d = 0; d < 4; d++) p->tiles[d] = tiles[d];
     free_graph(p);
     return MM_OK;
 }

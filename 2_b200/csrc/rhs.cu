@@ -18,6 +18,7 @@
 #include "fft.cuh"
 #include "fft4.cuh"
 #include "mm_internal.h"
+#include "kernel_view.cuh"
 
 namespace mm {
 using namespace mmfft;
@@ -678,6 +679,239 @@ __global__ void __launch_bounds__(384, M <= 512 ? 2 : 1) xinv4_epi_batch_kernel(
                                                                                 int L1, const float2* __restrict__ tw,
                                                                                 EpiArgs A) {
     xinv4_epi_body<M, TERMS, true, HALF>(S, hp, L1, tw, A);
+}
+
+static bool staged_scalars(const EpiArgs& A, int nsim);
+
+// ---------------------------------------------------------------- fused single-layer evaluation
+// One block per simulation of a single-layer film (n0 = 1) whose half spectrum
+// [3][N1][M+1] fits in shared memory: the R2C rows, the y transform with the kernel
+// multiply and its inverse, the C2R rows and the epilogue all run in one launch, and the
+// spectrum never leaves the SM.  Each phase uses the same four-step transforms and the
+// same arithmetic as the separate passes (xfwd4, colmul4, xinv4), so the results are
+// identical to theirs.  L1 = 2 N1 (padded column length), M = N2 (complex row length).
+template <int L1, int M>
+struct Fused2D {
+    using FR = FS<M>;
+    using FC = FS<L1>;
+    static constexpr int N1 = L1 / 2;
+    static constexpr int HP = M + 1;                             // spectrum row pitch (odd)
+    static constexpr int SPEC = 3 * N1 * HP;                     // float2
+    static constexpr int LPP = 512 / FR::P2;                     // row lines per pass
+    static constexpr int CC = (512 / (3 * FC::P2)) < 32 ? 512 / (3 * FC::P2) : 32;  // columns per batch
+    static constexpr int CSTR = FC::LBUF + ((FC::LBUF & 1) ? 0 : 1);                 // column line stride
+    static constexpr int RR = 512 / (3 * FR::P2);                // epilogue rows per chunk
+    static constexpr int W1 = LPP * FR::LBUF, W2 = 3 * CC * CSTR, W3 = 3 * RR * FR::LBUF;
+    static constexpr int WORK = W1 > W2 ? (W1 > W3 ? W1 : W3) : (W2 > W3 ? W2 : W3);
+    static constexpr int TOTAL = SPEC + WORK + FR::TWT + FC::TWT;  // float2
+    static constexpr size_t BYTES = (size_t)TOTAL * sizeof(float2);
+};
+
+template <int L1, int M, bool BATCH>
+__global__ void __launch_bounds__(512, 1) fused2d_kernel(const float* __restrict__ in_mask, long long mask_bstride,
+                                                         KernelView K, float scale, const float* __restrict__ sim_scale,
+                                                         const float2* __restrict__ tw, EpiArgs A) {
+    using G = Fused2D<L1, M>;
+    using FR = typename G::FR;
+    using FC = typename G::FC;
+    constexpr int N1 = G::N1, HP = G::HP;
+    const int sim = blockIdx.y;
+    const DevCtl* ctl = A.ctl ? A.ctl + sim : nullptr;
+    if (skip_eval(ctl, A.skip_retry)) return;
+    __shared__ SimScalars s_sim;
+    if (BATCH && threadIdx.x == 0) stage_scalars(A, ctl, s_sim);
+    if (sim_scale) scale = sim_scale[sim];
+    extern __shared__ unsigned char smem_raw[];
+    float2* sp = reinterpret_cast<float2*>(smem_raw);        // [3][N1][HP]
+    float2* work = sp + G::SPEC;
+    float2* twr = work + G::WORK;
+    float2* twc = twr + FR::TWT;
+    FR::fill_twiddles(twr, tw);
+    FC::fill_twiddles(twc, tw);
+    const int N2 = A.P.n[2];
+    const long long N = (long long)N1 * N2;
+    const float* m = A.op.m_in.get(ctl ? ctl->cur : 0) + (long long)sim * 3 * N;
+    const float* msk = in_mask ? in_mask + (long long)sim * mask_bstride : nullptr;
+    const int tid = threadIdx.x;
+
+    // ---- 1. R2C rows: (c, y) lines of 2M reals (N2 of them non-zero), packed complex
+    {
+        const int t = tid % FR::P2, ll = tid / FR::P2;
+        float2* buf = work + ll * FR::LBUF;
+        for (int l0 = 0; l0 < 3 * N1; l0 += G::LPP) {
+            const int l = l0 + ll;
+            const bool active = l < 3 * N1;
+            const int c = active ? l / N1 : 0, y = active ? l - c * N1 : 0;
+            const float* src = m + c * N + (long long)y * N2;
+            const float* mr = msk ? msk + (long long)y * N2 : nullptr;
+            float2 v[FR::P1];
+#pragma unroll
+            for (int j = 0; j < FR::P1; j++) {
+                const int n = FR::in_index(t, j);
+                float a = 0.f, b = 0.f;
+                if (active) {
+                    if (2 * n < N2) a = src[2 * n] * (mr ? mr[2 * n] : 1.f);
+                    if (2 * n + 1 < N2) b = src[2 * n + 1] * (mr ? mr[2 * n + 1] : 1.f);
+                }
+                v[j] = make_float2(a, b);
+            }
+            __syncthreads();
+            FR::template run<-1>(v, buf, t, active, twr, 1);
+            if (active) {
+#pragma unroll
+                for (int r = 0; r < FR::P1; r++) buf[FR::out_index(t, r)] = v[r];
+            }
+            __syncthreads();
+            if (active) {
+                float2* dst = sp + (c * N1 + y) * HP;
+                for (int k = t; k <= M / 2; k += FR::P2) {
+                    const float2 zk = buf[k & (M - 1)];
+                    const float2 zm = buf[(M - k) & (M - 1)];
+                    const float2 e = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
+                    const float2 od = make_float2(0.5f * (zk.y + zm.y), -0.5f * (zk.x - zm.x));
+                    const float2 w = TwSrc<-1, float2>::get(tw, k, 2 * M);
+                    dst[k] = cadd(e, cmul(w, od));
+                    if (k != M - k) dst[M - k] = cadd(cconj(e), cmul(make_float2(-w.x, w.y), cconj(od)));
+                }
+            }
+        }
+    }
+    __syncthreads();
+
+    // ---- 2. columns: forward y transform, symmetric kernel multiply, inverse
+    {
+        constexpr int CC = G::CC, CSTR = G::CSTR;
+        const int per = CC * FC::P2;
+        const int c = tid / per, r = tid - c * per;
+        const int col = r % CC, t = r / CC;
+        float2* line = work + ((c < 3 ? c : 0) * CC + col) * CSTR;
+        for (int kx0 = 0; kx0 < HP; kx0 += CC) {
+            const bool active = c < 3 && kx0 + col < HP;
+            const float2* colp = sp + (c < 3 ? c : 0) * N1 * HP + kx0 + col;
+            float2 v[FC::P1];
+#pragma unroll
+            for (int j = 0; j < FC::P1; j++) {
+                const int n = FC::in_index(t, j);
+                v[j] = (active && n < N1) ? colp[n * HP] : make_float2(0.f, 0.f);
+            }
+            __syncthreads();
+            FC::template run<-1>(v, line, t, active, twc, CC);
+            if (active) {
+#pragma unroll
+                for (int q = 0; q < FC::P1; q++) line[FC::out_index(t, q)] = v[q];
+            }
+            __syncthreads();
+            const int nh = min(CC, HP - kx0);
+            for (int e = tid; e < L1 * CC; e += blockDim.x) {
+                const int ky = e / CC, c2 = e - ky * CC;
+                if (c2 >= nh) continue;
+                float kk[6];
+                kernel_at(K, 0, ky, kx0 + c2, kk);
+                float2* l0 = work + (0 * CC + c2) * CSTR + ky;
+                float2* l1 = work + (1 * CC + c2) * CSTR + ky;
+                float2* l2 = work + (2 * CC + c2) * CSTR + ky;
+                const float2 m0 = *l0, m1 = *l1, m2 = *l2;
+                *l0 = make_float2(scale * (kk[0] * m0.x + kk[5] * m1.x + kk[4] * m2.x),
+                                  scale * (kk[0] * m0.y + kk[5] * m1.y + kk[4] * m2.y));
+                *l1 = make_float2(scale * (kk[5] * m0.x + kk[1] * m1.x + kk[3] * m2.x),
+                                  scale * (kk[5] * m0.y + kk[1] * m1.y + kk[3] * m2.y));
+                *l2 = make_float2(scale * (kk[4] * m0.x + kk[3] * m1.x + kk[2] * m2.x),
+                                  scale * (kk[4] * m0.y + kk[3] * m1.y + kk[2] * m2.y));
+            }
+            __syncthreads();
+            if (active) {
+#pragma unroll
+                for (int j = 0; j < FC::P1; j++) v[j] = line[FC::in_index(t, j)];
+            }
+            __syncthreads();
+            FC::template run<+1>(v, line, t, active, twc, CC);
+            if (active) {
+                float2* cold = sp + c * N1 * HP + kx0 + col;
+#pragma unroll
+                for (int q = 0; q < FC::P1; q++) {
+                    const int n = FC::out_index(t, q);
+                    if (n < N1) cold[n * HP] = v[q];
+                }
+            }
+            __syncthreads();
+        }
+    }
+
+    // ---- 3. C2R rows in chunks of RR, each followed by the epilogue of its rows
+    {
+        constexpr int RR = G::RR;
+        const int t = tid % FR::P2;
+        const int c = (tid / FR::P2) % 3;
+        const int lr = tid / (3 * FR::P2);
+        float2* buf = work + (lr < RR ? lr * 3 + c : 0) * FR::LBUF;
+        const SimScalars& S = pick_scalars<BATCH>(s_sim, A.P.s);
+        for (int row0 = 0; row0 < N1; row0 += RR) {
+            const int row = row0 + lr;
+            const bool active = lr < RR && row < N1;
+            const float2* src = sp + (c * N1 + (active ? row : 0)) * HP;
+            float2 v[FR::P1];
+#pragma unroll
+            for (int j = 0; j < FR::P1; j++) {
+                const int k = FR::in_index(t, j);
+                float2 val = make_float2(0.f, 0.f);
+                if (active) {
+                    const float2 a = src[k], b = src[M - k];
+                    const float2 s = make_float2(a.x + b.x, a.y - b.y);
+                    const float2 d = make_float2(a.x - b.x, a.y + b.y);
+                    const float2 wd = cmul(TwSrc<+1, float2>::get(tw, k, 2 * M), d);
+                    val = make_float2(s.x - wd.y, s.y + wd.x);
+                }
+                v[j] = val;
+            }
+            __syncthreads();
+            FR::template run<+1>(v, buf, t, active, twr, 1);
+            if (active) {
+#pragma unroll
+                for (int r = 0; r < FR::P1; r++) buf[FR::out_index(t, r)] = v[r];
+            }
+            __syncthreads();
+            epilogue_rows<false, false, BATCH>(A, S, work, FR::LBUF, row0, min(RR, N1 - row0));
+            __syncthreads();
+        }
+    }
+}
+
+// Whether the fused evaluation serves a single-layer geometry (n0 = 1, power-of-two N1,
+// N2 in 32..128 with N1 <= 64) within 227 KB of shared memory.
+bool fused2d_ok(const int n[3]) {
+    if (n[0] != 1) return false;
+    const int L1 = 2 * n[1], M = n[2];
+    size_t bytes = 0;
+#define F2(l, mm) if (L1 == l && M == mm) bytes = Fused2D<l, mm>::BYTES;
+    F2(32, 32) F2(32, 64) F2(32, 128) F2(64, 32) F2(64, 64) F2(64, 128) F2(128, 32) F2(128, 64) F2(128, 128)
+#undef F2
+    return bytes > 0 && bytes <= 227 * 1024;
+}
+
+template <int L1, int M>
+static cudaError_t launch_fused2d_t(const float* in_mask, long long mask_bstride, const KernelView& K, float scale,
+                                    const float* sim_scale, const float2* tw, const EpiArgs& A, bool batch,
+                                    cudaStream_t st, int nsim) {
+    using G = Fused2D<L1, M>;
+    auto kern = batch ? fused2d_kernel<L1, M, true> : fused2d_kernel<L1, M, false>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::BYTES);
+    if (e != cudaSuccess) return e;
+    kern<<<dim3(1u, (unsigned)nsim), 512, G::BYTES, st>>>(in_mask, mask_bstride, K, scale, sim_scale, tw, A);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fused2d(const float* in_mask, long long mask_bstride, const KernelView& K, float scale,
+                           const float* sim_scale, const float2* tw, const EpiArgs& A, cudaStream_t st, int* nblocks,
+                           int nsim) {
+    const int L1 = 2 * A.P.n[1], M = A.P.n[2];
+    const bool batch = staged_scalars(A, nsim);
+    *nblocks = 1;
+#define F2(l, mm)                                                                                          \
+    if (L1 == l && M == mm)                                                                                \
+        return launch_fused2d_t<l, mm>(in_mask, mask_bstride, K, scale, sim_scale, tw, A, batch, st, nsim);
+    F2(32, 32) F2(32, 64) F2(32, 128) F2(64, 32) F2(64, 64) F2(64, 128) F2(128, 32) F2(128, 64) F2(128, 128)
+#undef F2
+    return cudaErrorInvalidValue;
 }
 
 // ---------------------------------------------------------------- epilogue without demag

@@ -94,8 +94,8 @@ class Plan:
 
     def tiles(self):
         """(tiles, eval_us): the autotuned tile shifts of the row, column and epilogue
-        passes and the timed evaluation with them."""
-        t = (C.c_int * 3)()
+        passes, the fused single-layer flag, and the timed evaluation with them."""
+        t = (C.c_int * 4)()
         us = C.c_double(0.0)
         nat.check(nat.lib().mm_plan_tiles(self.h, t, C.byref(us)))
         return list(t[:]), us.value
@@ -110,7 +110,10 @@ class Plan:
         return out
 
     def set_tiles(self, tiles):
-        nat.check(nat.lib().mm_plan_set_tiles(self.h, (C.c_int * 3)(*tiles)))
+        """tiles: [row, column, epilogue] shifts, optionally a fourth entry (fused
+        single-layer evaluation, 0/1; 0 if left out)."""
+        tiles = list(tiles) + [0] * (4 - len(tiles))
+        nat.check(nat.lib().mm_plan_set_tiles(self.h, (C.c_int * 4)(*tiles)))
 
     def kernel_nonzero(self):
         out = (C.c_int * 6)()

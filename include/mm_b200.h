@@ -135,17 +135,19 @@ MM_API int mm_plan_nsim(mm_plan plan);
  * evaluations; MM_AUTOTUNE=0 in the environment keeps the defaults).  tiles[0]: rows per
  * block of the R2C row pass, tiles[1]: columns per block of the column passes, tiles[2]:
  * rows per block of the C2R + stencil/torque epilogue, each as a shift of the default
- * (-1 = half, 0 = default, +1 = double; tiles[2] in {-1, 0}).  eval_us (may be NULL): the
- * timed evaluation with the chosen tiles (0 if not tuned).  Results do not depend on the
- * tiles (energies up to the order of their block partial sums). */
-MM_API int mm_plan_tiles(mm_plan plan, int tiles[3], double* eval_us);
+ * (-1 = half, 0 = default, +1 = double; tiles[2] in {-1, 0}); tiles[3]: 1 = the fused
+ * single-layer evaluation (one launch per evaluation, one block per simulation, the half
+ * spectrum in shared memory; films with n0 = 1, N1 <= 64, N2 in 32..128).  eval_us (may
+ * be NULL): the timed evaluation with the chosen tiles (0 if not tuned).  Results do not
+ * depend on the tiles (energies up to the order of their block partial sums). */
+MM_API int mm_plan_tiles(mm_plan plan, int tiles[4], double* eval_us);
+MM_API int mm_plan_set_tiles(mm_plan plan, const int tiles[4]);
 /* The plan's transformed demag tensor, one octant: out[6][kd0][kd1][kd2] (host, may be
  * NULL to query kd), components xx yy zz yz xz xy in internal axis order, scaled by
  * 1/(L0 L1 L2) like the reference's fftKern (maxwell_convolution.go:576-612); the other
  * octants follow by symmetry (even along every axis for the diagonal, odd along s and d
  * for K_sd).  For demagexch plans this is the demag part alone. */
 MM_API int mm_plan_demag_kernel(mm_plan plan, float* out, int kd[3]);
-MM_API int mm_plan_set_tiles(mm_plan plan, const int tiles[3]);
 /* Replaces the per-simulation scalars of a batched plan. */
 MM_API int mm_batch_set_sims(mm_plan plan, const mm_sim* sims);
 /* Replaces multipliers/masks/terms of an existing plan (same grid, cell, pbc). */

@@ -1,5 +1,6 @@
-"""The tile autotuner: every tile variant of the row, column and epilogue passes gives
-bit-identical fields and torques (only the block decomposition changes), the tuned choice
+"""The tile autotuner: every tile variant of the row, column and epilogue passes, and the
+fused single-layer evaluation (one launch, spectrum in shared memory), gives bit-identical
+fields and torques (the same arithmetic in another block decomposition), the tuned choice
 is a valid variant with a measured evaluation time, and a stepped trajectory does not
 depend on the tiles."""
 import itertools
@@ -11,7 +12,7 @@ from helpers import rand_m, to_np
 
 pytestmark = pytest.mark.gpu
 
-VARIANTS = [list(t) for t in itertools.product((-1, 0, 1), (-1, 0, 1), (-1, 0))]
+VARIANTS = [list(t) + [0] for t in itertools.product((-1, 0, 1), (-1, 0, 1), (-1, 0))]
 
 
 def _plan(n, cell, nsim=1, **terms):
@@ -34,13 +35,16 @@ def test_tile_variants_are_bit_identical(n, cell, nsim):
     p = _plan(n, cell, nsim, demag=1, exchange=1, anis=1, ku=3e5, anisu=(0.0, 0.6, 0.8), zeeman=1,
               bext=(0.0, 0.01, 0.02))
     tiles, us = p.tiles()
-    assert tiles in VARIANTS and us > 0.0
+    assert tiles[:3] + [0] in VARIANTS and tiles[3] in (0, 1) and us > 0.0
+    if tiles[3]:
+        assert n[0] == 1
     m = np.concatenate([rand_m(n, seed=s) for s in range(nsim)])
     p.set_tiles([0, 0, 0])
     ref_t, _ = p.torque(m)
     ref_f = p.fields(m)["eff"]
     ref_t, ref_f = to_np(ref_t), to_np(ref_f)
-    for v in VARIANTS:
+    variants = VARIANTS + ([[0, 0, 0, 1], [0, -1, -1, 1]] if n[0] == 1 else [])
+    for v in variants:
         p.set_tiles(v)
         t, _ = p.torque(m)
         f = p.fields(m)["eff"]
@@ -74,3 +78,51 @@ def test_set_tiles_rejects_out_of_range():
     with pytest.raises(nat.MMError):
         p.set_tiles([2, 0, 0])
     p.close()
+
+
+@pytest.mark.parametrize("n", [(1, 32, 32), (1, 32, 64), (1, 64, 32), (1, 64, 64), (1, 32, 128), (1, 16, 32),
+                               (1, 128, 64)])
+def test_fused_single_layer_matches_passes(n):
+    """The fused evaluation against the separate passes on every single-layer size it
+    serves (and a size it does not, which must be refused), for a batched plan with
+    per-simulation masks and for a single plan; then a batched relaxation stepped both
+    ways gives the same states and step counts."""
+    import oracle as O
+    from mumax2 import Plan, _native as nat
+    from mumax2 import workloads as W
+    _, sims, _ = W.relax_set(6, seed=8)
+    rng = np.random.default_rng(3)
+    N = n[1] * n[2]
+    masks = (rng.uniform(size=6 * N) > 0.15).astype(np.float32)
+    prob = O.full_desc(n=n, cell=(3e-9, 4e-9, 4e-9), msat=8e5, aex=1.3e-11, demag=1, exchange=1, anis=1, ku=2e5,
+                       anisu=(0.0, 0.6, 0.8), zeeman=1, bext=(0.0, 0.01, 0.02))
+    p = Plan(prob, masks={"msat": masks}, sims=sims, masks_per_sim=True)
+    m = np.concatenate([rand_m(n, seed=s) for s in range(6)])
+    if n[1] > 64 or n[2] < 32:
+        with pytest.raises(nat.MMError):
+            p.set_tiles([0, 0, 0, 1])
+        p.close()
+        return
+    p.set_tiles([0, 0, 0, 0])
+    ref = to_np(p.torque(m)[0])
+    p.set_tiles([0, 0, 0, 1])
+    got = to_np(p.torque(m)[0])
+    assert np.array_equal(got, ref)
+    # stepping
+    out = []
+    for fused in (0, 1):
+        p.set_tiles([0, 0, 0, fused])
+        p.solver("rk23", dt=1e-14, maxerr=1e-6)
+        p.set_state(m)
+        before = [s["step"] for s in p.batch_stats()]
+        p.steps(15)
+        out.append((p.get_state(), [s["step"] - b for s, b in zip(p.batch_stats(), before)]))
+    assert np.array_equal(out[0][0], out[1][0]) and out[0][1] == out[1][1]
+    p.close()
+    single = Plan(prob)
+    single.set_tiles([0, 0, 0, 0])
+    r1 = to_np(single.torque(m[:3 * N])[0])
+    single.set_tiles([0, 0, 0, 1])
+    r2 = to_np(single.torque(m[:3 * N])[0])
+    assert np.array_equal(r1, r2)
+    single.close()

@@ -11,10 +11,10 @@ pytestmark = pytest.mark.gpu
 def test_warm_start_saves_steps():
     from mumax2 import warmstart as WS
     from mumax2 import workloads as W
-    problem, sims, masks, res = WS.generate(1024, seed=11)
+    problem, sims, masks, res = WS.generate(4096, seed=11)
     assert (res["maxtorque"] < WS.thresholds(sims)).all()
     data = WS.Dataset(problem, sims, masks, res["state"])
-    net, losses = WS.train(data, epochs=40, batch=256, lr=1e-3)
+    net, losses = WS.train(data, epochs=40, batch=256, lr=2e-3)
     assert losses[-1] < 0.5 * losses[0]
     _, hs, hm = W.relax_set(256, seed=77)
     ev = WS.evaluate(net, problem, hs, hm, max_steps=WS.step_budget(res["steps"]))
