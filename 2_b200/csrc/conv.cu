@@ -668,12 +668,12 @@ __global__ void __launch_bounds__(512) xfwd4_kernel(const float* __restrict__ in
 // and inverse-transformed; only the rows n < n_in are stored.  Replaces the Stockham
 // colmul_kernel for 2-D films (seven barrier-separated stages per transform and
 // component there, two barriers per transform here).
-template <int L>
+template <int L, int TC>
 __global__ void __launch_bounds__(384) colmul4_kernel(float2* __restrict__ S, KernelView K, int ncols,
                                                       long long comp_stride, long long line_stride, int n_in,
                                                       float scale, const float2* __restrict__ tw, const DevCtl* ctl,
                                                       int skip_retry, long long sim_stride,
-                                                      const float* __restrict__ sim_scale, int TC, int cstride) {
+                                                      const float* __restrict__ sim_scale, int cstride) {
     if (ctl) ctl += blockIdx.y;
     if (conv_skip(ctl, skip_retry)) return;
     S += blockIdx.y * sim_stride;
@@ -892,26 +892,46 @@ static cudaError_t launch_colmul_t(float2* S, const KernelView& K, int ncols, in
     return cudaGetLastError();
 }
 
+// columns per block: 64 / P2 (192 threads) by default, halved or doubled by the tile
+template <int L, int SHIFT>
+__host__ __device__ constexpr int colmul4_tc() {
+    constexpr int t0 = (64 / FS<L>::P2) > 0 ? 64 / FS<L>::P2 : 1;
+    constexpr int t = SHIFT > 0 ? t0 * 2 : (SHIFT < 0 ? t0 / 2 : t0);
+    return (t < 1 || t > 32 || 3 * t * FS<L>::P2 > 384) ? (t0 > 32 ? 32 : t0) : t;
+}
+
+template <int L, int SHIFT>
+static cudaError_t launch_colmul4_s(float2* S, const KernelView& K, int ncols, long long comp_stride,
+                                    long long line_stride, int n_in, float scale, const float2* tw,
+                                    const DevCtl* ctl, int skip_retry, cudaStream_t st, int nsim,
+                                    long long sim_stride, const float* sim_scale) {
+    using F = FS<L>;
+    constexpr int TC = colmul4_tc<L, SHIFT>();
+    const int cstride = col4_stride<L>(TC < 16 ? TC : 16) > F::LBUF ? col4_stride<L>(TC < 16 ? TC : 16) : F::LBUF;
+    const size_t smem = (size_t)(3 * TC * cstride + F::TWT) * sizeof(float2);
+    cudaError_t e = set_smem(colmul4_kernel<L, TC>, smem);
+    if (e != cudaSuccess) return e;
+    int threads = 3 * TC * F::P2;
+    if (threads < 32) threads = 32;
+    const int ntiles = (ncols + TC - 1) / TC;
+    colmul4_kernel<L, TC><<<dim3((unsigned)ntiles, (unsigned)nsim), threads, smem, st>>>(
+        S, K, ncols, comp_stride, line_stride, n_in, scale, tw, ctl, skip_retry, sim_stride, sim_scale, cstride);
+    return cudaGetLastError();
+}
+
 template <int L>
 static cudaError_t launch_colmul4_t(float2* S, const KernelView& K, int ncols, long long comp_stride,
                                     long long line_stride, int n_in, float scale, const float2* tw,
                                     const DevCtl* ctl, int skip_retry, cudaStream_t st, int nsim,
                                     long long sim_stride, const float* sim_scale, int tile) {
-    using F = FS<L>;
-    // columns per block: 64 / P2 (192 threads) by default, halved or doubled by the tile
-    int TC = shifted((64 / F::P2) > 0 ? 64 / F::P2 : 1, tile);
-    if (TC < 1 || TC > 32 || 3 * TC * F::P2 > 384) TC = (64 / F::P2) > 0 ? 64 / F::P2 : 1;
-    if (TC > 32) TC = 32;
-    const int cstride = col4_stride<L>(TC < 16 ? TC : 16) > F::LBUF ? col4_stride<L>(TC < 16 ? TC : 16) : F::LBUF;
-    const size_t smem = (size_t)(3 * TC * cstride + F::TWT) * sizeof(float2);
-    cudaError_t e = set_smem(colmul4_kernel<L>, smem);
-    if (e != cudaSuccess) return e;
-    int threads = 3 * TC * F::P2;
-    if (threads < 32) threads = 32;
-    const int ntiles = (ncols + TC - 1) / TC;
-    colmul4_kernel<L><<<dim3((unsigned)ntiles, (unsigned)nsim), threads, smem, st>>>(
-        S, K, ncols, comp_stride, line_stride, n_in, scale, tw, ctl, skip_retry, sim_stride, sim_scale, TC, cstride);
-    return cudaGetLastError();
+    if (tile < 0)
+        return launch_colmul4_s<L, -1>(S, K, ncols, comp_stride, line_stride, n_in, scale, tw, ctl, skip_retry, st,
+                                       nsim, sim_stride, sim_scale);
+    if (tile > 0)
+        return launch_colmul4_s<L, 1>(S, K, ncols, comp_stride, line_stride, n_in, scale, tw, ctl, skip_retry, st,
+                                      nsim, sim_stride, sim_scale);
+    return launch_colmul4_s<L, 0>(S, K, ncols, comp_stride, line_stride, n_in, scale, tw, ctl, skip_retry, st, nsim,
+                                  sim_stride, sim_scale);
 }
 
 cudaError_t launch_colmul(int L, float2* S, const KernelView& K, int ncols, int nouter, long long comp_stride,
