@@ -778,7 +778,237 @@ static cudaError_t launch_conv_tc(const bf16* in, int in_cs, int in_co, int Cin,
                                    band, stage_bytes);
 }
 
+// ---------------------------------------------------------------- tcgen05 weight gradient
+// dW_tap[co][ci] = sum_q dY[q][co] X[q + off(tap)][ci] over the padded positions q of the
+// halo-band layout (pads carry zero dY and zero X): nine GEMMs with K = positions, one
+// TMEM accumulator each (M = 128 output channels, N = 32 input channels; 9 x 32 of the 512
+// columns).  Both operands stay pixel-major as loaded, i.e. MN-major in the tcgen05
+// sense: a plane per 8 channels holds 16 bytes per position, 8 consecutive positions
+// form a core matrix (K-direction stride 128 bytes), planes are the MN-direction
+// stride.  The X operand of tap (dy, dx) is the stage's band shifted along K by
+// ((dy+1)(W+1) + dx+1) positions, a 16-byte-aligned descriptor offset.  Blocks split
+// the positions; each adds its nine 128 x 32 partial sums to dW with FP32 atomics.
+constexpr int WGT_KC = 64;  // positions per stage
+
+__device__ __forceinline__ int band_pixel(int q, int total, int img, int Wp, int H, int Wd) {
+    if (q < 0 || q >= total) return -1;
+    const int b = q / img, r = q - b * img;
+    const int y = r / Wp, xp = r - y * Wp;
+    return (y < H && xp > 0) ? (b * H + y) * Wd + xp - 1 : -1;
+}
+
+constexpr int WGT_BAND_MAX = WGT_KC + 2 * 257 + 2;  // widths up to 256
+
+template <int ST>
+__global__ void __launch_bounds__(256) conv3x3_wgrad_tc_kernel(const bf16* __restrict__ dy, int dy_cs, int dy_co,
+                                                               int Cout, const bf16* __restrict__ x, int x_cs,
+                                                               int x_co, int Cin, float* __restrict__ dW, int B,
+                                                               int H, int Wd, int* err, int band, int stage_bytes,
+                                                               int per_block) {
+    constexpr int M = 128, N = 32, KC = WGT_KC;
+    extern __shared__ __align__(1024) unsigned char smem[];
+    __shared__ __align__(8) unsigned long long mbar[ST];
+    __shared__ unsigned tmem_base_sh;
+    __shared__ int fail_sh;
+    __shared__ int s_pix[2][WGT_BAND_MAX];         // band position -> pixel (or -1), two stages
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int Wp = Wd + 1;
+    const int img = (H + 1) * Wp;
+    const int total = B * img;
+    const int q_begin = blockIdx.x * per_block;
+    const int q_end = q_begin + per_block < total ? q_begin + per_block : total;
+    const int ci0 = blockIdx.y * N, co0 = blockIdx.z * M;
+    // channel planes that exist: the others are never loaded, and the D rows / columns
+    // they would feed are never stored
+    const int ga = min(16, (Cout - co0 + 7) / 8), gb = min(4, (Cin - ci0 + 7) / 8);
+    constexpr int PLANE_A = KC * 16;                // bytes per 8-channel plane of dY
+    const int plane_b = band * 16;                  // bytes per 8-channel plane of the X band
+    const int a_bytes = 16 * PLANE_A;               // 16 planes = 128 output channels
+    if (tid == 0) {
+        fail_sh = 0;
+        for (int i = 0; i < ST; i++) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&mbar[i])));
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::);
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
+                         smem_u32(&tmem_base_sh)),
+                     "n"(512));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+    }
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+    const unsigned tmem = tmem_base_sh;
+    const int nstages = q_end > q_begin ? (q_end - q_begin + KC - 1) / KC : 0;
+    // BF16 A and B, F32 D, both operands MN-major (transpose bits 15 and 16)
+    const unsigned idesc = (1u << 4) | (1u << 7) | (1u << 10) | (1u << 15) | (1u << 16) | ((unsigned)(N >> 3) << 17) |
+                           ((unsigned)(M >> 4) << 24);
+    const long long LIMIT = 1LL << 26;
+    // the band of stage s: positions q0 - (W+2) .. q0 + KC + W, q0 = q_begin + s KC
+    auto fill_pix = [&](int s) {
+        const int qb = q_begin + s * KC - (Wp + 1);
+        for (int i = tid; i < band; i += 256) s_pix[s & 1][i] = band_pixel(qb + i, total, img, Wp, H, Wd);
+    };
+    auto load_stage = [&](int s) {
+        unsigned char* base = smem + (s % ST) * stage_bytes;
+        const int q0 = q_begin + s * KC;
+        const int* pixs = s_pix[s & 1];
+        // dY rows of positions q0 .. q0+KC-1 (band entries W+2 ..): zero past this block's range
+        for (int c = tid; c < ga * KC; c += 256) {
+            const int g = c / KC, i = c - g * KC;
+            const int pix = (q0 + i < q_end) ? pixs[Wp + 1 + i] : -1;
+            const bool ok = pix >= 0;
+            cp_async16(base + g * PLANE_A + i * 16, dy + (long long)(ok ? pix : 0) * dy_cs + dy_co + co0 + g * 8, ok);
+        }
+        unsigned char* bb = base + a_bytes;
+        for (int c = tid; c < gb * band; c += 256) {
+            const int g = c / band, i = c - g * band;
+            const int pix = pixs[i];
+            const bool ok = pix >= 0;
+            cp_async16(bb + g * plane_b + i * 16, x + (long long)(ok ? pix : 0) * x_cs + x_co + ci0 + g * 8, ok);
+        }
+    };
+    for (int s = 0; s < ST - 1; s++) {
+        if (s < nstages) {
+            fill_pix(s);
+            __syncthreads();
+            load_stage(s);
+        }
+        cp_commit();
+    }
+    int issued = 0;
+    for (int s = 0; s < nstages; s++) {
+        cp_wait<ST - 2>();
+        asm volatile("fence.proxy.async.shared::cta;\n" ::);
+        __syncthreads();
+        if (fail_sh) break;
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+            const unsigned base = smem_u32(smem + (s % ST) * stage_bytes);
+#pragma unroll 1
+            for (int tap = 0; tap < 9; tap++) {
+                const unsigned off = (unsigned)((tap / 3) * Wp + tap % 3);
+#pragma unroll 1
+                for (int kk = 0; kk < KC / 16; kk++) {
+                    const uint64_t ad = umma_desc(base + kk * 16 * 16, 128, PLANE_A);
+                    const uint64_t bd = umma_desc(base + a_bytes + (kk * 16 + off) * 16, 128, (unsigned)plane_b);
+                    const unsigned acc = (s > 0 || kk > 0) ? 1u : 0u;
+                    asm volatile(
+                        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+                        " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem + tap * N),
+                        "l"(ad), "l"(bd), "r"(idesc), "r"(acc));
+                }
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                smem_u32(&mbar[s % ST])));
+        }
+        issued = s + 1;
+        const int nx = s + ST - 1;
+        if (nx < nstages) {
+            if (s >= 1 && !mbar_wait(smem_u32(&mbar[(s - 1) % ST]), ((s - 1) / ST) & 1, LIMIT)) {
+                if (lane == 0) atomicExch(&fail_sh, 1);
+            }
+            fill_pix(nx);
+            __syncthreads();
+            if (!fail_sh) load_stage(nx);
+        }
+        cp_commit();
+    }
+    cp_wait<0>();
+    __syncthreads();
+    if (!fail_sh && issued > 0) {
+        const int last = issued - 1;
+        if (!mbar_wait(smem_u32(&mbar[last % ST]), (last / ST) & 1, LIMIT)) {
+            if (lane == 0) atomicExch(&fail_sh, 1);
+        }
+    }
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+    // epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31 (output channels); warps 0-3
+    // take taps 0-4, warps 4-7 taps 5-8
+    const int quad = warp & 3, half = warp >> 2;
+    if (!fail_sh && issued > 0) {
+        const int co = co0 + quad * 32 + lane;
+        for (int tap = half * 5; tap < (half ? 9 : 5); tap++) {
+#pragma unroll
+            for (int c0 = 0; c0 < N; c0 += 16) {
+                if (ci0 + c0 >= Cin) break;   // warp-uniform
+                unsigned v[16];
+                const unsigned ta = tmem + ((unsigned)(quad * 32) << 16) + (unsigned)(tap * N + c0);
+                asm volatile(
+                    "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
+                    "[%16];\n"
+                    : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+                      "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
+                      "=r"(v[15])
+                    : "r"(ta));
+                asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::);
+                if (co < Cout) {
+                    float* d = dW + ((long long)co * 9 + tap) * Cin + ci0 + c0;
+#pragma unroll
+                    for (int e = 0; e < 16; e++)
+                        if (ci0 + c0 + e < Cin) atomicAdd(d + e, __uint_as_float(v[e]));
+                }
+            }
+        }
+    } else if (fail_sh && tid == 0) {
+        atomicExch(err, 1);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "n"(512));
+    }
+}
+
+template <int ST>
+static cudaError_t launch_wgrad_tc_st(const bf16* dy, int dy_cs, int dy_co, int Cout, const bf16* x, int x_cs,
+                                      int x_co, int Cin, float* dW, int B, int H, int Wd, int* err, int band,
+                                      int stage_bytes, cudaStream_t st) {
+    // a block holds all 512 TMEM columns: at least 116 KB of shared memory keeps a second
+    // block off the SM, so no allocation ever waits for another block
+    const int smem = ST * stage_bytes > 116 * 1024 ? ST * stage_bytes : 116 * 1024;
+    cudaError_t e = cudaFuncSetAttribute(conv3x3_wgrad_tc_kernel<ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    const long long total = (long long)B * (H + 1) * (Wd + 1);
+    const int ct = (Cin + 31) / 32, mt = (Cout + 127) / 128;
+    // about two blocks' worth of work per SM, whole stages per block
+    long long chunks = (2LL * 148 + (long long)ct * mt - 1) / ((long long)ct * mt);
+    long long per = (total + chunks - 1) / chunks;
+    per = (per + WGT_KC - 1) / WGT_KC * WGT_KC;
+    chunks = (total + per - 1) / per;
+    dim3 grid((unsigned)chunks, (unsigned)ct, (unsigned)mt);
+    conv3x3_wgrad_tc_kernel<ST><<<grid, 256, smem, st>>>(dy, dy_cs, dy_co, Cout, x, x_cs, x_co, Cin, dW, B, H, Wd, err,
+                                                         band, stage_bytes, (int)per);
+    return cudaGetLastError();
+}
+
 }  // namespace mm
+
+// tcgen05 variant of mm_nn_conv3x3_wgrad (dW accumulated, so zero it first; plus a device
+// error flag that a timed-out wait sets).
+extern "C" MM_API int mm_nn_conv3x3_wgrad_tc(const void* dy, int dy_cs, int dy_co, int Cout, const void* x, int x_cs,
+                                             int x_co, int Cin, float* dW, int B, int H, int Wd, int* err,
+                                             mm_stream st) {
+    if (Cin % 8 || Cout % 8 || dy_cs % 8 || dy_co % 8 || x_cs % 8 || x_co % 8 || Wd < 1 || Wd > 256 || H < 1 ||
+        B < 1 || !err || (long long)B * (H + 1) * (Wd + 1) >= (1LL << 30))
+        return report_error(MM_ERR_ARG, "mm_nn_conv3x3_wgrad_tc: bad argument");
+    const int band = WGT_KC + 2 * (Wd + 1) + 2;
+    const int stage_bytes = ((16 * WGT_KC * 16 + 4 * band * 16) + 127) / 128 * 128;
+    const int fit = (200 * 1024) / stage_bytes;
+    cudaError_t e;
+    if (fit >= 4)
+        e = launch_wgrad_tc_st<4>((const bf16*)dy, dy_cs, dy_co, Cout, (const bf16*)x, x_cs, x_co, Cin, dW, B, H, Wd, err,
+                                  band, stage_bytes, (cudaStream_t)st);
+    else if (fit == 3)
+        e = launch_wgrad_tc_st<3>((const bf16*)dy, dy_cs, dy_co, Cout, (const bf16*)x, x_cs, x_co, Cin, dW, B, H, Wd, err,
+                                  band, stage_bytes, (cudaStream_t)st);
+    else
+        e = launch_wgrad_tc_st<2>((const bf16*)dy, dy_cs, dy_co, Cout, (const bf16*)x, x_cs, x_co, Cin, dW, B, H, Wd, err,
+                                  band, stage_bytes, (cudaStream_t)st);
+    if (e != cudaSuccess) return report_error(MM_ERR_CUDA, cudaGetErrorString(e));
+    return MM_OK;
+}
 
 // tcgen05 variant of mm_nn_conv3x3 (same arguments plus a device error flag that a
 // timed-out wait sets); N tile = 16..128 chosen from Cout.

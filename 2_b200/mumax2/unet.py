@@ -129,10 +129,14 @@ def state_from_output(out3, masks):
 class UNet:
     """Buffers for one batch size; forward, backward and Adam on the GPU."""
 
-    def __init__(self, batch, H=64, W=64, device=0, seed=0, params=None, tcgen05=True):
+    def __init__(self, batch, H=64, W=64, device=0, seed=0, params=None, tcgen05=True, tcgen05_wgrad=False):
+        """tcgen05: forward and data-gradient convolutions on the tcgen05 kernel (else
+        mma.sync); tcgen05_wgrad: weight gradients on the tcgen05 kernel (measured slower
+        than the mma.sync one at these sizes, so off by default)."""
         import torch
         self.torch = torch
         self.tcgen05 = tcgen05
+        self.tcgen05_wgrad = tcgen05_wgrad
         self.device = torch.device("cuda", device) if isinstance(device, int) else torch.device(device)
         self.B, self.H, self.W = batch, H, W
         bf = torch.bfloat16
@@ -281,9 +285,14 @@ class UNet:
                 if relu:
                     nat.check(L.mm_nn_relu_bwd(self._ptr(self.buf[ov]), self._cs((ov,)), oo, self._ptr(self.grad[ov]),
                                                self._cs((ov,)), oo, cout, P, None))
-                nat.check(L.mm_nn_conv3x3_wgrad(self._ptr(self.grad[ov]), self._cs((ov,)), oo, cout,
-                                                self._ptr(self.buf[iv]), self._cs((iv,)), io, cin, fp(d["gw"]),
-                                                B, H >> lvl, W >> lvl, None))
+                if self.tcgen05_wgrad:
+                    nat.check(L.mm_nn_conv3x3_wgrad_tc(self._ptr(self.grad[ov]), self._cs((ov,)), oo, cout,
+                                                       self._ptr(self.buf[iv]), self._cs((iv,)), io, cin, fp(d["gw"]),
+                                                       B, H >> lvl, W >> lvl, fp(self.err), None))
+                else:
+                    nat.check(L.mm_nn_conv3x3_wgrad(self._ptr(self.grad[ov]), self._cs((ov,)), oo, cout,
+                                                    self._ptr(self.buf[iv]), self._cs((iv,)), io, cin, fp(d["gw"]),
+                                                    B, H >> lvl, W >> lvl, None))
                 nat.check(L.mm_nn_bias_grad(self._ptr(self.grad[ov]), self._cs((ov,)), oo, cout, P, fp(d["gb"]), None))
                 if name != "e0a":
                     # dX over the whole input view (a concatenated input gets both parts)

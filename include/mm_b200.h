@@ -304,6 +304,12 @@ MM_API int mm_save_wait(mm_plan plan);
  * gradient. */
 MM_API int mm_nn_conv3x3(const void* in, int in_cs, int in_co, int Cin, const void* W, const float* bias, void* out,
                          int out_cs, int out_co, int Cout, int B, int H, int Wd, int relu, mm_stream st);
+/* tcgen05 weight gradient: dW[Cout][9][Cin] (FP32, accumulated: zero it first) of the 3x3
+ * convolution from dY [B*H*W][dy_cs] (channels dy_co..+Cout) and X [B*H*W][x_cs]
+ * (channels x_co..+Cin); channel counts, strides and offsets multiples of 8, W <= 256;
+ * *err set if an mbarrier wait runs out. */
+MM_API int mm_nn_conv3x3_wgrad_tc(const void* dy, int dy_cs, int dy_co, int Cout, const void* x, int x_cs, int x_co,
+                                  int Cin, float* dW, int B, int H, int W, int* err, mm_stream st);
 /* conv3x3 on the 5th-generation tensor cores (tcgen05.mma, TMEM accumulators); *err
  * (device int) is set if a bounded wait inside the kernel ran out. */
 MM_API int mm_nn_conv3x3_tc(const void* in, int in_cs, int in_co, int Cin, const void* W, const float* bias, void* out,

@@ -67,8 +67,8 @@ def test_conv3x3_forward_and_data_gradient(cin, cout, B, H, W, relu):
     assert _relnorm(db.cpu().numpy(), rdb) < 1e-3
 
 
-@pytest.mark.parametrize("tcgen05", [True, False])
-def test_network_gradients_match_oracle(tcgen05):
+@pytest.mark.parametrize("tcgen05,wgrad", [(True, False), (False, False), (True, True)])
+def test_network_gradients_match_oracle(tcgen05, wgrad):
     import unet_ref as R
     from mumax2 import unet as U
     B, H, W = 2, 16, 16
@@ -81,7 +81,7 @@ def test_network_gradients_match_oracle(tcgen05):
     feats[..., :9] = rng.normal(size=(B, H * W, 9))
     target = rng.normal(size=(B, H * W, 3)).astype(np.float32)
     mask = (rng.uniform(size=(B, H * W)) > 0.2).astype(np.float32)
-    net = U.UNet(B, H, W, params=params, tcgen05=tcgen05)
+    net = U.UNet(B, H, W, params=params, tcgen05=tcgen05, tcgen05_wgrad=wgrad)
     net.set_input(feats)
     net.forward()
     net.set_target(target, mask)
@@ -187,3 +187,28 @@ def test_output_state_kernel_matches_host_conversion():
     net.states(md, dst)
     ref = U.state_from_output(net.output3(), masks)
     assert np.abs(dst.cpu().numpy() - ref).max() < 1e-6
+
+
+@pytest.mark.parametrize("cin,cout,B,H,W", [(32, 32, 2, 8, 8), (16, 32, 2, 64, 64), (384, 128, 2, 16, 16),
+                                            (128, 256, 3, 8, 8), (32, 16, 1, 5, 7), (48, 64, 2, 1, 9),
+                                            (96, 32, 2, 8, 16)])
+def test_wgrad_tcgen05_matches(cin, cout, B, H, W):
+    """The tcgen05 weight gradient (nine TMEM accumulators over the halo band, MN-major
+    operands) against the numpy oracle, 1e-3 relative in norm (FP32 sums of bf16
+    products in another order)."""
+    import torch
+    import unet_ref as R
+    from mumax2 import _native as nat
+    rng = np.random.default_rng(cin + 3 * cout + W)
+    x = R.bf16(rng.normal(size=(B, H, W, cin)))
+    w = R.bf16(rng.normal(size=(cout, 9, cin)) / np.sqrt(9 * cin))
+    dy = R.bf16(rng.normal(size=(B, H, W, cout)))
+    xd, dyd = _dev(x, torch.bfloat16), _dev(dy, torch.bfloat16)
+    dw = torch.zeros(cout * 9 * cin, dtype=torch.float32, device="cuda")
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    nat.check(nat.lib().mm_nn_conv3x3_wgrad_tc(_p(dyd), cout, 0, cout, _p(xd), cin, 0, cin, _p(dw), B, H, W, _p(err),
+                                               None))
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    _, rdw, _ = R.conv3x3_backward(x, w, dy)
+    assert _relnorm(dw.cpu().numpy().reshape(rdw.shape), rdw) < 1e-3
