@@ -288,6 +288,8 @@ def evaluate(net, problem, sims, masks, slots=256, device=0, energy_tol=1e-4, ma
     B = min(slots, len(sims))
     plan = Plan(problem, masks={"msat": np.concatenate(masks[:B])}, sims=sims[:B], masks_per_sim=True,
                 device=device)
+    if B > 16:   # the drain plan of both pools, made outside the timed regions
+        _tail_plan(plan, problem, masks[0], sims[0], 16, device, 1e-6)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     rc = relax_pool(problem, sims, masks, [cold] * len(sims), thr, slots=slots, device=device, plan=plan)
