@@ -23,6 +23,7 @@
 #include "fft4.cuh"
 #include "mm_internal.h"
 #include "kernel_view.cuh"
+#include "pdl.cuh"
 
 namespace mm {
 using namespace mmfft;
@@ -384,6 +385,7 @@ __global__ void __launch_bounds__(128) zmul_reg4_kernel(float2* __restrict__ S, 
                                                          const float2* __restrict__ tw, const DevCtl* ctl,
                                                          int skip_retry, long long sim_stride,
                                                          const float* __restrict__ sim_scale) {
+    pdl_begin();
     if (BATCH) {  // the single-simulation variant keeps the shorter prologue
         if (ctl) ctl += blockIdx.y;
         S += blockIdx.y * sim_stride;
@@ -505,12 +507,10 @@ static cudaError_t launch_zmul_reg4_t(float2* S, const KernelView& K, int L1, in
     const long long threads = 4LL * L1 * h;
     const dim3 grid((unsigned)((threads + 127) / 128), (unsigned)nsim);
     if (nsim > 1)
-        zmul_reg4_kernel<P, true><<<grid, 128, 0, st>>>(S, K, L1, h, hp, comp_stride, zstride, scale, tw, ctl,
-                                                        skip_retry, sim_stride, sim_scale);
-    else
-        zmul_reg4_kernel<P, false><<<grid, 128, 0, st>>>(S, K, L1, h, hp, comp_stride, zstride, scale, tw, ctl,
-                                                         skip_retry, sim_stride, sim_scale);
-    return cudaGetLastError();
+        return launch_pdl(zmul_reg4_kernel<P, true>, grid, dim3(128), 0, st, S, K, L1, h, hp, comp_stride, zstride,
+                          scale, tw, ctl, skip_retry, sim_stride, sim_scale);
+    return launch_pdl(zmul_reg4_kernel<P, false>, grid, dim3(128), 0, st, S, K, L1, h, hp, comp_stride, zstride, scale,
+                      tw, ctl, skip_retry, sim_stride, sim_scale);
 }
 
 // P = N0 = L0/2 (zero-padded z); returns cudaErrorNotSupported for other shapes
@@ -558,6 +558,7 @@ __global__ void __launch_bounds__(512) colfft4_kernel(float2* __restrict__ S, in
                                                       long long line_stride, int n_in, int n_out,
                                                       const float2* __restrict__ tw, const DevCtl* ctl,
                                                       int skip_retry, long long sim_stride, int TC, int cstride) {
+    pdl_begin();
     if (ctl) ctl += blockIdx.y;
     if (conv_skip(ctl, skip_retry)) return;
     S += blockIdx.y * sim_stride;
@@ -596,6 +597,7 @@ __global__ void __launch_bounds__(512) xfwd4_kernel(const float* __restrict__ in
                                                     const float2* __restrict__ tw, const DevCtl* ctl, int skip_retry,
                                                     long long in_bstride, long long out_bstride,
                                                     long long mask_bstride, int RPB) {
+    pdl_begin();
     const int sim = blockIdx.y;
     if (ctl) ctl += sim;
     if (conv_skip(ctl, skip_retry)) return;
@@ -674,6 +676,7 @@ __global__ void __launch_bounds__(384) colmul4_kernel(float2* __restrict__ S, Ke
                                                       float scale, const float2* __restrict__ tw, const DevCtl* ctl,
                                                       int skip_retry, long long sim_stride,
                                                       const float* __restrict__ sim_scale, int cstride) {
+    pdl_begin();
     if (ctl) ctl += blockIdx.y;
     if (conv_skip(ctl, skip_retry)) return;
     S += blockIdx.y * sim_stride;
@@ -776,9 +779,8 @@ static cudaError_t launch_xfwd4_t(const float* in, PP pp, const float* mask, flo
     cudaError_t e = set_smem(xfwd4_kernel<M>, smem);
     if (e != cudaSuccess) return e;
     const dim3 grid((unsigned)((nrows + RPB - 1) / RPB), (unsigned)nsim);
-    xfwd4_kernel<M><<<grid, RPB * F::P2, smem, st>>>(in, pp, mask, out, nrows, Z, Y, Yout, in_pitch, n_in, hp, tw,
-                                                      ctl, skip_retry, in_bstride, out_bstride, mask_bstride, RPB);
-    return cudaGetLastError();
+    return launch_pdl(xfwd4_kernel<M>, grid, dim3(RPB * F::P2), smem, st, in, pp, mask, out, nrows, Z, Y, Yout, in_pitch,
+                      n_in, hp, tw, ctl, skip_retry, in_bstride, out_bstride, mask_bstride, RPB);
 }
 
 template <typename V, typename S>
@@ -831,9 +833,9 @@ static cudaError_t launch_colfft4_t(float2* S, int ncols, int nouter, long long 
     const int ntiles = (ncols + TC - 1) / TC;
     int threads = TC * F::P2;
     if (threads < 32) threads = 32;
-    colfft4_kernel<L, SIGN><<<dim3((unsigned)(nouter * ntiles), (unsigned)nsim), threads, smem, st>>>(
-        S, ncols, outer_stride, line_stride, n_in, n_out, tw, ctl, skip_retry, sim_stride, TC, col4_stride<L>(TC));
-    return cudaGetLastError();
+    return launch_pdl(colfft4_kernel<L, SIGN>, dim3((unsigned)(nouter * ntiles), (unsigned)nsim), dim3(threads), smem, st,
+                      S, ncols, outer_stride, line_stride, n_in, n_out, tw, ctl, skip_retry, sim_stride, TC,
+                      col4_stride<L>(TC));
 }
 
 template <typename V>
@@ -914,9 +916,8 @@ static cudaError_t launch_colmul4_s(float2* S, const KernelView& K, int ncols, l
     int threads = 3 * TC * F::P2;
     if (threads < 32) threads = 32;
     const int ntiles = (ncols + TC - 1) / TC;
-    colmul4_kernel<L, TC><<<dim3((unsigned)ntiles, (unsigned)nsim), threads, smem, st>>>(
-        S, K, ncols, comp_stride, line_stride, n_in, scale, tw, ctl, skip_retry, sim_stride, sim_scale, cstride);
-    return cudaGetLastError();
+    return launch_pdl(colmul4_kernel<L, TC>, dim3((unsigned)ntiles, (unsigned)nsim), dim3(threads), smem, st, S, K, ncols,
+                      comp_stride, line_stride, n_in, scale, tw, ctl, skip_retry, sim_stride, sim_scale, cstride);
 }
 
 template <int L>

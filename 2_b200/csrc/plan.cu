@@ -21,6 +21,7 @@
 
 #include "fft.cuh"
 #include "mm_internal.h"
+#include "pdl.cuh"
 
 namespace mm {
 int build_demag_kernel(const int L[3], const double cell[3], const int pbc[3], int accuracy, float* khat,
@@ -221,6 +222,7 @@ __device__ void summarise(const DevCtl* c, int nsim, CtlSummary* sum, int active
 
 __global__ void controller_kernel(DevCtl* ctl, int nsim, CtlSummary* sum, int mode, int adaptive, int q, int fsal,
                                   int nevals, int first_skippable) {
+    pdl_begin();
     int active = 0, bad = 0x7fffffff;
     long long left = 0;
     for (int b = threadIdx.x; b < nsim; b += blockDim.x) {
@@ -1280,9 +1282,8 @@ static int launch_combine(mm_plan p, PP base, PP next, int nk, const PP* kp, con
 static cudaError_t launch_controller(mm_plan p, cudaStream_t st, int mode, int adaptive, int q, int fsal, int nevals,
                                      int first_skippable) {
     const int threads = p->nsim >= 256 ? 256 : ((p->nsim + 31) / 32) * 32;
-    controller_kernel<<<1, threads, 0, st>>>(p->ctl, p->nsim, p->dsum, mode, adaptive, q, fsal, nevals,
-                                             first_skippable);
-    return cudaGetLastError();
+    return launch_pdl(controller_kernel, dim3(1), dim3(threads), 0, st, p->ctl, p->nsim, p->dsum, mode, adaptive, q,
+                      fsal, nevals, first_skippable);
 }
 
 // blocks per simulation of the record sums

@@ -19,6 +19,7 @@
 #include "fft4.cuh"
 #include "mm_internal.h"
 #include "kernel_view.cuh"
+#include "pdl.cuh"
 
 namespace mm {
 using namespace mmfft;
@@ -615,6 +616,7 @@ __host__ __device__ constexpr int xinv4_rows_c() {
 template <int M, bool TERMS, bool BATCH, bool HALF>
 __device__ __forceinline__ void xinv4_epi_body(const float2* __restrict__ S, int hp, int L1,
                                                const float2* __restrict__ tw, const EpiArgs& A) {
+    pdl_begin();
     constexpr int RPB = xinv4_rows_c<M, HALF>();
     const DevCtl* ctl = A.ctl ? A.ctl + blockIdx.y : nullptr;
     if (skip_eval(ctl, A.skip_retry)) return;
@@ -993,8 +995,7 @@ static cudaError_t launch_xinv4_h(const float2* S, int hp, int L1, const float2*
     int threads = RPB * 3 * FS<M>::P2;
     if (threads < 32) threads = 32;
     *nblocks = blocks;
-    kern<<<dim3((unsigned)blocks, (unsigned)nsim), threads, smem, st>>>(S, hp, L1, tw, A);
-    return cudaGetLastError();
+    return launch_pdl(kern, dim3((unsigned)blocks, (unsigned)nsim), dim3(threads), smem, st, S, hp, L1, tw, A);
 }
 
 template <int M, bool TERMS, bool BATCH>
