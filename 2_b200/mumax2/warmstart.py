@@ -1,4 +1,4 @@
-"""Learned warm start of batched relaxations.
+"""Learned warm start of batched relaxations of 64x64x1 films.
 
   relax_pool   plain relax() of many problems through one batched plan with continuous
                batching (a finished slot takes the next problem at once)
@@ -6,7 +6,7 @@
   train        the U-Net (unet.py) on them with this library's kernels
   predict      initial states for new problems, batched, built and kept on the GPU
   evaluate     cold vs warm relaxations of held-out problems: rate, steps, and the
-               final state judged against the cold relax (max torque and energy); a warm
+               final state checked against the cold relax (max torque and energy); a warm
                start that fails is redone from the cold start in the same pool
 """
 import time

@@ -548,9 +548,10 @@ def relax_bench(args, rank, world, local_rank, dist):
 
 # ---------------------------------------------------------------- single-simulation configs
 def single_bench(args, rank, world, local_rank, dist):
-    """configs[0] (--workload sp4: the 128x32x1 film, RK45, <m> every 10 ps) and configs[2]
-    (--workload wall: the 512x128x1 Neel wall under Zhang-Li current, RK45, with the wall
-    position from <m_x> every 10 ps, plus the Slonczewski variant on a 128x128x1 disk).
+    """The single-simulation workloads: --workload sp4 (the 128x32x1 film of the SP4
+    geometry, RK45, <m> every 10 ps) and --workload wall (the 512x128x1 Neel wall under
+    Zhang-Li current, RK45, with the wall position from <m_x> every 10 ps, plus the
+    Slonczewski variant on a 128x128x1 disk).
     Latency-bound sizes: the numbers are simulated time and steps per second."""
     import torch
     from mumax2 import Plan
@@ -626,8 +627,8 @@ def single_bench(args, rank, world, local_rank, dist):
 
 # ---------------------------------------------------------------- learned warm start
 def warmstart_bench(args, rank, world, local_rank, dist):
-    """relaxed states of --train problems (plain relax from the cold start,
-    continuous batching) train the BF16 U-Net on the GPU; on --nsim held-out problems the
+    """The learned warm start: relaxed states of --train problems (plain relax from the cold
+    start, continuous batching) train the BF16 U-Net on the GPU; on --nsim held-out problems the
     warm start (network inference + relax) is timed against the cold relax.  value =
     warm relaxations/s (fallbacks to the cold start included).  A warm relax gets the 99th
     percentile of the training relaxations' step counts as its budget."""
