@@ -542,6 +542,12 @@ extern "C" MM_API int mm_nn_to_bf16(const float* in, long long P, int C, void* o
 // and returns.
 namespace mm {
 
+// Iteration limit of the mbarrier waits of the tcgen05 kernels (mm_nn_set_wait_limit
+// changes it, e.g. to 0 so that a test sees the time-out path; the clean-up wait for
+// MMAs in flight always uses the default).
+constexpr long long kWaitLimitDefault = 1LL << 26;
+static long long g_wait_limit = kWaitLimitDefault;
+
 __device__ __forceinline__ uint64_t umma_desc(unsigned saddr, unsigned lbo, unsigned sbo) {
     uint64_t d = 0;
     d |= (uint64_t)((saddr >> 4) & 0x3FFF);
@@ -580,7 +586,7 @@ __global__ void __launch_bounds__(256) conv3x3_tc_kernel(const bf16* __restrict_
                                                          const bf16* __restrict__ W, const float* __restrict__ bias,
                                                          bf16* __restrict__ out, int out_cs, int out_co, int Cout,
                                                          int B, int H, int Wd, int relu, int* err, int band,
-                                                         int stage_bytes) {
+                                                         int stage_bytes, long long limit) {
     constexpr int M = 128;
     constexpr int TCOLS = N < 32 ? 32 : N;         // TMEM columns (power of two >= 32)
     extern __shared__ __align__(1024) unsigned char smem[];
@@ -621,7 +627,7 @@ __global__ void __launch_bounds__(256) conv3x3_tc_kernel(const bf16* __restrict_
     const unsigned tmem = tmem_base_sh;
     const int nstages = Cin / 16;
     const unsigned idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((unsigned)(N >> 3) << 17) | ((unsigned)(M >> 4) << 24);
-    const long long LIMIT = 1LL << 26;
+    const long long LIMIT = limit;
     // core-matrix offset of (row r, k-half h) in a 16-channel weight block: K-adjacent core
     // matrices 128 bytes apart, 8-row groups 256 bytes apart
     auto core_off = [](int r, int h) { return ((r >> 3) * 2 + h) * 128 + (r & 7) * 16; };
@@ -687,11 +693,14 @@ __global__ void __launch_bounds__(256) conv3x3_tc_kernel(const bf16* __restrict_
     }
     cp_wait<0>();
     __syncthreads();
-    // the last commit covers every MMA of the block
-    if (!fail_sh && issued > 0) {
+    // the last commit covers every MMA of the block; a block that gave up waits (bounded,
+    // with the default limit) for the MMAs it has in flight before its TMEM is freed
+    if (issued > 0) {
         const int last = issued - 1;
-        if (!mbar_wait(smem_u32(&mbar[last % ST]), (last / ST) & 1, LIMIT)) {
+        const bool ok = !fail_sh && mbar_wait(smem_u32(&mbar[last % ST]), (last / ST) & 1, LIMIT);
+        if (!ok) {
             if (lane == 0) atomicExch(&fail_sh, 1);
+            mbar_wait(smem_u32(&mbar[last % ST]), (last / ST) & 1, kWaitLimitDefault);
         }
     }
     __syncthreads();
@@ -757,7 +766,7 @@ static cudaError_t launch_conv_tc_st(const bf16* in, int in_cs, int in_co, int C
     const long long positions = (long long)B * (H + 1) * (Wd + 1);
     dim3 grid((unsigned)((positions + 127) / 128), (unsigned)((Cout + N - 1) / N));
     conv3x3_tc_kernel<N, ST><<<grid, 256, smem, st>>>(in, in_cs, in_co, Cin, W, bias, out, out_cs, out_co, Cout, B, H,
-                                                      Wd, relu, err, band, stage_bytes);
+                                                      Wd, relu, err, band, stage_bytes, g_wait_limit);
     return cudaGetLastError();
 }
 
@@ -804,7 +813,7 @@ __global__ void __launch_bounds__(256) conv3x3_wgrad_tc_kernel(const bf16* __res
                                                                int Cout, const bf16* __restrict__ x, int x_cs,
                                                                int x_co, int Cin, float* __restrict__ dW, int B,
                                                                int H, int Wd, int* err, int band, int stage_bytes,
-                                                               int per_block) {
+                                                               int per_block, long long limit) {
     constexpr int M = 128, N = 32, KC = WGT_KC;
     extern __shared__ __align__(1024) unsigned char smem[];
     __shared__ __align__(8) unsigned long long mbar[ST];
@@ -842,7 +851,7 @@ __global__ void __launch_bounds__(256) conv3x3_wgrad_tc_kernel(const bf16* __res
     // BF16 A and B, F32 D, both operands MN-major (transpose bits 15 and 16)
     const unsigned idesc = (1u << 4) | (1u << 7) | (1u << 10) | (1u << 15) | (1u << 16) | ((unsigned)(N >> 3) << 17) |
                            ((unsigned)(M >> 4) << 24);
-    const long long LIMIT = 1LL << 26;
+    const long long LIMIT = limit;
     // the band of stage s: positions q0 - (W+2) .. q0 + KC + W, q0 = q_begin + s KC
     auto fill_pix = [&](int s) {
         const int qb = q_begin + s * KC - (Wp + 1);
@@ -915,10 +924,13 @@ __global__ void __launch_bounds__(256) conv3x3_wgrad_tc_kernel(const bf16* __res
     }
     cp_wait<0>();
     __syncthreads();
-    if (!fail_sh && issued > 0) {
+    // every MMA done before the TMEM is freed (see the forward kernel)
+    if (issued > 0) {
         const int last = issued - 1;
-        if (!mbar_wait(smem_u32(&mbar[last % ST]), (last / ST) & 1, LIMIT)) {
+        const bool ok = !fail_sh && mbar_wait(smem_u32(&mbar[last % ST]), (last / ST) & 1, LIMIT);
+        if (!ok) {
             if (lane == 0) atomicExch(&fail_sh, 1);
+            mbar_wait(smem_u32(&mbar[last % ST]), (last / ST) & 1, kWaitLimitDefault);
         }
     }
     __syncthreads();
@@ -979,11 +991,16 @@ static cudaError_t launch_wgrad_tc_st(const bf16* dy, int dy_cs, int dy_co, int 
     chunks = (total + per - 1) / per;
     dim3 grid((unsigned)chunks, (unsigned)ct, (unsigned)mt);
     conv3x3_wgrad_tc_kernel<ST><<<grid, 256, smem, st>>>(dy, dy_cs, dy_co, Cout, x, x_cs, x_co, Cin, dW, B, H, Wd, err,
-                                                         band, stage_bytes, (int)per);
+                                                         band, stage_bytes, (int)per, g_wait_limit);
     return cudaGetLastError();
 }
 
 }  // namespace mm
+
+extern "C" MM_API int mm_nn_set_wait_limit(long long iterations) {
+    g_wait_limit = iterations < 0 ? kWaitLimitDefault : iterations;
+    return MM_OK;
+}
 
 // tcgen05 variant of mm_nn_conv3x3_wgrad (dW accumulated, so zero it first; plus a device
 // error flag that a timed-out wait sets).

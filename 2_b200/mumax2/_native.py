@@ -170,6 +170,7 @@ _PROTOS = {
     "mm_set_table": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
     "mm_nn_conv3x3": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
                                 C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p]),
+    "mm_nn_set_wait_limit": (C.c_int, [C.c_longlong]),
     "mm_nn_conv3x3_wgrad_tc": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int,
                                          C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p]),
     "mm_nn_conv3x3_tc": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,

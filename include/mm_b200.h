@@ -304,6 +304,11 @@ MM_API int mm_save_wait(mm_plan plan);
  * gradient. */
 MM_API int mm_nn_conv3x3(const void* in, int in_cs, int in_co, int Cin, const void* W, const float* bias, void* out,
                          int out_cs, int out_co, int Cout, int B, int H, int Wd, int relu, mm_stream st);
+/* Iteration limit of the mbarrier waits in the tcgen05 kernels (default 2^26; a
+ * negative value restores it).  A wait that runs out sets the kernel's error flag and the
+ * block returns after its MMAs in flight are done; a limit of 0 makes every such wait run
+ * out at once, which tests use to check that the time-out is reported. */
+MM_API int mm_nn_set_wait_limit(long long iterations);
 /* tcgen05 weight gradient: dW[Cout][9][Cin] (FP32, accumulated: zero it first) of the 3x3
  * convolution from dY [B*H*W][dy_cs] (channels dy_co..+Cout) and X [B*H*W][x_cs]
  * (channels x_co..+Cin); channel counts, strides and offsets multiples of 8, W <= 256;

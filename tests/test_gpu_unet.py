@@ -212,3 +212,43 @@ def test_wgrad_tcgen05_matches(cin, cout, B, H, W):
     assert int(err.item()) == 0
     _, rdw, _ = R.conv3x3_backward(x, w, dy)
     assert _relnorm(dw.cpu().numpy().reshape(rdw.shape), rdw) < 1e-3
+
+
+def test_tcgen05_wait_timeout_is_reported():
+    """Failure detection without a fault: with the wait limit at 0 every mbarrier wait of
+    the tcgen05 kernels runs out, each kernel sets its error flag and returns after its
+    MMAs in flight are done; with the default limit restored the next calls are correct."""
+    import torch
+    import unet_ref as R
+    from mumax2 import _native as nat
+    L = nat.lib()
+    rng = np.random.default_rng(12)
+    cin, cout, B, H, W = 64, 32, 2, 16, 16
+    x = R.bf16(rng.normal(size=(B, H, W, cin)))
+    w = R.bf16(rng.normal(size=(cout, 9, cin)) / np.sqrt(9 * cin))
+    dy = R.bf16(rng.normal(size=(B, H, W, cout)))
+    xd, wd, dyd = _dev(x, torch.bfloat16), _dev(w, torch.bfloat16), _dev(dy, torch.bfloat16)
+    out = torch.zeros(B * H * W * cout, dtype=torch.bfloat16, device="cuda")
+    dw = torch.zeros(cout * 9 * cin, dtype=torch.float32, device="cuda")
+    err = torch.zeros(2, dtype=torch.int32, device="cuda")
+    ep0 = C.c_void_p(err.data_ptr())
+    ep1 = C.c_void_p(err.data_ptr() + 4)
+    nat.check(L.mm_nn_set_wait_limit(0))
+    try:
+        nat.check(L.mm_nn_conv3x3_tc(_p(xd), cin, 0, cin, _p(wd), None, _p(out), cout, 0, cout, B, H, W, 0, ep0, None))
+        nat.check(L.mm_nn_conv3x3_wgrad_tc(_p(dyd), cout, 0, cout, _p(xd), cin, 0, cin, _p(dw), B, H, W, ep1, None))
+        torch.cuda.synchronize()
+        assert err.cpu().tolist() == [1, 1]
+    finally:
+        nat.check(L.mm_nn_set_wait_limit(-1))
+    err.zero_()
+    dw.zero_()
+    nat.check(L.mm_nn_conv3x3_tc(_p(xd), cin, 0, cin, _p(wd), None, _p(out), cout, 0, cout, B, H, W, 0, ep0, None))
+    nat.check(L.mm_nn_conv3x3_wgrad_tc(_p(dyd), cout, 0, cout, _p(xd), cin, 0, cin, _p(dw), B, H, W, ep1, None))
+    torch.cuda.synchronize()
+    assert err.cpu().tolist() == [0, 0]
+    ref = R.conv3x3(x, w)
+    got = out.float().cpu().numpy().reshape(ref.shape)
+    assert np.abs(got - ref).max() <= 2 ** -7 * np.abs(ref).max() + 1e-6
+    _, rdw, _ = R.conv3x3_backward(x, w, dy)
+    assert _relnorm(dw.cpu().numpy().reshape(rdw.shape), rdw) < 1e-3

@@ -42,3 +42,27 @@ def test_replica_aggregation_world2():
     assert out[0][0] == pytest.approx(15.0) and out[1][0] == pytest.approx(15.0)
     assert out[0][1] == pytest.approx(1000 * 4 * 2 / 0.015)
     assert out[0][2] != out[1][2]
+
+
+def _failing_worker(rank, world, port):
+    import sys
+    sys.path.insert(0, ROOT)
+    import datetime
+    import torch.distributed as dist
+    import bench
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=10))
+    if rank == 1:
+        raise RuntimeError("replica 1 fails before its step")
+    bench.aggregate(10.0, cells=1000, steps=4, world=world, dist=dist, device="cpu")
+    dist.destroy_process_group()
+
+
+def test_failing_replica_is_reported():
+    """A rank that raises between steps ends the job with an error on the host: the
+    launcher reports it and stops the other rank, which would otherwise wait in its
+    collective until the process-group timeout."""
+    world = 2
+    port = _free_port()
+    with pytest.raises(mp.ProcessRaisedException, match="replica 1 fails"):
+        mp.start_processes(_failing_worker, args=(world, port), nprocs=world, start_method="spawn", join=True)
