@@ -262,69 +262,103 @@ __global__ void __launch_bounds__(128) conv3x3_wgrad_kernel(const bf16* __restri
 
 // ---------------------------------------------------------------- elementwise pieces
 // 2x2 average pool: out (H/2 x W/2) <- in (H x W), channel views
+// 2x2 average pooling, nearest upsampling and their gradients on NHWC views, 8 channels
+// (16 bytes) per thread; the sums run in the same order as per channel.
+__device__ __forceinline__ void ld8(const bf16* p, float v[8]) {
+    const uint4 u = *reinterpret_cast<const uint4*>(p);
+    const __nv_bfloat162* h = reinterpret_cast<const __nv_bfloat162*>(&u);
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const float2 f = __bfloat1622float2(h[k]);
+        v[2 * k] = f.x;
+        v[2 * k + 1] = f.y;
+    }
+}
+__device__ __forceinline__ void st8(bf16* p, const float v[8]) {
+    uint4 u;
+    __nv_bfloat162* h = reinterpret_cast<__nv_bfloat162*>(&u);
+#pragma unroll
+    for (int k = 0; k < 4; k++) h[k] = __floats2bfloat162_rn(v[2 * k], v[2 * k + 1]);
+    *reinterpret_cast<uint4*>(p) = u;
+}
+
 __global__ void pool_fwd_kernel(const bf16* in, int in_cs, int in_co, bf16* out, int out_cs, int out_co, int C, int B,
                                 int Ho, int Wo) {
-    const long long n = (long long)B * Ho * Wo * C;
+    const int G = C >> 3;
+    const long long n = (long long)B * Ho * Wo * G;
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
-        const int c = (int)(e % C);
-        const long long p = e / C;
+        const int g = (int)(e % G);
+        const long long p = e / G;
         const int x = (int)(p % Wo);
         const long long t = p / Wo;
         const int y = (int)(t % Ho), b = (int)(t / Ho);
         const int Wi = 2 * Wo, Hi = 2 * Ho;
-        float s = 0.f;
+        float s[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, v[8];
         for (int i = 0; i < 2; i++)
-            for (int j = 0; j < 2; j++)
-                s += __bfloat162float(in[(((long long)b * Hi + 2 * y + i) * Wi + 2 * x + j) * in_cs + in_co + c]);
-        out[p * out_cs + out_co + c] = __float2bfloat16_rn(0.25f * s);
+            for (int j = 0; j < 2; j++) {
+                ld8(in + (((long long)b * Hi + 2 * y + i) * Wi + 2 * x + j) * in_cs + in_co + 8 * g, v);
+#pragma unroll
+                for (int k = 0; k < 8; k++) s[k] += v[k];
+            }
+#pragma unroll
+        for (int k = 0; k < 8; k++) s[k] *= 0.25f;
+        st8(out + p * out_cs + out_co + 8 * g, s);
     }
 }
-// gradient of the pool, added into din (the skip branch already wrote its part there)
 __global__ void pool_bwd_kernel(const bf16* dout, int do_cs, int do_co, bf16* din, int di_cs, int di_co, int C, int B,
                                 int Ho, int Wo) {
-    const long long n = (long long)B * (2 * Ho) * (2 * Wo) * C;
+    const int G = C >> 3;
+    const long long n = (long long)B * (2 * Ho) * (2 * Wo) * G;
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
-        const int c = (int)(e % C);
-        const long long p = e / C;
+        const int g = (int)(e % G);
+        const long long p = e / G;
         const int Wi = 2 * Wo, Hi = 2 * Ho;
         const int x = (int)(p % Wi);
         const long long t = p / Wi;
         const int y = (int)(t % Hi), b = (int)(t / Hi);
-        const float g = 0.25f * __bfloat162float(dout[(((long long)b * Ho + y / 2) * Wo + x / 2) * do_cs + do_co + c]);
-        bf16* d = din + p * di_cs + di_co + c;
-        *d = __float2bfloat16_rn(__bfloat162float(*d) + g);
+        float gv[8], dv[8];
+        ld8(dout + (((long long)b * Ho + y / 2) * Wo + x / 2) * do_cs + do_co + 8 * g, gv);
+        bf16* d = din + p * di_cs + di_co + 8 * g;
+        ld8(d, dv);
+#pragma unroll
+        for (int k = 0; k < 8; k++) dv[k] = dv[k] + 0.25f * gv[k];
+        st8(d, dv);
     }
 }
-// nearest 2x upsample: out (2H x 2W) <- in (H x W)
 __global__ void up_fwd_kernel(const bf16* in, int in_cs, int in_co, bf16* out, int out_cs, int out_co, int C, int B,
                               int Hi, int Wi) {
-    const long long n = (long long)B * (2 * Hi) * (2 * Wi) * C;
+    const int G = C >> 3;
+    const long long n = (long long)B * (2 * Hi) * (2 * Wi) * G;
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
-        const int c = (int)(e % C);
-        const long long p = e / C;
+        const int g = (int)(e % G);
+        const long long p = e / G;
         const int Wo = 2 * Wi, Ho = 2 * Hi;
         const int x = (int)(p % Wo);
         const long long t = p / Wo;
         const int y = (int)(t % Ho), b = (int)(t / Ho);
-        out[p * out_cs + out_co + c] = in[(((long long)b * Hi + y / 2) * Wi + x / 2) * in_cs + in_co + c];
+        *reinterpret_cast<uint4*>(out + p * out_cs + out_co + 8 * g) =
+            *reinterpret_cast<const uint4*>(in + (((long long)b * Hi + y / 2) * Wi + x / 2) * in_cs + in_co + 8 * g);
     }
 }
-// gradient of the upsample: din (H x W) = sum of the 2x2 block of dout
 __global__ void up_bwd_kernel(const bf16* dout, int do_cs, int do_co, bf16* din, int di_cs, int di_co, int C, int B,
                               int Hi, int Wi) {
-    const long long n = (long long)B * Hi * Wi * C;
+    const int G = C >> 3;
+    const long long n = (long long)B * Hi * Wi * G;
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
-        const int c = (int)(e % C);
-        const long long p = e / C;
+        const int g = (int)(e % G);
+        const long long p = e / G;
         const int x = (int)(p % Wi);
         const long long t = p / Wi;
         const int y = (int)(t % Hi), b = (int)(t / Hi);
         const int Wo = 2 * Wi, Ho = 2 * Hi;
-        float s = 0.f;
+        float s[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, v[8];
         for (int i = 0; i < 2; i++)
-            for (int j = 0; j < 2; j++)
-                s += __bfloat162float(dout[(((long long)b * Ho + 2 * y + i) * Wo + 2 * x + j) * do_cs + do_co + c]);
-        din[p * di_cs + di_co + c] = __float2bfloat16_rn(s);
+            for (int j = 0; j < 2; j++) {
+                ld8(dout + (((long long)b * Ho + 2 * y + i) * Wo + 2 * x + j) * do_cs + do_co + 8 * g, v);
+#pragma unroll
+                for (int k = 0; k < 8; k++) s[k] += v[k];
+            }
+        st8(din + p * di_cs + di_co + 8 * g, s);
     }
 }
 // dpre = dout * (out > 0) in place on the gradient view
@@ -337,6 +371,53 @@ __global__ void relu_bwd_kernel(const bf16* out, int o_cs, int o_co, bf16* d, in
     }
 }
 // db[c] += sum_p d[p][c]
+// ReLU backward and bias gradient in one pass: each thread takes 8 consecutive channels
+// of a pixel (16-byte loads; consecutive threads cover consecutive channels, then the
+// next pixels), zeroes the gradient where the forward output was not positive (relu),
+// keeps 8 register sums for its channels, and the block adds its per-channel sums to db.
+__global__ void relu_bias_bwd_kernel(const bf16* __restrict__ out, int o_cs, int o_co, bf16* __restrict__ d, int d_cs,
+                                     int d_co, int C, long long P, long long ppb, int relu, float* __restrict__ db) {
+    __shared__ float acc[512];
+    const int G = C / 8;                       // threads per pixel
+    const int K = blockDim.x / G;              // pixels per block iteration
+    const int g = threadIdx.x % G, r = threadIdx.x / G;
+    for (int i = threadIdx.x; i < C; i += blockDim.x) acc[i] = 0.f;
+    __syncthreads();
+    const long long p0 = blockIdx.x * ppb, p1 = min(P, p0 + ppb);
+    float s[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    if (r < K) {
+        for (long long p = p0 + r; p < p1; p += K) {
+            uint4* gp = reinterpret_cast<uint4*>(d + p * d_cs + d_co + 8 * g);
+            uint4 gv = *gp;
+            __nv_bfloat162* gh = reinterpret_cast<__nv_bfloat162*>(&gv);
+            if (relu) {
+                const uint4 ov = *reinterpret_cast<const uint4*>(out + p * o_cs + o_co + 8 * g);
+                const __nv_bfloat162* oh = reinterpret_cast<const __nv_bfloat162*>(&ov);
+                bool changed = false;
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    const float2 of = __bfloat1622float2(oh[k]);
+                    float2 gf = __bfloat1622float2(gh[k]);
+                    if (!(of.x > 0.f)) { gf.x = 0.f; changed = true; }
+                    if (!(of.y > 0.f)) { gf.y = 0.f; changed = true; }
+                    gh[k] = __floats2bfloat162_rn(gf.x, gf.y);
+                }
+                if (changed) *gp = gv;
+            }
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const float2 gf = __bfloat1622float2(gh[k]);
+                s[2 * k] += gf.x;
+                s[2 * k + 1] += gf.y;
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < 8; k++) atomicAdd(&acc[8 * g + k], s[k]);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < C; i += blockDim.x) atomicAdd(db + i, acc[i]);
+}
+
 __global__ void bias_grad_kernel(const bf16* d, int d_cs, int d_co, int C, long long P, float* db) {
     const int c = blockIdx.y;
     float s = 0.f;
@@ -463,7 +544,9 @@ extern "C" MM_API int mm_nn_conv3x3_wgrad(const void* dy, int dy_cs, int dy_co, 
 
 extern "C" MM_API int mm_nn_pool(const void* in, int in_cs, int in_co, void* out, int out_cs, int out_co, int C, int B,
                                  int Ho, int Wo, int backward, mm_stream st) {
-    const long long n = (long long)B * Ho * Wo * C * (backward ? 4 : 1);
+    if (C % 8 || in_cs % 8 || in_co % 8 || out_cs % 8 || out_co % 8)
+        return report_error(MM_ERR_ARG, "mm_nn_pool: channel counts, strides and offsets must be multiples of 8");
+    const long long n = (long long)B * Ho * Wo * (C / 8) * (backward ? 4 : 1);
     if (backward)
         pool_bwd_kernel<<<grid1(n), 256, 0, (cudaStream_t)st>>>((const bf16*)in, in_cs, in_co, (bf16*)out, out_cs,
                                                                  out_co, C, B, Ho, Wo);
@@ -476,7 +559,9 @@ extern "C" MM_API int mm_nn_pool(const void* in, int in_cs, int in_co, void* out
 
 extern "C" MM_API int mm_nn_upsample(const void* in, int in_cs, int in_co, void* out, int out_cs, int out_co, int C,
                                      int B, int Hi, int Wi, int backward, mm_stream st) {
-    const long long n = (long long)B * Hi * Wi * C * (backward ? 1 : 4);
+    if (C % 8 || in_cs % 8 || in_co % 8 || out_cs % 8 || out_co % 8)
+        return report_error(MM_ERR_ARG, "mm_nn_upsample: channel counts, strides and offsets must be multiples of 8");
+    const long long n = (long long)B * Hi * Wi * (C / 8) * (backward ? 1 : 4);
     if (backward)
         up_bwd_kernel<<<grid1(n), 256, 0, (cudaStream_t)st>>>((const bf16*)in, in_cs, in_co, (bf16*)out, out_cs, out_co,
                                                                C, B, Hi, Wi);
@@ -490,6 +575,23 @@ extern "C" MM_API int mm_nn_upsample(const void* in, int in_cs, int in_co, void*
 extern "C" MM_API int mm_nn_relu_bwd(const void* out, int o_cs, int o_co, void* d, int d_cs, int d_co, int C,
                                      long long P, mm_stream st) {
     relu_bwd_kernel<<<grid1(P * C), 256, 0, (cudaStream_t)st>>>((const bf16*)out, o_cs, o_co, (bf16*)d, d_cs, d_co, C, P);
+    NN_CHECK();
+    return MM_OK;
+}
+
+extern "C" MM_API int mm_nn_relu_bias_bwd(const void* out, int o_cs, int o_co, void* d, int d_cs, int d_co, int C,
+                                          long long P, int relu, float* db, mm_stream st) {
+    if (C < 8 || C > 512 || C % 8 || o_cs % 8 || o_co % 8 || d_cs % 8 || d_co % 8 || P < 0)
+        return report_error(MM_ERR_ARG, "mm_nn_relu_bias_bwd: C in 8..512, channel counts, strides and offsets multiples of 8");
+    const int G = C / 8;
+    const int K = G >= 256 ? 1 : 256 / G;
+    const long long blocks = 148LL * 4;
+    long long ppb = (P + blocks - 1) / blocks;
+    if (ppb < K) ppb = K;
+    const long long nb = (P + ppb - 1) / ppb;
+    if (nb > 0)
+        relu_bias_bwd_kernel<<<(unsigned)nb, G * K, 0, (cudaStream_t)st>>>((const bf16*)out, o_cs, o_co, (bf16*)d, d_cs,
+                                                                           d_co, C, P, ppb, relu, db);
     NN_CHECK();
     return MM_OK;
 }

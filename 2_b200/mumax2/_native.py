@@ -183,6 +183,8 @@ _PROTOS = {
                                  C.c_int, C.c_int, C.c_int, C.c_void_p]),
     "mm_nn_relu_bwd": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_longlong,
                                  C.c_void_p]),
+    "mm_nn_relu_bias_bwd": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_int,
+                                      C.c_longlong, C.c_int, C.c_void_p, C.c_void_p]),
     "mm_nn_bias_grad": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_longlong, C.c_void_p, C.c_void_p]),
     "mm_nn_mse": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_longlong, C.c_float, C.c_void_p, C.c_int,
                             C.c_void_p, C.c_void_p]),

@@ -282,9 +282,9 @@ class UNet:
                 lvl = BUFFERS[iv][0]
                 P = B * (H >> lvl) * (W >> lvl)
                 d = self.p[name]
-                if relu:
-                    nat.check(L.mm_nn_relu_bwd(self._ptr(self.buf[ov]), self._cs((ov,)), oo, self._ptr(self.grad[ov]),
-                                               self._cs((ov,)), oo, cout, P, None))
+                # ReLU backward (in place) and the bias gradient in one pass
+                nat.check(L.mm_nn_relu_bias_bwd(self._ptr(self.buf[ov]), self._cs((ov,)), oo, self._ptr(self.grad[ov]),
+                                                self._cs((ov,)), oo, cout, P, 1 if relu else 0, fp(d["gb"]), None))
                 if self.tcgen05_wgrad:
                     nat.check(L.mm_nn_conv3x3_wgrad_tc(self._ptr(self.grad[ov]), self._cs((ov,)), oo, cout,
                                                        self._ptr(self.buf[iv]), self._cs((iv,)), io, cin, fp(d["gw"]),
@@ -293,7 +293,6 @@ class UNet:
                     nat.check(L.mm_nn_conv3x3_wgrad(self._ptr(self.grad[ov]), self._cs((ov,)), oo, cout,
                                                     self._ptr(self.buf[iv]), self._cs((iv,)), io, cin, fp(d["gw"]),
                                                     B, H >> lvl, W >> lvl, None))
-                nat.check(L.mm_nn_bias_grad(self._ptr(self.grad[ov]), self._cs((ov,)), oo, cout, P, fp(d["gb"]), None))
                 if name != "e0a":
                     # dX over the whole input view (a concatenated input gets both parts)
                     self._conv(self.grad[ov], self._cs((ov,)), oo, d["cin_t"], d["wt"], None, self.grad[iv],

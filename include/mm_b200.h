@@ -327,6 +327,11 @@ MM_API int mm_nn_upsample(const void* in, int in_cs, int in_co, void* out, int o
                           int Hi, int Wi, int backward, mm_stream st);
 MM_API int mm_nn_relu_bwd(const void* out, int o_cs, int o_co, void* d, int d_cs, int d_co, int C, long long P,
                           mm_stream st);
+/* ReLU backward (relu != 0: d = 0 where out <= 0, in place) and bias gradient
+ * db[c] += sum_p d[p][c] in one pass over P pixels of C <= 512 channels (channel counts,
+ * strides and offsets multiples of 8). */
+MM_API int mm_nn_relu_bias_bwd(const void* out, int o_cs, int o_co, void* d, int d_cs, int d_co, int C, long long P,
+                               int relu, float* db, mm_stream st);
 MM_API int mm_nn_bias_grad(const void* d, int d_cs, int d_co, int C, long long P, float* db, mm_stream st);
 MM_API int mm_nn_mse(const void* out, int o_cs, const float* target, const float* mask, long long P, float norm,
                      void* dout, int d_cs, float* loss, mm_stream st);

@@ -91,12 +91,14 @@ def test_network_gradients_match_oracle(tcgen05, wgrad):
     arch = (U.BUFFERS, U.CONVS, U.POOLS, U.UPS, U.SCHEDULE)
     rloss, rgrads, rout = R.forward_backward(arch, params, feats, target, mask, H, W)
     assert loss == pytest.approx(rloss, rel=1e-2)
-    errs = {}
+    errs, berrs = {}, {}
     for name, (dw, db) in rgrads.items():
         d = net.p[name]
         errs[name] = _relnorm(d["gw"].cpu().numpy().reshape(dw.shape), dw)
-    print(errs)
+        berrs[name] = _relnorm(d["gb"].cpu().numpy(), db)
+    print(errs, berrs)
     assert max(errs.values()) < 3e-2
+    assert max(berrs.values()) < 3e-2
 
 
 def test_training_lowers_the_loss():
@@ -252,3 +254,21 @@ def test_tcgen05_wait_timeout_is_reported():
     assert np.abs(got - ref).max() <= 2 ** -7 * np.abs(ref).max() + 1e-6
     _, rdw, _ = R.conv3x3_backward(x, w, dy)
     assert _relnorm(dw.cpu().numpy().reshape(rdw.shape), rdw) < 1e-3
+
+
+@pytest.mark.parametrize("C,P,relu", [(16, 5000, 1), (32, 70000, 1), (384, 3000, 1), (64, 777, 0), (256, 12345, 1)])
+def test_relu_bias_bwd_matches(C, P, relu):
+    """The fused ReLU backward and bias gradient: the masked gradient exactly, the channel
+    sums to 1e-5 relative (FP32 sums in another order)."""
+    import torch
+    import unet_ref as R
+    from mumax2 import _native as nat
+    rng = np.random.default_rng(C + P)
+    out = R.bf16(rng.normal(size=(P, C)))
+    d = R.bf16(rng.normal(size=(P, C)))
+    od, dd = _dev(out, torch.bfloat16), _dev(d, torch.bfloat16)
+    db = torch.zeros(C, dtype=torch.float32, device="cuda")
+    nat.check(nat.lib().mm_nn_relu_bias_bwd(_p(od), C, 0, _p(dd), C, 0, C, P, relu, _p(db), None))
+    ref = np.where(out > 0, d, 0.0) if relu else d
+    assert np.array_equal(dd.float().cpu().numpy().reshape(P, C), ref)
+    assert _relnorm(db.cpu().numpy(), ref.sum(axis=0)) < 1e-5
