@@ -164,48 +164,47 @@ __global__ void __launch_bounds__(128) conv3x3_fwd_kernel(const bf16* __restrict
 __global__ void __launch_bounds__(128) conv3x3_wgrad_kernel(const bf16* __restrict__ dy, int dy_cs, int dy_co, int Cout,
                                                             const bf16* __restrict__ x, int x_cs, int x_co, int Cin,
                                                             float* __restrict__ dW, int B, int H, int Wd,
-                                                            long long pix_per_block) {
+                                                            int pix_per_block) {
     __shared__ __align__(128) bf16 sA[2][WG_BK * WG_PA];  // [pixel][co]
     __shared__ __align__(128) bf16 sB[2][WG_BK * WG_PB];  // [pixel][(tap, ci)]
-    const long long P = (long long)B * H * Wd;
+    const int P = B * H * Wd;
     const int m0 = blockIdx.x * WG_BM;
     const int n0 = blockIdx.y * WG_BN;
     const int Ncols = 9 * Cin;
-    const long long pstart = (long long)blockIdx.z * pix_per_block;
-    const long long pend = pstart + pix_per_block < P ? pstart + pix_per_block : P;
+    const int pstart = blockIdx.z * pix_per_block;
+    const int pend = pstart + pix_per_block < P ? pstart + pix_per_block : P;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int wm = (warp & 1) * 32, wn = (warp >> 1) * 32;
-    auto load = [&](int stage, long long pk) {
+    auto load = [&](int stage, int pk) {
         // A: 32 pixels x 64 channels = 256 chunks of 8 channels; 2 per thread
 #pragma unroll
         for (int r = 0; r < 2; r++) {
             const int c = tid + r * 128;
             const int row = c >> 3, ch = (c & 7) * 8;
-            const long long p = pk + row;
+            const int p = pk + row;
             const bool ok = p < pend && m0 + ch < Cout;
-            cp_async16(&sA[stage][row * WG_PA + ch], dy + (ok ? p : 0) * dy_cs + dy_co + (ok ? m0 + ch : 0), ok);
+            cp_async16(&sA[stage][row * WG_PA + ch], dy + (long long)(ok ? p : 0) * dy_cs + dy_co + (ok ? m0 + ch : 0),
+                       ok);
         }
         // B: 32 pixels x 64 (tap, ci) columns, 8 columns (one tap, 8 channels) per chunk
 #pragma unroll
         for (int r = 0; r < 2; r++) {
             const int c = tid + r * 128;
             const int row = c >> 3, col = (c & 7) * 8;
-            const long long p = pk + row;
+            const int p = pk + row;
             const int n = n0 + col;
             bool ok = p < pend && n < Ncols;
-            long long q = 0;
-            int ci = 0;
-            if (ok) {
+            int q = 0, ci = 0;
+            if (ok) {   // 32-bit index arithmetic (the host checks that the pixels fit)
                 const int tap = n / Cin;
                 ci = n - tap * Cin;
-                const int xx0 = (int)(p % Wd);
-                const long long tt = p / Wd;
-                const int yy = (int)(tt % H) + tap / 3 - 1, xx = xx0 + tap % 3 - 1;
-                const int bb = (int)(tt / H);
+                const int tt = p / Wd, xx0 = p - tt * Wd;
+                const int bb = tt / H, yy0 = tt - bb * H;
+                const int yy = yy0 + tap / 3 - 1, xx = xx0 + tap % 3 - 1;
                 ok = yy >= 0 && yy < H && xx >= 0 && xx < Wd;
-                q = ((long long)bb * H + yy) * Wd + xx;
+                q = (bb * H + yy) * Wd + xx;
             }
-            cp_async16(&sB[stage][row * WG_PB + col], x + (ok ? q : 0) * x_cs + x_co + (ok ? ci : 0), ok);
+            cp_async16(&sB[stage][row * WG_PB + col], x + (long long)(ok ? q : 0) * x_cs + x_co + (ok ? ci : 0), ok);
         }
     };
     float acc[2][4][4];
@@ -215,11 +214,11 @@ __global__ void __launch_bounds__(128) conv3x3_wgrad_kernel(const bf16* __restri
         for (int j = 0; j < 4; j++)
 #pragma unroll
             for (int q = 0; q < 4; q++) acc[i][j][q] = 0.f;
-    const long long nk = (pend - pstart + WG_BK - 1) / WG_BK;
+    const int nk = (pend - pstart + WG_BK - 1) / WG_BK;
     if (nk <= 0) return;
     load(0, pstart);
     cp_commit();
-    for (long long kk = 0; kk < nk; kk++) {
+    for (int kk = 0; kk < nk; kk++) {
         const int st = (int)(kk & 1);
         if (kk + 1 < nk) load(st ^ 1, pstart + (kk + 1) * WG_BK);
         cp_commit();
@@ -527,6 +526,7 @@ extern "C" MM_API int mm_nn_conv3x3_wgrad(const void* dy, int dy_cs, int dy_co, 
                                           int x_co, int Cin, float* dW, int B, int H, int Wd, mm_stream st) {
     if (Cin % 8 || Cout % 8 || dy_cs % 8 || dy_co % 8 || x_cs % 8 || x_co % 8)
         return report_error(MM_ERR_ARG, "mm_nn_conv3x3_wgrad: channel counts, strides and offsets must be multiples of 8");
+    if ((long long)B * H * Wd >= (1LL << 30)) return report_error(MM_ERR_ARG, "mm_nn_conv3x3_wgrad: too many pixels");
     const long long P = (long long)B * H * Wd;
     const int mt = (Cout + WG_BM - 1) / WG_BM, nt = (9 * Cin + WG_BN - 1) / WG_BN;
     // split the pixels so that about 4 waves of blocks cover the GPU
@@ -537,7 +537,7 @@ extern "C" MM_API int mm_nn_conv3x3_wgrad(const void* dy, int dy_cs, int dy_co, 
     splits = (P + ppb - 1) / ppb;
     dim3 grid((unsigned)mt, (unsigned)nt, (unsigned)splits);
     conv3x3_wgrad_kernel<<<grid, 128, 0, (cudaStream_t)st>>>((const bf16*)dy, dy_cs, dy_co, Cout, (const bf16*)x, x_cs,
-                                                             x_co, Cin, dW, B, H, Wd, ppb);
+                                                             x_co, Cin, dW, B, H, Wd, (int)ppb);
     NN_CHECK();
     return MM_OK;
 }
