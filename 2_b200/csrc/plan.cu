@@ -1000,15 +1000,22 @@ static int autotune(mm_plan p) {
         reps = std::max(5, std::min(200, (int)(2000.f / std::max(best, 1.f))));
         rc = time_eval(&best);
     }
+    // a variant whose launch fails (a refused shared-memory size, say) is dropped: its
+    // error is not sticky, so it is cleared and the previous choice kept
+    auto try_variant = [&](float* t) -> bool {
+        if (time_eval(t) == MM_OK) return true;
+        cudaGetLastError();
+        cudaStreamSynchronize(st);
+        return false;
+    };
     const int lo[3] = {-1, -1, -1}, hi[3] = {1, 1, 0};
     for (int d = 0; d < 3 && !rc; d++) {
         int keep = p->tiles[d];
-        for (int v = lo[d]; v <= hi[d] && !rc; v++) {
+        for (int v = lo[d]; v <= hi[d]; v++) {
             if (v == keep) continue;
             p->tiles[d] = v;
             float t = 0.f;
-            if ((rc = time_eval(&t))) break;
-            if (t < 0.98f * best) {
+            if (try_variant(&t) && t < 0.98f * best) {
                 best = t;
                 keep = v;
             }
@@ -1019,10 +1026,8 @@ static int autotune(mm_plan p) {
     if (!rc && fused2d_ok(p->g.n)) {
         p->tiles[3] = 1;
         float t = 0.f;
-        if (!(rc = time_eval(&t))) {
-            if (t < 0.98f * best) best = t;
-            else p->tiles[3] = 0;
-        }
+        if (try_variant(&t) && t < 0.98f * best) best = t;
+        else p->tiles[3] = 0;
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
