@@ -198,6 +198,13 @@ struct EpiArgs {
     int skip_retry;
     long long spec_bstride;    // complex elements between simulations in the spectrum
     double t_eval;             // time of a standalone evaluation (time tables)
+    // Row transform of the next stage state (four-step epilogue with op.do_combine only):
+    // when fwd is set, the epilogue also writes the R2C rows of next (times the Msat mask
+    // if fwd_mask) into fwd, the spectrum rows it has read, so that the next evaluation
+    // starts at its column pass.
+    float2* fwd;
+    int fwd_mask;
+    int fwd_pad;
 };
 
 // ---- launchers (conv.cu, rhs.cu)
@@ -243,6 +250,9 @@ cudaError_t am_copy(PP src, PP dst, const DevCtl* ctl, long long n3, int nsim, i
 cudaError_t am_normalize(PP m, const float* msat_mask, const DevCtl* ctl, long long N, long long mask_bstride, int nsim,
                          int bps, int skip, cudaStream_t st);
 int xinv_blocks(int M, int n0n1);
+// whether the C2R + epilogue pass for row length M can also write the R2C rows of the
+// next stage state (EpiArgs::fwd)
+bool epi_r2c_supported(int M);
 int report_error(int code, const char* msg);  // sets mm_last_error()
 int local_blocks(long long N, int nsim = 1);
 

@@ -448,6 +448,9 @@ struct mm_plan_s {
     // evaluation time measured with them (0 if not tuned)
     int tiles[4] = {0, 0, 0, 0};     // [3]: fused single-layer evaluation (fused2d_kernel)
     float tuned_us = 0.f;
+    // the epilogue of a stage that forms the next stage state also writes its R2C rows
+    // (MM_EPI_R2C=0 in the environment at plan creation turns this off)
+    bool epi_r2c = true;
     long long n3() const { return 3 * g.N; }
     long long spec_bstride() const { return 3LL * g.n[0] * g.L[1] * g.hp; }
 };
@@ -745,6 +748,10 @@ extern "C" MM_API int mm_plan_create_batch(const mm_problem* prob, int nsim, con
         mm_plan_destroy(p);
         return set_err(MM_ERR_CUDA, "ctl init failed");
     }
+    {
+        const char* e = getenv("MM_EPI_R2C");
+        p->epi_r2c = !(e && e[0] == '0');
+    }
     if ((rc = autotune(p))) {
         mm_plan_destroy(p);
         return rc;
@@ -852,8 +859,10 @@ static bool zreg_ok(const ConvGeom& g) {
 // ---------------------------------------------------------------- one evaluation
 // Launches of the five (3-D) or three (2-D) convolution passes for all simulations;
 // `ev` (optional) receives an event record after each pass.
+// rows_ready: the R2C rows of m_in are already in the spectrum (written by the epilogue
+// of the evaluation that formed m_in), so the row pass is left out.
 static int launch_conv(mm_plan p, PP m_in, const DevCtl* ctl, int skip_retry, cudaStream_t st,
-                       const std::vector<cudaEvent_t>* ev = nullptr) {
+                       const std::vector<cudaEvent_t>* ev = nullptr, bool rows_ready = false) {
     const ConvGeom& g = p->g;
     const int n0 = g.n[0], n1 = g.n[1], n2 = g.n[2];
     const int L0 = g.L[0], L1 = g.L[1];
@@ -870,8 +879,11 @@ static int launch_conv(mm_plan p, PP m_in, const DevCtl* ctl, int skip_retry, cu
     int rc;
     // demagexch convolves m itself (mod_demagexchange.go:207-209), demag convolves Ms_mask m
     const float* in_mask = p->khat_d ? nullptr : p->P.msat_mask;
-    CUCHK(launch_xfwd<float2, float>(g.M, nullptr, m_in, in_mask, p->S, 3 * n0 * n1, n0, n1, L1, n2, n2, g.hp,
-                                     p->tw, ctl, skip_retry, st, ns, p->n3(), sb, p->P.mask_bstride, p->tiles[0]));
+    if (!rows_ready) {
+        CUCHK(launch_xfwd<float2, float>(g.M, nullptr, m_in, in_mask, p->S, 3 * n0 * n1, n0, n1, L1, n2, n2, g.hp,
+                                         p->tw, ctl, skip_retry, st, ns, p->n3(), sb, p->P.mask_bstride, p->tiles[0]));
+        p->launches++;
+    }
     if ((rc = mark())) return rc;
     if (L0 == 1) {
         CUCHK(launch_colmul(L1, p->S, p->kv, g.h, 1, plane, 0, g.hp, n1, 1, scale, p->tw, ctl, skip_retry, st, ns, sb,
@@ -892,14 +904,25 @@ static int launch_conv(mm_plan p, PP m_in, const DevCtl* ctl, int skip_retry, cu
                                     sb, p->tiles[1]));
         if ((rc = mark())) return rc;
     }
-    p->launches += (L0 == 1) ? 2 : 4;
+    p->launches += (L0 == 1) ? 1 : 3;
     return MM_OK;
 }
 
+// Whether an evaluation of this plan can hand the R2C rows of the next stage state to
+// the following evaluation: the four-step row and epilogue passes, not the fused
+// single-layer kernel.
+static bool epi_r2c_ok(mm_plan p) {
+    return p->epi_r2c && p->demag && epi_r2c_supported(p->g.M) && !(p->tiles[3] && fused2d_ok(p->g.n));
+}
+
 // Launches the convolution passes (if demag) and the epilogue for one StageOp.
+// fwd: EVAL_EMIT_ROWS = the epilogue also writes the R2C rows of op.next (the m_in of the
+// evaluation that follows); EVAL_ROWS_READY = the R2C rows of op.m_in are in the spectrum.
+// Both only where epi_r2c_ok(p).
+enum { EVAL_EMIT_ROWS = 1, EVAL_ROWS_READY = 2 };
 static int launch_eval(mm_plan p, const StageOp& op, DevCtl* ctl, int skip_retry, float* const* dbg,
                        long long noise_step, double dt_thermal, float* red, unsigned int* tq_out, cudaStream_t st,
-                       int* nblocks_out) {
+                       int* nblocks_out, int fwd = 0) {
     const ConvGeom& g = p->g;
     EpiArgs A;
     memset(&A, 0, sizeof A);
@@ -918,6 +941,11 @@ static int launch_eval(mm_plan p, const StageOp& op, DevCtl* ctl, int skip_retry
     A.skip_retry = skip_retry;
     A.spec_bstride = p->spec_bstride();
     A.t_eval = p->t_eval;
+    if (fwd && (terms || !epi_r2c_ok(p))) fwd = 0;  // the per-term epilogue has no row output
+    if ((fwd & EVAL_EMIT_ROWS) && op.do_combine) {
+        A.fwd = p->S;
+        A.fwd_mask = p->khat_d ? 0 : 1;
+    }
     int nb = 0, rc;
     if (p->demag && p->tiles[3] && !terms && fused2d_ok(g.n)) {
         const float* in_mask = p->khat_d ? nullptr : p->P.msat_mask;
@@ -928,7 +956,7 @@ static int launch_eval(mm_plan p, const StageOp& op, DevCtl* ctl, int skip_retry
         return MM_OK;
     }
     if (p->demag) {
-        if ((rc = launch_conv(p, op.m_in, ctl, skip_retry, st))) return rc;
+        if ((rc = launch_conv(p, op.m_in, ctl, skip_retry, st, nullptr, (fwd & EVAL_ROWS_READY) != 0))) return rc;
         CUCHK(launch_xinv_epi(g.M, p->S, g.hp, g.L[1], p->tw, A, terms, st, &nb, p->nsim, p->tiles[2]));
     } else {
         CUCHK(launch_local_epi(A, terms, st, &nb, p->nsim));
@@ -1414,7 +1442,9 @@ static int enqueue_attempt(mm_plan p, cudaStream_t st) {
         }
         const int skip = (s == MM_RK12) ? 1 : 0;
         o0.c_time = 0.0;
-        if ((rc = launch_eval(p, o0, ctl, skip, nullptr, 0, 0, nullptr, nullptr, st, nullptr))) return rc;
+        // Heun's predictor Ma is the corrector's input: its rows come from this epilogue
+        const int fwd0 = (s == MM_HEUN) ? EVAL_EMIT_ROWS : 0;
+        if ((rc = launch_eval(p, o0, ctl, skip, nullptr, 0, 0, nullptr, nullptr, st, nullptr, fwd0))) return rc;
         if (p->run_until) {
             CUCHK(launch_controller(p, st, 2, 0, 0, 0, 0, 0));
             p->launches++;
@@ -1447,7 +1477,8 @@ static int enqueue_attempt(mm_plan p, cudaStream_t st) {
                 o1.ep[1] = fixed(p->Kst[0]);
                 o1.ek[1] = -1.0;
             }
-            if ((rc = launch_eval(p, o1, ctl, 0, nullptr, 0, 0, nullptr, nullptr, st, nullptr))) return rc;
+            const int fwd1 = (s == MM_HEUN) ? EVAL_ROWS_READY : 0;
+            if ((rc = launch_eval(p, o1, ctl, 0, nullptr, 0, 0, nullptr, nullptr, st, nullptr, fwd1))) return rc;
         }
         CUCHK(launch_controller(p, st, 1, s == MM_RK12 ? 1 : 0, 1, 0, s == MM_EULER ? 1 : 2, s == MM_RK12));
         p->launches++;
@@ -1503,7 +1534,10 @@ static int enqueue_attempt(mm_plan p, cudaStream_t st) {
                 o.ne++;
             }
         }
-        if ((rc = launch_eval(p, o, ctl, 0, nullptr, 0, 0, nullptr, nullptr, st, nullptr))) return rc;
+        // stage i + 1 reads mbuf(i + 1), which this epilogue forms: its rows come from here
+        int fwd = (i + 1 < S) ? EVAL_EMIT_ROWS : 0;
+        if (i > 1) fwd |= EVAL_ROWS_READY;
+        if ((rc = launch_eval(p, o, ctl, 0, nullptr, 0, 0, nullptr, nullptr, st, nullptr, fwd))) return rc;
     }
     CUCHK(launch_controller(p, st, 1, 1, dp ? 4 : 2, 1, S - 1, 0));
     p->launches++;

@@ -306,8 +306,11 @@ struct ThreadRed {
     KSum e[4];
 };
 
+// stg (optional): receives the next state as the R2C row pass would read it, i.e. the
+// stored value times the Msat mask when fwd_mask (the convolution input Ms_mask * m).
 __device__ __forceinline__ void cell_post(const FieldParams& P, const StageOp& op, const ResolvedOp& r, long long i,
-                                          long long mo, float3 m0, float3 k, ThreadRed& tr) {
+                                          long long mo, float3 m0, float3 k, ThreadRed& tr, float3* stg = nullptr,
+                                          int fwd_mask = 0) {
     const long long N = P.N;
     if (!(isfinite(k.x) && isfinite(k.y) && isfinite(k.z))) tr.bad = 1;
     if (r.k_out) {
@@ -331,9 +334,14 @@ __device__ __forceinline__ void cell_post(const FieldParams& P, const StageOp& o
         float mn = sqrtf(v.x * v.x + v.y * v.y + v.z * v.z);
         float sc = (norm == 0.0f) ? 0.0f : 1.0f;
         sc = (mn != 0.0f) ? sc / mn : 0.0f;
-        r.next[i] = v.x * sc;
-        r.next[N + i] = v.y * sc;
-        r.next[2 * N + i] = v.z * sc;
+        const float3 nx = make_float3(v.x * sc, v.y * sc, v.z * sc);
+        r.next[i] = nx.x;
+        r.next[N + i] = nx.y;
+        r.next[2 * N + i] = nx.z;
+        if (stg) {
+            const float fm = fwd_mask ? norm : 1.0f;
+            *stg = make_float3(nx.x * fm, nx.y * fm, nx.z * fm);
+        }
     }
     if (op.ne > 0) {
         float3 e = make_float3(0.f, 0.f, 0.f);
@@ -436,17 +444,17 @@ template <bool TERMS>
 __device__ __forceinline__ void process_cell(const EpiArgs& A, const SimScalars& S, const float* m,
                                              const ResolvedOp& r, float* const* dbg, long long i, long long mo,
                                              int z, int y, int x, float3 hd, long long ns, float dtth,
-                                             ThreadRed& tr) {
+                                             ThreadRed& tr, float3* stg = nullptr) {
     float3 m0;
     if (TERMS) {
         CellTerms t = {};
         float3 k = cell_rhs<true>(A.P, S, m, i, mo, z, y, x, hd, ns, dtth, m0, &t);
         if (A.op.want_energy) energy_acc(A.P, i, m0, t, tr);
         write_terms(dbg, A.P.N, i, t);
-        cell_post(A.P, A.op, r, i, mo, m0, k, tr);
+        cell_post(A.P, A.op, r, i, mo, m0, k, tr, stg, A.fwd_mask);
     } else {
         float3 k = cell_rhs<false>(A.P, S, m, i, mo, z, y, x, hd, ns, dtth, m0, nullptr);
-        cell_post(A.P, A.op, r, i, mo, m0, k, tr);
+        cell_post(A.P, A.op, r, i, mo, m0, k, tr, stg, A.fwd_mask);
     }
 }
 
@@ -519,9 +527,12 @@ __device__ __forceinline__ const SimScalars& pick_scalars(const SimScalars& stag
 // ---------------------------------------------------------------- C2R row pass + epilogue
 // Cells of the block's rows; H_demag of (row, c) at cell x is element x>>1 (real part for
 // even x, imaginary part for odd x) of shared-memory line (lrow*3 + c), stride LS.
-template <bool TERMS, bool PADDED, bool BATCH>
+// FWD: float x of line (lrow, c) then takes the cell's next state (times the Msat mask
+// when A.fwd_mask) for the R2C rows of the next evaluation (four-step lines only).
+template <bool TERMS, bool PADDED, bool BATCH, bool FWD = false>
 __device__ __forceinline__ void epilogue_rows(const EpiArgs& A, const SimScalars& S, const float2* sm, int LS,
                                               int row0, int nrow_here) {
+    static_assert(!(FWD && (PADDED || TERMS)), "row output: four-step lines, no per-term outputs");
     const int n1 = A.P.n[1], n2 = A.P.n[2];
     const DevCtl* ctl;
     ResolvedOp r;
@@ -544,7 +555,17 @@ __device__ __forceinline__ void epilogue_rows(const EpiArgs& A, const SimScalars
         const float2 v1 = sm[(lrow * 3 + 1) * LS + pi];
         const float2 v2 = sm[(lrow * 3 + 2) * LS + pi];
         const float3 hd = (x & 1) ? make_float3(v0.y, v1.y, v2.y) : make_float3(v0.x, v1.x, v2.x);
-        process_cell<TERMS>(A, S, m, r, dbg, i, mo, z, y, x, hd, ns, dtth, tr);
+        if constexpr (FWD) {
+            // float x of line (lrow, c) held H_demag of this cell only
+            float3 nx = make_float3(0.f, 0.f, 0.f);
+            process_cell<TERMS>(A, S, m, r, dbg, i, mo, z, y, x, hd, ns, dtth, tr, &nx);
+            float* fl = reinterpret_cast<float*>(const_cast<float2*>(sm)) + 2 * (long long)(lrow * 3) * LS + x;
+            fl[0] = nx.x;
+            fl[2 * LS] = nx.y;
+            fl[4 * LS] = nx.z;
+        } else {
+            process_cell<TERMS>(A, S, m, r, dbg, i, mo, z, y, x, hd, ns, dtth, tr);
+        }
         // advance by blockDim.x cells
         x += dx;
         int adv = dr;
@@ -613,8 +634,13 @@ __host__ __device__ constexpr int xinv4_rows_c() {
                                                                                           : xinv4_rpb<M>();
 }
 
-template <int M, bool TERMS, bool BATCH, bool HALF>
-__device__ __forceinline__ void xinv4_epi_body(const float2* __restrict__ S, int hp, int L1,
+// The spectrum argument of the C2R + epilogue pass: read-only, except in the FWD variant,
+// which writes the R2C rows of the next stage state back into the rows it has read.
+template <bool FWD> struct SpecIn { using type = const float2* __restrict__; };
+template <> struct SpecIn<true> { using type = const float2*; };
+
+template <int M, bool TERMS, bool BATCH, bool HALF, bool FWD>
+__device__ __forceinline__ void xinv4_epi_body(typename SpecIn<FWD>::type S, int hp, int L1,
                                                const float2* __restrict__ tw, const EpiArgs& A) {
     pdl_begin();
     constexpr int RPB = xinv4_rows_c<M, HALF>();
@@ -663,24 +689,64 @@ __device__ __forceinline__ void xinv4_epi_body(const float2* __restrict__ S, int
     }
     __syncthreads();
     const int row0 = blockIdx.x * RPB;
-    epilogue_rows<TERMS, false, BATCH>(A, pick_scalars<BATCH>(s_sim, A.P.s), sm, F::LBUF, row0,
-                                       min(RPB, nrows - row0));
+    epilogue_rows<TERMS, false, BATCH, FWD>(A, pick_scalars<BATCH>(s_sim, A.P.s), sm, F::LBUF, row0,
+                                            min(RPB, nrows - row0));
+    if constexpr (FWD) {
+        // R2C rows of the next stage state (float x of line (lr, c) = its value at cell x,
+        // staged by epilogue_rows) into the rows of the spectrum this block has read: the
+        // packing, transform and post-processing of xfwd4_kernel, value for value, so the
+        // spectrum is the one the separate row pass would write from the stored state.
+        __syncthreads();
+        const float* fl = reinterpret_cast<const float*>(buf);
+        const int n_in = A.P.n[2];
+#pragma unroll
+        for (int j = 0; j < F::P1; j++) {
+            const int n = F::in_index(t, j);
+            float a = 0.f, b = 0.f;
+            if (active) {
+                if (2 * n < n_in) a = fl[2 * n];
+                if (2 * n + 1 < n_in) b = fl[2 * n + 1];
+            }
+            v[j] = make_float2(a, b);
+        }
+        __syncthreads();
+        F::template run<-1>(v, buf, t, active, twt, 1);
+        if (active) {
+#pragma unroll
+            for (int r = 0; r < F::P1; r++) buf[F::out_index(t, r)] = v[r];
+        }
+        __syncthreads();
+        if (active) {
+            const int z = row / n1, y = row % n1;
+            float2* dst = A.fwd + blockIdx.y * A.spec_bstride + ((long long)(c * n0 + z) * L1 + y) * hp;
+            for (int k = t; k <= M / 2; k += F::P2) {
+                const float2 zk = buf[k & (M - 1)];
+                const float2 zm = buf[(M - k) & (M - 1)];
+                const float2 e = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
+                const float2 od = make_float2(0.5f * (zk.y + zm.y), -0.5f * (zk.x - zm.x));
+                const float2 w = TwSrc<-1, float2>::get(tw, k, 2 * M);
+                dst[k] = cadd(e, cmul(w, od));
+                if (k != M - k) dst[M - k] = cadd(cconj(e), cmul(make_float2(-w.x, w.y), cconj(od)));
+            }
+        }
+    }
 }
 
 // Single plans: launch bounds alone, so ptxas sizes the registers for the 384-thread tile
 // (78-80 registers); batched plans: two blocks per SM requested explicitly (their
 // staged-scalar variant would otherwise take 136-150 registers and one block).
-template <int M, bool TERMS, bool HALF>
-__global__ void __launch_bounds__(384) xinv4_epi_kernel(const float2* __restrict__ S, int hp, int L1,
+template <int M, bool TERMS, bool HALF, bool FWD>
+__global__ void __launch_bounds__(384) xinv4_epi_kernel(typename SpecIn<FWD>::type S, int hp, int L1,
                                                         const float2* __restrict__ tw, EpiArgs A) {
-    xinv4_epi_body<M, TERMS, false, HALF>(S, hp, L1, tw, A);
+    xinv4_epi_body<M, TERMS, false, HALF, FWD>(S, hp, L1, tw, A);
 }
 
-template <int M, bool TERMS, bool HALF>
-__global__ void __launch_bounds__(384, M <= 512 ? 2 : 1) xinv4_epi_batch_kernel(const float2* __restrict__ S, int hp,
-                                                                                int L1, const float2* __restrict__ tw,
+template <int M, bool TERMS, bool HALF, bool FWD>
+__global__ void __launch_bounds__(384, M <= 512 ? 2 : 1) xinv4_epi_batch_kernel(typename SpecIn<FWD>::type S,
+                                                                                int hp, int L1,
+                                                                                const float2* __restrict__ tw,
                                                                                 EpiArgs A) {
-    xinv4_epi_body<M, TERMS, true, HALF>(S, hp, L1, tw, A);
+    xinv4_epi_body<M, TERMS, true, HALF, FWD>(S, hp, L1, tw, A);
 }
 
 static bool staged_scalars(const EpiArgs& A, int nsim);
@@ -972,12 +1038,12 @@ static int xinv4_rows(int tile) {
     return tile < 0 ? xinv4_rows_c<M, true>() : xinv4_rows_c<M, false>();
 }
 
-template <int M, bool TERMS, bool BATCH, bool HALF>
+template <int M, bool TERMS, bool BATCH, bool HALF, bool FWD>
 static cudaError_t launch_xinv4_h(const float2* S, int hp, int L1, const float2* tw, const EpiArgs& A,
                                   cudaStream_t st, int* nblocks, int nsim) {
     constexpr int RPB = xinv4_rows_c<M, HALF>();
     const size_t smem = (size_t)(RPB * 3 * FS<M>::LBUF + FS<M>::TWT) * sizeof(float2);
-    auto kern = BATCH ? xinv4_epi_batch_kernel<M, TERMS, HALF> : xinv4_epi_kernel<M, TERMS, HALF>;
+    auto kern = BATCH ? xinv4_epi_batch_kernel<M, TERMS, HALF, FWD> : xinv4_epi_kernel<M, TERMS, HALF, FWD>;
     if (smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
@@ -998,15 +1064,32 @@ static cudaError_t launch_xinv4_h(const float2* S, int hp, int L1, const float2*
     return launch_pdl(kern, dim3((unsigned)blocks, (unsigned)nsim), dim3(threads), smem, st, S, hp, L1, tw, A);
 }
 
+template <int M, bool TERMS, bool BATCH, bool FWD>
+static cudaError_t launch_xinv4_f(const float2* S, int hp, int L1, const float2* tw, const EpiArgs& A,
+                                  cudaStream_t st, int* nblocks, int nsim, int tile) {
+    if (tile < 0 && xinv4_rows_c<M, true>() != xinv4_rows_c<M, false>())
+        return launch_xinv4_h<M, TERMS, BATCH, true, FWD>(S, hp, L1, tw, A, st, nblocks, nsim);
+    return launch_xinv4_h<M, TERMS, BATCH, false, FWD>(S, hp, L1, tw, A, st, nblocks, nsim);
+}
+
+// A.fwd selects the variant that also writes the R2C rows of the next stage state (no
+// per-term outputs there; the host never asks for both).
 template <int M, bool TERMS, bool BATCH>
 static cudaError_t launch_xinv4_t(const float2* S, int hp, int L1, const float2* tw, const EpiArgs& A,
                                   cudaStream_t st, int* nblocks, int nsim, int tile) {
-    if (tile < 0 && xinv4_rows_c<M, true>() != xinv4_rows_c<M, false>())
-        return launch_xinv4_h<M, TERMS, BATCH, true>(S, hp, L1, tw, A, st, nblocks, nsim);
-    return launch_xinv4_h<M, TERMS, BATCH, false>(S, hp, L1, tw, A, st, nblocks, nsim);
+    if constexpr (!TERMS) {
+        if (A.fwd) return launch_xinv4_f<M, false, BATCH, true>(S, hp, L1, tw, A, st, nblocks, nsim, tile);
+    } else {
+        if (A.fwd) return cudaErrorInvalidValue;
+    }
+    return launch_xinv4_f<M, TERMS, BATCH, false>(S, hp, L1, tw, A, st, nblocks, nsim, tile);
 }
 
 static bool use_xinv4(int M) { return M >= 4 && M <= 1024; }
+
+// The four-step epilogue (and the four-step row pass whose output it reproduces) serve
+// these row lengths.
+bool epi_r2c_supported(int M) { return use_xinv4(M); }
 
 int xinv_blocks(int M, int n0n1) {
     if (use_xinv4(M)) {
