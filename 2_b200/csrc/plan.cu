@@ -451,6 +451,10 @@ struct mm_plan_s {
     // the epilogue of a stage that forms the next stage state also writes its R2C rows
     // (MM_EPI_R2C=0 in the environment at plan creation turns this off)
     bool epi_r2c = true;
+    // programmatic dependent launch for this plan's passes and controller: batched plans
+    // only (their chains overlap the tails of many simulations' passes; on single plans
+    // the programmatic edges cost more than they hide: SP4 film 161 -> 183 us per step)
+    bool pdl = false;
     long long n3() const { return 3 * g.N; }
     long long spec_bstride() const { return 3LL * g.n[0] * g.L[1] * g.hp; }
 };
@@ -752,6 +756,7 @@ extern "C" MM_API int mm_plan_create_batch(const mm_problem* prob, int nsim, con
         const char* e = getenv("MM_EPI_R2C");
         p->epi_r2c = !(e && e[0] == '0');
     }
+    p->pdl = nsim > 1;
     if ((rc = autotune(p))) {
         mm_plan_destroy(p);
         return rc;
@@ -863,6 +868,7 @@ static bool zreg_ok(const ConvGeom& g) {
 // of the evaluation that formed m_in), so the row pass is left out.
 static int launch_conv(mm_plan p, PP m_in, const DevCtl* ctl, int skip_retry, cudaStream_t st,
                        const std::vector<cudaEvent_t>* ev = nullptr, bool rows_ready = false) {
+    PdlScope pdl_scope(p->pdl);
     const ConvGeom& g = p->g;
     const int n0 = g.n[0], n1 = g.n[1], n2 = g.n[2];
     const int L0 = g.L[0], L1 = g.L[1];
@@ -923,6 +929,7 @@ enum { EVAL_EMIT_ROWS = 1, EVAL_ROWS_READY = 2 };
 static int launch_eval(mm_plan p, const StageOp& op, DevCtl* ctl, int skip_retry, float* const* dbg,
                        long long noise_step, double dt_thermal, float* red, unsigned int* tq_out, cudaStream_t st,
                        int* nblocks_out, int fwd = 0) {
+    PdlScope pdl_scope(p->pdl);
     const ConvGeom& g = p->g;
     EpiArgs A;
     memset(&A, 0, sizeof A);
@@ -1314,6 +1321,7 @@ static int launch_combine(mm_plan p, PP base, PP next, int nk, const PP* kp, con
 // summary the host polls.
 static cudaError_t launch_controller(mm_plan p, cudaStream_t st, int mode, int adaptive, int q, int fsal, int nevals,
                                      int first_skippable) {
+    PdlScope pdl_scope(p->pdl);
     const int threads = p->nsim >= 256 ? 256 : ((p->nsim + 31) / 32) * 32;
     return launch_pdl(controller_kernel, dim3(1), dim3(threads), 0, st, p->ctl, p->nsim, p->dsum, mode, adaptive, q,
                       fsal, nevals, first_skippable);
@@ -2004,6 +2012,7 @@ extern "C" MM_API long long mm_plan_launch_count(mm_plan p) { return p ? p->laun
 // no demag: epilogue only.  Batched plans time all simulations together.
 extern "C" MM_API int mm_profile_eval(mm_plan p, int reps, double* ms_out, int* npass, mm_stream stream) {
     if (!p || !ms_out || !npass || reps < 1) return set_err(MM_ERR_ARG, "bad argument");
+    PdlScope pdl_scope(p->pdl);
     cudaStream_t st = (cudaStream_t)stream;
     int rc = read_ctl(p, st);
     if (rc) return rc;
