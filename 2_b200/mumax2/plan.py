@@ -86,11 +86,20 @@ class Plan:
         except Exception:
             pass
 
-    def _dev(self, a):
+    def _dev(self, a, count=None):
+        """a as a contiguous float32 device tensor of `count` states (default: all of the
+        plan's simulations), 3N floats each; any other size is refused here, since the
+        library reads exactly that many floats."""
         torch = self.torch
         if isinstance(a, torch.Tensor):
-            return a.to(self.device, torch.float32).contiguous()
-        return torch.as_tensor(np.ascontiguousarray(a, dtype=np.float32).ravel(), device=self.device)
+            t = a.to(self.device, torch.float32).contiguous()
+        else:
+            t = torch.as_tensor(np.ascontiguousarray(a, dtype=np.float32).ravel(), device=self.device)
+        want = 3 * self.N * (self.nsim if count is None else count)
+        if t.numel() != want:
+            raise ValueError("state array of %d floats, expected %d (%s x 3N, N = %d)"
+                             % (t.numel(), want, self.nsim if count is None else count, self.N))
+        return t
 
     def tiles(self):
         """(tiles, eval_us): the autotuned tile shifts of the row, column and epilogue
@@ -265,13 +274,16 @@ class Plan:
 
     # ---- batched plans: one entry per simulation
     def set_sims(self, sims):
+        if len(sims) != self.nsim:
+            raise ValueError("set_sims needs %d entries, got %d" % (self.nsim, len(sims)))
         self._sims = nat.make_sims(self.problem, sims)
         nat.check(nat.lib().mm_batch_set_sims(self.h, C.cast(self._sims, C.c_void_p)))
 
     def batch_run_until_maxtorque(self, thr, max_steps=0):
         """Each simulation b steps until its maxtorque < thr[b]."""
-        self._thr = np.ascontiguousarray(thr, dtype=np.float64)
-        assert self._thr.shape == (self.nsim,)
+        self._thr = np.ascontiguousarray(thr, dtype=np.float64).ravel()
+        if self._thr.shape != (self.nsim,):
+            raise ValueError("one threshold per simulation needed (%d), got %d" % (self.nsim, self._thr.size))
         nat.check(nat.lib().mm_batch_run_until_maxtorque(self.h, self._thr.ctypes.data_as(C.c_void_p),
                                                          int(max_steps), None))
 
@@ -280,14 +292,19 @@ class Plan:
         array, or a float32 tensor on this plan's device),
         torque thresholds thr [k], optional scalar dicts sims [k].  Per-simulation masks
         are updated by writing into this plan's mask tensors before the call."""
-        idx = np.ascontiguousarray(idx, dtype=np.int32)
+        idx = np.ascontiguousarray(idx, dtype=np.int32).ravel()
+        k = len(idx)
         if hasattr(m, "data_ptr"):   # device tensor [k][3N] float32
-            m = m.reshape(len(idx), -1).contiguous()
+            m = self._dev(m, k)
             mp, from_host = C.c_void_p(m.data_ptr()), 0
         else:
-            m = np.ascontiguousarray(m, dtype=np.float32).reshape(len(idx), -1)
+            m = np.ascontiguousarray(m, dtype=np.float32).ravel()
+            if m.size != 3 * self.N * k:
+                raise ValueError("batch_restart: %d floats for %d states of 3N = %d" % (m.size, k, 3 * self.N))
             mp, from_host = m.ctypes.data_as(C.c_void_p), 1
-        thr = np.ascontiguousarray(thr, dtype=np.float64)
+        thr = np.ascontiguousarray(thr, dtype=np.float64).ravel()
+        if thr.size != k or (sims is not None and len(sims) != k):
+            raise ValueError("batch_restart: one threshold (and one sims entry) per slot")
         sa = nat.make_sims(self.problem, sims) if sims is not None else None
         nat.check(nat.lib().mm_batch_restart(self.h, len(idx), idx.ctypes.data_as(C.c_void_p), mp, from_host,
                                              C.cast(sa, C.c_void_p) if sa is not None else None,

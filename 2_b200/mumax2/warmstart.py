@@ -32,10 +32,11 @@ def _tail_plan(plan, problem, masks0, sims0, slots, device, maxerr):
 
 def relax_pool(problem, sims, masks, states, thr, slots=256, maxerr=1e-6, max_steps=100000, device=0,
                keep_states=False, plan=None, accept=None, fallback=None, fallback_max_steps=100000,
-               tail_slots=16):
+               tail_slots=16, want_energy=True):
     """Relaxes problem q from states[q] until maxtorque < thr[q].  states: a list of host
     arrays or a float32 device tensor [nq][3N].  Returns a dict of arrays: steps,
-    maxtorque, energy (J) and, with keep_states, the relaxed states.
+    maxtorque, energy (J; zeros without want_energy, which accept needs) and, with
+    keep_states, the relaxed states.
 
     accept(q, steps, maxtorque, energy) -> bool and fallback (one host state): a relax that
     accept rejects is queued again at once, in the same pool, from the fallback state with
@@ -145,13 +146,13 @@ def relax_pool(problem, sims, masks, states, thr, slots=256, maxerr=1e-6, max_st
         st = cur.batch_stats()
         free = [b for b in range(nslot) if slot[b] >= 0 and st[b]["done"]]
         if free:
-            en = cur.batch_energy()
+            en = cur.batch_energy() if (want_energy or accept is not None) else None
             state = cur.get_state() if keep_states else None
             for b in free:
                 q = slot[b]
                 res["steps"][q] = offset[b] + st[b]["step"]
                 res["maxtorque"][q] = st[b]["maxtorque"]
-                res["energy"][q] = en[b][4]
+                res["energy"][q] = en[b][4] if en is not None else 0.0
                 if keep_states:
                     res["state"][q] = state[3 * N * b:3 * N * (b + 1)]
                 slot[b] = -1
