@@ -173,6 +173,13 @@ class UNet:
     def _ptr(self, t):
         return C.c_void_p(t.data_ptr())
 
+    def _need(self, t, count, what):
+        """t must be a contiguous device tensor of `count` elements: the kernels read and
+        write exactly that many."""
+        if t.numel() != count or not t.is_contiguous() or t.device.type != "cuda":
+            raise ValueError("%s: contiguous device tensor of %d elements needed, got %d" % (what, count, t.numel()))
+        return t
+
     def _cs(self, view):
         return BUFFERS[view[0]][1]
 
@@ -210,14 +217,18 @@ class UNet:
     def set_features(self, masks_dev, prm_dev):
         """Builds the input features on the GPU from masks [B][H*W] and param_table rows
         (device float32 tensors)."""
-        nat.check(nat.lib().mm_nn_features(self._ptr(masks_dev), self._ptr(prm_dev), self.B, self.H * self.W,
+        P = self.H * self.W
+        self._need(masks_dev, self.B * P, "masks")
+        self._need(prm_dev, self.B * 8, "parameter table")
+        nat.check(nat.lib().mm_nn_features(self._ptr(masks_dev), self._ptr(prm_dev), self.B, P,
                                            self._ptr(self.buf["in"]), None))
 
     def set_input(self, feats):
         """feats: float32 [B][H*W][FEAT] (numpy or device tensor)."""
         torch = self.torch
-        f = torch.as_tensor(feats, device=self.device, dtype=torch.float32).reshape(-1)
+        f = torch.as_tensor(feats, device=self.device, dtype=torch.float32).reshape(-1).contiguous()
         P = self.B * self.H * self.W
+        self._need(f, P * FEAT, "features")
         nat.check(nat.lib().mm_nn_to_bf16(self._ptr(f), P, FEAT, self._ptr(self.buf["in"]), FEAT, 0, None))
 
     def forward(self):
@@ -248,6 +259,9 @@ class UNet:
         torch = self.torch
         self.target = torch.as_tensor(target, device=self.device, dtype=torch.float32).reshape(-1).contiguous()
         self.mask = torch.as_tensor(mask, device=self.device, dtype=torch.float32).reshape(-1).contiguous()
+        P = self.B * self.H * self.W
+        self._need(self.target, P * 3, "target")
+        self._need(self.mask, P, "mask")
         cnt = float(mask_count) if mask_count is not None else float(self.mask.sum().item())
         self.norm = max(1.0, cnt) * 3.0
 
@@ -317,8 +331,11 @@ class UNet:
     def states(self, masks_dev, dst):
         """Initial states of this batch from the output: dst (float32 device tensor
         [B][3][H*W], internal SoA) = masks_dev [B][H*W] * normalised output."""
-        nat.check(nat.lib().mm_nn_output_state(self._ptr(self.buf["out"]), OUTC, self._ptr(masks_dev), self.B,
-                                               self.H * self.W, self._ptr(dst), None))
+        P = self.H * self.W
+        self._need(masks_dev, self.B * P, "masks")
+        self._need(dst, self.B * 3 * P, "states")
+        nat.check(nat.lib().mm_nn_output_state(self._ptr(self.buf["out"]), OUTC, self._ptr(masks_dev), self.B, P,
+                                               self._ptr(dst), None))
 
     def output3(self):
         """[B][H*W][3] float32 numpy of the first three output channels."""
