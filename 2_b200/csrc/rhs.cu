@@ -696,18 +696,20 @@ __device__ __forceinline__ void xinv4_epi_body(typename SpecIn<FWD>::type S, int
         // staged by epilogue_rows) into the rows of the spectrum this block has read: the
         // packing, transform and post-processing of xfwd4_kernel, value for value, so the
         // spectrum is the one the separate row pass would write from the stored state.
+        // post-processing twiddles W_2M^-k, k <= M/2, after the step-1 table (the launcher
+        // sizes the shared memory of this variant for them): the values TwSrc reads
+        float2* pw = twt + F::TWT;
+        for (int k = threadIdx.x; k <= M / 2; k += blockDim.x) pw[k] = TwSrc<-1, float2>::get(tw, k, 2 * M);
         __syncthreads();
         const float* fl = reinterpret_cast<const float*>(buf);
         const int n_in = A.P.n[2];
 #pragma unroll
         for (int j = 0; j < F::P1; j++) {
             const int n = F::in_index(t, j);
-            float a = 0.f, b = 0.f;
-            if (active) {
-                if (2 * n < n_in) a = fl[2 * n];
-                if (2 * n + 1 < n_in) b = fl[2 * n + 1];
-            }
-            v[j] = make_float2(a, b);
+            float2 val = make_float2(0.f, 0.f);
+            if (active && 2 * n + 1 < n_in) val = buf[n];          // the packed pair (x[2n], x[2n+1])
+            else if (active && 2 * n < n_in) val.x = fl[2 * n];
+            v[j] = val;
         }
         __syncthreads();
         F::template run<-1>(v, buf, t, active, twt, 1);
@@ -724,7 +726,7 @@ __device__ __forceinline__ void xinv4_epi_body(typename SpecIn<FWD>::type S, int
                 const float2 zm = buf[(M - k) & (M - 1)];
                 const float2 e = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
                 const float2 od = make_float2(0.5f * (zk.y + zm.y), -0.5f * (zk.x - zm.x));
-                const float2 w = TwSrc<-1, float2>::get(tw, k, 2 * M);
+                const float2 w = pw[k];
                 dst[k] = cadd(e, cmul(w, od));
                 if (k != M - k) dst[M - k] = cadd(cconj(e), cmul(make_float2(-w.x, w.y), cconj(od)));
             }
@@ -1042,7 +1044,7 @@ template <int M, bool TERMS, bool BATCH, bool HALF, bool FWD>
 static cudaError_t launch_xinv4_h(const float2* S, int hp, int L1, const float2* tw, const EpiArgs& A,
                                   cudaStream_t st, int* nblocks, int nsim) {
     constexpr int RPB = xinv4_rows_c<M, HALF>();
-    const size_t smem = (size_t)(RPB * 3 * FS<M>::LBUF + FS<M>::TWT) * sizeof(float2);
+    const size_t smem = (size_t)(RPB * 3 * FS<M>::LBUF + FS<M>::TWT + (FWD ? M / 2 + 1 : 0)) * sizeof(float2);
     auto kern = BATCH ? xinv4_epi_batch_kernel<M, TERMS, HALF, FWD> : xinv4_epi_kernel<M, TERMS, HALF, FWD>;
     if (smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
