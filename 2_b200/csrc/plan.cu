@@ -451,9 +451,10 @@ struct mm_plan_s {
     // the epilogue of a stage that forms the next stage state also writes its R2C rows
     // (MM_EPI_R2C=0 in the environment at plan creation turns this off)
     bool epi_r2c = true;
-    // programmatic dependent launch for this plan's passes and controller: batched plans
-    // only (their chains overlap the tails of many simulations' passes; on single plans
-    // the programmatic edges cost more than they hide: SP4 film 161 -> 183 us per step)
+    // programmatic dependent launch for this plan's passes and controller, on plans of at
+    // least 2^18 cells in all (RK23 step of 256 films of 64x64: 471 -> 454 us); on smaller
+    // ones the programmatic edges cost more than they hide (SP4 film 161 -> 183 us,
+    // 16 films of 64x64 93 -> 103 us per step)
     bool pdl = false;
     long long n3() const { return 3 * g.N; }
     long long spec_bstride() const { return 3LL * g.n[0] * g.L[1] * g.hp; }
@@ -756,7 +757,7 @@ extern "C" MM_API int mm_plan_create_batch(const mm_problem* prob, int nsim, con
         const char* e = getenv("MM_EPI_R2C");
         p->epi_r2c = !(e && e[0] == '0');
     }
-    p->pdl = nsim > 1;
+    p->pdl = (long long)nsim * p->g.N >= (1LL << 18);
     if ((rc = autotune(p))) {
         mm_plan_destroy(p);
         return rc;
