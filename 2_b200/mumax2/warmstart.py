@@ -13,6 +13,7 @@ import time
 
 import numpy as np
 
+from . import _native as nat
 from . import unet as U
 from . import workloads as W
 
@@ -32,17 +33,23 @@ def _tail_plan(plan, problem, masks0, sims0, slots, device, maxerr):
 
 def relax_pool(problem, sims, masks, states, thr, slots=256, maxerr=1e-6, max_steps=100000, device=0,
                keep_states=False, plan=None, accept=None, fallback=None, fallback_max_steps=100000,
-               tail_slots=16, want_energy=True):
+               tail_slots=16, want_energy=True, spec_steps=0):
     """Relaxes problem q from states[q] until maxtorque < thr[q].  states: a list of host
     arrays or a float32 device tensor [nq][3N].  Returns a dict of arrays: steps,
     maxtorque, energy (J; zeros without want_energy, which accept needs) and, with
     keep_states, the relaxed states.
 
     accept(q, steps, maxtorque, energy) -> bool and fallback (one host state): a relax that
-    accept rejects is queued again at once, in the same pool, from the fallback state with
+    accept rejects is redone, in the same pool, from the fallback state with
     fallback_max_steps as its step limit; the result arrays then hold the fallback's
     result, "first_*" arrays the first attempt's and "fell_back" marks the problems
-    concerned.
+    concerned.  Without spec_steps the redo is queued when the first attempt is rejected.
+    With spec_steps > 0 the redo of a problem starts speculatively, in a free slot beside
+    the first attempt, once that attempt has run spec_steps steps: the long first attempts
+    are the ones the step limit rejects, and their redo then no longer waits for them.  An
+    accepted first attempt cancels its redo; a rejected one takes the redo's result,
+    whenever it ends.  Each run is the same computation either way, so the results do not
+    depend on spec_steps ("spec_started" / "spec_cancelled" count the speculative runs).
 
     Drain phase: once nothing is queued and at most tail_slots relaxations are left, they
     move (state, scalars, mask and steps so far) to a plan of tail_slots simulations,
@@ -62,6 +69,7 @@ def relax_pool(problem, sims, masks, states, thr, slots=256, maxerr=1e-6, max_st
                     device=device)
     plan.solver("rk23", dt=1e-14, maxerr=maxerr)
     on_dev = hasattr(states, "data_ptr")
+    speculate = bool(spec_steps) and accept is not None and fallback is not None
     queue = collections.deque((q, False) for q in range(nq))
     res = {"steps": np.zeros(nq, dtype=np.int64), "maxtorque": np.zeros(nq), "energy": np.zeros(nq)}
     if accept is not None:
@@ -70,23 +78,29 @@ def relax_pool(problem, sims, masks, states, thr, slots=256, maxerr=1e-6, max_st
     if keep_states:
         res["state"] = np.zeros((nq, 3 * N), dtype=np.float32)
     thr = np.asarray(thr)
-    # per slot of the current plan: problem, fallback flag, steps done before this plan
+    # per slot of the current plan: problem, redo flag, steps done before this plan
     cur = plan
     nslot = B
     slot, retry, offset = [-1] * nslot, [False] * nslot, [0] * nslot
+    spec_slot = {}      # problem -> slot of its speculative redo while the first attempt runs
+    spec_result = {}    # problem -> result of a speculative redo that ended first
+    awaiting = set()    # problems whose first attempt was rejected while their redo runs
+    n_spec, n_cancel = 0, 0
 
     def restart(idx, m0, jobs, limits):
         cur.batch_restart(idx, m0, thr[jobs], sims=[sims[q] for q in jobs], max_steps=limits)
 
+    def place(b, q, is_fb):
+        cur.mask_tensor("msat")[b * N:(b + 1) * N].copy_(torch.from_numpy(np.asarray(masks[q], dtype=np.float32)))
+        slot[b], retry[b], offset[b] = q, is_fb, 0
+
     def fill(free):
-        mt = cur.mask_tensor("msat")
         idx, jobs, fb = [], [], []
         for b in free:
             if not queue:
                 break
             q, is_fb = queue.popleft()
-            mt[b * N:(b + 1) * N].copy_(torch.from_numpy(np.asarray(masks[q], dtype=np.float32)))
-            slot[b], retry[b], offset[b] = q, is_fb, 0
+            place(b, q, is_fb)
             idx.append(b)
             jobs.append(q)
             fb.append(is_fb)
@@ -119,6 +133,8 @@ def relax_pool(problem, sims, masks, states, thr, slots=256, maxerr=1e-6, max_st
             mt[i * N:(i + 1) * N].copy_(torch.from_numpy(np.asarray(masks[q], dtype=np.float32)))
             new_slot[i], new_retry[i] = q, retry[b]
             new_off[i] = offset[b] + st[b]["step"]
+            if retry[b] and spec_slot.get(q) == b:
+                spec_slot[q] = i
             m0.append(state[3 * N * b:3 * N * (b + 1)])
             js.append(q)
             limits.append(max(1, (fallback_max_steps if retry[b] else max_steps) - new_off[i]))
@@ -130,6 +146,12 @@ def relax_pool(problem, sims, masks, states, thr, slots=256, maxerr=1e-6, max_st
             sel = [i for i in range(len(run)) if limits[i] == lim]
             restart(sel, np.stack([m0[i] for i in sel]), [js[i] for i in sel], lim)
 
+    def record(q, r, first=False):
+        pre = "first_" if first else ""
+        res[pre + "steps"][q], res[pre + "maxtorque"][q], res[pre + "energy"][q] = r[0], r[1], r[2]
+        if not first and keep_states:
+            res["state"][q] = r[3]
+
     fill(range(B))
     done = 0
     refill = max(1, B // 8)
@@ -137,40 +159,97 @@ def relax_pool(problem, sims, masks, states, thr, slots=256, maxerr=1e-6, max_st
     t_all = time.perf_counter()
     while done < nq:
         t1 = time.perf_counter()
+        # with speculation the host looks at the running attempts' steps every 64 attempts
+        # (a drive that stops at that cap reports MM_ERR_TIMEOUT)
+        cap = 64 if speculate else 0
         if cur is plan:
             drain = tail_slots if nslot > tail_slots else 0
-            cur.batch_drive(target_active=max(0, nslot - refill) if queue else drain, max_attempts=0)
+            target = max(0, nslot - refill) if queue else drain
         else:
-            cur.batch_drive(target_active=max(0, nslot - 1) if queue else 0, max_attempts=0)
+            target = max(0, nslot - 1) if queue else 0
+        try:
+            cur.batch_drive(target_active=target, max_attempts=cap)
+        except nat.MMError as e:
+            if not (cap and e.code == nat.MM_ERR_TIMEOUT):
+                raise
         t_drive += time.perf_counter() - t1
         st = cur.batch_stats()
-        free = [b for b in range(nslot) if slot[b] >= 0 and st[b]["done"]]
-        if free:
+        ended = [b for b in range(nslot) if slot[b] >= 0 and st[b]["done"]]
+        ended.sort(key=lambda b: retry[b])          # first attempts before redos
+        free = []
+        if ended:
             en = cur.batch_energy() if (want_energy or accept is not None) else None
             state = cur.get_state() if keep_states else None
-            for b in free:
+            for b in ended:
+                if slot[b] < 0:                     # a redo cancelled by its first attempt above
+                    continue
                 q = slot[b]
-                res["steps"][q] = offset[b] + st[b]["step"]
-                res["maxtorque"][q] = st[b]["maxtorque"]
-                res["energy"][q] = en[b][4] if en is not None else 0.0
-                if keep_states:
-                    res["state"][q] = state[3 * N * b:3 * N * (b + 1)]
+                r = (offset[b] + st[b]["step"], st[b]["maxtorque"], en[b][4] if en is not None else 0.0,
+                     state[3 * N * b:3 * N * (b + 1)] if keep_states else None)
                 slot[b] = -1
-                if accept is not None and not retry[b]:
-                    res["first_steps"][q] = res["steps"][q]
-                    res["first_maxtorque"][q] = res["maxtorque"][q]
-                    res["first_energy"][q] = res["energy"][q]
-                    if not accept(q, res["steps"][q], res["maxtorque"][q], res["energy"][q]):
-                        res["fell_back"][q] = True
-                        queue.appendleft((q, True))
+                free.append(b)
+                if not retry[b]:
+                    record(q, r)
+                    if accept is None:
+                        done += 1
                         continue
-                done += 1
-            fill(free)
+                    record(q, r, first=True)
+                    if accept(q, r[0], r[1], r[2]):
+                        done += 1
+                        s = spec_slot.pop(q, None)
+                        if s is not None:           # its redo is not needed
+                            cur.batch_cancel([s])
+                            slot[s] = -1
+                            free.append(s)
+                            n_cancel += 1
+                        spec_result.pop(q, None)
+                        continue
+                    res["fell_back"][q] = True
+                    if q in spec_result:
+                        record(q, spec_result.pop(q))
+                        done += 1
+                    elif q in spec_slot:
+                        awaiting.add(q)
+                    else:
+                        queue.appendleft((q, True))
+                else:
+                    if q in awaiting:
+                        awaiting.discard(q)
+                        spec_slot.pop(q, None)
+                        record(q, r)
+                        done += 1
+                    elif spec_slot.get(q) == b:     # the redo ended before the first attempt
+                        spec_slot.pop(q)
+                        spec_result[q] = r
+                    else:
+                        record(q, r)
+                        done += 1
+        if speculate:
+            idle = sorted(set(free) | {b for b in range(nslot) if slot[b] < 0 and st[b]["done"]})
+            long_first = sorted((b for b in range(nslot) if slot[b] >= 0 and not retry[b]
+                                 and slot[b] not in spec_slot and slot[b] not in spec_result
+                                 and offset[b] + st[b]["step"] >= spec_steps), key=lambda b: -st[b]["step"])
+            started = []
+            for b in long_first:
+                if not idle:
+                    break
+                f = idle.pop(0)
+                q = slot[b]
+                place(f, q, True)
+                spec_slot[q] = f
+                started.append((f, q))
+            if started:
+                restart([f for f, _ in started], np.stack([fallback] * len(started)), [q for _, q in started],
+                        fallback_max_steps)
+                n_spec += len(started)
+                free = [b for b in free if slot[b] < 0]
+        fill(free)
         running = sum(1 for b in range(nslot) if slot[b] >= 0)
         if cur is plan and nslot > tail_slots and not queue and 0 < running <= tail_slots:
             migrate(cur.batch_stats())
     res["drive_s"] = t_drive
     res["host_s"] = time.perf_counter() - t_all - t_drive
+    res["spec_started"], res["spec_cancelled"] = n_spec, n_cancel
     if own:
         t = getattr(plan, "_tail_plan", None)
         if t is not None:
@@ -275,12 +354,14 @@ def predict(net, sims, masks, n, host=False):
     return out.cpu().numpy() if host else out
 
 
-def evaluate(net, problem, sims, masks, slots=256, device=0, energy_tol=1e-4, max_steps=20000):
+def evaluate(net, problem, sims, masks, slots=256, device=0, energy_tol=1e-4, max_steps=20000, spec_frac=0.25):
     """Cold and warm relaxations of the same problems (times include the network's
     inference for the warm start).  A warm relax that does not reach the threshold within
     max_steps (its step budget; step_budget() derives one from the training relaxations),
     or ends above the cold relax's energy by more than energy_tol (relative), counts as
-    failed and is redone from the cold start in the same pool (time included)."""
+    failed and is redone from the cold start in the same pool (time included).  The redo
+    of a warm relax that has run spec_frac * max_steps steps starts beside it (relax_pool's
+    spec_steps; 0 queues redos only once their warm relax is rejected)."""
     import torch
     from .plan import Plan
     n = problem["n"]
@@ -307,7 +388,7 @@ def evaluate(net, problem, sims, masks, slots=256, device=0, energy_tol=1e-4, ma
     torch.cuda.synchronize()
     t_inf = time.perf_counter() - t0
     rw = relax_pool(problem, sims, masks, init, thr, slots=slots, device=device, max_steps=max_steps, plan=plan,
-                    accept=accept, fallback=cold)
+                    accept=accept, fallback=cold, spec_steps=int(spec_frac * max_steps))
     torch.cuda.synchronize()
     t_warm = time.perf_counter() - t0
     t = getattr(plan, "_tail_plan", None)
@@ -329,6 +410,7 @@ def evaluate(net, problem, sims, masks, slots=256, device=0, energy_tol=1e-4, ma
         "cold_steps_max": int(rc["steps"].max()), "warm_steps_max": int(rw["first_steps"].max()),
         "warm_step_budget": int(max_steps),
         "warm_ok_frac": float(1 - fb.mean()), "fallbacks": int(fb.sum()),
+        "spec_redos_started": int(rw["spec_started"]), "spec_redos_cancelled": int(rw["spec_cancelled"]),
         "final_converged_frac": float((rw["maxtorque"] < thr).mean()),
         "energy_within_tol_frac": float((erel <= energy_tol).mean()),
         "energy_rel_median": float(np.median(erel)),

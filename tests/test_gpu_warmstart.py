@@ -40,3 +40,35 @@ def test_pool_drain_on_small_plan_matches():
     erel = np.abs(a["energy"] - b["energy"]) / np.abs(b["energy"])
     assert erel.max() < 1e-4
     assert (a["steps"] <= b["steps"] + 40).all()
+
+
+def test_speculative_redo_gives_the_same_results():
+    """Redos started speculatively beside long first attempts (here from the first step
+    on, so that most are started and cancelled) give the results of the queued redos: every
+    run is the same computation in whichever slot it lands, so without the drain phase the
+    arrays agree exactly; with it, within the drain test's bounds."""
+    import numpy as np
+    from mumax2 import warmstart as WS
+    from mumax2 import workloads as W
+    problem, sims, masks = W.relax_set(96, seed=21)
+    thr = WS.thresholds(sims)
+    n = problem["n"]
+    cold = W.cold_state(n, 1)
+    fallback = W.uniform_state(n, (0.0, 1.0, 0.0), 1)
+
+    def accept(q, steps, mt, e):
+        return q % 5 != 0
+
+    runs = {}
+    for spec, tail in ((0, 64), (1, 64), (0, 16), (1, 16)):
+        runs[spec, tail] = WS.relax_pool(problem, sims, masks, [cold] * 96, thr, slots=64, tail_slots=tail,
+                                         accept=accept, fallback=fallback, spec_steps=spec)
+    a, b = runs[0, 64], runs[1, 64]
+    assert b["spec_started"] > 0 and b["spec_cancelled"] > 0 and a["spec_started"] == 0
+    for k in ("steps", "maxtorque", "energy", "first_steps", "first_maxtorque", "first_energy", "fell_back"):
+        assert np.array_equal(a[k], b[k]), k
+    assert a["fell_back"].sum() == len(range(0, 96, 5))
+    c, d = runs[0, 16], runs[1, 16]
+    assert (d["maxtorque"] < thr).all() and np.array_equal(c["fell_back"], d["fell_back"])
+    erel = np.abs(d["energy"] - a["energy"]) / np.abs(a["energy"])
+    assert erel.max() < 1e-4
