@@ -354,14 +354,17 @@ def predict(net, sims, masks, n, host=False):
     return out.cpu().numpy() if host else out
 
 
-def evaluate(net, problem, sims, masks, slots=256, device=0, energy_tol=1e-4, max_steps=20000, spec_frac=0.25):
+def evaluate(net, problem, sims, masks, slots=256, device=0, energy_tol=1e-4, max_steps=20000, spec_frac=0.5):
     """Cold and warm relaxations of the same problems (times include the network's
     inference for the warm start).  A warm relax that does not reach the threshold within
     max_steps (its step budget; step_budget() derives one from the training relaxations),
     or ends above the cold relax's energy by more than energy_tol (relative), counts as
     failed and is redone from the cold start in the same pool (time included).  The redo
     of a warm relax that has run spec_frac * max_steps steps starts beside it (relax_pool's
-    spec_steps; 0 queues redos only once their warm relax is rejected)."""
+    spec_steps; 0 queues redos only once their warm relax is rejected).  Measured on 4096
+    held-out problems: 0.05, 0.1, 0.25 and 0.5 of the budget gave 0.96, 1.09, 1.16 and
+    1.18 times the cold rate (early redos take slots from the queue and are mostly
+    cancelled)."""
     import torch
     from .plan import Plan
     n = problem["n"]
