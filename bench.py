@@ -622,7 +622,10 @@ def warmstart_bench(args, rank, world, local_rank, dist):
     steps_per_epoch = len(data) // 256
     flops = 3 * U.conv_flops(64, 64) * 256 * steps_per_epoch * args.epochs
     _, hs, hm = W.relax_set(args.nsim, seed=5000 + rank)
+    sampler = ClockSampler(local_rank)
+    sampler.start()
     ev = WS.evaluate(net, problem, hs, hm, device=local_rank, max_steps=WS.step_budget(res["steps"]))
+    clocks = sampler.stop()
     peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     peak = float(json.load(open(peaks_path))["bf16_tflops_sustained"]) if os.path.exists(peaks_path) else 1400.0
     if rank == 0:
@@ -638,7 +641,8 @@ def warmstart_bench(args, rank, world, local_rank, dist):
                 "training": {"generate_s": t_gen, "train_s": t_train, "loss_first_epoch": losses[0],
                              "loss_last_epoch": losses[-1],
                              "tflops_achieved": flops / t_train / 1e12, "tflops_peak_sustained": peak,
-                             "frac": flops / t_train / 1e12 / peak}}
+                             "frac": flops / t_train / 1e12 / peak},
+                "clocks": clocks}
         print(json.dumps(line), flush=True)
 
 
