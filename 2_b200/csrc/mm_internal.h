@@ -185,6 +185,21 @@ struct KernelView {
     int nz[6];
 };
 
+// A Runge-Kutta stage state next = normalise(base + h * sum_j ak[j] * kp[j]) per cell, with
+// the Msat mask as norm map (combine_kernel in plan.cu; combine_rows_kernel in rhs.cu also
+// writes the state's R2C rows).
+struct CombineArgs {
+    PP base, next;
+    int nk;
+    PP kp[MM_MAXK];
+    double ak[MM_MAXK];
+    const float* msat_mask;
+    long long N;
+    long long bstride, mask_bstride;
+    DevCtl* ctl;
+    int no_norm;  // leave the result unnormalised (the AM12 Euler start)
+};
+
 // Arguments of the fused epilogue (rhs.cu).
 struct EpiArgs {
     FieldParams P;
@@ -253,6 +268,10 @@ int xinv_blocks(int M, int n0n1);
 // whether the C2R + epilogue pass for row length M can also write the R2C rows of the
 // next stage state (EpiArgs::fwd)
 bool epi_r2c_supported(int M);
+// combine_rows_kernel: the stage state of A (normalised, A.no_norm = 0) and its R2C rows
+// into the spectrum S (times the Msat mask when fwd_mask), for M with epi_r2c_supported(M)
+cudaError_t launch_combine_rows(int M, const CombineArgs& A, const int n[3], float2* S, int hp, int L1,
+                                long long spec_bstride, const float2* tw, int fwd_mask, int nsim, cudaStream_t st);
 int report_error(int code, const char* msg);  // sets mm_last_error()
 int local_blocks(long long N, int nsim = 1);
 

@@ -81,18 +81,6 @@ __global__ void normalize_kernel(float* m, const float* msat_mask, long long N, 
 }
 
 // next = normalise(base + h * sum_j a_j K_j); h from the simulation's control block.
-struct CombineArgs {
-    PP base, next;
-    int nk;
-    PP kp[MM_MAXK];
-    double ak[MM_MAXK];
-    const float* msat_mask;
-    long long N;
-    long long bstride, mask_bstride;
-    DevCtl* ctl;
-    int no_norm;  // leave the result unnormalised (the AM12 Euler start)
-};
-
 __global__ void combine_kernel(CombineArgs A) {
     const DevCtl* ctl = A.ctl + blockIdx.y;
     if (ctl->done) return;
@@ -1293,8 +1281,7 @@ static const double DP_E[7] = {35. / 384 - 5179. / 57600, 0, 500. / 1113 - 7571.
                                125. / 192 - 393. / 640, -2187. / 6784 + 92097. / 339200,
                                11. / 84 - 187. / 2100, -1. / 40};
 
-static int launch_combine(mm_plan p, PP base, PP next, int nk, const PP* kp, const double* ak, cudaStream_t st,
-                          int no_norm = 0) {
+static CombineArgs combine_args(mm_plan p, PP base, PP next, int nk, const PP* kp, const double* ak, int no_norm) {
     CombineArgs A;
     memset(&A, 0, sizeof A);
     A.no_norm = no_norm;
@@ -1312,8 +1299,25 @@ static int launch_combine(mm_plan p, PP base, PP next, int nk, const PP* kp, con
     A.bstride = p->n3();
     A.mask_bstride = p->P.mask_bstride;
     A.ctl = p->ctl;
+    return A;
+}
+
+static int launch_combine(mm_plan p, PP base, PP next, int nk, const PP* kp, const double* ak, cudaStream_t st,
+                          int no_norm = 0) {
+    const CombineArgs A = combine_args(p, base, next, nk, kp, ak, no_norm);
     combine_kernel<<<dim3((unsigned)local_blocks(p->g.N, p->nsim), (unsigned)p->nsim), 256, 0, st>>>(A);
     CUCHK(cudaGetLastError());
+    p->launches++;
+    return MM_OK;
+}
+
+// The same stage state, also written as its R2C rows into the spectrum (where
+// epi_r2c_ok(p)), so that the evaluation at `next` starts at its column pass
+// (launch_eval with EVAL_ROWS_READY).
+static int enqueue_combine_rows(mm_plan p, PP base, PP next, int nk, const PP* kp, const double* ak, cudaStream_t st) {
+    const CombineArgs A = combine_args(p, base, next, nk, kp, ak, 0);
+    CUCHK(launch_combine_rows(p->g.M, A, p->g.n, p->S, p->g.hp, p->g.L[1], p->spec_bstride(), p->tw,
+                              p->khat_d ? 0 : 1, p->nsim, st));
     p->launches++;
     return MM_OK;
 }
@@ -1458,11 +1462,15 @@ static int enqueue_attempt(mm_plan p, cudaStream_t st) {
             CUCHK(launch_controller(p, st, 2, 0, 0, 0, 0, 0));
             p->launches++;
         }
+        // RK12: the corrector's input, the Euler predictor, comes with its R2C rows
+        const bool rows12 = (s == MM_RK12) && epi_r2c_ok(p);
         if (s == MM_RK12) {
             // Euler predictor from the saved k0 (solve_rk12.go:133), also on retries
             PP kp[1] = {fixed(p->Kst[0])};
             double ak[1] = {1.0};
-            if ((rc = launch_combine(p, cur_of(p->Y), fixed(p->Ma), 1, kp, ak, st))) return rc;
+            if ((rc = rows12 ? enqueue_combine_rows(p, cur_of(p->Y), fixed(p->Ma), 1, kp, ak, st)
+                             : launch_combine(p, cur_of(p->Y), fixed(p->Ma), 1, kp, ak, st)))
+                return rc;
         }
         if (s == MM_HEUN || s == MM_RK12) {
             // corrector: y = y_pred + h/2 k1 - h/2 k0 (solve_rk12.go:154, solve_heun.go:63)
@@ -1486,7 +1494,7 @@ static int enqueue_attempt(mm_plan p, cudaStream_t st) {
                 o1.ep[1] = fixed(p->Kst[0]);
                 o1.ek[1] = -1.0;
             }
-            const int fwd1 = (s == MM_HEUN) ? EVAL_ROWS_READY : 0;
+            const int fwd1 = (s == MM_HEUN || rows12) ? EVAL_ROWS_READY : 0;
             if ((rc = launch_eval(p, o1, ctl, 0, nullptr, 0, 0, nullptr, nullptr, st, nullptr, fwd1))) return rc;
         }
         CUCHK(launch_controller(p, st, 1, s == MM_RK12 ? 1 : 0, 1, 0, s == MM_EULER ? 1 : 2, s == MM_RK12));
@@ -1509,10 +1517,14 @@ static int enqueue_attempt(mm_plan p, cudaStream_t st) {
         if (i == S - 1) return oth_of(p->Y);
         return fixed((i & 1) ? p->Ma : p->Mb);
     };
+    // the first stage state, with its R2C rows where the plan allows
+    const bool rows1 = epi_r2c_ok(p);
     {
         PP kp[1] = {kbuf(0)};
         double ak[1] = {A(1, 0)};
-        if ((rc = launch_combine(p, cur_of(p->Y), mbuf(1), 1, kp, ak, st))) return rc;
+        if ((rc = rows1 ? enqueue_combine_rows(p, cur_of(p->Y), mbuf(1), 1, kp, ak, st)
+                        : launch_combine(p, cur_of(p->Y), mbuf(1), 1, kp, ak, st)))
+            return rc;
     }
     for (int i = 1; i < S; i++) {
         StageOp o = op_blank();
@@ -1545,7 +1557,7 @@ static int enqueue_attempt(mm_plan p, cudaStream_t st) {
         }
         // stage i + 1 reads mbuf(i + 1), which this epilogue forms: its rows come from here
         int fwd = (i + 1 < S) ? EVAL_EMIT_ROWS : 0;
-        if (i > 1) fwd |= EVAL_ROWS_READY;
+        if (i > 1 || rows1) fwd |= EVAL_ROWS_READY;
         if ((rc = launch_eval(p, o, ctl, 0, nullptr, 0, 0, nullptr, nullptr, st, nullptr, fwd))) return rc;
     }
     CUCHK(launch_controller(p, st, 1, 1, dp ? 4 : 2, 1, S - 1, 0));

@@ -634,6 +634,50 @@ __host__ __device__ constexpr int xinv4_rows_c() {
                                                                                           : xinv4_rpb<M>();
 }
 
+// R2C rows from the block's shared-memory lines: float x of the line of (row, c) holds the
+// input at cell x (n_in reals; the rest of the length-2M row is zero).  The packing,
+// four-step transform and real-to-complex post-processing of xfwd4_kernel, value for
+// value, so dst (the line's spectrum row, hp >= M+1 complex; ignored when !active) gets
+// what the separate row pass would write from the same values.  The post-processing
+// twiddles W_2M^-k, k <= M/2, go to shared memory after the step-1 table (the launchers
+// size the shared memory for them).  All threads of the block call this.
+template <int M>
+__device__ __forceinline__ void r2c_staged_lines(float2 (&v)[FS<M>::P1], float2* buf, float2* twt,
+                                                 const float2* __restrict__ tw, int t, bool active, int n_in,
+                                                 float2* dst) {
+    using F = FS<M>;
+    float2* pw = twt + F::TWT;
+    for (int k = threadIdx.x; k <= M / 2; k += blockDim.x) pw[k] = TwSrc<-1, float2>::get(tw, k, 2 * M);
+    __syncthreads();
+    const float* fl = reinterpret_cast<const float*>(buf);
+#pragma unroll
+    for (int j = 0; j < F::P1; j++) {
+        const int n = F::in_index(t, j);
+        float2 val = make_float2(0.f, 0.f);
+        if (active && 2 * n + 1 < n_in) val = buf[n];          // the packed pair (x[2n], x[2n+1])
+        else if (active && 2 * n < n_in) val.x = fl[2 * n];
+        v[j] = val;
+    }
+    __syncthreads();
+    F::template run<-1>(v, buf, t, active, twt, 1);
+    if (active) {
+#pragma unroll
+        for (int r = 0; r < F::P1; r++) buf[F::out_index(t, r)] = v[r];
+    }
+    __syncthreads();
+    if (active) {
+        for (int k = t; k <= M / 2; k += F::P2) {
+            const float2 zk = buf[k & (M - 1)];
+            const float2 zm = buf[(M - k) & (M - 1)];
+            const float2 e = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
+            const float2 od = make_float2(0.5f * (zk.y + zm.y), -0.5f * (zk.x - zm.x));
+            const float2 w = pw[k];
+            dst[k] = cadd(e, cmul(w, od));
+            if (k != M - k) dst[M - k] = cadd(cconj(e), cmul(make_float2(-w.x, w.y), cconj(od)));
+        }
+    }
+}
+
 // The spectrum argument of the C2R + epilogue pass: read-only, except in the FWD variant,
 // which writes the R2C rows of the next stage state back into the rows it has read.
 template <bool FWD> struct SpecIn { using type = const float2* __restrict__; };
@@ -693,44 +737,13 @@ __device__ __forceinline__ void xinv4_epi_body(typename SpecIn<FWD>::type S, int
                                             min(RPB, nrows - row0));
     if constexpr (FWD) {
         // R2C rows of the next stage state (float x of line (lr, c) = its value at cell x,
-        // staged by epilogue_rows) into the rows of the spectrum this block has read: the
-        // packing, transform and post-processing of xfwd4_kernel, value for value, so the
-        // spectrum is the one the separate row pass would write from the stored state.
-        // post-processing twiddles W_2M^-k, k <= M/2, after the step-1 table (the launcher
-        // sizes the shared memory of this variant for them): the values TwSrc reads
-        float2* pw = twt + F::TWT;
-        for (int k = threadIdx.x; k <= M / 2; k += blockDim.x) pw[k] = TwSrc<-1, float2>::get(tw, k, 2 * M);
-        __syncthreads();
-        const float* fl = reinterpret_cast<const float*>(buf);
-        const int n_in = A.P.n[2];
-#pragma unroll
-        for (int j = 0; j < F::P1; j++) {
-            const int n = F::in_index(t, j);
-            float2 val = make_float2(0.f, 0.f);
-            if (active && 2 * n + 1 < n_in) val = buf[n];          // the packed pair (x[2n], x[2n+1])
-            else if (active && 2 * n < n_in) val.x = fl[2 * n];
-            v[j] = val;
-        }
-        __syncthreads();
-        F::template run<-1>(v, buf, t, active, twt, 1);
-        if (active) {
-#pragma unroll
-            for (int r = 0; r < F::P1; r++) buf[F::out_index(t, r)] = v[r];
-        }
-        __syncthreads();
+        // staged by epilogue_rows) into the rows of the spectrum this block has read
+        float2* dst = nullptr;
         if (active) {
             const int z = row / n1, y = row % n1;
-            float2* dst = A.fwd + blockIdx.y * A.spec_bstride + ((long long)(c * n0 + z) * L1 + y) * hp;
-            for (int k = t; k <= M / 2; k += F::P2) {
-                const float2 zk = buf[k & (M - 1)];
-                const float2 zm = buf[(M - k) & (M - 1)];
-                const float2 e = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
-                const float2 od = make_float2(0.5f * (zk.y + zm.y), -0.5f * (zk.x - zm.x));
-                const float2 w = pw[k];
-                dst[k] = cadd(e, cmul(w, od));
-                if (k != M - k) dst[M - k] = cadd(cconj(e), cmul(make_float2(-w.x, w.y), cconj(od)));
-            }
+            dst = A.fwd + blockIdx.y * A.spec_bstride + ((long long)(c * n0 + z) * L1 + y) * hp;
         }
+        r2c_staged_lines<M>(v, buf, twt, tw, t, active, A.P.n[2], dst);
     }
 }
 
@@ -749,6 +762,112 @@ __global__ void __launch_bounds__(384, M <= 512 ? 2 : 1) xinv4_epi_batch_kernel(
                                                                                 const float2* __restrict__ tw,
                                                                                 EpiArgs A) {
     xinv4_epi_body<M, TERMS, true, HALF, FWD>(S, hp, L1, tw, A);
+}
+
+// ---------------------------------------------------------------- stage combine + R2C rows
+// The first stage state of an attempt, formed as combine_kernel forms it (same operations
+// in the same order), written to A.next and, times the Msat mask when fwd_mask, turned
+// into its R2C rows in the spectrum: the attempt's first evaluation then starts at its
+// column pass.  Blocks and threads as the four-step C2R + epilogue pass: RPB rows (z, y)
+// per block, P2 threads per (row, component) line.
+template <int M>
+__global__ void __launch_bounds__(384) combine_rows_kernel(CombineArgs A, int n0, int n1, int n2, float2* S, int hp,
+                                                           int L1, long long spec_bstride,
+                                                           const float2* __restrict__ tw, int fwd_mask) {
+    constexpr int RPB = xinv4_rows_c<M, false>();
+    using F = FS<M>;
+    const DevCtl* ctl = A.ctl + blockIdx.y;
+    if (ctl->done) return;
+    const int cur = ctl->cur;
+    const long long off = blockIdx.y * A.bstride;
+    const float* base = A.base.get(cur) + off;
+    float* next = A.next.get(cur) + off;
+    const float* msk = A.msat_mask ? A.msat_mask + blockIdx.y * A.mask_bstride : nullptr;
+    const float* kp[MM_MAXK];
+    float ak[MM_MAXK];
+#pragma unroll
+    for (int j = 0; j < MM_MAXK; j++) {
+        kp[j] = j < A.nk ? A.kp[j].get(cur) + off : nullptr;
+        ak[j] = j < A.nk ? (float)(A.ak[j] * ctl->h) : 0.f;
+    }
+    extern __shared__ unsigned char smem_raw[];
+    float2* sm = reinterpret_cast<float2*>(smem_raw);
+    float* slots = reinterpret_cast<float*>(sm);
+    float2* twt = sm + RPB * 3 * F::LBUF;
+    F::fill_twiddles(twt, tw);
+    const long long N = A.N;
+    const int nrows = n0 * n1;
+    const int row0 = blockIdx.x * RPB;
+    const int here = min(RPB, nrows - row0);
+    for (int e = threadIdx.x; e < here * n2; e += blockDim.x) {
+        const int lrow = e / n2, x = e - lrow * n2;
+        const long long i = (long long)(row0 + lrow) * n2 + x;
+        float xv = base[i], yv = base[N + i], zv = base[2 * N + i];
+#pragma unroll
+        for (int j = 0; j < MM_MAXK; j++) {
+            if (j >= A.nk) break;
+            xv += ak[j] * kp[j][i];
+            yv += ak[j] * kp[j][N + i];
+            zv += ak[j] * kp[j][2 * N + i];
+        }
+        const float norm = msk ? msk[i] : 1.0f;
+        const float mn = sqrtf(xv * xv + yv * yv + zv * zv);
+        float sc = (norm == 0.0f) ? 0.0f : 1.0f;
+        sc = (mn != 0.0f) ? sc / mn : 0.0f;
+        const float3 nx = make_float3(xv * sc, yv * sc, zv * sc);
+        next[i] = nx.x;
+        next[N + i] = nx.y;
+        next[2 * N + i] = nx.z;
+        const float fm = fwd_mask ? norm : 1.0f;
+        float* fl = slots + 2 * (long long)(lrow * 3) * F::LBUF + x;
+        fl[0] = nx.x * fm;
+        fl[2 * F::LBUF] = nx.y * fm;
+        fl[4 * F::LBUF] = nx.z * fm;
+    }
+    __syncthreads();
+    const int t = threadIdx.x % F::P2;
+    const int c = (threadIdx.x / F::P2) % 3;
+    const int lr = threadIdx.x / (3 * F::P2);
+    const int row = row0 + lr;
+    const bool active = (lr < RPB) && (row < nrows);
+    float2* buf = sm + (lr < RPB ? lr * 3 + c : 0) * F::LBUF;
+    float2* dst = nullptr;
+    if (active) {
+        const int z = row / n1, y = row % n1;
+        dst = S + blockIdx.y * spec_bstride + ((long long)(c * n0 + z) * L1 + y) * hp;
+    }
+    float2 v[F::P1];
+    r2c_staged_lines<M>(v, buf, twt, tw, t, active, n2, dst);
+}
+
+template <int M>
+static cudaError_t launch_combine_rows_t(const CombineArgs& A, const int n[3], float2* S, int hp, int L1,
+                                         long long spec_bstride, const float2* tw, int fwd_mask, int nsim,
+                                         cudaStream_t st) {
+    constexpr int RPB = xinv4_rows_c<M, false>();
+    const size_t smem = (size_t)(RPB * 3 * FS<M>::LBUF + FS<M>::TWT + M / 2 + 1) * sizeof(float2);
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(combine_rows_kernel<M>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    const int blocks = (n[0] * n[1] + RPB - 1) / RPB;
+    int threads = RPB * 3 * FS<M>::P2;
+    if (threads < 32) threads = 32;
+    combine_rows_kernel<M><<<dim3((unsigned)blocks, (unsigned)nsim), threads, smem, st>>>(
+        A, n[0], n[1], n[2], S, hp, L1, spec_bstride, tw, fwd_mask);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_combine_rows(int M, const CombineArgs& A, const int n[3], float2* S, int hp, int L1,
+                                long long spec_bstride, const float2* tw, int fwd_mask, int nsim, cudaStream_t st) {
+    if (A.no_norm || A.nk > MM_MAXK) return cudaErrorInvalidValue;
+    switch (M) {
+#define X(m) case m: return launch_combine_rows_t<m>(A, n, S, hp, L1, spec_bstride, tw, fwd_mask, nsim, st);
+        X(4) X(8) X(16) X(32) X(64) X(128) X(256) X(512) X(1024)
+#undef X
+        default: return cudaErrorInvalidValue;
+    }
 }
 
 static bool staged_scalars(const EpiArgs& A, int nsim);

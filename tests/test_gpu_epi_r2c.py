@@ -1,6 +1,7 @@
 """The epilogue that forms the next stage state also writes its R2C rows, so that the next
 evaluation of the attempt starts at its column pass (RK23 / RK45 stages, Heun's
-corrector).  It packs, transforms and post-processes the rows exactly as the separate row
+corrector), and the combine that forms an attempt's first stage state (RK23 / RK45; the
+Euler predictor of RK12) writes them too.  It packs, transforms and post-processes the rows exactly as the separate row
 pass does, so the stepped trajectory must be bit-identical to the one of a plan created
 with MM_EPI_R2C=0 (every evaluation with its own row pass), and each fused attempt must
 launch fewer kernels."""
@@ -43,7 +44,7 @@ def _compare(monkeypatch, *args, **kw):
     return a, b
 
 
-@pytest.mark.parametrize("solver", ["rk23", "rk45"])
+@pytest.mark.parametrize("solver", ["rk23", "rk45", "rk12"])
 def test_film3d_masked(monkeypatch, solver):
     """3-D film with a non-binary Msat mask, anisotropy and Zeeman; row pass, y, z and
     inverse passes; adaptive steps with rejections allowed."""
