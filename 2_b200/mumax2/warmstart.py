@@ -87,12 +87,23 @@ def relax_pool(problem, sims, masks, states, thr, slots=256, maxerr=1e-6, max_st
     awaiting = set()    # problems whose first attempt was rejected while their redo runs
     n_spec, n_cancel = 0, 0
 
+    dev = plan.mask_tensor("msat").device
+
+    def to_dev(a):
+        """One host-to-device copy of a stack of host arrays (states or masks)."""
+        return torch.from_numpy(np.ascontiguousarray(a, dtype=np.float32)).to(dev)
+
     def restart(idx, m0, jobs, limits):
+        if not hasattr(m0, "data_ptr"):
+            m0 = to_dev(m0)
         cur.batch_restart(idx, m0, thr[jobs], sims=[sims[q] for q in jobs], max_steps=limits)
 
-    def place(b, q, is_fb):
-        cur.mask_tensor("msat")[b * N:(b + 1) * N].copy_(torch.from_numpy(np.asarray(masks[q], dtype=np.float32)))
-        slot[b], retry[b], offset[b] = q, is_fb, 0
+    def place(bs, qs, is_fb):
+        """Slots bs take problems qs: their masks in one copy, and the slot records."""
+        mt = cur.mask_tensor("msat").view(-1, N)
+        mt[torch.tensor(bs, device=dev)] = to_dev(np.stack([np.asarray(masks[q], dtype=np.float32) for q in qs]))
+        for b, q, f in zip(bs, qs, is_fb):
+            slot[b], retry[b], offset[b] = q, f, 0
 
     def fill(free):
         idx, jobs, fb = [], [], []
@@ -100,12 +111,12 @@ def relax_pool(problem, sims, masks, states, thr, slots=256, maxerr=1e-6, max_st
             if not queue:
                 break
             q, is_fb = queue.popleft()
-            place(b, q, is_fb)
             idx.append(b)
             jobs.append(q)
             fb.append(is_fb)
         if not idx:
             return
+        place(idx, jobs, fb)
         for flag, limit in ((False, max_steps), (True, fallback_max_steps)):
             sel = [k for k in range(len(idx)) if fb[k] == flag]
             if not sel:
@@ -125,12 +136,13 @@ def relax_pool(problem, sims, masks, states, thr, slots=256, maxerr=1e-6, max_st
         run = [b for b in range(nslot) if slot[b] >= 0]
         state = cur.get_state()
         tail = _tail_plan(plan, problem, masks[0], sims[0], tail_slots, device, maxerr)
-        mt = tail.mask_tensor("msat")
+        mt = tail.mask_tensor("msat").view(-1, N)
+        if run:
+            mt[:len(run)] = to_dev(np.stack([np.asarray(masks[slot[b]], dtype=np.float32) for b in run]))
         new_slot, new_retry, new_off = [-1] * tail_slots, [False] * tail_slots, [0] * tail_slots
         m0, js, limits = [], [], []
         for i, b in enumerate(run):
             q = slot[b]
-            mt[i * N:(i + 1) * N].copy_(torch.from_numpy(np.asarray(masks[q], dtype=np.float32)))
             new_slot[i], new_retry[i] = q, retry[b]
             new_off[i] = offset[b] + st[b]["step"]
             if retry[b] and spec_slot.get(q) == b:
@@ -233,12 +245,11 @@ def relax_pool(problem, sims, masks, states, thr, slots=256, maxerr=1e-6, max_st
             for b in long_first:
                 if not idle:
                     break
-                f = idle.pop(0)
-                q = slot[b]
-                place(f, q, True)
-                spec_slot[q] = f
-                started.append((f, q))
+                started.append((idle.pop(0), slot[b]))
             if started:
+                place([f for f, _ in started], [q for _, q in started], [True] * len(started))
+                for f, q in started:
+                    spec_slot[q] = f
                 restart([f for f, _ in started], np.stack([fallback] * len(started)), [q for _, q in started],
                         fallback_max_steps)
                 n_spec += len(started)
