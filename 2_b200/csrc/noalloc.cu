@@ -9,6 +9,7 @@
 // the caller passes the magnetisation and a 3-double output, and the partial sums live
 // in a fixed file-scope device array (every GPU that loads this library holds it, 192
 // KB, until the process exits).
+#include <cstdio>
 #include <mutex>
 
 #include "mm_internal.h"
@@ -68,6 +69,8 @@ __global__ void __launch_bounds__(NA_THREADS) na_partial_kernel(const float* __r
     }
 }
 
+// One thread per component sums the block partials serially (at most 8192, in block
+// order): a few microseconds at the largest size, and deterministic.
 __global__ void na_finish_kernel(const float* __restrict__ partials, int nblocks, long long N, double* out) {
     if (threadIdx.x >= 3) return;
     const int q = threadIdx.x;
@@ -80,7 +83,10 @@ __global__ void na_finish_kernel(const float* __restrict__ partials, int nblocks
 }
 
 // Device address of the scratch array on the current device, looked up once per device
-// (the array's name is a host-side stand-in in host code, not a device address).
+// (the array's name is a host-side stand-in in host code, not a device address).  The
+// cache is keyed by device number, so it assumes the runtime's primary context on each
+// device and no cudaDeviceReset between calls: after a reset the module is loaded again
+// and the cached address is stale.
 int na_scratch(float** out) {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= NA_MAX_DEVICES) return MM_ERR_CUDA;
@@ -103,23 +109,40 @@ int na_scratch(float** out) {
 //   out   : device, 3 doubles: sum_i m_c[i] / ncell, compensated FP32 partial sums
 // Asynchronous on `stream`.  The first call on a device looks up the scratch array's
 // device address (cudaGetSymbolAddress) and should come before any stream capture on
-// that device.  All calls share the one scratch array and it keeps the last call's
-// contents, so calls that overlap on the GPU (different streams, or host threads without
-// ordering) race: order them on one stream.
+// that device; the address is kept per device number (primary context, no
+// cudaDeviceReset in between).  A CUDA error left pending by earlier work is reported,
+// not attributed to this call's launches.  All calls share the one scratch array and it
+// keeps the last call's contents, so calls that overlap on the GPU (different streams,
+// or host threads without ordering) race: order them on one stream.
 extern "C" MM_API int mm_average_noalloc(const float* m, long long ncell, double* out, mm_stream stream) {
     if (!m || !out) return mm::report_error(MM_ERR_ARG, "mm_average_noalloc: null m or out");
     if (ncell < 1 || ncell > NA_MAX_CELLS)
         return mm::report_error(MM_ERR_ARG,
                                 "mm_average_noalloc: ncell must be in 1..16777216 (the fixed scratch array holds "
                                 "8192 blocks of 2048 cells); use mm_average with a plan for larger grids");
+    char msg[256];
+    // an error the caller left pending would otherwise be read back after our launches
+    // and reported as theirs: name it and stop
+    const cudaError_t prior = cudaGetLastError();
+    if (prior != cudaSuccess) {
+        snprintf(msg, sizeof msg, "mm_average_noalloc: a CUDA error was pending before the call: %s",
+                 cudaGetErrorString(prior));
+        return mm::report_error(MM_ERR_CUDA, msg);
+    }
     float* partials = nullptr;
     int rc = na_scratch(&partials);
     if (rc != MM_OK) return mm::report_error(rc, "mm_average_noalloc: cudaGetSymbolAddress of the scratch array failed");
     const int nblocks = (int)((ncell + NA_CELLS_PER_BLOCK - 1) / NA_CELLS_PER_BLOCK);
     cudaStream_t st = (cudaStream_t)stream;
     na_partial_kernel<<<nblocks, NA_THREADS, 0, st>>>(m, ncell, partials);
-    if (cudaGetLastError() != cudaSuccess) return mm::report_error(MM_ERR_CUDA, "mm_average_noalloc: launch failed");
-    na_finish_kernel<<<1, 32, 0, st>>>(partials, nblocks, ncell, out);
-    if (cudaGetLastError() != cudaSuccess) return mm::report_error(MM_ERR_CUDA, "mm_average_noalloc: launch failed");
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) {
+        na_finish_kernel<<<1, 32, 0, st>>>(partials, nblocks, ncell, out);
+        e = cudaGetLastError();
+    }
+    if (e != cudaSuccess) {
+        snprintf(msg, sizeof msg, "mm_average_noalloc: launch failed: %s", cudaGetErrorString(e));
+        return mm::report_error(MM_ERR_CUDA, msg);
+    }
     return MM_OK;
 }

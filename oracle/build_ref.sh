@@ -6,7 +6,8 @@
 # The reference targets sm_20/sm_30 (src/Make.inc:11-17); only the architecture flag
 # changes, and <stdio.h> is force-included because gpu_safe.h uses printf without it.
 set -e
-REF=${REF_ROOT:-/root/reference}/src/libmumax2
+[ -n "$REF_ROOT" ] || { echo "set REF_ROOT to the mumax/2 source tree" >&2; exit 1; }
+REF=$REF_ROOT/src/libmumax2
 HERE=$(cd "$(dirname "$0")" && pwd)
 OUT=$HERE/_ref
 [ -d "$REF" ] || { echo "reference sources not found at $REF" >&2; exit 1; }

@@ -1,6 +1,6 @@
 """Regenerates the golden fixtures of tests/golden from the reference's own data files.
 
-Reads (only when the mumax/2 tree is available, default /root/reference):
+Reads (only when the mumax/2 tree is available; its root is the first argument or $REF_ROOT):
   tests/stdsolution4.txt   muMAG standard problem 4, <m>(t) with t in ns
 and writes subsampled copies next to this script.  Run: python tests/golden/make_golden.py [REF_ROOT]
 """
@@ -25,4 +25,7 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("REF_ROOT")
+    if not root:
+        sys.exit("usage: make_golden.py REF_ROOT (or set REF_ROOT)")
+    main(root)

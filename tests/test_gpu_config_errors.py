@@ -1,6 +1,7 @@
 """Error of the GPU path against the FP64 oracle, one figure per configuration (each test
 prints it): the single-layer film over the full simulated nanosecond, the field of a
-3-D film, one member of the thermal ensemble stepped with the same Philox noise, and a
+3-D film, the benchmarked 256x256x16 film at full size (fields, energy, five RK23
+steps), one member of the thermal ensemble stepped with the same Philox noise, and a
 relaxation of the warm-start problem set.  Targets: 1e-5 relative on H_eff, 1e-4 on the
 averaged magnetisation, 1e-4 relative on the relaxed energy."""
 import numpy as np
@@ -38,9 +39,9 @@ def test_film_rk45_one_nanosecond():
     assert err < 1e-4
 
 
-def test_film3d_field():
+def test_film3d_field_64x64x16():
     """3-D film with the headline's material (Ms 1.1e6, Aex 1.5e-11, Ku1 5e5 along z) on a
-    64x64x16 grid (the 256x256x16 tensor is too slow for the CPU oracle): H_eff."""
+    64x64x16 grid: H_eff and torque."""
     import oracle as O
     from mumax2 import Plan
     n = (16, 64, 64)
@@ -53,6 +54,56 @@ def test_film3d_field():
     t_err = rel_err(to_np(g.torque(m)[0]), o.torque(m)[0])
     print("config film3d 64x64x16: H_eff rel err", err, "torque rel err", t_err)
     assert err < 1e-5 and t_err < 1e-5
+
+
+def test_headline_film3d_256x256x16_full_size():
+    """The benchmarked workload itself (bench.py WORKLOAD: 256x256x16 cells of 4x4x2 nm,
+    Ms 1.1e6, Aex 1.5e-11, Ku1 5e5 along z, alpha 0.1, RK23 at max error 1e-5, the
+    seeded random initial state of the bench) at full size against the FP64 oracle:
+    every field term, H_eff per component, the torque and the energy of that state
+    (1e-5 relative), then 5 RK23 steps with the same accepted and rejected step counts,
+    the same time reached and max |dm| < 2e-4."""
+    import bench
+    import oracle as O
+    from mumax2 import Plan
+    w = bench.WORKLOAD
+    d = O.full_desc(**bench.problem())
+    o = O.Oracle(d)
+    g = Plan(d)
+    m0 = bench.initial_m(0).astype(np.float64)
+    N = int(np.prod(w["n"]))
+    fg, fo = g.fields(m0), o.fields(m0)
+    for term in ["demag", "ex", "anis", "eff"]:
+        e = rel_err(to_np(fg[term]), fo[term])
+        print(f"headline 256x256x16: {term} rel err {e:.3e}")
+        assert e < 1e-5, term
+    heg, heo = to_np(fg["eff"]).reshape(3, N), fo["eff"].reshape(3, N)
+    per_comp = [float(np.abs(heg[c] - heo[c]).max() / np.abs(heo[c]).max()) for c in range(3)]
+    print("headline 256x256x16: H_eff rel err per component (z, y, x internal)", per_comp)
+    assert max(per_comp) < 1e-5
+    t_err = rel_err(to_np(g.torque(m0)[0]), o.torque(m0)[0])
+    print("headline 256x256x16: torque rel err", t_err)
+    assert t_err < 1e-5
+    g.solver(w["solver"], dt=w["dt0"], maxerr=w["maxerr"])
+    g.set_state(m0)
+    eg, eo = g.energy(), o.energy(m0)
+    for k in ["E_ex", "E_demag", "E_anis", "E"]:
+        e = abs(eg[k] - eo[k]) / abs(eo[k])
+        print(f"headline 256x256x16: {k} rel err {e:.3e}")
+        assert e < 1e-5, k
+    r = O.OracleRun(o, m0, solver=w["solver"], dt=w["dt0"], maxerr=w["maxerr"])
+    for _ in range(5):
+        r.step()
+    g.steps(5)
+    st = g.stats()
+    mg = g.get_state().astype(np.float64)
+    dm = np.abs(mg - o.normalize(r.m.copy())).max()
+    print("headline 256x256x16, 5 RK23 steps: gpu", st["step"], st["badsteps"], st["t"], "oracle", r.st.step,
+          r.st.badsteps, r.st.t, "max|dm|", dm)
+    assert st["status"] == 0
+    assert st["step"] == r.st.step and st["badsteps"] == r.st.badsteps
+    assert abs(st["t"] - r.st.t) <= 1e-6 * r.st.t
+    assert dm < 2e-4
 
 
 def test_thermal_ensemble_member():

@@ -1,4 +1,5 @@
-"""The allocation-free <m> entry point (mm_average_noalloc) against the plan-based one.
+"""The allocation-free <m> entry point (mm_average_noalloc) against the plan-based one
+and against an FP64 numpy mean of the same float32 state.
 
 mm_average_noalloc exists for callers that cannot allocate device memory (code running
 inside a CUDA stream capture, engines whose GPU memory is owned by another allocator):
@@ -35,8 +36,10 @@ def test_noalloc_average_matches_plan_average_twice(n):
     lib = nat.lib()
     p = _plan_and_state(n, seed=sum(n))
     want = p.average()                          # existing entry point (plan workspace)
-    md = torch.as_tensor(p.get_state(), device="cuda")   # the same float32 state
+    state = p.get_state()
+    md = torch.as_tensor(state, device="cuda")   # the same float32 state
     N = n[0] * n[1] * n[2]
+    exact = np.asarray(state, dtype=np.float32).astype(np.float64).reshape(3, N).mean(axis=1)
     for call in range(2):                       # two calls in a row share the scratch array
         out = torch.full((3,), float("nan"), dtype=torch.float64, device="cuda")
         rc = lib.mm_average_noalloc(C.c_void_p(md.data_ptr()), N, C.c_void_p(out.data_ptr()), None)
@@ -44,6 +47,7 @@ def test_noalloc_average_matches_plan_average_twice(n):
         torch.cuda.synchronize()
         got = out.cpu().numpy()
         assert np.abs(got - want).max() <= TOL, (call, got, want)
+        assert np.abs(got - exact).max() <= TOL, (call, got, exact)   # FP64 mean of the same floats
     p.close()
 
 
