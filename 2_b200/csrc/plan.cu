@@ -24,11 +24,13 @@
 #include "pdl.cuh"
 
 namespace mm {
-int build_demag_kernel(const int L[3], const double cell[3], const int pbc[3], int accuracy, float* khat,
+int build_demag_kernel(const int L[3], const double cell[3], const int pbc[3], int kind, int accuracy, float* khat,
                        const int kd[3], int nz[6], cudaStream_t st, char* err, int errlen);
 int build_exchange_kernel(const int L[3], const double cell[3], float* kex, const int kd[3], cudaStream_t st,
                           char* err, int errlen);
 int combine_dex(const float* kd, const float* kex, long long oct, double c, float* khat, cudaStream_t st);
+int fill_demag_tensor(const int L[3], const double cell[3], const int pbc[3], int kind, int accuracy, double* K,
+                      cudaStream_t st);
 }
 
 using namespace mm;
@@ -615,6 +617,9 @@ extern "C" MM_API int mm_plan_create_batch(const mm_problem* prob, int nsim, con
         p->prob.seed = m0.seed;
         for (int i = 0; i < 3; i++) { p->prob.bext[i] = m0.bext[i]; p->prob.anisu[i] = m0.anisu[i]; }
     }
+    if (prob->demag_tensor != MM_TENSOR_ARNE && prob->demag_tensor != MM_TENSOR_NEWELL)
+        return set_err(MM_ERR_ARG, "demag_tensor must be MM_TENSOR_ARNE (0) or MM_TENSOR_NEWELL (1), got %d",
+                       prob->demag_tensor);
     if (prob->demag_exchange && (!prob->demag || prob->aex_mask || nsim != 1)) {
         delete p;
         return set_err(MM_ERR_ARG, "demag_exchange needs demag = 1, a uniform Aex (no mask) and one simulation");
@@ -676,8 +681,8 @@ extern "C" MM_API int mm_plan_create_batch(const mm_problem* prob, int nsim, con
         if (prob->demag_exchange) {
             if (!(rc = dalloc(p, (void**)&p->khat_d, sizeof(float) * 6 * oct)) &&
                 !(rc = dalloc(p, (void**)&p->khat_ex, sizeof(float) * oct))) {
-                rc = build_demag_kernel(g.L, prob->cell, prob->pbc, prob->demag_accuracy, p->khat_d, g.kd, nz, st,
-                                        err, sizeof err);
+                rc = build_demag_kernel(g.L, prob->cell, prob->pbc, prob->demag_tensor, prob->demag_accuracy, p->khat_d,
+                                        g.kd, nz, st, err, sizeof err);
                 if (rc == MM_OK) rc = build_exchange_kernel(g.L, prob->cell, p->khat_ex, g.kd, st, err, sizeof err);
                 if (rc == MM_OK)
                     rc = combine_dex(p->khat_d, p->khat_ex, oct, 2.0 * prob->aex / (MU0 * prob->msat * prob->msat),
@@ -685,8 +690,8 @@ extern "C" MM_API int mm_plan_create_batch(const mm_problem* prob, int nsim, con
                 for (int q = 0; q < 3; q++) nz[q] = 1;
             }
         } else {
-            rc = build_demag_kernel(g.L, prob->cell, prob->pbc, prob->demag_accuracy, p->khat, g.kd, nz, st, err,
-                                    sizeof err);
+            rc = build_demag_kernel(g.L, prob->cell, prob->pbc, prob->demag_tensor, prob->demag_accuracy, p->khat, g.kd,
+                                    nz, st, err, sizeof err);
         }
         if (rc == MM_OK && cudaStreamSynchronize(st) != cudaSuccess) rc = MM_ERR_CUDA;
         cudaStreamDestroy(st);
@@ -813,6 +818,8 @@ extern "C" MM_API int mm_plan_set_problem(mm_plan p, const mm_problem* prob) {
     if ((prob->demag_exchange != 0) != (p->khat_d != nullptr))
         return set_err(MM_ERR_ARG, "demag_exchange on/off cannot change after plan creation");
     if (prob->demag_exchange && prob->aex_mask) return set_err(MM_ERR_ARG, "demag_exchange needs a uniform Aex");
+    if (prob->demag_tensor != p->prob.demag_tensor)
+        return set_err(MM_ERR_ARG, "the demag tensor kind cannot change after plan creation");
     if (!(prob->gamma != 0.0)) return set_err(MM_ERR_ARG, "gamma must be non-zero");
     if (p->nsim == 1 && !(prob->msat != 0.0)) return set_err(MM_ERR_ARG, "Msat must be non-zero");
     p->prob = *prob;
@@ -1068,6 +1075,23 @@ extern "C" MM_API int mm_plan_demag_kernel(mm_plan p, float* out, int kd[3]) {
     const long long oct = (long long)p->g.kd[0] * p->g.kd[1] * p->g.kd[2];
     const float* src = p->khat_d ? p->khat_d : p->khat;
     CUCHK(cudaMemcpy(out, src, sizeof(float) * 6 * (size_t)oct, cudaMemcpyDeviceToHost));
+    return MM_OK;
+}
+
+extern "C" MM_API int mm_demag_tensor(const int L[3], const double cell[3], const int pbc[3], int kind, int accuracy,
+                                      double* out, mm_stream stream) {
+    if (!L || !cell || !pbc || !out) return set_err(MM_ERR_ARG, "null argument");
+    if (kind != MM_TENSOR_ARNE && kind != MM_TENSOR_NEWELL) return set_err(MM_ERR_ARG, "unknown tensor kind %d", kind);
+    for (int i = 0; i < 3; i++) {
+        if (L[i] < 1 || L[i] > 65536) return set_err(MM_ERR_ARG, "padded size %d out of range", L[i]);
+        if (!(cell[i] > 0)) return set_err(MM_ERR_ARG, "cell size must be > 0");
+    }
+    if (kind == MM_TENSOR_ARNE && !(L[1] > 1 && L[2] > 1 && L[1] % 2 == 0 && L[2] % 2 == 0 &&
+                                    (L[0] == 1 || L[0] % 2 == 0)))
+        return set_err(MM_ERR_ARG, "Kernel_Arne needs even padded sizes > 1 in y and x (got %d %d %d)", L[0], L[1],
+                       L[2]);
+    const int rc = fill_demag_tensor(L, cell, pbc, kind, accuracy, out, (cudaStream_t)stream);
+    if (rc != MM_OK) return set_err(rc, "demag tensor launch failed: %s", cudaGetErrorString(cudaGetLastError()));
     return MM_OK;
 }
 

@@ -68,6 +68,7 @@ def read_field(path):
     return a.reshape(nc.value, n[0], n[1], n[2]), tuple(n), t.value
 
 SOLVERS = {"euler": 0, "heun": 1, "rk12": 2, "rk23": 3, "rk45": 4, "am12": 5}
+TENSORS = {"arne": 0, "newell": 1}
 
 
 class MMProblem(C.Structure):
@@ -91,6 +92,7 @@ class MMProblem(C.Structure):
         ("sl_pol_mask", C.c_void_p), ("lambda_mask", C.c_void_p), ("eps_prime_mask", C.c_void_p),
         ("t_fl_mask", C.c_void_p),
         ("demag_exchange", C.c_int),
+        ("demag_tensor", C.c_int),
     ]
 
 
@@ -208,6 +210,8 @@ _PROTOS = {
     "mm_tabulate_read": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "mm_plan_create_batch": (C.c_int, [C.POINTER(MMProblem), C.c_int, C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]),
     "mm_plan_demag_kernel": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "mm_demag_tensor": (C.c_int, [C.c_int * 3, C.c_double * 3, C.c_int * 3, C.c_int, C.c_int, C.c_void_p,
+                                  C.c_void_p]),
     "mm_plan_tiles": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "mm_plan_set_tiles": (C.c_int, [C.c_void_p, C.c_void_p]),
     "mm_plan_nsim": (C.c_int, [C.c_void_p]),
@@ -267,6 +271,8 @@ def make_problem(d, masks=None):
         setattr(s, k, int(d.get(k, 0)))
     s.demag_accuracy = int(d.get("demag_accuracy", 6))
     s.demag_exchange = int(d.get("demag_exchange", 0))
+    s.demag_tensor = TENSORS[d.get("demag_tensor", "arne")] if isinstance(d.get("demag_tensor", 0), str) \
+        else int(d.get("demag_tensor", 0))
     for k, dv in [("msat", 8e5), ("aex", 1.3e-11), ("alpha", 0.02), ("gamma", 2.211e5), ("ku", 0.0),
                   ("temp", 0.0), ("zl_pol", 1.0), ("xi", 0.05), ("sl_pol", 1.0), ("eps_prime", 0.0),
                   ("t_fl", 0.0)]:

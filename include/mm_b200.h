@@ -60,6 +60,9 @@ enum {
     MM_ERR_RANGE = -7          /* time outside a SetPointwise table (update_pointwise.go:66) */
 };
 
+/* demag tensor kinds (mm_problem.demag_tensor) */
+enum { MM_TENSOR_ARNE = 0, MM_TENSOR_NEWELL = 1 };
+
 /* solvers */
 enum { MM_EULER = 0, MM_HEUN = 1, MM_RK12 = 2, MM_RK23 = 3, MM_RK45 = 4, MM_AM12 = 5 };
 
@@ -90,6 +93,11 @@ typedef struct mm_problem {
      * and computed by the same convolution of m; the 6-neighbour stencil term is off.
      * Needs demag = 1, a uniform Aex (no aex_mask) and nsim = 1. */
     int demag_exchange;
+    /* MM_TENSOR_ARNE (0): Kernel_Arne face-charge integration (kernel_magnetostatic.go:
+     * 30-181), the reference's only tensor.  MM_TENSOR_NEWELL (1): the closed forms of
+     * Newell, Williams & Dunlop (1993) in FP64 within 8 cell sizes, the cell-averaged
+     * dipole tensor by Gauss quadrature beyond.  No counterpart in the reference. */
+    int demag_tensor;
 } mm_problem;
 
 /* Scalars of one simulation of a batched plan (the multipliers of Msat, Aex, alpha, B_ext,
@@ -142,6 +150,15 @@ MM_API int mm_plan_nsim(mm_plan plan);
  * depend on the tiles (energies up to the order of their block partial sums). */
 MM_API int mm_plan_tiles(mm_plan plan, int tiles[4], double* eval_us);
 MM_API int mm_plan_set_tiles(mm_plan plan, const int tiles[4]);
+/* Real-space demag tensor in FP64 on the GPU, the function Kernel_Arne
+ * (kernel_magnetostatic.go:30-181) computes on the host: out[6][L0][L1][L2] (device,
+ * caller-allocated; components 00 11 22 12 02 01 of the internal axes, K = -N so that
+ * H = K * M), for the padded sizes L, cell sizes and periodic flags of a plan; kind
+ * MM_TENSOR_ARNE (with `accuracy`, 6 for module demag) or MM_TENSOR_NEWELL.  Entries
+ * outside the reference's index ranges (the Nyquist planes) are zero.  Async on stream. */
+MM_API int mm_demag_tensor(const int L[3], const double cell[3], const int pbc[3], int kind, int accuracy,
+                           double* out, mm_stream stream);
+
 /* The plan's transformed demag tensor, one octant: out[6][kd0][kd1][kd2] (host, may be
  * NULL to query kd), components xx yy zz yz xz xy in internal axis order, scaled by
  * 1/(L0 L1 L2) like the reference's fftKern (maxwell_convolution.go:576-612); the other

@@ -78,6 +78,7 @@ typedef struct {
     const float *p_mask[3];
     const float *sl_pol_mask, *lambda_mask, *eps_prime_mask, *t_fl_mask;
     int demag_exchange;   // module demagexch: exchange inside the demag convolution
+    int demag_tensor;     // 0 Kernel_Arne, 1 Newell (closed forms near, dipole quadrature far)
 } or_desc;
 
 typedef struct {
@@ -267,6 +268,135 @@ extern "C" void or_kernel_arne(const int size[3], const double cs[3], const int 
     }
 }
 
+// ---------------------------------------------------------------- Newell tensor
+// Not in the reference (its only tensor is Kernel_Arne).  Restates the published method
+// the GPU's Newell mode uses: Newell, Williams & Dunlop, J. Geophys. Res. 98, 9551
+// (1993), f and g closed forms, N = 1/(4 pi V) * 27-point difference with weights
+// (2, -1, -1) per axis, within 8 largest-cell-edges of the origin; beyond, the cell-cell
+// average of the point-dipole tensor (delta r^2 - 3 r r) / (4 pi r^5) with tent weights
+// prod (d_k - |s_k|) / V, by Gauss-Legendre quadrature of Q points per half axis (Q = 6
+// below 16 edges, 4 below 32, 3 beyond).  Gauss nodes here come from Newton iteration on
+// the Legendre polynomials.  Output: K = -N in the 9-component layout of or_kernel_arne.
+static double nw_f(double x, double y, double z) {
+    const double x2 = x * x, y2 = y * y, z2 = z * z, R = std::sqrt(x2 + y2 + z2);
+    double r = (2 * x2 - y2 - z2) * R / 6;
+    if (x2 + z2 > 0) r += y / 2 * (z2 - x2) * std::asinh(y / std::sqrt(x2 + z2));
+    if (x2 + y2 > 0) r += z / 2 * (y2 - x2) * std::asinh(z / std::sqrt(x2 + y2));
+    if (x != 0) r -= x * y * z * std::atan(y * z / (x * R));
+    return r;
+}
+static double nw_g(double x, double y, double z) {
+    const double x2 = x * x, y2 = y * y, z2 = z * z, R = std::sqrt(x2 + y2 + z2);
+    double r = -x * y * R / 3;
+    if (x2 + y2 > 0) r += x * y * z * std::asinh(z / std::sqrt(x2 + y2));
+    if (y2 + z2 > 0) r += y / 6 * (3 * z2 - y2) * std::asinh(x / std::sqrt(y2 + z2));
+    if (x2 + z2 > 0) r += x / 6 * (3 * z2 - x2) * std::asinh(y / std::sqrt(x2 + z2));
+    if (z != 0) r -= z * z2 / 6 * std::atan(x * y / (z * R));
+    if (y != 0) r -= z * y2 / 2 * std::atan(x * z / (y * R));
+    if (x != 0) r -= z * x2 / 2 * std::atan(y * z / (x * R));
+    return r;
+}
+static double nw_diff(bool useg, double a, double b, double c, double da, double db, double dc) {
+    double s = 0;
+    for (int i = -1; i <= 1; i++)
+        for (int j = -1; j <= 1; j++)
+            for (int k = -1; k <= 1; k++) {
+                const double w = (i ? -1.0 : 2.0) * (j ? -1.0 : 2.0) * (k ? -1.0 : 2.0);
+                const double x = a + i * da, y = b + j * db, z = c + k * dc;
+                s += w * (useg ? nw_g(x, y, z) : nw_f(x, y, z));
+            }
+    return s / (4 * PI * da * db * dc);
+}
+static void gauss_legendre(int n, std::vector<double>& x, std::vector<double>& w) {
+    x.resize(n);
+    w.resize(n);
+    for (int i = 0; i < n; i++) {
+        double t = std::cos(PI * (i + 0.75) / (n + 0.5)), dp = 1;
+        for (int it = 0; it < 100; it++) {
+            double p0 = 1, p1 = t;
+            for (int k = 2; k <= n; k++) {
+                const double p2 = ((2 * k - 1) * t * p1 - (k - 1) * p0) / k;
+                p0 = p1;
+                p1 = p2;
+            }
+            dp = n * (t * p1 - p0) / (t * t - 1);
+            const double dt = p1 / dp;
+            t -= dt;
+            if (std::fabs(dt) < 1e-17) break;
+        }
+        x[i] = t;
+        w[i] = 2 / ((1 - t * t) * dp * dp);
+    }
+}
+static void nw_far(const double X[3], const double d[3], int Q, double N[6]) {
+    std::vector<double> gx, gw;
+    gauss_legendre(Q, gx, gw);
+    std::vector<double> s[3], w[3];
+    for (int a = 0; a < 3; a++)
+        for (int q = 0; q < Q; q++) {
+            const double xi = 0.5 * (gx[q] + 1), wi = 0.5 * gw[q] * d[a] * d[a] * (1 - xi);
+            s[a].push_back(d[a] * xi);  w[a].push_back(wi);
+            s[a].push_back(-d[a] * xi); w[a].push_back(wi);
+        }
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    for (size_t i = 0; i < s[0].size(); i++)
+        for (size_t j = 0; j < s[1].size(); j++)
+            for (size_t k = 0; k < s[2].size(); k++) {
+                const double r0 = X[0] + s[0][i], r1 = X[1] + s[1][j], r2 = X[2] + s[2][k];
+                const double rr = r0 * r0 + r1 * r1 + r2 * r2;
+                const double W = w[0][i] * w[1][j] * w[2][k] / (rr * rr * std::sqrt(rr));
+                acc[0] += W * (rr - 3 * r0 * r0);
+                acc[1] += W * (rr - 3 * r1 * r1);
+                acc[2] += W * (rr - 3 * r2 * r2);
+                acc[3] += W * (-3 * r1 * r2);
+                acc[4] += W * (-3 * r0 * r2);
+                acc[5] += W * (-3 * r0 * r1);
+            }
+    for (int q = 0; q < 6; q++) N[q] = acc[q] / (4 * PI * d[0] * d[1] * d[2]);
+}
+
+extern "C" void or_kernel_newell(const int size[3], const double cs[3], const int periodic[3], double* K) {
+    const long NL = (long)size[0] * size[1] * size[2];
+    std::fill(K, K + 9 * NL, 0.0);
+    int x1 = -(size[0] - 1) / 2, x2 = size[0] / 2 - 1;
+    int y1 = -(size[1] - 1) / 2, y2 = size[1] / 2 - 1;
+    int z1 = -(size[2] - 1) / 2, z2 = size[2] / 2 - 1;
+    if (size[0] == 1 && periodic[0] == 0) x2 = 0;
+    x1 *= (periodic[0] + 1); x2 *= (periodic[0] + 1);
+    y1 *= (periodic[1] + 1); y2 *= (periodic[1] + 1);
+    z1 *= (periodic[2] + 1); z2 *= (periodic[2] + 1);
+    const double lam = std::max(cs[0], std::max(cs[1], cs[2]));
+    const double d[3] = {cs[0] / lam, cs[1] / lam, cs[2] / lam};
+    // (s, d) component of each of the 6 results 00 11 22 12 02 01
+    static const int QS[6] = {0, 1, 2, 1, 0, 0}, QD[6] = {0, 1, 2, 2, 2, 1};
+    const bool par_ok = (periodic[0] == 0);
+#pragma omp parallel for schedule(dynamic) if (par_ok)
+    for (int x = x1; x <= x2; x++) {
+        for (int y = y1; y <= y2; y++)
+            for (int z = z1; z <= z2; z++) {
+                const double X[3] = {x * d[0], y * d[1], z * d[2]};
+                const double rho = std::sqrt(X[0] * X[0] + X[1] * X[1] + X[2] * X[2]);
+                double N[6];
+                if (rho < 8.0) {
+                    N[0] = nw_diff(false, X[0], X[1], X[2], d[0], d[1], d[2]);
+                    N[1] = nw_diff(false, X[1], X[0], X[2], d[1], d[0], d[2]);
+                    N[2] = nw_diff(false, X[2], X[1], X[0], d[2], d[1], d[0]);
+                    N[3] = nw_diff(true, X[1], X[2], X[0], d[1], d[2], d[0]);
+                    N[4] = nw_diff(true, X[0], X[2], X[1], d[0], d[2], d[1]);
+                    N[5] = nw_diff(true, X[0], X[1], X[2], d[0], d[1], d[2]);
+                } else {
+                    nw_far(X, d, rho < 16.0 ? 6 : rho < 32.0 ? 4 : 3, N);
+                }
+                const long idx = ((long)wrap_idx(x, size[0]) * size[1] + wrap_idx(y, size[1])) * size[2] +
+                                 wrap_idx(z, size[2]);
+                for (int q = 0; q < 6; q++) {
+                    K[(long)(QS[q] * 3 + QD[q]) * NL + idx] += -N[q];
+                    if (QS[q] != QD[q]) K[(long)(QD[q] * 3 + QS[q]) * NL + idx] += -N[q];
+                }
+            }
+    }
+}
+
 // ---------------------------------------------------------------- Philox4x32-10
 // Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as easy as 1, 2, 3", SC'11.
 static inline void philox4x32_10(uint32_t ctr[4], uint32_t key0, uint32_t key1) {
@@ -428,7 +558,10 @@ extern "C" void* or_create(const or_desc* desc) {
     if (d.demag_exchange) d.exchange = 0;  // the stencil term is inside the kernel
     if (d.demag) {
         std::vector<double> K(9 * P->NL);
-        or_kernel_arne(P->L, d.cell, d.pbc, d.demag_accuracy > 0 ? d.demag_accuracy : 6, 0, K.data());
+        if (d.demag_tensor == 1)
+            or_kernel_newell(P->L, d.cell, d.pbc, K.data());
+        else
+            or_kernel_arne(P->L, d.cell, d.pbc, d.demag_accuracy > 0 ? d.demag_accuracy : 6, 0, K.data());
         double kmax = 0;
         for (double v : K) kmax = std::max(kmax, std::fabs(v));
         for (int q = 0; q < 6; q++) {

@@ -37,6 +37,7 @@ class OrDesc(C.Structure):
         ("p_mask", FP * 3),
         ("sl_pol_mask", FP), ("lambda_mask", FP), ("eps_prime_mask", FP), ("t_fl_mask", FP),
         ("demag_exchange", C.c_int),
+        ("demag_tensor", C.c_int),
     ]
 
 
@@ -67,6 +68,7 @@ def lib():
         L.or_create.argtypes = [C.POINTER(OrDesc)]
         L.or_destroy.argtypes = [C.c_void_p]
         L.or_kernel_arne.argtypes = [C.c_int * 3, C.c_double * 3, C.c_int * 3, C.c_int, C.c_int, DP]
+        L.or_kernel_newell.argtypes = [C.c_int * 3, C.c_double * 3, C.c_int * 3, DP]
         L.or_padded_size.argtypes = [C.c_int * 3, C.c_int * 3, C.c_int * 3]
         L.or_kernel_nonzero.argtypes = [C.c_void_p, C.POINTER(C.c_int)]
         L.or_normalize.argtypes = [C.c_void_p, DP]
@@ -122,6 +124,7 @@ def make_desc(d):
               "demag_accuracy"]:
         setattr(s, k, int(d[k]))
     s.demag_exchange = int(d.get("demag_exchange", 0))
+    s.demag_tensor = {"arne": 0, "newell": 1}.get(d.get("demag_tensor", 0), d.get("demag_tensor", 0))
     for k in ["msat", "aex", "alpha", "gamma", "ku", "temp", "zl_pol", "xi", "sl_pol",
               "eps_prime", "t_fl"]:
         setattr(s, k, float(d[k]))
@@ -278,6 +281,13 @@ def kernel_arne(L, cell, pbc=(0, 0, 0), accuracy=6, round_f32=False):
     K = np.zeros(9 * L[0] * L[1] * L[2])
     lib().or_kernel_arne((C.c_int * 3)(*L), (C.c_double * 3)(*cell), (C.c_int * 3)(*pbc), accuracy,
                          int(round_f32), _dp(K))
+    return K.reshape(3, 3, L[0], L[1], L[2])
+
+
+def kernel_newell(L, cell, pbc=(0, 0, 0)):
+    """Newell tensor K = -N, 9 components [s][d][L0][L1][L2] like kernel_arne."""
+    K = np.zeros(9 * L[0] * L[1] * L[2])
+    lib().or_kernel_newell((C.c_int * 3)(*L), (C.c_double * 3)(*cell), (C.c_int * 3)(*pbc), _dp(K))
     return K.reshape(3, 3, L[0], L[1], L[2])
 
 
