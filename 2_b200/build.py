@@ -9,8 +9,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libmm_b200.so")
-SOURCES = ["conv.cu", "rhs.cu", "demag_setup.cu", "plan.cu", "compat.cu", "noalloc.cu", "io.cpp", "am12.cu", "unet.cu"]
-HEADERS = ["fft.cuh", "fft4.cuh", "kernel_view.cuh", "pdl.cuh", "mm_internal.h"]
+SOURCES = ["conv.cu", "mixed.cu", "rhs.cu", "demag_setup.cu", "plan.cu", "compat.cu", "noalloc.cu", "io.cpp", "am12.cu", "unet.cu"]
+HEADERS = ["fft.cuh", "fft4.cuh", "mixed.cuh", "kernel_view.cuh", "pdl.cuh", "mm_internal.h"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
          "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden", "--diag-suppress", "177"]

@@ -28,12 +28,6 @@
 namespace mm {
 using namespace mmfft;
 
-// skip_retry: 1 = the kernel belongs to a retried attempt's reusable first evaluation
-// (skipped when tries > 0); 2 = an evaluation inside an AM12 fixed-point loop (skipped
-// once the loop has ended or the attempt was abandoned)
-__device__ __forceinline__ bool conv_skip(const DevCtl* ctl, int skip_retry) {
-    return ctl && (ctl->done || (skip_retry == 1 && ctl->tries > 0) || (skip_retry == 2 && ctl->am_skip));
-}
 
 // ---------------------------------------------------------------- R2C row pass
 // rows (per simulation): r = (c*Z + z)*Y + y over C components; input row r starts at in + r*in_pitch
@@ -799,7 +793,9 @@ cudaError_t launch_xfwd(int M, const S* in, PP pp, const float* mask, V* out, in
 #define X(m) case m: return launch_xfwd_t<m, V, S>(in, pp, mask, out, nrows, Z, Y, Yout, in_pitch, n_in, hp, tw, ctl, skip_retry, st, XFWD_SIM_PASS);
         MM_FOR_POW2(X)
 #undef X
-        default: return cudaErrorInvalidValue;
+        default:  // not a power of two: the mixed-radix pass (mixed.cu)
+            return launch_mr_xfwd<V, S>(M, in, pp, mask, out, nrows, Z, Y, Yout, in_pitch, n_in, hp, ctl, skip_retry,
+                                        st, XFWD_SIM_PASS);
     }
 }
 
@@ -864,14 +860,18 @@ cudaError_t launch_colfft(int L, int sign, V* S, int ncols, int nouter, long lon
 #define X(l) case l: return launch_colfft_t<l, -1, V>(S, ncols, nouter, outer_stride, line_stride, n_in, n_out, tw, ctl, skip_retry, st, nsim, sim_stride);
             MM_FOR_POW2(X)
 #undef X
-            default: return cudaErrorInvalidValue;
+            default:
+                return launch_mr_colfft<V>(L, -1, S, ncols, nouter, outer_stride, line_stride, n_in, n_out, ctl,
+                                           skip_retry, st, nsim, sim_stride);
         }
     } else {
         switch (L) {
 #define X(l) case l: return launch_colfft_t<l, 1, V>(S, ncols, nouter, outer_stride, line_stride, n_in, n_out, tw, ctl, skip_retry, st, nsim, sim_stride);
             MM_FOR_POW2(X)
 #undef X
-            default: return cudaErrorInvalidValue;
+            default:
+                return launch_mr_colfft<V>(L, 1, S, ncols, nouter, outer_stride, line_stride, n_in, n_out, ctl,
+                                           skip_retry, st, nsim, sim_stride);
         }
     }
 }
@@ -952,7 +952,9 @@ cudaError_t launch_colmul(int L, float2* S, const KernelView& K, int ncols, int 
 #define X(l) case l: return launch_colmul_t<l>(S, K, ncols, nouter, comp_stride, outer_stride, line_stride, n_in, kaxis, scale, tw, ctl, skip_retry, st, nsim, sim_stride, sim_scale);
         MM_FOR_POW2(X)
 #undef X
-        default: return cudaErrorInvalidValue;
+        default:
+            return launch_mr_colmul(L, S, K, ncols, nouter, comp_stride, outer_stride, line_stride, n_in, kaxis, scale,
+                                    ctl, skip_retry, st, nsim, sim_stride, sim_scale);
     }
 }
 

@@ -222,6 +222,15 @@ struct EpiArgs {
     int fwd_pad;
 };
 
+#ifdef __CUDACC__
+// skip_retry: 1 = the kernel belongs to a retried attempt's reusable first evaluation
+// (skipped when tries > 0); 2 = an evaluation inside an AM12 fixed-point loop (skipped
+// once the loop has ended or the attempt was abandoned)
+__device__ __forceinline__ bool conv_skip(const DevCtl* ctl, int skip_retry) {
+    return ctl && (ctl->done || (skip_retry == 1 && ctl->tries > 0) || (skip_retry == 2 && ctl->am_skip));
+}
+#endif
+
 // ---- launchers (conv.cu, rhs.cu)
 // Every launcher runs nsim simulations (gridDim.y = nsim); *_bstride are the element
 // strides between simulations, ctl (if not NULL) points to nsim control blocks, and
@@ -265,6 +274,21 @@ cudaError_t am_copy(PP src, PP dst, const DevCtl* ctl, long long n3, int nsim, i
 cudaError_t am_normalize(PP m, const float* msat_mask, const DevCtl* ctl, long long N, long long mask_bstride, int nsim,
                          int bps, int skip, cudaStream_t st);
 int xinv_blocks(int M, int n0n1);
+// mixed-radix passes (mixed.cu) for lengths that are not powers of two; the launchers of
+// conv.cu and rhs.cu hand those lengths to them.  Their twiddle tables must have been
+// prepared (mr_prepare, mixed.cuh) on the device for M and 2M, L1 and L0.
+template <typename V, typename S>
+cudaError_t launch_mr_xfwd(int M, const S* in, PP pp, const float* mask, V* out, int nrows, int Z, int Y, int Yout,
+                           int in_pitch, int n_in, int hp, const DevCtl* ctl, int skip_retry, cudaStream_t st,
+                           int nsim, long long in_bstride, long long out_bstride, long long mask_bstride);
+template <typename V>
+cudaError_t launch_mr_colfft(int L, int sign, V* S, int ncols, int nouter, long long outer_stride,
+                             long long line_stride, int n_in, int n_out, const DevCtl* ctl, int skip_retry,
+                             cudaStream_t st, int nsim, long long sim_stride);
+cudaError_t launch_mr_colmul(int L, float2* S, const KernelView& K, int ncols, int nouter, long long comp_stride,
+                             long long outer_stride, long long line_stride, int n_in, int kaxis, float scale,
+                             const DevCtl* ctl, int skip_retry, cudaStream_t st, int nsim, long long sim_stride,
+                             const float* sim_scale);
 // whether the C2R + epilogue pass for row length M can also write the R2C rows of the
 // next stage state (EpiArgs::fwd)
 bool epi_r2c_supported(int M);

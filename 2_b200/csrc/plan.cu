@@ -21,6 +21,7 @@
 
 #include "fft.cuh"
 #include "mm_internal.h"
+#include "mixed.cuh"
 #include "pdl.cuh"
 
 namespace mm {
@@ -644,12 +645,37 @@ extern "C" MM_API int mm_plan_create_batch(const mm_problem* prob, int nsim, con
             return set_err(MM_ERR_ARG, "demag needs even padded sizes > 1 in y and x (got %d %d %d)", g.L[0], g.L[1],
                            g.L[2]);
         }
-        if (!pow2(g.L[0]) || !pow2(g.L[1]) || !pow2(g.L[2]) || g.L[2] > 4096 || g.L[1] > 4096 || g.L[0] > 4096) {
-            mm_plan_destroy(p);
-            return set_err(MM_ERR_ARG, "demag transform sizes must be powers of two <= 4096 (got %d %d %d)", g.L[0],
-                           g.L[1], g.L[2]);
+        // transform lengths: powers of two go to the power-of-two passes, every other length
+        // up to 4096 with prime factors <= 31 to the mixed-radix ones (the reference takes
+        // any size through cuFFT, fftplanX.go:59-64; gridsize.go:16-33 recommends
+        // 2^n * {1, 3, 5, 7})
+        {
+            const int lens[4] = {g.L[0], g.L[1], g.L[2] / 2, g.L[2]};
+            for (int q = 0; q < 4; q++) {
+                const int len = lens[q];
+                if (len <= 1 || pow2(len)) {
+                    if (len > 4096) {
+                        mm_plan_destroy(p);
+                        return set_err(MM_ERR_ARG, "demag transform sizes must be <= 4096 (got %d %d %d)", g.L[0],
+                                       g.L[1], g.L[2]);
+                    }
+                    continue;
+                }
+                MrLine f;
+                if (!mr_factor(len, &f)) {
+                    mm_plan_destroy(p);
+                    return set_err(MM_ERR_ARG,
+                                   "demag transform size %d (padded %d %d %d) is above 4096 or has a prime factor "
+                                   "above 31; use sizes 2^n * {1, 3, 5, 7}",
+                                   len, g.L[0], g.L[1], g.L[2]);
+                }
+                if ((rc = mr_prepare(len)) != MM_OK) {
+                    mm_plan_destroy(p);
+                    return set_err(rc, "twiddle tables of length %d could not be built", len);
+                }
+            }
         }
-        if (nsim > 1 && (g.L[2] < 8 || g.L[2] > 2048)) {
+        if (nsim > 1 && pow2(g.L[2]) && (g.L[2] < 8 || g.L[2] > 2048)) {
             mm_plan_destroy(p);
             return set_err(MM_ERR_ARG, "batched plans with demag need 8 <= padded L2 <= 2048 (got %d)", g.L[2]);
         }
@@ -995,6 +1021,8 @@ static StageOp op_blank() {
 // arithmetic is the same, and so are the fields, torques and step sequences.
 static int autotune(mm_plan p) {
     if (!p->demag) return MM_OK;
+    // the tiles are those of the power-of-two passes
+    if (!pow2(p->g.L[0]) || !pow2(p->g.L[1]) || !pow2(p->g.L[2])) return MM_OK;
     const char* env = getenv("MM_AUTOTUNE");
     if (env && env[0] == '0') return MM_OK;
     cudaStream_t st = nullptr;

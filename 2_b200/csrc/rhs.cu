@@ -17,6 +17,7 @@
 
 #include "fft.cuh"
 #include "fft4.cuh"
+#include "mixed.cuh"
 #include "mm_internal.h"
 #include "kernel_view.cuh"
 #include "pdl.cuh"
@@ -1154,6 +1155,83 @@ static cudaError_t launch_xinv_t(const float2* S, int hp, int L1, const float2* 
     return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------- mixed-radix C2R + epilogue
+// Row lengths M that are not powers of two: the pre-processing of xinv_epi_kernel, the
+// mixed-radix inverse transform of mixed.cuh, then the same epilogue.  rpb rows of three
+// component lines per block (line (row, c) at sm + (row*3 + c)*M, natural order; the
+// scratch lines follow), blockDim.x / (3 rpb) threads per line.  BATCH: the simulation's
+// scalars are staged in shared memory (batched plans, time tables).
+template <bool TERMS, bool BATCH>
+__global__ void __launch_bounds__(384) mr_xinv_epi_kernel(const float2* __restrict__ S, int hp, int L1, MrLine f,
+                                                          const float2* __restrict__ twM,
+                                                          const float2* __restrict__ tw2M, EpiArgs A, int rpb) {
+    const DevCtl* ctl = A.ctl ? A.ctl + blockIdx.y : nullptr;
+    if (skip_eval(ctl, A.skip_retry)) return;
+    S += blockIdx.y * A.spec_bstride;
+    __shared__ SimScalars s_sim;  // covered by the barriers of the transform
+    if (BATCH && threadIdx.x == 0) stage_scalars(A, ctl, s_sim);
+    const int M = f.L;
+    const int nlines = 3 * rpb;
+    const int nt = blockDim.x / nlines;
+    const int li = threadIdx.x / nt, t = threadIdx.x % nt;
+    const int lr = li / 3, c = li % 3;
+    const int n0 = A.P.n[0], n1 = A.P.n[1];
+    const int nrows = n0 * n1;
+    const int row = blockIdx.x * rpb + lr;
+    const bool active = (li < nlines) && (row < nrows);
+    extern __shared__ unsigned char smem_raw[];
+    float2* sm = reinterpret_cast<float2*>(smem_raw);
+    const int lc = li < nlines ? li : 0;
+    float2* xl = sm + (size_t)lc * M;
+    float2* scratch = sm + (size_t)(nlines + lc) * M;
+    if (active) {
+        const int z = row / n1, y = row % n1;
+        const float2* src = S + ((long long)(c * n0 + z) * L1 + y) * hp;
+        // Z[k] = (X[k] + conj X[M-k]) + i W^-k (X[k] - conj X[M-k]),  W = exp(-2 pi i / 2M)
+        for (int k = t; k < M; k += nt) {
+            const float2 a = src[k], b = src[M - k];
+            const float2 s = make_float2(a.x + b.x, a.y - b.y);
+            const float2 d = make_float2(a.x - b.x, a.y + b.y);
+            const float2 w0 = tw2M[k];
+            const float2 wd = cmul(make_float2(w0.x, -w0.y), d);
+            xl[k] = make_float2(s.x - wd.y, s.y + wd.x);
+        }
+    }
+    mr_fft<+1, float2>(xl, scratch, f, twM, t, nt, active);
+    const int row0 = blockIdx.x * rpb;
+    epilogue_rows<TERMS, false, BATCH>(A, pick_scalars<BATCH>(s_sim, A.P.s), sm, M, row0, min(rpb, nrows - row0));
+}
+
+// rows per block and threads per line of the mixed-radix epilogue
+static void mr_xinv_shape(int M, int* rpb, int* nt) {
+    *nt = M >= 256 ? 128 : (M >= 64 ? 64 : 32);
+    *rpb = 384 / (3 * *nt) > 0 ? 384 / (3 * *nt) : 1;
+    while (*rpb > 1 && (size_t)*rpb * 6 * M * sizeof(float2) > 96 * 1024) *rpb /= 2;
+}
+
+template <bool TERMS, bool BATCH>
+static cudaError_t launch_mr_xinv_t(int M, const float2* S, int hp, int L1, const EpiArgs& A, cudaStream_t st,
+                                    int* nblocks, int nsim) {
+    MrLine f;
+    const float2 *twM = nullptr, *tw2M = nullptr;
+    if (!mr_factor(M, &f) || !mr_tables(M, &twM, nullptr) || !mr_tables(2 * M, &tw2M, nullptr))
+        return cudaErrorInvalidValue;
+    int rpb, nt;
+    mr_xinv_shape(M, &rpb, &nt);
+    const size_t smem = (size_t)rpb * 6 * M * sizeof(float2);
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(mr_xinv_epi_kernel<TERMS, BATCH>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    const int nrows = A.P.n[0] * A.P.n[1];
+    const int blocks = (nrows + rpb - 1) / rpb;
+    *nblocks = blocks;
+    mr_xinv_epi_kernel<TERMS, BATCH><<<dim3((unsigned)blocks, (unsigned)nsim), 3 * rpb * nt, smem, st>>>(
+        S, hp, L1, f, twM, tw2M, A, rpb);
+    return cudaGetLastError();
+}
+
 template <int M>
 static int xinv4_rows(int tile) {
     return tile < 0 ? xinv4_rows_c<M, true>() : xinv4_rows_c<M, false>();
@@ -1206,13 +1284,18 @@ static cudaError_t launch_xinv4_t(const float2* S, int hp, int L1, const float2*
     return launch_xinv4_f<M, TERMS, BATCH, false>(S, hp, L1, tw, A, st, nblocks, nsim, tile);
 }
 
-static bool use_xinv4(int M) { return M >= 4 && M <= 1024; }
+static bool use_xinv4(int M) { return M >= 4 && M <= 1024 && mr_pow2(M); }
 
 // The four-step epilogue (and the four-step row pass whose output it reproduces) serve
 // these row lengths.
 bool epi_r2c_supported(int M) { return use_xinv4(M); }
 
 int xinv_blocks(int M, int n0n1) {
+    if (!mr_pow2(M)) {
+        int rpb, nt;
+        mr_xinv_shape(M, &rpb, &nt);
+        return (n0n1 + rpb - 1) / rpb;
+    }
     if (use_xinv4(M)) {
         int rpb = 1;
         switch (M) {
@@ -1247,6 +1330,13 @@ cudaError_t launch_xinv_epi(int M, const float2* S, int hp, int L1, const float2
             X(4) X(8) X(16) X(32) X(64) X(128) X(256) X(512) X(1024)
 #undef X
         }
+    }
+    if (!mr_pow2(M)) {  // not a power of two: the mixed-radix pass
+        if (staged)
+            return terms ? launch_mr_xinv_t<true, true>(M, S, hp, L1, A, st, nblocks, nsim)
+                         : launch_mr_xinv_t<false, true>(M, S, hp, L1, A, st, nblocks, nsim);
+        return terms ? launch_mr_xinv_t<true, false>(M, S, hp, L1, A, st, nblocks, 1)
+                     : launch_mr_xinv_t<false, false>(M, S, hp, L1, A, st, nblocks, 1);
     }
     if (staged) return cudaErrorNotSupported;  // batched plans and time tables use the four-step pass
     switch (M) {

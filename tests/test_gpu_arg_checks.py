@@ -58,3 +58,14 @@ def test_batch_restart_sizes_are_checked():
         p.batch_run_until_maxtorque(np.ones(p.nsim + 1))
     p.batch_restart([0, 1], np.stack([cold, cold]), thr)   # the right sizes still work
     p.close()
+
+
+def test_transform_sizes_with_large_prime_factors_are_refused():
+    """Padded sizes whose prime factors are at most 31 are transformed (mixed radix);
+    others (here L1 = 2 x 37) are refused with a message naming the size."""
+    from mumax2 import Plan
+    from mumax2 import _native as nat
+    with pytest.raises(nat.MMError) as ei:
+        Plan(dict(n=(1, 37, 8), cell=(3e-9, 3e-9, 3e-9), demag=1, msat=8e5))
+    assert "74" in str(ei.value)
+    Plan(dict(n=(1, 31, 8), cell=(3e-9, 3e-9, 3e-9), demag=1, msat=8e5)).close()   # 62 = 2 x 31 is served

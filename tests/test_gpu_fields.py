@@ -31,6 +31,13 @@ def _pair(problem, masks_host=None):
     ((4, 8, 16), (2e-9, 4e-9, 4e-9)),        # 3-D, 6 components
     ((2, 4, 4), (4e-9, 4e-9, 3e-9)),         # tiny 3-D
     ((8, 16, 8), (3e-9, 3e-9, 3e-9)),
+    # padded sizes that are not powers of two (mixed-radix passes): 2^n * {3, 5, 7}
+    ((1, 24, 40), (3e-9, 4e-9, 5e-9)),       # L = 1 x 48 x 80
+    ((3, 20, 28), (2e-9, 4e-9, 4e-9)),       # L = 6 x 40 x 56: every axis mixed
+    ((1, 15, 21), (3e-9, 4e-9, 4e-9)),       # L = 1 x 30 x 42, odd row length 21
+    ((5, 16, 32), (2e-9, 4e-9, 4e-9)),       # mixed z (L0 = 10) with power-of-two y, x
+    ((2, 12, 64), (2e-9, 4e-9, 4e-9)),       # mixed y (L1 = 24) only
+    ((1, 11, 26), (3e-9, 4e-9, 4e-9)),       # prime factors 11 and 13 (direct-DFT stages)
 ])
 def test_demag_field(n, cell):
     o, g = _pair(dict(n=n, cell=cell, demag=1, exchange=0, msat=8e5))
@@ -163,7 +170,8 @@ def test_stt_with_masks():
 
 
 @pytest.mark.parametrize("n,pbc", [((1, 16, 32), (0, 0, 1)), ((1, 16, 32), (0, 1, 0)), ((1, 8, 16), (0, 1, 1)),
-                                   ((4, 8, 16), (1, 0, 0)), ((2, 8, 8), (0, 1, 1))])
+                                   ((4, 8, 16), (1, 0, 0)), ((2, 8, 8), (0, 1, 1)),
+                                   ((1, 12, 36), (0, 1, 1)), ((6, 10, 24), (1, 0, 0)), ((1, 20, 24), (0, 0, 1))])
 def test_demag_periodic(n, pbc):
     """Periodic dimensions are not padded (zeropad.go:12-22) and the tensor sums the
     periodic images (kernel_magnetostatic.go:55-65)."""
@@ -269,3 +277,25 @@ def test_newell_minus_arne_per_configuration():
         d = rel_err(hn, ha)
         print(f"Newell - Kernel_Arne, {nm}: max |dH| / max |H| = {d:.3e}")
         assert d < 5e-3
+
+
+def test_mixed_radix_batch_equals_single_plans():
+    """A batched plan of two simulations on a grid with non-power-of-two padded sizes
+    (3-D, 3 x 20 x 28 cells) gives each simulation the torque its own plan gives."""
+    from mumax2 import Plan
+    n = (3, 20, 28)
+    prob = dict(n=n, cell=(2e-9, 4e-9, 4e-9), demag=1, exchange=1, anis=1, zeeman=1, msat=8e5, aex=1.3e-11,
+                ku=2e5, anisu=(0.0, 0.6, 0.8), alpha=0.05, bext=(0.0, 0.01, 0.02))
+    sims = [dict(msat=8e5, aex=1.3e-11, alpha=0.05, bext=(0.0, 0.01, 0.02), ku=2e5, anisu=(0.0, 0.6, 0.8)),
+            dict(msat=6e5, aex=1.0e-11, alpha=0.1, bext=(0.02, 0.0, 0.0), ku=1e5, anisu=(1.0, 0.0, 0.0))]
+    N = n[0] * n[1] * n[2]
+    m = np.concatenate([rand_m(n, seed=40), rand_m(n, seed=41)])
+    gb = Plan(prob, sims=sims)
+    tb = to_np(gb.torque(m)[0])
+    for b, sm in enumerate(sims):
+        q = dict(prob)
+        q.update(sm)
+        ts = to_np(Plan(q).torque(m[3 * N * b:3 * N * (b + 1)])[0])
+        err = rel_err(tb[3 * N * b:3 * N * (b + 1)], ts)
+        print("mixed-radix batch vs single", b, err)
+        assert err < 1e-6

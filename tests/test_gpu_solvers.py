@@ -154,3 +154,24 @@ def test_sp4_against_golden_trace():
     print("sp4 max/rms per component", errs)
     for mx, rms in errs:
         assert mx < 0.05 and rms < 0.025
+
+
+def test_rk23_trajectory_on_mixed_radix_grid():
+    """RK23 on a film whose padded sizes are not powers of two (24 x 40 cells, padded
+    48 x 80): the same accepted and rejected steps as the oracle, m within 2e-4."""
+    import oracle as O
+    prob = dict(FILM)
+    prob["n"] = (1, 24, 40)
+    o, g = _pair(prob)
+    m0 = rand_m(prob["n"], seed=14, kind="near_x")
+    r = O.OracleRun(o, m0, solver="rk23", dt=1e-15, mindt=1e-18, maxerr=1e-5)
+    for _ in range(20):
+        r.step()
+    g.solver("rk23", dt=1e-15, mindt=1e-18, maxerr=1e-5)
+    g.set_state(m0)
+    g.steps(20)
+    st = g.stats()
+    err = np.abs(g.get_state().astype(np.float64) - o.normalize(r.m.copy())).max()
+    print("mixed-radix rk23: gpu", st["step"], st["badsteps"], "oracle", r.st.step, r.st.badsteps, "max|dm|", err)
+    assert st["status"] == 0 and st["step"] == r.st.step and st["badsteps"] == r.st.badsteps
+    assert err < 2e-4
