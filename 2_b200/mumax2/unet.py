@@ -80,6 +80,11 @@ def init_params(seed=0):
     return params
 
 
+# feature channels that carry the y components of the anisotropy axis and the field
+FEAT_AXIS_Y = 5
+FEAT_B_Y = 7
+
+
 def features(sims, masks, n):
     """Input features [nsim][H*W][FEAT] (float32) of relaxation problems (workloads.relax_set)."""
     ny, nx = n[1], n[2]

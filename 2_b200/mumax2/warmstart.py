@@ -33,7 +33,7 @@ def _tail_plan(plan, problem, masks0, sims0, slots, device, maxerr):
 
 def relax_pool(problem, sims, masks, states, thr, slots=256, maxerr=1e-6, max_steps=100000, device=0,
                keep_states=False, plan=None, accept=None, fallback=None, fallback_max_steps=100000,
-               tail_slots=16, want_energy=True, spec_steps=0):
+               tail_slots=16, want_energy=True, spec_steps=0, order=None, masks_dev=None):
     """Relaxes problem q from states[q] until maxtorque < thr[q].  states: a list of host
     arrays or a float32 device tensor [nq][3N].  Returns a dict of arrays: steps,
     maxtorque, energy (J; zeros without want_energy, which accept needs) and, with
@@ -55,7 +55,11 @@ def relax_pool(problem, sims, masks, states, thr, slots=256, maxerr=1e-6, max_st
     move (state, scalars, mask and steps so far) to a plan of tail_slots simulations,
     whose launches carry that many simulations' blocks instead of the pool's (a step of
     the 256-slot pool costs about the same with one slot active as with all).  The moved
-    relaxations restart their step-size control from dt = 1e-14 s."""
+    relaxations restart their step-size control from dt = 1e-14 s.
+
+    order (optional): the problems in the order the pool starts them (default 0..nq-1);
+    starting the longest relaxations first keeps them from forming the pool's end.
+    masks_dev (optional): the problems' masks already on the device ([nq][N] float32)."""
     import collections
     import torch
     from .plan import Plan
@@ -70,7 +74,7 @@ def relax_pool(problem, sims, masks, states, thr, slots=256, maxerr=1e-6, max_st
     plan.solver("rk23", dt=1e-14, maxerr=maxerr)
     on_dev = hasattr(states, "data_ptr")
     speculate = bool(spec_steps) and accept is not None and fallback is not None
-    queue = collections.deque((q, False) for q in range(nq))
+    queue = collections.deque((int(q), False) for q in (range(nq) if order is None else order))
     res = {"steps": np.zeros(nq, dtype=np.int64), "maxtorque": np.zeros(nq), "energy": np.zeros(nq)}
     if accept is not None:
         res.update({"first_steps": np.zeros(nq, dtype=np.int64), "first_maxtorque": np.zeros(nq),
@@ -93,6 +97,13 @@ def relax_pool(problem, sims, masks, states, thr, slots=256, maxerr=1e-6, max_st
         """One host-to-device copy of a stack of host arrays (states or masks)."""
         return torch.from_numpy(np.ascontiguousarray(a, dtype=np.float32)).to(dev)
 
+    def pick_masks(qs):
+        """The masks of problems qs on the device: gathered from masks_dev when the caller
+        keeps them there, else uploaded in one copy."""
+        if masks_dev is not None:
+            return masks_dev[torch.tensor(qs, device=masks_dev.device)]
+        return to_dev(np.stack([np.asarray(masks[q], dtype=np.float32) for q in qs]))
+
     def restart(idx, m0, jobs, limits):
         if not hasattr(m0, "data_ptr"):
             m0 = to_dev(m0)
@@ -101,7 +112,7 @@ def relax_pool(problem, sims, masks, states, thr, slots=256, maxerr=1e-6, max_st
     def place(bs, qs, is_fb):
         """Slots bs take problems qs: their masks in one copy, and the slot records."""
         mt = cur.mask_tensor("msat").view(-1, N)
-        mt[torch.tensor(bs, device=dev)] = to_dev(np.stack([np.asarray(masks[q], dtype=np.float32) for q in qs]))
+        mt[torch.tensor(bs, device=dev)] = pick_masks(qs)
         for b, q, f in zip(bs, qs, is_fb):
             slot[b], retry[b], offset[b] = q, f, 0
 
@@ -138,7 +149,7 @@ def relax_pool(problem, sims, masks, states, thr, slots=256, maxerr=1e-6, max_st
         tail = _tail_plan(plan, problem, masks[0], sims[0], tail_slots, device, maxerr)
         mt = tail.mask_tensor("msat").view(-1, N)
         if run:
-            mt[:len(run)] = to_dev(np.stack([np.asarray(masks[slot[b]], dtype=np.float32) for b in run]))
+            mt[:len(run)] = pick_masks([slot[b] for b in run])
         new_slot, new_retry, new_off = [-1] * tail_slots, [False] * tail_slots, [0] * tail_slots
         m0, js, limits = [], [], []
         for i, b in enumerate(run):
@@ -281,9 +292,19 @@ def thresholds(sims, gamma=2.211e5, rel=1e-4):
 
 
 class Dataset:
-    """Features, targets and masks of relaxed problems, resident on the GPU."""
+    """Features, targets and masks of relaxed problems, resident on the GPU.
 
-    def __init__(self, problem, sims, masks, states, device=0):
+    mirror=True adds, for every relaxed problem, its mirror image x -> -x: mask and
+    fields reflected along x, the in-plane field and anisotropy axis (Bx, By) -> (Bx, -By),
+    (ux, uy) -> (ux, -uy), and the relaxed state m -> (mx, -my, -mz) at the mirrored cell.
+    Magnetisation and field are axial vectors, so a mirror R acts on them as -det(R) R =
+    diag(1, -1, -1) here; the LLG equation, every energy term, the grid and the cold start
+    (uniform +x) are invariant under this map, so the mirrored state is exactly what the
+    plain relaxer gives for the mirrored problem.  (The other flips and rotations of the
+    square map the +x cold start to another direction and are not used: where a problem
+    has several minima, the relaxer's choice depends on the start.)"""
+
+    def __init__(self, problem, sims, masks, states, device=0, mirror=False):
         import torch
         n = problem["n"]
         self.n = n
@@ -294,6 +315,20 @@ class Dataset:
         mk = np.stack([np.asarray(m, dtype=np.float32) for m in masks])
         self.masks = torch.tensor(mk, device=dev)
         self.mask_counts = mk.sum(axis=1).astype(np.float64)   # host copy: no device read per batch
+        if mirror:
+            ny, nx = n[1], n[2]
+            f = torch.flip(self.feats.view(-1, ny, nx, self.feats.shape[-1]), dims=[2]).reshape(self.feats.shape)
+            f = f.clone()
+            f[:, :, U.FEAT_AXIS_Y] *= -1.0   # (ux, uy) -> (ux, -uy)
+            f[:, :, U.FEAT_B_Y] *= -1.0      # (Bx, By) -> (Bx, -By)
+            t = torch.flip(self.targets.view(-1, ny, nx, 3), dims=[2]).reshape(self.targets.shape).clone()
+            t[:, :, 1] *= -1.0
+            t[:, :, 2] *= -1.0
+            m2 = torch.flip(self.masks.view(-1, ny, nx), dims=[2]).reshape(self.masks.shape)
+            self.feats = torch.cat([self.feats, f])
+            self.targets = torch.cat([self.targets, t])
+            self.masks = torch.cat([self.masks, m2])
+            self.mask_counts = np.concatenate([self.mask_counts, self.mask_counts])
 
     def __len__(self):
         return self.feats.shape[0]
@@ -365,7 +400,8 @@ def predict(net, sims, masks, n, host=False):
     return out.cpu().numpy() if host else out
 
 
-def evaluate(net, problem, sims, masks, slots=256, device=0, energy_tol=1e-4, max_steps=20000, spec_frac=0.5):
+def evaluate(net, problem, sims, masks, slots=256, device=0, energy_tol=1e-4, max_steps=20000, spec_frac=0.5,
+             longest_first=True):
     """Cold and warm relaxations of the same problems (times include the network's
     inference for the warm start).  A warm relax that does not reach the threshold within
     max_steps (its step budget; step_budget() derives one from the training relaxations),
@@ -375,7 +411,8 @@ def evaluate(net, problem, sims, masks, slots=256, device=0, energy_tol=1e-4, ma
     spec_steps; 0 queues redos only once their warm relax is rejected).  Measured on 4096
     held-out problems: 0.05, 0.1, 0.25 and 0.5 of the budget gave 0.96, 1.09, 1.16 and
     1.18 times the cold rate (early redos take slots from the queue and are mostly
-    cancelled)."""
+    cancelled).  longest_first: the warm pool starts its problems in decreasing order of the
+    maxtorque / (gamma Ms) of their predicted start (computed in the timed region)."""
     import torch
     from .plan import Plan
     n = problem["n"]
@@ -386,9 +423,16 @@ def evaluate(net, problem, sims, masks, slots=256, device=0, energy_tol=1e-4, ma
                 device=device)
     if B > 16:   # the drain plan of both pools, made outside the timed regions
         _tail_plan(plan, problem, masks[0], sims[0], 16, device, 1e-6)
+    # the problems' masks resident on the device for both pools (input data)
+    masks_dev = torch.from_numpy(np.stack([np.asarray(m, dtype=np.float32) for m in masks])).to(
+        plan.mask_tensor("msat").device)
+    sims_arr = nat.make_sims(problem, sims)
+    if longest_first:   # loads the tensor kernels of the ordering pass outside the timed regions
+        initial_torques(plan, problem, sims[:1], masks[:1], None, masks_dev[:1])
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    rc = relax_pool(problem, sims, masks, [cold] * len(sims), thr, slots=slots, device=device, plan=plan)
+    rc = relax_pool(problem, sims, masks, [cold] * len(sims), thr, slots=slots, device=device, plan=plan,
+                    masks_dev=masks_dev)
     torch.cuda.synchronize()
     t_cold = time.perf_counter() - t0
 
@@ -399,17 +443,33 @@ def evaluate(net, problem, sims, masks, slots=256, device=0, energy_tol=1e-4, ma
 
     t0 = time.perf_counter()
     init = predict(net, sims, masks, n)
+    t0_warm = None
+    order = None
+    if longest_first:
+        # the warm relaxations' lengths grow with the maxtorque of their start (about 130
+        # steps per decade): start the problems in decreasing order of it
+        t0_warm = initial_torques(plan, problem, sims, masks, init, masks_dev, sims_arr)
+        order = np.argsort(-t0_warm, kind="stable")
     torch.cuda.synchronize()
     t_inf = time.perf_counter() - t0
     rw = relax_pool(problem, sims, masks, init, thr, slots=slots, device=device, max_steps=max_steps, plan=plan,
-                    accept=accept, fallback=cold, spec_steps=int(spec_frac * max_steps))
+                    accept=accept, fallback=cold, spec_steps=int(spec_frac * max_steps), order=order,
+                    masks_dev=masks_dev)
     torch.cuda.synchronize()
     t_warm = time.perf_counter() - t0
+    # outside the timed regions: the maxtorque / (gamma Ms) of each start (cold and
+    # predicted), one batched torque evaluation per slot group, against the steps taken
+    if t0_warm is None:
+        t0_warm = initial_torques(plan, problem, sims, masks, init, masks_dev, sims_arr)
+    t0_cold = initial_torques(plan, problem, sims, masks, None, masks_dev, sims_arr)
     t = getattr(plan, "_tail_plan", None)
     if t is not None:
         t.close()
     plan.close()
     fb = rw["fell_back"]
+    ok = ~fb
+    lt = np.log10(np.maximum(t0_warm[ok], 1e-30))
+    slope, icpt = np.polyfit(lt, rw["first_steps"][ok], 1) if ok.sum() > 2 else (float("nan"), float("nan"))
     erel = np.abs(rw["first_energy"] - rc["energy"]) / np.maximum(np.abs(rc["energy"]), 1e-30)
     return {
         "relaxations": len(sims),
@@ -419,6 +479,7 @@ def evaluate(net, problem, sims, masks, slots=256, device=0, energy_tol=1e-4, ma
         "steps_saved_frac": float(1 - rw["first_steps"].sum() / max(1, rc["steps"].sum())),
         "warm_steps_incl_fallbacks_mean": float((rw["first_steps"] + np.where(fb, rw["steps"], 0)).mean()),
         "inference_s": t_inf, "warm_relax_only_per_s": len(sims) / (t_warm - t_inf),
+        "warm_order": "decreasing initial maxtorque" if longest_first else "index",
         "cold_drive_s": rc["drive_s"], "cold_host_s": rc["host_s"], "warm_drive_s": rw["drive_s"],
         "warm_host_s": rw["host_s"],
         "cold_steps_max": int(rc["steps"].max()), "warm_steps_max": int(rw["first_steps"].max()),
@@ -429,4 +490,54 @@ def evaluate(net, problem, sims, masks, slots=256, device=0, energy_tol=1e-4, ma
         "energy_within_tol_frac": float((erel <= energy_tol).mean()),
         "energy_rel_median": float(np.median(erel)),
         "warm_lower_energy_frac": float((rw["first_energy"] < rc["energy"]).mean()),
+        "initial_torque_cold_median": float(np.median(t0_cold)),
+        "initial_torque_warm_median": float(np.median(t0_warm)),
+        "initial_torque_warm_p90": float(np.percentile(t0_warm, 90)),
+        "warm_steps_vs_log10_initial_torque": {"slope": float(slope), "intercept": float(icpt),
+                                               "fit_on": int(ok.sum())},
     }
+
+
+def initial_torques(plan, problem, sims, masks, states, masks_dev=None, sims_arr=None):
+    """maxtorque / (gamma Ms) of start states (a float32 device tensor [nq][3N], or the cold
+    start when None), computed through the batched plan's torque, plan.nsim problems at a
+    time (the plan's slots take their masks and scalars); one host read at the end.
+    masks_dev: the problems' masks already on the device ([nq][N] float32), else they are
+    uploaded here; sims_arr: their scalars as an mm_sim array (_native.make_sims)."""
+    import ctypes as C
+
+    import torch
+    n = problem["n"]
+    N = int(np.prod(n))
+    B = plan.nsim
+    nq = len(sims)
+    mt = plan.mask_tensor("msat").view(-1, N)
+    dev = mt.device
+    if masks_dev is None:
+        masks_dev = torch.from_numpy(np.stack([np.asarray(m, dtype=np.float32) for m in masks])).to(dev)
+    if sims_arr is None:
+        sims_arr = nat.make_sims(problem, sims)
+    pad = nat.make_sims(problem, [sims[-1]] * B)   # fills the slots past the last problem
+    cold = torch.tensor(W.cold_state(n, B), device=dev).view(-1) if states is None else None
+    ms_all = torch.tensor([s["msat"] for s in sims], dtype=torch.float32, device=dev)
+    out = torch.zeros(nq, dtype=torch.float32, device=dev)
+    mbuf = torch.empty(3 * N * B, dtype=torch.float32, device=dev)
+    tq = torch.empty(3 * N * B, dtype=torch.float32, device=dev)
+    L = nat.lib()
+    ptr = lambda t: C.c_void_p(t.data_ptr())
+    size = C.sizeof(nat.MMSim)
+    for i in range(0, nq, B):
+        k = min(B, nq - i)
+        idx = torch.arange(i, i + B, device=dev).clamp(max=nq - 1)
+        mt.copy_(masks_dev[idx])
+        if k == B:
+            nat.check(L.mm_batch_set_sims(plan.h, C.c_void_p(C.addressof(sims_arr) + i * size)))
+        else:
+            C.memmove(pad, C.addressof(sims_arr) + i * size, k * size)
+            nat.check(L.mm_batch_set_sims(plan.h, C.cast(pad, C.c_void_p)))
+        mbuf.copy_(cold if states is None else states[idx].reshape(-1))
+        nat.check(L.mm_torque(plan.h, ptr(mbuf), 0, 0.0, ptr(tq), None))
+        t3 = tq.view(B, 3, N)
+        mx = torch.sqrt((t3 * t3).sum(dim=1)).max(dim=1).values
+        out[i:i + k] = (mx / ms_all[idx])[:k]
+    return out.cpu().numpy().astype(np.float64)

@@ -644,7 +644,7 @@ def warmstart_bench(args, rank, world, local_rank, dist, emit=True):
     t0 = time.perf_counter()
     problem, sims, masks, res = WS.generate(args.train, seed=1000 + rank, device=local_rank)
     t_gen = time.perf_counter() - t0
-    data = WS.Dataset(problem, sims, masks, res["state"], device=local_rank)
+    data = WS.Dataset(problem, sims, masks, res["state"], device=local_rank, mirror=not args.no_mirror)
     t0 = time.perf_counter()
     net, losses = WS.train(data, epochs=args.epochs, batch=256, lr=2e-3, device=local_rank,
                            tcgen05=not args.mma_sync)
@@ -655,7 +655,8 @@ def warmstart_bench(args, rank, world, local_rank, dist, emit=True):
     _, hs, hm = W.relax_set(args.nsim, seed=5000 + rank)
     sampler = ClockSampler(local_rank)
     sampler.start()
-    ev = WS.evaluate(net, problem, hs, hm, device=local_rank, max_steps=WS.step_budget(res["steps"]))
+    ev = WS.evaluate(net, problem, hs, hm, device=local_rank, max_steps=WS.step_budget(res["steps"]),
+                     longest_first=not args.warm_index_order)
     clocks = sampler.stop()
     peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     peak = float(json.load(open(peaks_path))["bf16_tflops_sustained"]) if os.path.exists(peaks_path) else 1400.0
@@ -666,6 +667,8 @@ def warmstart_bench(args, rank, world, local_rank, dist, emit=True):
                 "data": "synthetic",
                 "config": {"workload": "relax_64x64x1_warm_start", "held_out": args.nsim, "train": args.train,
                            "epochs": args.epochs, "net": "U-Net 4 levels, 32/64/128/256 channels, 3x3, bf16",
+                           "training_set": "relaxed states" + ("" if args.no_mirror else
+                                                               " and their x-mirror images"),
                            "conv": "mma.sync" if args.mma_sync else "tcgen05",
                            "parallelism": f"replicas{world}"},
                 "warm_vs_cold": ev,
@@ -689,7 +692,7 @@ def extra_workloads(args, rank, world, local_rank, dist):
     import copy
     out = {}
     a = copy.copy(args)
-    a.nsim, a.train, a.epochs, a.mma_sync = 4096, args.train, args.epochs, False
+    a.nsim, a.mma_sync = 4096, False
     t0 = time.perf_counter()
     try:
         ws = warmstart_bench(a, rank, world, local_rank, dist, emit=False)
@@ -742,7 +745,11 @@ def main():
                          "relax: batched cold relaxations of 64x64x1 films; sp4: the 128x32x1 RK45 film; "
                          "wall: Zhang-Li domain wall and Slonczewski disk; warmstart: the learned warm start")
     ap.add_argument("--train", type=int, default=20000, help="warmstart: training relaxations")
-    ap.add_argument("--epochs", type=int, default=20, help="warmstart: training epochs")
+    ap.add_argument("--epochs", type=int, default=40, help="warmstart: training epochs")
+    ap.add_argument("--warm-index-order", action="store_true",
+                    help="warmstart: start the warm relaxations in index order (not longest first)")
+    ap.add_argument("--no-mirror", action="store_true",
+                    help="warmstart: train without the mirror-image copies of the relaxed problems")
     ap.add_argument("--mma-sync", action="store_true",
                     help="warmstart: forward and data-gradient convolutions on the mma.sync kernel")
     ap.add_argument("--duration", type=float, default=0.0, help="sp4/wall: simulated time (s)")

@@ -72,3 +72,36 @@ def test_speculative_redo_gives_the_same_results():
     assert (d["maxtorque"] < thr).all() and np.array_equal(c["fell_back"], d["fell_back"])
     erel = np.abs(d["energy"] - a["energy"]) / np.abs(a["energy"])
     assert erel.max() < 1e-4
+
+
+def test_mirror_x_is_a_symmetry_of_the_plain_relax():
+    """The training set's mirror augmentation: reflecting a problem along x (mask and
+    fields, B_y -> -B_y, u_y -> -u_y) and relaxing it from the same cold start (+x) gives
+    the mirror image of the original relaxed state with m -> (m_x, -m_y, -m_z), the
+    energy unchanged."""
+    from mumax2 import warmstart as WS
+    from mumax2 import workloads as W
+    problem, sims, masks = W.relax_set(16, seed=5)
+    n = problem["n"]
+    ny, nx = n[1], n[2]
+    N = ny * nx
+    msims = []
+    for s in sims:
+        q = dict(s)
+        q["anisu"] = (s["anisu"][0], -s["anisu"][1], s["anisu"][2])   # internal (z, y, x)
+        q["bext"] = (s["bext"][0], -s["bext"][1], s["bext"][2])
+        msims.append(q)
+    mmasks = [np.asarray(m).reshape(ny, nx)[:, ::-1].ravel().copy() for m in masks]
+    thr = WS.thresholds(sims)
+    cold = W.cold_state(n, 1)
+    a = WS.relax_pool(problem, sims, masks, [cold] * 16, thr, slots=16, keep_states=True)
+    b = WS.relax_pool(problem, msims, mmasks, [cold] * 16, thr, slots=16, keep_states=True)
+    assert (a["maxtorque"] < thr).all() and (b["maxtorque"] < thr).all()
+    sa = a["state"].reshape(16, 3, ny, nx)
+    sb = b["state"].reshape(16, 3, ny, nx)
+    want = sa[:, :, :, ::-1] * np.array([-1.0, -1.0, 1.0])[None, :, None, None]   # internal (z, y, x) comps
+    dm = np.abs(sb - want).max(axis=(1, 2, 3))
+    erel = np.abs(a["energy"] - b["energy"]) / np.abs(a["energy"])
+    print("mirror: max |dm| per problem", dm, "energy", erel.max(), "steps", a["steps"], b["steps"])
+    assert erel.max() < 1e-4
+    assert np.median(dm) < 1e-2
