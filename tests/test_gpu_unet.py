@@ -272,3 +272,45 @@ def test_relu_bias_bwd_matches(C, P, relu):
     ref = np.where(out > 0, d, 0.0) if relu else d
     assert np.array_equal(dd.float().cpu().numpy().reshape(P, C), ref)
     assert _relnorm(db.cpu().numpy(), ref.sum(axis=0)) < 1e-5
+
+
+@pytest.mark.parametrize("kernel", ["tcgen05", "mma.sync"])
+@pytest.mark.parametrize("cin,cout,B,H,W", [(384, 128, 4, 16, 16), (32, 32, 3, 64, 64), (96, 32, 2, 8, 16),
+                                            (16, 16, 3, 5, 7)])
+def test_convolution_writes_only_its_output(kernel, cin, cout, B, H, W):
+    """Output canary: the convolution writes a channel slice (offset 16, Cout channels) of a
+    wider pixel-major buffer that sits between two guard regions.  Every element outside
+    the slice -- the other channels of each pixel and both guards -- must keep its canary
+    value, and the slice must match the oracle."""
+    import torch
+    import unet_ref as R
+    from mumax2 import _native as nat
+    rng = np.random.default_rng(cin + 3 * cout + B)
+    x = R.bf16(rng.normal(size=(B, H, W, cin)))
+    w = R.bf16(rng.normal(size=(cout, 9, cin)) / np.sqrt(9 * cin))
+    b = rng.normal(size=cout).astype(np.float32)
+    xd, wd = _dev(x, torch.bfloat16), _dev(w, torch.bfloat16)
+    bd = torch.tensor(b, device="cuda")
+    P = B * H * W
+    cs, co, guard = cout + 48, 16, 1 << 16            # row stride, channel offset, guard elements
+    canary = 0x7F7B                                   # a bf16 NaN payload no kernel computes
+    buf = torch.full((2 * guard + P * cs,), canary, dtype=torch.int16, device="cuda")
+    out = buf[guard:guard + P * cs]
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    L = nat.lib()
+    if kernel == "tcgen05":
+        nat.check(L.mm_nn_conv3x3_tc(_p(xd), cin, 0, cin, _p(wd), _p(bd), _p(out), cs, co, cout, B, H, W, 1,
+                                     _p(err), None))
+    else:
+        nat.check(L.mm_nn_conv3x3(_p(xd), cin, 0, cin, _p(wd), _p(bd), _p(out), cs, co, cout, B, H, W, 1, None))
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    h = buf.cpu().numpy()
+    assert (h[:guard] == canary).all() and (h[guard + P * cs:] == canary).all(), "store outside the buffer"
+    body = h[guard:guard + P * cs].reshape(P, cs)
+    outside = np.ones(cs, dtype=bool)
+    outside[co:co + cout] = False
+    assert (body[:, outside] == canary).all(), "store into a channel outside the slice"
+    got = torch.from_numpy(body[:, co:co + cout].copy()).view(torch.bfloat16).float().numpy()
+    ref = np.maximum(R.conv3x3(x, w, b), 0).reshape(P, cout)
+    assert np.abs(got - ref).max() <= 2 ** -7 * np.abs(ref).max() + 1e-6
