@@ -15,6 +15,8 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <string>
 #include <thread>
 #include <vector>
@@ -1019,12 +1021,83 @@ static StageOp op_blank() {
 // try the fused evaluation (fused2d_kernel: convolution and epilogue in one launch).
 // Runs once at plan creation; MM_AUTOTUNE=0 in the environment keeps the defaults.  Tile variants change the block decomposition only: every cell's
 // arithmetic is the same, and so are the fields, torques and step sequences.
+// Tuning results are kept per device and plan shape for the life of the process, so
+// that plans of a shape tuned before (the slots of a relaxation pool, an engine that
+// rebuilds its plan, the plans of an ensemble's grid classes) take the earlier choice
+// without timing again.  The shape covers everything the passes' launch configuration and
+// work depend on: grid, padded sizes, simulations, which terms and masks are present.
+namespace {
+struct TuneKey {
+    int v[24];
+    bool operator<(const TuneKey& o) const { return std::lexicographical_compare(v, v + 24, o.v, o.v + 24); }
+};
+struct TuneVal {
+    int tiles[4];
+    float us;
+};
+std::mutex g_tune_mu;
+std::map<TuneKey, TuneVal> g_tune;
+long long g_tune_runs = 0;
+}  // namespace
+
+static TuneKey tune_key(mm_plan p) {
+    TuneKey k;
+    memset(k.v, 0, sizeof k.v);
+    const FieldParams& P = p->P;
+    int i = 0;
+    k.v[i++] = p->device;
+    for (int d = 0; d < 3; d++) { k.v[i++] = p->g.n[d]; k.v[i++] = p->g.L[d]; }
+    k.v[i++] = p->nsim;
+    k.v[i++] = p->masks_per_sim;
+    k.v[i++] = p->khat_d ? 1 : 0;
+    k.v[i++] = P.exchange | P.anis << 1 | P.zeeman << 2 | P.thermal << 3 | P.zhangli << 4 | P.slonczewski << 5;
+    const void* masks[] = {P.msat_mask, P.aex_mask, P.alpha_mask, P.ku_mask, P.anisu_mask[0], P.bext_mask[0],
+                           P.j_mask[0], P.temp_mask, P.xi_mask, P.zl_pol_mask, P.p_mask[0], P.sl_pol_mask,
+                           P.lambda_mask, P.eps_prime_mask, P.t_fl_mask};
+    int bits = 0;
+    for (int q = 0; q < 15; q++) bits |= (masks[q] ? 1 : 0) << q;
+    k.v[i++] = bits;
+    k.v[i++] = (P.tab[0].n ? 1 : 0) | (P.tab[1].n ? 2 : 0);
+    k.v[i++] = p->pdl ? 1 : 0;
+    return k;
+}
+
+extern "C" MM_API long long mm_autotune_runs(void) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    return g_tune_runs;
+}
+
+static int autotune_run(mm_plan p);
+
 static int autotune(mm_plan p) {
     if (!p->demag) return MM_OK;
     // the tiles are those of the power-of-two passes
     if (!pow2(p->g.L[0]) || !pow2(p->g.L[1]) || !pow2(p->g.L[2])) return MM_OK;
     const char* env = getenv("MM_AUTOTUNE");
     if (env && env[0] == '0') return MM_OK;
+    const TuneKey key = tune_key(p);
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = g_tune.find(key);
+        if (it != g_tune.end()) {
+            for (int d = 0; d < 4; d++) p->tiles[d] = it->second.tiles[d];
+            p->tuned_us = it->second.us;
+            return MM_OK;
+        }
+    }
+    const int rc = autotune_run(p);
+    if (rc == MM_OK && p->tuned_us > 0.f) {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        TuneVal v;
+        for (int d = 0; d < 4; d++) v.tiles[d] = p->tiles[d];
+        v.us = p->tuned_us;
+        g_tune[key] = v;
+        g_tune_runs++;
+    }
+    return rc;
+}
+
+static int autotune_run(mm_plan p) {
     cudaStream_t st = nullptr;
     const long long launches = p->launches;
     CUCHK(cudaMemsetAsync(p->Y[0], 0, sizeof(float) * (size_t)p->n3() * p->nsim, st));

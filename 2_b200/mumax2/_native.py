@@ -213,6 +213,7 @@ _PROTOS = {
     "mm_demag_tensor": (C.c_int, [C.c_int * 3, C.c_double * 3, C.c_int * 3, C.c_int, C.c_int, C.c_void_p,
                                   C.c_void_p]),
     "mm_plan_tiles": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "mm_autotune_runs": (C.c_longlong, []),
     "mm_plan_set_tiles": (C.c_int, [C.c_void_p, C.c_void_p]),
     "mm_plan_nsim": (C.c_int, [C.c_void_p]),
     "mm_batch_set_sims": (C.c_int, [C.c_void_p, C.c_void_p]),

@@ -58,6 +58,65 @@ def ensemble(nsim=2048, seed=0):
     return out
 
 
+def partition(weights, world):
+    """Contiguous blocks of items, one per rank, balanced by weight: rank r takes the items
+    whose weight prefix (the sum up to and including the item's midpoint) falls in the r-th
+    of `world` equal parts.  Returns [(start, end)] per rank (end exclusive)."""
+    w = np.asarray(weights, dtype=np.float64)
+    if world <= 1 or len(w) == 0:
+        return [(0, len(w))] + [(len(w), len(w))] * max(0, world - 1)
+    mid = np.cumsum(w) - 0.5 * w
+    owner = np.minimum((mid / w.sum() * world).astype(int), world - 1)
+    out = []
+    for r in range(world):
+        idx = np.nonzero(owner == r)[0]
+        if len(idx):
+            out.append((int(idx[0]), int(idx[-1]) + 1))
+        else:
+            prev = out[-1][1] if out else 0
+            out.append((prev, prev))
+    return out
+
+
+def ensemble_shard(nsim, seed, rank, world):
+    """This rank's share of the ensemble of `nsim` simulations (ensemble(nsim, seed), drawn
+    identically on every rank): a contiguous block of simulation indices balanced by cells
+    per simulation (the byte model of a Heun step is proportional to the cells), the grid
+    classes restricted to it.  Returns (classes, (start, end))."""
+    full = ensemble(nsim, seed=seed)
+    cells = np.zeros(nsim)
+    for c in full:
+        cells[c["ids"]] = float(np.prod(c["n"]))
+    lo, hi = partition(cells, world)[rank]
+    out = []
+    for c in full:
+        keep = [k for k, i in enumerate(c["ids"]) if lo <= i < hi]
+        if not keep:
+            continue
+        d = dict(c)
+        d["ids"] = c["ids"][keep]
+        d["sims"] = [c["sims"][k] for k in keep]
+        d["m0"] = [c["m0"][k] for k in keep]
+        out.append(d)
+    return out, (lo, hi)
+
+
+def gather_per_sim(dist, ids, rows, nsim):
+    """Per-simulation result rows of every rank, gathered to rank 0 in simulation order
+    (one all-gather of a few KB over the process group; None on the other ranks)."""
+    payload = (np.asarray(ids, dtype=np.int64), np.asarray(rows, dtype=np.float64))
+    world = dist.get_world_size()
+    parts = [None] * world
+    dist.all_gather_object(parts, payload)
+    if dist.get_rank() != 0:
+        return None
+    width = payload[1].shape[1] if payload[1].ndim > 1 else 1
+    out = np.full((nsim, width), np.nan)
+    for pid, prow in parts:
+        out[pid] = np.asarray(prow).reshape(len(pid), width)
+    return out
+
+
 def uniform_state(n, direction, count=1):
     """SoA state of `count` simulations, each uniform along its direction."""
     N = int(n[0]) * int(n[1]) * int(n[2])

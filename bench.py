@@ -338,13 +338,19 @@ def ensemble_bench(args, rank, world, local_rank, dist, emit=True):
     all stepped from one CUDA graph (stochastic Heun, fixed 50 fs).  A step advances every
     simulation by one Heun step; value = total cells x steps / device time.  Beside it:
     the same simulations run one at a time (a sample of one per grid size) and their <m>
-    against the batched run."""
+    against the batched run.  With N > 1 ranks the 2048 simulations are split into
+    contiguous cell-balanced blocks, one per rank (strong scaling, no collective while
+    stepping), and the per-simulation <m> are gathered to rank 0 at the end."""
     import ctypes as C
     import torch
     from mumax2 import Ensemble, Plan
     from mumax2 import _native as nat
     from mumax2 import workloads as W
-    classes = W.ensemble(nsim=args.nsim, seed=rank)
+    if world > 1:
+        # the same ensemble on every rank, a contiguous cell-balanced block of it per rank
+        classes, shard = W.ensemble_shard(args.nsim, seed=0, rank=rank, world=world)
+    else:
+        classes, shard = W.ensemble(nsim=args.nsim, seed=0), (0, args.nsim)
     plans, states = [], []
     for c in classes:
         p = Plan(c["problem"], sims=c["sims"], device=local_rank)
@@ -374,6 +380,14 @@ def ensemble_bench(args, rank, world, local_rank, dist, emit=True):
     ms = e0.elapsed_time(e1)
     launches = ens.launch_count() - l0
     ms_max, value = aggregate(ms, cells, args.steps, world, dist, "cuda")
+    total_cells = cells
+    if dist is not None and world > 1:
+        # sharded: the ranks' cells add up to the ensemble's (not world x cells)
+        import torch
+        t = torch.tensor([float(cells)], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t)
+        total_cells = int(t.item())
+        value = total_cells * args.steps / (ms_max / 1e3)
     step_b = 0
     for c, p in zip(classes, plans):
         step_b += step_bytes_heun(p.geometry(), c["n"]) * len(c["sims"])
@@ -403,6 +417,10 @@ def ensemble_bench(args, rank, world, local_rank, dist, emit=True):
     # unbatched comparison: the first simulation of each grid size alone, same inputs
     # and steps (warm-up + timed + end-to-end run), then its <m> against the batch
     avg_b = [p.batch_average() for p in plans]
+    gathered = None
+    if dist is not None and world > 1:   # per-simulation <m> of every rank to rank 0
+        g = W.gather_per_sim(dist, np.concatenate([c["ids"] for c in classes]), np.concatenate(avg_b), args.nsim)
+        gathered = None if g is None else int(np.isfinite(g).all(axis=1).sum())
     uni_cells_steps, uni_ms, dm = 0, 0.0, 0.0
     for c, p, m0, ab in zip(classes, plans, states, avg_b):
         q = dict(c["problem"])
@@ -430,7 +448,8 @@ def ensemble_bench(args, rank, world, local_rank, dist, emit=True):
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic",
-                "config": {"workload": f"thermal_ensemble_{args.nsim}", "simulations": args.nsim, "cells": cells,
+                "config": {"workload": f"thermal_ensemble_{args.nsim}", "simulations": args.nsim,
+                           "cells": total_cells, "shard_of_rank0": list(shard),
                            "grids_xyz": [list(g) for g in W.ENSEMBLE_GRIDS_USER],
                            "sims_per_grid": [len(c["sims"]) for c in classes], "cell_nm": [4, 4, 3],
                            "solver": "heun", "dt_fs": 50, "temperature_K": W.ENSEMBLE_TEMP,
@@ -446,6 +465,9 @@ def ensemble_bench(args, rank, world, local_rank, dist, emit=True):
                                         f"{args.steps} steps", "batched_over_unbatched": value / unbatched,
                               "max_abs_avg_m_diff": dm},
                 "gpu_launches": launches, "clocks": clocks}
+        if world > 1:
+            line["scaling"] = "strong"
+            line["per_sim_avg_m_gathered"] = gathered
         if emit:
             print(json.dumps(line), flush=True)
     ens.close()

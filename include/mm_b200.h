@@ -150,6 +150,9 @@ MM_API int mm_plan_nsim(mm_plan plan);
  * depend on the tiles (energies up to the order of their block partial sums). */
 MM_API int mm_plan_tiles(mm_plan plan, int tiles[4], double* eval_us);
 MM_API int mm_plan_set_tiles(mm_plan plan, const int tiles[4]);
+/* Tuning runs made in this process (the autotuner keeps each plan shape's result per
+ * device and reuses it for later plans of that shape; no counterpart in the reference). */
+MM_API long long mm_autotune_runs(void);
 /* Real-space demag tensor in FP64 on the GPU, the function Kernel_Arne
  * (kernel_magnetostatic.go:30-181) computes on the host: out[6][L0][L1][L2] (device,
  * caller-allocated; components 00 11 22 12 02 01 of the internal axes, K = -N so that

@@ -126,3 +126,26 @@ def test_fused_single_layer_matches_passes(n):
     r2 = to_np(single.torque(m[:3 * N])[0])
     assert np.array_equal(r1, r2)
     single.close()
+
+
+def test_tuning_is_reused_for_plans_of_the_same_shape():
+    """The autotuner times a plan shape once per process and device: a second plan of the
+    same shape takes the first one's tiles without a tuning run, a new shape runs it."""
+    import os
+    from mumax2 import Plan
+    from mumax2 import _native as nat
+    if os.environ.get("MM_AUTOTUNE", "1").startswith("0"):
+        return
+    L = nat.lib()
+    prob = dict(n=(1, 8, 512), cell=(3e-9, 4e-9, 4e-9), demag=1, exchange=1, msat=8e5, aex=1.3e-11)
+    r0 = L.mm_autotune_runs()
+    a = Plan(prob)
+    r1 = L.mm_autotune_runs()
+    b = Plan(prob)
+    r2 = L.mm_autotune_runs()
+    assert r1 == r0 + 1 and r2 == r1
+    assert a.tiles() == b.tiles()
+    c = Plan(dict(prob, n=(1, 8, 256)))
+    assert L.mm_autotune_runs() == r2 + 1
+    for p in (a, b, c):
+        p.close()

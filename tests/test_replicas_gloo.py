@@ -66,3 +66,56 @@ def test_failing_replica_is_reported():
     port = _free_port()
     with pytest.raises(mp.ProcessRaisedException, match="replica 1 fails"):
         mp.start_processes(_failing_worker, args=(world, port), nprocs=world, start_method="spawn", join=True)
+
+
+def _shard_worker(rank, world, port, out):
+    import sys
+    sys.path.insert(0, os.path.join(ROOT, "2_b200"))
+    import datetime
+    import numpy as np
+    import torch.distributed as dist
+    from mumax2 import workloads as W
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=60))
+    classes, (lo, hi) = W.ensemble_shard(2048, seed=0, rank=rank, world=world)
+    ids = np.concatenate([c["ids"] for c in classes])
+    cells = sum(len(c["ids"]) * int(np.prod(c["n"])) for c in classes)
+    # a stand-in per-simulation result: <m> of its initial direction
+    rows = np.concatenate([np.asarray(c["m0"]) for c in classes])
+    g = W.gather_per_sim(dist, ids, rows, 2048)
+    out[rank] = (lo, hi, int(cells), None if g is None else g.tolist())
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_ensemble_sharded_over_ranks_and_gathered_world2():
+    """N > 1 ensemble: each rank takes a contiguous, cell-balanced block of the same 2048
+    simulations (no collective while stepping), and the per-simulation results come
+    back to rank 0 in simulation order with one all-gather."""
+    import sys
+    import numpy as np
+    sys.path.insert(0, os.path.join(ROOT, "2_b200"))
+    from mumax2 import workloads as W
+    world = 2
+    port = _free_port()
+    mgr = mp.get_context("spawn").Manager()
+    out = mgr.dict()
+    mp.start_processes(_shard_worker, args=(world, port, out), nprocs=world, start_method="spawn", join=True)
+    (lo0, hi0, c0, g0), (lo1, hi1, c1, g1) = out[0], out[1]
+    assert lo0 == 0 and hi0 == lo1 and hi1 == 2048
+    assert abs(c0 - c1) / (c0 + c1) < 0.05            # balanced by cells
+    assert g1 is None
+    full = W.ensemble(2048, seed=0)
+    want = np.zeros((2048, 3))
+    for c in full:
+        want[c["ids"]] = np.asarray(c["m0"])
+    assert np.array_equal(np.asarray(g0), want)
+
+
+def test_partition_is_contiguous_and_balanced():
+    from mumax2 import workloads as W
+    w = [1, 1, 1, 10, 1, 1, 1, 1, 10, 1]
+    parts = W.partition(w, 3)
+    assert parts[0][0] == 0 and parts[-1][1] == len(w)
+    assert all(a[1] == b[0] for a, b in zip(parts, parts[1:]))
+    assert W.partition(w, 1) == [(0, len(w))]
