@@ -15,6 +15,7 @@
 // K = pixels, split over blocks and accumulated in FP32 with atomics.
 #include <cuda_bf16.h>
 #include <cstdint>
+#include <cstdlib>
 
 #include "mm_internal.h"
 
@@ -644,6 +645,41 @@ extern "C" MM_API int mm_nn_to_bf16(const float* in, long long P, int C, void* o
 // and returns.
 namespace mm {
 
+// Epilogue store of one pixel's 16 consecutive output channels c0 .. c0+15 (FP32 from
+// TMEM): bias, ReLU, bf16.  With vec (the row start 16-byte aligned and all 16 channels
+// present) two 16-byte stores, else bf16 pairs and a last single channel.
+__device__ __forceinline__ void store16(const unsigned (&v)[16], bf16* row, int c0, int Cout,
+                                        const float* __restrict__ bias, int relu, bool vec) {
+    float f[16];
+#pragma unroll
+    for (int e = 0; e < 16; e++) {
+        float a = __uint_as_float(v[e]);
+        if (bias && c0 + e < Cout) a += bias[c0 + e];
+        if (relu) a = fmaxf(a, 0.f);
+        f[e] = a;
+    }
+    if (vec && c0 + 16 <= Cout) {
+        unsigned w[8];
+#pragma unroll
+        for (int e = 0; e < 8; e++) {
+            __nv_bfloat162 h = __floats2bfloat162_rn(f[2 * e], f[2 * e + 1]);
+            w[e] = *reinterpret_cast<unsigned*>(&h);
+        }
+        uint4* o = reinterpret_cast<uint4*>(row + c0);
+        o[0] = make_uint4(w[0], w[1], w[2], w[3]);
+        o[1] = make_uint4(w[4], w[5], w[6], w[7]);
+        return;
+    }
+#pragma unroll
+    for (int e = 0; e < 16; e += 2) {
+        const int co = c0 + e;
+        if (co >= Cout) break;
+        bf16* o = row + co;
+        if (co + 1 < Cout) *reinterpret_cast<__nv_bfloat162*>(o) = __floats2bfloat162_rn(f[e], f[e + 1]);
+        else o[0] = __float2bfloat16_rn(f[e]);
+    }
+}
+
 // Iteration limit of the mbarrier waits of the tcgen05 kernels (mm_nn_set_wait_limit
 // changes it, e.g. to 0 so that a test sees the time-out path; the clean-up wait for
 // MMAs in flight always uses the default).
@@ -703,6 +739,7 @@ __global__ void __launch_bounds__(256) conv3x3_tc_kernel(const bf16* __restrict_
     const long long q0 = (long long)blockIdx.x * M;
     const int n0 = blockIdx.y * N;
     const int plane = band * 16;                   // bytes of one 8-channel plane of the band
+    const bool vec = (out_cs % 8 == 0) && (out_co % 8 == 0) && ((reinterpret_cast<uintptr_t>(out) & 15) == 0);
     for (int i = tid; i < band; i += 256) {
         const long long q = q0 - (Wp + 1) + i;
         int pix = -1;
@@ -826,25 +863,7 @@ __global__ void __launch_bounds__(256) conv3x3_tc_kernel(const bf16* __restrict_
                   "=r"(v[15])
                 : "r"(ta));
             asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::);
-            if (pix >= 0) {
-#pragma unroll
-                for (int e = 0; e < 16; e += 2) {
-                    const int co = n0 + c0 + e;
-                    if (co >= Cout) break;
-                    float a = __uint_as_float(v[e]), b = __uint_as_float(v[e + 1]);
-                    if (bias) {
-                        a += bias[co];
-                        if (co + 1 < Cout) b += bias[co + 1];
-                    }
-                    if (relu) {
-                        a = fmaxf(a, 0.f);
-                        b = fmaxf(b, 0.f);
-                    }
-                    bf16* o = out + (long long)pix * out_cs + out_co + co;
-                    if (co + 1 < Cout) *reinterpret_cast<__nv_bfloat162*>(o) = __floats2bfloat162_rn(a, b);
-                    else o[0] = __float2bfloat16_rn(a);
-                }
-            }
+            if (pix >= 0) store16(v, out + (long long)pix * out_cs + out_co, n0 + c0, Cout, bias, relu, vec);
         }
     } else if (fail_sh && tid == 0) {
         atomicExch(err, 1);
@@ -887,6 +906,275 @@ static cudaError_t launch_conv_tc(const bf16* in, int in_cs, int in_co, int Cin,
                                        st, band, stage_bytes);
     return launch_conv_tc_st<N, 2>(in, in_cs, in_co, Cin, W, bias, out, out_cs, out_co, Cout, B, H, Wd, relu, err, st,
                                    band, stage_bytes);
+}
+
+// ---------------------------------------------------------------- tcgen05 convolution, persistent
+// The same halo-band implicit GEMM as conv3x3_tc_kernel, as a persistent, warp-specialised
+// kernel: each block walks tiles blockIdx.x, + gridDim.x, ... with
+//   warps 0-3  loading (cp.async) the band slice and weights of each (tile, stage) into a
+//              ring of ST stages; a loader thread signals a stage on its `full` mbarrier
+//              once its own copies have landed (waited lazily, ST-1 stages behind, then
+//              a proxy fence for the tensor core's reads);
+//   warp 4     one thread issuing the nine MMAs of every stage into one of two TMEM
+//              accumulators (tile parity) and releasing the stage (`empty`, by
+//              tcgen05.commit) and the finished accumulator (`accfull`);
+//   warps 5-8  draining an accumulator (TMEM lane quarter = warp % 4) to the output
+//              while the next tile accumulates in the other one, then `accempty`.
+// So loads, MMAs and the epilogue of consecutive tiles overlap, and the per-block set-up
+// (barriers, TMEM allocation) happens once per SM slot instead of once per tile.  Every
+// wait is bounded; a block that runs out sets *err and all its roles stop.
+constexpr int TCP_THREADS = 288;
+
+__device__ __forceinline__ void mbar_init(unsigned long long* b, int count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(b)), "r"(count));
+}
+__device__ __forceinline__ void mbar_arrive(unsigned long long* b) {
+    asm volatile("{\n .reg .b64 st;\n mbarrier.arrive.shared::cta.b64 st, [%0];\n}\n" ::"r"(smem_u32(b)) : "memory");
+}
+
+template <int N, int ST>
+__global__ void __launch_bounds__(TCP_THREADS, 1) conv3x3_tcp_kernel(
+    const bf16* __restrict__ in, int in_cs, int in_co, int Cin, const bf16* __restrict__ W,
+    const float* __restrict__ bias, bf16* __restrict__ out, int out_cs, int out_co, int Cout, int B, int H, int Wd,
+    int relu, int* err, int band, int stage_bytes, long long limit, int ntiles) {
+    constexpr int M = 128;
+    constexpr int TCOLS = N < 32 ? 32 : N;
+    constexpr int ACOLS = 2 * TCOLS;               // two accumulators
+    constexpr int D = ST - 1;                      // stages whose loads are awaited lazily
+    extern __shared__ __align__(1024) unsigned char smem[];
+    __shared__ __align__(8) unsigned long long full[ST], empty[ST], accfull[2], accempty[2];
+    __shared__ unsigned tmem_base_sh;
+    __shared__ int fail_sh;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int Wp = Wd + 1;
+    const unsigned img = (unsigned)(H + 1) * (unsigned)Wp;
+    const long long total = (long long)B * img;
+    const int n0 = blockIdx.y * N;
+    const int plane = band * 16;
+    const int bwt = 2 * plane;
+    const int nstages = Cin / 16;
+    const bool vec = (out_cs % 8 == 0) && (out_co % 8 == 0) && ((reinterpret_cast<uintptr_t>(out) & 15) == 0);
+    const int nt = (ntiles - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;
+    if (tid == 0) {
+        fail_sh = 0;
+        for (int i = 0; i < ST; i++) {
+            mbar_init(&full[i], 128);
+            mbar_init(&empty[i], 1);
+        }
+        for (int i = 0; i < 2; i++) {
+            mbar_init(&accfull[i], 1);
+            mbar_init(&accempty[i], 128);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::);
+    }
+    if (warp == 4) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
+                         smem_u32(&tmem_base_sh)),
+                     "n"(ACOLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+    }
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+    const unsigned tmem = tmem_base_sh;
+    const long long LIMIT = limit;
+    volatile int* failp = &fail_sh;
+    // padded position -> input pixel, or -1 (pad column, pad row, outside the batch)
+    auto pix_of = [&](long long q) -> int {
+        if (q < 0 || q >= total) return -1;
+        const unsigned uq = (unsigned)q;
+        const unsigned b = uq / img, r = uq - b * img;
+        const unsigned y = r / (unsigned)Wp, xp = r - y * (unsigned)Wp;
+        return (y < (unsigned)H && xp > 0u) ? (int)((b * (unsigned)H + y) * (unsigned)Wd + xp - 1u) : -1;
+    };
+    auto core_off = [](int r, int h) { return ((r >> 3) * 2 + h) * 128 + (r & 7) * 16; };
+    int last_commit_slot = -1, last_commit_parity = 0;  // MMA thread: its last release of a stage
+    if (warp < 4) {
+        // ---- loaders
+        int g = 0;
+        bool ok = true;
+        for (int j = 0; j < nt && ok; j++) {
+            const long long q0 = (long long)((int)blockIdx.x + j * (int)gridDim.x) * M;
+            for (int s = 0; s < nstages; s++, g++) {
+                const int slot = g % ST;
+                if (g >= ST && !mbar_wait(smem_u32(&empty[slot]), ((g / ST) - 1) & 1, LIMIT)) {
+                    atomicExch(&fail_sh, 1);
+                    ok = false;
+                    break;
+                }
+                if (*failp) { ok = false; break; }
+                unsigned char* base = smem + slot * stage_bytes;
+                const int cs = s * 16;
+                for (int c = tid; c < 2 * band; c += 128) {
+                    const int h = c >= band ? 1 : 0, i = c - h * band;
+                    const int pix = pix_of(q0 - (Wp + 1) + i);
+                    cp_async16(base + h * plane + i * 16, in + (long long)(pix >= 0 ? pix : 0) * in_cs + in_co + cs + h * 8,
+                               pix >= 0);
+                }
+                for (int c = tid; c < 9 * 2 * N; c += 128) {
+                    const int tap = c / (2 * N), rem = c - tap * 2 * N;
+                    const int rr = rem >> 1, h = rem & 1;
+                    const int co = n0 + rr;
+                    const bool okb = co < Cout;
+                    cp_async16(base + bwt + tap * N * 32 + core_off(rr, h),
+                               W + ((long long)(okb ? co : 0) * 9 + tap) * Cin + cs + h * 8, okb);
+                }
+                cp_commit();
+                if (g >= D) {  // this thread's copies of stage g - D have landed
+                    cp_wait<D>();
+                    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+                    mbar_arrive(&full[(g - D) % ST]);
+                }
+            }
+        }
+        // the stages not yet signalled
+        cp_wait<0>();
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        if (ok)
+            for (int k = (g - D > 0 ? g - D : 0); k < g; k++) mbar_arrive(&full[k % ST]);
+    } else if (warp == 4) {
+        // ---- MMA issuer
+        if (lane == 0) {
+            const unsigned idesc =
+                (1u << 4) | (1u << 7) | (1u << 10) | ((unsigned)(N >> 3) << 17) | ((unsigned)(M >> 4) << 24);
+            int g = 0;
+            bool ok = true;
+            for (int j = 0; j < nt && ok; j++) {
+                const int acc = j & 1;
+                if (j >= 2 && !mbar_wait(smem_u32(&accempty[acc]), ((j >> 1) - 1) & 1, LIMIT)) {
+                    atomicExch(&fail_sh, 1);
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+                const unsigned dtm = tmem + (unsigned)(acc * TCOLS);
+                for (int s = 0; s < nstages; s++, g++) {
+                    const int slot = g % ST;
+                    if (*failp || !mbar_wait(smem_u32(&full[slot]), (g / ST) & 1, LIMIT)) {
+                        atomicExch(&fail_sh, 1);
+                        ok = false;
+                        break;
+                    }
+                    asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+                    const unsigned base = smem_u32(smem + slot * stage_bytes);
+#pragma unroll 1
+                    for (int tap = 0; tap < 9; tap++) {
+                        const unsigned off = (unsigned)(((tap / 3) * Wp + tap % 3) * 16);
+                        const uint64_t ad = umma_desc(base + off, (unsigned)plane, 128);
+                        const uint64_t bd = umma_desc(base + bwt + tap * N * 32, 128, 256);
+                        const unsigned accf = (s > 0 || tap > 0) ? 1u : 0u;
+                        asm volatile(
+                            "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+                            " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(dtm),
+                            "l"(ad), "l"(bd), "r"(idesc), "r"(accf));
+                    }
+                    asm volatile(
+                        "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                            smem_u32(&empty[slot])));
+                    last_commit_slot = slot;
+                    last_commit_parity = (g / ST) & 1;
+                }
+                if (!ok) break;
+                asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                    smem_u32(&accfull[acc])));
+            }
+        }
+        __syncwarp();
+    } else {
+        // ---- epilogue: TMEM lane quarter of this warp = its rows of the tile
+        const int quad = warp & 3;
+        for (int j = 0; j < nt; j++) {
+            const int acc = j & 1;
+            if (*failp || !mbar_wait(smem_u32(&accfull[acc]), (j >> 1) & 1, LIMIT)) {
+                atomicExch(&fail_sh, 1);
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+            const long long q0 = (long long)((int)blockIdx.x + j * (int)gridDim.x) * M;
+            const int pix = pix_of(q0 + quad * 32 + lane);
+#pragma unroll 1
+            for (int c0 = 0; c0 < N; c0 += 16) {
+                unsigned v[16];
+                const unsigned ta = tmem + ((unsigned)(quad * 32) << 16) + (unsigned)(acc * TCOLS + c0);
+                asm volatile(
+                    "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
+                    "[%16];\n"
+                    : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+                      "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
+                      "=r"(v[15])
+                    : "r"(ta));
+                asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::);
+                if (pix >= 0) store16(v, out + (long long)pix * out_cs + out_co, n0 + c0, Cout, bias, relu, vec);
+            }
+            asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
+            mbar_arrive(&accempty[acc]);
+        }
+    }
+    __syncthreads();
+    // a block that gave up waits (bounded, default limit) for the MMAs it has in flight
+    // before its TMEM is freed
+    if (warp == 4 && lane == 0 && *failp && last_commit_slot >= 0)
+        mbar_wait(smem_u32(&empty[last_commit_slot]), last_commit_parity, kWaitLimitDefault);
+    if (tid == 0 && *failp) atomicExch(err, 1);
+    __syncthreads();
+    if (warp == 4) {
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "n"(ACOLS));
+    }
+}
+
+template <int N, int ST>
+static cudaError_t launch_conv_tcp_st(const bf16* in, int in_cs, int in_co, int Cin, const bf16* W, const float* bias,
+                                      bf16* out, int out_cs, int out_co, int Cout, int B, int H, int Wd, int relu,
+                                      int* err, cudaStream_t st, int band, int stage_bytes) {
+    const int smem = ST * stage_bytes;
+    cudaError_t e = cudaFuncSetAttribute(conv3x3_tcp_kernel<N, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    const long long positions = (long long)B * (H + 1) * (Wd + 1);
+    const int ntiles = (int)((positions + 127) / 128);
+    constexpr int ACOLS = 2 * (N < 32 ? 32 : N);
+    int bps = (227 * 1024) / (smem + 2048);
+    if (bps > 512 / ACOLS) bps = 512 / ACOLS;
+    if (bps > 2) bps = 2;
+    if (bps < 1) bps = 1;
+    const int ny = (Cout + N - 1) / N;
+    int gx = (148 * bps + ny - 1) / ny;
+    if (gx > ntiles) gx = ntiles;
+    conv3x3_tcp_kernel<N, ST><<<dim3((unsigned)gx, (unsigned)ny), TCP_THREADS, smem, st>>>(
+        in, in_cs, in_co, Cin, W, bias, out, out_cs, out_co, Cout, B, H, Wd, relu, err, band, stage_bytes,
+        g_wait_limit, ntiles);
+    return cudaGetLastError();
+}
+
+// Stages of the ring: as many (2..4) as fit in 110 KB, so that two blocks share an SM.
+template <int N>
+static cudaError_t launch_conv_tcp(const bf16* in, int in_cs, int in_co, int Cin, const bf16* W, const float* bias,
+                                   bf16* out, int out_cs, int out_co, int Cout, int B, int H, int Wd, int relu,
+                                   int* err, cudaStream_t st) {
+    const int band = 128 + 2 * (Wd + 1) + 2;
+    const int stage_bytes = ((2 * band * 16 + 9 * N * 32) + 127) / 128 * 128;
+    const int fit = (110 * 1024) / stage_bytes;
+    if (fit >= 4)
+        return launch_conv_tcp_st<N, 4>(in, in_cs, in_co, Cin, W, bias, out, out_cs, out_co, Cout, B, H, Wd, relu,
+                                        err, st, band, stage_bytes);
+    if (fit == 3)
+        return launch_conv_tcp_st<N, 3>(in, in_cs, in_co, Cin, W, bias, out, out_cs, out_co, Cout, B, H, Wd, relu,
+                                        err, st, band, stage_bytes);
+    return launch_conv_tcp_st<N, 2>(in, in_cs, in_co, Cin, W, bias, out, out_cs, out_co, Cout, B, H, Wd, relu, err,
+                                    st, band, stage_bytes);
+}
+
+// The kernel of mm_nn_conv3x3_tc: the one-tile-per-block halo-band kernel (default), or
+// the persistent warp-specialised one (mm_nn_set_conv_kernel(1), or MM_NN_CONV=persistent
+// in the environment).  Measured per layer of the network at batch 256, the persistent
+// kernel is ahead only on the 16x16 layers with 128 output channels (d2a 161 vs 169 us)
+// and behind on the 64x64 ones (d0a 441 vs 292 us): its 128 loader threads per block
+// bring in less of the band at a time than the 256 of the other kernel.
+static int g_conv_kind = -1;
+static bool conv_persistent() {
+    if (g_conv_kind < 0) {
+        const char* e = getenv("MM_NN_CONV");
+        g_conv_kind = (e && e[0] == 'p') ? 1 : 0;
+    }
+    return g_conv_kind == 1;
 }
 
 // ---------------------------------------------------------------- tcgen05 weight gradient
@@ -1131,6 +1419,12 @@ extern "C" MM_API int mm_nn_conv3x3_wgrad_tc(const void* dy, int dy_cs, int dy_c
 
 // tcgen05 variant of mm_nn_conv3x3 (same arguments plus a device error flag that a
 // timed-out wait sets); N tile = 16..128 chosen from Cout.
+extern "C" MM_API int mm_nn_set_conv_kernel(int persistent) {
+    if (persistent != 0 && persistent != 1) return report_error(MM_ERR_ARG, "mm_nn_set_conv_kernel: 0 or 1");
+    g_conv_kind = persistent;
+    return MM_OK;
+}
+
 extern "C" MM_API int mm_nn_conv3x3_tc(const void* in, int in_cs, int in_co, int Cin, const void* W, const float* bias,
                                        void* out, int out_cs, int out_co, int Cout, int B, int H, int Wd, int relu,
                                        int* err, mm_stream st) {
@@ -1142,7 +1436,13 @@ extern "C" MM_API int mm_nn_conv3x3_tc(const void* in, int in_cs, int in_co, int
     const bf16* w = (const bf16*)W;
     bf16* o = (bf16*)out;
     cudaStream_t s = (cudaStream_t)st;
-    if (Cout <= 16) e = launch_conv_tc<16>(i, in_cs, in_co, Cin, w, bias, o, out_cs, out_co, Cout, B, H, Wd, relu, err, s);
+    const bool pers = conv_persistent() && (long long)B * (H + 1) * (Wd + 1) < (1LL << 31);
+    if (pers) {
+        if (Cout <= 16) e = launch_conv_tcp<16>(i, in_cs, in_co, Cin, w, bias, o, out_cs, out_co, Cout, B, H, Wd, relu, err, s);
+        else if (Cout <= 32) e = launch_conv_tcp<32>(i, in_cs, in_co, Cin, w, bias, o, out_cs, out_co, Cout, B, H, Wd, relu, err, s);
+        else if (Cout <= 64) e = launch_conv_tcp<64>(i, in_cs, in_co, Cin, w, bias, o, out_cs, out_co, Cout, B, H, Wd, relu, err, s);
+        else e = launch_conv_tcp<128>(i, in_cs, in_co, Cin, w, bias, o, out_cs, out_co, Cout, B, H, Wd, relu, err, s);
+    } else if (Cout <= 16) e = launch_conv_tc<16>(i, in_cs, in_co, Cin, w, bias, o, out_cs, out_co, Cout, B, H, Wd, relu, err, s);
     else if (Cout <= 32) e = launch_conv_tc<32>(i, in_cs, in_co, Cin, w, bias, o, out_cs, out_co, Cout, B, H, Wd, relu, err, s);
     else if (Cout <= 64) e = launch_conv_tc<64>(i, in_cs, in_co, Cin, w, bias, o, out_cs, out_co, Cout, B, H, Wd, relu, err, s);
     else e = launch_conv_tc<128>(i, in_cs, in_co, Cin, w, bias, o, out_cs, out_co, Cout, B, H, Wd, relu, err, s);

@@ -335,6 +335,10 @@ MM_API int mm_nn_set_wait_limit(long long iterations);
  * *err set if an mbarrier wait runs out. */
 MM_API int mm_nn_conv3x3_wgrad_tc(const void* dy, int dy_cs, int dy_co, int Cout, const void* x, int x_cs, int x_co,
                                   int Cin, float* dW, int B, int H, int W, int* err, mm_stream st);
+/* Kernel behind mm_nn_conv3x3_tc: 0 = one 128-position tile per block (default),
+ * 1 = persistent warp-specialised (loader warps, one MMA thread, epilogue warps, two TMEM
+ * accumulators).  Same results.  No counterpart in the reference. */
+MM_API int mm_nn_set_conv_kernel(int persistent);
 /* conv3x3 on the 5th-generation tensor cores (tcgen05.mma, TMEM accumulators); *err
  * (device int) is set if a bounded wait inside the kernel ran out. */
 MM_API int mm_nn_conv3x3_tc(const void* in, int in_cs, int in_co, int Cin, const void* W, const float* bias, void* out,

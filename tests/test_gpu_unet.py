@@ -127,16 +127,19 @@ def test_training_lowers_the_loss():
     assert losses[-1] < 0.2 * losses[0]
 
 
+@pytest.mark.parametrize("persistent", [0, 1])
 @pytest.mark.parametrize("cin,cout,B,H,W,relu", [(16, 32, 2, 8, 8, 1), (64, 128, 1, 16, 16, 0), (96, 32, 2, 8, 16, 1),
                                                  (32, 16, 1, 4, 4, 0), (384, 128, 2, 16, 16, 1), (256, 256, 4, 8, 8, 1),
                                                  (32, 32, 2, 64, 64, 1), (16, 16, 3, 5, 7, 1), (48, 64, 2, 1, 9, 0)])
-def test_conv3x3_tcgen05_matches(cin, cout, B, H, W, relu):
-    """The tcgen05 convolution (TMEM accumulators, halo band over padded positions)
-    against the numpy oracle, including widths that are not multiples of 8, single-row
-    images and tiles that span several images."""
+def test_conv3x3_tcgen05_matches(cin, cout, B, H, W, relu, persistent):
+    """The tcgen05 convolution (TMEM accumulators, halo band over padded positions), the
+    one-tile-per-block kernel and the persistent warp-specialised one, against the numpy
+    oracle, including widths that are not multiples of 8, single-row images and tiles
+    that span several images."""
     import torch
     import unet_ref as R
     from mumax2 import _native as nat
+    nat.check(nat.lib().mm_nn_set_conv_kernel(persistent))
     rng = np.random.default_rng(cin * 7 + cout)
     x = R.bf16(rng.normal(size=(B, H, W, cin)))
     w = R.bf16(rng.normal(size=(cout, 9, cin)) / np.sqrt(9 * cin))
@@ -153,6 +156,7 @@ def test_conv3x3_tcgen05_matches(cin, cout, B, H, W, relu):
     if relu:
         ref = np.maximum(ref, 0)
     got = out.float().cpu().numpy().reshape(ref.shape)
+    nat.check(nat.lib().mm_nn_set_conv_kernel(0))
     assert np.abs(got - ref).max() <= 2 ** -7 * np.abs(ref).max() + 1e-6
 
 
@@ -274,12 +278,14 @@ def test_relu_bias_bwd_matches(C, P, relu):
     assert _relnorm(db.cpu().numpy(), ref.sum(axis=0)) < 1e-5
 
 
-@pytest.mark.parametrize("kernel", ["tcgen05", "mma.sync"])
+@pytest.mark.parametrize("co", [16, 2])
+@pytest.mark.parametrize("kernel", ["tcgen05", "tcgen05-persistent", "mma.sync"])
 @pytest.mark.parametrize("cin,cout,B,H,W", [(384, 128, 4, 16, 16), (32, 32, 3, 64, 64), (96, 32, 2, 8, 16),
                                             (16, 16, 3, 5, 7)])
-def test_convolution_writes_only_its_output(kernel, cin, cout, B, H, W):
-    """Output canary: the convolution writes a channel slice (offset 16, Cout channels) of a
-    wider pixel-major buffer that sits between two guard regions.  Every element outside
+def test_convolution_writes_only_its_output(kernel, cin, cout, B, H, W, co):
+    """Output canary: the convolution writes a channel slice (offset co, Cout channels) of a
+    wider pixel-major buffer that sits between two guard regions (offset 16: 16-byte
+    vector stores; offset 2: the pair stores).  Every element outside
     the slice -- the other channels of each pixel and both guards -- must keep its canary
     value, and the slice must match the oracle."""
     import torch
@@ -292,15 +298,17 @@ def test_convolution_writes_only_its_output(kernel, cin, cout, B, H, W):
     xd, wd = _dev(x, torch.bfloat16), _dev(w, torch.bfloat16)
     bd = torch.tensor(b, device="cuda")
     P = B * H * W
-    cs, co, guard = cout + 48, 16, 1 << 16            # row stride, channel offset, guard elements
+    cs, guard = cout + 48, 1 << 16                    # row stride, guard elements
     canary = 0x7F7B                                   # a bf16 NaN payload no kernel computes
     buf = torch.full((2 * guard + P * cs,), canary, dtype=torch.int16, device="cuda")
     out = buf[guard:guard + P * cs]
     err = torch.zeros(1, dtype=torch.int32, device="cuda")
     L = nat.lib()
-    if kernel == "tcgen05":
+    if kernel.startswith("tcgen05"):
+        nat.check(L.mm_nn_set_conv_kernel(1 if kernel.endswith("persistent") else 0))
         nat.check(L.mm_nn_conv3x3_tc(_p(xd), cin, 0, cin, _p(wd), _p(bd), _p(out), cs, co, cout, B, H, W, 1,
                                      _p(err), None))
+        nat.check(L.mm_nn_set_conv_kernel(0))
     else:
         nat.check(L.mm_nn_conv3x3(_p(xd), cin, 0, cin, _p(wd), _p(bd), _p(out), cs, co, cout, B, H, W, 1, None))
     torch.cuda.synchronize()
