@@ -1198,13 +1198,14 @@ __device__ __forceinline__ int band_pixel(int q, int total, int img, int Wp, int
 
 constexpr int WGT_BAND_MAX = WGT_KC + 2 * 257 + 2;  // widths up to 256
 
-template <int ST>
+template <int ST, int TG>
 __global__ void __launch_bounds__(256) conv3x3_wgrad_tc_kernel(const bf16* __restrict__ dy, int dy_cs, int dy_co,
                                                                int Cout, const bf16* __restrict__ x, int x_cs,
                                                                int x_co, int Cin, float* __restrict__ dW, int B,
                                                                int H, int Wd, int* err, int band, int stage_bytes,
                                                                int per_block, long long limit) {
     constexpr int M = 128, N = 32, KC = WGT_KC;
+    constexpr int TCOLS = TG * N > 256 ? 512 : (TG * N > 128 ? 256 : (TG * N > 64 ? 128 : 64));
     extern __shared__ __align__(1024) unsigned char smem[];
     __shared__ __align__(8) unsigned long long mbar[ST];
     __shared__ unsigned tmem_base_sh;
@@ -1216,7 +1217,10 @@ __global__ void __launch_bounds__(256) conv3x3_wgrad_tc_kernel(const bf16* __res
     const int total = B * img;
     const int q_begin = blockIdx.x * per_block;
     const int q_end = q_begin + per_block < total ? q_begin + per_block : total;
-    const int ci0 = blockIdx.y * N, co0 = blockIdx.z * M;
+    // blockIdx.y: input-channel tile and group of TG taps (taps tap0 .. tap0 + TG - 1)
+    const int ngroups = 9 / TG;
+    const int tap0 = (blockIdx.y % ngroups) * TG;
+    const int ci0 = (blockIdx.y / ngroups) * N, co0 = blockIdx.z * M;
     // channel planes that exist: the others are never loaded, and the D rows / columns
     // they would feed are never stored
     const int ga = min(16, (Cout - co0 + 7) / 8), gb = min(4, (Cin - ci0 + 7) / 8);
@@ -1231,7 +1235,7 @@ __global__ void __launch_bounds__(256) conv3x3_wgrad_tc_kernel(const bf16* __res
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
                          smem_u32(&tmem_base_sh)),
-                     "n"(512));
+                     "n"(TCOLS));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
     }
     __syncthreads();
@@ -1284,7 +1288,8 @@ __global__ void __launch_bounds__(256) conv3x3_wgrad_tc_kernel(const bf16* __res
             asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
             const unsigned base = smem_u32(smem + (s % ST) * stage_bytes);
 #pragma unroll 1
-            for (int tap = 0; tap < 9; tap++) {
+            for (int tg = 0; tg < TG; tg++) {
+                const int tap = tap0 + tg;
                 const unsigned off = (unsigned)((tap / 3) * Wp + tap % 3);
 #pragma unroll 1
                 for (int kk = 0; kk < KC / 16; kk++) {
@@ -1293,7 +1298,7 @@ __global__ void __launch_bounds__(256) conv3x3_wgrad_tc_kernel(const bf16* __res
                     const unsigned acc = (s > 0 || kk > 0) ? 1u : 0u;
                     asm volatile(
                         "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
-                        " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem + tap * N),
+                        " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem + tg * N),
                         "l"(ad), "l"(bd), "r"(idesc), "r"(acc));
                 }
             }
@@ -1326,16 +1331,18 @@ __global__ void __launch_bounds__(256) conv3x3_wgrad_tc_kernel(const bf16* __res
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
     // epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31 (output channels); warps 0-3
-    // take taps 0-4, warps 4-7 taps 5-8
+    // take the first (TG+1)/2 taps of the block, warps 4-7 the others
     const int quad = warp & 3, half = warp >> 2;
+    constexpr int TH = (TG + 1) / 2;
     if (!fail_sh && issued > 0) {
         const int co = co0 + quad * 32 + lane;
-        for (int tap = half * 5; tap < (half ? 9 : 5); tap++) {
+        for (int tg = half * TH; tg < (half ? TG : TH); tg++) {
+            const int tap = tap0 + tg;
 #pragma unroll
             for (int c0 = 0; c0 < N; c0 += 16) {
                 if (ci0 + c0 >= Cin) break;   // warp-uniform
                 unsigned v[16];
-                const unsigned ta = tmem + ((unsigned)(quad * 32) << 16) + (unsigned)(tap * N + c0);
+                const unsigned ta = tmem + ((unsigned)(quad * 32) << 16) + (unsigned)(tg * N + c0);
                 asm volatile(
                     "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
                     "[%16];\n"
@@ -1359,30 +1366,45 @@ __global__ void __launch_bounds__(256) conv3x3_wgrad_tc_kernel(const bf16* __res
     __syncthreads();
     if (warp == 0) {
         asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "n"(512));
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "n"(TCOLS));
     }
 }
 
-template <int ST>
+// TG taps per block: 9 (one block per SM, all 512 TMEM columns) or 3 (three tap groups
+// as separate blocks, 128 columns each, up to four blocks per SM).
+template <int ST, int TG>
 static cudaError_t launch_wgrad_tc_st(const bf16* dy, int dy_cs, int dy_co, int Cout, const bf16* x, int x_cs,
                                       int x_co, int Cin, float* dW, int B, int H, int Wd, int* err, int band,
                                       int stage_bytes, cudaStream_t st) {
-    // a block holds all 512 TMEM columns: at least 116 KB of shared memory keeps a second
-    // block off the SM, so no allocation ever waits for another block
-    const int smem = ST * stage_bytes > 116 * 1024 ? ST * stage_bytes : 116 * 1024;
-    cudaError_t e = cudaFuncSetAttribute(conv3x3_wgrad_tc_kernel<ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    // with all 512 TMEM columns in one block, at least 116 KB of shared memory keeps a
+    // second block off the SM, so no allocation ever waits for another block; with 128
+    // columns, four blocks fit the TMEM and shared memory is limited to a quarter
+    const int smem = TG == 9 ? (ST * stage_bytes > 116 * 1024 ? ST * stage_bytes : 116 * 1024)
+                             : (ST * stage_bytes > 56 * 1024 ? ST * stage_bytes : 56 * 1024);
+    cudaError_t e =
+        cudaFuncSetAttribute(conv3x3_wgrad_tc_kernel<ST, TG>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
     const long long total = (long long)B * (H + 1) * (Wd + 1);
     const int ct = (Cin + 31) / 32, mt = (Cout + 127) / 128;
-    // about two blocks' worth of work per SM, whole stages per block
-    long long chunks = (2LL * 148 + (long long)ct * mt - 1) / ((long long)ct * mt);
+    const int ng = 9 / TG;
+    // about two (TG = 9) or eight (TG = 3) blocks' worth of work per SM, whole stages per block
+    long long chunks = ((TG == 9 ? 2LL : 8LL) * 148 + (long long)ct * mt * ng - 1) / ((long long)ct * mt * ng);
     long long per = (total + chunks - 1) / chunks;
     per = (per + WGT_KC - 1) / WGT_KC * WGT_KC;
     chunks = (total + per - 1) / per;
-    dim3 grid((unsigned)chunks, (unsigned)ct, (unsigned)mt);
-    conv3x3_wgrad_tc_kernel<ST><<<grid, 256, smem, st>>>(dy, dy_cs, dy_co, Cout, x, x_cs, x_co, Cin, dW, B, H, Wd, err,
-                                                         band, stage_bytes, (int)per, g_wait_limit);
+    dim3 grid((unsigned)chunks, (unsigned)(ct * ng), (unsigned)mt);
+    conv3x3_wgrad_tc_kernel<ST, TG><<<grid, 256, smem, st>>>(dy, dy_cs, dy_co, Cout, x, x_cs, x_co, Cin, dW, B, H, Wd,
+                                                             err, band, stage_bytes, (int)per, g_wait_limit);
     return cudaGetLastError();
+}
+
+static int g_wgrad_tg = -1;  // taps per block of the tcgen05 weight gradient: 9 or 3
+static int wgrad_taps() {
+    if (g_wgrad_tg < 0) {
+        const char* e = getenv("MM_NN_WGRAD_TAPS");
+        g_wgrad_tg = (e && e[0] == '9') ? 9 : 3;
+    }
+    return g_wgrad_tg;
 }
 
 }  // namespace mm
@@ -1402,29 +1424,36 @@ extern "C" MM_API int mm_nn_conv3x3_wgrad_tc(const void* dy, int dy_cs, int dy_c
         return report_error(MM_ERR_ARG, "mm_nn_conv3x3_wgrad_tc: bad argument");
     const int band = WGT_KC + 2 * (Wd + 1) + 2;
     const int stage_bytes = ((16 * WGT_KC * 16 + 4 * band * 16) + 127) / 128 * 128;
-    const int fit = (200 * 1024) / stage_bytes;
     cudaError_t e;
-    if (fit >= 4)
-        e = launch_wgrad_tc_st<4>((const bf16*)dy, dy_cs, dy_co, Cout, (const bf16*)x, x_cs, x_co, Cin, dW, B, H, Wd, err,
-                                  band, stage_bytes, (cudaStream_t)st);
-    else if (fit == 3)
-        e = launch_wgrad_tc_st<3>((const bf16*)dy, dy_cs, dy_co, Cout, (const bf16*)x, x_cs, x_co, Cin, dW, B, H, Wd, err,
-                                  band, stage_bytes, (cudaStream_t)st);
-    else
-        e = launch_wgrad_tc_st<2>((const bf16*)dy, dy_cs, dy_co, Cout, (const bf16*)x, x_cs, x_co, Cin, dW, B, H, Wd, err,
-                                  band, stage_bytes, (cudaStream_t)st);
+    const bf16 *dyb = (const bf16*)dy, *xb = (const bf16*)x;
+    cudaStream_t s = (cudaStream_t)st;
+    if (wgrad_taps() == 9) {
+        const int fit = (200 * 1024) / stage_bytes;
+        if (fit >= 4)
+            e = launch_wgrad_tc_st<4, 9>(dyb, dy_cs, dy_co, Cout, xb, x_cs, x_co, Cin, dW, B, H, Wd, err, band, stage_bytes, s);
+        else if (fit == 3)
+            e = launch_wgrad_tc_st<3, 9>(dyb, dy_cs, dy_co, Cout, xb, x_cs, x_co, Cin, dW, B, H, Wd, err, band, stage_bytes, s);
+        else
+            e = launch_wgrad_tc_st<2, 9>(dyb, dy_cs, dy_co, Cout, xb, x_cs, x_co, Cin, dW, B, H, Wd, err, band, stage_bytes, s);
+    } else {
+        const int fit = (56 * 1024) / stage_bytes;
+        if (fit >= 3)
+            e = launch_wgrad_tc_st<3, 3>(dyb, dy_cs, dy_co, Cout, xb, x_cs, x_co, Cin, dW, B, H, Wd, err, band, stage_bytes, s);
+        else
+            e = launch_wgrad_tc_st<2, 3>(dyb, dy_cs, dy_co, Cout, xb, x_cs, x_co, Cin, dW, B, H, Wd, err, band, stage_bytes, s);
+    }
     if (e != cudaSuccess) return report_error(MM_ERR_CUDA, cudaGetErrorString(e));
     return MM_OK;
 }
 
-// tcgen05 variant of mm_nn_conv3x3 (same arguments plus a device error flag that a
-// timed-out wait sets); N tile = 16..128 chosen from Cout.
 extern "C" MM_API int mm_nn_set_conv_kernel(int persistent) {
     if (persistent != 0 && persistent != 1) return report_error(MM_ERR_ARG, "mm_nn_set_conv_kernel: 0 or 1");
     g_conv_kind = persistent;
     return MM_OK;
 }
 
+// tcgen05 variant of mm_nn_conv3x3 (same arguments plus a device error flag that a
+// timed-out wait sets); N tile = 16..128 chosen from Cout.
 extern "C" MM_API int mm_nn_conv3x3_tc(const void* in, int in_cs, int in_co, int Cin, const void* W, const float* bias,
                                        void* out, int out_cs, int out_co, int Cout, int B, int H, int Wd, int relu,
                                        int* err, mm_stream st) {
