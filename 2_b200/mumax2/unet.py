@@ -80,9 +80,12 @@ def init_params(seed=0):
     return params
 
 
-# feature channels that carry the y components of the anisotropy axis and the field
+# feature channels that carry the y components of the anisotropy axis and the field,
+# and their columns in param_table
 FEAT_AXIS_Y = 5
 FEAT_B_Y = 7
+PRM_AXIS_Y = 4
+PRM_B_Y = 6
 
 
 def features(sims, masks, n):

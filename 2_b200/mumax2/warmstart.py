@@ -375,14 +375,20 @@ def train(data, epochs=20, batch=256, lr=1e-3, seed=0, device=0, log=None, tcgen
     return net, losses
 
 
-def predict(net, sims, masks, n, host=False):
+def predict(net, sims, masks, n, host=False, mirror=True):
     """Initial states [nq][3N] (internal SoA, normalised, masked) for the problems, net.B
     per launch, built on the GPU from the problems' masks and parameters: a float32 device
-    tensor (a host array with host=True)."""
+    tensor (a host array with host=True).
+
+    mirror=True also runs each problem's x-mirror image (Dataset's exact symmetry: mask
+    reflected, u_y and B_y negated), maps that prediction back (reflected, m ->
+    (m_x, -m_y, -m_z)) and averages the two before normalising: the network's errors on
+    a problem and on its mirror image are partly independent."""
     import torch
     B = net.B
     nq = len(sims)
-    P = n[1] * n[2]
+    ny, nx = n[1], n[2]
+    P = ny * nx
     nqp = ((nq + B - 1) // B) * B
     mk = np.zeros((nqp, P), dtype=np.float32)
     mk[:nq] = np.stack(masks)
@@ -391,10 +397,26 @@ def predict(net, sims, masks, n, host=False):
     mk_d = torch.tensor(mk, device=net.device)
     prm_d = torch.tensor(prm, device=net.device)
     out = torch.empty((nqp, 3 * P), dtype=torch.float32, device=net.device)
+    if mirror:
+        mk_m = torch.flip(mk_d.view(-1, ny, nx), dims=[2]).reshape(nqp, P).contiguous()
+        prm_m = prm_d.clone()
+        prm_m[:, U.PRM_AXIS_Y] *= -1.0
+        prm_m[:, U.PRM_B_Y] *= -1.0
+        tmp = torch.empty((B, 3 * P), dtype=torch.float32, device=net.device)
+        sign = torch.tensor([-1.0, -1.0, 1.0], device=net.device).view(1, 3, 1, 1)   # internal (z, y, x)
     for i in range(0, nq, B):
         net.set_features(mk_d[i:i + B], prm_d[i:i + B])
         net.forward()
         net.states(mk_d[i:i + B], out[i:i + B])
+        if mirror:
+            net.set_features(mk_m[i:i + B], prm_m[i:i + B])
+            net.forward()
+            net.states(mk_m[i:i + B], tmp)
+            back = torch.flip(tmp.view(B, 3, ny, nx), dims=[3]) * sign
+            avg = out[i:i + B].view(B, 3, ny, nx) + back
+            nrm = torch.sqrt((avg * avg).sum(dim=1, keepdim=True))
+            avg = torch.where(nrm > 0, avg / nrm.clamp_min(1e-30), avg)
+            out[i:i + B] = (avg * mk_d[i:i + B].view(B, 1, ny, nx)).reshape(B, 3 * P)
     net.check()
     out = out[:nq]
     return out.cpu().numpy() if host else out
