@@ -513,7 +513,9 @@ cudaError_t launch_zmul_reg(int P, float2* S, const KernelView& K, int L1, int h
                             cudaStream_t st, int nsim, long long sim_stride, const float* sim_scale) {
     switch (P) {
 #define X(p, f) case p: return f<p>(S, K, L1, h, hp, comp_stride, zstride, scale, tw, ctl, skip_retry, st, nsim, sim_stride, sim_scale);
-        X(1, launch_zmul_reg_t) X(2, launch_zmul_reg_t) X(4, launch_zmul_reg4_t) X(8, launch_zmul_reg4_t)
+        // two lanes per column up to P = 8 (measured: P = 4, 128x128x4 ensemble class
+        // 1073 -> 1012 us; P = 8, 8x128x128 film 11.8 -> 11.0 us), four at P = 16
+        X(1, launch_zmul_reg_t) X(2, launch_zmul_reg_t) X(4, launch_zmul_reg_t) X(8, launch_zmul_reg_t)
         X(16, launch_zmul_reg4_t)
 #undef X
         default: return cudaErrorNotSupported;
