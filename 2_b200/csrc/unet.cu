@@ -911,19 +911,21 @@ static cudaError_t launch_conv_tc(const bf16* in, int in_cs, int in_co, int Cin,
 // ---------------------------------------------------------------- tcgen05 convolution, persistent
 // The same halo-band implicit GEMM as conv3x3_tc_kernel, as a persistent, warp-specialised
 // kernel: each block walks tiles blockIdx.x, + gridDim.x, ... with
-//   warps 0-3  loading (cp.async) the band slice and weights of each (tile, stage) into a
+//   warps 0-7  loading (cp.async) the band slice and weights of each (tile, stage) into a
 //              ring of ST stages; a loader thread signals a stage on its `full` mbarrier
 //              once its own copies have landed (waited lazily, ST-1 stages behind, then
 //              a proxy fence for the tensor core's reads);
-//   warp 4     one thread issuing the nine MMAs of every stage into one of two TMEM
+//   warp 8     one thread issuing the nine MMAs of every stage into one of two TMEM
 //              accumulators (tile parity) and releasing the stage (`empty`, by
 //              tcgen05.commit) and the finished accumulator (`accfull`);
-//   warps 5-8  draining an accumulator (TMEM lane quarter = warp % 4) to the output
+//   warps 9-12 draining an accumulator (TMEM lane quarter = warp % 4) to the output
 //              while the next tile accumulates in the other one, then `accempty`.
 // So loads, MMAs and the epilogue of consecutive tiles overlap, and the per-block set-up
 // (barriers, TMEM allocation) happens once per SM slot instead of once per tile.  Every
 // wait is bounded; a block that runs out sets *err and all its roles stop.
-constexpr int TCP_THREADS = 288;
+constexpr int TCP_LW = 8;                          // loader warps (0 .. TCP_LW-1)
+constexpr int TCP_LOAD_THREADS = 32 * TCP_LW;
+constexpr int TCP_THREADS = 32 * (TCP_LW + 1 + 4);   // + the MMA warp + four epilogue warps
 
 __device__ __forceinline__ void mbar_init(unsigned long long* b, int count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(b)), "r"(count));
@@ -958,7 +960,7 @@ __global__ void __launch_bounds__(TCP_THREADS, 1) conv3x3_tcp_kernel(
     if (tid == 0) {
         fail_sh = 0;
         for (int i = 0; i < ST; i++) {
-            mbar_init(&full[i], 128);
+            mbar_init(&full[i], TCP_LOAD_THREADS);
             mbar_init(&empty[i], 1);
         }
         for (int i = 0; i < 2; i++) {
@@ -967,7 +969,7 @@ __global__ void __launch_bounds__(TCP_THREADS, 1) conv3x3_tcp_kernel(
         }
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::);
     }
-    if (warp == 4) {
+    if (warp == TCP_LW) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
                          smem_u32(&tmem_base_sh)),
                      "n"(ACOLS));
@@ -988,7 +990,7 @@ __global__ void __launch_bounds__(TCP_THREADS, 1) conv3x3_tcp_kernel(
     };
     auto core_off = [](int r, int h) { return ((r >> 3) * 2 + h) * 128 + (r & 7) * 16; };
     int last_commit_slot = -1, last_commit_parity = 0;  // MMA thread: its last release of a stage
-    if (warp < 4) {
+    if (warp < TCP_LW) {
         // ---- loaders
         int g = 0;
         bool ok = true;
@@ -1004,13 +1006,13 @@ __global__ void __launch_bounds__(TCP_THREADS, 1) conv3x3_tcp_kernel(
                 if (*failp) { ok = false; break; }
                 unsigned char* base = smem + slot * stage_bytes;
                 const int cs = s * 16;
-                for (int c = tid; c < 2 * band; c += 128) {
+                for (int c = tid; c < 2 * band; c += TCP_LOAD_THREADS) {
                     const int h = c >= band ? 1 : 0, i = c - h * band;
                     const int pix = pix_of(q0 - (Wp + 1) + i);
                     cp_async16(base + h * plane + i * 16, in + (long long)(pix >= 0 ? pix : 0) * in_cs + in_co + cs + h * 8,
                                pix >= 0);
                 }
-                for (int c = tid; c < 9 * 2 * N; c += 128) {
+                for (int c = tid; c < 9 * 2 * N; c += TCP_LOAD_THREADS) {
                     const int tap = c / (2 * N), rem = c - tap * 2 * N;
                     const int rr = rem >> 1, h = rem & 1;
                     const int co = n0 + rr;
@@ -1031,7 +1033,7 @@ __global__ void __launch_bounds__(TCP_THREADS, 1) conv3x3_tcp_kernel(
         asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
         if (ok)
             for (int k = (g - D > 0 ? g - D : 0); k < g; k++) mbar_arrive(&full[k % ST]);
-    } else if (warp == 4) {
+    } else if (warp == TCP_LW) {
         // ---- MMA issuer
         if (lane == 0) {
             const unsigned idesc =
@@ -1111,11 +1113,11 @@ __global__ void __launch_bounds__(TCP_THREADS, 1) conv3x3_tcp_kernel(
     __syncthreads();
     // a block that gave up waits (bounded, default limit) for the MMAs it has in flight
     // before its TMEM is freed
-    if (warp == 4 && lane == 0 && *failp && last_commit_slot >= 0)
+    if (warp == TCP_LW && lane == 0 && *failp && last_commit_slot >= 0)
         mbar_wait(smem_u32(&empty[last_commit_slot]), last_commit_parity, kWaitLimitDefault);
     if (tid == 0 && *failp) atomicExch(err, 1);
     __syncthreads();
-    if (warp == 4) {
+    if (warp == TCP_LW) {
         asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "n"(ACOLS));
     }
