@@ -294,6 +294,7 @@ __global__ void __launch_bounds__(128) zmul_reg_kernel(float2* __restrict__ S, K
                                                        const float2* __restrict__ tw, const DevCtl* ctl,
                                                        int skip_retry, long long sim_stride,
                                                        const float* __restrict__ sim_scale) {
+    pdl_begin();
     if (BATCH) {
         if (ctl) ctl += blockIdx.y;
         S += blockIdx.y * sim_stride;
@@ -485,12 +486,10 @@ static cudaError_t launch_zmul_reg_t(float2* S, const KernelView& K, int L1, int
     const long long threads = 2LL * L1 * h;
     const dim3 grid((unsigned)((threads + 127) / 128), (unsigned)nsim);
     if (nsim > 1)
-        zmul_reg_kernel<P, true><<<grid, 128, 0, st>>>(S, K, L1, h, hp, comp_stride, zstride, scale, tw, ctl,
-                                                       skip_retry, sim_stride, sim_scale);
-    else
-        zmul_reg_kernel<P, false><<<grid, 128, 0, st>>>(S, K, L1, h, hp, comp_stride, zstride, scale, tw, ctl,
-                                                        skip_retry, sim_stride, sim_scale);
-    return cudaGetLastError();
+        return launch_pdl(zmul_reg_kernel<P, true>, grid, dim3(128), 0, st, S, K, L1, h, hp, comp_stride, zstride,
+                          scale, tw, ctl, skip_retry, sim_stride, sim_scale);
+    return launch_pdl(zmul_reg_kernel<P, false>, grid, dim3(128), 0, st, S, K, L1, h, hp, comp_stride, zstride, scale,
+                      tw, ctl, skip_retry, sim_stride, sim_scale);
 }
 
 template <int P>
