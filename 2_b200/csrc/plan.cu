@@ -1440,6 +1440,7 @@ static int launch_combine(mm_plan p, PP base, PP next, int nk, const PP* kp, con
 // epi_r2c_ok(p)), so that the evaluation at `next` starts at its column pass
 // (launch_eval with EVAL_ROWS_READY).
 static int enqueue_combine_rows(mm_plan p, PP base, PP next, int nk, const PP* kp, const double* ak, cudaStream_t st) {
+    PdlScope pdl_scope(p->pdl);
     const CombineArgs A = combine_args(p, base, next, nk, kp, ak, 0);
     CUCHK(launch_combine_rows(p->g.M, A, p->g.n, p->S, p->g.hp, p->g.L[1], p->spec_bstride(), p->tw,
                               p->khat_d ? 0 : 1, p->nsim, st));

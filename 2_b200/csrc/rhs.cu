@@ -775,6 +775,7 @@ template <int M>
 __global__ void __launch_bounds__(384) combine_rows_kernel(CombineArgs A, int n0, int n1, int n2, float2* S, int hp,
                                                            int L1, long long spec_bstride,
                                                            const float2* __restrict__ tw, int fwd_mask) {
+    pdl_begin();
     constexpr int RPB = xinv4_rows_c<M, false>();
     using F = FS<M>;
     const DevCtl* ctl = A.ctl + blockIdx.y;
@@ -855,9 +856,8 @@ static cudaError_t launch_combine_rows_t(const CombineArgs& A, const int n[3], f
     const int blocks = (n[0] * n[1] + RPB - 1) / RPB;
     int threads = RPB * 3 * FS<M>::P2;
     if (threads < 32) threads = 32;
-    combine_rows_kernel<M><<<dim3((unsigned)blocks, (unsigned)nsim), threads, smem, st>>>(
-        A, n[0], n[1], n[2], S, hp, L1, spec_bstride, tw, fwd_mask);
-    return cudaGetLastError();
+    return launch_pdl(combine_rows_kernel<M>, dim3((unsigned)blocks, (unsigned)nsim), dim3(threads), smem, st, A, n[0],
+                      n[1], n[2], S, hp, L1, spec_bstride, tw, fwd_mask);
 }
 
 cudaError_t launch_combine_rows(int M, const CombineArgs& A, const int n[3], float2* S, int hp, int L1,
