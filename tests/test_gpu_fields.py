@@ -185,12 +185,15 @@ def test_demag_periodic(n, pbc):
         assert err < TOL_FIELD
 
 
-@pytest.mark.parametrize("n,pbc", [((1, 16, 32), (0, 0, 0)), ((4, 8, 16), (0, 0, 0)), ((2, 8, 8), (0, 1, 1)),
-                                   ((1, 8, 16), (0, 0, 1))])
-def test_demagexch_field_and_torque(n, pbc):
-    """Module demagexch: exchange folded into the demag kernel (mod_demagexchange.go)."""
+@pytest.mark.parametrize("n,pbc,tensor", [((1, 16, 32), (0, 0, 0), "arne"), ((4, 8, 16), (0, 0, 0), "arne"),
+                                          ((2, 8, 8), (0, 1, 1), "arne"), ((1, 8, 16), (0, 0, 1), "arne"),
+                                          ((3, 12, 20), (0, 0, 0), "arne"), ((1, 16, 32), (0, 0, 0), "newell"),
+                                          ((3, 10, 12), (0, 1, 0), "newell")])
+def test_demagexch_field_and_torque(n, pbc, tensor):
+    """Module demagexch: exchange folded into the demag kernel (mod_demagexchange.go), on
+    power-of-two and mixed-radix grids, with either demag tensor."""
     prob = dict(n=n, cell=(3e-9, 4e-9, 4e-9), pbc=pbc, demag=1, exchange=1, msat=8e5, aex=1.3e-11,
-                demag_exchange=1, demag_accuracy=8)
+                demag_exchange=1, demag_accuracy=8, demag_tensor=tensor)
     o, g = _pair(prob)
     assert g.kernel_nonzero()[:3] == [1, 1, 1]
     m = rand_m(n, seed=31)

@@ -125,3 +125,29 @@ def test_script_setpointwise():
     mo = o.average(o.normalize(r.m))[::-1]
     assert np.abs(np.array(m_user) - mo).max() < 1e-4
     mm.reset()
+
+
+def test_bext_table_on_mixed_radix_batched_plan():
+    """A B_ext time table on a batched plan whose padded sizes are not powers of two (the
+    mixed-radix C2R epilogue with staged per-simulation scalars): each simulation's
+    fields at a table time equal its own single plan's and the oracle's."""
+    import oracle as O
+    from mumax2 import Plan
+    n = (1, 12, 20)
+    prob = dict(FILM, n=n)
+    sims = [dict(msat=8e5, aex=1.3e-11, alpha=0.05, bext=(0.0, 0.0, 0.0)),
+            dict(msat=6e5, aex=1.0e-11, alpha=0.1, bext=(0.0, 0.01, 0.0))]
+    g = Plan(O.full_desc(**prob), sims=sims)
+    g.set_table("bext", TIMES, VALUES)
+    g.set_time(1.3e-11)
+    N = n[1] * n[2]
+    m = np.concatenate([rand_m(n, seed=8), rand_m(n, seed=9)])
+    fg = to_np(g.fields(m)["eff"])
+    for b, sm in enumerate(sims):
+        q = O.full_desc(**dict(prob, **sm))
+        o = O.Oracle(q)
+        o.set_table(0, TIMES, VALUES)
+        o.set_time(1.3e-11)
+        err = rel_err(fg[3 * N * b:3 * N * (b + 1)], o.fields(m[3 * N * b:3 * N * (b + 1)])["eff"])
+        print("mixed-radix batched table", b, err)
+        assert err < 1e-5
