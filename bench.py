@@ -314,24 +314,26 @@ def reference_arm(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
-def e2e_pipelined(plan, host_in, device, steps=20):
+def e2e_pipelined(plan, host_in, device, steps=20, jobs=2):
     """End-to-end rate of independent jobs through the C-ABI with host buffers: each job
     uploads its input state from pinned host memory (mm_set_state from the host), takes
-    one step (mm_step) and downloads the resulting state (mm_get_state to the host).  A
-    second plan of the same workload runs the other half of the jobs from its own host
-    thread and stream, so that the copies of one job overlap the step of another (the
-    two copy directions and the kernels use separate engines).  Device time from the
-    first to the last event on the two streams."""
+    one step (mm_step) and downloads the resulting state (mm_get_state to the host).
+    `jobs` plans of the same workload (`plan` and jobs-1 more) run the jobs from their own
+    host threads and streams, so that the copies of one job overlap the steps of the
+    others (the two copy directions and the kernels use separate engines).  Device time
+    from the first to the last event on the streams."""
     import ctypes as C
     import torch
     from mumax2 import Plan
     from mumax2 import _native as nat
     w = WORKLOAD
     L = nat.lib()
-    plan2 = Plan(problem(), device=device)
-    plan2.solver(w["solver"], dt=w["dt0"], maxerr=w["maxerr"])
-    plans = [plan, plan2]
-    streams = [torch.cuda.Stream(), torch.cuda.Stream()]
+    plans = [plan]
+    for _ in range(jobs - 1):
+        q = Plan(problem(), device=device)
+        q.solver(w["solver"], dt=w["dt0"], maxerr=w["maxerr"])
+        plans.append(q)
+    streams = [torch.cuda.Stream() for _ in plans]
     outs = [torch.empty_like(host_in).pin_memory() for _ in plans]
 
     def job(k, n):
@@ -341,24 +343,26 @@ def e2e_pipelined(plan, host_in, device, steps=20):
             nat.check(L.mm_step(h, st))
             nat.check(L.mm_get_state(h, C.c_void_p(outs[k].data_ptr()), 1, st))
 
-    for k in range(2):   # warm-up: graph capture of each plan on its stream
+    for k in range(jobs):   # warm-up: graph capture of each plan on its stream
         job(k, 2)
     torch.cuda.synchronize()
-    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in range(2)]
-    for k in range(2):
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in range(jobs)]
+    for k in range(jobs):
         ev[k][0].record(streams[k])
-    th = [threading.Thread(target=job, args=(k, steps // 2)) for k in range(2)]
+    per = steps // jobs
+    th = [threading.Thread(target=job, args=(k, per)) for k in range(jobs)]
     for t in th:
         t.start()
     for t in th:
         t.join()
-    for k in range(2):
+    for k in range(jobs):
         ev[k][1].record(streams[k])
     torch.cuda.synchronize()
-    t0 = 0 if ev[0][0].elapsed_time(ev[1][0]) >= 0 else 1   # the earlier start
-    ms = max(ev[t0][0].elapsed_time(ev[k][1]) for k in range(2))
-    plan2.close()
-    return {"ms": ms, "steps": 2 * (steps // 2)}
+    t0 = min(range(jobs), key=lambda k: ev[0][0].elapsed_time(ev[k][0]))   # the earliest start
+    ms = max(ev[t0][0].elapsed_time(ev[k][1]) for k in range(jobs))
+    for q in plans[1:]:
+        q.close()
+    return {"ms": ms, "steps": jobs * per, "jobs": jobs}
 
 
 # ---------------------------------------------------------------- replicas
@@ -938,7 +942,7 @@ def main():
     f1.record()
     torch.cuda.synchronize()
     e2e_ms, e2e_value = aggregate(f0.elapsed_time(f1), N, e2e_steps, world, dist, "cuda")
-    e2e_pipe = e2e_pipelined(plan, host_in, local_rank, steps=2 * e2e_steps)
+    e2e_pipe = e2e_pipelined(plan, host_in, local_rank, steps=4 * e2e_steps, jobs=4)
     _, e2e_pipe_value = aggregate(e2e_pipe["ms"], N, e2e_pipe["steps"], world, dist, "cuda")
 
     cb = None
@@ -981,8 +985,9 @@ def main():
             "e2e": {"value": e2e_pipe_value, "unit": "cell-steps/s", "h2d_bytes_per_step": 12 * N,
                     "d2h_bytes_per_step": 12 * N, "steps": e2e_pipe["steps"],
                     "how": "independent jobs, each: H2D of its input state from pinned memory, one mm_step, D2H of "
-                           "the result; two plans driven by two host threads on their own streams, so that one "
-                           "job's copies overlap the other's step",
+                           "the result; four plans driven by four host threads on their own streams, so that the "
+                           "copies of some jobs overlap the steps of the others",
+                    "jobs": e2e_pipe["jobs"],
                     "serial": {"value": e2e_value, "steps": e2e_steps,
                                "how": "one plan, one stream: H2D, mm_step, D2H back to back"}},
             "gpu_launches": int(launches),
