@@ -684,6 +684,43 @@ __device__ __forceinline__ void r2c_staged_lines(float2 (&v)[FS<M>::P1], float2*
 template <bool FWD> struct SpecIn { using type = const float2* __restrict__; };
 template <> struct SpecIn<true> { using type = const float2*; };
 
+// L2 prefetch of the stage inputs (base, kp, ep) that the epilogue of rows
+// [row0, row0 + nrow) will read.  Issued at the start of the block, so the lines arrive
+// while its spectrum is loaded and transformed; the epilogue reads them only after it has
+// stored k (the pointers may alias), one dependent round trip per cell that now hits L2.
+// Measured on the 256x256x16 film: RK23 step 505 -> 497-498 us.  Prefetching m and its
+// exchange neighbours as well made the standalone evaluation slower (45.8 -> 47.5 us).
+// Hints only: every address is a cell of the named rows.
+__device__ __forceinline__ void prefetch_l2_range(const float* p, long long n) {
+    if (!p || n <= 0) return;
+    const long long lines = (n * 4 + 127) / 128;
+    for (long long l = threadIdx.x; l < lines; l += blockDim.x) {
+        const long long e = l * 32 < n - 1 ? l * 32 : n - 1;
+        asm volatile("prefetch.global.L2 [%0];\n" ::"l"(p + e));
+    }
+}
+
+template <bool BATCH>
+__device__ __forceinline__ void prefetch_epilogue_rows(const EpiArgs& A, int row0, int nrow) {
+    if (nrow <= 0) return;
+    const int sim = BATCH ? (int)blockIdx.y : 0;
+    const long long off = BATCH ? (long long)sim * A.P.bstride : 0;
+    const DevCtl* ctl = A.ctl ? A.ctl + sim : nullptr;
+    const int cur = ctl ? ctl->cur : 0;
+    const long long N = A.P.N, n2 = A.P.n[2];
+    const StageOp& op = A.op;
+    const long long c0 = (long long)row0 * n2, nc = (long long)nrow * n2;
+    auto streams3 = [&](const float* q) {
+        if (!q) return;
+        for (int c = 0; c < 3; c++) prefetch_l2_range(q + off + c * N + c0, nc);
+    };
+    if (op.do_combine && !op.base_is_cur) streams3(op.base.get(cur));
+    for (int j = 0; j < op.nk && j < MM_MAXK; j++)
+        if (j != op.kcur) streams3(op.kp[j].get(cur));
+    for (int j = 0; j < op.ne && j < MM_MAXK; j++)
+        if (j != op.ecur) streams3(op.ep[j].get(cur));
+}
+
 template <int M, bool TERMS, bool BATCH, bool HALF, bool FWD>
 __device__ __forceinline__ void xinv4_epi_body(typename SpecIn<FWD>::type S, int hp, int L1,
                                                const float2* __restrict__ tw, const EpiArgs& A) {
@@ -692,6 +729,10 @@ __device__ __forceinline__ void xinv4_epi_body(typename SpecIn<FWD>::type S, int
     const DevCtl* ctl = A.ctl ? A.ctl + blockIdx.y : nullptr;
     if (skip_eval(ctl, A.skip_retry)) return;
     S += blockIdx.y * A.spec_bstride;
+    {
+        const int nr = A.P.n[0] * A.P.n[1] - (int)blockIdx.x * RPB;
+        prefetch_epilogue_rows<BATCH>(A, (int)blockIdx.x * RPB, nr < RPB ? nr : RPB);
+    }
     __shared__ SimScalars s_sim;  // this simulation's scalars (BATCH); covered by the barriers below
     if (BATCH && threadIdx.x == 0) stage_scalars(A, ctl, s_sim);
     using F = FS<M>;
@@ -1168,6 +1209,10 @@ __global__ void __launch_bounds__(384) mr_xinv_epi_kernel(const float2* __restri
     const DevCtl* ctl = A.ctl ? A.ctl + blockIdx.y : nullptr;
     if (skip_eval(ctl, A.skip_retry)) return;
     S += blockIdx.y * A.spec_bstride;
+    {
+        const int nr = A.P.n[0] * A.P.n[1] - (int)blockIdx.x * rpb;
+        prefetch_epilogue_rows<BATCH>(A, (int)blockIdx.x * rpb, nr < rpb ? nr : rpb);
+    }
     __shared__ SimScalars s_sim;  // covered by the barriers of the transform
     if (BATCH && threadIdx.x == 0) stage_scalars(A, ctl, s_sim);
     const int M = f.L;
