@@ -798,12 +798,22 @@ __device__ __forceinline__ void xinv4_epi_body(typename SpecIn<FWD>::type S, int
 }
 
 // Single plans: launch bounds alone, so ptxas sizes the registers for the 384-thread tile
-// (78-80 registers); batched plans: two blocks per SM requested explicitly (their
-// staged-scalar variant would otherwise take 136-150 registers and one block).
+// (78-80 registers; the LEAN epilogue 56-69); batched plans: two blocks per SM requested
+// explicitly (their staged-scalar variant would otherwise take 136-150 registers and one
+// block).
 template <int M, bool TERMS, bool HALF, bool FWD, bool LEAN>
 __global__ void __launch_bounds__(384) xinv4_epi_kernel(typename SpecIn<FWD>::type S, int hp, int L1,
                                                         const float2* __restrict__ tw, EpiArgs A) {
     xinv4_epi_body<M, TERMS, false, HALF, FWD, LEAN>(S, hp, L1, tw, A);
+}
+
+// The LEAN epilogue without the next stage's rows fits 56 registers: three blocks per SM
+// requested (RK23 film step 478 -> 476 us; the variant that writes the rows spills at 56
+// and keeps the kernel above, two blocks per SM).
+template <int M, bool HALF>
+__global__ void __launch_bounds__(384, 3) xinv4_epi_lean3_kernel(const float2* __restrict__ S, int hp, int L1,
+                                                                 const float2* __restrict__ tw, EpiArgs A) {
+    xinv4_epi_body<M, false, false, HALF, false, true>(S, hp, L1, tw, A);
 }
 
 template <int M, bool TERMS, bool HALF, bool FWD>
@@ -1309,9 +1319,12 @@ static cudaError_t launch_xinv4_h(const float2* S, int hp, int L1, const float2*
                                   cudaStream_t st, int* nblocks, int nsim) {
     constexpr int RPB = xinv4_rows_c<M, HALF>();
     const size_t smem = (size_t)(RPB * 3 * FS<M>::LBUF + FS<M>::TWT + (FWD ? M / 2 + 1 : 0)) * sizeof(float2);
-    auto kern = BATCH ? xinv4_epi_batch_kernel<M, TERMS, HALF, FWD>
-                      : (!TERMS && lean_epilogue(A.P) ? xinv4_epi_kernel<M, TERMS, HALF, FWD, !TERMS>
-                                                      : xinv4_epi_kernel<M, TERMS, HALF, FWD, false>);
+    auto kern = xinv4_epi_kernel<M, TERMS, HALF, FWD, false>;
+    if (BATCH) kern = xinv4_epi_batch_kernel<M, TERMS, HALF, FWD>;
+    else if (!TERMS && lean_epilogue(A.P)) {
+        if constexpr (FWD) kern = xinv4_epi_kernel<M, false, HALF, true, true>;
+        else kern = xinv4_epi_lean3_kernel<M, HALF>;
+    }
     if (smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
