@@ -122,6 +122,20 @@ __device__ __forceinline__ float3 cell_rhs(const FieldParams& P, const SimScalar
             if (P.n[d] == 1) continue;  // both neighbours clamp onto the cell itself: no contribution
             int lo = nb6(c[d], -1, P.n[d], P.pbc[d]);
             int hi = nb6(c[d], +1, P.n[d], P.pbc[d]);
+            if constexpr (LEAN) {
+                // unit weights (no masks); neighbour offsets in 32 bits from the cell's
+                // component pointers (a simulation holds fewer than 2^31 cells)
+                const int st = d == 0 ? n1 * n2 : (d == 1 ? n2 : 1);
+                const int dl = (lo - c[d]) * st, dh = (hi - c[d]) * st;
+                const float* mc = m + i;
+                const float f = S.ex_pre * P.cinv2[d];
+                float3 a = make_float3(__ldg(mc + dl), __ldg(mc + N + dl), __ldg(mc + 2 * N + dl));
+                float3 b = make_float3(__ldg(mc + dh), __ldg(mc + N + dh), __ldg(mc + 2 * N + dh));
+                hex.x += f * ((a.x - m0.x) + (b.x - m0.x));
+                hex.y += f * ((a.y - m0.y) + (b.y - m0.y));
+                hex.z += f * ((a.z - m0.z) + (b.z - m0.z));
+                continue;
+            }
             long long il = i + (long long)(lo - c[d]) * str[d];
             long long ih = i + (long long)(hi - c[d]) * str[d];
             float l1 = 1.f, l2 = 1.f;
