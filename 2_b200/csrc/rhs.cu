@@ -102,13 +102,16 @@ struct CellTerms {
 // Effective field and torque at one cell.  Returns k (tau/gamma + STT/gamma).
 // m points at this simulation's state, i is the cell within the simulation, mo the
 // offset of the simulation's masks (0 when masks are shared), S its scalars.
-// LEAN: the plan has no per-cell masks and no thermal, Zhang-Li or Slonczewski term (the
-// launcher checks); every mask reads as absent and those terms are compiled out, which
-// leaves the same arithmetic with fewer registers and instructions per cell.
-template <bool LEAN>
-__device__ __forceinline__ const float* lean_mask(const float* q) { return LEAN ? nullptr : q; }
+// SPEC: what the evaluation is known, at compile time, not to have (the launcher checks):
+// SPEC_NOMASK no per-cell mask of any kind (every mask reads as absent, unit exchange
+// weights, 32-bit neighbour offsets), SPEC_NOTHERMAL no thermal term, SPEC_NOSTT no
+// Zhang-Li or Slonczewski term.  The absent parts are compiled out, which leaves the same
+// arithmetic with fewer registers and instructions per cell.  SPEC_LEAN has all three.
+constexpr int SPEC_NOMASK = 1, SPEC_NOTHERMAL = 2, SPEC_NOSTT = 4, SPEC_LEAN = 7;
+template <int SPEC>
+__device__ __forceinline__ const float* lean_mask(const float* q) { return (SPEC & SPEC_NOMASK) ? nullptr : q; }
 
-template <bool WANT_TERMS, bool LEAN = false>
+template <bool WANT_TERMS, int SPEC = 0>
 __device__ __forceinline__ float3 cell_rhs(const FieldParams& P, const SimScalars& S, const float* __restrict__ m,
                                            long long i, long long mo, int z, int y, int x, float3 hd,
                                            long long noise_step, float dt_th, float3& m0, CellTerms* terms) {
@@ -119,7 +122,7 @@ __device__ __forceinline__ float3 cell_rhs(const FieldParams& P, const SimScalar
     if (WANT_TERMS) { terms->hd[0] = hd.x; terms->hd[1] = hd.y; terms->hd[2] = hd.z; }
     if (P.exchange) {
         const int n1 = P.n[1], n2 = P.n[2];
-        const bool masked = !LEAN && (P.msat_mask || P.aex_mask);
+        const bool masked = !(SPEC & SPEC_NOMASK) && (P.msat_mask || P.aex_mask);
         const float lex0 = masked ? fdiv_zero(mval(P.aex_mask, im), mval(P.msat_mask, im)) : 1.0f;
         float3 hex = make_float3(0.f, 0.f, 0.f);
         const int c[3] = {z, y, x};
@@ -129,7 +132,7 @@ __device__ __forceinline__ float3 cell_rhs(const FieldParams& P, const SimScalar
             if (P.n[d] == 1) continue;  // both neighbours clamp onto the cell itself: no contribution
             int lo = nb6(c[d], -1, P.n[d], P.pbc[d]);
             int hi = nb6(c[d], +1, P.n[d], P.pbc[d]);
-            if constexpr (LEAN) {
+            if constexpr ((SPEC & SPEC_NOMASK) != 0) {
                 // unit weights (no masks); neighbour offsets in 32 bits from the cell's
                 // component pointers (a simulation holds fewer than 2^31 cells)
                 const int st = d == 0 ? n1 * n2 : (d == 1 ? n2 : 1);
@@ -161,31 +164,31 @@ __device__ __forceinline__ float3 cell_rhs(const FieldParams& P, const SimScalar
         if (WANT_TERMS) { terms->hex[0] = hex.x; terms->hex[1] = hex.y; terms->hex[2] = hex.z; }
     }
     if (P.zeeman) {
-        float3 hz = make_float3(S.hz[0] * mval(lean_mask<LEAN>(P.bext_mask[0]), im),
-                                S.hz[1] * mval(lean_mask<LEAN>(P.bext_mask[1]), im),
-                                S.hz[2] * mval(lean_mask<LEAN>(P.bext_mask[2]), im));
+        float3 hz = make_float3(S.hz[0] * mval(lean_mask<SPEC>(P.bext_mask[0]), im),
+                                S.hz[1] * mval(lean_mask<SPEC>(P.bext_mask[1]), im),
+                                S.hz[2] * mval(lean_mask<SPEC>(P.bext_mask[2]), im));
         H.x += hz.x; H.y += hz.y; H.z += hz.z;
         if (WANT_TERMS) { terms->hz[0] = hz.x; terms->hz[1] = hz.y; terms->hz[2] = hz.z; }
     }
     if (P.anis) {
-        float msm = mval(lean_mask<LEAN>(P.msat_mask), im);
+        float msm = mval(lean_mask<SPEC>(P.msat_mask), im);
         if (msm == 0.0f) msm = 1.0f;
-        float k2 = (S.kmul / msm) * mval(lean_mask<LEAN>(P.ku_mask), im);
-        float ux = S.anisu[0] * mval(lean_mask<LEAN>(P.anisu_mask[0]), im);
-        float uy = S.anisu[1] * mval(lean_mask<LEAN>(P.anisu_mask[1]), im);
-        float uz = S.anisu[2] * mval(lean_mask<LEAN>(P.anisu_mask[2]), im);
+        float k2 = (S.kmul / msm) * mval(lean_mask<SPEC>(P.ku_mask), im);
+        float ux = S.anisu[0] * mval(lean_mask<SPEC>(P.anisu_mask[0]), im);
+        float uy = S.anisu[1] * mval(lean_mask<SPEC>(P.anisu_mask[1]), im);
+        float uz = S.anisu[2] * mval(lean_mask<SPEC>(P.anisu_mask[2]), im);
         float mu = m0.x * ux + m0.y * uy + m0.z * uz;
         float3 ha = make_float3(k2 * mu * ux, k2 * mu * uy, k2 * mu * uz);
         H.x += ha.x; H.y += ha.y; H.z += ha.z;
         if (WANT_TERMS) { terms->han[0] = ha.x; terms->han[1] = ha.y; terms->han[2] = ha.z; }
     }
-    if (!LEAN && P.thermal) {
-        float ms = mval(P.msat_mask, im);
+    if (!(SPEC & SPEC_NOTHERMAL) && P.thermal) {
+        float ms = mval(lean_mask<SPEC>(P.msat_mask), im);
         float3 ht = make_float3(0.f, 0.f, 0.f);
         if (ms != 0.0f) {
             float eta[3];
             thermal_normals(S.seed, i, noise_step, eta);
-            float a = mval(P.alpha_mask, im), tm = mval(P.temp_mask, im);
+            float a = mval(lean_mask<SPEC>(P.alpha_mask), im), tm = mval(lean_mask<SPEC>(P.temp_mask), im);
             float den = (float)(S.therm_den * (double)dt_th);
             float sc = sqrtf((a * tm * S.therm_num) / (den * ms));
             ht = make_float3(eta[0] * sc, eta[1] * sc, eta[2] * sc);
@@ -194,12 +197,12 @@ __device__ __forceinline__ float3 cell_rhs(const FieldParams& P, const SimScalar
         if (WANT_TERMS) { terms->hth[0] = ht.x; terms->hth[1] = ht.y; terms->hth[2] = ht.z; }
     }
     // LLG torque
-    const float al = S.alpha * mval(lean_mask<LEAN>(P.alpha_mask), im);
+    const float al = S.alpha * mval(lean_mask<SPEC>(P.alpha_mask), im);
     float cx = m0.y * H.z - H.y * m0.z, cy = -m0.x * H.z + H.x * m0.z, cz = m0.x * H.y - H.x * m0.y;
     float dx = -m0.y * cz + cy * m0.z, dy = m0.x * cz - cx * m0.z, dz = -m0.x * cy + cx * m0.y;
     float g = 1.0f / (1.0f + al * al);
     float3 k = make_float3(g * (cx + dx * al), g * (cy + dy * al), g * (cz + dz * al));
-    if (!LEAN && P.zhangli) {
+    if (!(SPEC & SPEC_NOSTT) && P.zhangli) {
         float msat = P.msat_mask ? __ldg(P.msat_mask + im) : 1.0f;
         float3 j0 = make_float3(P.j_mask[0] ? __ldg(P.j_mask[0] + im) * S.jmul[0] : S.jmul[0],
                                 P.j_mask[1] ? __ldg(P.j_mask[1] + im) * S.jmul[1] : S.jmul[1],
@@ -242,7 +245,7 @@ __device__ __forceinline__ float3 cell_rhs(const FieldParams& P, const SimScalar
             k.z += P.inv_gamma * msat * (pred * mxdmxm.z + pret * dmdjxm.z);
         }
     }
-    if (!LEAN && P.slonczewski) {
+    if (!(SPEC & SPEC_NOSTT) && P.slonczewski) {
         float Ms = P.msat_mask ? __ldg(P.msat_mask + im) : 1.0f;
         float3 J = make_float3(P.j_mask[0] ? __ldg(P.j_mask[0] + im) * S.jmul[0] : S.jmul[0],
                                P.j_mask[1] ? __ldg(P.j_mask[1] + im) * S.jmul[1] : S.jmul[1],
@@ -337,7 +340,7 @@ struct ThreadRed {
 
 // stg (optional): receives the next state as the R2C row pass would read it, i.e. the
 // stored value times the Msat mask when fwd_mask (the convolution input Ms_mask * m).
-template <bool LEAN = false>
+template <int SPEC = 0>
 __device__ __forceinline__ void cell_post(const FieldParams& P, const StageOp& op, const ResolvedOp& r, long long i,
                                           long long mo, float3 m0, float3 k, ThreadRed& tr, float3* stg = nullptr,
                                           int fwd_mask = 0) {
@@ -360,7 +363,7 @@ __device__ __forceinline__ void cell_post(const FieldParams& P, const StageOp& o
             v.z += r.ak[j] * kj.z;
         }
         // normalize.cu:14-42 with the Msat mask as norm map
-        float norm = mval(lean_mask<LEAN>(P.msat_mask), i + mo);
+        float norm = mval(lean_mask<SPEC>(P.msat_mask), i + mo);
         float mn = sqrtf(v.x * v.x + v.y * v.y + v.z * v.z);
         float sc = (norm == 0.0f) ? 0.0f : 1.0f;
         sc = (mn != 0.0f) ? sc / mn : 0.0f;
@@ -470,7 +473,7 @@ __device__ __forceinline__ void write_terms(float* const* dbg, long long N, long
 }
 
 // i: cell within the simulation; m, r and the dbg outputs already point at the simulation
-template <bool TERMS, bool LEAN = false>
+template <bool TERMS, int SPEC = 0>
 __device__ __forceinline__ void process_cell(const EpiArgs& A, const SimScalars& S, const float* m,
                                              const ResolvedOp& r, float* const* dbg, long long i, long long mo,
                                              int z, int y, int x, float3 hd, long long ns, float dtth,
@@ -483,8 +486,8 @@ __device__ __forceinline__ void process_cell(const EpiArgs& A, const SimScalars&
         write_terms(dbg, A.P.N, i, t);
         cell_post(A.P, A.op, r, i, mo, m0, k, tr, stg, A.fwd_mask);
     } else {
-        float3 k = cell_rhs<false, LEAN>(A.P, S, m, i, mo, z, y, x, hd, ns, dtth, m0, nullptr);
-        cell_post<LEAN>(A.P, A.op, r, i, mo, m0, k, tr, stg, A.fwd_mask);
+        float3 k = cell_rhs<false, SPEC>(A.P, S, m, i, mo, z, y, x, hd, ns, dtth, m0, nullptr);
+        cell_post<SPEC>(A.P, A.op, r, i, mo, m0, k, tr, stg, A.fwd_mask);
     }
 }
 
@@ -559,7 +562,7 @@ __device__ __forceinline__ const SimScalars& pick_scalars(const SimScalars& stag
 // even x, imaginary part for odd x) of shared-memory line (lrow*3 + c), stride LS.
 // FWD: float x of line (lrow, c) then takes the cell's next state (times the Msat mask
 // when A.fwd_mask) for the R2C rows of the next evaluation (four-step lines only).
-template <bool TERMS, bool PADDED, bool BATCH, bool FWD = false, bool LEAN = false>
+template <bool TERMS, bool PADDED, bool BATCH, bool FWD = false, int SPEC = 0>
 __device__ __forceinline__ void epilogue_rows(const EpiArgs& A, const SimScalars& S, const float2* sm, int LS,
                                               int row0, int nrow_here) {
     static_assert(!(FWD && (PADDED || TERMS)), "row output: four-step lines, no per-term outputs");
@@ -588,13 +591,13 @@ __device__ __forceinline__ void epilogue_rows(const EpiArgs& A, const SimScalars
         if constexpr (FWD) {
             // float x of line (lrow, c) held H_demag of this cell only
             float3 nx = make_float3(0.f, 0.f, 0.f);
-            process_cell<TERMS, LEAN>(A, S, m, r, dbg, i, mo, z, y, x, hd, ns, dtth, tr, &nx);
+            process_cell<TERMS, SPEC>(A, S, m, r, dbg, i, mo, z, y, x, hd, ns, dtth, tr, &nx);
             float* fl = reinterpret_cast<float*>(const_cast<float2*>(sm)) + 2 * (long long)(lrow * 3) * LS + x;
             fl[0] = nx.x;
             fl[2 * LS] = nx.y;
             fl[4 * LS] = nx.z;
         } else {
-            process_cell<TERMS, LEAN>(A, S, m, r, dbg, i, mo, z, y, x, hd, ns, dtth, tr);
+            process_cell<TERMS, SPEC>(A, S, m, r, dbg, i, mo, z, y, x, hd, ns, dtth, tr);
         }
         // advance by blockDim.x cells
         x += dx;
@@ -750,7 +753,7 @@ __device__ __forceinline__ void prefetch_epilogue_rows(const EpiArgs& A, int row
         if (j != op.ecur) streams3(op.ep[j].get(cur));
 }
 
-template <int M, bool TERMS, bool BATCH, bool HALF, bool FWD, bool LEAN>
+template <int M, bool TERMS, bool BATCH, bool HALF, bool FWD, int SPEC>
 __device__ __forceinline__ void xinv4_epi_body(typename SpecIn<FWD>::type S, int hp, int L1,
                                                const float2* __restrict__ tw, const EpiArgs& A) {
     pdl_begin();
@@ -804,7 +807,7 @@ __device__ __forceinline__ void xinv4_epi_body(typename SpecIn<FWD>::type S, int
     }
     __syncthreads();
     const int row0 = blockIdx.x * RPB;
-    epilogue_rows<TERMS, false, BATCH, FWD, LEAN>(A, pick_scalars<BATCH>(s_sim, A.P.s), sm, F::LBUF, row0,
+    epilogue_rows<TERMS, false, BATCH, FWD, SPEC>(A, pick_scalars<BATCH>(s_sim, A.P.s), sm, F::LBUF, row0,
                                             min(RPB, nrows - row0));
     if constexpr (FWD) {
         // R2C rows of the next stage state (float x of line (lr, c) = its value at cell x,
@@ -819,30 +822,30 @@ __device__ __forceinline__ void xinv4_epi_body(typename SpecIn<FWD>::type S, int
 }
 
 // Single plans: launch bounds alone, so ptxas sizes the registers for the 384-thread tile
-// (78-80 registers; the LEAN epilogue 56-69); batched plans: two blocks per SM requested
+// (78-80 registers; the SPEC_LEAN epilogue 56-69); batched plans: two blocks per SM requested
 // explicitly (their staged-scalar variant would otherwise take 136-150 registers and one
 // block).
-template <int M, bool TERMS, bool HALF, bool FWD, bool LEAN>
+template <int M, bool TERMS, bool HALF, bool FWD, int SPEC>
 __global__ void __launch_bounds__(384) xinv4_epi_kernel(typename SpecIn<FWD>::type S, int hp, int L1,
                                                         const float2* __restrict__ tw, EpiArgs A) {
-    xinv4_epi_body<M, TERMS, false, HALF, FWD, LEAN>(S, hp, L1, tw, A);
+    xinv4_epi_body<M, TERMS, false, HALF, FWD, SPEC>(S, hp, L1, tw, A);
 }
 
-// The LEAN epilogue without the next stage's rows fits 56 registers: three blocks per SM
+// The SPEC_LEAN epilogue without the next stage's rows fits 56 registers: three blocks per SM
 // requested (RK23 film step 478 -> 476 us; the variant that writes the rows spills at 56
 // and keeps the kernel above, two blocks per SM).
 template <int M, bool HALF>
 __global__ void __launch_bounds__(384, 3) xinv4_epi_lean3_kernel(const float2* __restrict__ S, int hp, int L1,
                                                                  const float2* __restrict__ tw, EpiArgs A) {
-    xinv4_epi_body<M, false, false, HALF, false, true>(S, hp, L1, tw, A);
+    xinv4_epi_body<M, false, false, HALF, false, SPEC_LEAN>(S, hp, L1, tw, A);
 }
 
-template <int M, bool TERMS, bool HALF, bool FWD>
+template <int M, bool TERMS, bool HALF, bool FWD, int SPEC>
 __global__ void __launch_bounds__(384, M <= 512 ? 2 : 1) xinv4_epi_batch_kernel(typename SpecIn<FWD>::type S,
                                                                                 int hp, int L1,
                                                                                 const float2* __restrict__ tw,
                                                                                 EpiArgs A) {
-    xinv4_epi_body<M, TERMS, true, HALF, FWD, false>(S, hp, L1, tw, A);
+    xinv4_epi_body<M, TERMS, true, HALF, FWD, SPEC>(S, hp, L1, tw, A);
 }
 
 // ---------------------------------------------------------------- stage combine + R2C rows
@@ -1321,18 +1324,20 @@ static int xinv4_rows(int tile) {
     return tile < 0 ? xinv4_rows_c<M, true>() : xinv4_rows_c<M, false>();
 }
 
-// The plan qualifies for the LEAN epilogue: no per-cell mask of any kind and no thermal,
-// Zhang-Li or Slonczewski term.
-static bool lean_epilogue(const FieldParams& P) {
-    if (P.thermal || P.zhangli || P.slonczewski) return false;
+// What the evaluation lacks, as SPEC_* bits: no per-cell mask of any kind, no thermal
+// term, no Zhang-Li or Slonczewski term.
+static int epilogue_spec(const FieldParams& P) {
+    int spec = SPEC_NOMASK;
+    if (!P.thermal) spec |= SPEC_NOTHERMAL;
+    if (!P.zhangli && !P.slonczewski) spec |= SPEC_NOSTT;
     const float* masks[] = {P.msat_mask,      P.aex_mask,      P.alpha_mask,     P.ku_mask,        P.anisu_mask[0],
                             P.anisu_mask[1],  P.anisu_mask[2], P.bext_mask[0],   P.bext_mask[1],   P.bext_mask[2],
                             P.j_mask[0],      P.j_mask[1],     P.j_mask[2],      P.temp_mask,      P.xi_mask,
                             P.zl_pol_mask,    P.p_mask[0],     P.p_mask[1],      P.p_mask[2],      P.sl_pol_mask,
                             P.lambda_mask,    P.eps_prime_mask, P.t_fl_mask};
     for (const float* q : masks)
-        if (q) return false;
-    return true;
+        if (q) spec &= ~SPEC_NOMASK;
+    return spec;
 }
 
 template <int M, bool TERMS, bool BATCH, bool HALF, bool FWD>
@@ -1340,10 +1345,20 @@ static cudaError_t launch_xinv4_h(const float2* S, int hp, int L1, const float2*
                                   cudaStream_t st, int* nblocks, int nsim) {
     constexpr int RPB = xinv4_rows_c<M, HALF>();
     const size_t smem = (size_t)(RPB * 3 * FS<M>::LBUF + FS<M>::TWT + (FWD ? M / 2 + 1 : 0)) * sizeof(float2);
-    auto kern = xinv4_epi_kernel<M, TERMS, HALF, FWD, false>;
-    if (BATCH) kern = xinv4_epi_batch_kernel<M, TERMS, HALF, FWD>;
-    else if (!TERMS && lean_epilogue(A.P)) {
-        if constexpr (FWD) kern = xinv4_epi_kernel<M, false, HALF, true, true>;
+    // Single plans: the SPEC_LEAN kernels when nothing of the three is present, else the
+    // general one.  Batched plans: without thermal and spin-transfer terms (relaxation
+    // pools, masks kept) or without masks and spin-transfer terms (thermal ensembles).
+    const int spec = TERMS ? 0 : epilogue_spec(A.P);
+    auto kern = xinv4_epi_kernel<M, TERMS, HALF, FWD, 0>;
+    if (BATCH) {
+        constexpr int NOTS = SPEC_NOTHERMAL | SPEC_NOSTT, NOMS = SPEC_NOMASK | SPEC_NOSTT;
+        kern = xinv4_epi_batch_kernel<M, TERMS, HALF, FWD, 0>;
+        if constexpr (!TERMS) {
+            if ((spec & NOTS) == NOTS) kern = xinv4_epi_batch_kernel<M, false, HALF, FWD, NOTS>;
+            else if ((spec & NOMS) == NOMS) kern = xinv4_epi_batch_kernel<M, false, HALF, FWD, NOMS>;
+        }
+    } else if (spec == SPEC_LEAN) {
+        if constexpr (FWD) kern = xinv4_epi_kernel<M, false, HALF, true, SPEC_LEAN>;
         else kern = xinv4_epi_lean3_kernel<M, HALF>;
     }
     if (smem > 48 * 1024) {
