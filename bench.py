@@ -625,7 +625,7 @@ def relax_bench(args, rank, world, local_rank, dist):
 
 
 # ---------------------------------------------------------------- single-simulation configs
-def single_bench(args, rank, world, local_rank, dist):
+def single_bench(args, rank, world, local_rank, dist, emit=True):
     """The single-simulation workloads: --workload sp4 (the 128x32x1 film of the SP4
     geometry, RK45, <m> every 10 ps) and --workload wall (the 512x128x1 Neel wall under
     Zhang-Li current, RK45, with the wall position from <m_x> every 10 ps, plus the
@@ -700,7 +700,10 @@ def single_bench(args, rank, world, local_rank, dist):
                 "data": "synthetic", "config": {"workload": first["workload"], "solver": "rk45", "maxerr": 1e-5,
                                                 "parallelism": f"replicas{world}"},
                 "runs": out, "clocks": clocks}
-        print(json.dumps(line), flush=True)
+        if emit:
+            print(json.dumps(line), flush=True)
+        return line
+    return None
 
 
 # ---------------------------------------------------------------- learned warm start
@@ -759,8 +762,9 @@ def warmstart_bench(args, rank, world, local_rank, dist, emit=True):
 def extra_workloads(args, rank, world, local_rank, dist):
     """The other halves of the headline metric, measured in the default run on the same
     GPU after the film: the learned warm start (20,000 training relaxations, 4,096
-    held-out problems relaxed cold and warm, batch 256) and the thermal ensemble (2048
-    simulations of five grid sizes, 200 stochastic Heun steps after 5 warm-up steps).
+    held-out problems relaxed cold and warm, batch 256), the thermal ensemble (2048
+    simulations of five grid sizes, 200 stochastic Heun steps after 5 warm-up steps) and
+    the RK45 single-simulation configurations (SP4 film, Neel wall, Slonczewski disk).
     Each is summarised under its own key; its full line is what --workload prints."""
     import copy
     out = {}
@@ -794,6 +798,18 @@ def extra_workloads(args, rank, world, local_rank, dist):
                            "clocks": en["clocks"], "seconds": time.perf_counter() - t0}
     except Exception as ex:  # reported, not fatal
         out["ensemble"] = {"failed": f"{type(ex).__name__}: {ex}"}
+    # the RK45 single-simulation configurations: the SP4 film (1 ns) and the Neel wall under
+    # Zhang-Li current with the Slonczewski disk (5 ns each)
+    for wl in ("sp4", "wall"):
+        a = copy.copy(args)
+        a.workload, a.duration = wl, 0.0
+        t0 = time.perf_counter()
+        try:
+            sl = single_bench(a, rank, world, local_rank, dist, emit=False)
+            out["rk45_" + wl] = {"metric": "cell-steps/s", "runs": sl["runs"], "clocks": sl["clocks"],
+                                 "seconds": time.perf_counter() - t0}
+        except Exception as ex:  # reported, not fatal
+            out["rk45_" + wl] = {"failed": f"{type(ex).__name__}: {ex}"}
     return out
 
 
