@@ -1348,7 +1348,7 @@ static cudaError_t launch_xinv4_h(const float2* S, int hp, int L1, const float2*
     constexpr int RPB = xinv4_rows_c<M, HALF>();
     const size_t smem = (size_t)(RPB * 3 * FS<M>::LBUF + FS<M>::TWT + (FWD ? M / 2 + 1 : 0)) * sizeof(float2);
     // Single plans: the SPEC_LEAN kernels when nothing of the three is present, else the
-    // general one.  Batched plans: without thermal and spin-transfer terms (relaxation
+    // kernel without what is absent of masks and thermal (see below), else the general one.  Batched plans: without thermal and spin-transfer terms (relaxation
     // pools, masks kept) or without masks and spin-transfer terms (thermal ensembles).
     const int spec = TERMS ? 0 : epilogue_spec(A.P);
     auto kern = xinv4_epi_kernel<M, TERMS, HALF, FWD, 0>;
@@ -1362,6 +1362,12 @@ static cudaError_t launch_xinv4_h(const float2* S, int hp, int L1, const float2*
     } else if (spec == SPEC_LEAN) {
         if constexpr (FWD) kern = xinv4_epi_kernel<M, false, HALF, true, SPEC_LEAN>;
         else kern = xinv4_epi_lean3_kernel<M, HALF>;
+    } else if constexpr (!TERMS) {
+        // masked films without thermal and spin-transfer terms; unmasked ones with a
+        // spin-transfer term and no thermal one (the Neel wall under current)
+        constexpr int NOTS = SPEC_NOTHERMAL | SPEC_NOSTT, NOMT = SPEC_NOMASK | SPEC_NOTHERMAL;
+        if ((spec & NOTS) == NOTS) kern = xinv4_epi_kernel<M, false, HALF, FWD, NOTS>;
+        else if ((spec & NOMT) == NOMT) kern = xinv4_epi_kernel<M, false, HALF, FWD, NOMT>;
     }
     if (smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
