@@ -550,6 +550,33 @@ def relax_bench(args, rank, world, local_rank, dist):
     plan = Plan(problem, masks={"msat": np.concatenate(masks[:B])}, sims=sims[:B], masks_per_sim=True,
                 device=local_rank)
     plan.solver("rk23", dt=1e-14, maxerr=args.relax_maxerr)
+    if args.profile_only:
+        # pass timing of one evaluation and the batched RK23 step, on the plan of B slots
+        # and on the 16-slot plan that finishes a pool (cold states, CUDA events)
+        out = {}
+        for k, p in (("slots%d" % B, plan), ("slots16", None)):
+            if p is None:
+                p = Plan(problem, masks={"msat": np.concatenate(masks[:16])}, sims=sims[:16], masks_per_sim=True,
+                         device=local_rank)
+                p.solver("rk23", dt=1e-14, maxerr=args.relax_maxerr)
+            k_slots = B if p is plan else 16
+            p.set_state(W.cold_state(n, k_slots))
+            p.steps(20)
+            torch.cuda.synchronize()
+            pass_ms = p.profile_eval(args.profile_reps)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            p.steps(300)
+            e1.record()
+            torch.cuda.synchronize()
+            out[k] = {"passes_us": [round(t * 1000, 1) for t in pass_ms], "tiles": p.tiles()[0],
+                      "rk23_step_us": round(e0.elapsed_time(e1) / 300 * 1000, 1)}
+            if p is not plan:
+                p.close()
+        plan.close()
+        if rank == 0:
+            print(json.dumps({"workload": "relax_64x64x1_cold", "profile": out}), flush=True)
+        return None
     sampler = ClockSampler(local_rank)
     sampler.start()
 
@@ -825,9 +852,10 @@ def main():
                     help="skip the reference-kernels-on-this-GPU comparison (RK12) of the film workload")
     ap.add_argument("--profile-reps", type=int, default=10)
     ap.add_argument("--no-extras", action="store_true",
-                    help="film3d: leave out the warm-start and ensemble measurements of the default line")
+                    help="film3d: leave out the warm-start, ensemble and RK45 measurements of the default line")
     ap.add_argument("--profile-only", action="store_true",
-                    help="only time the passes of one field evaluation (few launches; for ncu captures)")
+                    help="film3d: only time the passes of one field evaluation (few launches; for ncu "
+                         "captures); relax: the passes and the batched RK23 step of the pool's plans")
     ap.add_argument("--workload", default="film3d",
                     choices=["film3d", "ensemble", "relax", "sp4", "wall", "warmstart"],
                     help="film3d: the 256x256x16 RK23 film (default); ensemble: 2048 thermal simulations; "
