@@ -1240,13 +1240,29 @@ static cudaError_t launch_xinv_t(const float2* S, int hp, int L1, const float2* 
     return cudaGetLastError();
 }
 
+// What the evaluation lacks, as SPEC_* bits: no per-cell mask of any kind, no thermal
+// term, no Zhang-Li or Slonczewski term.
+static int epilogue_spec(const FieldParams& P) {
+    int spec = SPEC_NOMASK;
+    if (!P.thermal) spec |= SPEC_NOTHERMAL;
+    if (!P.zhangli && !P.slonczewski) spec |= SPEC_NOSTT;
+    const float* masks[] = {P.msat_mask,      P.aex_mask,      P.alpha_mask,     P.ku_mask,        P.anisu_mask[0],
+                            P.anisu_mask[1],  P.anisu_mask[2], P.bext_mask[0],   P.bext_mask[1],   P.bext_mask[2],
+                            P.j_mask[0],      P.j_mask[1],     P.j_mask[2],      P.temp_mask,      P.xi_mask,
+                            P.zl_pol_mask,    P.p_mask[0],     P.p_mask[1],      P.p_mask[2],      P.sl_pol_mask,
+                            P.lambda_mask,    P.eps_prime_mask, P.t_fl_mask};
+    for (const float* q : masks)
+        if (q) spec &= ~SPEC_NOMASK;
+    return spec;
+}
+
 // ---------------------------------------------------------------- mixed-radix C2R + epilogue
 // Row lengths M that are not powers of two: the pre-processing of xinv_epi_kernel, the
 // mixed-radix inverse transform of mixed.cuh, then the same epilogue.  rpb rows of three
 // component lines per block (line (row, c) at sm + (row*3 + c)*M, natural order; the
 // scratch lines follow), blockDim.x / (3 rpb) threads per line.  BATCH: the simulation's
 // scalars are staged in shared memory (batched plans, time tables).
-template <bool TERMS, bool BATCH>
+template <bool TERMS, bool BATCH, int SPEC>
 __global__ void __launch_bounds__(384) mr_xinv_epi_kernel(const float2* __restrict__ S, int hp, int L1, MrLine f,
                                                           const float2* __restrict__ twM,
                                                           const float2* __restrict__ tw2M, EpiArgs A, int rpb) {
@@ -1288,7 +1304,8 @@ __global__ void __launch_bounds__(384) mr_xinv_epi_kernel(const float2* __restri
     }
     mr_fft<+1, float2>(xl, scratch, f, twM, t, nt, active);
     const int row0 = blockIdx.x * rpb;
-    epilogue_rows<TERMS, false, BATCH>(A, pick_scalars<BATCH>(s_sim, A.P.s), sm, M, row0, min(rpb, nrows - row0));
+    epilogue_rows<TERMS, false, BATCH, false, SPEC>(A, pick_scalars<BATCH>(s_sim, A.P.s), sm, M, row0,
+                                                    min(rpb, nrows - row0));
 }
 
 // rows per block and threads per line of the mixed-radix epilogue
@@ -1308,38 +1325,31 @@ static cudaError_t launch_mr_xinv_t(int M, const float2* S, int hp, int L1, cons
     int rpb, nt;
     mr_xinv_shape(M, &rpb, &nt);
     const size_t smem = (size_t)rpb * 6 * M * sizeof(float2);
+    // the epilogue without what the evaluation lacks (as the four-step pass chooses it)
+    auto kern = mr_xinv_epi_kernel<TERMS, BATCH, 0>;
+    if constexpr (!TERMS) {
+        const int spec = epilogue_spec(A.P);
+        constexpr int NOTS = SPEC_NOTHERMAL | SPEC_NOSTT, NOMS = SPEC_NOMASK | SPEC_NOSTT,
+                      NOMT = SPEC_NOMASK | SPEC_NOTHERMAL;
+        if (spec == SPEC_LEAN) kern = mr_xinv_epi_kernel<false, BATCH, SPEC_LEAN>;
+        else if ((spec & NOTS) == NOTS) kern = mr_xinv_epi_kernel<false, BATCH, NOTS>;
+        else if ((spec & NOMS) == NOMS) kern = mr_xinv_epi_kernel<false, BATCH, NOMS>;
+        else if ((spec & NOMT) == NOMT) kern = mr_xinv_epi_kernel<false, BATCH, NOMT>;
+    }
     if (smem > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(mr_xinv_epi_kernel<TERMS, BATCH>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
     }
     const int nrows = A.P.n[0] * A.P.n[1];
     const int blocks = (nrows + rpb - 1) / rpb;
     *nblocks = blocks;
-    mr_xinv_epi_kernel<TERMS, BATCH><<<dim3((unsigned)blocks, (unsigned)nsim), 3 * rpb * nt, smem, st>>>(
-        S, hp, L1, f, twM, tw2M, A, rpb);
+    kern<<<dim3((unsigned)blocks, (unsigned)nsim), 3 * rpb * nt, smem, st>>>(S, hp, L1, f, twM, tw2M, A, rpb);
     return cudaGetLastError();
 }
 
 template <int M>
 static int xinv4_rows(int tile) {
     return tile < 0 ? xinv4_rows_c<M, true>() : xinv4_rows_c<M, false>();
-}
-
-// What the evaluation lacks, as SPEC_* bits: no per-cell mask of any kind, no thermal
-// term, no Zhang-Li or Slonczewski term.
-static int epilogue_spec(const FieldParams& P) {
-    int spec = SPEC_NOMASK;
-    if (!P.thermal) spec |= SPEC_NOTHERMAL;
-    if (!P.zhangli && !P.slonczewski) spec |= SPEC_NOSTT;
-    const float* masks[] = {P.msat_mask,      P.aex_mask,      P.alpha_mask,     P.ku_mask,        P.anisu_mask[0],
-                            P.anisu_mask[1],  P.anisu_mask[2], P.bext_mask[0],   P.bext_mask[1],   P.bext_mask[2],
-                            P.j_mask[0],      P.j_mask[1],     P.j_mask[2],      P.temp_mask,      P.xi_mask,
-                            P.zl_pol_mask,    P.p_mask[0],     P.p_mask[1],      P.p_mask[2],      P.sl_pol_mask,
-                            P.lambda_mask,    P.eps_prime_mask, P.t_fl_mask};
-    for (const float* q : masks)
-        if (q) spec &= ~SPEC_NOMASK;
-    return spec;
 }
 
 template <int M, bool TERMS, bool BATCH, bool HALF, bool FWD>

@@ -1,8 +1,8 @@
 """The specialised C2R epilogues against the general one on the same problem.
 
 A single-simulation plan with no per-cell mask and no thermal or spin-transfer term runs
-the LEAN instantiation of the four-step C2R + epilogue kernels (those terms compiled out,
-32-bit exchange offsets).  An all-ones Msat mask changes no result: every mask factor is
+the LEAN instantiation of the C2R + epilogue kernels, four-step or mixed-radix (those terms
+compiled out, 32-bit exchange offsets).  An all-ones Msat mask changes no result: every mask factor is
 1.0, the exchange weight 2ab/(a+b) of two unit ratios is 1.0 and the normalisation keeps
 its norm map of 1.0.  But it sends the same plan through the general kernels.  Torques and
 RK23 trajectories of the two plans must therefore agree bit for bit, and the LEAN torque
@@ -23,6 +23,8 @@ CASES = [
     dict(n=(16, 64, 64), cell=(2e-9, 4e-9, 4e-9)),
     # periodic in-plane exchange and demag images
     dict(n=(2, 32, 32), cell=(3e-9, 4e-9, 4e-9), pbc=(0, 1, 1)),
+    # padded sizes that are not powers of two (L = 6 x 40 x 56): the mixed-radix C2R pass
+    dict(n=(3, 20, 28), cell=(2e-9, 4e-9, 4e-9)),
 ]
 
 
@@ -51,7 +53,7 @@ def test_lean_torque_bit_identical_and_oracle(case):
     gen.close()
 
 
-@pytest.mark.parametrize("case", CASES[:2])
+@pytest.mark.parametrize("case", CASES[:2] + CASES[3:])
 def test_lean_rk23_steps_bit_identical(case):
     from mumax2 import Plan
     prob = _problem(case)
